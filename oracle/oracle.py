@@ -1,0 +1,234 @@
+"""ctypes view of the CPU oracle (test infrastructure only).
+
+The oracle is a C++ restatement of sesmesh 1.3.2's CPU back end for the SES
+mesh stage (see oracle.hpp).  Only the tests, the smoke check and the
+benchmark's CPU-baseline leg load it; the product never does.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build():
+    """Builds liboracle.so with make (no-op when it is up to date)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        vp, sz, dp, fp = C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_float)
+        u32p, i32p = C.POINTER(C.c_uint32), C.POINTER(C.c_int32)
+        L.orc_engine_new.restype = vp
+        L.orc_engine_new.argtypes = [dp, sz, C.c_double, C.c_double, sz, C.c_char_p, sz]
+        L.orc_engine_free.argtypes = [vp]
+        L.orc_engine_info.argtypes = [vp, dp]
+        L.orc_engine_arrangement.argtypes = [vp, dp, C.POINTER(C.c_uint8), u32p, dp, dp]
+        L.orc_engine_csr.argtypes = [vp, C.c_int, u32p, u32p]
+        L.orc_engine_classify.restype = C.c_long
+        L.orc_engine_classify.argtypes = [vp, i32p, sz, C.POINTER(sz), C.c_char_p, sz]
+        L.orc_engine_sub_states.argtypes = [vp, i32p, sz, C.POINTER(C.c_int8)]
+        L.orc_engine_values.argtypes = [vp, i32p, sz, fp]
+        L.orc_engine_gather.restype = sz
+        L.orc_engine_gather.argtypes = [vp, i32p, C.c_int, u32p, sz]
+        L.orc_mc_brick.argtypes = [C.c_int, fp, u32p, u32p, C.POINTER(sz)]
+        L.orc_engine_field.argtypes = [vp, dp, sz, dp]
+        L.orc_surface_new.restype = vp
+        L.orc_surface_new.argtypes = [dp, sz, C.c_double, C.c_double, sz, C.c_char_p, sz]
+        L.orc_surface_free.argtypes = [vp]
+        L.orc_surface_stats.argtypes = [vp, dp]
+        L.orc_surface_mesh.argtypes = [vp, fp, fp, u32p, u32p, C.POINTER(C.c_uint8)]
+        L.orc_surface_obj.restype = sz
+        L.orc_surface_obj.argtypes = [vp, C.c_char_p, sz]
+        L.orc_obj_of.restype = sz
+        L.orc_obj_of.argtypes = [fp, fp, sz, u32p, sz, C.c_int, C.c_char_p, sz]
+        L.orc_push_fixed.restype = sz
+        L.orc_push_fixed.argtypes = [C.c_float, C.c_int, C.c_char_p, sz]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_threads.restype = C.c_int
+        _LIB = L
+    return _LIB
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def _xyzr(spheres):
+    a = np.ascontiguousarray(spheres, dtype=np.float64).reshape(-1, 4)
+    return a
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def threads():
+    return lib().orc_threads()
+
+
+INFO_KEYS = ("frame_x", "frame_y", "frame_z", "band", "coord_max", "f32_ok", "n_spheres", "n_contained",
+             "n_circles", "n_vertices", "max_expanded", "rho_max", "nb_items", "cb_items", "sub", "nsub",
+             "edge_clamp")
+
+STAT_KEYS = ("touched", "surface_bricks", "vertices", "triangles", "components", "area", "volume", "euler",
+             "refine_evaluations", "t_geometry", "t_classify", "t_mesh", "t_assemble", "t_measure")
+
+
+class Engine:
+    """SesField + Engine of the oracle for one sphere set."""
+
+    def __init__(self, spheres, probe, spacing, brick=10):
+        s = _xyzr(spheres)
+        self._keep = s
+        err = C.create_string_buffer(512)
+        self.h = lib().orc_engine_new(_p(s, C.c_double), len(s), probe, spacing, brick, err, 512)
+        if not self.h:
+            raise ValueError(err.value.decode())
+        self.brick = brick
+        self.info = self._info()
+
+    def _info(self):
+        out = np.zeros(len(INFO_KEYS))
+        lib().orc_engine_info(self.h, _p(out, C.c_double))
+        return dict(zip(INFO_KEYS, out.tolist()))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_engine_free(self.h)
+            self.h = None
+
+    def arrangement(self):
+        n, nc, nv = int(self.info["n_spheres"]), int(self.info["n_circles"]), int(self.info["n_vertices"])
+        sph = np.zeros((n, 5))
+        st = np.zeros(n, np.uint8)
+        orig = np.zeros(n, np.uint32)
+        circ = np.zeros((nc, 12))
+        vert = np.zeros((nv, 6))
+        lib().orc_engine_arrangement(self.h, _p(sph, C.c_double), _p(st, C.c_uint8), _p(orig, C.c_uint32),
+                                     _p(circ, C.c_double), _p(vert, C.c_double))
+        return dict(spheres=sph, status=st, orig=orig, circles=circ, vertices=vert)
+
+    def csr(self, which):
+        rows = int(self.info["n_spheres"] if which == 0 else self.info["n_circles"])
+        total = int(self.info["nb_items"] if which == 0 else self.info["cb_items"])
+        off = np.zeros(rows + 1, np.uint32)
+        items = np.zeros(max(total, 1), np.uint32)
+        lib().orc_engine_csr(self.h, which, _p(off, C.c_uint32), _p(items, C.c_uint32))
+        return off, items[:total]
+
+    def classify(self):
+        err = C.create_string_buffer(512)
+        touched = C.c_size_t(0)
+        n = lib().orc_engine_classify(self.h, None, 0, C.byref(touched), err, 512)
+        if n < 0:
+            raise ValueError(err.value.decode())
+        out = np.zeros((max(n, 1), 3), np.int32)
+        lib().orc_engine_classify(self.h, _p(out, C.c_int32), n, C.byref(touched), err, 512)
+        return out[:n], touched.value
+
+    def sub_states(self, bricks):
+        b = np.ascontiguousarray(bricks, np.int32).reshape(-1, 3)
+        out = np.zeros((len(b), 8), np.int8)
+        lib().orc_engine_sub_states(self.h, _p(b, C.c_int32), len(b), _p(out, C.c_int8))
+        return out
+
+    def values(self, bricks):
+        b = np.ascontiguousarray(bricks, np.int32).reshape(-1, 3)
+        s = self.brick + 1
+        out = np.zeros((len(b), s * s * s), np.float32)
+        lib().orc_engine_values(self.h, _p(b, C.c_int32), len(b), _p(out, C.c_float))
+        return out
+
+    def gather(self, brick, sb):
+        b = np.ascontiguousarray(brick, np.int32).reshape(3)
+        n = lib().orc_engine_gather(self.h, _p(b, C.c_int32), sb, None, 0)
+        w = np.zeros(n, np.uint32)
+        lib().orc_engine_gather(self.h, _p(b, C.c_int32), sb, _p(w, C.c_uint32), n)
+        n_in, n_near, n_s, n_c, n_v, n_sb, n_cb = (int(x) for x in w[:7])
+        pos = 7
+        out = {"n_inside": n_in}
+        for key, cnt in (("near", n_near), ("s", n_s), ("s_off", n_s + 1), ("s_blk", n_sb), ("c", n_c),
+                         ("c_off", n_c + 1), ("c_blk", n_cb), ("v", n_v)):
+            out[key] = w[pos:pos + cnt].copy()
+            pos += cnt
+        return out
+
+    def field(self, pts):
+        p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        out = np.zeros(len(p))
+        lib().orc_engine_field(self.h, _p(p, C.c_double), len(p), _p(out, C.c_double))
+        return out
+
+
+def mc_brick(b, values):
+    v = np.ascontiguousarray(values, np.float32)
+    cap = 3 * b * b * b
+    edges = np.zeros(cap, np.uint32)
+    tris = np.zeros((5 * b * b * b, 3), np.uint32)
+    n = (C.c_size_t * 2)()
+    lib().orc_mc_brick(b, _p(v, C.c_float), _p(edges, C.c_uint32), _p(tris, C.c_uint32), n)
+    return edges[:n[0]], tris[:n[1]]
+
+
+class Surface:
+    """The oracle's whole CPU pipeline (compute_surface, CPU back end)."""
+
+    def __init__(self, spheres, probe, spacing, brick=10):
+        s = _xyzr(spheres)
+        err = C.create_string_buffer(512)
+        self.h = lib().orc_surface_new(_p(s, C.c_double), len(s), probe, spacing, brick, err, 512)
+        if not self.h:
+            raise ValueError(err.value.decode())
+        out = np.zeros(len(STAT_KEYS))
+        lib().orc_surface_stats(self.h, _p(out, C.c_double))
+        self.stats = dict(zip(STAT_KEYS, out.tolist()))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_surface_free(self.h)
+            self.h = None
+
+    def mesh(self):
+        nv, nt = int(self.stats["vertices"]), int(self.stats["triangles"])
+        pos = np.zeros((nv, 3), np.float32)
+        nrm = np.zeros((nv, 3), np.float32)
+        tris = np.zeros((nt, 3), np.uint32)
+        atoms = np.zeros(nv, np.uint32)
+        patches = np.zeros(nv, np.uint8)
+        lib().orc_surface_mesh(self.h, _p(pos, C.c_float), _p(nrm, C.c_float), _p(tris, C.c_uint32),
+                               _p(atoms, C.c_uint32), _p(patches, C.c_uint8))
+        return dict(positions=pos, normals=nrm, triangles=tris, atoms=atoms, patches=patches)
+
+    def obj(self):
+        n = lib().orc_surface_obj(self.h, None, 0)
+        buf = C.create_string_buffer(n)
+        lib().orc_surface_obj(self.h, buf, n)
+        return buf.raw[:n]
+
+
+def obj_of(positions, normals, triangles, precision=4):
+    p = np.ascontiguousarray(positions, np.float32)
+    t = np.ascontiguousarray(triangles, np.uint32)
+    nrm = None if normals is None else np.ascontiguousarray(normals, np.float32)
+    n = lib().orc_obj_of(_p(p, C.c_float), None if nrm is None else _p(nrm, C.c_float), len(p),
+                         _p(t, C.c_uint32), len(t), precision, None, 0)
+    buf = C.create_string_buffer(n)
+    lib().orc_obj_of(_p(p, C.c_float), None if nrm is None else _p(nrm, C.c_float), len(p),
+                     _p(t, C.c_uint32), len(t), precision, buf, n)
+    return buf.raw[:n]
+
+
+def push_fixed(x, prec):
+    buf = C.create_string_buffer(600)
+    n = lib().orc_push_fixed(C.c_float(x), prec, buf, 600)
+    return buf.raw[:n].decode()
