@@ -1,0 +1,165 @@
+/*
+ * sesmesh_b200 — C ABI of the B200 (sm_100a) SES mesh-stage back end.
+ *
+ * The entry points replace sesmesh's CUDA back-end crate
+ * (crates/sesmesh-gpu/src/cuda/*.rs behind the DeviceResident / DeviceBatch
+ * traits of crates/sesmesh-gpu/src/batch.rs:165-236), which
+ * crates/sesmesh/src/field/gpu.rs drives from the mesh stage
+ * (crates/sesmesh/src/surface.rs:953-999).  Each declaration names the
+ * reference interface it stands in for.  Plain pointers and sizes only; all
+ * functions return SMB_OK or an SMB_ERR_* code and write a message to
+ * err[0..errlen) on failure (the reference panics on malformed shapes; this
+ * ABI reports them instead).
+ *
+ * Differences from the reference boundary, each additive:
+ *   - the arrangement is passed in f64 (the reference passes frame-local f32
+ *     copies); brick classes, candidate lists and sample values are then
+ *     computed with the CPU back end's f64 decisions and are bit-identical;
+ *   - brick classification (lattice::touched_bricks / surface_bricks,
+ *     crates/sesmesh/src/field/lattice.rs:105-181) runs on the device;
+ *   - a run also extracts marching-cubes edges and triangle references per
+ *     brick in the host mesher's encoding (crates/sesmesh/src/mesh/
+ *     extract.rs:59-72, 146-265).
+ */
+#ifndef SESMESH_B200_H
+#define SESMESH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    SMB_OK = 0,
+    SMB_ERR_ARG = 1,       /* invalid argument or malformed table */
+    SMB_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    SMB_ERR_NODEVICE = 3,  /* no such device */
+    SMB_ERR_SELFTEST = 4,  /* device arithmetic differs from IEEE */
+    SMB_ERR_RANGE = 5,     /* coordinates beyond the brick key range */
+    SMB_ERR_MEMORY = 6,    /* allocation failed or a list exceeds a limit */
+    SMB_ERR_STATE = 7,     /* call out of order (e.g. run before classify) */
+    SMB_ERR_TIMEOUT = 8    /* a bounded device wait gave up */
+};
+
+typedef struct smb_device smb_device;
+typedef struct smb_resident smb_resident;
+typedef struct smb_batch smb_batch;
+
+typedef struct {
+    char name[256];
+    int major, minor;
+    int multiprocessors;
+    size_t memory;
+} smb_device_info;
+
+/* Opens CUDA device `index` and runs the arithmetic self-test.
+ * Replaces cuda::Runtime::load/open + Device (crates/sesmesh-gpu/src/cuda/
+ * mod.rs:93-240, 418-485) and the K0 self-test (cuda/selftest.rs:16-40). */
+int smb_open(int index, smb_device** out, char* err, size_t errlen);
+void smb_close(smb_device* dev);
+/* Device::info (cuda/mod.rs:418-470). */
+int smb_device_info_get(const smb_device* dev, smb_device_info* out);
+/* Device self-test on n pairs (tests/cuda.rs:65-71 runs 2^20). */
+int smb_self_test(smb_device* dev, uint32_t n, char* err, size_t errlen);
+
+/* A cell grid (GridRef, batch.rs:44-56; CellGrid::parts, geom/cells.rs:86-89):
+ * items of cell c are items[starts[c]..starts[c+1]], cells x-fastest. */
+typedef struct {
+    double origin[3];
+    double cell;
+    uint32_t dims[3];
+    const uint32_t* starts; /* dims[0]*dims[1]*dims[2] + 1 */
+    const uint32_t* items;
+    size_t n_items;
+} smb_grid_ref;
+
+/* The SAS arrangement in sesmesh's internal sphere order (ArrangementRef,
+ * batch.rs:59-83, extended to f64; geom/arrangement.rs:205-228). */
+typedef struct {
+    size_t n_spheres;
+    const double* center;     /* 3 per sphere */
+    const double* expanded;   /* R = r + probe */
+    const double* radius;     /* vdW radius r */
+    const uint32_t* status;   /* 0 exposed, 1 buried, 2 contained */
+    const uint32_t* nb_off;   /* n_spheres + 1: neighbour rows of exposed spheres */
+    const uint32_t* nb_items;
+    size_t n_circles;
+    const double* circle;     /* 10 per circle: centre xyz, axis xyz, e1 xyz, radius */
+    const uint32_t* cb_off;   /* n_circles + 1: circle blockers */
+    const uint32_t* cb_items;
+    size_t n_vertices;
+    const double* vertex;     /* 3 per SAS vertex */
+    smb_grid_ref sphere_grid, circle_grid, vertex_grid;
+    double max_expanded, rho_max, probe;
+} smb_arrangement_ref;
+
+/* The sampling lattice (Lattice, field/lattice.rs:26-45; Engine::new,
+ * field/kernel.rs:204-271).  brick must be even, 4..32 (the device path
+ * splits bricks into 2x2x2 sub-blocks, field/gpu.rs:243-250). */
+typedef struct {
+    double spacing;
+    uint32_t brick;
+    int64_t frame[3]; /* lattice index of the f32 frame origin */
+    double band;      /* sqrt(3) * spacing * 1.01 */
+} smb_lattice_ref;
+
+/* Uploads the arrangement (cuda::Resident::new, cuda/resident.rs:407-480;
+ * tables are validated as batch.rs:323-338 does). */
+int smb_resident_new(smb_device* dev, const smb_arrangement_ref* arr, const smb_lattice_ref* lat,
+                     smb_resident** out, char* err, size_t errlen);
+void smb_resident_free(smb_resident* res);
+/* DeviceResident::resident_bytes (batch.rs:203). */
+size_t smb_resident_bytes(const smb_resident* res);
+
+/* Surface bricks on the device: lattice::touched_bricks + surface_bricks
+ * (field/lattice.rs:105-181, f64).  Keeps the list (packed-key order) on the
+ * device; *touched and *surface get the counts. */
+int smb_classify(smb_resident* res, size_t* touched, size_t* surface, char* err, size_t errlen);
+/* Copies up to cap surface-brick keys (3 int32 each) to out. */
+int smb_resident_bricks(const smb_resident* res, int32_t* out, size_t cap);
+
+/* Empty batch buffers (DeviceResident::new_batch, batch.rs:175-181). */
+int smb_batch_new(smb_resident* res, smb_batch** out, char* err, size_t errlen);
+void smb_batch_free(smb_batch* batch);
+
+/* Device times of one run, milliseconds (BatchTimes, batch.rs:118-129). */
+typedef struct {
+    double substates, gather, sample, mc, total;
+} smb_batch_times;
+
+/* Sub-block classification, candidate gather, field sampling and marching
+ * cubes for surface bricks [first, first + count) of the classified list
+ * (cuda::Resident::run, cuda/resident.rs:494-572, plus the MC pass). */
+int smb_run(smb_resident* res, size_t first, size_t count, smb_batch* batch, smb_batch_times* times, char* err,
+            size_t errlen);
+
+/* Accessors of the last run (DeviceBatch, batch.rs:211-236), copied to
+ * caller memory. */
+size_t smb_batch_bricks(const smb_batch* batch);
+/* SMB_REC_WORDS words per sub-block (8 per brick, sub-block sb = x | y<<1 |
+ * z<<2): state (0 sampled, 1 uniformly outside, 2 inside), ids base,
+ * n_inside, n_near, n_s, n_c, n_v, n_s_blockers, n_c_blockers, pack base,
+ * pack units, flags. */
+#define SMB_REC_WORDS 12
+int smb_batch_records(const smb_batch* batch, uint32_t* out);
+/* (b+1)^3 values per brick, x fastest (DeviceBatch::brick_values). */
+int smb_batch_values(const smb_batch* batch, float* out);
+/* Candidate lists of all sampled sub-blocks: at each record's ids base,
+ * near ids (n_near, those that can contain a sample first), S ids, S
+ * offsets (n_s + 1), S blockers (near positions), C ids, C offsets,
+ * C blockers, V ids -- the lists of Engine::gather_ses (kernel.rs:671-752). */
+size_t smb_batch_ids_words(const smb_batch* batch);
+int smb_batch_ids(const smb_batch* batch, uint32_t* out);
+/* Marching cubes: totals, then per brick (count + 1 offsets) the owned
+ * crossing edges (local ids ((z*b+y)*b+x)*3+axis, ascending), their sample
+ * values (fa, fb) and the triangle references (code << 28 | local id). */
+int smb_batch_mc_counts(const smb_batch* batch, size_t* edges, size_t* triangles);
+int smb_batch_mc(const smb_batch* batch, uint32_t* edge_off, uint32_t* edges, float* edge_vals, uint32_t* tri_off,
+                 uint32_t* tris);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -99,6 +99,19 @@ void orc_engine_csr(void* hp, int which, uint32_t* off, uint32_t* items) {
     if (items && !c.items.empty()) std::memcpy(items, c.items.data(), c.items.size() * 4);
 }
 
+// Cell grid `which` (0 spheres, 1 circle centres, 2 SAS vertices): oc gets
+// origin xyz and cell; dims 3; starts (cells + 1) and items when non-null.
+// Returns the number of cells.
+size_t orc_engine_grid(void* hp, int which, double* oc, uint32_t* dims, uint32_t* starts, uint32_t* items) {
+    const Engine& e = static_cast<Handle*>(hp)->e;
+    const CellGrid& g = which == 0 ? e.field.arr.cells : (which == 1 ? e.field.circle_cells : e.field.vertex_cells);
+    if (oc) oc[0] = g.origin.x, oc[1] = g.origin.y, oc[2] = g.origin.z, oc[3] = g.cell;
+    if (dims) for (int k = 0; k < 3; k++) dims[k] = uint32_t(g.dims[k]);
+    if (starts) std::memcpy(starts, g.starts.data(), g.starts.size() * 4);
+    if (items && !g.items.empty()) std::memcpy(items, g.items.data(), g.items.size() * 4);
+    return g.starts.size() - 1;
+}
+
 // Surface bricks (3 ints each, packed-key order); returns their count, or -1
 // with err set.  *touched gets the touched-brick count.
 long orc_engine_classify(void* hp, int32_t* out, size_t cap, size_t* touched, char* err, size_t errlen) {

@@ -34,6 +34,8 @@ def lib():
         L.orc_engine_info.argtypes = [vp, dp]
         L.orc_engine_arrangement.argtypes = [vp, dp, C.POINTER(C.c_uint8), u32p, dp, dp]
         L.orc_engine_csr.argtypes = [vp, C.c_int, u32p, u32p]
+        L.orc_engine_grid.restype = sz
+        L.orc_engine_grid.argtypes = [vp, C.c_int, dp, u32p, u32p, u32p]
         L.orc_engine_classify.restype = C.c_long
         L.orc_engine_classify.argtypes = [vp, i32p, sz, C.POINTER(sz), C.c_char_p, sz]
         L.orc_engine_sub_states.argtypes = [vp, i32p, sz, C.POINTER(C.c_int8)]
@@ -125,6 +127,17 @@ class Engine:
         items = np.zeros(max(total, 1), np.uint32)
         lib().orc_engine_csr(self.h, which, _p(off, C.c_uint32), _p(items, C.c_uint32))
         return off, items[:total]
+
+    def grid(self, which):
+        n_items = [self.info["n_spheres"], self.info["n_circles"], self.info["n_vertices"]][which]
+        cells = lib().orc_engine_grid(self.h, which, None, None, None, None)
+        oc = np.zeros(4)
+        dims = np.zeros(3, np.uint32)
+        starts = np.zeros(cells + 1, np.uint32)
+        items = np.zeros(max(int(n_items), 1), np.uint32)
+        lib().orc_engine_grid(self.h, which, _p(oc, C.c_double), _p(dims, C.c_uint32), _p(starts, C.c_uint32),
+                              _p(items, C.c_uint32))
+        return dict(origin=oc[:3].copy(), cell=float(oc[3]), dims=dims, starts=starts, items=items[:int(n_items)])
 
     def classify(self):
         err = C.create_string_buffer(512)

@@ -1,0 +1,218 @@
+// Device-side data layout and the f64 geometry shared by the kernels.
+//
+// Every f64 and f32 expression here keeps the operation order of the
+// sesmesh CPU code it restates (left to right, no FMA: the library is built
+// with -fmad=false -prec-div=true -prec-sqrt=true -ftz=false), so brick
+// classes, candidate lists and sample values equal the CPU back end's bit
+// for bit.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace smb {
+
+constexpr double CLASSIFY_EPS = 2e-3;      // field/lattice.rs:20
+constexpr double GEOM_EPS = 1e-9;          // geom/arrangement.rs:26
+constexpr float INSIDE_TOL = 2e-5f;        // field/kernel.rs:40
+constexpr int64_t KEY_BIAS = int64_t(1) << 20;  // field/lattice.rs:15
+
+constexpr uint32_t ST_SAMPLE = 0, ST_OUT = 1, ST_IN = 2;
+constexpr uint32_t STATUS_EXPOSED = 0, STATUS_BURIED = 1, STATUS_CONTAINED = 2;
+
+// Record words per sub-block (see include/sesmesh_b200.h).
+constexpr int REC_WORDS = 12;
+enum RecWord {
+    R_STATE = 0, R_IDS = 1, R_INSIDE = 2, R_NEAR = 3, R_S = 4, R_C = 5, R_V = 6, R_SBLK = 7, R_CBLK = 8,
+    R_PACK = 9, R_PACKLEN = 10, R_FLAGS = 11
+};
+constexpr uint32_t REC_OVERFLOW = 1;
+
+// A cell grid over points (geom/cells.rs:12): items of cell c are
+// items[starts[c]..starts[c+1]], cells x-fastest.
+struct DGrid {
+    double ox, oy, oz, cell;
+    uint32_t dx, dy, dz, pad;
+    const uint32_t* starts;
+    const uint32_t* items;
+};
+
+// The resident arrangement, internal (Morton) sphere order.
+struct DArr {
+    uint32_t n, nc, nv, pad;
+    const double4* sph;      // centre x, y, z, expanded radius R
+    const double* rvdw;      // vdW radius r
+    const uint32_t* status;  // STATUS_*
+    const uint32_t* nb_off;  // class-S blockers: neighbour CSR of exposed spheres
+    const uint32_t* nb_items;
+    const double* circ;      // 12 per circle: centre xyz, axis xyz, e1 xyz, radius, 0, 0
+    const uint32_t* cb_off;  // circle blocker CSR
+    const uint32_t* cb_items;
+    const double4* vert;     // SAS vertex x, y, z, 0
+    DGrid gs, gc, gv;
+    double max_expanded, rho_max, probe;
+};
+
+// Lattice and sampling constants (field/lattice.rs:26-45, kernel.rs:204-271).
+struct DLat {
+    double h;
+    double fx, fy, fz;       // frame origin (a lattice point), f64
+    long long frame[3];      // lattice index of the frame origin
+    double band;             // sqrt(3) h 1.01
+    double rho_sub;          // 0.5 sqrt(3) sub h
+    double rho_brick;        // 0.5 sqrt(3) b h
+    float h32, band32, probe32, cutoff2;
+    int b, sub, spb, pad;    // brick edge, sub-block edge, samples per brick
+};
+
+// geom/cells.rs:91-104 on one axis.
+__device__ __forceinline__ uint32_t cell_coord(double p, double o, double cell, uint32_t dim) {
+    double c = floor((p - o) / cell);
+    if (!(c > 0.0)) return 0;
+    if (c >= double(dim - 1)) return dim - 1;
+    return uint32_t(c);
+}
+
+struct CellBox {
+    uint32_t x0, x1, y0, y1, z0, z1;
+};
+
+// The cells overlapping the cube of half-size r around (x, y, z)
+// (geom/cells.rs:113-130: coord(center - r) .. coord(center + r)).
+__device__ __forceinline__ CellBox cell_box(const DGrid& g, double x, double y, double z, double r) {
+    CellBox b;
+    b.x0 = cell_coord(x - r, g.ox, g.cell, g.dx);
+    b.y0 = cell_coord(y - r, g.oy, g.cell, g.dy);
+    b.z0 = cell_coord(z - r, g.oz, g.cell, g.dz);
+    b.x1 = cell_coord(x + r, g.ox, g.cell, g.dx);
+    b.y1 = cell_coord(y + r, g.oy, g.cell, g.dy);
+    b.z1 = cell_coord(z + r, g.oz, g.cell, g.dz);
+    return b;
+}
+
+// |a - b| as Vec3::dist computes it (geom/vec.rs:27-55).
+__device__ __forceinline__ double dist3(double ax, double ay, double az, double bx, double by, double bz) {
+    double dx = ax - bx, dy = ay - by, dz = az - bz;
+    return sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+__device__ __forceinline__ double warp_min(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Lanes stride over the items of each row of the box: every item of the box
+// is visited once, by some lane.
+template <class F>
+__device__ __forceinline__ void warp_for_near(const DGrid& g, double x, double y, double z, double r, int lane, F&& f) {
+    CellBox bx = cell_box(g, x, y, z, r);
+    for (uint32_t zc = bx.z0; zc <= bx.z1; zc++)
+        for (uint32_t yc = bx.y0; yc <= bx.y1; yc++) {
+            size_t row = (size_t(zc) * g.dy + yc) * g.dx;
+            uint32_t a = g.starts[row + bx.x0], e = g.starts[row + bx.x1 + 1];
+            for (uint32_t i = a + lane; i < e; i += 32) f(g.items[i]);
+        }
+}
+
+// SesField::try_sphere_with (field/point.rs:422-444): the candidate's
+// distance if its radial projection is unblocked and below best, else best.
+__device__ __forceinline__ double try_sphere(const DArr& A, double x, double y, double z, uint32_t i, double best) {
+    double4 c = A.sph[i];
+    double vx = x - c.x, vy = y - c.y, vz = z - c.z;
+    double len = sqrt(vx * vx + vy * vy + vz * vz);
+    double lb = fabs(len - c.w);
+    if (lb >= best || len < 1e-12) return best;
+    double s = c.w / len;
+    double qx = c.x + vx * s, qy = c.y + vy * s, qz = c.z + vz * s;
+    for (uint32_t p = A.nb_off[i], e = A.nb_off[i + 1]; p < e; p++) {
+        double4 k = A.sph[A.nb_items[p]];
+        if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - GEOM_EPS)) return best;
+    }
+    return lb;
+}
+
+// SesField::try_circle_with (field/point.rs:452-476).
+__device__ __forceinline__ double try_circle(const DArr& A, double x, double y, double z, uint32_t ci, double best) {
+    const double* c = A.circ + 12 * size_t(ci);
+    double yx = x - c[0], yy = y - c[1], yz = z - c[2];
+    double along = yx * c[3] + yy * c[4] + yz * c[5];
+    double wx = yx - c[3] * along, wy = yy - c[4] * along, wz = yz - c[5] * along;
+    double wl = sqrt(wx * wx + wy * wy + wz * wz);
+    double t = wl - c[9];
+    double dist = sqrt(along * along + t * t);
+    if (dist >= best) return best;
+    double dx, dy, dz;
+    if (wl > 1e-12) {
+        dx = wx / wl, dy = wy / wl, dz = wz / wl;
+    } else {
+        dx = c[6], dy = c[7], dz = c[8];
+    }
+    double qx = c[0] + dx * c[9], qy = c[1] + dy * c[9], qz = c[2] + dz * c[9];
+    for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++) {
+        double4 k = A.sph[A.cb_items[p]];
+        if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - GEOM_EPS)) return best;
+    }
+    return dist;
+}
+
+// Distance from (x, y, z) to the circle ci as gather_ses / gather_local
+// compute it for the reach test (field/kernel.rs:714-722).
+__device__ __forceinline__ double circle_reach_dist(const DArr& A, double x, double y, double z, uint32_t ci) {
+    const double* c = A.circ + 12 * size_t(ci);
+    double yx = x - c[0], yy = y - c[1], yz = z - c[2];
+    double along = yx * c[3] + yy * c[4] + yz * c[5];
+    double wx = yx - c[3] * along, wy = yy - c[4] * along, wz = yz - c[5] * along;
+    double wl = sqrt(wx * wx + wy * wy + wz * wz);
+    return sqrt(along * along + (wl - c[9]) * (wl - c[9]));
+}
+
+// SesField::ses_eval distance (field/point.rs:385-411), one warp.  The result
+// is min(cutoff, min over unblocked candidates), which does not depend on the
+// visiting order, so lanes keep partial minima that are merged at the end.
+__device__ inline double ses_eval_warp(const DArr& A, double x, double y, double z, double cutoff, int lane) {
+    bool inside = false;
+    warp_for_near(A.gs, x, y, z, A.max_expanded, lane, [&](uint32_t k) {
+        if (!inside && A.status[k] != STATUS_CONTAINED) {
+            double4 c = A.sph[k];
+            if (dist3(x, y, z, c.x, c.y, c.z) < c.w) inside = true;
+        }
+    });
+    if (!__any_sync(0xffffffffu, inside)) return 0.0;
+    double best = cutoff;
+    warp_for_near(A.gs, x, y, z, cutoff + A.max_expanded, lane, [&](uint32_t i) {
+        if (A.status[i] == STATUS_EXPOSED) best = try_sphere(A, x, y, z, i, best);
+    });
+    best = warp_min(best);
+    warp_for_near(A.gc, x, y, z, cutoff + A.rho_max, lane, [&](uint32_t ci) { best = try_circle(A, x, y, z, ci, best); });
+    warp_for_near(A.gv, x, y, z, cutoff, lane, [&](uint32_t vi) {
+        double4 p = A.vert[vi];
+        double d = dist3(x, y, z, p.x, p.y, p.z);
+        if (d < best) best = d;
+    });
+    return warp_min(best);
+}
+
+// lattice::uniform_sign (field/lattice.rs:190-227), one warp: 1 uniformly
+// outside, 0 uniformly inside, -1 the surface may pass.
+__device__ inline int uniform_sign_warp(const DArr& A, double x, double y, double z, double rho, int lane) {
+    double margin = rho + CLASSIFY_EPS;
+    double s_sas = __longlong_as_double(0x7ff0000000000000LL), s_vdw = s_sas;
+    warp_for_near(A.gs, x, y, z, margin + A.max_expanded, lane, [&](uint32_t k) {
+        if (A.status[k] != STATUS_CONTAINED) {
+            double4 c = A.sph[k];
+            double d = dist3(x, y, z, c.x, c.y, c.z);
+            s_sas = fmin(s_sas, d - c.w);
+            s_vdw = fmin(s_vdw, d - A.rvdw[k]);
+        }
+    });
+    s_sas = warp_min(s_sas);
+    s_vdw = warp_min(s_vdw);
+    if (s_sas >= margin) return 1;
+    if (s_vdw <= -margin) return 0;
+    double cutoff = A.probe + margin + CLASSIFY_EPS;
+    double v = A.probe - ses_eval_warp(A, x, y, z, cutoff, lane);
+    if (v > margin) return 1;
+    if (v < -margin) return 0;
+    return -1;
+}
+
+}  // namespace smb

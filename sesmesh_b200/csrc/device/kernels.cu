@@ -1,0 +1,840 @@
+// sm_100a kernels of the SES mesh stage: brick classification (a), ordered
+// candidate gather (b), exact field sampling with TMA-staged candidates (c),
+// marching-cubes edge/cell compaction (d).  Host launchers at the end.
+//
+// Numerics: built with -fmad=false -prec-div=true -prec-sqrt=true
+// -ftz=false.  f64 decisions (classification, list membership, list order)
+// and f32 sample values follow the CPU back end of sesmesh 1.3.2
+// operation by operation, so every output is bit-identical to it.
+#include <cstdio>
+
+#include "common.cuh"
+#include "kernels.hpp"
+#include "scan.cuh"
+#define SMB_MC_QUAL __constant__
+#include "../mc_table.inc"
+
+namespace smb {
+
+// ---------------------------------------------------------------------------
+// Arithmetic self-test: IEEE f32 and f64 operations whose results the host
+// recomputes; a build with contracted multiply-adds or approximate division
+// or square root fails it.  Eight f32 and four f64 results per pair.
+__global__ void k_selftest(const float* a, const float* b, uint32_t* out, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float x = a[i], y = b[i];
+    float dx = x - y, dy = y * 0.75f - x, dz = x * y - 1.0f;
+    float d = sqrtf(dx * dx + dy * dy + dz * dz);
+    float r[8] = {x + y, x * y, x / y, sqrtf(fabsf(x)), d, (d - y) / d, fminf(x, y), fabsf(d - fabsf(y))};
+    for (int k = 0; k < 8; k++) out[12 * i + k] = __float_as_uint(r[k]);
+    double X = double(x) * 1.0000001, Y = double(y) - 0.3;
+    double D = X * Y + X, E = sqrt(fabs(X * X + Y * Y - X)), F = X / (Y + 2.5), G = floor(X * 3.7);
+    double rr[4] = {D, E, F, G};
+    for (int k = 0; k < 4; k++) {
+        unsigned long long u = __double_as_longlong(rr[k]);
+        out[12 * i + 8 + k] = uint32_t(u ^ (u >> 32));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Device-wide exclusive scan of u32 values (three passes over tiles).
+__global__ void k_scan_tiles(const uint32_t* in, uint32_t n, unsigned long long* tile_sums) {
+    __shared__ unsigned long long sh[SCAN_THREADS / 32];
+    uint64_t base = uint64_t(blockIdx.x) * SCAN_TILE;
+    unsigned long long s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        uint64_t i = base + uint64_t(k) * SCAN_THREADS + threadIdx.x;
+        if (i < n) s += in[i];
+    }
+    unsigned long long total;
+    block_exclusive_scan<SCAN_THREADS>(s, sh, &total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_tile_sums(unsigned long long* tile_sums, uint32_t n_tiles, unsigned long long* total) {
+    __shared__ unsigned long long sh[SCAN_THREADS / 32];
+    unsigned long long carry = 0;
+    for (uint32_t b0 = 0; b0 < n_tiles; b0 += SCAN_THREADS) {
+        uint32_t i = b0 + threadIdx.x;
+        unsigned long long v = i < n_tiles ? tile_sums[i] : 0, t;
+        unsigned long long e = block_exclusive_scan<SCAN_THREADS>(v, sh, &t);
+        if (i < n_tiles) tile_sums[i] = carry + e;
+        carry += t;
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// out[i] = exclusive prefix of in; with keep != null, also writes the
+// indices i with in[i] != 0 to keep[prefix] (order-preserving compaction).
+__global__ void k_scan_apply(const uint32_t* in, uint32_t n, const unsigned long long* tile_sums, uint32_t* out,
+                             uint32_t* keep) {
+    __shared__ unsigned long long sh[SCAN_THREADS / 32];
+    uint64_t base = uint64_t(blockIdx.x) * SCAN_TILE + uint64_t(threadIdx.x) * SCAN_ITEMS;
+    uint32_t v[SCAN_ITEMS];
+    unsigned long long s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        uint64_t i = base + k;
+        v[k] = i < n ? in[i] : 0u;
+        s += v[k];
+    }
+    unsigned long long t;
+    unsigned long long run = tile_sums[blockIdx.x] + block_exclusive_scan<SCAN_THREADS>(s, sh, &t);
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        uint64_t i = base + k;
+        if (i < n) {
+            if (out) out[i] = uint32_t(run);
+            if (keep && v[k]) keep[run] = uint32_t(i);
+        }
+        run += v[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// (a) Classification.
+__device__ __forceinline__ long long sat_floor(double v) {
+    double f = floor(v);
+    if (isnan(f)) return 0;
+    if (f <= -9.2e18) return LLONG_MIN;
+    if (f >= 9.2e18) return LLONG_MAX;
+    return (long long)f;
+}
+
+// lattice::touched_bricks (field/lattice.rs:105-163): every non-contained
+// sphere marks the bricks its ball of radius R + CLASSIFY_EPS overlaps, in a
+// dense flag grid over the bricks' bounding box.
+__global__ void k_mark_touched(DArr A, DLat L, BrickBox box, uint32_t* flags, int* err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.n || A.status[i] == STATUS_CONTAINED) return;
+    double4 c = A.sph[i];
+    double r = c.w + CLASSIFY_EPS;
+    double bh = double(L.b) * L.h;
+    long long lo[3] = {sat_floor((c.x - r) / bh), sat_floor((c.y - r) / bh), sat_floor((c.z - r) / bh)};
+    long long hi[3] = {sat_floor((c.x + r) / bh), sat_floor((c.y + r) / bh), sat_floor((c.z + r) / bh)};
+    for (int a = 0; a < 3; a++) {
+        if (llabs(lo[a]) >= KEY_BIAS - 1 || llabs(hi[a]) >= KEY_BIAS - 1) {
+            atomicExch(err, ERR_KEY_RANGE);
+            return;
+        }
+        if (lo[a] < box.lo[a] || hi[a] > box.lo[a] + (long long)box.n[a] - 1) {
+            atomicExch(err, ERR_BOX);
+            return;
+        }
+    }
+    for (long long z = lo[2]; z <= hi[2]; z++)
+        for (long long y = lo[1]; y <= hi[1]; y++)
+            for (long long x = lo[0]; x <= hi[0]; x++)
+                flags[((uint64_t(z - box.lo[2]) * box.n[1]) + uint64_t(y - box.lo[1])) * box.n[0] + uint64_t(x - box.lo[0])] = 1;
+}
+
+__device__ __forceinline__ void cell_key(const BrickBox& box, uint32_t cell, int k[3]) {
+    k[0] = int(box.lo[0] + cell % box.n[0]);
+    k[1] = int(box.lo[1] + (cell / box.n[0]) % box.n[1]);
+    k[2] = int(box.lo[2] + cell / (box.n[0] * box.n[1]));
+}
+
+// lattice::surface_bricks (field/lattice.rs:168-181): the exact f64 test at
+// each touched brick's centre, one warp per brick.
+__global__ void k_classify_bricks(DArr A, DLat L, BrickBox box, const uint32_t* touched, uint32_t n_touched,
+                                  uint32_t* surface) {
+    uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (w >= n_touched) return;
+    uint32_t cell = touched[w];
+    int k[3];
+    cell_key(box, cell, k);
+    double bh = double(L.b);
+    double cx = (double(k[0]) + 0.5) * bh * L.h, cy = (double(k[1]) + 0.5) * bh * L.h, cz = (double(k[2]) + 0.5) * bh * L.h;
+    int s = uniform_sign_warp(A, cx, cy, cz, L.rho_brick, lane);
+    if (lane == 0) surface[cell] = s < 0 ? 1u : 0u;
+}
+
+__global__ void k_cells_to_keys(BrickBox box, const uint32_t* cells, uint32_t n, int4* keys) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int k[3];
+    cell_key(box, cells[i], k);
+    keys[i] = make_int4(k[0], k[1], k[2], 0);
+}
+
+// Owner of a brick sample (Engine::assign, field/kernel.rs:489-546): the
+// first sub-block in (z, y, x) order that contains the sample and is not
+// uniform; -1 if all containing sub-blocks are uniform, then *positive is
+// the sign of the last one visited.
+__device__ __forceinline__ int sample_owner(int x, int y, int z, int sub, const uint32_t st[8], bool* positive) {
+    auto range = [&](int v, int& lo, int& hi) {
+        hi = min(v / sub, 1);
+        lo = (v > 0 && v % sub == 0) ? min(v / sub - 1, 1) : hi;
+    };
+    int x0, x1, y0, y1, z0, z1;
+    range(x, x0, x1);
+    range(y, y0, y1);
+    range(z, z0, z1);
+    bool pos = true;
+    for (int sz = z0; sz <= z1; sz++)
+        for (int sy = y0; sy <= y1; sy++)
+            for (int sx = x0; sx <= x1; sx++) {
+                int sb = sx + 2 * sy + 4 * sz;
+                if (st[sb] == ST_SAMPLE) return sb;
+                pos = st[sb] == ST_OUT;
+            }
+    *positive = pos;
+    return -1;
+}
+
+// Engine::sub_states (field/kernel.rs:467-482), one warp per sub-block of a
+// brick, then the +-band values of samples no sampled sub-block owns.
+__global__ void __launch_bounds__(256) k_substates(DArr A, DLat L, const int4* keys, uint32_t n_bricks, uint32_t* rec,
+                                                   uint32_t* sampled, float* values) {
+    __shared__ uint32_t st[8];
+    uint32_t brick = blockIdx.x;
+    if (brick >= n_bricks) return;
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int4 key = keys[brick];
+    double h = L.h, sub = double(L.sub), half = double(L.sub) * 0.5;
+    double bx = double((long long)key.x * L.b) * h, by = double((long long)key.y * L.b) * h,
+           bz = double((long long)key.z * L.b) * h;
+    double ox = double(w & 1) * sub + half, oy = double((w >> 1) & 1) * sub + half, oz = double((w >> 2) & 1) * sub + half;
+    int s = uniform_sign_warp(A, bx + ox * h, by + oy * h, bz + oz * h, L.rho_sub, lane);
+    if (lane == 0) {
+        uint32_t state = s < 0 ? ST_SAMPLE : (s == 1 ? ST_OUT : ST_IN);
+        st[w] = state;
+        uint32_t j = brick * 8 + w;
+        uint32_t* r = rec + size_t(j) * REC_WORDS;
+        for (int q = 0; q < REC_WORDS; q++) r[q] = 0;
+        r[R_STATE] = state;
+        sampled[j] = state == ST_SAMPLE ? 1u : 0u;
+    }
+    __syncthreads();
+    uint32_t sts[8];
+    for (int q = 0; q < 8; q++) sts[q] = st[q];
+    int side = L.b + 1;
+    float* v = values + size_t(brick) * L.spb;
+    for (int i = threadIdx.x; i < L.spb; i += blockDim.x) {
+        int x = i % side, y = (i / side) % side, z = i / (side * side);
+        bool positive;
+        if (sample_owner(x, y, z, L.sub, sts, &positive) < 0) v[i] = positive ? L.band32 : -L.band32;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// (b) Candidate gather, one warp per sampled sub-block (Engine::gather_ses,
+// field/kernel.rs:671-752, with gather_near :614-651).  Lists keep the CPU's
+// order: near spheres in cell-scan order, those that can contain a sample
+// first; S by (lb, index) and C by (distance, index), both f64; V in
+// cell-scan order.  Blockers are near-list positions.
+
+__device__ __forceinline__ int warp_append(bool p, int& count) {
+    unsigned m = __ballot_sync(0xffffffffu, p);
+    int lane = threadIdx.x & 31;
+    int pos = count + __popc(m & ((1u << lane) - 1u));
+    count += __popc(m);
+    return p ? pos : -1;
+}
+
+// All lanes run the same iterations (item valid or not), so warp_append
+// sees the items in scan order.
+template <class F>
+__device__ __forceinline__ void warp_scan_box(const DGrid& g, double x, double y, double z, double r, int lane, F&& f) {
+    CellBox bx = cell_box(g, x, y, z, r);
+    for (uint32_t zc = bx.z0; zc <= bx.z1; zc++)
+        for (uint32_t yc = bx.y0; yc <= bx.y1; yc++) {
+            size_t row = (size_t(zc) * g.dy + yc) * g.dx;
+            uint32_t a = g.starts[row + bx.x0], e = g.starts[row + bx.x1 + 1];
+            for (uint32_t b = a; b < e; b += 32) {
+                uint32_t i = b + lane;
+                bool valid = i < e;
+                f(valid, valid ? g.items[i] : 0u);
+            }
+        }
+}
+
+__device__ __forceinline__ int lookup_local(const uint32_t* sorted_ids, const uint32_t* sorted_loc, int n, uint32_t id) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (sorted_ids[mid] < id) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && sorted_ids[lo] == id) ? int(sorted_loc[lo]) : -1;
+}
+
+__device__ __forceinline__ unsigned warp_inclusive_scan(unsigned v) {
+    int lane = threadIdx.x & 31;
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+    }
+    return v;
+}
+
+
+__global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
+                         GatherCaps caps) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t item = blockIdx.x * (blockDim.x >> 5) + wib;
+    if (item >= n_work) return;
+    unsigned char* base = smem_raw + size_t(wib) * gather_smem_bytes(caps);
+    double* s_key = reinterpret_cast<double*>(base);
+    double* c_key = s_key + caps.s;
+    uint32_t* near_ids = reinterpret_cast<uint32_t*>(c_key + caps.c);
+    uint32_t* sorted_ids = near_ids + caps.near;
+    uint32_t* sorted_loc = sorted_ids + caps.near;
+    uint32_t* s_id = sorted_loc + caps.near;
+    uint32_t* s_loc = s_id + caps.s;
+    uint32_t* s_perm = s_loc + caps.s;
+    uint32_t* s_off = s_perm + caps.s;
+    uint32_t* c_id = s_off + caps.s + 1;
+    uint32_t* c_perm = c_id + caps.c;
+    uint32_t* c_off = c_perm + caps.c;
+    uint32_t* v_id = c_off + caps.c + 1;
+
+    const uint32_t j = work[item];
+    const uint32_t brick = j >> 3, sb = j & 7;
+    uint32_t* rec = O.rec + size_t(j) * REC_WORDS;
+    const int4 key = keys[brick];
+    // Sub-block centre as Engine::prepare_sub computes it (kernel.rs:575-583).
+    const double h = L.h, sub = double(L.sub), half = double(L.sub) * 0.5;
+    const double px = double((long long)key.x * L.b) * h, py = double((long long)key.y * L.b) * h,
+                 pz = double((long long)key.z * L.b) * h;
+    const double bx = px + (double(sb & 1) * sub + half) * h, by = py + (double((sb >> 1) & 1) * sub + half) * h,
+                 bz = pz + (double((sb >> 2) & 1) * sub + half) * h;
+    const double rho = L.rho_sub;
+    const double reach = A.probe + L.band + rho;
+
+    if (lane == 0) rec[R_FLAGS] = 0;
+    auto overflow = [&](uint32_t bit) {
+        if (lane == 0) {
+            rec[R_FLAGS] |= bit;
+            unsigned long long q = atomicAdd(&O.counters[bit == REC_OVERFLOW ? CNT_OVERFLOW : CNT_NOMEM], 1ull);
+            if (bit == REC_OVERFLOW && O.retry) O.retry[q] = j;
+        }
+    };
+
+    // Near spheres, two passes (gather_near).
+    int nn = 0, n_in = 0;
+    for (int pass = 0; pass < 2; pass++) {
+        warp_scan_box(A.gs, bx, by, bz, reach + A.max_expanded, lane, [&](bool valid, uint32_t k) {
+            bool keep = false;
+            if (valid && A.status[k] != STATUS_CONTAINED) {
+                double4 c = A.sph[k];
+                double d = dist3(bx, by, bz, c.x, c.y, c.z);
+                bool contains = d < c.w + rho;
+                keep = !(d >= c.w + reach) && (contains == (pass == 0));
+            }
+            int pos = warp_append(keep, nn);
+            if (pos >= 0 && pos < caps.near) near_ids[pos] = k;
+        });
+        if (pass == 0) n_in = nn;
+    }
+    if (nn > caps.near) return overflow(REC_OVERFLOW);
+    __syncwarp();
+    // Sorted copy of the near ids for blocker lookups.
+    for (int i = lane; i < nn; i += 32) {
+        uint32_t id = near_ids[i];
+        int rank = 0;
+        for (int q = 0; q < nn; q++) rank += near_ids[q] < id;
+        sorted_ids[rank] = id;
+        sorted_loc[rank] = uint32_t(i);
+    }
+    // Class S candidates among the near spheres.
+    int ns = 0;
+    for (int b0 = 0; b0 < nn; b0 += 32) {
+        int i = b0 + lane;
+        bool p = false;
+        double lb = 0;
+        uint32_t k = 0;
+        if (i < nn) {
+            k = near_ids[i];
+            if (A.status[k] == STATUS_EXPOSED) {
+                double4 c = A.sph[k];
+                lb = fabs(dist3(bx, by, bz, c.x, c.y, c.z) - c.w);
+                p = lb <= reach;
+            }
+        }
+        int pos = warp_append(p, ns);
+        if (pos >= 0 && pos < caps.s) s_key[pos] = lb, s_id[pos] = k, s_loc[pos] = uint32_t(i);
+    }
+    // Class C candidates.
+    int nc = 0;
+    warp_scan_box(A.gc, bx, by, bz, reach + A.rho_max, lane, [&](bool valid, uint32_t ci) {
+        double d = valid ? circle_reach_dist(A, bx, by, bz, ci) : 0.0;
+        bool p = valid && d <= reach;
+        int pos = warp_append(p, nc);
+        if (pos >= 0 && pos < caps.c) c_key[pos] = d, c_id[pos] = ci;
+    });
+    // Class V, cell-scan order.
+    int nv = 0;
+    warp_scan_box(A.gv, bx, by, bz, reach, lane, [&](bool valid, uint32_t vi) {
+        bool p = false;
+        if (valid) {
+            double4 q = A.vert[vi];
+            p = dist3(bx, by, bz, q.x, q.y, q.z) <= reach;
+        }
+        int pos = warp_append(p, nv);
+        if (pos >= 0 && pos < caps.v) v_id[pos] = vi;
+    });
+    if (ns > caps.s || nc > caps.c || nv > caps.v) return overflow(REC_OVERFLOW);
+    __syncwarp();
+    // Rank sorts: (key, index) pairs are distinct, so ranks are a permutation.
+    for (int i = lane; i < ns; i += 32) {
+        double kv = s_key[i];
+        uint32_t id = s_id[i];
+        int rank = 0;
+        for (int q = 0; q < ns; q++) rank += (s_key[q] < kv) || (s_key[q] == kv && s_id[q] < id);
+        s_perm[rank] = uint32_t(i);
+    }
+    for (int i = lane; i < nc; i += 32) {
+        double kv = c_key[i];
+        uint32_t id = c_id[i];
+        int rank = 0;
+        for (int q = 0; q < nc; q++) rank += (c_key[q] < kv) || (c_key[q] == kv && c_id[q] < id);
+        c_perm[rank] = uint32_t(i);
+    }
+    __syncwarp();
+    // Blocker counts and offsets, in sorted order.
+    unsigned run = 0;
+    if (lane == 0) s_off[0] = 0;
+    for (int b0 = 0; b0 < ns; b0 += 32) {
+        int r = b0 + lane;
+        unsigned cnt = 0;
+        if (r < ns) {
+            uint32_t k = s_id[s_perm[r]];
+            for (uint32_t p = A.nb_off[k], e = A.nb_off[k + 1]; p < e; p++)
+                cnt += lookup_local(sorted_ids, sorted_loc, nn, A.nb_items[p]) >= 0;
+        }
+        unsigned inc = warp_inclusive_scan(cnt);
+        if (r < ns) s_off[r + 1] = run + inc;
+        run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    const unsigned nsb = run;
+    run = 0;
+    if (lane == 0) c_off[0] = 0;
+    for (int b0 = 0; b0 < nc; b0 += 32) {
+        int r = b0 + lane;
+        unsigned cnt = 0;
+        if (r < nc) {
+            uint32_t ci = c_id[c_perm[r]];
+            for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++)
+                cnt += lookup_local(sorted_ids, sorted_loc, nn, A.cb_items[p]) >= 0;
+        }
+        unsigned inc = warp_inclusive_scan(cnt);
+        if (r < nc) c_off[r + 1] = run + inc;
+        run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    const unsigned ncb = run;
+    __syncwarp();
+
+    // Space: ids (CSR words) and the packed f32 block the sampler stages.
+    const unsigned long long ids_words =
+        (unsigned long long)nn + 2ull * ns + 1 + nsb + 2ull * nc + 1 + ncb + nv;
+    const unsigned long long tail_words = (unsigned long long)ns + 1 + nsb + nc + 1 + ncb;
+    const unsigned long long units = 2ull * nn + ns + 3ull * nc + nv + (tail_words + 3) / 4;
+    unsigned long long ids_base = 0, pack_base = 0;
+    if (lane == 0) {
+        ids_base = atomicAdd(&O.counters[CNT_IDS], ids_words);
+        pack_base = atomicAdd(&O.counters[CNT_PACK], units);
+        atomicMax(&O.counters[CNT_MAXPACK], units);
+    }
+    ids_base = __shfl_sync(0xffffffffu, ids_base, 0);
+    pack_base = __shfl_sync(0xffffffffu, pack_base, 0);
+    if (ids_base + ids_words > O.ids_cap || pack_base + units > O.pack_cap) return overflow(REC_NOMEM);
+
+    // CSR ids: near, S, s_off, s_blk, C, c_off, c_blk, V.
+    uint32_t* ids = O.ids + ids_base;
+    uint32_t* w_near = ids;
+    uint32_t* w_s = w_near + nn;
+    uint32_t* w_soff = w_s + ns;
+    uint32_t* w_sblk = w_soff + ns + 1;
+    uint32_t* w_c = w_sblk + nsb;
+    uint32_t* w_coff = w_c + nc;
+    uint32_t* w_cblk = w_coff + nc + 1;
+    uint32_t* w_v = w_cblk + ncb;
+    // Packed block: nearA (x,y,z,R^2), nearT (x,y,z,(R-tol)^2), S (x,y,z,R),
+    // C (3 x float4), V (x,y,z,0), then s_off, s_blk, c_off, c_blk words.
+    float4* pk = reinterpret_cast<float4*>(O.pack + pack_base);
+    float4* p_nearA = pk;
+    float4* p_nearT = p_nearA + nn;
+    float4* p_s = p_nearT + nn;
+    float4* p_c = p_s + ns;
+    float4* p_v = p_c + 3 * nc;
+    uint32_t* p_tail = reinterpret_cast<uint32_t*>(p_v + nv);
+    uint32_t* p_soff = p_tail;
+    uint32_t* p_sblk = p_soff + ns + 1;
+    uint32_t* p_coff = p_sblk + nsb;
+    uint32_t* p_cblk = p_coff + nc + 1;
+
+    for (int i = lane; i < nn; i += 32) {
+        uint32_t k = near_ids[i];
+        w_near[i] = k;
+        double4 c = A.sph[k];
+        float x = float(c.x - L.fx), y = float(c.y - L.fy), z = float(c.z - L.fz);
+        float r32 = float(c.w);
+        float rt = fmaxf(r32 - INSIDE_TOL, 0.0f);
+        p_nearA[i] = make_float4(x, y, z, r32 * r32);
+        p_nearT[i] = make_float4(x, y, z, rt * rt);
+    }
+    for (int r = lane; r <= ns; r += 32) w_soff[r] = s_off[r], p_soff[r] = s_off[r];
+    for (int r = lane; r < ns; r += 32) {
+        uint32_t i = s_perm[r], k = s_id[i];
+        w_s[r] = k;
+        double4 c = A.sph[k];
+        p_s[r] = make_float4(float(c.x - L.fx), float(c.y - L.fy), float(c.z - L.fz), float(c.w));
+        uint32_t o = s_off[r];
+        for (uint32_t p = A.nb_off[k], e = A.nb_off[k + 1]; p < e; p++) {
+            int l = lookup_local(sorted_ids, sorted_loc, nn, A.nb_items[p]);
+            if (l >= 0) w_sblk[o] = uint32_t(l), p_sblk[o] = uint32_t(l), o++;
+        }
+    }
+    for (int r = lane; r <= nc; r += 32) w_coff[r] = c_off[r], p_coff[r] = c_off[r];
+    for (int r = lane; r < nc; r += 32) {
+        uint32_t ci = c_id[c_perm[r]];
+        w_c[r] = ci;
+        const double* c = A.circ + 12 * size_t(ci);
+        p_c[3 * r] = make_float4(float(c[0] - L.fx), float(c[1] - L.fy), float(c[2] - L.fz), float(c[9]));
+        p_c[3 * r + 1] = make_float4(float(c[3]), float(c[4]), float(c[5]), float(c[6]));
+        p_c[3 * r + 2] = make_float4(float(c[7]), float(c[8]), 0.0f, 0.0f);
+        uint32_t o = c_off[r];
+        for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++) {
+            int l = lookup_local(sorted_ids, sorted_loc, nn, A.cb_items[p]);
+            if (l >= 0) w_cblk[o] = uint32_t(l), p_cblk[o] = uint32_t(l), o++;
+        }
+    }
+    for (int i = lane; i < nv; i += 32) {
+        uint32_t vi = v_id[i];
+        w_v[i] = vi;
+        double4 q = A.vert[vi];
+        p_v[i] = make_float4(float(q.x - L.fx), float(q.y - L.fy), float(q.z - L.fz), 0.0f);
+    }
+    if (lane == 0) {
+        rec[R_IDS] = uint32_t(ids_base);
+        rec[R_INSIDE] = uint32_t(n_in);
+        rec[R_NEAR] = uint32_t(nn);
+        rec[R_S] = uint32_t(ns);
+        rec[R_C] = uint32_t(nc);
+        rec[R_V] = uint32_t(nv);
+        rec[R_SBLK] = nsb;
+        rec[R_CBLK] = ncb;
+        rec[R_PACK] = uint32_t(pack_base);
+        rec[R_PACKLEN] = uint32_t(units);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// (c) Sampling: one CTA per sampled sub-block.  Its packed candidate block
+// is one contiguous, 16-byte aligned run of global memory, staged in shared
+// memory by the TMA bulk-copy engine (cp.async.bulk, mbarrier completion);
+// each thread then evaluates owned samples against it with broadcast
+// shared-memory reads.  ses_kernel (field/kernel.rs:837-952) per lane.
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+constexpr uint32_t BULK_CHUNK = 32768;            // bytes per bulk copy
+constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;     // bounded wait
+
+template <bool TMA>
+__global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const uint32_t* work, uint32_t n_work,
+                                                const uint32_t* rec, const uint4* pack, float* values,
+                                                unsigned long long* counters) {
+    extern __shared__ __align__(16) uint4 sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t sts[8];
+    const uint32_t j = work[blockIdx.x];
+    const uint32_t brick = j >> 3, sb = j & 7;
+    const uint32_t* R = rec + size_t(j) * REC_WORDS;
+    if (R[R_FLAGS] != 0) return;
+    const int nn = int(R[R_NEAR]), n_in = int(R[R_INSIDE]), ns = int(R[R_S]), nc = int(R[R_C]), nv = int(R[R_V]);
+    const int nsb = int(R[R_SBLK]);
+    const uint32_t units = R[R_PACKLEN];
+    const uint4* src = pack + R[R_PACK];
+    if (threadIdx.x < 8) sts[threadIdx.x] = rec[(size_t(brick) * 8 + threadIdx.x) * REC_WORDS + R_STATE];
+    if (TMA) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            uint32_t bytes = units * 16u;
+            mbar_expect_tx(&bar, bytes);
+            for (uint32_t o = 0; o < bytes; o += BULK_CHUNK)
+                bulk_g2s(reinterpret_cast<unsigned char*>(sm) + o, reinterpret_cast<const unsigned char*>(src) + o,
+                         min(BULK_CHUNK, bytes - o), &bar);
+        }
+        __syncthreads();
+        uint32_t spins = 0;
+        while (!mbar_try_wait(&bar, 0)) {
+            if (++spins >= MBAR_SPIN_LIMIT) {
+                if (threadIdx.x == 0) atomicAdd(&counters[CNT_TIMEOUT], 1ull);
+                return;
+            }
+        }
+    } else {
+        for (uint32_t u = threadIdx.x; u < units; u += blockDim.x) sm[u] = src[u];
+        __syncthreads();
+    }
+    const float4* nearA = reinterpret_cast<const float4*>(sm);
+    const float4* nearT = nearA + nn;
+    const float4* S = nearT + nn;
+    const float4* C = S + ns;
+    const float4* V = C + 3 * nc;
+    const uint32_t* s_off = reinterpret_cast<const uint32_t*>(V + nv);
+    const uint32_t* s_blk = s_off + ns + 1;
+    const uint32_t* c_off = s_blk + nsb;
+    const uint32_t* c_blk = c_off + nc + 1;
+    uint32_t st[8];
+    for (int q = 0; q < 8; q++) st[q] = sts[q];
+
+    const int sub = L.sub, side = L.b + 1, sp = sub + 1;
+    const int ox = int(sb & 1) * sub, oy = int((sb >> 1) & 1) * sub, oz = int((sb >> 2) & 1) * sub;
+    const int4 key = keys[brick];
+    const long long gx = (long long)key.x * L.b - L.frame[0], gy = (long long)key.y * L.b - L.frame[1],
+                    gz = (long long)key.z * L.b - L.frame[2];
+    const float probe = L.probe32, cutoff2 = L.cutoff2;
+    float* out = values + size_t(brick) * L.spb;
+    for (int t = threadIdx.x; t < sp * sp * sp; t += blockDim.x) {
+        int x = ox + t % sp, y = oy + (t / sp) % sp, z = oz + t / (sp * sp);
+        bool positive;
+        if (sample_owner(x, y, z, sub, st, &positive) != int(sb)) continue;
+        // Lattice::local (field/lattice.rs:69): from integers only.
+        const float px = float(gx + x) * L.h32, py = float(gy + y) * L.h32, pz = float(gz + z) * L.h32;
+        bool inside = false;
+        for (int k = 0; k < n_in; k++) {
+            float4 a = nearA[k];
+            float dx = px - a.x, dy = py - a.y, dz = pz - a.z;
+            inside |= (dx * dx + dy * dy + dz * dz) < a.w;
+        }
+        float value = probe;
+        if (inside) {
+            float best2 = cutoff2;
+            for (int v = 0; v < nv; v++) {
+                float4 q = V[v];
+                float dx = px - q.x, dy = py - q.y, dz = pz - q.z;
+                best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
+            }
+            for (int si = 0; si < ns; si++) {
+                float4 c = S[si];
+                float dx = px - c.x, dy = py - c.y, dz = pz - c.z;
+                float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+                float lb = fabsf(dist - c.w);
+                float lb2 = lb * lb;
+                bool valid = lb2 < best2 && 1e-6f < dist;
+                if (!valid) continue;
+                float scale = c.w / dist;
+                float qx = c.x + dx * scale, qy = c.y + dy * scale, qz = c.z + dz * scale;
+                for (uint32_t p = s_off[si], e = s_off[si + 1]; p < e; p++) {
+                    float4 b = nearT[s_blk[p]];
+                    float ex = qx - b.x, ey = qy - b.y, ez = qz - b.z;
+                    if (!((ex * ex + ey * ey + ez * ez) >= b.w)) {
+                        valid = false;
+                        break;
+                    }
+                }
+                if (valid) best2 = lb2;
+            }
+            for (int ci = 0; ci < nc; ci++) {
+                float4 m = C[3 * ci], u = C[3 * ci + 1], e2 = C[3 * ci + 2];
+                float yx = px - m.x, yy = py - m.y, yz = pz - m.z;
+                float along = yx * u.x + yy * u.y + yz * u.z;
+                float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
+                float wl = sqrtf(wx * wx + wy * wy + wz * wz);
+                float tt = wl - m.w;
+                float d2 = along * along + tt * tt;
+                if (!(d2 < best2)) continue;
+                bool degenerate = wl < 1e-6f;
+                float s = m.w / wl;
+                float qx = degenerate ? m.x + u.w * m.w : m.x + wx * s;
+                float qy = degenerate ? m.y + e2.x * m.w : m.y + wy * s;
+                float qz = degenerate ? m.z + e2.y * m.w : m.z + wz * s;
+                bool valid = true;
+                for (uint32_t p = c_off[ci], e = c_off[ci + 1]; p < e; p++) {
+                    float4 b = nearT[c_blk[p]];
+                    float ex = qx - b.x, ey = qy - b.y, ez = qz - b.z;
+                    if (!((ex * ex + ey * ey + ez * ez) >= b.w)) {
+                        valid = false;
+                        break;
+                    }
+                }
+                if (valid) best2 = d2;
+            }
+            value = probe - sqrtf(best2);
+        }
+        out[(z * side + y) * side + x] = value;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// (d) Marching cubes per brick (mesh_brick edge scan and cells(),
+// mesh/extract.rs:146-265): owned crossing edges in (z, y, x, axis) order
+// and triangle references (code << 28 | local edge id) in cell order, both
+// compacted with a block scan over contiguous cell ranges per thread.
+constexpr int MC_THREADS = 256;
+__constant__ uint8_t c_edge_lower[12] = {0, 2, 4, 6, 0, 1, 4, 5, 0, 1, 2, 3};
+
+template <bool FILL>
+__global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L, uint32_t n_bricks, const float* values, uint32_t* counts,
+                                                   const uint32_t* edge_off, const uint32_t* tri_off, uint32_t* edges,
+                                                   float2* edge_vals, uint32_t* tris) {
+    extern __shared__ float v[];
+    __shared__ uint16_t t_off[257];
+    __shared__ uint8_t t_edges[SMB_MC_TRIANGLES * 3];
+    __shared__ unsigned long long sh[MC_THREADS / 32];
+    const uint32_t brick = blockIdx.x;
+    if (brick >= n_bricks) return;
+    const int b = L.b, s = b + 1;
+    const float* src = values + size_t(brick) * L.spb;
+    for (int i = threadIdx.x; i < L.spb; i += blockDim.x) v[i] = src[i];
+    for (int i = threadIdx.x; i < 257; i += blockDim.x) t_off[i] = SMB_TRI_OFFSET[i];
+    for (int i = threadIdx.x; i < SMB_MC_TRIANGLES * 3; i += blockDim.x) t_edges[i] = SMB_TRI_EDGES[i / 3][i % 3];
+    __syncthreads();
+    const int cells = b * b * b;
+    const int per = (cells + MC_THREADS - 1) / MC_THREADS;
+    const int c0 = min(int(threadIdx.x) * per, cells), c1 = min(c0 + per, cells);
+    const int st[3] = {1, s, s * s};
+    const int corner[8] = {0, 1, s, s + 1, s * s, s * s + 1, s * s + s, s * s + s + 1};
+    unsigned ne = 0, nt = 0;
+    for (int c = c0; c < c1; c++) {
+        int x = c % b, y = (c / b) % b, z = c / (b * b);
+        int i = (z * s + y) * s + x;
+        bool a = v[i] < 0.0f;
+        for (int ax = 0; ax < 3; ax++) ne += (a != (v[i + st[ax]] < 0.0f));
+        int cs = 0;
+        for (int q = 0; q < 8; q++) cs |= (v[i + corner[q]] < 0.0f) << q;
+        nt += t_off[cs + 1] - t_off[cs];
+    }
+    unsigned long long te, tt;
+    unsigned long long pe = block_exclusive_scan<MC_THREADS>(ne, sh, &te);
+    unsigned long long pt = block_exclusive_scan<MC_THREADS>(nt, sh, &tt);
+    if (!FILL) {
+        if (threadIdx.x == 0) counts[brick] = uint32_t(te), counts[n_bricks + brick] = uint32_t(tt);
+        return;
+    }
+    uint32_t eo = edge_off[brick] + uint32_t(pe), to = tri_off[brick] + uint32_t(pt);
+    for (int c = c0; c < c1; c++) {
+        int x = c % b, y = (c / b) % b, z = c / (b * b);
+        int i = (z * s + y) * s + x;
+        float va = v[i];
+        for (int ax = 0; ax < 3; ax++) {
+            float vb = v[i + st[ax]];
+            if ((va < 0.0f) != (vb < 0.0f)) {
+                edges[eo] = uint32_t(c * 3 + ax);
+                edge_vals[eo] = make_float2(va, vb);
+                eo++;
+            }
+        }
+        int cs = 0;
+        for (int q = 0; q < 8; q++) cs |= (v[i + corner[q]] < 0.0f) << q;
+        for (int t = t_off[cs]; t < t_off[cs + 1]; t++) {
+            for (int k = 0; k < 3; k++) {
+                int e = t_edges[3 * t + k];
+                int axis = e >> 2, lo = c_edge_lower[e];
+                int l[3] = {x + (lo & 1), y + ((lo >> 1) & 1), z + ((lo >> 2) & 1)};
+                uint32_t code = 0;
+                int lc[3] = {0, 0, 0};
+                for (int a2 = 0; a2 < 3; a2++) {
+                    if (l[a2] == b) code |= 1u << a2;
+                    else lc[a2] = l[a2];
+                }
+                tris[3 * size_t(to) + k] = (code << 28) | uint32_t(((lc[2] * b + lc[1]) * b + lc[0]) * 3 + axis);
+            }
+            to++;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers.
+void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s) {
+    k_selftest<<<(n + 255) / 256, 256, 0, s>>>(a, b, out, n);
+}
+
+void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, unsigned long long* tiles,
+                 unsigned long long* total, cudaStream_t s) {
+    uint32_t n_tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (n_tiles == 0) {
+        cudaMemsetAsync(total, 0, sizeof(unsigned long long), s);
+        return;
+    }
+    k_scan_tiles<<<n_tiles, SCAN_THREADS, 0, s>>>(in, n, tiles);
+    k_scan_tile_sums<<<1, SCAN_THREADS, 0, s>>>(tiles, n_tiles, total);
+    k_scan_apply<<<n_tiles, SCAN_THREADS, 0, s>>>(in, n, tiles, out, keep);
+}
+
+uint32_t scan_tiles_needed(uint32_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE + 1; }
+
+void launch_mark_touched(const DArr& A, const DLat& L, const BrickBox& box, uint32_t* flags, int* err, cudaStream_t s) {
+    if (A.n) k_mark_touched<<<(A.n + 127) / 128, 128, 0, s>>>(A, L, box, flags, err);
+}
+
+void launch_classify_bricks(const DArr& A, const DLat& L, const BrickBox& box, const uint32_t* touched, uint32_t n,
+                            uint32_t* surface, cudaStream_t s) {
+    if (n) k_classify_bricks<<<(n + 7) / 8, 256, 0, s>>>(A, L, box, touched, n, surface);
+}
+
+void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n, int4* keys, cudaStream_t s) {
+    if (n) k_cells_to_keys<<<(n + 255) / 256, 256, 0, s>>>(box, cells, n, keys);
+}
+
+void launch_substates(const DArr& A, const DLat& L, const int4* keys, uint32_t n, uint32_t* rec, uint32_t* sampled,
+                      float* values, cudaStream_t s) {
+    if (n) k_substates<<<n, 256, 0, s>>>(A, L, keys, n, rec, sampled, values);
+}
+
+cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const uint32_t* work, uint32_t n,
+                          const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s) {
+    if (!n) return cudaSuccess;
+    size_t smem = gather_smem_bytes(caps) * size_t(warps);
+    cudaError_t e = cudaFuncSetAttribute(k_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    k_gather<<<(n + warps - 1) / warps, 32 * warps, smem, s>>>(A, L, keys, work, n, O, caps);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
+                          const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
+                          cudaStream_t s) {
+    if (!n) return cudaSuccess;
+    size_t smem = size_t(max_units) * 16;
+    auto kern = tma ? k_sample<true> : k_sample<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    kern<<<n, 128, smem, s>>>(L, keys, work, n, rec, pack, values, counters);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mc(const DLat& L, uint32_t n, const float* values, uint32_t* counts, const uint32_t* edge_off,
+                      const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
+                      cudaStream_t s) {
+    if (!n) return cudaSuccess;
+    size_t smem = size_t(L.spb) * 4;
+    auto kern = fill ? k_mc<true> : k_mc<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    kern<<<n, MC_THREADS, smem, s>>>(L, n, values, counts, edge_off, tri_off, edges, edge_vals, tris);
+    return cudaGetLastError();
+}
+
+}  // namespace smb

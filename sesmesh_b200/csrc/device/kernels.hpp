@@ -1,0 +1,61 @@
+// Host-visible declarations of the device kernels' launchers.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace smb {
+
+// Dense box of brick keys [lo, lo + n) per axis (touched-brick flags).
+struct BrickBox {
+    long long lo[3];
+    uint32_t n[3], pad;
+};
+
+enum : int { ERR_NONE = 0, ERR_KEY_RANGE = 1, ERR_BOX = 2 };
+
+// Per-warp shared-memory capacities of the gather kernel.
+struct GatherCaps {
+    int near, s, c, v;
+};
+
+__host__ __device__ inline size_t gather_smem_bytes(const GatherCaps& c) {
+    size_t b = size_t(c.near) * 12 + size_t(c.s) * 24 + size_t(c.c) * 20 + size_t(c.v) * 4 + 8;
+    return (b + 15) & ~size_t(15);
+}
+
+// Device counters of one gather/sample pass.
+enum : int { CNT_IDS = 0, CNT_PACK = 1, CNT_MAXPACK = 2, CNT_OVERFLOW = 3, CNT_NOMEM = 4, CNT_TIMEOUT = 5, CNT_N = 8 };
+constexpr uint32_t REC_NOMEM = 2;
+
+struct GatherOut {
+    uint32_t* rec;
+    uint32_t* ids;
+    uint4* pack;
+    uint32_t* retry;  // sub-blocks whose lists exceeded the shared-memory caps
+    unsigned long long* counters;
+    unsigned long long ids_cap, pack_cap;
+};
+
+void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);
+void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, unsigned long long* tiles,
+                 unsigned long long* total, cudaStream_t s);
+uint32_t scan_tiles_needed(uint32_t n);
+void launch_mark_touched(const DArr& A, const DLat& L, const BrickBox& box, uint32_t* flags, int* err, cudaStream_t s);
+void launch_classify_bricks(const DArr& A, const DLat& L, const BrickBox& box, const uint32_t* touched, uint32_t n,
+                            uint32_t* surface, cudaStream_t s);
+void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n, int4* keys, cudaStream_t s);
+void launch_substates(const DArr& A, const DLat& L, const int4* keys, uint32_t n, uint32_t* rec, uint32_t* sampled,
+                      float* values, cudaStream_t s);
+cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const uint32_t* work, uint32_t n,
+                          const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s);
+cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
+                          const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
+                          cudaStream_t s);
+cudaError_t launch_mc(const DLat& L, uint32_t n, const float* values, uint32_t* counts, const uint32_t* edge_off,
+                      const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
+                      cudaStream_t s);
+
+}  // namespace smb

@@ -52,12 +52,16 @@ def main():
         "#pragma once",
         "#include <stdint.h>",
         "#define SMB_MC_TRIANGLES %d" % len(tris),
-        "static const uint16_t SMB_TRI_OFFSET[257] = {",
+        "// Storage qualifier (__constant__ when included by device code).",
+        "#ifndef SMB_MC_QUAL",
+        "#define SMB_MC_QUAL",
+        "#endif",
+        "static SMB_MC_QUAL const uint16_t SMB_TRI_OFFSET[257] = {",
     ]
     for i in range(0, 257, 16):
         lines.append("    " + ", ".join(str(v) for v in offsets[i:i + 16]) + ",")
     lines.append("};")
-    lines.append("static const uint8_t SMB_TRI_EDGES[%d][3] = {" % len(tris))
+    lines.append("static SMB_MC_QUAL const uint8_t SMB_TRI_EDGES[%d][3] = {" % len(tris))
     for case in range(256):
         row = tris[offsets[case]:offsets[case + 1]]
         if row:

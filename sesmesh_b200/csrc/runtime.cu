@@ -1,0 +1,664 @@
+// Host runtime behind the C ABI of include/sesmesh_b200.h: device open and
+// self-test, the resident arrangement, device-side brick classification and
+// batch runs (sub-block states, gather, sampling, marching cubes).
+//
+// Stands in for sesmesh's CUDA back-end crate (crates/sesmesh-gpu/src/cuda/
+// {mod.rs,resident.rs,memory.rs,stream.rs}): one stream per device, device
+// buffers grown on demand and reused across runs, CUDA events around each
+// pass.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/sesmesh_b200.h"
+#include "device/kernels.hpp"
+#include "runtime.hpp"
+
+using namespace smb;
+
+namespace {
+
+void set_err(char* err, size_t len, const char* fmt, ...) {
+    if (!err || !len) return;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, len, fmt, ap);
+    va_end(ap);
+}
+
+#define CK(call)                                                                                 \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            set_err(err, errlen, "%s failed: %s", #call, cudaGetErrorString(e_));                \
+            return SMB_ERR_CUDA;                                                                 \
+        }                                                                                        \
+    } while (0)
+
+uint64_t splitmix(uint64_t& s) {
+    s += 0x9E3779B97F4A7C15ULL;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// Host recomputation of k_selftest (built without FMA contraction).
+void selftest_ref(float x, float y, uint32_t out[12]) {
+    float dx = x - y, dy = y * 0.75f - x, dz = x * y - 1.0f;
+    float d = std::sqrt(dx * dx + dy * dy + dz * dz);
+    float r[8] = {x + y, x * y, x / y, std::sqrt(std::fabs(x)), d, (d - y) / d, std::fmin(x, y), std::fabs(d - std::fabs(y))};
+    for (int k = 0; k < 8; k++) std::memcpy(&out[k], &r[k], 4);
+    double X = double(x) * 1.0000001, Y = double(y) - 0.3;
+    double D = X * Y + X, E = std::sqrt(std::fabs(X * X + Y * Y - X)), F = X / (Y + 2.5), G = std::floor(X * 3.7);
+    double rr[4] = {D, E, F, G};
+    for (int k = 0; k < 4; k++) {
+        uint64_t u;
+        std::memcpy(&u, &rr[k], 8);
+        out[8 + k] = uint32_t(u ^ (u >> 32));
+    }
+}
+
+}  // namespace
+
+namespace smb {
+
+int dev_alloc(void** p, size_t bytes, std::vector<void*>* owned, size_t* total, char* err, size_t errlen) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        set_err(err, errlen, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+        *p = nullptr;
+        return e == cudaErrorMemoryAllocation ? SMB_ERR_MEMORY : SMB_ERR_CUDA;
+    }
+    if (owned) owned->push_back(*p);
+    if (total) *total += bytes;
+    return SMB_OK;
+}
+
+// Grows a batch buffer to at least `bytes` (contents discarded).
+int DBuf::reserve(size_t bytes, char* err, size_t errlen) {
+    if (bytes <= cap) return SMB_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes + bytes / 4 + 256;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        set_err(err, errlen, "cudaMalloc(%zu bytes) failed: %s", want, cudaGetErrorString(e));
+        p = nullptr;
+        return e == cudaErrorMemoryAllocation ? SMB_ERR_MEMORY : SMB_ERR_CUDA;
+    }
+    cap = want;
+    return SMB_OK;
+}
+
+void DBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+
+}  // namespace smb
+
+extern "C" {
+
+int smb_open(int index, smb_device** out, char* err, size_t errlen) {
+    if (!out) return set_err(err, errlen, "null output"), SMB_ERR_ARG;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        set_err(err, errlen, "no CUDA device: %s", e == cudaSuccess ? "count is 0" : cudaGetErrorString(e));
+        return SMB_ERR_NODEVICE;
+    }
+    if (index < 0 || index >= count) return set_err(err, errlen, "device %d of %d", index, count), SMB_ERR_NODEVICE;
+    CK(cudaSetDevice(index));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, index));
+    if (prop.major < 10) {
+        set_err(err, errlen, "device %d (%s) is sm_%d%d; this build targets sm_100a", index, prop.name, prop.major,
+                prop.minor);
+        return SMB_ERR_NODEVICE;
+    }
+    auto* d = new smb_device();
+    d->index = index;
+    std::snprintf(d->info.name, sizeof d->info.name, "%s", prop.name);
+    d->info.major = prop.major;
+    d->info.minor = prop.minor;
+    d->info.multiprocessors = prop.multiProcessorCount;
+    d->info.memory = prop.totalGlobalMem;
+    d->smem_optin = prop.sharedMemPerBlockOptin;
+    e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete d;
+        set_err(err, errlen, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
+        return SMB_ERR_CUDA;
+    }
+    int rc = smb_self_test(d, 4096, err, errlen);
+    if (rc != SMB_OK) {
+        smb_close(d);
+        return rc;
+    }
+    *out = d;
+    return SMB_OK;
+}
+
+void smb_close(smb_device* d) {
+    if (!d) return;
+    cudaSetDevice(d->index);
+    if (d->stream) cudaStreamDestroy(d->stream);
+    delete d;
+}
+
+int smb_device_info_get(const smb_device* d, smb_device_info* out) {
+    if (!d || !out) return SMB_ERR_ARG;
+    *out = d->info;
+    return SMB_OK;
+}
+
+int smb_self_test(smb_device* d, uint32_t n, char* err, size_t errlen) {
+    if (!d || n == 0) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
+    CK(cudaSetDevice(d->index));
+    std::vector<float> a(n), b(n);
+    uint64_t s = 0x5e5e5e5eULL + n;
+    for (uint32_t i = 0; i < n; i++) {
+        a[i] = float(int64_t(splitmix(s) >> 40) - (int64_t(1) << 23)) / 65536.0f;
+        b[i] = 0.1f + float(splitmix(s) >> 40) / 262144.0f;
+    }
+    float *da = nullptr, *db = nullptr;
+    uint32_t* dout = nullptr;
+    std::vector<uint32_t> got(size_t(n) * 12);
+    auto cleanup = [&] {
+        cudaFree(da);
+        cudaFree(db);
+        cudaFree(dout);
+    };
+    if (cudaMalloc(&da, n * 4) != cudaSuccess || cudaMalloc(&db, n * 4) != cudaSuccess ||
+        cudaMalloc(&dout, size_t(n) * 48) != cudaSuccess) {
+        cleanup();
+        return set_err(err, errlen, "self-test allocation failed"), SMB_ERR_MEMORY;
+    }
+    cudaMemcpyAsync(da, a.data(), n * 4, cudaMemcpyHostToDevice, d->stream);
+    cudaMemcpyAsync(db, b.data(), n * 4, cudaMemcpyHostToDevice, d->stream);
+    launch_selftest(da, db, dout, n, d->stream);
+    cudaMemcpyAsync(got.data(), dout, size_t(n) * 48, cudaMemcpyDeviceToHost, d->stream);
+    cudaError_t e = cudaStreamSynchronize(d->stream);
+    cleanup();
+    if (e != cudaSuccess) return set_err(err, errlen, "self-test failed: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t want[12];
+        selftest_ref(a[i], b[i], want);
+        for (int k = 0; k < 12; k++)
+            if (want[k] != got[size_t(i) * 12 + k]) {
+                set_err(err, errlen, "arithmetic self-test: pair %u op %d differs (device %08x, host %08x)", i, k,
+                        got[size_t(i) * 12 + k], want[k]);
+                return SMB_ERR_SELFTEST;
+            }
+    }
+    return SMB_OK;
+}
+
+static bool csr_ok(const uint32_t* off, size_t rows, size_t items) {
+    if (!off || off[0] != 0) return false;
+    for (size_t i = 0; i < rows; i++)
+        if (off[i + 1] < off[i]) return false;
+    return off[rows] == items;
+}
+
+int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_lattice_ref* lat, smb_resident** out,
+                     char* err, size_t errlen) {
+    if (!d || !a || !lat || !out) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
+    *out = nullptr;
+    if (lat->brick < 4 || lat->brick > 32 || lat->brick % 2)
+        return set_err(err, errlen, "brick must be even and 4..32, got %u", lat->brick), SMB_ERR_ARG;
+    if (!(lat->spacing >= 0.01) || !std::isfinite(lat->spacing))
+        return set_err(err, errlen, "grid spacing must be at least 0.01"), SMB_ERR_ARG;
+    size_t n = a->n_spheres, nc = a->n_circles, nv = a->n_vertices;
+    if (n >= (size_t(1) << 32) || nc >= (size_t(1) << 32) || nv >= (size_t(1) << 32))
+        return set_err(err, errlen, "too many spheres, circles or vertices"), SMB_ERR_ARG;
+    // Shapes, as batch::validate (batch.rs:323-338).
+    if (n && (!a->center || !a->expanded || !a->radius || !a->status || !a->nb_off))
+        return set_err(err, errlen, "missing sphere arrays"), SMB_ERR_ARG;
+    if (n && !csr_ok(a->nb_off, n, a->nb_off[n])) return set_err(err, errlen, "malformed neighbour CSR"), SMB_ERR_ARG;
+    if (nc && (!a->circle || !a->cb_off || !csr_ok(a->cb_off, nc, a->cb_off[nc])))
+        return set_err(err, errlen, "malformed circle tables"), SMB_ERR_ARG;
+    if (nv && !a->vertex) return set_err(err, errlen, "missing vertices"), SMB_ERR_ARG;
+    size_t nb_items = n ? a->nb_off[n] : 0, cb_items = nc ? a->cb_off[nc] : 0;
+    for (size_t i = 0; i < nb_items; i++)
+        if (a->nb_items[i] >= n) return set_err(err, errlen, "neighbour index out of range"), SMB_ERR_ARG;
+    for (size_t i = 0; i < cb_items; i++)
+        if (a->cb_items[i] >= n) return set_err(err, errlen, "circle blocker index out of range"), SMB_ERR_ARG;
+    for (size_t i = 0; i < n; i++)
+        if (a->status[i] > 2) return set_err(err, errlen, "bad sphere status"), SMB_ERR_ARG;
+    const smb_grid_ref* grids[3] = {&a->sphere_grid, &a->circle_grid, &a->vertex_grid};
+    size_t grid_items[3] = {n, nc, nv};
+    for (int g = 0; g < 3; g++) {
+        const smb_grid_ref* G = grids[g];
+        size_t cells = size_t(G->dims[0]) * G->dims[1] * G->dims[2];
+        if (!G->dims[0] || !G->dims[1] || !G->dims[2] || !G->starts || !(G->cell > 0))
+            return set_err(err, errlen, "malformed cell grid %d", g), SMB_ERR_ARG;
+        if (!csr_ok(G->starts, cells, G->n_items) || G->n_items != grid_items[g])
+            return set_err(err, errlen, "malformed cell grid %d table", g), SMB_ERR_ARG;
+        for (size_t i = 0; i < G->n_items; i++)
+            if (G->items[i] >= grid_items[g]) return set_err(err, errlen, "grid %d item out of range", g), SMB_ERR_ARG;
+    }
+    CK(cudaSetDevice(d->index));
+    auto* r = new smb_resident();
+    r->dev = d;
+    int rc = SMB_OK;
+    auto fail = [&](int code) {
+        smb_resident_free(r);
+        return code;
+    };
+    // Spheres: (x, y, z, R) f64 rows, vdW radii, status.
+    std::vector<double> sph(4 * n);
+    for (size_t i = 0; i < n; i++) {
+        sph[4 * i] = a->center[3 * i], sph[4 * i + 1] = a->center[3 * i + 1], sph[4 * i + 2] = a->center[3 * i + 2];
+        sph[4 * i + 3] = a->expanded[i];
+        for (int k = 0; k < 3; k++) {
+            r->lo[k] = i ? std::fmin(r->lo[k], a->center[3 * i + k]) : a->center[3 * i + k];
+            r->hi[k] = i ? std::fmax(r->hi[k], a->center[3 * i + k]) : a->center[3 * i + k];
+        }
+    }
+    std::vector<double> circ(12 * nc, 0.0);
+    for (size_t c = 0; c < nc; c++)
+        for (int k = 0; k < 10; k++) circ[12 * c + k] = a->circle[10 * c + k];
+    std::vector<double> vert(4 * nv, 0.0);
+    for (size_t v = 0; v < nv; v++)
+        for (int k = 0; k < 3; k++) vert[4 * v + k] = a->vertex[3 * v + k];
+    auto up = [&](void** dst, const void* src, size_t bytes) -> int {
+        int c = dev_alloc(dst, bytes, &r->owned, &r->bytes, err, errlen);
+        if (c != SMB_OK) return c;
+        if (bytes && src) {
+            cudaError_t e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, d->stream);
+            if (e != cudaSuccess) return set_err(err, errlen, "upload failed: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+        }
+        return SMB_OK;
+    };
+    DArr& A = r->A;
+    A.n = uint32_t(n), A.nc = uint32_t(nc), A.nv = uint32_t(nv);
+    void* p;
+    if ((rc = up(&p, sph.data(), sph.size() * 8)) != SMB_OK) return fail(rc);
+    A.sph = static_cast<const double4*>(p);
+    if ((rc = up(&p, a->radius, n * 8)) != SMB_OK) return fail(rc);
+    A.rvdw = static_cast<const double*>(p);
+    if ((rc = up(&p, a->status, n * 4)) != SMB_OK) return fail(rc);
+    A.status = static_cast<const uint32_t*>(p);
+    std::vector<uint32_t> zero_off(1, 0);
+    if ((rc = up(&p, n ? a->nb_off : zero_off.data(), (n + 1) * 4)) != SMB_OK) return fail(rc);
+    A.nb_off = static_cast<const uint32_t*>(p);
+    if ((rc = up(&p, a->nb_items, nb_items * 4)) != SMB_OK) return fail(rc);
+    A.nb_items = static_cast<const uint32_t*>(p);
+    if ((rc = up(&p, circ.data(), circ.size() * 8)) != SMB_OK) return fail(rc);
+    A.circ = static_cast<const double*>(p);
+    if ((rc = up(&p, nc ? a->cb_off : zero_off.data(), (nc + 1) * 4)) != SMB_OK) return fail(rc);
+    A.cb_off = static_cast<const uint32_t*>(p);
+    if ((rc = up(&p, a->cb_items, cb_items * 4)) != SMB_OK) return fail(rc);
+    A.cb_items = static_cast<const uint32_t*>(p);
+    if ((rc = up(&p, vert.data(), vert.size() * 8)) != SMB_OK) return fail(rc);
+    A.vert = static_cast<const double4*>(p);
+    DGrid* dg[3] = {&A.gs, &A.gc, &A.gv};
+    for (int g = 0; g < 3; g++) {
+        const smb_grid_ref* G = grids[g];
+        DGrid& D = *dg[g];
+        D.ox = G->origin[0], D.oy = G->origin[1], D.oz = G->origin[2], D.cell = G->cell;
+        D.dx = G->dims[0], D.dy = G->dims[1], D.dz = G->dims[2];
+        size_t cells = size_t(G->dims[0]) * G->dims[1] * G->dims[2];
+        if ((rc = up(&p, G->starts, (cells + 1) * 4)) != SMB_OK) return fail(rc);
+        D.starts = static_cast<const uint32_t*>(p);
+        if ((rc = up(&p, G->items, G->n_items * 4)) != SMB_OK) return fail(rc);
+        D.items = static_cast<const uint32_t*>(p);
+    }
+    A.max_expanded = a->max_expanded, A.rho_max = a->rho_max, A.probe = a->probe;
+    // Lattice constants, computed here in the CPU's f64 operation order.
+    DLat& L = r->L;
+    L.h = lat->spacing;
+    L.b = int(lat->brick);
+    L.sub = L.b / 2;
+    L.spb = (L.b + 1) * (L.b + 1) * (L.b + 1);
+    for (int k = 0; k < 3; k++) L.frame[k] = (long long)lat->frame[k];
+    L.fx = double(lat->frame[0]) * L.h, L.fy = double(lat->frame[1]) * L.h, L.fz = double(lat->frame[2]) * L.h;
+    L.band = lat->band;
+    L.rho_sub = 0.5 * std::sqrt(3.0) * double(L.sub) * L.h;   // kernel.rs:474
+    L.rho_brick = 0.5 * std::sqrt(3.0) * double(L.b) * L.h;   // lattice.rs:78-80
+    L.h32 = float(L.h);
+    L.band32 = float(L.band);
+    L.probe32 = float(a->probe);
+    float cutoff = float(a->probe + L.band);                   // kernel.rs:425
+    L.cutoff2 = cutoff * cutoff;
+    cudaError_t e = cudaStreamSynchronize(d->stream);
+    if (e != cudaSuccess) {
+        set_err(err, errlen, "upload failed: %s", cudaGetErrorString(e));
+        return fail(SMB_ERR_CUDA);
+    }
+    *out = r;
+    return SMB_OK;
+}
+
+void smb_resident_free(smb_resident* r) {
+    if (!r) return;
+    cudaSetDevice(r->dev->index);
+    cudaStreamSynchronize(r->dev->stream);
+    for (void* p : r->owned) cudaFree(p);
+    if (r->keys) cudaFree(r->keys);
+    delete r;
+}
+
+size_t smb_resident_bytes(const smb_resident* r) { return r ? r->bytes : 0; }
+
+int smb_classify(smb_resident* r, size_t* touched, size_t* surface, char* err, size_t errlen) {
+    if (!r) return SMB_ERR_ARG;
+    smb_device* d = r->dev;
+    CK(cudaSetDevice(d->index));
+    cudaStream_t s = d->stream;
+    const DLat& L = r->L;
+    if (r->keys) cudaFree(r->keys);
+    r->keys = nullptr;
+    r->n_bricks = 0;
+    r->classified = false;
+    if (r->A.n == 0) {
+        if (touched) *touched = 0;
+        if (surface) *surface = 0;
+        r->classified = true;
+        return SMB_OK;
+    }
+    // Box of all bricks any sphere can touch: brick_of is monotone, so the
+    // extreme centres with the largest radius bound every sphere's range.
+    BrickBox box{};
+    double rr = r->A.max_expanded + CLASSIFY_EPS, bh = double(L.b) * L.h;
+    double ncell = 1;
+    for (int k = 0; k < 3; k++) {
+        double lo = std::floor((r->lo[k] - rr) / bh), hi = std::floor((r->hi[k] + rr) / bh);
+        if (!(std::fabs(lo) < double(KEY_BIAS) && std::fabs(hi) < double(KEY_BIAS)))
+            return set_err(err, errlen, "coordinates too far from the origin for grid spacing %g", L.h), SMB_ERR_RANGE;
+        box.lo[k] = (long long)lo;
+        box.n[k] = uint32_t(hi - lo + 1);
+        ncell *= double(box.n[k]);
+    }
+    if (ncell > double(1u << 31))
+        return set_err(err, errlen, "brick grid of %.0f bricks exceeds the dense classification limit", ncell), SMB_ERR_RANGE;
+    uint32_t nb = uint32_t(ncell);
+    DBuf flags, list, surf, cells, tiles, tot, errbuf;
+    auto cleanup = [&] {
+        flags.release(), list.release(), surf.release(), cells.release(), tiles.release(), tot.release(), errbuf.release();
+    };
+    int rc;
+    if ((rc = flags.reserve(size_t(nb) * 4, err, errlen)) || (rc = list.reserve(size_t(nb) * 4, err, errlen)) ||
+        (rc = surf.reserve(size_t(nb) * 4, err, errlen)) || (rc = cells.reserve(size_t(nb) * 4, err, errlen)) ||
+        (rc = tiles.reserve(size_t(scan_tiles_needed(nb)) * 8, err, errlen)) || (rc = tot.reserve(16, err, errlen)) ||
+        (rc = errbuf.reserve(16, err, errlen))) {
+        cleanup();
+        return rc;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    cudaMemsetAsync(flags.p, 0, size_t(nb) * 4, s);
+    cudaMemsetAsync(surf.p, 0, size_t(nb) * 4, s);
+    cudaMemsetAsync(errbuf.p, 0, 16, s);
+    launch_mark_touched(r->A, L, box, flags.as<uint32_t>(), errbuf.as<int>(), s);
+    launch_scan(flags.as<uint32_t>(), nb, nullptr, list.as<uint32_t>(), tiles.as<unsigned long long>(),
+                tot.as<unsigned long long>(), s);
+    unsigned long long n_touched = 0;
+    int kerr = 0;
+    cudaMemcpyAsync(&n_touched, tot.p, 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&kerr, errbuf.p, 4, cudaMemcpyDeviceToHost, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess || kerr) {
+        cleanup();
+        if (e != cudaSuccess) return set_err(err, errlen, "classification failed: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+        return set_err(err, errlen, "coordinates too far from the origin for grid spacing %g", L.h), SMB_ERR_RANGE;
+    }
+    launch_classify_bricks(r->A, L, box, list.as<uint32_t>(), uint32_t(n_touched), surf.as<uint32_t>(), s);
+    launch_scan(surf.as<uint32_t>(), nb, nullptr, cells.as<uint32_t>(), tiles.as<unsigned long long>(),
+                tot.as<unsigned long long>(), s);
+    unsigned long long n_surface = 0;
+    cudaMemcpyAsync(&n_surface, tot.p, 8, cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && n_surface) e = cudaMalloc(&r->keys, n_surface * sizeof(int4));
+    if (e == cudaSuccess) launch_cells_to_keys(box, cells.as<uint32_t>(), uint32_t(n_surface), r->keys, s);
+    cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cleanup();
+    if (e != cudaSuccess) return set_err(err, errlen, "classification failed: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    r->classify_ms = ms;
+    r->n_touched = n_touched;
+    r->n_bricks = uint32_t(n_surface);
+    r->classified = true;
+    if (touched) *touched = n_touched;
+    if (surface) *surface = n_surface;
+    return SMB_OK;
+}
+
+int smb_resident_bricks(const smb_resident* r, int32_t* out, size_t cap) {
+    if (!r || !r->classified) return SMB_ERR_STATE;
+    cudaSetDevice(r->dev->index);
+    size_t n = r->n_bricks < cap ? r->n_bricks : cap;
+    std::vector<int4> k(n);
+    if (n && cudaMemcpy(k.data(), r->keys, n * sizeof(int4), cudaMemcpyDeviceToHost) != cudaSuccess) return SMB_ERR_CUDA;
+    for (size_t i = 0; i < n; i++) out[3 * i] = k[i].x, out[3 * i + 1] = k[i].y, out[3 * i + 2] = k[i].z;
+    return SMB_OK;
+}
+
+int smb_batch_new(smb_resident* r, smb_batch** out, char* err, size_t errlen) {
+    if (!r || !out) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
+    CK(cudaSetDevice(r->dev->index));
+    auto* b = new smb_batch();
+    b->res = r;
+    for (auto& ev : b->ev) cudaEventCreate(&ev);
+    *out = b;
+    return SMB_OK;
+}
+
+void smb_batch_free(smb_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->res->dev->index);
+    cudaStreamSynchronize(b->res->dev->stream);
+    for (DBuf* p : b->bufs()) p->release();
+    for (auto& ev : b->ev) cudaEventDestroy(ev);
+    delete b;
+}
+
+int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch_times* times, char* err,
+            size_t errlen) {
+    if (!r || !b || b->res != r) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
+    if (!r->classified) return set_err(err, errlen, "smb_classify must run first"), SMB_ERR_STATE;
+    if (first > r->n_bricks || count > r->n_bricks - first) return set_err(err, errlen, "brick range"), SMB_ERR_ARG;
+    smb_device* d = r->dev;
+    CK(cudaSetDevice(d->index));
+    cudaStream_t s = d->stream;
+    const DLat& L = r->L;
+    b->n = uint32_t(count);
+    b->n_work = 0;
+    b->n_edges = b->n_tris = 0;
+    b->ids_words = 0;
+    if (count == 0) {
+        if (times) *times = smb_batch_times{};
+        return SMB_OK;
+    }
+    const int4* keys = r->keys + first;
+    const size_t nsub = count * 8;
+    int rc;
+    if ((rc = b->rec.reserve(nsub * REC_WORDS * 4, err, errlen)) || (rc = b->sampled.reserve(nsub * 4, err, errlen)) ||
+        (rc = b->work.reserve(nsub * 4, err, errlen)) || (rc = b->retry_a.reserve(nsub * 4, err, errlen)) ||
+        (rc = b->retry_b.reserve(nsub * 4, err, errlen)) ||
+        (rc = b->values.reserve(count * size_t(L.spb) * 4, err, errlen)) ||
+        (rc = b->tiles.reserve(size_t(scan_tiles_needed(uint32_t(nsub))) * 8, err, errlen)) ||
+        (rc = b->totals.reserve(64, err, errlen)) || (rc = b->counters.reserve(CNT_N * 8, err, errlen)) ||
+        (rc = b->mc_counts.reserve(count * 8, err, errlen)) || (rc = b->edge_off.reserve(count * 4 + 4, err, errlen)) ||
+        (rc = b->tri_off.reserve(count * 4 + 4, err, errlen)))
+        return rc;
+    cudaEventRecord(b->ev[0], s);
+    launch_substates(r->A, L, keys, uint32_t(count), b->rec.as<uint32_t>(), b->sampled.as<uint32_t>(),
+                     b->values.as<float>(), s);
+    launch_scan(b->sampled.as<uint32_t>(), uint32_t(nsub), nullptr, b->work.as<uint32_t>(),
+                b->tiles.as<unsigned long long>(), b->totals.as<unsigned long long>(), s);
+    cudaEventRecord(b->ev[1], s);
+    unsigned long long n_work = 0;
+    cudaMemcpyAsync(&n_work, b->totals.p, 8, cudaMemcpyDeviceToHost, s);
+    CK(cudaStreamSynchronize(s));
+    b->n_work = uint32_t(n_work);
+
+    // (b) gather, with list memory grown and shared-memory caps raised as
+    // needed (bit-identical results at any capacity).
+    GatherCaps caps = b->caps;
+    unsigned long long cnt[CNT_N];
+    size_t want_ids = std::max<size_t>(b->ids.cap / 4, size_t(n_work) * 1024),
+           want_pack = std::max<size_t>(b->pack.cap / 16, size_t(n_work) * 512);
+    for (int attempt = 0;; attempt++) {
+        if ((rc = b->ids.reserve(want_ids * 4, err, errlen)) || (rc = b->pack.reserve(want_pack * 16, err, errlen)))
+            return rc;
+        CK(cudaMemsetAsync(b->counters.p, 0, CNT_N * 8, s));
+        GatherOut O{b->rec.as<uint32_t>(), b->ids.as<uint32_t>(), b->pack.as<uint4>(), b->retry_a.as<uint32_t>(),
+                    b->counters.as<unsigned long long>(), b->ids.cap / 4, b->pack.cap / 16};
+        cudaError_t e = launch_gather(r->A, L, keys, b->work.as<uint32_t>(), uint32_t(n_work), O, caps, b->gather_warps, s);
+        if (e != cudaSuccess) return set_err(err, errlen, "gather launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+        CK(cudaMemcpyAsync(cnt, b->counters.p, CNT_N * 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (cnt[CNT_NOMEM] && attempt < 4) {
+            want_ids = size_t(cnt[CNT_IDS]) + size_t(cnt[CNT_IDS]) / 4 + 1024;
+            want_pack = size_t(cnt[CNT_PACK]) + size_t(cnt[CNT_PACK]) / 4 + 1024;
+            continue;
+        }
+        if (cnt[CNT_NOMEM]) return set_err(err, errlen, "candidate list memory could not be sized"), SMB_ERR_MEMORY;
+        // Sub-blocks over the shared-memory caps: again with larger caps, one
+        // warp per block, until every list fits.
+        GatherCaps big = caps;
+        DBuf* from = &b->retry_a;
+        DBuf* to = &b->retry_b;
+        unsigned long long pending = cnt[CNT_OVERFLOW];
+        while (pending) {
+            big.near *= 2, big.s *= 2, big.c *= 2, big.v *= 2;
+            if (gather_smem_bytes(big) > size_t(d->smem_optin))
+                return set_err(err, errlen, "a sub-block's candidate lists exceed shared memory"), SMB_ERR_MEMORY;
+            CK(cudaMemsetAsync(b->counters.as<unsigned long long>() + CNT_OVERFLOW, 0, 8, s));
+            GatherOut O2 = O;
+            O2.retry = to->as<uint32_t>();
+            e = launch_gather(r->A, L, keys, from->as<uint32_t>(), uint32_t(pending), O2, big, 1, s);
+            if (e != cudaSuccess) return set_err(err, errlen, "gather launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+            CK(cudaMemcpyAsync(cnt, b->counters.p, CNT_N * 8, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+            if (cnt[CNT_NOMEM]) break;
+            pending = cnt[CNT_OVERFLOW];
+            std::swap(from, to);
+        }
+        if (cnt[CNT_NOMEM] && attempt < 4) {
+            want_ids = size_t(cnt[CNT_IDS]) + size_t(cnt[CNT_IDS]) / 4 + 1024;
+            want_pack = size_t(cnt[CNT_PACK]) + size_t(cnt[CNT_PACK]) / 4 + 1024;
+            continue;
+        }
+        if (cnt[CNT_NOMEM]) return set_err(err, errlen, "candidate list memory could not be sized"), SMB_ERR_MEMORY;
+        break;
+    }
+    b->ids_words = size_t(cnt[CNT_IDS]);
+    b->max_pack = uint32_t(cnt[CNT_MAXPACK]);
+    cudaEventRecord(b->ev[2], s);
+
+    // (c) sampling.
+    if (size_t(b->max_pack) * 16 > size_t(d->smem_optin))
+        return set_err(err, errlen, "a sub-block's candidates (%u x 16 bytes) exceed shared memory", b->max_pack),
+               SMB_ERR_MEMORY;
+    cudaError_t e = launch_sample(L, keys, b->work.as<uint32_t>(), uint32_t(n_work), b->rec.as<uint32_t>(),
+                                  b->pack.as<uint4>(), b->max_pack, b->values.as<float>(),
+                                  b->counters.as<unsigned long long>(), b->use_tma, s);
+    if (e != cudaSuccess) return set_err(err, errlen, "sample launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    cudaEventRecord(b->ev[3], s);
+
+    // (d) marching cubes: counts, offsets, fill.
+    e = launch_mc(L, uint32_t(count), b->values.as<float>(), b->mc_counts.as<uint32_t>(), nullptr, nullptr, nullptr,
+                  nullptr, nullptr, false, s);
+    if (e != cudaSuccess) return set_err(err, errlen, "mc launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    unsigned long long* tot = b->totals.as<unsigned long long>();
+    launch_scan(b->mc_counts.as<uint32_t>(), uint32_t(count), b->edge_off.as<uint32_t>(), nullptr,
+                b->tiles.as<unsigned long long>(), tot + 1, s);
+    launch_scan(b->mc_counts.as<uint32_t>() + count, uint32_t(count), b->tri_off.as<uint32_t>(), nullptr,
+                b->tiles.as<unsigned long long>(), tot + 2, s);
+    unsigned long long t2[3];
+    CK(cudaMemcpyAsync(t2, tot, 24, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    CK(cudaMemcpyAsync(cnt, b->counters.p, CNT_N * 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (cnt[CNT_TIMEOUT]) return set_err(err, errlen, "a bounded wait for a bulk copy gave up"), SMB_ERR_TIMEOUT;
+    b->n_edges = size_t(t2[1]);
+    b->n_tris = size_t(t2[2]);
+    if (b->n_edges >= (size_t(1) << 32) || b->n_tris >= (size_t(1) << 32))
+        return set_err(err, errlen, "batch too large for 32-bit offsets"), SMB_ERR_MEMORY;
+    uint32_t ne32 = uint32_t(b->n_edges), nt32 = uint32_t(b->n_tris);
+    CK(cudaMemcpyAsync(b->edge_off.as<uint32_t>() + count, &ne32, 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(b->tri_off.as<uint32_t>() + count, &nt32, 4, cudaMemcpyHostToDevice, s));
+    if ((rc = b->edges.reserve(b->n_edges * 4, err, errlen)) || (rc = b->edge_vals.reserve(b->n_edges * 8, err, errlen)) ||
+        (rc = b->tris.reserve(b->n_tris * 12, err, errlen)))
+        return rc;
+    e = launch_mc(L, uint32_t(count), b->values.as<float>(), nullptr, b->edge_off.as<uint32_t>(),
+                  b->tri_off.as<uint32_t>(), b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->tris.as<uint32_t>(),
+                  true, s);
+    if (e != cudaSuccess) return set_err(err, errlen, "mc launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    cudaEventRecord(b->ev[4], s);
+    CK(cudaStreamSynchronize(s));
+    if (times) {
+        float t[4];
+        for (int k = 0; k < 4; k++) cudaEventElapsedTime(&t[k], b->ev[k], b->ev[k + 1]);
+        times->substates = t[0], times->gather = t[1], times->sample = t[2], times->mc = t[3];
+        times->total = double(t[0]) + t[1] + t[2] + t[3];
+    }
+    return SMB_OK;
+}
+
+size_t smb_batch_bricks(const smb_batch* b) { return b ? b->n : 0; }
+
+int smb_batch_records(const smb_batch* b, uint32_t* out) {
+    if (!b || !out) return SMB_ERR_ARG;
+    cudaSetDevice(b->res->dev->index);
+    return cudaMemcpy(out, b->rec.p, size_t(b->n) * 8 * REC_WORDS * 4, cudaMemcpyDeviceToHost) == cudaSuccess
+               ? SMB_OK : SMB_ERR_CUDA;
+}
+
+int smb_batch_values(const smb_batch* b, float* out) {
+    if (!b || !out) return SMB_ERR_ARG;
+    cudaSetDevice(b->res->dev->index);
+    return cudaMemcpy(out, b->values.p, size_t(b->n) * b->res->L.spb * 4, cudaMemcpyDeviceToHost) == cudaSuccess
+               ? SMB_OK : SMB_ERR_CUDA;
+}
+
+size_t smb_batch_ids_words(const smb_batch* b) { return b ? b->ids_words : 0; }
+
+int smb_batch_ids(const smb_batch* b, uint32_t* out) {
+    if (!b || !out) return SMB_ERR_ARG;
+    if (!b->ids_words) return SMB_OK;
+    cudaSetDevice(b->res->dev->index);
+    return cudaMemcpy(out, b->ids.p, b->ids_words * 4, cudaMemcpyDeviceToHost) == cudaSuccess ? SMB_OK : SMB_ERR_CUDA;
+}
+
+int smb_batch_mc_counts(const smb_batch* b, size_t* edges, size_t* triangles) {
+    if (!b) return SMB_ERR_ARG;
+    if (edges) *edges = b->n_edges;
+    if (triangles) *triangles = b->n_tris;
+    return SMB_OK;
+}
+
+int smb_batch_mc(const smb_batch* b, uint32_t* edge_off, uint32_t* edges, float* edge_vals, uint32_t* tri_off,
+                 uint32_t* tris) {
+    if (!b) return SMB_ERR_ARG;
+    cudaSetDevice(b->res->dev->index);
+    size_t n = b->n;
+    bool ok = true;
+    if (edge_off) ok &= cudaMemcpy(edge_off, b->edge_off.p, (n + 1) * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (tri_off) ok &= cudaMemcpy(tri_off, b->tri_off.p, (n + 1) * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (edges && b->n_edges) ok &= cudaMemcpy(edges, b->edges.p, b->n_edges * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (edge_vals && b->n_edges)
+        ok &= cudaMemcpy(edge_vals, b->edge_vals.p, b->n_edges * 8, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (tris && b->n_tris) ok &= cudaMemcpy(tris, b->tris.p, b->n_tris * 12, cudaMemcpyDeviceToHost) == cudaSuccess;
+    return ok ? SMB_OK : SMB_ERR_CUDA;
+}
+
+}  // extern "C"

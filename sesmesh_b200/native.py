@@ -1,0 +1,333 @@
+"""ctypes bindings of the C ABI in include/sesmesh_b200.h.
+
+Loads the in-tree libsesmesh_b200.so (built by `make -C sesmesh_b200`); there
+is no fallback: without the library, or without a CUDA device, the calls
+raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libsesmesh_b200.so")
+SYNTH_PATH = os.path.join(_HERE, "libsesmesh_synth.so")
+
+SMB_OK = 0
+ERRORS = {1: "argument", 2: "cuda", 3: "no device", 4: "self-test", 5: "range", 6: "memory", 7: "state",
+          8: "timeout"}
+REC_WORDS = 12
+
+
+class SmbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("sesmesh_b200 %s error: %s" % (ERRORS.get(code, code), msg))
+        self.code = code
+
+
+class GridRef(C.Structure):
+    _fields_ = [("origin", C.c_double * 3), ("cell", C.c_double), ("dims", C.c_uint32 * 3),
+                ("starts", C.POINTER(C.c_uint32)), ("items", C.POINTER(C.c_uint32)), ("n_items", C.c_size_t)]
+
+
+class ArrangementRef(C.Structure):
+    _fields_ = [("n_spheres", C.c_size_t), ("center", C.POINTER(C.c_double)), ("expanded", C.POINTER(C.c_double)),
+                ("radius", C.POINTER(C.c_double)), ("status", C.POINTER(C.c_uint32)),
+                ("nb_off", C.POINTER(C.c_uint32)), ("nb_items", C.POINTER(C.c_uint32)),
+                ("n_circles", C.c_size_t), ("circle", C.POINTER(C.c_double)), ("cb_off", C.POINTER(C.c_uint32)),
+                ("cb_items", C.POINTER(C.c_uint32)), ("n_vertices", C.c_size_t), ("vertex", C.POINTER(C.c_double)),
+                ("sphere_grid", GridRef), ("circle_grid", GridRef), ("vertex_grid", GridRef),
+                ("max_expanded", C.c_double), ("rho_max", C.c_double), ("probe", C.c_double)]
+
+
+class LatticeRef(C.Structure):
+    _fields_ = [("spacing", C.c_double), ("brick", C.c_uint32), ("frame", C.c_int64 * 3), ("band", C.c_double)]
+
+
+class BatchTimes(C.Structure):
+    _fields_ = [("substates", C.c_double), ("gather", C.c_double), ("sample", C.c_double), ("mc", C.c_double),
+                ("total", C.c_double)]
+
+
+class DeviceInfo(C.Structure):
+    _fields_ = [("name", C.c_char * 256), ("major", C.c_int), ("minor", C.c_int), ("multiprocessors", C.c_int),
+                ("memory", C.c_size_t)]
+
+
+# Every entry point of include/sesmesh_b200.h with its ctypes signature.
+_vp, _sz, _cp = C.c_void_p, C.c_size_t, C.c_char_p
+_u32p, _i32p, _fp = C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.POINTER(C.c_float)
+SIGNATURES = {
+    "smb_open": (C.c_int, [C.c_int, C.POINTER(_vp), _cp, _sz]),
+    "smb_close": (None, [_vp]),
+    "smb_device_info_get": (C.c_int, [_vp, C.POINTER(DeviceInfo)]),
+    "smb_self_test": (C.c_int, [_vp, C.c_uint32, _cp, _sz]),
+    "smb_resident_new": (C.c_int, [_vp, C.POINTER(ArrangementRef), C.POINTER(LatticeRef), C.POINTER(_vp), _cp, _sz]),
+    "smb_resident_free": (None, [_vp]),
+    "smb_resident_bytes": (_sz, [_vp]),
+    "smb_classify": (C.c_int, [_vp, C.POINTER(_sz), C.POINTER(_sz), _cp, _sz]),
+    "smb_resident_bricks": (C.c_int, [_vp, _i32p, _sz]),
+    "smb_batch_new": (C.c_int, [_vp, C.POINTER(_vp), _cp, _sz]),
+    "smb_batch_free": (None, [_vp]),
+    "smb_run": (C.c_int, [_vp, _sz, _sz, _vp, C.POINTER(BatchTimes), _cp, _sz]),
+    "smb_batch_bricks": (_sz, [_vp]),
+    "smb_batch_records": (C.c_int, [_vp, _u32p]),
+    "smb_batch_values": (C.c_int, [_vp, _fp]),
+    "smb_batch_ids_words": (_sz, [_vp]),
+    "smb_batch_ids": (C.c_int, [_vp, _u32p]),
+    "smb_batch_mc_counts": (C.c_int, [_vp, C.POINTER(_sz), C.POINTER(_sz)]),
+    "smb_batch_mc": (C.c_int, [_vp, _u32p, _u32p, _fp, _u32p, _u32p]),
+}
+
+_LIB = None
+
+
+def lib():
+    """The loaded C-ABI library (raises if it was not built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libsesmesh_b200.so is not built (run `make -C sesmesh_b200`)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _p(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+def _check(rc, err):
+    if rc != SMB_OK:
+        raise SmbError(rc, err.value.decode(errors="replace"))
+
+
+class Device:
+    """An open CUDA device (smb_open: self-test included)."""
+
+    def __init__(self, index=0):
+        err = C.create_string_buffer(1024)
+        h = _vp()
+        _check(lib().smb_open(index, C.byref(h), err, 1024), err)
+        self.h = h
+        info = DeviceInfo()
+        lib().smb_device_info_get(self.h, C.byref(info))
+        self.name = info.name.decode()
+        self.capability = (info.major, info.minor)
+        self.multiprocessors = info.multiprocessors
+        self.memory = info.memory
+
+    def self_test(self, n):
+        err = C.create_string_buffer(1024)
+        _check(lib().smb_self_test(self.h, n, err, 1024), err)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().smb_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def _grid(g, keep):
+    starts = np.ascontiguousarray(g["starts"], np.uint32)
+    items = np.ascontiguousarray(g["items"], np.uint32)
+    if len(items) == 0:
+        items = np.zeros(1, np.uint32)
+        n_items = 0
+    else:
+        n_items = len(g["items"])
+    keep += [starts, items]
+    r = GridRef()
+    r.origin[:] = [float(v) for v in g["origin"]]
+    r.cell = float(g["cell"])
+    r.dims[:] = [int(v) for v in g["dims"]]
+    r.starts = _p(starts, C.c_uint32)
+    r.items = _p(items, C.c_uint32)
+    r.n_items = n_items
+    return r
+
+
+class Resident:
+    """The arrangement resident on a device (smb_resident_new).
+
+    `arr` holds numpy arrays in internal sphere order: center (n, 3),
+    expanded (n,), radius (n,), status (n,), nb_off/nb_items,
+    circle (nc, 10), cb_off/cb_items, vertex (nv, 3), grids
+    sphere_grid/circle_grid/vertex_grid (dicts of origin, cell, dims, starts,
+    items) and max_expanded, rho_max, probe.  `lat` holds spacing, brick,
+    frame (3 ints) and band.
+    """
+
+    def __init__(self, device, arr, lat):
+        self.device = device
+        keep = []
+
+        def arrf(x, dt, shape=None):
+            a = np.ascontiguousarray(x, dt)
+            if a.size == 0:
+                a = np.zeros(1, dt)
+            keep.append(a)
+            return _p(a, C.c_double if dt == np.float64 else C.c_uint32)
+
+        n = len(arr["expanded"])
+        ref = ArrangementRef()
+        ref.n_spheres = n
+        ref.center = arrf(arr["center"], np.float64)
+        ref.expanded = arrf(arr["expanded"], np.float64)
+        ref.radius = arrf(arr["radius"], np.float64)
+        ref.status = arrf(arr["status"], np.uint32)
+        ref.nb_off = arrf(arr["nb_off"], np.uint32)
+        ref.nb_items = arrf(arr["nb_items"], np.uint32)
+        ref.n_circles = len(arr["circle"])
+        ref.circle = arrf(arr["circle"], np.float64)
+        ref.cb_off = arrf(arr["cb_off"], np.uint32)
+        ref.cb_items = arrf(arr["cb_items"], np.uint32)
+        ref.n_vertices = len(arr["vertex"])
+        ref.vertex = arrf(arr["vertex"], np.float64)
+        ref.sphere_grid = _grid(arr["sphere_grid"], keep)
+        ref.circle_grid = _grid(arr["circle_grid"], keep)
+        ref.vertex_grid = _grid(arr["vertex_grid"], keep)
+        ref.max_expanded = float(arr["max_expanded"])
+        ref.rho_max = float(arr["rho_max"])
+        ref.probe = float(arr["probe"])
+        L = LatticeRef()
+        L.spacing = float(lat["spacing"])
+        L.brick = int(lat["brick"])
+        L.frame[:] = [int(v) for v in lat["frame"]]
+        L.band = float(lat["band"])
+        self.brick = int(lat["brick"])
+        err = C.create_string_buffer(1024)
+        h = _vp()
+        _check(lib().smb_resident_new(device.h, C.byref(ref), C.byref(L), C.byref(h), err, 1024), err)
+        self.h = h
+        self.n_bricks = 0
+
+    def classify(self):
+        err = C.create_string_buffer(1024)
+        t, s = _sz(0), _sz(0)
+        _check(lib().smb_classify(self.h, C.byref(t), C.byref(s), err, 1024), err)
+        self.n_bricks = s.value
+        return t.value, s.value
+
+    def bricks(self):
+        out = np.zeros((max(self.n_bricks, 1), 3), np.int32)
+        rc = lib().smb_resident_bricks(self.h, _p(out, C.c_int32), self.n_bricks)
+        if rc != SMB_OK:
+            raise SmbError(rc, "smb_resident_bricks")
+        return out[:self.n_bricks]
+
+    @property
+    def bytes(self):
+        return lib().smb_resident_bytes(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().smb_resident_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Batch:
+    """Batch buffers (smb_batch_new) and the results of the last run."""
+
+    def __init__(self, resident):
+        self.res = resident
+        err = C.create_string_buffer(1024)
+        h = _vp()
+        _check(lib().smb_batch_new(resident.h, C.byref(h), err, 1024), err)
+        self.h = h
+
+    def run(self, first=0, count=None):
+        if count is None:
+            count = self.res.n_bricks - first
+        err = C.create_string_buffer(1024)
+        t = BatchTimes()
+        _check(lib().smb_run(self.res.h, first, count, self.h, C.byref(t), err, 1024), err)
+        return dict(substates=t.substates, gather=t.gather, sample=t.sample, mc=t.mc, total=t.total)
+
+    @property
+    def n(self):
+        return lib().smb_batch_bricks(self.h)
+
+    def records(self):
+        out = np.zeros((self.n * 8, REC_WORDS), np.uint32)
+        if self.n:
+            lib().smb_batch_records(self.h, _p(out, C.c_uint32))
+        return out
+
+    def values(self):
+        s = self.res.brick + 1
+        out = np.zeros((self.n, s * s * s), np.float32)
+        if self.n:
+            lib().smb_batch_values(self.h, _p(out, C.c_float))
+        return out
+
+    def ids(self):
+        n = lib().smb_batch_ids_words(self.h)
+        out = np.zeros(max(n, 1), np.uint32)
+        if n:
+            lib().smb_batch_ids(self.h, _p(out, C.c_uint32))
+        return out[:n]
+
+    def lists(self, rec, ids):
+        """The candidate lists of one sampled sub-block's record."""
+        base, n_in, nn, ns, nc, nv, nsb, ncb = (int(rec[k]) for k in (1, 2, 3, 4, 5, 6, 7, 8))
+        out = {"n_inside": n_in}
+        pos = base
+        for key, cnt in (("near", nn), ("s", ns), ("s_off", ns + 1), ("s_blk", nsb), ("c", nc),
+                         ("c_off", nc + 1), ("c_blk", ncb), ("v", nv)):
+            out[key] = ids[pos:pos + cnt]
+            pos += cnt
+        return out
+
+    def mc(self):
+        ne, nt = _sz(0), _sz(0)
+        lib().smb_batch_mc_counts(self.h, C.byref(ne), C.byref(nt))
+        n = self.n
+        eo = np.zeros(n + 1, np.uint32)
+        to = np.zeros(n + 1, np.uint32)
+        edges = np.zeros(max(ne.value, 1), np.uint32)
+        vals = np.zeros((max(ne.value, 1), 2), np.float32)
+        tris = np.zeros((max(nt.value, 1), 3), np.uint32)
+        if n:
+            lib().smb_batch_mc(self.h, _p(eo, C.c_uint32), _p(edges, C.c_uint32), _p(vals, C.c_float),
+                               _p(to, C.c_uint32), _p(tris, C.c_uint32))
+        return dict(edge_off=eo, edges=edges[:ne.value], edge_vals=vals[:ne.value], tri_off=to,
+                    tris=tris[:nt.value])
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().smb_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+# ---- seeded synthetic inputs (libsesmesh_synth.so) -------------------------
+_SYN = None
+
+
+def synth():
+    global _SYN
+    if _SYN is None:
+        if not os.path.exists(SYNTH_PATH):
+            raise OSError("libsesmesh_synth.so is not built (run `make -C sesmesh_b200`)")
+        L = C.CDLL(SYNTH_PATH)
+        L.smb_synth_globule.restype = _sz
+        L.smb_synth_globule.argtypes = [C.c_uint64, _sz, C.c_double, C.POINTER(C.c_double)]
+        L.smb_synth_rings.restype = _sz
+        L.smb_synth_rings.argtypes = [C.c_uint64, _sz, C.c_double, C.c_int, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.smb_synth_icosahedral.restype = _sz
+        L.smb_synth_icosahedral.argtypes = [C.c_uint64, _sz, C.c_double, C.c_double, C.POINTER(C.c_double)]
+        _SYN = L
+    return _SYN
