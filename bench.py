@@ -1,0 +1,323 @@
+#!/usr/bin/env python3
+"""Benchmark of the SES mesh stage on B200 (one JSON line on rank 0).
+
+Workload (N=1): rings58800 -- 58,800 spheres (21 copies of a seeded
+2,800-sphere globule on three stacked 7-fold rings), probe 1.4 A, spacing
+0.25 A, brick 10, exact mode: sesmesh's 1AON-at-0.25-A analogue.
+
+* value -- device mesh-stage throughput in Mgridpts/s (grid points =
+  surface bricks x (b+1)^3, as sesmesh counts samples) with the arrangement
+  resident in HBM: brick classification, sub-block states, candidate gather,
+  field sampling and marching-cubes compaction, timed with CUDA events on the
+  library's stream; L2 flushed (256 MiB write) before every step.
+* e2e -- the same metric through the public API (compute_surface from host
+  sphere arrays): host arrangement, upload, device stage, copies back, host
+  f64 refinement, assembly, validation, components; wall clock.
+* roofline -- the dominant kernel against its bound.
+* cpu_baseline -- the CPU oracle (C++ restatement of sesmesh's CPU back end)
+  meshing a sample of the same bricks on all host cores.
+
+--impl reference runs that CPU path alone (the reference's own CPU back end
+is Rust and cannot be built here; the oracle is its restatement).
+Multi-GPU: independent replicas (one structure per GPU, no collective on the
+data path); value = all ranks' grid points / max-over-ranks step time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# FP32 lanes x SMs x max clock, one operation per lane per cycle: the bound
+# of kernels that may not contract multiply-adds (bit-exact f32).
+FP32_NOFMA_TOPS = 148 * 128 * 1.965e9 / 1e12
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="rings58800", choices=["rings58800", "globule330", "shell2400k"])
+    p.add_argument("--refine", default=None, choices=[None, "exact", "fast"])
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    return p.parse_args()
+
+
+def workload(name, refine=None):
+    from sesmesh_b200 import workloads
+    w = {"rings58800": workloads.rings58800, "globule330": workloads.globule330,
+         "shell2400k": workloads.shell2400k}[name]()
+    if refine:
+        w["refine"] = refine
+    return w
+
+
+def describe(w):
+    return ("%s: %d spheres, probe %.1f A, spacing %g A, brick %d, %s" %
+            (w["name"], len(w["spheres"]), w["probe"], w["spacing"], w["brick"], w["refine"]))
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_leg(w, budget_s=20.0):
+    """CPU oracle on a deterministic sample of the workload's surface bricks
+    (every k-th brick), all host threads: grid points per second."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    eng = O.Engine(w["spheres"], w["probe"], w["spacing"], w["brick"])
+    bricks, _ = eng.classify()
+    spb = (w["brick"] + 1) ** 3
+    # Calibrate on a small sample, then size the sample to the time budget.
+    k0 = max(1, len(bricks) // 500)
+    t, _ = eng.mesh_sample(bricks[::k0])
+    per_brick = t / max(1, len(bricks[::k0]))
+    n_want = int(min(len(bricks), max(256, budget_s / max(per_brick, 1e-9))))
+    k = max(1, len(bricks) // n_want)
+    sample = bricks[::k]
+    return eng, sample, spb, k, len(bricks)
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload(a.workload, a.refine)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    eng, sample, spb, k, nb = cpu_leg(w, budget_s=6.0)
+    for _ in range(a.warmup):
+        eng.mesh_sample(sample[: max(1, len(sample) // 4)])
+    times = []
+    for _ in range(a.steps):
+        t, _ = eng.mesh_sample(sample)
+        times.append(t)
+    ms = 1e3 * float(np.mean(times))
+    value = len(sample) * spb / (np.mean(times)) / 1e6
+    cores = O.threads()
+    line = {
+        "impl": "reference", "metric": "Mgridpts/s (SES mesh stage)", "value": value, "unit": "Mgridpts/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+        "config": {"workload": describe(w), "surface_bricks": nb, "sample": "every %d-th surface brick (%d bricks)" % (k, len(sample)),
+                   "stage": "Engine::evaluate + mesh_brick (exact f64 refinement) per brick"},
+        "cpu_baseline": {"value": value, "unit": "Mgridpts/s", "cores": cores, "kind": "port",
+                         "sample": "%d of %d surface bricks of %s" % (len(sample), nb, w["name"])},
+        "e2e": {"value": value, "unit": "Mgridpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(a):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(x):
+        t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
+        if dist is not None:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from sesmesh_b200 import native
+    from sesmesh_b200 import surface as S
+    w = workload(a.workload, a.refine)
+    params = S.SurfaceParams.ses(w["probe"]).with_spacing(w["spacing"]).with_brick_size(w["brick"]).with_refine(
+        w["refine"])
+    params = S.SurfaceParams(**{**params.__dict__, "device": local})
+    eng = S.SurfaceEngine(w["spheres"], params)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for _ in range(max(3, a.warmup)):
+        eng.run_device()
+    n_bricks = eng.bricks
+    spb = (w["brick"] + 1) ** 3
+    grid_points = n_bricks * spb
+    launches0 = native.lib().smb_kernel_launches()
+    clocks = Clocks(local)
+    barrier()
+    step_ms, parts = [], []
+    for _ in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t = eng.run_device()
+        cls = eng.batch_info()["classify_ms"]
+        step_ms.append(cls + t["total"])
+        parts.append(dict(t, classify=cls))
+    barrier()
+    clk = clocks.stop()
+    launches = native.lib().smb_kernel_launches() - launches0
+    mean_ms = max_over_ranks(float(np.mean(step_ms)))
+    value = world * grid_points / (mean_ms / 1e3) / 1e6
+    stage = {k: float(np.mean([p[k] for p in parts])) for k in ("classify", "substates", "gather", "sample", "mc")}
+    if w["refine"] == "fast":
+        stage["refine"] = float(np.mean([p["total"] - p["substates"] - p["gather"] - p["sample"] - p["mc"]
+                                         for p in parts]))
+    dominant = max(stage, key=stage.get)
+
+    # End to end through the public API, host arrays in, mesh out.
+    e2e_ms, st = [], None
+    out = S.compute_surface(w["spheres"], params)  # warm-up
+    for _ in range(a.e2e_steps):
+        barrier()
+        t0 = time.perf_counter()
+        out = S.compute_surface(w["spheres"], params)
+        torch.cuda.synchronize(dev)
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    st = out.stats
+    e2e_mean = max_over_ranks(float(np.mean(e2e_ms)))
+    info = eng.batch_info()
+    h2d = int(info["resident_bytes"])
+    d2h = int(n_bricks * 16 + (n_bricks + 1) * 8 + st["vertices"] * 12 + st["triangles"] * 12)
+    if w["refine"] == "fast":
+        d2h += int(st["vertices"] * 24)
+
+    pk, pk_kind = peaks()
+    ops, owned = eng.count_ops()
+    roof = roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks)
+    line = {
+        "metric": "Mgridpts/s (SES mesh stage)", "value": value, "unit": "Mgridpts/s", "n_gpus": world,
+        "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": mean_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+        "config": {"workload": describe(w), "spheres": int(len(w["spheres"])), "surface_bricks": int(n_bricks),
+                   "grid_points": int(grid_points), "refine": w["refine"], "parallelism": "replicas x%d" % world,
+                   "l2": "flushed before every step (256 MiB write)"},
+        "stage_ms": stage,
+        "e2e": {"value": world * grid_points / (e2e_mean / 1e3) / 1e6, "unit": "Mgridpts/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_mesh": e2e_mean,
+                "host_threads": st["host_threads"],
+                "stages_ms": {k: st[k] for k in ("t_geometry", "t_upload", "t_device", "t_d2h", "t_host_refine",
+                                                 "t_assemble", "t_measure", "t_total")},
+                "mesh": {"vertices": st["vertices"], "triangles": st["triangles"], "area": st["area"],
+                         "volume": st["volume"], "refine_evaluations": st["refine_evaluations"],
+                         "refine_cpu_edges": st["refine_cpu_edges"]}},
+        "roofline": roof,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not a.no_cpu:
+        ceng, sample, spb_, k, nb = cpu_leg(w)
+        t, _ = ceng.mesh_sample(sample)
+        import oracle as O
+        line["cpu_baseline"] = {"value": len(sample) * spb_ / t / 1e6, "unit": "Mgridpts/s", "cores": O.threads(),
+                                "kind": "port",
+                                "sample": "every %d-th of %d surface bricks (%d bricks, %.1f s): CPU oracle evaluate + "
+                                          "mesh_brick (exact f64 refinement)" % (k, nb, len(sample), t)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    del out
+    eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks):
+    """Roofline of the dominant kernel (per-unit counts in DESIGN.md)."""
+    ms = stage[dominant]
+    hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
+    spb = (w["brick"] + 1) ** 3
+    if dominant == "sample":
+        achieved = ops / (ms / 1e3) / 1e12
+        return {"kernel": "k_sample", "bound": "fp32", "achieved": achieved, "peak": FP32_NOFMA_TOPS,
+                "unit": "Tops/s", "frac": achieved / FP32_NOFMA_TOPS, "traffic": None,
+                "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 1965 MHz, one op per lane-cycle "
+                               "(no FMA contraction, bit-exact f32)",
+                "algorithmic_ops": ops, "evaluated_samples": owned, "ms": ms}
+    if dominant == "gather":
+        algo = info["ids_words"] * 4 + info["pack_units"] * 16
+        kern = "k_gather"
+    elif dominant == "mc":
+        algo = n_bricks * spb * 4 + info["edges"] * 12 + info["triangles"] * 12
+        kern = "k_mc"
+    else:
+        algo = n_bricks * spb * 4
+        kern = "k_" + dominant
+    achieved = algo / (ms / 1e3) / 1e9
+    return {"kernel": kern, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": None, "peak_source": pk_kind, "algorithmic_bytes": algo, "ms": ms}
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

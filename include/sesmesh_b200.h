@@ -159,6 +159,37 @@ int smb_batch_mc_counts(const smb_batch* batch, size_t* edges, size_t* triangles
 int smb_batch_mc(const smb_batch* batch, uint32_t* edge_off, uint32_t* edges, float* edge_vals, uint32_t* tri_off,
                  uint32_t* tris);
 
+/* Fast mode: refinement settings (Resident::set_refinement and RefineRef,
+ * batch.rs:133-150, field/gpu.rs:207-221): tolerance 1e-5 A, at most 8
+ * Newton / Illinois evaluations then 64 bisection steps, f32 brick-local
+ * coordinates from double-float pairs. */
+int smb_resident_set_refinement(smb_resident* res, char* err, size_t errlen);
+/* Refines the crossing edges of the last run in f32 on the device
+ * (cuda::Resident::refine, cuda/resident.rs:632-688); *ms gets the device
+ * time.  Results are indexed like the marching-cubes edges. */
+int smb_refine(smb_resident* res, smb_batch* batch, double* ms, char* err, size_t errlen);
+/* Per edge: parameter t, feature (kind << 29 | id; kinds 0 solvent,
+ * 1 beyond, 2 sphere, 3 circle, 4 SAS vertex), closest point relative to the
+ * brick origin (3 floats), evaluations | 1 << 31 if Newton / Illinois
+ * converged (DeviceBatch::edge_*, batch.rs:222-232). */
+int smb_batch_edges(const smb_batch* batch, float* t, uint32_t* feat, float* closest, uint32_t* evals);
+
+/* Sizes and times of the last run of a batch (diagnostics; BatchTimes and
+ * DeviceBatch::bytes, batch.rs:118-129, 233). */
+typedef struct {
+    size_t bricks, sampled_subblocks, ids_words, max_pack_units, edges, triangles, touched, resident_bytes;
+    unsigned long long pack_units;
+    double classify_ms;
+} smb_batch_info;
+int smb_batch_info_get(const smb_batch* batch, smb_batch_info* out);
+/* Re-runs the sampling pass of the last run counting its f32 arithmetic
+ * operations as executed and the samples it evaluated (the algorithmic
+ * count of the roofline; values are rewritten identically). */
+int smb_batch_count_ops(smb_batch* batch, unsigned long long* ops, unsigned long long* samples, char* err,
+                        size_t errlen);
+/* Kernels this library has launched in the process (diagnostics). */
+unsigned long long smb_kernel_launches(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,87 @@
+/*
+ * sesmesh_b200 — host API of the mesh stage with the B200 back end: the
+ * counterpart of compute_surface / SurfaceEngine with Backend::Cuda
+ * (crates/sesmesh/src/surface.rs:599-711) for the SES, refine exact or fast.
+ * The host keeps what sesmesh keeps on the CPU (arrangement, f64 root
+ * refinement in exact mode, assembly, validation, components, OBJ); the
+ * device runs classification, gather, sampling, marching cubes and, in fast
+ * mode, f32 refinement through include/sesmesh_b200.h.
+ */
+#ifndef SESMESH_B200_SURFACE_H
+#define SESMESH_B200_SURFACE_H
+
+#include "sesmesh_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { SMB_SES = 0 };
+enum { SMB_REFINE_EXACT = 0, SMB_REFINE_LINEAR = 1, SMB_REFINE_FAST = 2 };
+
+/* SurfaceParams (surface.rs:195-241) restricted to what the device path
+ * takes: SES, spacing, brick_size (even, 4..32; reference default 10),
+ * refine exact | fast.  threads: host threads (0 = all cores). */
+typedef struct {
+    int kind;
+    double probe_radius;
+    double spacing;
+    uint32_t brick_size;
+    int refine;
+    int threads;
+} smb_surface_params;
+
+/* SurfaceStats (surface.rs:506-562) plus per-stage times in milliseconds. */
+typedef struct {
+    size_t spheres, touched_bricks, surface_bricks, samples, vertices, triangles, components;
+    double area, volume;
+    int64_t euler;
+    uint64_t refine_evaluations, refine_cpu_edges;
+    double t_geometry, t_upload, t_classify, t_substates, t_gather, t_sample, t_mc, t_device, t_d2h, t_host_refine,
+        t_mesh_stage, t_assemble, t_measure, t_total;
+    int host_threads;
+} smb_surface_stats;
+
+typedef struct smb_engine smb_engine;
+typedef struct smb_surface smb_surface;
+
+/* compute_surface (surface.rs:599): spheres as n rows (x, y, z, r). */
+int smb_compute_surface(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p,
+                        smb_surface** out, char* err, size_t errlen);
+/* SurfaceEngine-style reuse: arrangement and upload once, then meshes. */
+int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out,
+                   char* err, size_t errlen);
+void smb_engine_free(smb_engine* e);
+int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size_t errlen);
+size_t smb_engine_bricks(const smb_engine* e);
+int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen);
+/* The engine's device batch (sizes, counters, operation counts). */
+smb_batch* smb_engine_batch(smb_engine* e);
+
+void smb_surface_free(smb_surface* s);
+int smb_surface_stats_get(const smb_surface* s, smb_surface_stats* out);
+/* Mesh arrays (Mesh, mesh/mod.rs:48-67), triangles grouped by component. */
+int smb_surface_mesh(const smb_surface* s, float* positions, float* normals, uint32_t* triangles, uint32_t* atoms,
+                     uint8_t* patches, uint32_t* components);
+/* OBJ bytes with the default options (export/obj.rs:37-73): returns the
+ * length, copies at most cap bytes. */
+size_t smb_surface_obj(smb_surface* s, char* out, size_t cap);
+int smb_surface_write_obj(smb_surface* s, const char* path, char* err, size_t errlen);
+
+/* The host arrangement of an engine (views valid while it lives). */
+typedef struct {
+    size_t n_spheres, n_contained, n_circles, n_vertices;
+    const double *center, *expanded, *circle, *vertex;
+    const uint32_t *status, *orig, *circle_ij, *vertex_atoms, *nb_off, *nb_items, *cb_off, *cb_items;
+    double max_expanded, rho_max, band, t_min;
+    int64_t frame[3];
+} smb_arrangement_info;
+int smb_engine_arrangement(const smb_engine* e, smb_arrangement_info* out);
+/* Builds only the host arrangement (no device; smb_engine_arrangement). */
+int smb_arrangement_build(const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out, char* err,
+                          size_t errlen);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -197,6 +197,30 @@ void orc_engine_field(void* hp, const double* pts, size_t n, double* out) {
     });
 }
 
+// CPU mesh stage on a sample of bricks (Engine::evaluate + mesh_brick per
+// brick, chunks of bricks over all threads, as fold_brick_chunks_with):
+// wall seconds; *evals gets the refinement evaluations.
+double orc_engine_mesh_sample(void* hp, const int32_t* bricks, size_t n, uint64_t* evals) {
+    const Engine& e = static_cast<Handle*>(hp)->e;
+    auto t0 = std::chrono::steady_clock::now();
+    size_t chunk = std::min<size_t>(std::max<size_t>(n / 256, 1), 4096);
+    size_t nchunks = (n + chunk - 1) / chunk;
+    std::vector<BrickMesh> parts(nchunks);
+    std::vector<BrickScratch> sc(static_cast<size_t>(threads()));
+    for (auto& s : sc) s.init(e);
+    parallel_for(nchunks, [&](size_t c, int w) {
+        for (size_t i = c * chunk; i < std::min(n, (c + 1) * chunk); i++) {
+            evaluate(e, bricks + 3 * i, sc[size_t(w)]);
+            mesh_brick(e, bricks + 3 * i, sc[size_t(w)].values.data(), parts[c]);
+        }
+    });
+    double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    uint64_t ev = 0;
+    for (auto& p : parts) ev += p.evals;
+    if (evals) *evals = ev;
+    return s;
+}
+
 // Whole CPU pipeline; returns a handle or null with err set.
 void* orc_surface_new(const double* xyzr, size_t n, double probe, double spacing, size_t brick, char* err,
                       size_t errlen) {

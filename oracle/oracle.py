@@ -44,6 +44,8 @@ def lib():
         L.orc_engine_gather.argtypes = [vp, i32p, C.c_int, u32p, sz]
         L.orc_mc_brick.argtypes = [C.c_int, fp, u32p, u32p, C.POINTER(sz)]
         L.orc_engine_field.argtypes = [vp, dp, sz, dp]
+        L.orc_engine_mesh_sample.restype = C.c_double
+        L.orc_engine_mesh_sample.argtypes = [vp, i32p, sz, C.POINTER(C.c_uint64)]
         L.orc_surface_new.restype = vp
         L.orc_surface_new.argtypes = [dp, sz, C.c_double, C.c_double, sz, C.c_char_p, sz]
         L.orc_surface_free.argtypes = [vp]
@@ -175,6 +177,14 @@ class Engine:
             out[key] = w[pos:pos + cnt].copy()
             pos += cnt
         return out
+
+    def mesh_sample(self, bricks):
+        """Wall seconds of the CPU mesh stage (evaluate + mesh_brick) on the
+        given bricks, all threads; and the refinement evaluations."""
+        b = np.ascontiguousarray(bricks, np.int32).reshape(-1, 3)
+        ev = C.c_uint64(0)
+        s = lib().orc_engine_mesh_sample(self.h, _p(b, C.c_int32), len(b), C.byref(ev))
+        return s, ev.value
 
     def field(self, pts):
         p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)

@@ -6,6 +6,7 @@
 // -ftz=false.  f64 decisions (classification, list membership, list order)
 // and f32 sample values follow the CPU back end of sesmesh 1.3.2
 // operation by operation, so every output is bit-identical to it.
+#include <atomic>
 #include <cstdio>
 
 #include "common.cuh"
@@ -559,7 +560,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 constexpr uint32_t BULK_CHUNK = 32768;            // bytes per bulk copy
 constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;     // bounded wait
 
-template <bool TMA>
+template <bool TMA, bool COUNT>
 __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const uint32_t* work, uint32_t n_work,
                                                 const uint32_t* rec, const uint4* pack, float* values,
                                                 unsigned long long* counters) {
@@ -615,12 +616,16 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
                     gz = (long long)key.z * L.b - L.frame[2];
     const float probe = L.probe32, cutoff2 = L.cutoff2;
     float* out = values + size_t(brick) * L.spb;
+    // COUNT: arithmetic operations as executed (the algorithmic count of the
+    // roofline; compares and selects are not counted).
+    unsigned long long ops = 0, owned = 0;
     for (int t = threadIdx.x; t < sp * sp * sp; t += blockDim.x) {
         int x = ox + t % sp, y = oy + (t / sp) % sp, z = oz + t / (sp * sp);
         bool positive;
         if (sample_owner(x, y, z, sub, st, &positive) != int(sb)) continue;
         // Lattice::local (field/lattice.rs:69): from integers only.
         const float px = float(gx + x) * L.h32, py = float(gy + y) * L.h32, pz = float(gz + z) * L.h32;
+        if (COUNT) owned++, ops += 8ull * n_in;
         bool inside = false;
         for (int k = 0; k < n_in; k++) {
             float4 a = nearA[k];
@@ -629,6 +634,7 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
         }
         float value = probe;
         if (inside) {
+            if (COUNT) ops += 9ull * nv + 12ull * ns + 26ull * nc + 2;
             float best2 = cutoff2;
             for (int v = 0; v < nv; v++) {
                 float4 q = V[v];
@@ -643,9 +649,11 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
                 float lb2 = lb * lb;
                 bool valid = lb2 < best2 && 1e-6f < dist;
                 if (!valid) continue;
+                if (COUNT) ops += 7;
                 float scale = c.w / dist;
                 float qx = c.x + dx * scale, qy = c.y + dy * scale, qz = c.z + dz * scale;
                 for (uint32_t p = s_off[si], e = s_off[si + 1]; p < e; p++) {
+                    if (COUNT) ops += 8;
                     float4 b = nearT[s_blk[p]];
                     float ex = qx - b.x, ey = qy - b.y, ez = qz - b.z;
                     if (!((ex * ex + ey * ey + ez * ez) >= b.w)) {
@@ -664,6 +672,7 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
                 float tt = wl - m.w;
                 float d2 = along * along + tt * tt;
                 if (!(d2 < best2)) continue;
+                if (COUNT) ops += 7;
                 bool degenerate = wl < 1e-6f;
                 float s = m.w / wl;
                 float qx = degenerate ? m.x + u.w * m.w : m.x + wx * s;
@@ -671,6 +680,7 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
                 float qz = degenerate ? m.z + e2.y * m.w : m.z + wz * s;
                 bool valid = true;
                 for (uint32_t p = c_off[ci], e = c_off[ci + 1]; p < e; p++) {
+                    if (COUNT) ops += 8;
                     float4 b = nearT[c_blk[p]];
                     float ex = qx - b.x, ey = qy - b.y, ez = qz - b.z;
                     if (!((ex * ex + ey * ey + ez * ez) >= b.w)) {
@@ -683,6 +693,10 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
             value = probe - sqrtf(best2);
         }
         out[(z * side + y) * side + x] = value;
+    }
+    if (COUNT) {
+        atomicAdd(&counters[CNT_OPS], ops);
+        atomicAdd(&counters[CNT_OWNED], owned);
     }
 }
 
@@ -765,9 +779,280 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L, uint32_t n_bricks, co
     }
 }
 
+
 // ---------------------------------------------------------------------------
-// Host launchers.
+// (e) Fast mode: f32 root refinement of the crossing edges on the device,
+// the reference's definition of plain f32 refinement (sesmesh-gpu
+// kernels/sesmesh.cuh:445-750): brick-local coordinates from double-float
+// pairs (frame-local f32 value + f32 residual, minus the brick origin as an
+// exact product pair), safeguarded Newton / Illinois (at most max_iter
+// evaluations) then bisection.  One CTA per sampled sub-block: its candidate
+// lists (the gather's, bit-identical to the CPU's) are turned into
+// brick-local coordinates once, in shared memory; each thread refines the
+// brick's crossing edges whose lower sample lies in the sub-block.
+
+__device__ __forceinline__ void split_df(double v, float& hi, float& lo) {
+    hi = float(v);
+    lo = float(v - double(hi));
+}
+
+// O * h as a pair (hi, lo): hi = O h_hi rounded, lo = its error + O h_lo.
+__device__ __forceinline__ void origin_pair(long long o, float h_hi, float h_lo, float& hi, float& lo) {
+    float of = float(o);
+    hi = of * h_hi;
+    lo = fmaf(of, h_hi, -hi) + of * h_lo;
+}
+
+struct RefOut {
+    float* t;
+    uint32_t* feat;
+    float* q;
+    uint32_t* evals;
+};
+
+constexpr uint32_t FEAT_SHIFT_D = 29;
+
+__global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC, const int4* keys, const uint32_t* work,
+                                                uint32_t n_work, const uint32_t* rec, const uint32_t* ids,
+                                                const uint32_t* edge_off, const uint32_t* edges,
+                                                const float2* edge_vals, RefOut out) {
+    extern __shared__ __align__(16) float4 rs[];
+    const uint32_t j = work[blockIdx.x];
+    const uint32_t brick = j >> 3, sb = j & 7;
+    const uint32_t* R = rec + size_t(j) * REC_WORDS;
+    if (R[R_STATE] != ST_SAMPLE || R[R_FLAGS] != 0) return;
+    const int nn = int(R[R_NEAR]), n_in = int(R[R_INSIDE]), ns = int(R[R_S]), nc = int(R[R_C]), nv = int(R[R_V]);
+    const int nsb = int(R[R_SBLK]), ncb = int(R[R_CBLK]);
+    const uint32_t* l_near = ids + R[R_IDS];
+    const uint32_t* l_s = l_near + nn;
+    const uint32_t* l_soff = l_s + ns;
+    const uint32_t* l_sblk = l_soff + ns + 1;
+    const uint32_t* l_c = l_sblk + nsb;
+    const uint32_t* l_coff = l_c + nc;
+    const uint32_t* l_cblk = l_coff + nc + 1;
+    const uint32_t* l_v = l_cblk + ncb;
+    // Shared layout: near (x, y, z, R) and (x, y, z, (R - tol)^2), S
+    // (x, y, z, R), C 3 x float4, V (x, y, z, id), all brick-local; then
+    // S ids, s_off, s_blk, c_off, c_blk words.
+    float4* nearA = rs;
+    float4* nearT = nearA + nn;
+    float4* S = nearT + nn;
+    float4* C = S + ns;
+    float4* V = C + 3 * nc;
+    uint32_t* s_id = reinterpret_cast<uint32_t*>(V + nv);
+    uint32_t* s_off = s_id + ns;
+    uint32_t* s_blk = s_off + ns + 1;
+    uint32_t* c_off = s_blk + nsb;
+    uint32_t* c_blk = c_off + nc + 1;
+    const int4 key = keys[brick];
+    const long long ox = (long long)key.x * L.b - L.frame[0], oy = (long long)key.y * L.b - L.frame[1],
+                    oz = (long long)key.z * L.b - L.frame[2];
+    float ohx, olx, ohy, oly, ohz, olz;
+    origin_pair(ox, RC.h_hi, RC.h_lo, ohx, olx);
+    origin_pair(oy, RC.h_hi, RC.h_lo, ohy, oly);
+    origin_pair(oz, RC.h_hi, RC.h_lo, ohz, olz);
+    auto local3 = [&](double x, double y, double z, float& lx, float& ly, float& lz) {
+        float hx, lo_x, hy, lo_y, hz, lo_z;
+        split_df(x - L.fx, hx, lo_x);
+        split_df(y - L.fy, hy, lo_y);
+        split_df(z - L.fz, hz, lo_z);
+        lx = (hx - ohx) + (lo_x - olx);
+        ly = (hy - ohy) + (lo_y - oly);
+        lz = (hz - ohz) + (lo_z - olz);
+    };
+    for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+        double4 c = A.sph[l_near[i]];
+        float x, y, z;
+        local3(c.x, c.y, c.z, x, y, z);
+        float r32 = float(c.w), rt = fmaxf(r32 - INSIDE_TOL, 0.0f);
+        nearA[i] = make_float4(x, y, z, r32);
+        nearT[i] = make_float4(x, y, z, rt * rt);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i <= ns; i += blockDim.x) s_off[i] = l_soff[i];
+    for (int i = threadIdx.x; i < nsb; i += blockDim.x) s_blk[i] = l_sblk[i];
+    for (int i = threadIdx.x; i <= nc; i += blockDim.x) c_off[i] = l_coff[i];
+    for (int i = threadIdx.x; i < ncb; i += blockDim.x) c_blk[i] = l_cblk[i];
+    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+        // S candidates are near spheres: find the position (lists are short).
+        uint32_t k = l_s[i];
+        int pos = 0;
+        for (int q = 0; q < nn; q++)
+            if (l_near[q] == k) {
+                pos = q;
+                break;
+            }
+        S[i] = nearA[pos];
+        s_id[i] = k;
+    }
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        const double* c = A.circ + 12 * size_t(l_c[i]);
+        float x, y, z;
+        local3(c[0], c[1], c[2], x, y, z);
+        C[3 * i] = make_float4(x, y, z, float(c[9]));
+        C[3 * i + 1] = make_float4(float(c[3]), float(c[4]), float(c[5]), float(c[6]));
+        C[3 * i + 2] = make_float4(float(c[7]), float(c[8]), __int_as_float(int(l_c[i])), 0.0f);
+    }
+    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+        double4 p = A.vert[l_v[i]];
+        float x, y, z;
+        local3(p.x, p.y, p.z, x, y, z);
+        V[i] = make_float4(x, y, z, __int_as_float(int(l_v[i])));
+    }
+    __syncthreads();
+    const float probe = L.probe32, band = L.band32, h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
+    const int b = L.b, side = b + 1, sub = L.sub;
+    struct Eval {
+        float value, qx, qy, qz;
+        uint32_t feat;
+    };
+    // eval_local in f32, brick-local (sesmesh.cuh eval_point semantics).
+    auto eval = [&](float x, float y, float z) {
+        Eval e;
+        e.qx = x, e.qy = y, e.qz = z;
+        bool inside = false;
+        for (int k = 0; k < n_in && !inside; k++) {
+            float4 a = nearA[k];
+            float dx = x - a.x, dy = y - a.y, dz = z - a.z;
+            inside = sqrtf(dx * dx + dy * dy + dz * dz) < a.w;
+        }
+        if (!inside) {
+            e.value = probe;
+            e.feat = 0u << FEAT_SHIFT_D;
+            return e;
+        }
+        float best = probe + band;
+        e.feat = 1u << FEAT_SHIFT_D;
+        for (int i = 0; i < ns; i++) {
+            float4 c = S[i];
+            const uint32_t k = s_id[i];
+            const float cx = c.x, cy = c.y, cz = c.z, rr = c.w;
+            float dx = x - cx, dy = y - cy, dz = z - cz;
+            float len = sqrtf(dx * dx + dy * dy + dz * dz);
+            float lb = fabsf(len - rr);
+            if (lb >= best || len < 1e-12f) continue;
+            float sc = rr / len;
+            float qx = cx + dx * sc, qy = cy + dy * sc, qz = cz + dz * sc;
+            bool free = true;
+            for (uint32_t p = s_off[i], e2 = s_off[i + 1]; p < e2 && free; p++) {
+                float4 t = nearT[s_blk[p]];
+                float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
+                free = ex * ex + ey * ey + ez * ez >= t.w;
+            }
+            if (free) best = lb, e.feat = (2u << FEAT_SHIFT_D) | k, e.qx = qx, e.qy = qy, e.qz = qz;
+        }
+        for (int i = 0; i < nc; i++) {
+            float4 m = C[3 * i], u = C[3 * i + 1], w2 = C[3 * i + 2];
+            float yx = x - m.x, yy = y - m.y, yz = z - m.z;
+            float along = yx * u.x + yy * u.y + yz * u.z;
+            float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
+            float wl = sqrtf(wx * wx + wy * wy + wz * wz);
+            float tt = wl - m.w;
+            float dist = sqrtf(along * along + tt * tt);
+            if (dist >= best) continue;
+            float qx, qy, qz;
+            if (wl > 1e-12f) {
+                qx = m.x + (wx / wl) * m.w, qy = m.y + (wy / wl) * m.w, qz = m.z + (wz / wl) * m.w;
+            } else {
+                qx = m.x + u.w * m.w, qy = m.y + w2.x * m.w, qz = m.z + w2.y * m.w;
+            }
+            bool free = true;
+            for (uint32_t p = c_off[i], e2 = c_off[i + 1]; p < e2 && free; p++) {
+                float4 t = nearT[c_blk[p]];
+                float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
+                free = ex * ex + ey * ey + ez * ez >= t.w;
+            }
+            if (free)
+                best = dist, e.feat = (3u << FEAT_SHIFT_D) | uint32_t(__float_as_int(w2.z)), e.qx = qx, e.qy = qy, e.qz = qz;
+        }
+        for (int i = 0; i < nv; i++) {
+            float4 p = V[i];
+            float dx = x - p.x, dy = y - p.y, dz = z - p.z;
+            float d = sqrtf(dx * dx + dy * dy + dz * dz);
+            if (d < best) best = d, e.feat = (4u << FEAT_SHIFT_D) | uint32_t(__float_as_int(p.w)), e.qx = p.x, e.qy = p.y, e.qz = p.z;
+        }
+        e.value = probe - best;
+        return e;
+    };
+    const uint32_t e0 = edge_off[brick], e1 = edge_off[brick + 1];
+    for (uint32_t k = e0 + threadIdx.x; k < e1; k += blockDim.x) {
+        const uint32_t code = edges[k];
+        const uint32_t cell = code / 3, axis = code % 3;
+        const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
+        if (min(ex / sub, 1) + 2 * min(ey / sub, 1) + 4 * min(ez / sub, 1) != int(sb)) continue;
+        const float2 fv = edge_vals[k];
+        const float fa = fv.x, fb = fv.y;
+        const float ax = float(ex) * h + float(ex) * RC.h_lo, ay = float(ey) * h + float(ey) * RC.h_lo,
+                    az = float(ez) * h + float(ez) * RC.h_lo;
+        float t = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
+        float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
+        int side_ = 0;
+        bool converged = false;
+        uint32_t evals = 0;
+        Eval last;
+        last.feat = 1u << FEAT_SHIFT_D, last.qx = last.qy = last.qz = 0.0f, last.value = 0.0f;
+        for (uint32_t it = 0; it < RC.max_iter; it++) {
+            float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
+            Eval e = eval(x, y, z);
+            evals++;
+            last = e;
+            float gv = e.value;
+            if (fabsf(gv) <= RC.tol) {
+                converged = true;
+                break;
+            }
+            if ((gv < 0.0f) == (g0 < 0.0f)) {
+                t0 = t, g0 = gv;
+                if (side_ == -1) g1 *= 0.5f;
+                side_ = -1;
+            } else {
+                t1 = t, g1 = gv;
+                if (side_ == 1) g0 *= 0.5f;
+                side_ = 1;
+            }
+            float slope = 0.0f;
+            uint32_t kind = e.feat >> FEAT_SHIFT_D;
+            if (kind != 0 && kind != 1) {
+                float wx = e.qx - x, wy = e.qy - y, wz = e.qz - z;
+                float len = sqrtf(wx * wx + wy * wy + wz * wz);
+                if (len > 1e-12f) slope = ((axis == 0 ? wx : (axis == 1 ? wy : wz)) / len) * h;
+            }
+            float newton = t - gv / slope;
+            if (fabsf(slope) > 1e-3f * hd && newton > t0 && newton < t1) {
+                t = newton;
+            } else {
+                float s = (t0 * g1 - t1 * g0) / (g1 - g0);
+                t = (isfinite(s) && s > t0 && s < t1) ? s : 0.5f * (t0 + t1);
+            }
+        }
+        if (!converged) {
+            bool neg0 = g0 < 0.0f;
+            for (uint32_t it = 0; it < RC.max_bisect; it++) {
+                t = 0.5f * (t0 + t1);
+                float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
+                Eval e = eval(x, y, z);
+                evals++;
+                last = e;
+                if (fabsf(e.value) <= RC.tol || (t1 - t0) * hd <= 2.0f * RC.tol) break;
+                if ((e.value < 0.0f) == neg0) t0 = t;
+                else t1 = t;
+            }
+        }
+        out.t[k] = t;
+        out.feat[k] = last.feat;
+        out.q[3 * size_t(k)] = last.qx, out.q[3 * size_t(k) + 1] = last.qy, out.q[3 * size_t(k) + 2] = last.qz;
+        out.evals[k] = evals | (converged ? 0x80000000u : 0u);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers.  Each counts the kernels it launches.
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long kernel_launches() { return g_launches.load(); }
+#define COUNT(n) g_launches.fetch_add(n, std::memory_order_relaxed)
+
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s) {
+    COUNT(1);
     k_selftest<<<(n + 255) / 256, 256, 0, s>>>(a, b, out, n);
 }
 
@@ -778,6 +1063,7 @@ void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, 
         cudaMemsetAsync(total, 0, sizeof(unsigned long long), s);
         return;
     }
+    COUNT(3);
     k_scan_tiles<<<n_tiles, SCAN_THREADS, 0, s>>>(in, n, tiles);
     k_scan_tile_sums<<<1, SCAN_THREADS, 0, s>>>(tiles, n_tiles, total);
     k_scan_apply<<<n_tiles, SCAN_THREADS, 0, s>>>(in, n, tiles, out, keep);
@@ -786,21 +1072,21 @@ void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, 
 uint32_t scan_tiles_needed(uint32_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE + 1; }
 
 void launch_mark_touched(const DArr& A, const DLat& L, const BrickBox& box, uint32_t* flags, int* err, cudaStream_t s) {
-    if (A.n) k_mark_touched<<<(A.n + 127) / 128, 128, 0, s>>>(A, L, box, flags, err);
+    if (A.n) COUNT(1), k_mark_touched<<<(A.n + 127) / 128, 128, 0, s>>>(A, L, box, flags, err);
 }
 
 void launch_classify_bricks(const DArr& A, const DLat& L, const BrickBox& box, const uint32_t* touched, uint32_t n,
                             uint32_t* surface, cudaStream_t s) {
-    if (n) k_classify_bricks<<<(n + 7) / 8, 256, 0, s>>>(A, L, box, touched, n, surface);
+    if (n) COUNT(1), k_classify_bricks<<<(n + 7) / 8, 256, 0, s>>>(A, L, box, touched, n, surface);
 }
 
 void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n, int4* keys, cudaStream_t s) {
-    if (n) k_cells_to_keys<<<(n + 255) / 256, 256, 0, s>>>(box, cells, n, keys);
+    if (n) COUNT(1), k_cells_to_keys<<<(n + 255) / 256, 256, 0, s>>>(box, cells, n, keys);
 }
 
 void launch_substates(const DArr& A, const DLat& L, const int4* keys, uint32_t n, uint32_t* rec, uint32_t* sampled,
                       float* values, cudaStream_t s) {
-    if (n) k_substates<<<n, 256, 0, s>>>(A, L, keys, n, rec, sampled, values);
+    if (n) COUNT(1), k_substates<<<n, 256, 0, s>>>(A, L, keys, n, rec, sampled, values);
 }
 
 cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const uint32_t* work, uint32_t n,
@@ -809,18 +1095,20 @@ cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const 
     size_t smem = gather_smem_bytes(caps) * size_t(warps);
     cudaError_t e = cudaFuncSetAttribute(k_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
+    COUNT(1);
     k_gather<<<(n + warps - 1) / warps, 32 * warps, smem, s>>>(A, L, keys, work, n, O, caps);
     return cudaGetLastError();
 }
 
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
-                          cudaStream_t s) {
+                          bool count, cudaStream_t s) {
     if (!n) return cudaSuccess;
     size_t smem = size_t(max_units) * 16;
-    auto kern = tma ? k_sample<true> : k_sample<false>;
+    auto kern = count ? k_sample<true, true> : (tma ? k_sample<true, false> : k_sample<false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
+    COUNT(1);
     kern<<<n, 128, smem, s>>>(L, keys, work, n, rec, pack, values, counters);
     return cudaGetLastError();
 }
@@ -833,7 +1121,24 @@ cudaError_t launch_mc(const DLat& L, uint32_t n, const float* values, uint32_t* 
     auto kern = fill ? k_mc<true> : k_mc<false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
+    COUNT(1);
     kern<<<n, MC_THREADS, smem, s>>>(L, n, values, counts, edge_off, tri_off, edges, edge_vals, tris);
+    return cudaGetLastError();
+}
+
+size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uint32_t nsb, uint32_t ncb) {
+    return (size_t(2) * nn + ns + 3 * size_t(nc) + nv) * 16 + (size_t(ns) * 2 + 1 + nsb + nc + 1 + ncb) * 4;
+}
+
+cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
+                          uint32_t n, const uint32_t* rec, const uint32_t* ids, const uint32_t* edge_off,
+                          const uint32_t* edges, const float2* edge_vals, float* t, uint32_t* feat, float* q,
+                          uint32_t* evals, size_t smem, cudaStream_t s) {
+    if (!n) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    COUNT(1);
+    k_refine<<<n, 128, smem, s>>>(A, L, RC, keys, work, n, rec, ids, edge_off, edges, edge_vals, RefOut{t, feat, q, evals});
     return cudaGetLastError();
 }
 

@@ -27,7 +27,10 @@ __host__ __device__ inline size_t gather_smem_bytes(const GatherCaps& c) {
 }
 
 // Device counters of one gather/sample pass.
-enum : int { CNT_IDS = 0, CNT_PACK = 1, CNT_MAXPACK = 2, CNT_OVERFLOW = 3, CNT_NOMEM = 4, CNT_TIMEOUT = 5, CNT_N = 8 };
+enum : int {
+    CNT_IDS = 0, CNT_PACK = 1, CNT_MAXPACK = 2, CNT_OVERFLOW = 3, CNT_NOMEM = 4, CNT_TIMEOUT = 5, CNT_OPS = 6,
+    CNT_OWNED = 7, CNT_N = 8
+};
 constexpr uint32_t REC_NOMEM = 2;
 
 struct GatherOut {
@@ -39,6 +42,19 @@ struct GatherOut {
     unsigned long long ids_cap, pack_cap;
 };
 
+// Fast-mode refinement constants (RefineRef, sesmesh-gpu batch.rs:133-150).
+struct RefineConsts {
+    float h_hi, h_lo, tol;
+    uint32_t max_iter, max_bisect;
+};
+
+size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uint32_t nsb, uint32_t ncb);
+cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
+                          uint32_t n, const uint32_t* rec, const uint32_t* ids, const uint32_t* edge_off,
+                          const uint32_t* edges, const float2* edge_vals, float* t, uint32_t* feat, float* q,
+                          uint32_t* evals, size_t smem, cudaStream_t s);
+
+unsigned long long kernel_launches();
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);
 void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, unsigned long long* tiles,
                  unsigned long long* total, cudaStream_t s);
@@ -53,7 +69,7 @@ cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const 
                           const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s);
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
-                          cudaStream_t s);
+                          bool count, cudaStream_t s);
 cudaError_t launch_mc(const DLat& L, uint32_t n, const float* values, uint32_t* counts, const uint32_t* edge_off,
                       const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
                       cudaStream_t s);

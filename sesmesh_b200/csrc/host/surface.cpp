@@ -1,0 +1,378 @@
+// compute_surface with the CUDA back end (crates/sesmesh/src/surface.rs:
+// 599-633, 953-1300) above the C ABI: host arrangement, device
+// classification and mesh-stage kernels, host f64 refinement (exact) or
+// placement of the device's f32 roots (fast), assembly, validation,
+// components and OBJ output.
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+
+#include "../../../include/sesmesh_b200.h"
+#include "../../../include/sesmesh_b200_surface.h"
+#include "../runtime.hpp"
+#include "geom.hpp"
+#include "mesher.hpp"
+
+using namespace smbh;
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+double ms_since(clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); }
+
+void set_err(char* err, size_t len, const char* fmt, ...) {
+    if (!err || !len) return;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, len, fmt, ap);
+    va_end(ap);
+}
+
+}  // namespace
+
+struct smb_engine {
+    smb_device* dev = nullptr;
+    smb_surface_params params{};
+    Arrangement arr;
+    MeshParams mp;
+    smb_resident* res = nullptr;
+    smb_batch* batch = nullptr;
+    double t_geometry = 0, t_upload = 0;
+    // Host copies of the last device run.
+    std::vector<int32_t> keys;
+    std::vector<uint32_t> edge_off, edges, tri_off, tris;
+    std::vector<float> edge_vals, t, closest;
+    std::vector<uint32_t> feat, evals;
+    size_t touched = 0;
+    smb_batch_times times{};
+    double t_classify = 0;
+};
+
+struct smb_surface {
+    Mesh mesh;
+    std::vector<Component> comps;
+    smb_surface_stats stats{};
+    std::string obj;
+};
+
+extern "C" {
+
+int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out,
+                   char* err, size_t errlen) {
+    if (!dev || !p || !out || (n && !xyzr)) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
+    *out = nullptr;
+    if (p->kind != SMB_SES) return set_err(err, errlen, "only the SES is meshed on the device"), SMB_ERR_ARG;
+    if (p->refine != SMB_REFINE_EXACT && p->refine != SMB_REFINE_FAST)
+        return set_err(err, errlen, "refine mode must be exact or fast on the device"), SMB_ERR_ARG;
+    if (!(p->spacing >= 0.01) || !std::isfinite(p->spacing))
+        return set_err(err, errlen, "grid spacing must be at least 0.01 A, got %g", p->spacing), SMB_ERR_ARG;
+    if (p->brick_size < 4 || p->brick_size > 32 || p->brick_size % 2)
+        return set_err(err, errlen, "brick size must be even and 4..32 on the device, got %u", p->brick_size), SMB_ERR_ARG;
+    set_threads(p->threads);
+    auto e = std::make_unique<smb_engine>();
+    e->dev = dev;
+    e->params = *p;
+    auto t0 = clk::now();
+    std::string m = build_arrangement(xyzr, n, p->probe_radius, e->arr);
+    if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
+    const Arrangement& A = e->arr;
+    // Engine::new (field/kernel.rs:204-271).
+    V3 center;
+    double half = 0.0;
+    if (A.n) {
+        V3 lo = A.c(0), hi = lo;
+        for (size_t i = 0; i < A.n; i++) lo = lo.lo(A.c(uint32_t(i))), hi = hi.hi(A.c(uint32_t(i)));
+        V3 d = hi - lo;
+        center = (lo + hi) * 0.5;
+        half = 0.5 * std::fmax(std::fmax(d.x, d.y), d.z);
+    }
+    MeshParams& P = e->mp;
+    P.h = p->spacing;
+    P.b = int(p->brick_size);
+    P.sub = P.b / 2;
+    P.frame[0] = to_i64(std::round(center.x / P.h));
+    P.frame[1] = to_i64(std::round(center.y / P.h));
+    P.frame[2] = to_i64(std::round(center.z / P.h));
+    double reach = half + 2.0 * A.max_expanded + 2.0 * p->probe_radius + 4.0 * double(P.b) * P.h;
+    P.f32_ok = reach < 2000.0 && reach / P.h < double(1u << 23);
+    if (!P.f32_ok)
+        return set_err(err, errlen, "extent beyond the f32 frame (%g A): the device path does not take it", reach),
+               SMB_ERR_RANGE;
+    P.band = std::sqrt(3.0) * P.h * 1.01;
+    P.coord_max = std::fmax(std::fmax(std::fabs(center.x), std::fabs(center.y)), std::fabs(center.z)) + half +
+                  A.max_expanded + p->probe_radius + 2.0 * P.band;
+    {  // edge_clamp (extract.rs:47-51)
+        double cm = P.coord_max < 1.0 ? 1.0 : (P.coord_max > double(3.4028234663852886e38f) / 4.0 ? double(3.4028234663852886e38f) / 4.0 : P.coord_max);
+        float mf = float(cm), nx;
+        uint32_t bits;
+        std::memcpy(&bits, &mf, 4);
+        bits++;
+        std::memcpy(&nx, &bits, 4);
+        double ulp = double(nx - mf), tm = 4.0 * ulp / P.h;
+        P.t_min = tm < 1e-4 ? 1e-4 : (tm > 0.25 ? 0.25 : tm);
+    }
+    e->t_geometry = ms_since(t0);
+    // Upload (Resident::new).
+    auto t1 = clk::now();
+    smb_arrangement_ref r{};
+    r.n_spheres = A.n;
+    r.center = A.center.data();
+    r.expanded = A.expanded.data();
+    r.radius = A.radius.data();
+    r.status = A.status.data();
+    r.nb_off = A.nb_off.data();
+    r.nb_items = A.nb_items.data();
+    r.n_circles = A.n_circles();
+    r.circle = A.circle.data();
+    r.cb_off = A.cb_off.data();
+    r.cb_items = A.cb_items.data();
+    r.n_vertices = A.n_vertices();
+    r.vertex = A.vertex.data();
+    const Grid* gs[3] = {&A.cells, &A.circle_cells, &A.vertex_cells};
+    smb_grid_ref* gr[3] = {&r.sphere_grid, &r.circle_grid, &r.vertex_grid};
+    for (int g = 0; g < 3; g++) {
+        for (int k = 0; k < 3; k++) gr[g]->origin[k] = gs[g]->origin[k], gr[g]->dims[k] = gs[g]->dims[k];
+        gr[g]->cell = gs[g]->cell;
+        gr[g]->starts = gs[g]->starts.data();
+        gr[g]->items = gs[g]->items.data();
+        gr[g]->n_items = gs[g]->items.size();
+    }
+    r.max_expanded = A.max_expanded;
+    r.rho_max = A.rho_max;
+    r.probe = A.probe;
+    smb_lattice_ref lat{};
+    lat.spacing = P.h;
+    lat.brick = uint32_t(P.b);
+    for (int k = 0; k < 3; k++) lat.frame[k] = P.frame[k];
+    lat.band = P.band;
+    int rc = smb_resident_new(dev, &r, &lat, &e->res, err, errlen);
+    if (rc != SMB_OK) return rc;
+    rc = smb_batch_new(e->res, &e->batch, err, errlen);
+    if (rc != SMB_OK) return rc;
+    if (p->refine == SMB_REFINE_FAST) {
+        rc = smb_resident_set_refinement(e->res, err, errlen);
+        if (rc != SMB_OK) return rc;
+    }
+    e->t_upload = ms_since(t1);
+    *out = e.release();
+    return SMB_OK;
+}
+
+void smb_engine_free(smb_engine* e) {
+    if (!e) return;
+    smb_batch_free(e->batch);
+    smb_resident_free(e->res);
+    delete e;
+}
+
+// Device part of the mesh stage on the resident arrangement: classification,
+// sub-block states, gather, sampling, marching cubes (and fast-mode
+// refinement); results stay on the device.
+int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size_t errlen) {
+    if (!e) return SMB_ERR_ARG;
+    size_t touched = 0, surface = 0;
+    auto t0 = clk::now();
+    int rc = smb_classify(e->res, &touched, &surface, err, errlen);
+    if (rc != SMB_OK) return rc;
+    e->t_classify = ms_since(t0);
+    e->touched = touched;
+    smb_batch_times t{};
+    rc = smb_run(e->res, 0, surface, e->batch, &t, err, errlen);
+    if (rc != SMB_OK) return rc;
+    if (e->params.refine == SMB_REFINE_FAST) {
+        double ms = 0;
+        rc = smb_refine(e->res, e->batch, &ms, err, errlen);
+        if (rc != SMB_OK) return rc;
+        t.total += ms;
+    }
+    e->times = t;
+    if (times) *times = t;
+    return SMB_OK;
+}
+
+size_t smb_engine_bricks(const smb_engine* e) { return e && e->res ? e->res->n_bricks : 0; }
+
+smb_batch* smb_engine_batch(smb_engine* e) { return e ? e->batch : nullptr; }
+
+// Whole mesh stage and the stages after it: device part, results to the
+// host, f64 refinement (exact) or placement (fast), assembly, validation,
+// components and grouping.
+int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) {
+    if (!e || !out) return SMB_ERR_ARG;
+    *out = nullptr;
+    auto t_all = clk::now();
+    int rc = smb_engine_run_device(e, nullptr, err, errlen);
+    if (rc != SMB_OK) return rc;
+    auto t0 = clk::now();
+    size_t nb = e->res->n_bricks, ne = 0, nt = 0;
+    smb_batch_mc_counts(e->batch, &ne, &nt);
+    e->keys.resize(3 * nb);
+    e->edge_off.resize(nb + 1);
+    e->tri_off.resize(nb + 1);
+    e->edges.resize(ne);
+    e->edge_vals.resize(2 * ne);
+    e->tris.resize(3 * nt);
+    if (nb) {
+        if ((rc = smb_resident_bricks(e->res, e->keys.data(), nb)) != SMB_OK) return set_err(err, errlen, "bricks copy"), rc;
+        if ((rc = smb_batch_mc(e->batch, e->edge_off.data(), e->edges.data(), e->edge_vals.data(), e->tri_off.data(),
+                               e->tris.data())) != SMB_OK)
+            return set_err(err, errlen, "mc copy"), rc;
+    } else {
+        e->edge_off.assign(1, 0);
+        e->tri_off.assign(1, 0);
+    }
+    bool fast = e->params.refine == SMB_REFINE_FAST;
+    if (fast && ne) {
+        e->t.resize(ne), e->feat.resize(ne), e->closest.resize(3 * ne), e->evals.resize(ne);
+        if ((rc = smb_batch_edges(e->batch, e->t.data(), e->feat.data(), e->closest.data(), e->evals.data())) != SMB_OK)
+            return set_err(err, errlen, "edge results copy"), rc;
+    }
+    double t_d2h = ms_since(t0);
+    auto t1 = clk::now();
+    MeshOut mo;
+    if (fast)
+        place_fast(e->arr, e->mp, e->keys.data(), nb, e->edge_off.data(), e->edges.data(), e->edge_vals.data(),
+                   DeviceRefine{e->t.data(), e->feat.data(), e->closest.data(), e->evals.data()}, mo);
+    else
+        refine_exact(e->arr, e->mp, e->keys.data(), nb, e->edge_off.data(), e->edges.data(), e->edge_vals.data(), mo);
+    double t_host = ms_since(t1);
+    auto t2 = clk::now();
+    auto s = std::make_unique<smb_surface>();
+    Mesh& mesh = s->mesh;
+    std::string m = assemble(e->keys.data(), nb, e->edge_off.data(), e->edges.data(), e->tri_off.data(), e->tris.data(), mesh);
+    if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_STATE;
+    mesh.positions.swap(mo.positions);
+    mesh.normals.swap(mo.normals);
+    mesh.vertex_atom.swap(mo.atoms);
+    mesh.vertex_patch.swap(mo.patches);
+    double t_assemble = ms_since(t2);
+    auto t3 = clk::now();
+    size_t bad = defects(mesh);
+    if (bad) return set_err(err, errlen, "mesh failed validation (%zu defects)", bad), SMB_ERR_STATE;
+    components_and_group(mesh, s->comps);
+    double t_measure = ms_since(t3);
+    smb_surface_stats& st = s->stats;
+    st.spheres = e->arr.n;
+    st.touched_bricks = e->touched;
+    st.surface_bricks = nb;
+    st.samples = nb * size_t(e->mp.b + 1) * size_t(e->mp.b + 1) * size_t(e->mp.b + 1);
+    st.vertices = mesh.positions.size();
+    st.triangles = mesh.triangles.size();
+    st.components = s->comps.size();
+    for (auto& c : s->comps) st.area += c.area, st.volume += c.volume, st.euler += c.euler;
+    for (uint32_t v : mo.evals) st.refine_evaluations += v;
+    for (uint32_t v : mo.cpu_refined) st.refine_cpu_edges += v;
+    st.t_geometry = e->t_geometry;
+    st.t_upload = e->t_upload;
+    st.t_classify = e->t_classify;
+    st.t_substates = e->times.substates;
+    st.t_gather = e->times.gather;
+    st.t_sample = e->times.sample;
+    st.t_mc = e->times.mc;
+    st.t_device = e->t_classify + e->times.total;
+    st.t_d2h = t_d2h;
+    st.t_host_refine = t_host;
+    st.t_assemble = t_assemble;
+    st.t_measure = t_measure;
+    st.t_mesh_stage = ms_since(t_all) - t_assemble - t_measure;
+    st.host_threads = threads();
+    *out = s.release();
+    return SMB_OK;
+}
+
+int smb_compute_surface(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p, smb_surface** out,
+                        char* err, size_t errlen) {
+    auto t0 = clk::now();
+    smb_engine* e = nullptr;
+    int rc = smb_engine_new(dev, xyzr, n, p, &e, err, errlen);
+    if (rc != SMB_OK) return rc;
+    rc = smb_engine_mesh(e, out, err, errlen);
+    smb_engine_free(e);
+    if (rc == SMB_OK) (*out)->stats.t_total = ms_since(t0);
+    return rc;
+}
+
+void smb_surface_free(smb_surface* s) { delete s; }
+
+int smb_surface_stats_get(const smb_surface* s, smb_surface_stats* out) {
+    if (!s || !out) return SMB_ERR_ARG;
+    *out = s->stats;
+    return SMB_OK;
+}
+
+int smb_surface_mesh(const smb_surface* s, float* pos, float* nrm, uint32_t* tris, uint32_t* atoms, uint8_t* patches,
+                     uint32_t* components) {
+    if (!s) return SMB_ERR_ARG;
+    const Mesh& m = s->mesh;
+    if (pos && !m.positions.empty()) std::memcpy(pos, m.positions.data(), m.positions.size() * 12);
+    if (nrm && !m.normals.empty()) std::memcpy(nrm, m.normals.data(), m.normals.size() * 12);
+    if (tris && !m.triangles.empty()) std::memcpy(tris, m.triangles.data(), m.triangles.size() * 12);
+    if (atoms && !m.vertex_atom.empty()) std::memcpy(atoms, m.vertex_atom.data(), m.vertex_atom.size() * 4);
+    if (patches && !m.vertex_patch.empty()) std::memcpy(patches, m.vertex_patch.data(), m.vertex_patch.size());
+    if (components && !m.vertex_component.empty())
+        std::memcpy(components, m.vertex_component.data(), m.vertex_component.size() * 4);
+    return SMB_OK;
+}
+
+size_t smb_surface_obj(smb_surface* s, char* out, size_t cap) {
+    if (!s) return 0;
+    if (s->obj.empty()) s->obj = obj_text(s->mesh);
+    if (out) std::memcpy(out, s->obj.data(), s->obj.size() < cap ? s->obj.size() : cap);
+    return s->obj.size();
+}
+
+int smb_surface_write_obj(smb_surface* s, const char* path, char* err, size_t errlen) {
+    if (!s || !path) return SMB_ERR_ARG;
+    if (s->obj.empty()) s->obj = obj_text(s->mesh);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return set_err(err, errlen, "cannot open %s", path), SMB_ERR_ARG;
+    size_t w = std::fwrite(s->obj.data(), 1, s->obj.size(), f);
+    std::fclose(f);
+    if (w != s->obj.size()) return set_err(err, errlen, "short write to %s", path), SMB_ERR_ARG;
+    return SMB_OK;
+}
+
+// The host arrangement of an engine (tests compare it with the oracle's).
+int smb_engine_arrangement(const smb_engine* e, smb_arrangement_info* out) {
+    if (!e || !out) return SMB_ERR_ARG;
+    const Arrangement& A = e->arr;
+    out->n_spheres = A.n;
+    out->n_contained = A.n_contained;
+    out->n_circles = A.n_circles();
+    out->n_vertices = A.n_vertices();
+    out->center = A.center.data();
+    out->expanded = A.expanded.data();
+    out->status = A.status.data();
+    out->orig = A.orig.data();
+    out->circle = A.circle.data();
+    out->circle_ij = A.circle_ij.data();
+    out->vertex = A.vertex.data();
+    out->vertex_atoms = A.vertex_atoms.data();
+    out->nb_off = A.nb_off.data();
+    out->nb_items = A.nb_items.data();
+    out->cb_off = A.cb_off.data();
+    out->cb_items = A.cb_items.data();
+    out->max_expanded = A.max_expanded;
+    out->rho_max = A.rho_max;
+    for (int k = 0; k < 3; k++) out->frame[k] = e->mp.frame[k];
+    out->band = e->mp.band;
+    out->t_min = e->mp.t_min;
+    return SMB_OK;
+}
+
+// Host-only construction (no device): the arrangement and lattice constants.
+int smb_arrangement_build(const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out, char* err,
+                          size_t errlen) {
+    if (!p || !out) return SMB_ERR_ARG;
+    auto e = std::make_unique<smb_engine>();
+    e->params = *p;
+    set_threads(p->threads);
+    std::string m = build_arrangement(xyzr, n, p->probe_radius, e->arr);
+    if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
+    *out = e.release();
+    return SMB_OK;
+}
+
+}  // extern "C"

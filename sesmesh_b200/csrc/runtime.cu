@@ -479,6 +479,8 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     cudaStream_t s = d->stream;
     const DLat& L = r->L;
     b->n = uint32_t(count);
+    b->first = first;
+    b->refined = false;
     b->n_work = 0;
     b->n_edges = b->n_tris = 0;
     b->ids_words = 0;
@@ -570,7 +572,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
                SMB_ERR_MEMORY;
     cudaError_t e = launch_sample(L, keys, b->work.as<uint32_t>(), uint32_t(n_work), b->rec.as<uint32_t>(),
                                   b->pack.as<uint4>(), b->max_pack, b->values.as<float>(),
-                                  b->counters.as<unsigned long long>(), b->use_tma, s);
+                                  b->counters.as<unsigned long long>(), b->use_tma, false, s);
     if (e != cudaSuccess) return set_err(err, errlen, "sample launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     cudaEventRecord(b->ev[3], s);
 
@@ -614,7 +616,110 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     return SMB_OK;
 }
 
+int smb_resident_set_refinement(smb_resident* r, char* err, size_t errlen) {
+    if (!r) return set_err(err, errlen, "null resident"), SMB_ERR_ARG;
+    // RefineRef (batch.rs:133-150; field/gpu.rs:207-221): h as an f32 pair,
+    // TOL, MAX_ITER and MAX_BISECT of mesh/extract.rs:29-35.
+    r->rc.h_hi = float(r->L.h);
+    r->rc.h_lo = float(r->L.h - double(r->rc.h_hi));
+    r->rc.tol = float(1e-5);
+    r->rc.max_iter = 8;
+    r->rc.max_bisect = 64;
+    r->refine_ready = true;
+    return SMB_OK;
+}
+
+int smb_refine(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errlen) {
+    if (!r || !b || b->res != r) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
+    if (!r->refine_ready) return set_err(err, errlen, "smb_resident_set_refinement must run first"), SMB_ERR_STATE;
+    smb_device* d = r->dev;
+    CK(cudaSetDevice(d->index));
+    cudaStream_t s = d->stream;
+    size_t ne = b->n_edges;
+    int rc;
+    if ((rc = b->e_t.reserve(ne * 4, err, errlen)) || (rc = b->e_feat.reserve(ne * 4, err, errlen)) ||
+        (rc = b->e_q.reserve(ne * 12, err, errlen)) || (rc = b->e_evals.reserve(ne * 4, err, errlen)))
+        return rc;
+    b->refined = false;
+    if (ms) *ms = 0;
+    if (ne == 0 || b->n_work == 0) {
+        b->refined = true;
+        return SMB_OK;
+    }
+    size_t smem = size_t(b->max_pack) * 18 + 64;
+    if (smem > size_t(d->smem_optin))
+        return set_err(err, errlen, "a sub-block's candidates exceed shared memory for refinement"), SMB_ERR_MEMORY;
+    cudaEventRecord(b->ev[4], s);
+    CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
+    cudaError_t e = launch_refine(r->A, r->L, r->rc, r->keys + b->first, b->work.as<uint32_t>(), b->n_work,
+                                  b->rec.as<uint32_t>(), b->ids.as<uint32_t>(), b->edge_off.as<uint32_t>(),
+                                  b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->e_t.as<float>(),
+                                  b->e_feat.as<uint32_t>(), b->e_q.as<float>(), b->e_evals.as<uint32_t>(), smem, s);
+    if (e != cudaSuccess) return set_err(err, errlen, "refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    cudaEventRecord(b->ev[5], s);
+    CK(cudaStreamSynchronize(s));
+    float t = 0;
+    cudaEventElapsedTime(&t, b->ev[4], b->ev[5]);
+    if (ms) *ms = t;
+    b->refined = true;
+    return SMB_OK;
+}
+
+int smb_batch_edges(const smb_batch* b, float* t, uint32_t* feat, float* closest, uint32_t* evals) {
+    if (!b || !b->refined) return SMB_ERR_STATE;
+    cudaSetDevice(b->res->dev->index);
+    size_t ne = b->n_edges;
+    if (!ne) return SMB_OK;
+    bool ok = true;
+    if (t) ok &= cudaMemcpy(t, b->e_t.p, ne * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (feat) ok &= cudaMemcpy(feat, b->e_feat.p, ne * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (closest) ok &= cudaMemcpy(closest, b->e_q.p, ne * 12, cudaMemcpyDeviceToHost) == cudaSuccess;
+    if (evals) ok &= cudaMemcpy(evals, b->e_evals.p, ne * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    return ok ? SMB_OK : SMB_ERR_CUDA;
+}
+
 size_t smb_batch_bricks(const smb_batch* b) { return b ? b->n : 0; }
+
+unsigned long long smb_kernel_launches(void) { return kernel_launches(); }
+
+int smb_batch_info_get(const smb_batch* b, smb_batch_info* out) {
+    if (!b || !out) return SMB_ERR_ARG;
+    out->bricks = b->n;
+    out->sampled_subblocks = b->n_work;
+    out->ids_words = b->ids_words;
+    out->max_pack_units = b->max_pack;
+    out->edges = b->n_edges;
+    out->triangles = b->n_tris;
+    out->classify_ms = b->res->classify_ms;
+    out->touched = b->res->n_touched;
+    out->resident_bytes = b->res->bytes;
+    unsigned long long c[CNT_N] = {0};
+    if (b->counters.p) {
+        cudaSetDevice(b->res->dev->index);
+        if (cudaMemcpy(c, b->counters.p, sizeof c, cudaMemcpyDeviceToHost) != cudaSuccess) return SMB_ERR_CUDA;
+    }
+    out->pack_units = c[CNT_PACK];
+    return SMB_OK;
+}
+
+int smb_batch_count_ops(smb_batch* b, unsigned long long* ops, unsigned long long* samples, char* err, size_t errlen) {
+    if (!b) return SMB_ERR_ARG;
+    smb_resident* r = b->res;
+    smb_device* d = r->dev;
+    CK(cudaSetDevice(d->index));
+    cudaStream_t s = d->stream;
+    CK(cudaMemsetAsync(b->counters.as<unsigned long long>() + CNT_OPS, 0, 16, s));
+    cudaError_t e = launch_sample(r->L, r->keys + b->first, b->work.as<uint32_t>(), b->n_work, b->rec.as<uint32_t>(),
+                                  b->pack.as<uint4>(), b->max_pack, b->values.as<float>(),
+                                  b->counters.as<unsigned long long>(), true, true, s);
+    if (e != cudaSuccess) return set_err(err, errlen, "count launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    unsigned long long c[CNT_N];
+    CK(cudaMemcpyAsync(c, b->counters.p, sizeof c, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (ops) *ops = c[CNT_OPS];
+    if (samples) *samples = c[CNT_OWNED];
+    return SMB_OK;
+}
 
 int smb_batch_records(const smb_batch* b, uint32_t* out) {
     if (!b || !out) return SMB_ERR_ARG;

@@ -44,20 +44,25 @@ struct smb_resident {
     size_t n_touched = 0;
     bool classified = false;
     float classify_ms = 0;
+    smb::RefineConsts rc{};
+    bool refine_ready = false;
 };
 
 struct smb_batch {
     smb_resident* res = nullptr;
     uint32_t n = 0, n_work = 0, max_pack = 0;
+    size_t first = 0;
+    bool refined = false;
     size_t n_edges = 0, n_tris = 0, ids_words = 0;
     smb::DBuf rec, sampled, work, retry_a, retry_b, values, tiles, totals, counters;
     smb::DBuf ids, pack, mc_counts, edge_off, tri_off, edges, edge_vals, tris;
+    smb::DBuf e_t, e_feat, e_q, e_evals;  // fast-mode refinement results
     smb::GatherCaps caps{192, 128, 384, 128};
     int gather_warps = 4;
     bool use_tma = true;
     cudaEvent_t ev[6] = {};
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
-                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris};
+                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals};
     }
 };

@@ -54,7 +54,42 @@ class DeviceInfo(C.Structure):
                 ("memory", C.c_size_t)]
 
 
-# Every entry point of include/sesmesh_b200.h with its ctypes signature.
+class SurfaceParams_(C.Structure):
+    _fields_ = [("kind", C.c_int), ("probe_radius", C.c_double), ("spacing", C.c_double), ("brick_size", C.c_uint32),
+                ("refine", C.c_int), ("threads", C.c_int)]
+
+
+STAT_FIELDS = ["spheres", "touched_bricks", "surface_bricks", "samples", "vertices", "triangles", "components"]
+TIME_FIELDS = ["t_geometry", "t_upload", "t_classify", "t_substates", "t_gather", "t_sample", "t_mc", "t_device",
+               "t_d2h", "t_host_refine", "t_mesh_stage", "t_assemble", "t_measure", "t_total"]
+
+
+class SurfaceStats_(C.Structure):
+    _fields_ = ([(f, C.c_size_t) for f in STAT_FIELDS] + [("area", C.c_double), ("volume", C.c_double),
+                                                           ("euler", C.c_int64), ("refine_evaluations", C.c_uint64),
+                                                           ("refine_cpu_edges", C.c_uint64)]
+                + [(f, C.c_double) for f in TIME_FIELDS] + [("host_threads", C.c_int)])
+
+
+class ArrangementInfo(C.Structure):
+    _fields_ = [("n_spheres", C.c_size_t), ("n_contained", C.c_size_t), ("n_circles", C.c_size_t),
+                ("n_vertices", C.c_size_t), ("center", C.POINTER(C.c_double)), ("expanded", C.POINTER(C.c_double)),
+                ("circle", C.POINTER(C.c_double)), ("vertex", C.POINTER(C.c_double)),
+                ("status", C.POINTER(C.c_uint32)), ("orig", C.POINTER(C.c_uint32)),
+                ("circle_ij", C.POINTER(C.c_uint32)), ("vertex_atoms", C.POINTER(C.c_uint32)),
+                ("nb_off", C.POINTER(C.c_uint32)), ("nb_items", C.POINTER(C.c_uint32)),
+                ("cb_off", C.POINTER(C.c_uint32)), ("cb_items", C.POINTER(C.c_uint32)),
+                ("max_expanded", C.c_double), ("rho_max", C.c_double), ("band", C.c_double), ("t_min", C.c_double),
+                ("frame", C.c_int64 * 3)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [(f, C.c_size_t) for f in ("bricks", "sampled_subblocks", "ids_words", "max_pack_units", "edges",
+                                          "triangles", "touched", "resident_bytes")] + \
+               [("pack_units", C.c_ulonglong), ("classify_ms", C.c_double)]
+
+
+# Every entry point of include/*.h with its ctypes signature.
 _vp, _sz, _cp = C.c_void_p, C.c_size_t, C.c_char_p
 _u32p, _i32p, _fp = C.POINTER(C.c_uint32), C.POINTER(C.c_int32), C.POINTER(C.c_float)
 SIGNATURES = {
@@ -77,6 +112,30 @@ SIGNATURES = {
     "smb_batch_ids": (C.c_int, [_vp, _u32p]),
     "smb_batch_mc_counts": (C.c_int, [_vp, C.POINTER(_sz), C.POINTER(_sz)]),
     "smb_batch_mc": (C.c_int, [_vp, _u32p, _u32p, _fp, _u32p, _u32p]),
+    "smb_resident_set_refinement": (C.c_int, [_vp, _cp, _sz]),
+    "smb_refine": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
+    "smb_batch_edges": (C.c_int, [_vp, _fp, _u32p, _fp, _u32p]),
+    "smb_kernel_launches": (C.c_ulonglong, []),
+    "smb_batch_info_get": (C.c_int, [_vp, C.POINTER(BatchInfo)]),
+    "smb_batch_count_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _cp, _sz]),
+    "smb_engine_batch": (_vp, [_vp]),
+    # include/sesmesh_b200_surface.h
+    "smb_compute_surface": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_), C.POINTER(_vp),
+                                      _cp, _sz]),
+    "smb_engine_new": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_), C.POINTER(_vp), _cp,
+                                 _sz]),
+    "smb_engine_free": (None, [_vp]),
+    "smb_engine_run_device": (C.c_int, [_vp, C.POINTER(BatchTimes), _cp, _sz]),
+    "smb_engine_bricks": (_sz, [_vp]),
+    "smb_engine_mesh": (C.c_int, [_vp, C.POINTER(_vp), _cp, _sz]),
+    "smb_surface_free": (None, [_vp]),
+    "smb_surface_stats_get": (C.c_int, [_vp, C.POINTER(SurfaceStats_)]),
+    "smb_surface_mesh": (C.c_int, [_vp, _fp, _fp, _u32p, _u32p, C.POINTER(C.c_uint8), _u32p]),
+    "smb_surface_obj": (_sz, [_vp, _cp, _sz]),
+    "smb_surface_write_obj": (C.c_int, [_vp, _cp, _cp, _sz]),
+    "smb_engine_arrangement": (C.c_int, [_vp, C.POINTER(ArrangementInfo)]),
+    "smb_arrangement_build": (C.c_int, [C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_), C.POINTER(_vp), _cp,
+                                        _sz]),
 }
 
 _LIB = None
@@ -287,6 +346,17 @@ class Batch:
             out[key] = ids[pos:pos + cnt]
             pos += cnt
         return out
+
+    def info(self):
+        i = BatchInfo()
+        lib().smb_batch_info_get(self.h, C.byref(i))
+        return {name: getattr(i, name) for name, _ in i._fields_}
+
+    def count_ops(self):
+        err = C.create_string_buffer(1024)
+        ops, n = C.c_ulonglong(0), C.c_ulonglong(0)
+        _check(lib().smb_batch_count_ops(self.h, C.byref(ops), C.byref(n), err, 1024), err)
+        return ops.value, n.value
 
     def mc(self):
         ne, nt = _sz(0), _sz(0)

@@ -1,0 +1,217 @@
+"""compute_surface / SurfaceParams / SurfaceEngine over the B200 back end.
+
+The Python face of include/sesmesh_b200_surface.h, shaped like sesmesh's
+library API (crates/sesmesh/src/surface.rs:106-241, 599-711) for what the
+device path takes: the SES, `refine` exact or fast, `backend` cuda.  Exact
+mode gives the CPU back end's mesh and OBJ bytes; fast mode refines edges in
+f32 on the device (same triangles, area and volume within 4e-7 relative).
+"""
+import ctypes as C
+from dataclasses import dataclass, replace
+
+import numpy as np
+
+from . import native
+from .native import SmbError, _check, _p, lib
+
+REFINE = {"exact": 0, "linear": 1, "fast": 2}
+QUALITY = {"draft": 1.0, "medium": 0.5, "high": 0.25, "ultra": 0.125}
+
+
+@dataclass(frozen=True)
+class SurfaceParams:
+    """SurfaceParams (surface.rs:195-241): SES with probe radius, grid spacing
+    (default Quality::Medium, 0.5 A), refine mode, brick edge (default 10),
+    CUDA device, host threads (0 = all)."""
+    probe_radius: float = 1.4
+    spacing: float = 0.5
+    refine: str = "exact"
+    brick_size: int = 10
+    device: int = 0
+    threads: int = 0
+    kind: str = "ses"
+
+    @staticmethod
+    def ses(probe_radius):
+        return SurfaceParams(probe_radius=float(probe_radius))
+
+    def with_spacing(self, h):
+        return replace(self, spacing=float(h))
+
+    def with_quality(self, q):
+        return replace(self, spacing=QUALITY[q])
+
+    def with_refine(self, mode):
+        if mode not in REFINE:
+            raise ValueError("refine must be exact, linear or fast")
+        return replace(self, refine=mode)
+
+    def with_brick_size(self, b):
+        return replace(self, brick_size=int(b))
+
+    def _c(self):
+        if self.kind != "ses":
+            raise SmbError(1, "only the SES is meshed on the device")
+        p = native.SurfaceParams_()
+        p.kind = 0
+        p.probe_radius = float(self.probe_radius)
+        p.spacing = float(self.spacing)
+        p.brick_size = int(self.brick_size)
+        p.refine = REFINE[self.refine]
+        p.threads = int(self.threads)
+        return p
+
+
+class SurfaceOutput:
+    """Mesh, statistics (SurfaceStats + stage times in ms) and OBJ text."""
+
+    def __init__(self, h):
+        self._h = h
+        st = native.SurfaceStats_()
+        lib().smb_surface_stats_get(h, C.byref(st))
+        self.stats = {name: getattr(st, name) for name, _ in st._fields_}
+        nv, nt = st.vertices, st.triangles
+        self.positions = np.zeros((nv, 3), np.float32)
+        self.normals = np.zeros((nv, 3), np.float32)
+        self.triangles = np.zeros((nt, 3), np.uint32)
+        self.vertex_atom = np.zeros(nv, np.uint32)
+        self.vertex_patch = np.zeros(nv, np.uint8)
+        self.vertex_component = np.zeros(nv, np.uint32)
+        if nv:
+            lib().smb_surface_mesh(h, _p(self.positions, C.c_float), _p(self.normals, C.c_float),
+                                   _p(self.triangles, C.c_uint32), _p(self.vertex_atom, C.c_uint32),
+                                   _p(self.vertex_patch, C.c_uint8), _p(self.vertex_component, C.c_uint32))
+
+    def obj(self):
+        """OBJ bytes with the default options (export/obj.rs:37-73)."""
+        n = lib().smb_surface_obj(self._h, None, 0)
+        buf = C.create_string_buffer(n)
+        lib().smb_surface_obj(self._h, buf, n)
+        return buf.raw[:n]
+
+    def write_obj(self, path):
+        err = C.create_string_buffer(512)
+        _check(lib().smb_surface_write_obj(self._h, path.encode(), err, 512), err)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().smb_surface_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+_DEVICES = {}
+
+
+def _device(index):
+    """Process-wide open devices (backend.rs:163-218 caches them the same way)."""
+    if index not in _DEVICES:
+        _DEVICES[index] = native.Device(index)
+    return _DEVICES[index]
+
+
+def _spheres(spheres):
+    a = np.ascontiguousarray(spheres, np.float64).reshape(-1, 4)
+    return a
+
+
+def compute_surface(spheres, params=SurfaceParams()):
+    """compute_surface (surface.rs:599) with Backend::Cuda: spheres as (n, 4)
+    rows x, y, z, r."""
+    s = _spheres(spheres)
+    dev = _device(params.device)
+    err = C.create_string_buffer(1024)
+    h = C.c_void_p()
+    p = params._c()
+    _check(lib().smb_compute_surface(dev.h, _p(s, C.c_double), len(s), C.byref(p), C.byref(h), err, 1024), err)
+    return SurfaceOutput(h)
+
+
+class SurfaceEngine:
+    """SurfaceEngine (surface.rs:633-711): arrangement built and uploaded
+    once, then meshed (or its device stage run) any number of times."""
+
+    def __init__(self, spheres, params=SurfaceParams()):
+        s = _spheres(spheres)
+        self.params = params
+        self.dev = _device(params.device)
+        err = C.create_string_buffer(1024)
+        h = C.c_void_p()
+        p = params._c()
+        _check(lib().smb_engine_new(self.dev.h, _p(s, C.c_double), len(s), C.byref(p), C.byref(h), err, 1024), err)
+        self.h = h
+
+    def run_device(self):
+        """Classification, gather, sampling and marching cubes (and fast-mode
+        refinement) on the resident arrangement; device times in ms."""
+        err = C.create_string_buffer(1024)
+        t = native.BatchTimes()
+        _check(lib().smb_engine_run_device(self.h, C.byref(t), err, 1024), err)
+        return dict(substates=t.substates, gather=t.gather, sample=t.sample, mc=t.mc, total=t.total)
+
+    @property
+    def bricks(self):
+        return lib().smb_engine_bricks(self.h)
+
+    def batch_info(self):
+        """Sizes and classification time of the last device run."""
+        b = lib().smb_engine_batch(self.h)
+        i = native.BatchInfo()
+        lib().smb_batch_info_get(b, C.byref(i))
+        return {name: getattr(i, name) for name, _ in i._fields_}
+
+    def count_ops(self):
+        """f32 operations and evaluated samples of the last run's sampling pass."""
+        b = lib().smb_engine_batch(self.h)
+        err = C.create_string_buffer(1024)
+        ops, n = C.c_ulonglong(0), C.c_ulonglong(0)
+        _check(lib().smb_batch_count_ops(b, C.byref(ops), C.byref(n), err, 1024), err)
+        return ops.value, n.value
+
+    def mesh(self):
+        err = C.create_string_buffer(1024)
+        h = C.c_void_p()
+        _check(lib().smb_engine_mesh(self.h, C.byref(h), err, 1024), err)
+        return SurfaceOutput(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().smb_engine_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def host_arrangement(spheres, params=SurfaceParams()):
+    """The host-built arrangement (no device), as numpy copies."""
+    s = _spheres(spheres)
+    err = C.create_string_buffer(1024)
+    h = C.c_void_p()
+    p = params._c()
+    _check(lib().smb_arrangement_build(_p(s, C.c_double), len(s), C.byref(p), C.byref(h), err, 1024), err)
+    try:
+        info = native.ArrangementInfo()
+        lib().smb_engine_arrangement(h, C.byref(info))
+        n, nc, nv = info.n_spheres, info.n_circles, info.n_vertices
+
+        def arr(ptr, count, dt):
+            if count == 0:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt).copy()
+
+        out = dict(center=arr(info.center, 3 * n, np.float64).reshape(-1, 3),
+                   expanded=arr(info.expanded, n, np.float64), status=arr(info.status, n, np.uint32),
+                   orig=arr(info.orig, n, np.uint32), circle=arr(info.circle, 10 * nc, np.float64).reshape(-1, 10),
+                   circle_ij=arr(info.circle_ij, 2 * nc, np.uint32).reshape(-1, 2),
+                   vertex=arr(info.vertex, 3 * nv, np.float64).reshape(-1, 3),
+                   vertex_atoms=arr(info.vertex_atoms, 3 * nv, np.uint32).reshape(-1, 3),
+                   nb_off=arr(info.nb_off, n + 1, np.uint32), cb_off=arr(info.cb_off, nc + 1, np.uint32),
+                   n_contained=info.n_contained, max_expanded=info.max_expanded, rho_max=info.rho_max)
+        out["nb_items"] = arr(info.nb_items, int(out["nb_off"][-1]), np.uint32)
+        out["cb_items"] = arr(info.cb_items, int(out["cb_off"][-1]), np.uint32)
+        return out
+    finally:
+        lib().smb_engine_free(h)

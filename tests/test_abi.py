@@ -10,11 +10,11 @@ import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "sesmesh_b200.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("sesmesh_b200.h", "sesmesh_b200_surface.h")]
 
 
 def declared():
-    text = open(HEADER).read()
+    text = "".join(open(h).read() for h in HEADERS)
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(smb_[a-z0-9_]+)\s*\(", text)))
 
