@@ -49,17 +49,20 @@ def args_():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="rings58800", choices=["rings58800", "globule330", "shell2400k"])
     p.add_argument("--refine", default=None, choices=[None, "exact", "fast"])
+    p.add_argument("--spacing", type=float, default=None, help="override the workload's grid spacing")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     return p.parse_args()
 
 
-def workload(name, refine=None):
+def workload(name, refine=None, spacing=None):
     from sesmesh_b200 import workloads
     w = {"rings58800": workloads.rings58800, "globule330": workloads.globule330,
          "shell2400k": workloads.shell2400k}[name]()
     if refine:
         w["refine"] = refine
+    if spacing:
+        w["spacing"] = spacing
     return w
 
 
@@ -141,7 +144,7 @@ def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    w = workload(a.workload, a.refine)
+    w = workload(a.workload, a.refine, a.spacing)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     eng, sample, spb, k, nb = cpu_leg(w, budget_s=6.0)
@@ -195,7 +198,7 @@ def run_ours(a):
 
     from sesmesh_b200 import native
     from sesmesh_b200 import surface as S
-    w = workload(a.workload, a.refine)
+    w = workload(a.workload, a.refine, a.spacing)
     params = S.SurfaceParams.ses(w["probe"]).with_spacing(w["spacing"]).with_brick_size(w["brick"]).with_refine(
         w["refine"])
     params = S.SurfaceParams(**{**params.__dict__, "device": local})
@@ -230,15 +233,18 @@ def run_ours(a):
 
     # End to end through the public API, host arrays in, mesh out.
     e2e_ms, st = [], None
-    out = S.compute_surface(w["spheres"], params)  # warm-up
+    out = S.compute_surface(w["spheres"], params) if a.e2e_steps else None  # warm-up
     for _ in range(a.e2e_steps):
         barrier()
         t0 = time.perf_counter()
         out = S.compute_surface(w["spheres"], params)
         torch.cuda.synchronize(dev)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
-    st = out.stats
-    e2e_mean = max_over_ranks(float(np.mean(e2e_ms)))
+    st = out.stats if out is not None else {k: 0 for k in ("vertices", "triangles", "host_threads", "area", "volume",
+                                                          "refine_evaluations", "refine_cpu_edges", "t_geometry",
+                                                          "t_upload", "t_device", "t_d2h", "t_host_refine",
+                                                          "t_assemble", "t_measure", "t_total")}
+    e2e_mean = max_over_ranks(float(np.mean(e2e_ms)) if e2e_ms else float("nan"))
     info = eng.batch_info()
     h2d = int(info["resident_bytes"])
     d2h = int(n_bricks * 16 + (n_bricks + 1) * 8 + st["vertices"] * 12 + st["triangles"] * 12)
