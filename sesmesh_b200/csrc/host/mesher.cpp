@@ -426,41 +426,37 @@ static void area_volume(const Mesh& m, const std::array<uint32_t, 3>& t, const d
     v = (p[0][0] * x[0] + p[0][1] * x[1] + p[0][2] * x[2]) / 6.0;
 }
 
-// Directed edge uses bucketed by the smaller vertex: use = max << 1 | forward.
-struct EdgeUses {
-    std::vector<uint64_t> start;
-    std::vector<uint64_t> uses;
-    void build(const Mesh& m) {
-        size_t nv = m.positions.size(), nt = m.triangles.size();
-        std::vector<std::atomic<uint32_t>> cnt(nv + 1);
-        for (auto& c : cnt) c.store(0, std::memory_order_relaxed);
-        parallel_for((nt + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
-            for (size_t t = c * SUM_CHUNK; t < std::min(nt, (c + 1) * SUM_CHUNK); t++)
-                for (int k = 0; k < 3; k++) {
-                    uint32_t a = m.triangles[t][k], b = m.triangles[t][(k + 1) % 3];
-                    cnt[std::min(a, b)].fetch_add(1, std::memory_order_relaxed);
-                }
-        });
-        start.assign(nv + 1, 0);
-        for (size_t v = 0; v < nv; v++) start[v + 1] = start[v] + cnt[v].load(std::memory_order_relaxed);
-        std::vector<std::atomic<uint64_t>> fill(nv);
-        for (size_t v = 0; v < nv; v++) fill[v].store(start[v], std::memory_order_relaxed);
-        uses.resize(start[nv]);
-        parallel_for((nt + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
-            for (size_t t = c * SUM_CHUNK; t < std::min(nt, (c + 1) * SUM_CHUNK); t++)
-                for (int k = 0; k < 3; k++) {
-                    uint32_t a = m.triangles[t][k], b = m.triangles[t][(k + 1) % 3];
-                    uint32_t lo = std::min(a, b), hi = std::max(a, b);
-                    uses[fill[lo].fetch_add(1, std::memory_order_relaxed)] = (uint64_t(hi) << 1) | (a < b ? 1u : 0u);
-                }
-        });
-        parallel_for((nv + 4095) / 4096, [&](size_t c, int) {
-            for (size_t v = c * 4096; v < std::min(nv, (c + 1) * 4096); v++) std::sort(uses.begin() + start[v], uses.begin() + start[v + 1]);
-        });
-    }
-};
 
-size_t defects(const Mesh& m) {
+void EdgeUses::build(const Mesh& m) {
+    size_t nv = m.positions.size(), nt = m.triangles.size();
+    std::vector<std::atomic<uint32_t>> cnt(nv + 1);
+    for (auto& c : cnt) c.store(0, std::memory_order_relaxed);
+    parallel_for((nt + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
+        for (size_t t = c * SUM_CHUNK; t < std::min(nt, (c + 1) * SUM_CHUNK); t++)
+            for (int k = 0; k < 3; k++) {
+                uint32_t a = m.triangles[t][k], b = m.triangles[t][(k + 1) % 3];
+                cnt[std::min(a, b)].fetch_add(1, std::memory_order_relaxed);
+            }
+    });
+    start.assign(nv + 1, 0);
+    for (size_t v = 0; v < nv; v++) start[v + 1] = start[v] + cnt[v].load(std::memory_order_relaxed);
+    std::vector<std::atomic<uint64_t>> fill(nv);
+    for (size_t v = 0; v < nv; v++) fill[v].store(start[v], std::memory_order_relaxed);
+    uses.resize(start[nv]);
+    parallel_for((nt + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
+        for (size_t t = c * SUM_CHUNK; t < std::min(nt, (c + 1) * SUM_CHUNK); t++)
+            for (int k = 0; k < 3; k++) {
+                uint32_t a = m.triangles[t][k], b = m.triangles[t][(k + 1) % 3];
+                uint32_t lo = std::min(a, b), hi = std::max(a, b);
+                uses[fill[lo].fetch_add(1, std::memory_order_relaxed)] = (uint64_t(hi) << 1) | (a < b ? 1u : 0u);
+            }
+    });
+    parallel_for((nv + 4095) / 4096, [&](size_t c, int) {
+        for (size_t v = c * 4096; v < std::min(nv, (c + 1) * 4096); v++) std::sort(uses.begin() + start[v], uses.begin() + start[v + 1]);
+    });
+}
+
+size_t defects(const Mesh& m, EdgeUses* keep) {
     const size_t nv = m.positions.size(), nt = m.triangles.size();
     std::atomic<size_t> bad{0};
     parallel_for((nv + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
@@ -490,7 +486,8 @@ size_t defects(const Mesh& m) {
         }
         bad += b;
     });
-    EdgeUses E;
+    EdgeUses local;
+    EdgeUses& E = keep ? *keep : local;
     E.build(m);
     parallel_for((nv + 4095) / 4096, [&](size_t c, int) {
         size_t b = 0;
@@ -504,36 +501,84 @@ size_t defects(const Mesh& m) {
             }
         bad += b;
     });
-    // Duplicate triangles: equal sorted vertex triples, bucketed by the smallest.
-    std::vector<std::array<uint32_t, 3>> s(m.triangles);
-    parallel_for((nt + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
-        for (size_t t = c * SUM_CHUNK; t < std::min(nt, (c + 1) * SUM_CHUNK); t++) std::sort(s[t].begin(), s[t].end());
-    });
-    std::sort(s.begin(), s.end());
-    for (size_t t = 1; t < nt; t++)
-        if (s[t] == s[t - 1]) bad++;
+    // Duplicate triangles: equal sorted vertex triples, bucketed by the
+    // smallest vertex (counting sort), pairs (s1, s2) sorted per bucket.
+    {
+        std::vector<std::atomic<uint32_t>> cnt(nv + 1);
+        for (auto& c : cnt) c.store(0, std::memory_order_relaxed);
+        auto sorted3 = [&](size_t t) {
+            std::array<uint32_t, 3> a = m.triangles[t];
+            if (a[0] > a[1]) std::swap(a[0], a[1]);
+            if (a[1] > a[2]) std::swap(a[1], a[2]);
+            if (a[0] > a[1]) std::swap(a[0], a[1]);
+            return a;
+        };
+        parallel_for((nt + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
+            for (size_t t = c * SUM_CHUNK; t < std::min(nt, (c + 1) * SUM_CHUNK); t++)
+                cnt[sorted3(t)[0]].fetch_add(1, std::memory_order_relaxed);
+        });
+        std::vector<uint64_t> start(nv + 1, 0);
+        for (size_t v = 0; v < nv; v++) start[v + 1] = start[v] + cnt[v].load(std::memory_order_relaxed);
+        std::vector<std::atomic<uint64_t>> fill(nv);
+        for (size_t v = 0; v < nv; v++) fill[v].store(start[v], std::memory_order_relaxed);
+        std::vector<uint64_t> pairs(nt);
+        parallel_for((nt + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
+            for (size_t t = c * SUM_CHUNK; t < std::min(nt, (c + 1) * SUM_CHUNK); t++) {
+                auto a = sorted3(t);
+                pairs[fill[a[0]].fetch_add(1, std::memory_order_relaxed)] = (uint64_t(a[1]) << 32) | a[2];
+            }
+        });
+        parallel_for((nv + 4095) / 4096, [&](size_t c, int) {
+            size_t b = 0;
+            for (size_t v = c * 4096; v < std::min(nv, (c + 1) * 4096); v++) {
+                std::sort(pairs.begin() + start[v], pairs.begin() + start[v + 1]);
+                for (uint64_t i = start[v] + 1; i < start[v + 1]; i++) b += pairs[i] == pairs[i - 1];
+            }
+            bad += b;
+        });
+    }
     return bad.load();
 }
 
-void components_and_group(Mesh& m, std::vector<Component>& comps) {
+void components_and_group(Mesh& m, std::vector<Component>& comps, const EdgeUses* uses) {
     const size_t nv = m.positions.size(), nt = m.triangles.size();
-    std::vector<uint32_t> parent(nv);
-    for (size_t v = 0; v < nv; v++) parent[v] = uint32_t(v);
+    // Lock-free union-find linking the larger root to the smaller (mesh/
+    // mod.rs:190-230): parents only decrease, every root is its component's
+    // smallest vertex, and the partition does not depend on scheduling.
+    std::vector<std::atomic<uint32_t>> parent(nv);
+    for (size_t v = 0; v < nv; v++) parent[v].store(uint32_t(v), std::memory_order_relaxed);
     auto find = [&](uint32_t x) {
-        while (parent[x] != x) x = parent[x] = parent[parent[x]];
-        return x;
-    };
-    for (auto& t : m.triangles) {
-        for (int k = 1; k < 3; k++) {
-            uint32_t a = find(t[0]), b = find(t[k]);
-            if (a != b) parent[std::max(a, b)] = std::min(a, b);
+        for (;;) {
+            uint32_t p = parent[x].load(std::memory_order_relaxed);
+            if (p == x) return x;
+            uint32_t g = parent[p].load(std::memory_order_relaxed);
+            if (g != p) parent[x].compare_exchange_weak(p, g, std::memory_order_relaxed);
+            x = g;
         }
-    }
+    };
+    auto unite = [&](uint32_t a, uint32_t b) {
+        for (;;) {
+            uint32_t ra = find(a), rb = find(b);
+            if (ra == rb) return;
+            uint32_t lo = std::min(ra, rb), hi = std::max(ra, rb);
+            if (parent[hi].compare_exchange_strong(hi, lo, std::memory_order_relaxed)) return;
+        }
+    };
+    parallel_for((nt + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
+        for (size_t t = c * SUM_CHUNK; t < std::min(nt, (c + 1) * SUM_CHUNK); t++) {
+            unite(m.triangles[t][0], m.triangles[t][1]);
+            unite(m.triangles[t][0], m.triangles[t][2]);
+        }
+    });
+    std::vector<uint32_t> root(nv);
+    parallel_for((nv + SUM_CHUNK - 1) / SUM_CHUNK, [&](size_t c, int) {
+        for (size_t v = c * SUM_CHUNK; v < std::min(nv, (c + 1) * SUM_CHUNK); v++) root[v] = find(uint32_t(v));
+    });
     std::vector<uint32_t>& id = m.vertex_component;
     id.assign(nv, 0);
     comps.clear();
     for (size_t v = 0; v < nv; v++) {
-        uint32_t r = find(uint32_t(v));
+        uint32_t r = root[v];
         if (r == v) id[v] = uint32_t(comps.size()), comps.emplace_back();
         else id[v] = id[r];
         comps[id[v]].vertices++;
@@ -565,8 +610,9 @@ void components_and_group(Mesh& m, std::vector<Component>& comps) {
     });
     for (auto& p : parts)
         for (auto& x : p) comps[x.comp].triangles += x.t, comps[x.comp].area += x.a, comps[x.comp].volume += x.v;
-    EdgeUses E;
-    E.build(m);
+    EdgeUses local;
+    if (!uses) local.build(m);
+    const EdgeUses& E = uses ? *uses : local;
     std::vector<int64_t> ecount(comps.size(), 0);
     for (size_t v = 0; v < nv; v++)
         for (uint64_t i = E.start[v]; i < E.start[v + 1]; i++)

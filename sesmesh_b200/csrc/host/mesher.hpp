@@ -91,10 +91,20 @@ struct Component {
 std::string assemble(const int32_t* keys, size_t n, const uint32_t* edge_off, const uint32_t* edges,
                      const uint32_t* tri_off, const uint32_t* tri_refs, Mesh& mesh);
 
-// validate_with (mesh/mod.rs:638-700): total defect count (0 = valid).
-size_t defects(const Mesh& m);
+// Directed edge uses of a mesh bucketed by their smaller vertex (each
+// bucket sorted): use = larger vertex << 1 | (min -> max direction); the
+// uses of one undirected edge are adjacent (Edges, mesh/mod.rs:300-380).
+struct EdgeUses {
+    std::vector<uint64_t> start;
+    std::vector<uint64_t> uses;
+    void build(const Mesh& m);
+};
+
+// validate_with (mesh/mod.rs:638-700): total defect count (0 = valid); the
+// edge uses are kept in *keep when given.
+size_t defects(const Mesh& m, EdgeUses* keep = nullptr);
 // components_with + group_by_component (mesh/mod.rs:185-297, post.rs:14-32).
-void components_and_group(Mesh& m, std::vector<Component>& comps);
+void components_and_group(Mesh& m, std::vector<Component>& comps, const EdgeUses* uses = nullptr);
 std::string obj_text(const Mesh& m, int precision = 4, bool normals = true);
 void push_fixed(std::string& buf, float x, int prec);
 

@@ -249,9 +249,10 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
     mesh.vertex_patch.swap(mo.patches);
     double t_assemble = ms_since(t2);
     auto t3 = clk::now();
-    size_t bad = defects(mesh);
+    EdgeUses uses;
+    size_t bad = defects(mesh, &uses);
     if (bad) return set_err(err, errlen, "mesh failed validation (%zu defects)", bad), SMB_ERR_STATE;
-    components_and_group(mesh, s->comps);
+    components_and_group(mesh, s->comps, &uses);
     double t_measure = ms_since(t3);
     smb_surface_stats& st = s->stats;
     st.spheres = e->arr.n;
