@@ -15,6 +15,7 @@ constexpr double CLASSIFY_EPS = 2e-3;      // field/lattice.rs:20
 constexpr double GEOM_EPS = 1e-9;          // geom/arrangement.rs:26
 constexpr float INSIDE_TOL = 2e-5f;        // field/kernel.rs:40
 constexpr int64_t KEY_BIAS = int64_t(1) << 20;  // field/lattice.rs:15
+constexpr double PRUNE_MARGIN = 1e-3;      // f32 safety margin of the sampler's candidate pruning
 
 constexpr uint32_t ST_SAMPLE = 0, ST_OUT = 1, ST_IN = 2;
 constexpr uint32_t STATUS_EXPOSED = 0, STATUS_BURIED = 1, STATUS_CONTAINED = 2;

@@ -183,39 +183,25 @@ __device__ __forceinline__ int sample_owner(int x, int y, int z, int sub, const 
     return -1;
 }
 
-// Engine::sub_states (field/kernel.rs:467-482), one warp per sub-block of a
-// brick, then the +-band values of samples no sampled sub-block owns.
+// Engine::sub_states (field/kernel.rs:467-482): one warp per sub-block,
+// independent of the brick's other sub-blocks (the +-band values of samples
+// no sampled sub-block owns are written by the marching-cubes count pass).
 __global__ void __launch_bounds__(256) k_substates(DArr A, DLat L, const int4* keys, uint32_t n_bricks, uint32_t* rec,
-                                                   uint32_t* sampled, float* values) {
-    __shared__ uint32_t st[8];
-    uint32_t brick = blockIdx.x;
-    if (brick >= n_bricks) return;
-    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                                                   uint32_t* sampled) {
+    const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (j >= n_bricks * 8) return;
+    const uint32_t brick = j >> 3, w = j & 7;
     int4 key = keys[brick];
     double h = L.h, sub = double(L.sub), half = double(L.sub) * 0.5;
     double bx = double((long long)key.x * L.b) * h, by = double((long long)key.y * L.b) * h,
            bz = double((long long)key.z * L.b) * h;
     double ox = double(w & 1) * sub + half, oy = double((w >> 1) & 1) * sub + half, oz = double((w >> 2) & 1) * sub + half;
     int s = uniform_sign_warp(A, bx + ox * h, by + oy * h, bz + oz * h, L.rho_sub, lane);
-    if (lane == 0) {
-        uint32_t state = s < 0 ? ST_SAMPLE : (s == 1 ? ST_OUT : ST_IN);
-        st[w] = state;
-        uint32_t j = brick * 8 + w;
-        uint32_t* r = rec + size_t(j) * REC_WORDS;
-        for (int q = 0; q < REC_WORDS; q++) r[q] = 0;
-        r[R_STATE] = state;
-        sampled[j] = state == ST_SAMPLE ? 1u : 0u;
-    }
-    __syncthreads();
-    uint32_t sts[8];
-    for (int q = 0; q < 8; q++) sts[q] = st[q];
-    int side = L.b + 1;
-    float* v = values + size_t(brick) * L.spb;
-    for (int i = threadIdx.x; i < L.spb; i += blockDim.x) {
-        int x = i % side, y = (i / side) % side, z = i / (side * side);
-        bool positive;
-        if (sample_owner(x, y, z, L.sub, sts, &positive) < 0) v[i] = positive ? L.band32 : -L.band32;
-    }
+    uint32_t state = s < 0 ? ST_SAMPLE : (s == 1 ? ST_OUT : ST_IN);
+    uint32_t* r = rec + size_t(j) * REC_WORDS;
+    if (lane < REC_WORDS) r[lane] = lane == R_STATE ? state : 0u;
+    if (lane == 0) sampled[j] = state == ST_SAMPLE ? 1u : 0u;
 }
 
 // ---------------------------------------------------------------------------
@@ -329,6 +315,7 @@ __global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work,
         });
         if (pass == 0) n_in = nn;
     }
+    if (lane == 0) atomicMax(&O.counters[CNT_MAXNN], (unsigned long long)nn);
     if (nn > caps.near) return overflow(REC_OVERFLOW);
     __syncwarp();
     // Sorted copy of the near ids for blocker lookups.
@@ -376,6 +363,11 @@ __global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work,
         int pos = warp_append(p, nv);
         if (pos >= 0 && pos < caps.v) v_id[pos] = vi;
     });
+    if (lane == 0) {
+        atomicMax(&O.counters[CNT_MAXNS], (unsigned long long)ns);
+        atomicMax(&O.counters[CNT_MAXNC], (unsigned long long)nc);
+        atomicMax(&O.counters[CNT_MAXNV], (unsigned long long)nv);
+    }
     if (ns > caps.s || nc > caps.c || nv > caps.v) return overflow(REC_OVERFLOW);
     __syncwarp();
     // Rank sorts: (key, index) pairs are distinct, so ranks are a permutation.
@@ -430,7 +422,7 @@ __global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work,
     // Space: ids (CSR words) and the packed f32 block the sampler stages.
     const unsigned long long ids_words =
         (unsigned long long)nn + 2ull * ns + 1 + nsb + 2ull * nc + 1 + ncb + nv;
-    const unsigned long long tail_words = (unsigned long long)ns + 1 + nsb + nc + 1 + ncb;
+    const unsigned long long tail_words = 2ull * ns + 1 + nsb + 2ull * nc + 1 + ncb;
     const unsigned long long units = 2ull * nn + ns + 3ull * nc + nv + (tail_words + 3) / 4;
     unsigned long long ids_base = 0, pack_base = 0;
     if (lane == 0) {
@@ -453,15 +445,17 @@ __global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work,
     uint32_t* w_cblk = w_coff + nc + 1;
     uint32_t* w_v = w_cblk + ncb;
     // Packed block: nearA (x,y,z,R^2), nearT (x,y,z,(R-tol)^2), S (x,y,z,R),
-    // C (3 x float4), V (x,y,z,0), then s_off, s_blk, c_off, c_blk words.
+    // C (3 x float4), V (x,y,z,0), then the S and C pruning keys (f32) and
+    // the s_off, s_blk, c_off, c_blk words.
     float4* pk = reinterpret_cast<float4*>(O.pack + pack_base);
     float4* p_nearA = pk;
     float4* p_nearT = p_nearA + nn;
     float4* p_s = p_nearT + nn;
     float4* p_c = p_s + ns;
     float4* p_v = p_c + 3 * nc;
-    uint32_t* p_tail = reinterpret_cast<uint32_t*>(p_v + nv);
-    uint32_t* p_soff = p_tail;
+    float* p_skey = reinterpret_cast<float*>(p_v + nv);
+    float* p_ckey = p_skey + ns;
+    uint32_t* p_soff = reinterpret_cast<uint32_t*>(p_ckey + nc);
     uint32_t* p_sblk = p_soff + ns + 1;
     uint32_t* p_coff = p_sblk + nsb;
     uint32_t* p_cblk = p_coff + nc + 1;
@@ -477,6 +471,15 @@ __global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work,
         p_nearT[i] = make_float4(x, y, z, rt * rt);
     }
     for (int r = lane; r <= ns; r += 32) w_soff[r] = s_off[r], p_soff[r] = s_off[r];
+    // Pruning keys: every sample the sub-block evaluates lies within rho of
+    // its centre, and |d - R| and the circle distance are 1-Lipschitz, so a
+    // candidate whose centre value minus rho exceeds the sample's current best
+    // cannot improve it; PRUNE_MARGIN (1e-3 A) covers f32 rounding, so the
+    // skipped candidates are exactly those whose test would fail.
+    for (int r = lane; r < ns; r += 32)
+        p_skey[r] = __double2float_rd(s_key[s_perm[r]] - rho - PRUNE_MARGIN);
+    for (int r = lane; r < nc; r += 32)
+        p_ckey[r] = __double2float_rd(c_key[c_perm[r]] - rho - PRUNE_MARGIN);
     for (int r = lane; r < ns; r += 32) {
         uint32_t i = s_perm[r], k = s_id[i];
         w_s[r] = k;
@@ -602,7 +605,9 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
     const float4* S = nearT + nn;
     const float4* C = S + ns;
     const float4* V = C + 3 * nc;
-    const uint32_t* s_off = reinterpret_cast<const uint32_t*>(V + nv);
+    const float* s_key = reinterpret_cast<const float*>(V + nv);
+    const float* c_key = s_key + ns;
+    const uint32_t* s_off = reinterpret_cast<const uint32_t*>(c_key + nc);
     const uint32_t* s_blk = s_off + ns + 1;
     const uint32_t* c_off = s_blk + nsb;
     const uint32_t* c_blk = c_off + nc + 1;
@@ -634,7 +639,7 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
         }
         float value = probe;
         if (inside) {
-            if (COUNT) ops += 9ull * nv + 12ull * ns + 26ull * nc + 2;
+            if (COUNT) ops += 9ull * nv + 2;
             float best2 = cutoff2;
             for (int v = 0; v < nv; v++) {
                 float4 q = V[v];
@@ -642,6 +647,9 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
                 best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
             }
             for (int si = 0; si < ns; si++) {
+                const float kk = s_key[si];
+                if (kk > 0.0f && kk * kk >= best2) break;
+                if (COUNT) ops += 12;
                 float4 c = S[si];
                 float dx = px - c.x, dy = py - c.y, dz = pz - c.z;
                 float dist = sqrtf(dx * dx + dy * dy + dz * dz);
@@ -664,6 +672,9 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
                 if (valid) best2 = lb2;
             }
             for (int ci = 0; ci < nc; ci++) {
+                const float kk = c_key[ci];
+                if (kk > 0.0f && kk * kk >= best2) break;
+                if (COUNT) ops += 26;
                 float4 m = C[3 * ci], u = C[3 * ci + 1], e2 = C[3 * ci + 2];
                 float yx = px - m.x, yy = py - m.y, yz = pz - m.z;
                 float along = yx * u.x + yy * u.y + yz * u.z;
@@ -709,18 +720,40 @@ constexpr int MC_THREADS = 256;
 __constant__ uint8_t c_edge_lower[12] = {0, 2, 4, 6, 0, 1, 4, 5, 0, 1, 2, 3};
 
 template <bool FILL>
-__global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L, uint32_t n_bricks, const float* values, uint32_t* counts,
+__global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L, uint32_t n_bricks, float* values, const uint32_t* rec, uint32_t* counts,
                                                    const uint32_t* edge_off, const uint32_t* tri_off, uint32_t* edges,
                                                    float2* edge_vals, uint32_t* tris) {
     extern __shared__ float v[];
     __shared__ uint16_t t_off[257];
     __shared__ uint8_t t_edges[SMB_MC_TRIANGLES * 3];
     __shared__ unsigned long long sh[MC_THREADS / 32];
+    __shared__ uint32_t sts[8];
     const uint32_t brick = blockIdx.x;
     if (brick >= n_bricks) return;
     const int b = L.b, s = b + 1;
-    const float* src = values + size_t(brick) * L.spb;
-    for (int i = threadIdx.x; i < L.spb; i += blockDim.x) v[i] = src[i];
+    float* src = values + size_t(brick) * L.spb;
+    if (!FILL) {
+        // Samples that no sampled sub-block owns get +-band here (Engine::
+        // assign, field/kernel.rs:489-546): the sign of the last containing
+        // uniform sub-block.
+        if (threadIdx.x < 8) sts[threadIdx.x] = rec[(size_t(brick) * 8 + threadIdx.x) * REC_WORDS + R_STATE];
+        __syncthreads();
+        uint32_t st[8];
+        for (int q = 0; q < 8; q++) st[q] = sts[q];
+        for (int i = threadIdx.x; i < L.spb; i += blockDim.x) {
+            int x = i % s, y = (i / s) % s, z = i / (s * s);
+            bool positive;
+            if (sample_owner(x, y, z, L.sub, st, &positive) < 0) {
+                float bv = positive ? L.band32 : -L.band32;
+                src[i] = bv;
+                v[i] = bv;
+            } else {
+                v[i] = src[i];
+            }
+        }
+    } else {
+        for (int i = threadIdx.x; i < L.spb; i += blockDim.x) v[i] = src[i];
+    }
     for (int i = threadIdx.x; i < 257; i += blockDim.x) t_off[i] = SMB_TRI_OFFSET[i];
     for (int i = threadIdx.x; i < SMB_MC_TRIANGLES * 3; i += blockDim.x) t_edges[i] = SMB_TRI_EDGES[i / 3][i % 3];
     __syncthreads();
@@ -901,7 +934,7 @@ __global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC,
     }
     __syncthreads();
     const float probe = L.probe32, band = L.band32, h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
-    const int b = L.b, side = b + 1, sub = L.sub;
+    const int b = L.b, sub = L.sub;
     struct Eval {
         float value, qx, qy, qz;
         uint32_t feat;
@@ -1085,8 +1118,8 @@ void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n
 }
 
 void launch_substates(const DArr& A, const DLat& L, const int4* keys, uint32_t n, uint32_t* rec, uint32_t* sampled,
-                      float* values, cudaStream_t s) {
-    if (n) COUNT(1), k_substates<<<n, 256, 0, s>>>(A, L, keys, n, rec, sampled, values);
+                      cudaStream_t s) {
+    if (n) COUNT(1), k_substates<<<n, 256, 0, s>>>(A, L, keys, n, rec, sampled);
 }
 
 cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const uint32_t* work, uint32_t n,
@@ -1113,7 +1146,7 @@ cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work,
     return cudaGetLastError();
 }
 
-cudaError_t launch_mc(const DLat& L, uint32_t n, const float* values, uint32_t* counts, const uint32_t* edge_off,
+cudaError_t launch_mc(const DLat& L, uint32_t n, float* values, const uint32_t* rec, uint32_t* counts, const uint32_t* edge_off,
                       const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
                       cudaStream_t s) {
     if (!n) return cudaSuccess;
@@ -1122,7 +1155,7 @@ cudaError_t launch_mc(const DLat& L, uint32_t n, const float* values, uint32_t* 
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     COUNT(1);
-    kern<<<n, MC_THREADS, smem, s>>>(L, n, values, counts, edge_off, tri_off, edges, edge_vals, tris);
+    kern<<<n, MC_THREADS, smem, s>>>(L, n, values, rec, counts, edge_off, tri_off, edges, edge_vals, tris);
     return cudaGetLastError();
 }
 

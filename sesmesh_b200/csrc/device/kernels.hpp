@@ -29,7 +29,7 @@ __host__ __device__ inline size_t gather_smem_bytes(const GatherCaps& c) {
 // Device counters of one gather/sample pass.
 enum : int {
     CNT_IDS = 0, CNT_PACK = 1, CNT_MAXPACK = 2, CNT_OVERFLOW = 3, CNT_NOMEM = 4, CNT_TIMEOUT = 5, CNT_OPS = 6,
-    CNT_OWNED = 7, CNT_N = 8
+    CNT_OWNED = 7, CNT_MAXNN = 8, CNT_MAXNS = 9, CNT_MAXNC = 10, CNT_MAXNV = 11, CNT_N = 16
 };
 constexpr uint32_t REC_NOMEM = 2;
 
@@ -64,13 +64,13 @@ void launch_classify_bricks(const DArr& A, const DLat& L, const BrickBox& box, c
                             uint32_t* surface, cudaStream_t s);
 void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n, int4* keys, cudaStream_t s);
 void launch_substates(const DArr& A, const DLat& L, const int4* keys, uint32_t n, uint32_t* rec, uint32_t* sampled,
-                      float* values, cudaStream_t s);
+                      cudaStream_t s);
 cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const uint32_t* work, uint32_t n,
                           const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s);
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
                           bool count, cudaStream_t s);
-cudaError_t launch_mc(const DLat& L, uint32_t n, const float* values, uint32_t* counts, const uint32_t* edge_off,
+cudaError_t launch_mc(const DLat& L, uint32_t n, float* values, const uint32_t* rec, uint32_t* counts, const uint32_t* edge_off,
                       const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
                       cudaStream_t s);
 

@@ -6,6 +6,7 @@
 // {mod.rs,resident.rs,memory.rs,stream.rs}): one stream per device, device
 // buffers grown on demand and reused across runs, CUDA events around each
 // pass.
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -501,8 +502,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
         (rc = b->tri_off.reserve(count * 4 + 4, err, errlen)))
         return rc;
     cudaEventRecord(b->ev[0], s);
-    launch_substates(r->A, L, keys, uint32_t(count), b->rec.as<uint32_t>(), b->sampled.as<uint32_t>(),
-                     b->values.as<float>(), s);
+    launch_substates(r->A, L, keys, uint32_t(count), b->rec.as<uint32_t>(), b->sampled.as<uint32_t>(), s);
     launch_scan(b->sampled.as<uint32_t>(), uint32_t(nsub), nullptr, b->work.as<uint32_t>(),
                 b->tiles.as<unsigned long long>(), b->totals.as<unsigned long long>(), s);
     cudaEventRecord(b->ev[1], s);
@@ -564,6 +564,18 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     }
     b->ids_words = size_t(cnt[CNT_IDS]);
     b->max_pack = uint32_t(cnt[CNT_MAXPACK]);
+    {
+        // Caps for the next run of this batch: the list sizes seen, with an
+        // eighth to spare, rounded to 16; warps per block so that a block's
+        // scratch stays near 64 KB (several blocks per SM).
+        auto up = [](unsigned long long v) { return std::max(32, int((v + v / 8 + 16 + 15) / 16 * 16)); };
+        GatherCaps next{up(cnt[CNT_MAXNN]), up(cnt[CNT_MAXNS]), up(cnt[CNT_MAXNC]), up(cnt[CNT_MAXNV])};
+        size_t per = gather_smem_bytes(next);
+        if (per <= size_t(d->smem_optin)) {
+            b->caps = next;
+            b->gather_warps = int(std::max<size_t>(1, std::min<size_t>(8, size_t(65536) / per)));
+        }
+    }
     cudaEventRecord(b->ev[2], s);
 
     // (c) sampling.
@@ -577,8 +589,8 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     cudaEventRecord(b->ev[3], s);
 
     // (d) marching cubes: counts, offsets, fill.
-    e = launch_mc(L, uint32_t(count), b->values.as<float>(), b->mc_counts.as<uint32_t>(), nullptr, nullptr, nullptr,
-                  nullptr, nullptr, false, s);
+    e = launch_mc(L, uint32_t(count), b->values.as<float>(), b->rec.as<uint32_t>(), b->mc_counts.as<uint32_t>(), nullptr,
+                  nullptr, nullptr, nullptr, nullptr, false, s);
     if (e != cudaSuccess) return set_err(err, errlen, "mc launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     unsigned long long* tot = b->totals.as<unsigned long long>();
     launch_scan(b->mc_counts.as<uint32_t>(), uint32_t(count), b->edge_off.as<uint32_t>(), nullptr,
@@ -601,7 +613,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     if ((rc = b->edges.reserve(b->n_edges * 4, err, errlen)) || (rc = b->edge_vals.reserve(b->n_edges * 8, err, errlen)) ||
         (rc = b->tris.reserve(b->n_tris * 12, err, errlen)))
         return rc;
-    e = launch_mc(L, uint32_t(count), b->values.as<float>(), nullptr, b->edge_off.as<uint32_t>(),
+    e = launch_mc(L, uint32_t(count), b->values.as<float>(), b->rec.as<uint32_t>(), nullptr, b->edge_off.as<uint32_t>(),
                   b->tri_off.as<uint32_t>(), b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->tris.as<uint32_t>(),
                   true, s);
     if (e != cudaSuccess) return set_err(err, errlen, "mc launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
@@ -646,7 +658,7 @@ int smb_refine(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errl
         b->refined = true;
         return SMB_OK;
     }
-    size_t smem = size_t(b->max_pack) * 18 + 64;
+    size_t smem = size_t(b->max_pack) * 16 + 64;
     if (smem > size_t(d->smem_optin))
         return set_err(err, errlen, "a sub-block's candidates exceed shared memory for refinement"), SMB_ERR_MEMORY;
     cudaEventRecord(b->ev[4], s);
