@@ -262,6 +262,10 @@ def run_ours(a):
                    "grid_points": int(grid_points), "refine": w["refine"], "parallelism": "replicas x%d" % world,
                    "l2": "flushed before every step (256 MiB write)"},
         "stage_ms": stage,
+        "lists": {"sampled_subblocks": int(info["sampled_subblocks"]), "ids_words": int(info["ids_words"]),
+                  "pack_bytes_mean": float(info["pack_units"]) * 16 / max(1, info["sampled_subblocks"]),
+                  "pack_bytes_max": int(info["max_pack_units"]) * 16, "edges": int(info["edges"]),
+                  "triangles": int(info["triangles"])},
         "e2e": {"value": world * grid_points / (e2e_mean / 1e3) / 1e6, "unit": "Mgridpts/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_mesh": e2e_mean,
                 "host_threads": st["host_threads"],

@@ -226,9 +226,18 @@ void resize(MeshOut& out, size_t nv, size_t nb) {
 }  // namespace
 
 // point.rs:496-582 (SES)
+// Pruning: every point evaluated with a ball's candidates lies in the ball,
+// and |d - R|, the circle distance and the vertex distance are 1-Lipschitz,
+// so a candidate whose centre value minus the radius exceeds the current best
+// by more than f64 rounding cannot pass its test; the lists are sorted by
+// that centre value, so evaluation stops at the first such candidate.  The
+// result (value, feature, closest point) is unchanged.
+constexpr double PRUNE_MARGIN = 1e-9;
+
 void gather_local(const Arrangement& A, const V3& b, double rho, double band, Local& out) {
     out.inside.clear(), out.near.clear(), out.spheres.clear(), out.s_blk.clear(), out.circles.clear();
     out.c_blk.clear(), out.vertices.clear(), out.order.clear();
+    out.s_key.clear(), out.c_key.clear(), out.v_key.clear();
     out.s_off.assign(1, 0), out.c_off.assign(1, 0);
     const double reach = A.probe + band + rho;
     A.cells.near(b, reach + A.max_expanded, [&](uint32_t k) {
@@ -247,6 +256,7 @@ void gather_local(const Arrangement& A, const V3& b, double rho, double band, Lo
     };
     for (auto& o : out.order) {
         out.spheres.push_back(o.second);
+        out.s_key.push_back(o.first - rho - PRUNE_MARGIN);
         keep_near(A.nb_items.data() + A.nb_off[o.second], A.nb_items.data() + A.nb_off[o.second + 1], out.s_blk);
         out.s_off.push_back(uint32_t(out.s_blk.size()));
     }
@@ -262,6 +272,7 @@ void gather_local(const Arrangement& A, const V3& b, double rho, double band, Lo
     nearest_first(out.order);
     for (auto& o : out.order) {
         out.circles.push_back(o.second);
+        out.c_key.push_back(o.first - rho - PRUNE_MARGIN);
         keep_near(A.cb_items.data() + A.cb_off[o.second], A.cb_items.data() + A.cb_off[o.second + 1], out.c_blk);
         out.c_off.push_back(uint32_t(out.c_blk.size()));
     }
@@ -271,7 +282,7 @@ void gather_local(const Arrangement& A, const V3& b, double rho, double band, Lo
         if (d <= reach) out.order.push_back({d, vi});
     });
     nearest_first(out.order);
-    for (auto& o : out.order) out.vertices.push_back(o.second);
+    for (auto& o : out.order) out.vertices.push_back(o.second), out.v_key.push_back(o.first - rho - PRUNE_MARGIN);
 }
 
 // point.rs:686-738 (SES)
@@ -284,11 +295,12 @@ NearEval eval_local(const Arrangement& A, const V3& x, double band, const Local&
         }
     if (!inside) return NearEval{A.probe, Feature{F_SOLVENT, 0}, x};
     Best best{A.probe + band, x, Feature{F_BEYOND, 0}};
-    for (size_t k = 0; k < l.spheres.size(); k++)
+    for (size_t k = 0; k < l.spheres.size() && l.s_key[k] < best.d; k++)
         try_sphere(A, x, l.spheres[k], l.s_blk.data() + l.s_off[k], l.s_blk.data() + l.s_off[k + 1], best);
-    for (size_t k = 0; k < l.circles.size(); k++)
+    for (size_t k = 0; k < l.circles.size() && l.c_key[k] < best.d; k++)
         try_circle(A, x, l.circles[k], l.c_blk.data() + l.c_off[k], l.c_blk.data() + l.c_off[k + 1], best);
-    for (uint32_t vi : l.vertices) {
+    for (size_t k = 0; k < l.vertices.size() && l.v_key[k] < best.d; k++) {
+        uint32_t vi = l.vertices[k];
         V3 p = V3::at(&A.vertex[3 * size_t(vi)]);
         double d = x.dist(p);
         if (d < best.d) best = Best{d, p, Feature{F_VERTEX, vi}};

@@ -23,9 +23,12 @@ struct NearEval {
     V3 closest;
 };
 
-// Candidates of one ball (SesField::gather_local, field/point.rs:496-582).
+// Candidates of one ball (SesField::gather_local, field/point.rs:496-582),
+// with pruning keys: the candidate's value at the ball centre minus the
+// ball radius and a margin, ascending like the lists.
 struct Local {
     std::vector<uint32_t> inside, near, spheres, s_off, s_blk, circles, c_off, c_blk, vertices;
+    std::vector<double> s_key, c_key, v_key;
     std::vector<std::pair<double, uint32_t>> order;
 };
 
