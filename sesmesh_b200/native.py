@@ -119,6 +119,8 @@ SIGNATURES = {
     "smb_batch_info_get": (C.c_int, [_vp, C.POINTER(BatchInfo)]),
     "smb_batch_count_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _cp, _sz]),
     "smb_engine_batch": (_vp, [_vp]),
+    "smb_mc_noalloc": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _sz, C.POINTER(_sz),
+                                 C.POINTER(_sz), _cp, _sz]),
     # include/sesmesh_b200_surface.h
     "smb_compute_surface": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_), C.POINTER(_vp),
                                       _cp, _sz]),
