@@ -187,6 +187,22 @@ int smb_batch_info_get(const smb_batch* batch, smb_batch_info* out);
  * count of the roofline; values are rewritten identically). */
 int smb_batch_count_ops(smb_batch* batch, unsigned long long* ops, unsigned long long* samples, char* err,
                         size_t errlen);
+/* Learned warm start of fast mode (no counterpart in the reference; the
+ * reference's fast mode starts every edge from the linear guess): an MLP
+ * 32 -> 64 -> 64 -> 1 (GELU, sigmoid output t in [0, 1]) with BF16 weights
+ * on the tensor cores and FP32 accumulation, proposing each crossing edge's
+ * root parameter.  Parameters are SMB_MLP_NPARAM f32 values: W1 [64][32],
+ * b1 [64], W2 [64][64], b2 [64], w3 [64], b3 (row-major, out x in). */
+#define SMB_MLP_NPARAM 6337
+#define SMB_MLP_FEATURES 32
+typedef struct smb_mlp smb_mlp;
+int smb_mlp_new(smb_device* dev, const float* params, smb_mlp** out, char* err, size_t errlen);
+void smb_mlp_free(smb_mlp* mlp);
+int smb_mlp_set_params(smb_mlp* mlp, const float* params, char* err, size_t errlen);
+int smb_mlp_get_params(const smb_mlp* mlp, float* params);
+/* t[i] = MLP(x[32 i .. 32 i + 31]) for host arrays (tests, diagnostics). */
+int smb_mlp_forward(smb_mlp* mlp, const float* x, size_t n, float* t, char* err, size_t errlen);
+
 /* Marching cubes (the last pass of smb_run) over caller-owned device
  * buffers, with no device allocation at all.  This entry point has no
  * counterpart in the reference: it serves callers that cannot allocate

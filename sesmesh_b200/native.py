@@ -119,6 +119,11 @@ SIGNATURES = {
     "smb_batch_info_get": (C.c_int, [_vp, C.POINTER(BatchInfo)]),
     "smb_batch_count_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _cp, _sz]),
     "smb_engine_batch": (_vp, [_vp]),
+    "smb_mlp_new": (C.c_int, [_vp, _fp, C.POINTER(_vp), _cp, _sz]),
+    "smb_mlp_free": (None, [_vp]),
+    "smb_mlp_set_params": (C.c_int, [_vp, _fp, _cp, _sz]),
+    "smb_mlp_get_params": (C.c_int, [_vp, _fp]),
+    "smb_mlp_forward": (C.c_int, [_vp, _fp, _sz, _fp, _cp, _sz]),
     "smb_mc_noalloc": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _sz, C.POINTER(_sz),
                                  C.POINTER(_sz), _cp, _sz]),
     # include/sesmesh_b200_surface.h
@@ -378,6 +383,47 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             lib().smb_batch_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+MLP_NPARAM = 6337
+MLP_FEATURES = 32
+
+
+class Mlp:
+    """The warm-start MLP on a device (smb_mlp_*)."""
+
+    def __init__(self, device, params):
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == MLP_NPARAM
+        err = C.create_string_buffer(1024)
+        h = _vp()
+        _check(lib().smb_mlp_new(device.h, _p(p, C.c_float), C.byref(h), err, 1024), err)
+        self.h = h
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        err = C.create_string_buffer(1024)
+        _check(lib().smb_mlp_set_params(self.h, _p(p, C.c_float), err, 1024), err)
+
+    def params(self):
+        out = np.zeros(MLP_NPARAM, np.float32)
+        lib().smb_mlp_get_params(self.h, _p(out, C.c_float))
+        return out
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_FEATURES)
+        t = np.zeros(len(x), np.float32)
+        err = C.create_string_buffer(1024)
+        _check(lib().smb_mlp_forward(self.h, _p(x, C.c_float), len(x), _p(t, C.c_float), err, 1024), err)
+        return t
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().smb_mlp_free(self.h)
             self.h = None
 
     def __del__(self):
