@@ -41,7 +41,7 @@ def gelu_grad(z):
 
 def forward(p, x, quantize=True):
     w1, b1, w2, b2, w3, b3 = unpack(p)
-    q = bf16 if quantize else (lambda a: np.asarray(a, np.float32))
+    q = bf16 if quantize else (lambda a: np.asarray(a, np.float64))
     xq = q(x).astype(np.float64)
     z1 = xq @ q(w1).astype(np.float64).T + b1
     a1 = gelu(z1)
