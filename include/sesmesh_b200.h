@@ -202,6 +202,16 @@ int smb_mlp_set_params(smb_mlp* mlp, const float* params, char* err, size_t errl
 int smb_mlp_get_params(const smb_mlp* mlp, float* params);
 /* t[i] = MLP(x[32 i .. 32 i + 31]) for host arrays (tests, diagnostics). */
 int smb_mlp_forward(smb_mlp* mlp, const float* x, size_t n, float* t, char* err, size_t errlen);
+/* Loss (mean squared error of t, *loss) and its gradient over the
+ * parameter vector for n rows as one batch (at most 2^20 rows); the
+ * products of forward and backward run on the tensor cores. */
+int smb_mlp_gradient(smb_mlp* mlp, const float* x, const float* target, size_t n, float* loss, float* grad,
+                     char* err, size_t errlen);
+/* One epoch of Adam over the rows in order, minibatches of `batch` rows (a
+ * multiple of 128); losses[k] gets minibatch k's loss before its step
+ * (ceil(n / batch) values) when non-null. */
+int smb_mlp_train_epoch(smb_mlp* mlp, const float* x, const float* target, size_t n, size_t batch, float lr,
+                        float* losses, char* err, size_t errlen);
 
 /* Marching cubes (the last pass of smb_run) over caller-owned device
  * buffers, with no device allocation at all.  This entry point has no

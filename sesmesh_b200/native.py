@@ -124,6 +124,8 @@ SIGNATURES = {
     "smb_mlp_set_params": (C.c_int, [_vp, _fp, _cp, _sz]),
     "smb_mlp_get_params": (C.c_int, [_vp, _fp]),
     "smb_mlp_forward": (C.c_int, [_vp, _fp, _sz, _fp, _cp, _sz]),
+    "smb_mlp_gradient": (C.c_int, [_vp, _fp, _fp, _sz, _fp, _fp, _cp, _sz]),
+    "smb_mlp_train_epoch": (C.c_int, [_vp, _fp, _fp, _sz, _sz, C.c_float, _fp, _cp, _sz]),
     "smb_mc_noalloc": (C.c_int, [_vp, _vp, _vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _sz, C.POINTER(_sz),
                                  C.POINTER(_sz), _cp, _sz]),
     # include/sesmesh_b200_surface.h
@@ -420,6 +422,26 @@ class Mlp:
         err = C.create_string_buffer(1024)
         _check(lib().smb_mlp_forward(self.h, _p(x, C.c_float), len(x), _p(t, C.c_float), err, 1024), err)
         return t
+
+    def gradient(self, x, target):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_FEATURES)
+        y = np.ascontiguousarray(target, np.float32)
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(MLP_NPARAM, np.float32)
+        err = C.create_string_buffer(1024)
+        _check(lib().smb_mlp_gradient(self.h, _p(x, C.c_float), _p(y, C.c_float), len(x), _p(loss, C.c_float),
+                                      _p(g, C.c_float), err, 1024), err)
+        return float(loss[0]), g
+
+    def train_epoch(self, x, target, batch=4096, lr=1e-3):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_FEATURES)
+        y = np.ascontiguousarray(target, np.float32)
+        steps = (len(x) + batch - 1) // batch
+        losses = np.zeros(steps, np.float32)
+        err = C.create_string_buffer(1024)
+        _check(lib().smb_mlp_train_epoch(self.h, _p(x, C.c_float), _p(y, C.c_float), len(x), batch, lr,
+                                         _p(losses, C.c_float), err, 1024), err)
+        return losses
 
     def close(self):
         if getattr(self, "h", None):
