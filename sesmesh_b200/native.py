@@ -399,6 +399,7 @@ class Mlp:
     """The warm-start MLP on a device (smb_mlp_*)."""
 
     def __init__(self, device, params):
+        self.device = device  # the device must outlive the MLP
         p = np.ascontiguousarray(params, np.float32)
         assert p.size == MLP_NPARAM
         err = C.create_string_buffer(1024)
