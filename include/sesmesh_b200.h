@@ -58,6 +58,9 @@ typedef struct {
  * Replaces cuda::Runtime::load/open + Device (crates/sesmesh-gpu/src/cuda/
  * mod.rs:93-240, 418-485) and the K0 self-test (cuda/selftest.rs:16-40). */
 int smb_open(int index, smb_device** out, char* err, size_t errlen);
+/* Handles may be freed in any order: a closed device stays open until the
+ * residents and MLPs made on it are freed, a freed resident until its
+ * batches are (the handle must not be used after its own free). */
 void smb_close(smb_device* dev);
 /* Device::info (cuda/mod.rs:418-470). */
 int smb_device_info_get(const smb_device* dev, smb_device_info* out);
@@ -212,6 +215,33 @@ int smb_mlp_gradient(smb_mlp* mlp, const float* x, const float* target, size_t n
  * (ceil(n / batch) values) when non-null. */
 int smb_mlp_train_epoch(smb_mlp* mlp, const float* x, const float* target, size_t n, size_t batch, float lr,
                         float* losses, char* err, size_t errlen);
+/* smb_refine with each edge's starting point chosen by the MLP.  For the
+ * sphere candidate whose contact sphere (radius R - probe) best explains the
+ * edge's two samples, the kernel runs smb_refine's own iteration on that
+ * sphere alone (no field evaluation): where the sphere is the surface's
+ * nearest feature along the whole edge, that is where smb_refine would stop.
+ * Where the MLP answers >= 0.5 the edge starts there, else at the linear
+ * guess fa / (fa - fb) that smb_refine always takes (x:
+ * smb_batch_edge_features).  The iteration that follows is smb_refine's,
+ * with its bracket, tolerance, budgets and outputs: a start the field
+ * judges within the tolerance is accepted after one evaluation, any other
+ * start falls back to the bracketed refinement.  The MLP runs inside the
+ * refinement kernel, 128 edges per tensor-core tile.  A null mlp is
+ * smb_refine. */
+int smb_refine_warm(smb_resident* res, smb_batch* batch, const smb_mlp* mlp, double* ms, char* err, size_t errlen);
+/* The MLP's input for every crossing edge of the last run (32 f32 per edge,
+ * marching-cubes edge order; zeros for edges the device does not refine)
+ * and covered[k] = 1 where the device refines edge k (its sub-block was
+ * sampled).  Features: fa / h, fb / h; finite-difference gradients of the
+ * samples at both ends (6); the 4 sphere candidates whose contact spheres
+ * best explain the two samples, centre offset from the edge midpoint and
+ * contact radius, / 4 A (16); the mismatch of the first two,
+ * log10(max(m, 1e-9)) / 9 + 1 (2); (t_c - t_lin) * 8 clamped to [-4, 4],
+ * t_c the contact iteration's result and t_lin the linear guess; t_lin; h;
+ * probe radius; both gradients along the edge scaled by h / (fb - fa),
+ * clamped to [-10, 10].  Discards the last refinement. */
+int smb_batch_edge_features(smb_resident* res, smb_batch* batch, float* features, uint8_t* covered, char* err,
+                            size_t errlen);
 
 /* Marching cubes (the last pass of smb_run) over caller-owned device
  * buffers, with no device allocation at all.  This entry point has no

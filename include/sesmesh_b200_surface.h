@@ -57,6 +57,21 @@ size_t smb_engine_bricks(const smb_engine* e);
 int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen);
 /* The engine's device batch (sizes, counters, operation counts). */
 smb_batch* smb_engine_batch(smb_engine* e);
+/* Learned warm start of fast mode (no counterpart in the reference): the
+ * engine's device refinement starts each edge from the MLP's proposal
+ * (smb_refine_warm); null restores the linear start.  The MLP must stay
+ * alive while the engine uses it. */
+int smb_engine_set_warm_start(smb_engine* e, const smb_mlp* mlp);
+/* Training rows of the warm start (no counterpart in the reference): runs
+ * the device stage, then for every edge the device refines (marching-cubes
+ * order) its SMB_MLP_FEATURES features and, as the label, the root
+ * parameter that exact mode's f64 host refinement finds on that edge
+ * (before the edge clamp).  *n gets the row count; the rows are copied when
+ * features and labels are non-null (SMB_ERR_MEMORY if cap < *n).  The rows
+ * are kept until the next device run, so a first call with null buffers
+ * sizes them and a second one copies them. */
+int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, size_t cap, size_t* n, char* err,
+                               size_t errlen);
 
 void smb_surface_free(smb_surface* s);
 int smb_surface_stats_get(const smb_surface* s, smb_surface_stats* out);

@@ -11,6 +11,7 @@
 
 #include "common.cuh"
 #include "kernels.hpp"
+#include "mlp.cuh"
 #include "scan.cuh"
 #define SMB_MC_QUAL __constant__
 #include "../mc_table.inc"
@@ -845,11 +846,132 @@ struct RefOut {
 
 constexpr uint32_t FEAT_SHIFT_D = 29;
 
+// The refinement iteration of k_refine (Newton with the Illinois bracket,
+// MAX_ITER steps) run on one atom's contact sphere alone, F(x) = |x - c| - r:
+// where that sphere is the surface's nearest feature along the whole edge,
+// this is the iteration k_refine itself would run, so its result is where
+// the reference's fast mode would stop.  No field evaluation.
+__device__ __forceinline__ float contact_iteration(float ax, float ay, float az, int axis, float h, float hd,
+                                                   float4 c, float r, float fa, float fb, const RefineConsts& RC) {
+    float t = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
+    float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
+    int side = 0;
+    for (uint32_t it = 0; it < RC.max_iter; it++) {
+        float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f),
+              z = az + (axis == 2 ? hd * t : 0.0f);
+        float dx = x - c.x, dy = y - c.y, dz = z - c.z;
+        float len = sqrtf(dx * dx + dy * dy + dz * dz);
+        float gv = len - r;
+        if (fabsf(gv) <= RC.tol) break;
+        if ((gv < 0.0f) == (g0 < 0.0f)) {
+            t0 = t, g0 = gv;
+            if (side == -1) g1 *= 0.5f;
+            side = -1;
+        } else {
+            t1 = t, g1 = gv;
+            if (side == 1) g0 *= 0.5f;
+            side = 1;
+        }
+        float slope = len > 1e-12f ? ((axis == 0 ? dx : (axis == 1 ? dy : dz)) / len) * h : 0.0f;
+        float newton = t - gv / slope;
+        if (fabsf(slope) > 1e-3f * hd && newton > t0 && newton < t1) {
+            t = newton;
+        } else {
+            float s = (t0 * g1 - t1 * g0) / (g1 - g0);
+            t = (isfinite(s) && s > t0 && s < t1) ? s : 0.5f * (t0 + t1);
+        }
+    }
+    return t;
+}
+
+// Features of one crossing edge for the warm-start MLP (32 values):
+//   0-1   fa / h, fb / h (sample values at the ends)
+//   2-7   finite-difference gradients of the sampled field at both ends
+//         (central where both neighbours are in the brick, else one-sided)
+//   8-23  the 4 class-S candidates whose contact spheres (radius
+//         r = R - probe) best explain the two end samples (smallest
+//         mismatch max(| |a - c| - r - fa |, | |b - c| - r - fb |)):
+//         centre minus edge midpoint / 4 A, and r / 4 A (zeros when fewer)
+//   24-25 the mismatch of the first two, log10(max(m, 1e-9)) / 9 + 1
+//   26    (t_c - t_lin) * 8 clamped to [-4, 4]: t_c the contact iteration
+//         on the first candidate's sphere (contact_iteration)
+//   27    t_lin = fa / (fa - fb) (the linear guess)
+//   28-29 spacing h and probe radius (A)
+//   30-31 the gradients' components along the edge times h / (fb - fa),
+//         clamped to [-10, 10]
+// Returns t_c (t_lin without candidates), in f32 at full precision.
+__device__ __forceinline__ float edge_features(const float* val, int b, float h, float hd, float probe, int ex, int ey,
+                                               int ez, float ax, float ay, float az, int axis, float fa, float fb,
+                                               const float4* S, int ns, const RefineConsts& RC, float* f) {
+    const int side = b + 1;
+    auto V = [&](int x, int y, int z) { return val[(z * side + y) * side + x]; };
+    auto grad = [&](int x, int y, int z, float* g) {
+        int c[3] = {x, y, z};
+        for (int d = 0; d < 3; d++) {
+            int lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
+            lo[d]--, hi[d]++;
+            if (lo[d] >= 0 && hi[d] <= b) g[d] = (V(hi[0], hi[1], hi[2]) - V(lo[0], lo[1], lo[2])) / (2.0f * h);
+            else if (hi[d] <= b) g[d] = (V(hi[0], hi[1], hi[2]) - V(x, y, z)) / h;
+            else g[d] = (V(x, y, z) - V(lo[0], lo[1], lo[2])) / h;
+        }
+    };
+    const float t_lin = fa / (fa - fb);
+    f[0] = fa / h, f[1] = fb / h;
+    grad(ex, ey, ez, f + 2);
+    grad(ex + (axis == 0), ey + (axis == 1), ez + (axis == 2), f + 5);
+    const float mx = (float(ex) + (axis == 0 ? 0.5f : 0.0f)) * h, my = (float(ey) + (axis == 1 ? 0.5f : 0.0f)) * h,
+                mz = (float(ez) + (axis == 2 ? 0.5f : 0.0f)) * h;
+    const float bx = ax + (axis == 0 ? hd : 0.0f), by = ay + (axis == 1 ? hd : 0.0f), bz = az + (axis == 2 ? hd : 0.0f);
+    float bd[4] = {3.4e38f, 3.4e38f, 3.4e38f, 3.4e38f};
+    int bi[4] = {-1, -1, -1, -1};
+    for (int i = 0; i < ns; i++) {
+        float4 c = S[i];
+        const float r = c.w - probe;
+        float dx = ax - c.x, dy = ay - c.y, dz = az - c.z;
+        float ea = fabsf(sqrtf(dx * dx + dy * dy + dz * dz) - r - fa);
+        dx = bx - c.x, dy = by - c.y, dz = bz - c.z;
+        float eb = fabsf(sqrtf(dx * dx + dy * dy + dz * dz) - r - fb);
+        float d = fmaxf(ea, eb);
+        if (d < bd[3]) {
+            int q = 3;
+            while (q > 0 && d < bd[q - 1]) bd[q] = bd[q - 1], bi[q] = bi[q - 1], q--;
+            bd[q] = d, bi[q] = i;
+        }
+    }
+    for (int q = 0; q < 4; q++) {
+        if (bi[q] >= 0) {
+            float4 c = S[bi[q]];
+            f[8 + 4 * q] = (c.x - mx) * 0.25f, f[9 + 4 * q] = (c.y - my) * 0.25f, f[10 + 4 * q] = (c.z - mz) * 0.25f;
+            f[11 + 4 * q] = (c.w - probe) * 0.25f;
+        } else {
+            f[8 + 4 * q] = f[9 + 4 * q] = f[10 + 4 * q] = f[11 + 4 * q] = 0.0f;
+        }
+    }
+    f[24] = bi[0] >= 0 ? log10f(fmaxf(bd[0], 1e-9f)) / 9.0f + 1.0f : 1.0f;
+    f[25] = bi[1] >= 0 ? log10f(fmaxf(bd[1], 1e-9f)) / 9.0f + 1.0f : 1.0f;
+    float t_c = t_lin;
+    if (bi[0] >= 0) {
+        float4 c = S[bi[0]];
+        t_c = contact_iteration(ax, ay, az, axis, h, hd, c, c.w - probe, fa, fb, RC);
+    }
+    f[26] = fminf(fmaxf(t_c - t_lin, -0.5f), 0.5f) * 8.0f;
+    f[27] = t_lin;
+    f[28] = h, f[29] = probe;
+    const float inv = h / (fb - fa);
+    f[30] = fminf(fmaxf(f[2 + axis] * inv, -10.0f), 10.0f);
+    f[31] = fminf(fmaxf(f[5 + axis] * inv, -10.0f), 10.0f);
+    return t_c;
+}
+
+template <int MODE>
 __global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC, const int4* keys, const uint32_t* work,
                                                 uint32_t n_work, const uint32_t* rec, const uint32_t* ids,
                                                 const uint32_t* edge_off, const uint32_t* edges,
-                                                const float2* edge_vals, RefOut out) {
-    extern __shared__ __align__(16) float4 rs[];
+                                                const float2* edge_vals, RefOut out, const float* values, MlpDev mlp,
+                                                float* feat_out, uint32_t mlp_off, uint32_t list_off,
+                                                unsigned long long* counters) {
+    extern __shared__ __align__(128) float4 rs[];
+    __shared__ uint32_t ecount;
     const uint32_t j = work[blockIdx.x];
     const uint32_t brick = j >> 3, sb = j & 7;
     const uint32_t* R = rec + size_t(j) * REC_WORDS;
@@ -1007,17 +1129,65 @@ __global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC,
         e.value = probe - best;
         return e;
     };
+    // This sub-block's crossing edges (lower sample in it); outputs go to
+    // each edge's own index, so the order of the list does not matter.
     const uint32_t e0 = edge_off[brick], e1 = edge_off[brick + 1];
+    uint32_t* elist = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(rs) + list_off);
+    if (threadIdx.x == 0) ecount = 0;
+    __syncthreads();
     for (uint32_t k = e0 + threadIdx.x; k < e1; k += blockDim.x) {
-        const uint32_t code = edges[k];
+        const uint32_t cell = edges[k] / 3;
+        const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
+        if (min(ex / sub, 1) + 2 * min(ey / sub, 1) + 4 * min(ez / sub, 1) == int(sb)) elist[atomicAdd(&ecount, 1u)] = k;
+    }
+    __syncthreads();
+    const uint32_t ne = ecount;
+    MlpSmem* M = reinterpret_cast<MlpSmem*>(reinterpret_cast<unsigned char*>(rs) + mlp_off);
+    if (MODE == REFINE_MLP) mlp_setup(*M, mlp, 64);
+    uint32_t phase = 0;
+    const float* val = values + size_t(brick) * L.spb;
+    for (uint32_t c0 = 0; c0 < ne; c0 += blockDim.x) {
+        const uint32_t idx = c0 + threadIdx.x;
+        const bool have = idx < ne;
+        const uint32_t k = have ? elist[idx] : 0u;
+        const uint32_t code = have ? edges[k] : 0u;
         const uint32_t cell = code / 3, axis = code % 3;
         const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
-        if (min(ex / sub, 1) + 2 * min(ey / sub, 1) + 4 * min(ez / sub, 1) != int(sb)) continue;
-        const float2 fv = edge_vals[k];
+        const float2 fv = have ? edge_vals[k] : make_float2(-1.0f, 1.0f);
         const float fa = fv.x, fb = fv.y;
+        float t_start = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
+        if (MODE != REFINE_PLAIN) {
+            float f[MLP_IN];
+            float t_contact = t_start;
+            if (have) {
+                const float ax = float(ex) * h + float(ex) * RC.h_lo, ay = float(ey) * h + float(ey) * RC.h_lo,
+                            az = float(ez) * h + float(ez) * RC.h_lo;
+                t_contact = edge_features(val, b, h, hd, probe, ex, ey, ez, ax, ay, az, int(axis), fa, fb, S, ns, RC, f);
+            } else {
+                for (int q = 0; q < MLP_IN; q++) f[q] = 0.0f;
+            }
+            if (MODE == EDGE_FEATURES) {
+                if (have) {
+                    for (int q = 0; q < MLP_IN; q++) feat_out[size_t(k) * MLP_IN + q] = f[q];
+                    out.evals[k] = 1;
+                }
+                continue;
+            }
+            mlp_put_row(*M, f);
+            float tm;
+            // The MLP chooses the start: the contact iteration's result
+            // where it answers >= 0.5 (and that is within half an edge of the
+            // linear guess), else the linear guess.
+            if (mlp_forward(*M, phase, &tm, nullptr, nullptr, nullptr, 0)) {
+                if (tm >= 0.5f && fabsf(f[26]) < 4.0f) t_start = t_contact;
+            } else if (threadIdx.x == 0) {
+                atomicAdd(&counters[CNT_TIMEOUT], 1ull);
+            }
+        }
+        if (!have) continue;
         const float ax = float(ex) * h + float(ex) * RC.h_lo, ay = float(ey) * h + float(ey) * RC.h_lo,
                     az = float(ez) * h + float(ez) * RC.h_lo;
-        float t = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
+        float t = t_start;
         float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
         int side_ = 0;
         bool converged = false;
@@ -1076,6 +1246,7 @@ __global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC,
         out.q[3 * size_t(k)] = last.qx, out.q[3 * size_t(k) + 1] = last.qy, out.q[3 * size_t(k) + 2] = last.qz;
         out.evals[k] = evals | (converged ? 0x80000000u : 0u);
     }
+    if (MODE == REFINE_MLP) mlp_teardown(*M, 64);
 }
 
 // ---------------------------------------------------------------------------
@@ -1166,12 +1337,20 @@ size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uin
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
                           uint32_t n, const uint32_t* rec, const uint32_t* ids, const uint32_t* edge_off,
                           const uint32_t* edges, const float2* edge_vals, float* t, uint32_t* feat, float* q,
-                          uint32_t* evals, size_t smem, cudaStream_t s) {
+                          uint32_t* evals, size_t cand_bytes, int mode, const float* values, const MlpDev* mlp,
+                          float* feat_out, unsigned long long* counters, cudaStream_t s) {
     if (!n) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(k_refine, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const uint32_t mlp_off = uint32_t((cand_bytes + 127) / 128 * 128);
+    const uint32_t list_off = mlp_off + (mode == REFINE_MLP ? uint32_t((sizeof(MlpSmem) + 127) / 128 * 128) : 0u);
+    const size_t smem = size_t(list_off) + size_t(3) * L.sub * L.sub * L.sub * 4 + 16;
+    auto kern = mode == REFINE_MLP ? k_refine<REFINE_MLP> : (mode == EDGE_FEATURES ? k_refine<EDGE_FEATURES>
+                                                                                 : k_refine<REFINE_PLAIN>);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     COUNT(1);
-    k_refine<<<n, 128, smem, s>>>(A, L, RC, keys, work, n, rec, ids, edge_off, edges, edge_vals, RefOut{t, feat, q, evals});
+    MlpDev md = mlp ? *mlp : MlpDev{nullptr, nullptr, nullptr};
+    kern<<<n, 128, smem, s>>>(A, L, RC, keys, work, n, rec, ids, edge_off, edges, edge_vals, RefOut{t, feat, q, evals},
+                              values, md, feat_out, mlp_off, list_off, counters);
     return cudaGetLastError();
 }
 

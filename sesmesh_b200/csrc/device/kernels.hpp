@@ -49,10 +49,13 @@ struct RefineConsts {
 };
 
 size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uint32_t nsb, uint32_t ncb);
+enum : int { REFINE_PLAIN = 0, REFINE_MLP = 1, EDGE_FEATURES = 2 };
+struct MlpDev;
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
                           uint32_t n, const uint32_t* rec, const uint32_t* ids, const uint32_t* edge_off,
                           const uint32_t* edges, const float2* edge_vals, float* t, uint32_t* feat, float* q,
-                          uint32_t* evals, size_t smem, cudaStream_t s);
+                          uint32_t* evals, size_t cand_bytes, int mode, const float* values, const MlpDev* mlp,
+                          float* feat_out, unsigned long long* counters, cudaStream_t s);
 
 unsigned long long kernel_launches();
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);

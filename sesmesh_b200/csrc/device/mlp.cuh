@@ -56,8 +56,9 @@ __device__ __forceinline__ float gelu_grad(float z) {
     return 0.5f * (1.0f + th) + 0.5f * z * (1.0f - th * th) * k * (1.0f + 3.0f * 0.044715f * z * z);
 }
 
-// Loads the weights into shared memory and allocates TMEM (all threads).
-__device__ __forceinline__ void mlp_setup(MlpSmem& S, const MlpDev& P) {
+// Loads the weights into shared memory and allocates `ncols` TMEM columns
+// (all threads; 64 suffice for inference, see mlp_forward).
+__device__ __forceinline__ void mlp_setup(MlpSmem& S, const MlpDev& P, uint32_t ncols = 128) {
     const int t = threadIdx.x;
     const uint4* w1 = reinterpret_cast<const uint4*>(P.w1t);
     const uint4* w2 = reinterpret_cast<const uint4*>(P.w2t);
@@ -72,24 +73,26 @@ __device__ __forceinline__ void mlp_setup(MlpSmem& S, const MlpDev& P) {
         S.b3 = P.p[MLP_B3];
         umma::bar_init(&S.bar, 1);
     }
-    if (t < 32) umma::tmem_alloc(&S.tmem, 128);
+    if (t < 32) umma::tmem_alloc(&S.tmem, ncols);
     umma::fence_before();
     __syncthreads();
     umma::fence_after();
 }
 
-__device__ __forceinline__ void mlp_teardown(MlpSmem& S) {
+__device__ __forceinline__ void mlp_teardown(MlpSmem& S, uint32_t ncols = 128) {
     umma::fence_before();
     __syncthreads();
-    if (threadIdx.x < 32) umma::tmem_dealloc(S.tmem, 128);
+    if (threadIdx.x < 32) umma::tmem_dealloc(S.tmem, ncols);
 }
 
 // Forward pass of the tile whose inputs thread r has placed in S.x (row r);
 // returns thread r's output t and, when z1/z2 are given, the hidden
 // pre-activations of its row.  `phase` is the mbarrier parity of the first of
-// the two waits (it advances by 2 per call); false if a wait gave up.
+// the two waits (it advances by 2 per call); false if a wait gave up.  Layer
+// 2 accumulates at TMEM column `l2col`: 0 reuses layer 1's columns (every
+// thread has read them before the layer-2 MMA is issued), 64 keeps them.
 __device__ __forceinline__ bool mlp_forward(MlpSmem& S, uint32_t& phase, float* t_out, float* z1, float* z2,
-                                            float* a2_out) {
+                                            float* a2_out, uint32_t l2col = 64) {
     const int r = threadIdx.x, warp = r >> 5;
     umma::fence_smem_async();
     __syncthreads();
@@ -124,7 +127,7 @@ __device__ __forceinline__ bool mlp_forward(MlpSmem& S, uint32_t& phase, float* 
         const uint32_t id = umma::idesc_bf16(MLP_ROWS, MLP_H);
         const uint32_t aa = umma::saddr(S.a1), wa = umma::saddr(S.w2);
         for (int k = 0; k < MLP_H / 16; k++)
-            umma::mma_bf16(S.tmem + 64, umma::desc_kmajor(aa + k * 256, MLP_H), umma::desc_kmajor(wa + k * 256, MLP_H),
+            umma::mma_bf16(S.tmem + l2col, umma::desc_kmajor(aa + k * 256, MLP_H), umma::desc_kmajor(wa + k * 256, MLP_H),
                            id, k > 0);
         umma::commit(&S.bar);
     }
@@ -134,7 +137,7 @@ __device__ __forceinline__ bool mlp_forward(MlpSmem& S, uint32_t& phase, float* 
     float y = S.b3;
     for (int c = 0; c < MLP_H; c += 8) {
         float v[8];
-        umma::ld8(S.tmem, warp, 64 + c, v);
+        umma::ld8(S.tmem, warp, l2col + c, v);
         umma::ld_wait();
         for (int i = 0; i < 8; i++) {
             float z = v[i] + S.b2[c + i];

@@ -109,6 +109,7 @@ struct Vertex {
     V3 pos, normal;
     uint8_t patch;
     uint32_t atom;
+    double t;  // root parameter before the edge clamp
 };
 
 // extract::vertex (extract.rs:425-535), exact mode.
@@ -168,6 +169,7 @@ Vertex refine_edge(const Arrangement& A, const MeshParams& P, const V3& pa, cons
         }
     }
     Vertex out;
+    out.t = t;
     out.pos = pa + d * clamp(t, P.t_min, 1.0 - P.t_min);
     if (!have) {
         evals++;
@@ -212,6 +214,7 @@ void put(MeshOut& out, size_t at, const Vertex& v) {
     out.normals[at] = {float(v.normal.x), float(v.normal.y), float(v.normal.z)};
     out.atoms[at] = v.atom;
     out.patches[at] = v.patch;
+    out.t[at] = float(v.t);
 }
 
 void resize(MeshOut& out, size_t nv, size_t nb) {
@@ -219,6 +222,7 @@ void resize(MeshOut& out, size_t nv, size_t nb) {
     out.normals.resize(nv);
     out.atoms.resize(nv);
     out.patches.resize(nv);
+    out.t.resize(nv);
     out.evals.assign(nb, 0);
     out.cpu_refined.assign(nb, 0);
 }
@@ -356,6 +360,7 @@ void place_fast(const Arrangement& A, const MeshParams& P, const int32_t* keys, 
                 if (ok) {
                     V3 d = g.pb - g.pa;
                     Vertex v;
+                    v.t = t;
                     v.pos = g.pa + d * clamp(t, P.t_min, 1.0 - P.t_min);
                     NearEval e{0.0, Feature{kind, id},
                                base + V3(double(dev.closest[3 * k]), double(dev.closest[3 * k + 1]), double(dev.closest[3 * k + 2]))};

@@ -47,6 +47,7 @@ struct MeshOut {
     std::vector<std::array<float, 3>> positions, normals;
     std::vector<uint32_t> atoms;
     std::vector<uint8_t> patches;
+    std::vector<float> t;         // per vertex: root parameter on its edge (before the clamp)
     std::vector<uint32_t> evals;  // per brick
     std::vector<uint32_t> cpu_refined;  // per brick (fast mode)
 };

@@ -48,6 +48,10 @@ struct smb_engine {
     size_t touched = 0;
     smb_batch_times times{};
     double t_classify = 0;
+    const smb_mlp* warm = nullptr;  // warm start of fast-mode refinement
+    // Warm-start training rows of the last device run.
+    bool rows_ready = false;
+    std::vector<float> row_x, row_t;
 };
 
 struct smb_surface {
@@ -181,9 +185,11 @@ int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size
     smb_batch_times t{};
     rc = smb_run(e->res, 0, surface, e->batch, &t, err, errlen);
     if (rc != SMB_OK) return rc;
+    e->rows_ready = false;
     if (e->params.refine == SMB_REFINE_FAST) {
         double ms = 0;
-        rc = smb_refine(e->res, e->batch, &ms, err, errlen);
+        rc = e->warm ? smb_refine_warm(e->res, e->batch, e->warm, &ms, err, errlen)
+                     : smb_refine(e->res, e->batch, &ms, err, errlen);
         if (rc != SMB_OK) return rc;
         t.total += ms;
     }
@@ -196,17 +202,10 @@ size_t smb_engine_bricks(const smb_engine* e) { return e && e->res ? e->res->n_b
 
 smb_batch* smb_engine_batch(smb_engine* e) { return e ? e->batch : nullptr; }
 
-// Whole mesh stage and the stages after it: device part, results to the
-// host, f64 refinement (exact) or placement (fast), assembly, validation,
-// components and grouping.
-int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) {
-    if (!e || !out) return SMB_ERR_ARG;
-    *out = nullptr;
-    auto t_all = clk::now();
-    int rc = smb_engine_run_device(e, nullptr, err, errlen);
-    if (rc != SMB_OK) return rc;
-    auto t0 = clk::now();
+// Brick keys and marching-cubes lists of the last device run to the host.
+static int fetch_mc(smb_engine* e, char* err, size_t errlen) {
     size_t nb = e->res->n_bricks, ne = 0, nt = 0;
+    int rc;
     smb_batch_mc_counts(e->batch, &ne, &nt);
     e->keys.resize(3 * nb);
     e->edge_off.resize(nb + 1);
@@ -223,6 +222,21 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
         e->edge_off.assign(1, 0);
         e->tri_off.assign(1, 0);
     }
+    return SMB_OK;
+}
+
+// Whole mesh stage and the stages after it: device part, results to the
+// host, f64 refinement (exact) or placement (fast), assembly, validation,
+// components and grouping.
+int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) {
+    if (!e || !out) return SMB_ERR_ARG;
+    *out = nullptr;
+    auto t_all = clk::now();
+    int rc = smb_engine_run_device(e, nullptr, err, errlen);
+    if (rc != SMB_OK) return rc;
+    auto t0 = clk::now();
+    if ((rc = fetch_mc(e, err, errlen)) != SMB_OK) return rc;
+    size_t nb = e->res->n_bricks, ne = e->edges.size();
     bool fast = e->params.refine == SMB_REFINE_FAST;
     if (fast && ne) {
         e->t.resize(ne), e->feat.resize(ne), e->closest.resize(3 * ne), e->evals.resize(ne);
@@ -280,6 +294,43 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
     st.t_mesh_stage = ms_since(t_all) - t_assemble - t_measure;
     st.host_threads = threads();
     *out = s.release();
+    return SMB_OK;
+}
+
+int smb_engine_set_warm_start(smb_engine* e, const smb_mlp* mlp) {
+    if (!e) return SMB_ERR_ARG;
+    e->warm = mlp;
+    return SMB_OK;
+}
+
+int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, size_t cap, size_t* n, char* err,
+                               size_t errlen) {
+    if (!e || !n) return SMB_ERR_ARG;
+    if (!e->rows_ready) {
+        int rc = smb_engine_run_device(e, nullptr, err, errlen);
+        if (rc != SMB_OK) return rc;
+        if ((rc = fetch_mc(e, err, errlen)) != SMB_OK) return rc;
+        if ((rc = smb_resident_set_refinement(e->res, err, errlen)) != SMB_OK) return rc;
+        size_t ne = e->edges.size();
+        std::vector<float> x(ne * SMB_MLP_FEATURES);
+        std::vector<uint8_t> covered(ne);
+        if ((rc = smb_batch_edge_features(e->res, e->batch, x.data(), covered.data(), err, errlen)) != SMB_OK) return rc;
+        MeshOut mo;
+        refine_exact(e->arr, e->mp, e->keys.data(), e->res->n_bricks, e->edge_off.data(), e->edges.data(),
+                     e->edge_vals.data(), mo);
+        e->row_x.clear(), e->row_t.clear();
+        for (size_t k = 0; k < ne; k++) {
+            if (!covered[k]) continue;
+            e->row_x.insert(e->row_x.end(), x.begin() + k * SMB_MLP_FEATURES, x.begin() + (k + 1) * SMB_MLP_FEATURES);
+            e->row_t.push_back(mo.t[k]);
+        }
+        e->rows_ready = true;
+    }
+    *n = e->row_t.size();
+    if (!features || !labels) return SMB_OK;
+    if (cap < *n) return set_err(err, errlen, "%zu rows do not fit in %zu", *n, cap), SMB_ERR_MEMORY;
+    std::copy(e->row_x.begin(), e->row_x.end(), features);
+    std::copy(e->row_t.begin(), e->row_t.end(), labels);
     return SMB_OK;
 }
 

@@ -295,6 +295,7 @@ MlpDev mlp_dev(const smb_mlp* m) {
     return MlpDev{m->p.as<float>(), m->w1t.as<__nv_bfloat16>(), m->w2t.as<__nv_bfloat16>()};
 }
 size_t mlp_smem_bytes() { return sizeof(MlpSmem) + 128; }
+const smb_device* mlp_device(const smb_mlp* m) { return m->dev; }
 }  // namespace smb
 
 extern "C" {
@@ -305,6 +306,7 @@ int smb_mlp_new(smb_device* dev, const float* params, smb_mlp** out, char* err, 
     CK(cudaSetDevice(dev->index));
     auto* m = new smb_mlp();
     m->dev = dev;
+    dev_retain(dev);
     int rc;
     if ((rc = m->p.reserve(MLP_NPARAM * 4, err, errlen)) || (rc = m->w1t.reserve(MLP_H * MLP_IN * 2, err, errlen)) ||
         (rc = m->w2t.reserve(MLP_H * MLP_H * 2, err, errlen)) || (rc = m->w2tt.reserve(MLP_H * MLP_H * 2, err, errlen)) ||
@@ -323,7 +325,9 @@ void smb_mlp_free(smb_mlp* m) {
     for (DBuf* b : {&m->p, &m->w1t, &m->w2t, &m->w2tt, &m->x, &m->y, &m->t, &m->counters, &m->partial, &m->loss,
                     &m->grad, &m->m, &m->v})
         b->release();
+    smb_device* d = m->dev;
     delete m;
+    dev_release(d);
 }
 
 int smb_mlp_set_params(smb_mlp* m, const float* params, char* err, size_t errlen) {

@@ -16,6 +16,7 @@
 
 #include "../../include/sesmesh_b200.h"
 #include "device/kernels.hpp"
+#include "device/mlp.cuh"
 #include "runtime.hpp"
 
 using namespace smb;
@@ -104,6 +105,19 @@ void DBuf::release() {
     cap = 0;
 }
 
+static void destroy_device(smb_device* d) {
+    if (d->gone.exchange(true)) return;
+    cudaSetDevice(d->index);
+    if (d->stream) cudaStreamDestroy(d->stream);
+    delete d;
+}
+
+void dev_retain(smb_device* d) { d->refs.fetch_add(1); }
+
+void dev_release(smb_device* d) {
+    if (d->refs.fetch_sub(1) == 1 && d->closed.load()) destroy_device(d);
+}
+
 }  // namespace smb
 
 extern "C" {
@@ -151,9 +165,8 @@ int smb_open(int index, smb_device** out, char* err, size_t errlen) {
 
 void smb_close(smb_device* d) {
     if (!d) return;
-    cudaSetDevice(d->index);
-    if (d->stream) cudaStreamDestroy(d->stream);
-    delete d;
+    d->closed.store(true);
+    if (d->refs.load() == 0) destroy_device(d);
 }
 
 int smb_device_info_get(const smb_device* d, smb_device_info* out) {
@@ -251,6 +264,7 @@ int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_latt
     CK(cudaSetDevice(d->index));
     auto* r = new smb_resident();
     r->dev = d;
+    dev_retain(d);
     int rc = SMB_OK;
     auto fail = [&](int code) {
         smb_resident_free(r);
@@ -341,13 +355,21 @@ int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_latt
     return SMB_OK;
 }
 
-void smb_resident_free(smb_resident* r) {
-    if (!r) return;
-    cudaSetDevice(r->dev->index);
-    cudaStreamSynchronize(r->dev->stream);
+static void destroy_resident(smb_resident* r) {
+    if (r->gone.exchange(true)) return;
+    smb_device* d = r->dev;
+    cudaSetDevice(d->index);
+    cudaStreamSynchronize(d->stream);
     for (void* p : r->owned) cudaFree(p);
     if (r->keys) cudaFree(r->keys);
     delete r;
+    dev_release(d);
+}
+
+void smb_resident_free(smb_resident* r) {
+    if (!r) return;
+    r->freed.store(true);
+    if (r->refs.load() == 0) destroy_resident(r);
 }
 
 size_t smb_resident_bytes(const smb_resident* r) { return r ? r->bytes : 0; }
@@ -456,6 +478,7 @@ int smb_batch_new(smb_resident* r, smb_batch** out, char* err, size_t errlen) {
     CK(cudaSetDevice(r->dev->index));
     auto* b = new smb_batch();
     b->res = r;
+    r->refs.fetch_add(1);
     for (auto& ev : b->ev) cudaEventCreate(&ev);
     *out = b;
     return SMB_OK;
@@ -467,7 +490,9 @@ void smb_batch_free(smb_batch* b) {
     cudaStreamSynchronize(b->res->dev->stream);
     for (DBuf* p : b->bufs()) p->release();
     for (auto& ev : b->ev) cudaEventDestroy(ev);
+    smb_resident* r = b->res;
     delete b;
+    if (r->refs.fetch_sub(1) == 1 && r->freed.load()) destroy_resident(r);
 }
 
 int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch_times* times, char* err,
@@ -641,10 +666,16 @@ int smb_resident_set_refinement(smb_resident* r, char* err, size_t errlen) {
     return SMB_OK;
 }
 
-int smb_refine(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errlen) {
+// One refinement-kernel pass over the sampled sub-blocks of the last run:
+// plain (linear start), warm (MLP start) or the feature pass (features of
+// each covered edge into e_x, evals = 1 marks it covered).
+static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* mlp, double* ms, char* err,
+                       size_t errlen) {
     if (!r || !b || b->res != r) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
     if (!r->refine_ready) return set_err(err, errlen, "smb_resident_set_refinement must run first"), SMB_ERR_STATE;
     smb_device* d = r->dev;
+    if (mode == REFINE_MLP && (!mlp || mlp_device(mlp) != d))
+        return set_err(err, errlen, "the MLP must live on the resident's device"), SMB_ERR_ARG;
     CK(cudaSetDevice(d->index));
     cudaStream_t s = d->stream;
     size_t ne = b->n_edges;
@@ -652,28 +683,68 @@ int smb_refine(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errl
     if ((rc = b->e_t.reserve(ne * 4, err, errlen)) || (rc = b->e_feat.reserve(ne * 4, err, errlen)) ||
         (rc = b->e_q.reserve(ne * 12, err, errlen)) || (rc = b->e_evals.reserve(ne * 4, err, errlen)))
         return rc;
+    if (mode == EDGE_FEATURES && (rc = b->e_x.reserve(ne * 4 * 32, err, errlen))) return rc;
     b->refined = false;
     if (ms) *ms = 0;
     if (ne == 0 || b->n_work == 0) {
-        b->refined = true;
+        if (ne) CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
+        if (ne && mode == EDGE_FEATURES) CK(cudaMemsetAsync(b->e_x.p, 0, ne * 4 * 32, s));
+        CK(cudaStreamSynchronize(s));
+        b->refined = mode != EDGE_FEATURES;
         return SMB_OK;
     }
-    size_t smem = size_t(b->max_pack) * 16 + 64;
+    const size_t cand = size_t(b->max_pack) * 16 + 64;
+    const size_t smem = (cand + 127) / 128 * 128 + (mode == REFINE_MLP ? mlp_smem_bytes() : 0) +
+                        size_t(3) * r->L.sub * r->L.sub * r->L.sub * 4 + 16;
     if (smem > size_t(d->smem_optin))
         return set_err(err, errlen, "a sub-block's candidates exceed shared memory for refinement"), SMB_ERR_MEMORY;
     cudaEventRecord(b->ev[4], s);
     CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
+    if (mode == EDGE_FEATURES) CK(cudaMemsetAsync(b->e_x.p, 0, ne * 4 * 32, s));
+    CK(cudaMemsetAsync(b->counters.as<unsigned long long>() + CNT_TIMEOUT, 0, 8, s));
+    MlpDev md{nullptr, nullptr, nullptr};
+    if (mlp) md = mlp_dev(mlp);
     cudaError_t e = launch_refine(r->A, r->L, r->rc, r->keys + b->first, b->work.as<uint32_t>(), b->n_work,
                                   b->rec.as<uint32_t>(), b->ids.as<uint32_t>(), b->edge_off.as<uint32_t>(),
                                   b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->e_t.as<float>(),
-                                  b->e_feat.as<uint32_t>(), b->e_q.as<float>(), b->e_evals.as<uint32_t>(), smem, s);
+                                  b->e_feat.as<uint32_t>(), b->e_q.as<float>(), b->e_evals.as<uint32_t>(), cand, mode,
+                                  b->values.as<float>(), mode == REFINE_MLP ? &md : nullptr, b->e_x.as<float>(),
+                                  b->counters.as<unsigned long long>(), s);
     if (e != cudaSuccess) return set_err(err, errlen, "refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     cudaEventRecord(b->ev[5], s);
     CK(cudaStreamSynchronize(s));
+    unsigned long long timeouts = 0;
+    CK(cudaMemcpy(&timeouts, b->counters.as<unsigned long long>() + CNT_TIMEOUT, 8, cudaMemcpyDeviceToHost));
+    if (timeouts) return set_err(err, errlen, "tensor-core wait timed out in %llu tiles", timeouts), SMB_ERR_CUDA;
     float t = 0;
     cudaEventElapsedTime(&t, b->ev[4], b->ev[5]);
     if (ms) *ms = t;
-    b->refined = true;
+    b->refined = mode != EDGE_FEATURES;
+    return SMB_OK;
+}
+
+int smb_refine(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errlen) {
+    return refine_pass(r, b, REFINE_PLAIN, nullptr, ms, err, errlen);
+}
+
+int smb_refine_warm(smb_resident* r, smb_batch* b, const smb_mlp* mlp, double* ms, char* err, size_t errlen) {
+    if (!mlp) return refine_pass(r, b, REFINE_PLAIN, nullptr, ms, err, errlen);
+    return refine_pass(r, b, REFINE_MLP, mlp, ms, err, errlen);
+}
+
+int smb_batch_edge_features(smb_resident* r, smb_batch* b, float* features, uint8_t* covered, char* err,
+                            size_t errlen) {
+    int rc = refine_pass(r, b, EDGE_FEATURES, nullptr, nullptr, err, errlen);
+    if (rc != SMB_OK) return rc;
+    size_t ne = b->n_edges;
+    if (!ne) return SMB_OK;
+    if (features)
+        CK(cudaMemcpy(features, b->e_x.p, ne * 4 * 32, cudaMemcpyDeviceToHost));
+    if (covered) {
+        std::vector<uint32_t> ev(ne);
+        CK(cudaMemcpy(ev.data(), b->e_evals.p, ne * 4, cudaMemcpyDeviceToHost));
+        for (size_t k = 0; k < ne; k++) covered[k] = ev[k] ? 1 : 0;
+    }
     return SMB_OK;
 }
 

@@ -1,5 +1,6 @@
 // Internal state behind the opaque handles of include/sesmesh_b200.h.
 #pragma once
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <vector>
@@ -23,6 +24,18 @@ struct DBuf {
 
 int dev_alloc(void** p, size_t bytes, std::vector<void*>* owned, size_t* total, char* err, size_t errlen);
 
+// Handle lifetimes: a device stays open while residents or MLPs made on it
+// live, a resident while batches made on it live, whatever order the caller
+// frees them in (a garbage-collected host may finalize them in any order).
+void dev_retain(smb_device* d);
+void dev_release(smb_device* d);
+
+// The warm-start MLP's device parameters and device (mlp.cu).
+struct MlpDev;
+MlpDev mlp_dev(const smb_mlp* m);
+const smb_device* mlp_device(const smb_mlp* m);
+size_t mlp_smem_bytes();
+
 }  // namespace smb
 
 struct smb_device {
@@ -30,6 +43,8 @@ struct smb_device {
     cudaStream_t stream = nullptr;
     smb_device_info info{};
     size_t smem_optin = 0;
+    std::atomic<int> refs{0};
+    std::atomic<bool> closed{false}, gone{false};
 };
 
 struct smb_resident {
@@ -46,6 +61,8 @@ struct smb_resident {
     float classify_ms = 0;
     smb::RefineConsts rc{};
     bool refine_ready = false;
+    std::atomic<int> refs{0};  // batches made on this resident
+    std::atomic<bool> freed{false}, gone{false};
 };
 
 struct smb_batch {
@@ -57,12 +74,13 @@ struct smb_batch {
     smb::DBuf rec, sampled, work, retry_a, retry_b, values, tiles, totals, counters;
     smb::DBuf ids, pack, mc_counts, edge_off, tri_off, edges, edge_vals, tris;
     smb::DBuf e_t, e_feat, e_q, e_evals;  // fast-mode refinement results
+    smb::DBuf e_x;                        // warm-start features (32 f32 per edge)
     smb::GatherCaps caps{192, 128, 384, 128};
     int gather_warps = 4;
     bool use_tma = true;
     cudaEvent_t ev[6] = {};
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
-                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals};
+                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x};
     }
 };

@@ -115,6 +115,8 @@ SIGNATURES = {
     "smb_resident_set_refinement": (C.c_int, [_vp, _cp, _sz]),
     "smb_refine": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
     "smb_batch_edges": (C.c_int, [_vp, _fp, _u32p, _fp, _u32p]),
+    "smb_refine_warm": (C.c_int, [_vp, _vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
+    "smb_batch_edge_features": (C.c_int, [_vp, _vp, _fp, C.POINTER(C.c_uint8), _cp, _sz]),
     "smb_kernel_launches": (C.c_ulonglong, []),
     "smb_batch_info_get": (C.c_int, [_vp, C.POINTER(BatchInfo)]),
     "smb_batch_count_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _cp, _sz]),
@@ -137,6 +139,8 @@ SIGNATURES = {
     "smb_engine_run_device": (C.c_int, [_vp, C.POINTER(BatchTimes), _cp, _sz]),
     "smb_engine_bricks": (_sz, [_vp]),
     "smb_engine_mesh": (C.c_int, [_vp, C.POINTER(_vp), _cp, _sz]),
+    "smb_engine_set_warm_start": (C.c_int, [_vp, _vp]),
+    "smb_engine_warm_start_rows": (C.c_int, [_vp, _fp, _fp, _sz, C.POINTER(_sz), _cp, _sz]),
     "smb_surface_free": (None, [_vp]),
     "smb_surface_stats_get": (C.c_int, [_vp, C.POINTER(SurfaceStats_)]),
     "smb_surface_mesh": (C.c_int, [_vp, _fp, _fp, _u32p, _u32p, C.POINTER(C.c_uint8), _u32p]),
@@ -366,6 +370,48 @@ class Batch:
         ops, n = C.c_ulonglong(0), C.c_ulonglong(0)
         _check(lib().smb_batch_count_ops(self.h, C.byref(ops), C.byref(n), err, 1024), err)
         return ops.value, n.value
+
+    def refine(self, mlp=None):
+        """Fast-mode f32 refinement of the last run's crossing edges on the
+        device (smb_refine; smb_refine_warm with an Mlp); device ms."""
+        err = C.create_string_buffer(1024)
+        lib().smb_resident_set_refinement(self.res.h, err, 1024)
+        ms = C.c_double(0)
+        if mlp is None:
+            _check(lib().smb_refine(self.res.h, self.h, C.byref(ms), err, 1024), err)
+        else:
+            _check(lib().smb_refine_warm(self.res.h, self.h, mlp.h, C.byref(ms), err, 1024), err)
+        return ms.value
+
+    def edges(self):
+        """Per crossing edge: t, feature, closest point, evaluations (bit 31:
+        converged) of the last refinement."""
+        ne, nt = _sz(0), _sz(0)
+        lib().smb_batch_mc_counts(self.h, C.byref(ne), C.byref(nt))
+        n = max(ne.value, 1)
+        t = np.zeros(n, np.float32)
+        feat = np.zeros(n, np.uint32)
+        q = np.zeros((n, 3), np.float32)
+        ev = np.zeros(n, np.uint32)
+        rc = lib().smb_batch_edges(self.h, _p(t, C.c_float), _p(feat, C.c_uint32), _p(q, C.c_float),
+                                   _p(ev, C.c_uint32))
+        if rc != SMB_OK:
+            raise SmbError(rc, "smb_batch_edges")
+        k = ne.value
+        return t[:k], feat[:k], q[:k], ev[:k]
+
+    def edge_features(self):
+        """Warm-start features (n_edges, 32) and the covered mask."""
+        ne, nt = _sz(0), _sz(0)
+        lib().smb_batch_mc_counts(self.h, C.byref(ne), C.byref(nt))
+        n = max(ne.value, 1)
+        x = np.zeros((n, MLP_FEATURES), np.float32)
+        cov = np.zeros(n, np.uint8)
+        err = C.create_string_buffer(1024)
+        lib().smb_resident_set_refinement(self.res.h, err, 1024)
+        _check(lib().smb_batch_edge_features(self.res.h, self.h, _p(x, C.c_float), _p(cov, C.c_uint8), err, 1024),
+               err)
+        return x[:ne.value], cov[:ne.value].astype(bool)
 
     def mc(self):
         ne, nt = _sz(0), _sz(0)

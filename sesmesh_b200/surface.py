@@ -176,7 +176,26 @@ class SurfaceEngine:
         _check(lib().smb_engine_mesh(self.h, C.byref(h), err, 1024), err)
         return SurfaceOutput(h)
 
+    def set_warm_start(self, mlp):
+        """Start fast-mode refinement from `mlp` (a native.Mlp on this
+        engine's device; None: the linear guess)."""
+        self.warm = mlp  # kept alive while the engine uses it
+        lib().smb_engine_set_warm_start(self.h, mlp.h if mlp is not None else None)
+
+    def warm_start_rows(self):
+        """(features (n, 32), exact root parameters (n,)) for every edge the
+        device refines, from a fresh device run."""
+        err = C.create_string_buffer(1024)
+        n = C.c_size_t(0)
+        _check(lib().smb_engine_warm_start_rows(self.h, None, None, 0, C.byref(n), err, 1024), err)
+        x = np.zeros((max(n.value, 1), native.MLP_FEATURES), np.float32)
+        t = np.zeros(max(n.value, 1), np.float32)
+        _check(lib().smb_engine_warm_start_rows(self.h, _p(x, C.c_float), _p(t, C.c_float), len(t), C.byref(n), err,
+                                                1024), err)
+        return x[:n.value], t[:n.value]
+
     def close(self):
+        self.warm = None
         if getattr(self, "h", None):
             lib().smb_engine_free(self.h)
             self.h = None
