@@ -10,6 +10,8 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include <cstddef>
+
 #include "kernels.hpp"
 #include "mlp.cuh"
 #include "scan.cuh"
@@ -884,12 +886,16 @@ __device__ __forceinline__ float contact_iteration(float ax, float ay, float az,
     return t;
 }
 
+// Sphere candidates scanned for the features: the first of the sub-block's
+// S list, which is sorted by the candidate's value at the sub-block centre.
+constexpr int FEATURE_SCAN = 32;
+
 // Features of one crossing edge for the warm-start MLP (32 values):
 //   0-1   fa / h, fb / h (sample values at the ends)
 //   2-7   finite-difference gradients of the sampled field at both ends
 //         (central where both neighbours are in the brick, else one-sided)
-//   8-23  the 4 class-S candidates whose contact spheres (radius
-//         r = R - probe) best explain the two end samples (smallest
+//   8-23  the 4 class-S candidates (of the first FEATURE_SCAN) whose contact
+//         spheres (radius r = R - probe) best explain the two end samples (smallest
 //         mismatch max(| |a - c| - r - fa |, | |b - c| - r - fb |)):
 //         centre minus edge midpoint / 4 A, and r / 4 A (zeros when fewer)
 //   24-25 the mismatch of the first two, log10(max(m, 1e-9)) / 9 + 1
@@ -924,7 +930,7 @@ __device__ __forceinline__ float edge_features(const float* val, int b, float h,
     const float bx = ax + (axis == 0 ? hd : 0.0f), by = ay + (axis == 1 ? hd : 0.0f), bz = az + (axis == 2 ? hd : 0.0f);
     float bd[4] = {3.4e38f, 3.4e38f, 3.4e38f, 3.4e38f};
     int bi[4] = {-1, -1, -1, -1};
-    for (int i = 0; i < ns; i++) {
+    for (int i = 0; i < min(ns, FEATURE_SCAN); i++) {
         float4 c = S[i];
         const float r = c.w - probe;
         float dx = ax - c.x, dy = ay - c.y, dz = az - c.z;
@@ -963,19 +969,87 @@ __device__ __forceinline__ float edge_features(const float* val, int b, float h,
     return t_c;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC, const int4* keys, const uint32_t* work,
-                                                uint32_t n_work, const uint32_t* rec, const uint32_t* ids,
-                                                const uint32_t* edge_off, const uint32_t* edges,
-                                                const float2* edge_vals, RefOut out, const float* values, MlpDev mlp,
-                                                float* feat_out, uint32_t mlp_off, uint32_t list_off,
-                                                unsigned long long* counters) {
-    extern __shared__ __align__(128) float4 rs[];
-    __shared__ uint32_t ecount;
-    const uint32_t j = work[blockIdx.x];
-    const uint32_t brick = j >> 3, sb = j & 7;
+// Sub-block edge lists for refinement: per work item (a sampled sub-block
+// without flags), its brick's crossing edges whose lower sample lies in the
+// sub-block, in the brick's (ascending) order.  Warp per item; FILL = false
+// counts (and records the largest count), FILL = true writes at item_off[i]
+// and the list's tail item_off[n] = *total.
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_item_edges(const DLat L, const uint32_t* work, uint32_t n,
+                                                    const uint32_t* rec, const uint32_t* edge_off,
+                                                    const uint32_t* edges, uint32_t* counts, uint32_t* item_off,
+                                                    uint32_t* item_edges, const unsigned long long* total,
+                                                    unsigned long long* counters) {
+    const uint32_t lane = threadIdx.x & 31, i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (FILL && blockIdx.x == 0 && threadIdx.x == 0) item_off[n] = uint32_t(*total);
+    if (i >= n) return;
+    const uint32_t j = work[i], brick = j >> 3, sb = j & 7;
     const uint32_t* R = rec + size_t(j) * REC_WORDS;
-    if (R[R_STATE] != ST_SAMPLE || R[R_FLAGS] != 0) return;
+    if (R[R_STATE] != ST_SAMPLE || R[R_FLAGS] != 0) {
+        if (!FILL && lane == 0) counts[i] = 0;
+        return;
+    }
+    const int b = L.b, sub = L.sub;
+    const uint32_t e0 = edge_off[brick], e1 = edge_off[brick + 1];
+    uint32_t at = FILL ? item_off[i] : 0u;
+    for (uint32_t base = e0; base < e1; base += 32) {
+        const uint32_t k = base + lane;
+        bool mine = false;
+        if (k < e1) {
+            const uint32_t cell = edges[k] / 3;
+            const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
+            mine = uint32_t(min(ex / sub, 1) + 2 * min(ey / sub, 1) + 4 * min(ez / sub, 1)) == sb;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, mine);
+        if (FILL && mine) item_edges[at + __popc(m & ((1u << lane) - 1u))] = k;
+        at += __popc(m);
+    }
+    if (!FILL && lane == 0) {
+        counts[i] = at;
+        atomicMax(reinterpret_cast<unsigned int*>(&counters[CNT_MAXITEM]), at);
+    }
+}
+
+// Brick-local frame of one brick: the origin (key * b - frame) * h as an f32
+// pair, and the f64 -> brick-local f32 transform of the refinement.
+struct BrickFrame {
+    float ohx, olx, ohy, oly, ohz, olz;
+};
+
+__device__ __forceinline__ BrickFrame brick_frame(const DLat& L, const RefineConsts& RC, int4 key) {
+    BrickFrame F;
+    origin_pair((long long)key.x * L.b - L.frame[0], RC.h_hi, RC.h_lo, F.ohx, F.olx);
+    origin_pair((long long)key.y * L.b - L.frame[1], RC.h_hi, RC.h_lo, F.ohy, F.oly);
+    origin_pair((long long)key.z * L.b - L.frame[2], RC.h_hi, RC.h_lo, F.ohz, F.olz);
+    return F;
+}
+
+__device__ __forceinline__ void to_local(const DLat& L, const BrickFrame& F, double x, double y, double z, float& lx,
+                                         float& ly, float& lz) {
+    float hx, lo_x, hy, lo_y, hz, lo_z;
+    split_df(x - L.fx, hx, lo_x);
+    split_df(y - L.fy, hy, lo_y);
+    split_df(z - L.fz, hz, lo_z);
+    lx = (hx - F.ohx) + (lo_x - F.olx);
+    ly = (hy - F.ohy) + (lo_y - F.oly);
+    lz = (hz - F.ohz) + (lo_z - F.olz);
+}
+
+// One sub-block's candidates staged in shared memory, brick-local f32:
+// near (x, y, z, R) and (x, y, z, (R - tol)^2), S (x, y, z, R), C 3 x float4,
+// V (x, y, z, id); then S ids, s_off, s_blk, c_off, c_blk words.
+struct RefStage {
+    const float4 *nearA, *nearT, *S, *C, *V;
+    const uint32_t *s_id, *s_off, *s_blk, *c_off, *c_blk;
+    int n_in, ns, nc, nv;
+};
+
+// One warp (BLOCK = false) or the whole block: stages work item j's
+// candidates at `base` and returns the view (ends with a warp / block barrier).
+template <bool BLOCK>
+__device__ RefStage stage_candidates(const DArr& A, const DLat& L, const BrickFrame& F, const uint32_t* R,
+                                     const uint32_t* ids, unsigned char* base) {
+    const int lane = BLOCK ? int(threadIdx.x) : int(threadIdx.x & 31), step = BLOCK ? int(blockDim.x) : 32;
     const int nn = int(R[R_NEAR]), n_in = int(R[R_INSIDE]), ns = int(R[R_S]), nc = int(R[R_C]), nv = int(R[R_V]);
     const int nsb = int(R[R_SBLK]), ncb = int(R[R_CBLK]);
     const uint32_t* l_near = ids + R[R_IDS];
@@ -986,10 +1060,7 @@ __global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC,
     const uint32_t* l_coff = l_c + nc;
     const uint32_t* l_cblk = l_coff + nc + 1;
     const uint32_t* l_v = l_cblk + ncb;
-    // Shared layout: near (x, y, z, R) and (x, y, z, (R - tol)^2), S
-    // (x, y, z, R), C 3 x float4, V (x, y, z, id), all brick-local; then
-    // S ids, s_off, s_blk, c_off, c_blk words.
-    float4* nearA = rs;
+    float4* nearA = reinterpret_cast<float4*>(base);
     float4* nearT = nearA + nn;
     float4* S = nearT + nn;
     float4* C = S + ns;
@@ -999,36 +1070,21 @@ __global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC,
     uint32_t* s_blk = s_off + ns + 1;
     uint32_t* c_off = s_blk + nsb;
     uint32_t* c_blk = c_off + nc + 1;
-    const int4 key = keys[brick];
-    const long long ox = (long long)key.x * L.b - L.frame[0], oy = (long long)key.y * L.b - L.frame[1],
-                    oz = (long long)key.z * L.b - L.frame[2];
-    float ohx, olx, ohy, oly, ohz, olz;
-    origin_pair(ox, RC.h_hi, RC.h_lo, ohx, olx);
-    origin_pair(oy, RC.h_hi, RC.h_lo, ohy, oly);
-    origin_pair(oz, RC.h_hi, RC.h_lo, ohz, olz);
-    auto local3 = [&](double x, double y, double z, float& lx, float& ly, float& lz) {
-        float hx, lo_x, hy, lo_y, hz, lo_z;
-        split_df(x - L.fx, hx, lo_x);
-        split_df(y - L.fy, hy, lo_y);
-        split_df(z - L.fz, hz, lo_z);
-        lx = (hx - ohx) + (lo_x - olx);
-        ly = (hy - ohy) + (lo_y - oly);
-        lz = (hz - ohz) + (lo_z - olz);
-    };
-    for (int i = threadIdx.x; i < nn; i += blockDim.x) {
+    for (int i = lane; i < nn; i += step) {
         double4 c = A.sph[l_near[i]];
         float x, y, z;
-        local3(c.x, c.y, c.z, x, y, z);
+        to_local(L, F, c.x, c.y, c.z, x, y, z);
         float r32 = float(c.w), rt = fmaxf(r32 - INSIDE_TOL, 0.0f);
         nearA[i] = make_float4(x, y, z, r32);
         nearT[i] = make_float4(x, y, z, rt * rt);
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i <= ns; i += blockDim.x) s_off[i] = l_soff[i];
-    for (int i = threadIdx.x; i < nsb; i += blockDim.x) s_blk[i] = l_sblk[i];
-    for (int i = threadIdx.x; i <= nc; i += blockDim.x) c_off[i] = l_coff[i];
-    for (int i = threadIdx.x; i < ncb; i += blockDim.x) c_blk[i] = l_cblk[i];
-    for (int i = threadIdx.x; i < ns; i += blockDim.x) {
+    if (BLOCK) __syncthreads();
+    else __syncwarp();
+    for (int i = lane; i <= ns; i += step) s_off[i] = l_soff[i];
+    for (int i = lane; i < nsb; i += step) s_blk[i] = l_sblk[i];
+    for (int i = lane; i <= nc; i += step) c_off[i] = l_coff[i];
+    for (int i = lane; i < ncb; i += step) c_blk[i] = l_cblk[i];
+    for (int i = lane; i < ns; i += step) {
         // S candidates are near spheres: find the position (lists are short).
         uint32_t k = l_s[i];
         int pos = 0;
@@ -1040,211 +1096,347 @@ __global__ void __launch_bounds__(128) k_refine(DArr A, DLat L, RefineConsts RC,
         S[i] = nearA[pos];
         s_id[i] = k;
     }
-    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+    for (int i = lane; i < nc; i += step) {
         const double* c = A.circ + 12 * size_t(l_c[i]);
         float x, y, z;
-        local3(c[0], c[1], c[2], x, y, z);
+        to_local(L, F, c[0], c[1], c[2], x, y, z);
         C[3 * i] = make_float4(x, y, z, float(c[9]));
         C[3 * i + 1] = make_float4(float(c[3]), float(c[4]), float(c[5]), float(c[6]));
         C[3 * i + 2] = make_float4(float(c[7]), float(c[8]), __int_as_float(int(l_c[i])), 0.0f);
     }
-    for (int i = threadIdx.x; i < nv; i += blockDim.x) {
+    for (int i = lane; i < nv; i += step) {
         double4 p = A.vert[l_v[i]];
         float x, y, z;
-        local3(p.x, p.y, p.z, x, y, z);
+        to_local(L, F, p.x, p.y, p.z, x, y, z);
         V[i] = make_float4(x, y, z, __int_as_float(int(l_v[i])));
     }
-    __syncthreads();
-    const float probe = L.probe32, band = L.band32, h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
-    const int b = L.b, sub = L.sub;
-    struct Eval {
-        float value, qx, qy, qz;
-        uint32_t feat;
-    };
-    // eval_local in f32, brick-local (sesmesh.cuh eval_point semantics).
-    auto eval = [&](float x, float y, float z) {
-        Eval e;
-        e.qx = x, e.qy = y, e.qz = z;
-        bool inside = false;
-        for (int k = 0; k < n_in && !inside; k++) {
-            float4 a = nearA[k];
-            float dx = x - a.x, dy = y - a.y, dz = z - a.z;
-            inside = sqrtf(dx * dx + dy * dy + dz * dz) < a.w;
-        }
-        if (!inside) {
-            e.value = probe;
-            e.feat = 0u << FEAT_SHIFT_D;
-            return e;
-        }
-        float best = probe + band;
-        e.feat = 1u << FEAT_SHIFT_D;
-        for (int i = 0; i < ns; i++) {
-            float4 c = S[i];
-            const uint32_t k = s_id[i];
-            const float cx = c.x, cy = c.y, cz = c.z, rr = c.w;
-            float dx = x - cx, dy = y - cy, dz = z - cz;
-            float len = sqrtf(dx * dx + dy * dy + dz * dz);
-            float lb = fabsf(len - rr);
-            if (lb >= best || len < 1e-12f) continue;
-            float sc = rr / len;
-            float qx = cx + dx * sc, qy = cy + dy * sc, qz = cz + dz * sc;
-            bool free = true;
-            for (uint32_t p = s_off[i], e2 = s_off[i + 1]; p < e2 && free; p++) {
-                float4 t = nearT[s_blk[p]];
-                float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
-                free = ex * ex + ey * ey + ez * ez >= t.w;
-            }
-            if (free) best = lb, e.feat = (2u << FEAT_SHIFT_D) | k, e.qx = qx, e.qy = qy, e.qz = qz;
-        }
-        for (int i = 0; i < nc; i++) {
-            float4 m = C[3 * i], u = C[3 * i + 1], w2 = C[3 * i + 2];
-            float yx = x - m.x, yy = y - m.y, yz = z - m.z;
-            float along = yx * u.x + yy * u.y + yz * u.z;
-            float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
-            float wl = sqrtf(wx * wx + wy * wy + wz * wz);
-            float tt = wl - m.w;
-            float dist = sqrtf(along * along + tt * tt);
-            if (dist >= best) continue;
-            float qx, qy, qz;
-            if (wl > 1e-12f) {
-                qx = m.x + (wx / wl) * m.w, qy = m.y + (wy / wl) * m.w, qz = m.z + (wz / wl) * m.w;
-            } else {
-                qx = m.x + u.w * m.w, qy = m.y + w2.x * m.w, qz = m.z + w2.y * m.w;
-            }
-            bool free = true;
-            for (uint32_t p = c_off[i], e2 = c_off[i + 1]; p < e2 && free; p++) {
-                float4 t = nearT[c_blk[p]];
-                float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
-                free = ex * ex + ey * ey + ez * ez >= t.w;
-            }
-            if (free)
-                best = dist, e.feat = (3u << FEAT_SHIFT_D) | uint32_t(__float_as_int(w2.z)), e.qx = qx, e.qy = qy, e.qz = qz;
-        }
-        for (int i = 0; i < nv; i++) {
-            float4 p = V[i];
-            float dx = x - p.x, dy = y - p.y, dz = z - p.z;
-            float d = sqrtf(dx * dx + dy * dy + dz * dz);
-            if (d < best) best = d, e.feat = (4u << FEAT_SHIFT_D) | uint32_t(__float_as_int(p.w)), e.qx = p.x, e.qy = p.y, e.qz = p.z;
-        }
-        e.value = probe - best;
-        return e;
-    };
-    // This sub-block's crossing edges (lower sample in it); outputs go to
-    // each edge's own index, so the order of the list does not matter.
-    const uint32_t e0 = edge_off[brick], e1 = edge_off[brick + 1];
-    uint32_t* elist = reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(rs) + list_off);
-    if (threadIdx.x == 0) ecount = 0;
-    __syncthreads();
-    for (uint32_t k = e0 + threadIdx.x; k < e1; k += blockDim.x) {
-        const uint32_t cell = edges[k] / 3;
-        const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
-        if (min(ex / sub, 1) + 2 * min(ey / sub, 1) + 4 * min(ez / sub, 1) == int(sb)) elist[atomicAdd(&ecount, 1u)] = k;
+    if (BLOCK) __syncthreads();
+    else __syncwarp();
+    return RefStage{nearA, nearT, S, C, V, s_id, s_off, s_blk, c_off, c_blk, n_in, ns, nc, nv};
+}
+
+struct Eval {
+    float value, qx, qy, qz;
+    uint32_t feat;
+};
+
+// eval_local in f32, brick-local (sesmesh.cuh eval_point semantics).
+__device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float band, float x, float y, float z) {
+    Eval e;
+    e.qx = x, e.qy = y, e.qz = z;
+    bool inside = false;
+    for (int k = 0; k < st.n_in && !inside; k++) {
+        float4 a = st.nearA[k];
+        float dx = x - a.x, dy = y - a.y, dz = z - a.z;
+        inside = sqrtf(dx * dx + dy * dy + dz * dz) < a.w;
     }
-    __syncthreads();
-    const uint32_t ne = ecount;
-    MlpSmem* M = reinterpret_cast<MlpSmem*>(reinterpret_cast<unsigned char*>(rs) + mlp_off);
-    if (MODE == REFINE_MLP) mlp_setup(*M, mlp, 64);
-    uint32_t phase = 0;
-    const float* val = values + size_t(brick) * L.spb;
-    for (uint32_t c0 = 0; c0 < ne; c0 += blockDim.x) {
-        const uint32_t idx = c0 + threadIdx.x;
-        const bool have = idx < ne;
-        const uint32_t k = have ? elist[idx] : 0u;
-        const uint32_t code = have ? edges[k] : 0u;
-        const uint32_t cell = code / 3, axis = code % 3;
-        const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
-        const float2 fv = have ? edge_vals[k] : make_float2(-1.0f, 1.0f);
-        const float fa = fv.x, fb = fv.y;
-        float t_start = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
-        if (MODE != REFINE_PLAIN) {
-            float f[MLP_IN];
-            float t_contact = t_start;
-            if (have) {
-                const float ax = float(ex) * h + float(ex) * RC.h_lo, ay = float(ey) * h + float(ey) * RC.h_lo,
-                            az = float(ez) * h + float(ez) * RC.h_lo;
-                t_contact = edge_features(val, b, h, hd, probe, ex, ey, ez, ax, ay, az, int(axis), fa, fb, S, ns, RC, f);
-            } else {
-                for (int q = 0; q < MLP_IN; q++) f[q] = 0.0f;
-            }
-            if (MODE == EDGE_FEATURES) {
-                if (have) {
-                    for (int q = 0; q < MLP_IN; q++) feat_out[size_t(k) * MLP_IN + q] = f[q];
-                    out.evals[k] = 1;
-                }
-                continue;
-            }
-            mlp_put_row(*M, f);
-            float tm;
-            // The MLP chooses the start: the contact iteration's result
-            // where it answers >= 0.5 (and that is within half an edge of the
-            // linear guess), else the linear guess.
-            if (mlp_forward(*M, phase, &tm, nullptr, nullptr, nullptr, 0)) {
-                if (tm >= 0.5f && fabsf(f[26]) < 4.0f) t_start = t_contact;
-            } else if (threadIdx.x == 0) {
-                atomicAdd(&counters[CNT_TIMEOUT], 1ull);
-            }
+    if (!inside) {
+        e.value = probe;
+        e.feat = 0u << FEAT_SHIFT_D;
+        return e;
+    }
+    float best = probe + band;
+    e.feat = 1u << FEAT_SHIFT_D;
+    for (int i = 0; i < st.ns; i++) {
+        float4 c = st.S[i];
+        const uint32_t k = st.s_id[i];
+        const float cx = c.x, cy = c.y, cz = c.z, rr = c.w;
+        float dx = x - cx, dy = y - cy, dz = z - cz;
+        float len = sqrtf(dx * dx + dy * dy + dz * dz);
+        float lb = fabsf(len - rr);
+        if (lb >= best || len < 1e-12f) continue;
+        float sc = rr / len;
+        float qx = cx + dx * sc, qy = cy + dy * sc, qz = cz + dz * sc;
+        bool free = true;
+        for (uint32_t p = st.s_off[i], e2 = st.s_off[i + 1]; p < e2 && free; p++) {
+            float4 t = st.nearT[st.s_blk[p]];
+            float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
+            free = ex * ex + ey * ey + ez * ez >= t.w;
         }
-        if (!have) continue;
-        const float ax = float(ex) * h + float(ex) * RC.h_lo, ay = float(ey) * h + float(ey) * RC.h_lo,
-                    az = float(ez) * h + float(ez) * RC.h_lo;
-        float t = t_start;
-        float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
-        int side_ = 0;
-        bool converged = false;
-        uint32_t evals = 0;
-        Eval last;
-        last.feat = 1u << FEAT_SHIFT_D, last.qx = last.qy = last.qz = 0.0f, last.value = 0.0f;
-        for (uint32_t it = 0; it < RC.max_iter; it++) {
+        if (free) best = lb, e.feat = (2u << FEAT_SHIFT_D) | k, e.qx = qx, e.qy = qy, e.qz = qz;
+    }
+    for (int i = 0; i < st.nc; i++) {
+        float4 m = st.C[3 * i], u = st.C[3 * i + 1], w2 = st.C[3 * i + 2];
+        float yx = x - m.x, yy = y - m.y, yz = z - m.z;
+        float along = yx * u.x + yy * u.y + yz * u.z;
+        float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
+        float wl = sqrtf(wx * wx + wy * wy + wz * wz);
+        float tt = wl - m.w;
+        float dist = sqrtf(along * along + tt * tt);
+        if (dist >= best) continue;
+        float qx, qy, qz;
+        if (wl > 1e-12f) {
+            qx = m.x + (wx / wl) * m.w, qy = m.y + (wy / wl) * m.w, qz = m.z + (wz / wl) * m.w;
+        } else {
+            qx = m.x + u.w * m.w, qy = m.y + w2.x * m.w, qz = m.z + w2.y * m.w;
+        }
+        bool free = true;
+        for (uint32_t p = st.c_off[i], e2 = st.c_off[i + 1]; p < e2 && free; p++) {
+            float4 t = st.nearT[st.c_blk[p]];
+            float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
+            free = ex * ex + ey * ey + ez * ez >= t.w;
+        }
+        if (free)
+            best = dist, e.feat = (3u << FEAT_SHIFT_D) | uint32_t(__float_as_int(w2.z)), e.qx = qx, e.qy = qy, e.qz = qz;
+    }
+    for (int i = 0; i < st.nv; i++) {
+        float4 p = st.V[i];
+        float dx = x - p.x, dy = y - p.y, dz = z - p.z;
+        float d = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (d < best) best = d, e.feat = (4u << FEAT_SHIFT_D) | uint32_t(__float_as_int(p.w)), e.qx = p.x, e.qy = p.y, e.qz = p.z;
+    }
+    e.value = probe - best;
+    return e;
+}
+
+// The f32 root search of one crossing edge (extract.rs:425-535 iteration:
+// Newton with the Illinois bracket for MAX_ITER evaluations, then
+// bisection), from t_start; writes edge k's outputs.
+__device__ __forceinline__ void refine_edge_f32(const RefStage& st, const RefineConsts& RC, float probe, float band,
+                                                float ax, float ay, float az, uint32_t axis, float fa, float fb,
+                                                float t_start, uint32_t k, const RefOut& out) {
+    const float h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
+    float t = t_start;
+    float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
+    int side_ = 0;
+    bool converged = false;
+    uint32_t evals = 0;
+    Eval last;
+    last.feat = 1u << FEAT_SHIFT_D, last.qx = last.qy = last.qz = 0.0f, last.value = 0.0f;
+    for (uint32_t it = 0; it < RC.max_iter; it++) {
+        float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
+        Eval e = eval_f32(st, probe, band, x, y, z);
+        evals++;
+        last = e;
+        float gv = e.value;
+        if (fabsf(gv) <= RC.tol) {
+            converged = true;
+            break;
+        }
+        if ((gv < 0.0f) == (g0 < 0.0f)) {
+            t0 = t, g0 = gv;
+            if (side_ == -1) g1 *= 0.5f;
+            side_ = -1;
+        } else {
+            t1 = t, g1 = gv;
+            if (side_ == 1) g0 *= 0.5f;
+            side_ = 1;
+        }
+        float slope = 0.0f;
+        uint32_t kind = e.feat >> FEAT_SHIFT_D;
+        if (kind != 0 && kind != 1) {
+            float wx = e.qx - x, wy = e.qy - y, wz = e.qz - z;
+            float len = sqrtf(wx * wx + wy * wy + wz * wz);
+            if (len > 1e-12f) slope = ((axis == 0 ? wx : (axis == 1 ? wy : wz)) / len) * h;
+        }
+        float newton = t - gv / slope;
+        if (fabsf(slope) > 1e-3f * hd && newton > t0 && newton < t1) {
+            t = newton;
+        } else {
+            float s = (t0 * g1 - t1 * g0) / (g1 - g0);
+            t = (isfinite(s) && s > t0 && s < t1) ? s : 0.5f * (t0 + t1);
+        }
+    }
+    if (!converged) {
+        bool neg0 = g0 < 0.0f;
+        for (uint32_t it = 0; it < RC.max_bisect; it++) {
+            t = 0.5f * (t0 + t1);
             float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
-            Eval e = eval(x, y, z);
+            Eval e = eval_f32(st, probe, band, x, y, z);
             evals++;
             last = e;
-            float gv = e.value;
-            if (fabsf(gv) <= RC.tol) {
-                converged = true;
-                break;
+            if (fabsf(e.value) <= RC.tol || (t1 - t0) * hd <= 2.0f * RC.tol) break;
+            if ((e.value < 0.0f) == neg0) t0 = t;
+            else t1 = t;
+        }
+    }
+    out.t[k] = t;
+    out.feat[k] = last.feat;
+    out.q[3 * size_t(k)] = last.qx, out.q[3 * size_t(k) + 1] = last.qy, out.q[3 * size_t(k) + 2] = last.qz;
+    out.evals[k] = evals | (converged ? 0x80000000u : 0u);
+}
+
+// Fast-mode refinement over the work items' edge lists (k_item_edges).
+// Work is claimed from a queue (counters[CNT_QUEUE]) by persistent CTAs:
+//   REFINE_PLAIN:  each warp claims items and refines the item's edges from
+//                  the linear guess (the reference's fast mode), lane per
+//                  edge, candidates staged in the warp's shared region;
+//   REFINE_MLP:    each CTA claims REFINE_BATCH quads of REFINE_WARPS items.
+//                  Phase A: the batch's edges, packed densely in 128-row
+//                  tiles (thread r holds row r), get their features and one
+//                  tensor-core MLP pass per tile gives each its start.
+//                  Phase B: the warps refine the batch's items as PLAIN from
+//                  those starts.  Weights and TMEM are set up once per CTA;
+//                  the tiles share bytes with the candidate staging;
+//   EDGE_FEATURES: the features alone, to feat_out (evals[k] = 1 marks the
+//                  edges covered).
+// WIDE: candidates too large for a region per warp; the CTA refines one
+// item at a time with all its threads.
+constexpr int REFINE_WARPS = 4;
+// Most quads a CTA claims at once: phase A for all of them, then phase B
+// with the warps claiming the batch's items one by one (a barrier per batch,
+// not per quad, so warps with quick items do not wait for slow ones).  Small
+// runs claim fewer, so that every CTA gets several claims.
+constexpr uint32_t REFINE_BATCH = 8;
+
+struct RefinePlan {
+    uint32_t batch;       // quads per claim, 1..REFINE_BATCH
+    uint32_t cand_bytes;  // one staging region
+    uint32_t stage_off;   // first staging region (after the MLP's weights)
+    uint32_t first_off;   // phase A: first S candidates, REFINE_WARPS x REFINE_BATCH x FEATURE_SCAN float4
+};
+
+template <int MODE, bool WIDE>
+__global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
+    DArr A, DLat L, RefineConsts RC, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
+    const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
+    uint32_t n_items, RefOut out, const float* values, MlpDev mlp, float* feat_out, RefinePlan P,
+    unsigned long long* counters) {
+    extern __shared__ __align__(128) float4 rs[];
+    __shared__ uint32_t sh_q, sh_next;
+    __shared__ uint32_t sh_off[REFINE_WARPS * REFINE_BATCH + 1], sh_sbase[REFINE_WARPS * REFINE_BATCH],
+        sh_brick[REFINE_WARPS * REFINE_BATCH];
+    __shared__ int sh_ns[REFINE_WARPS * REFINE_BATCH];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* smem = reinterpret_cast<unsigned char*>(rs);
+    MlpSmem* M = reinterpret_cast<MlpSmem*>(smem);
+    float4* first_s = reinterpret_cast<float4*>(smem + P.first_off);  // per batch item, FEATURE_SCAN each
+    unsigned char* mine = smem + P.stage_off + (WIDE ? 0 : size_t(warp) * P.cand_bytes);
+    unsigned int* queue = reinterpret_cast<unsigned int*>(&counters[CNT_QUEUE]);
+    const float probe = L.probe32, band = L.band32, h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
+    const int b = L.b;
+    const uint32_t n_quads = (n_items + REFINE_WARPS - 1) / REFINE_WARPS;
+    auto edge_geom = [&](uint32_t k, uint32_t& axis, int& ex, int& ey, int& ez, float& ax, float& ay, float& az) {
+        const uint32_t code = edges[k], cell = code / 3;
+        axis = code % 3;
+        ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
+        ax = float(ex) * h + float(ex) * RC.h_lo, ay = float(ey) * h + float(ey) * RC.h_lo,
+        az = float(ez) * h + float(ez) * RC.h_lo;
+    };
+    // Refines item i's edges with the lanes of one warp (WIDE: the block).
+    auto refine_item = [&](uint32_t i) {
+        const uint32_t a0 = item_off[i], a1 = item_off[i + 1];
+        if (a0 == a1) return;
+        const uint32_t j = work[i], brick = j >> 3;
+        const BrickFrame F = brick_frame(L, RC, keys[brick]);
+        const uint32_t* R = rec + size_t(j) * REC_WORDS;
+        if (WIDE) __syncthreads();
+        else __syncwarp();
+        const RefStage st = WIDE ? stage_candidates<true>(A, L, F, R, ids, mine)
+                                 : stage_candidates<false>(A, L, F, R, ids, mine);
+        const uint32_t step = WIDE ? blockDim.x : 32u;
+        for (uint32_t e = a0 + (WIDE ? threadIdx.x : lane); e < a1; e += step) {
+            const uint32_t k = item_edges[e];
+            uint32_t axis;
+            int ex, ey, ez;
+            float ax, ay, az;
+            edge_geom(k, axis, ex, ey, ez, ax, ay, az);
+            const float2 fv = edge_vals[k];
+            const float t0 = MODE == REFINE_MLP ? out.t[k] : fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
+            refine_edge_f32(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, k, out);
+        }
+    };
+    if constexpr (MODE == REFINE_PLAIN && !WIDE) {
+        for (;;) {
+            uint32_t i = 0;
+            if (lane == 0) i = atomicAdd(queue, 1u);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= n_items) break;
+            refine_item(i);
+        }
+        return;
+    }
+    if (MODE == REFINE_MLP) mlp_setup(*M, mlp, 64);
+    uint32_t phase = 0;
+    for (;;) {
+        __syncthreads();  // sh_q, sh_next and the shared regions are free again
+        if (threadIdx.x == 0) sh_q = atomicAdd(queue, P.batch), sh_next = 0;
+        __syncthreads();
+        const uint32_t q0 = sh_q;
+        if (q0 >= n_quads) break;
+        const uint32_t q1 = min(q0 + P.batch, n_quads);
+        // Phase A: the batch's edges, densely packed in 128-row tiles,
+        // through the features and the MLP.  First each item's first S
+        // candidates, frame and offsets into shared memory.
+        const uint32_t i0 = q0 * REFINE_WARPS, i1 = min(q1 * REFINE_WARPS, n_items), ni = i1 - i0;
+        if (MODE != REFINE_PLAIN) {
+            if (threadIdx.x <= ni) sh_off[threadIdx.x] = item_off[i0 + threadIdx.x];
+            if (threadIdx.x < ni) {
+                const uint32_t j = work[i0 + threadIdx.x];
+                const uint32_t* R = rec + size_t(j) * REC_WORDS;
+                sh_ns[threadIdx.x] = min(int(R[R_S]), FEATURE_SCAN);
+                sh_sbase[threadIdx.x] = R[R_IDS] + R[R_NEAR];
+                sh_brick[threadIdx.x] = j >> 3;
             }
-            if ((gv < 0.0f) == (g0 < 0.0f)) {
-                t0 = t, g0 = gv;
-                if (side_ == -1) g1 *= 0.5f;
-                side_ = -1;
-            } else {
-                t1 = t, g1 = gv;
-                if (side_ == 1) g0 *= 0.5f;
-                side_ = 1;
+            __syncthreads();
+            for (uint32_t x = threadIdx.x; x < ni * FEATURE_SCAN; x += blockDim.x) {
+                const uint32_t it = x / FEATURE_SCAN, c = x % FEATURE_SCAN;
+                if (int(c) >= sh_ns[it] || sh_off[it] == sh_off[it + 1]) continue;
+                const BrickFrame F = brick_frame(L, RC, keys[sh_brick[it]]);
+                double4 sp = A.sph[ids[sh_sbase[it] + c]];
+                float lx, ly, lz;
+                to_local(L, F, sp.x, sp.y, sp.z, lx, ly, lz);
+                first_s[x] = make_float4(lx, ly, lz, float(sp.w));
             }
-            float slope = 0.0f;
-            uint32_t kind = e.feat >> FEAT_SHIFT_D;
-            if (kind != 0 && kind != 1) {
-                float wx = e.qx - x, wy = e.qy - y, wz = e.qz - z;
-                float len = sqrtf(wx * wx + wy * wy + wz * wz);
-                if (len > 1e-12f) slope = ((axis == 0 ? wx : (axis == 1 ? wy : wz)) / len) * h;
+            __syncthreads();
+            const uint32_t E0 = sh_off[0], E1 = sh_off[ni];
+            for (uint32_t c0 = E0; c0 < E1; c0 += blockDim.x) {
+                const uint32_t e = c0 + threadIdx.x;
+                const bool have = e < E1;
+                float f[MLP_IN];
+                for (int c = 0; c < MLP_IN; c++) f[c] = 0.0f;
+                float t_c = 0.0f, t_lin = 0.0f;
+                uint32_t k = 0;
+                if (have) {
+                    uint32_t lo = 0, hi = ni;  // the item holding edge e: sh_off[lo] <= e < sh_off[lo + 1]
+                    while (hi - lo > 1) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (sh_off[mid] <= e) lo = mid;
+                        else hi = mid;
+                    }
+                    k = item_edges[e];
+                    uint32_t axis;
+                    int ex, ey, ez;
+                    float ax, ay, az;
+                    edge_geom(k, axis, ex, ey, ez, ax, ay, az);
+                    const float2 fv = edge_vals[k];
+                    t_c = edge_features(values + size_t(sh_brick[lo]) * L.spb, b, h, hd, probe, ex, ey, ez, ax, ay,
+                                        az, int(axis), fv.x, fv.y, first_s + lo * FEATURE_SCAN, sh_ns[lo], RC, f);
+                    t_lin = fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
+                }
+                if (MODE == EDGE_FEATURES) {
+                    if (have) {
+                        for (int c = 0; c < MLP_IN; c++) feat_out[size_t(k) * MLP_IN + c] = f[c];
+                        out.evals[k] = 1;
+                    }
+                    continue;
+                }
+                mlp_put_row(*M, f);
+                float tm = 0.0f;
+                const bool ok = mlp_forward(*M, phase, &tm, nullptr, nullptr, nullptr, 0);
+                if (!ok && threadIdx.x == 0) atomicAdd(&counters[CNT_TIMEOUT], 1ull);
+                // The MLP chooses the start: the contact iteration's result
+                // where it answers >= 0.5 (and that is within half an edge
+                // of the linear guess), else the linear guess.
+                if (have) out.t[k] = (ok && tm >= 0.5f && fabsf(f[26]) < 4.0f) ? t_c : t_lin;
             }
-            float newton = t - gv / slope;
-            if (fabsf(slope) > 1e-3f * hd && newton > t0 && newton < t1) {
-                t = newton;
-            } else {
-                float s = (t0 * g1 - t1 * g0) / (g1 - g0);
-                t = (isfinite(s) && s > t0 && s < t1) ? s : 0.5f * (t0 + t1);
+            __syncthreads();  // the tiles' bytes become staging regions
+        }
+        if (MODE == EDGE_FEATURES) continue;
+        // Phase B: the batch's items, claimed one at a time by the warps
+        // (WIDE: taken in order by the whole block).  The starts written
+        // above are this block's.
+        if (WIDE) {
+            for (uint32_t i = i0; i < i1; i++) refine_item(i);
+        } else {
+            for (;;) {
+                uint32_t i = 0;
+                if (lane == 0) i = i0 + atomicAdd(&sh_next, 1u);
+                i = __shfl_sync(0xffffffffu, i, 0);
+                if (i >= i1) break;
+                refine_item(i);
             }
         }
-        if (!converged) {
-            bool neg0 = g0 < 0.0f;
-            for (uint32_t it = 0; it < RC.max_bisect; it++) {
-                t = 0.5f * (t0 + t1);
-                float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
-                Eval e = eval(x, y, z);
-                evals++;
-                last = e;
-                if (fabsf(e.value) <= RC.tol || (t1 - t0) * hd <= 2.0f * RC.tol) break;
-                if ((e.value < 0.0f) == neg0) t0 = t;
-                else t1 = t;
-            }
-        }
-        out.t[k] = t;
-        out.feat[k] = last.feat;
-        out.q[3 * size_t(k)] = last.qx, out.q[3 * size_t(k) + 1] = last.qy, out.q[3 * size_t(k) + 2] = last.qz;
-        out.evals[k] = evals | (converged ? 0x80000000u : 0u);
     }
     if (MODE == REFINE_MLP) mlp_teardown(*M, 64);
 }
@@ -1334,23 +1526,67 @@ size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uin
     return (size_t(2) * nn + ns + 3 * size_t(nc) + nv) * 16 + (size_t(ns) * 2 + 1 + nsb + nc + 1 + ncb) * 4;
 }
 
+void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const uint32_t* rec, const uint32_t* edge_off,
+                       const uint32_t* edges, uint32_t* counts, uint32_t* item_off, uint32_t* item_edges,
+                       unsigned long long* tiles, unsigned long long* total, unsigned long long* counters,
+                       cudaStream_t s) {
+    const uint32_t blocks = (n * 32 + 255) / 256;
+    if (n) COUNT(1), k_item_edges<false><<<blocks, 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
+                                                                item_edges, total, counters);
+    launch_scan(counts, n, item_off, nullptr, tiles, total, s);
+    COUNT(1);
+    k_item_edges<true><<<max(blocks, 1u), 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off, item_edges,
+                                                      total, counters);
+}
+
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
-                          uint32_t n, const uint32_t* rec, const uint32_t* ids, const uint32_t* edge_off,
-                          const uint32_t* edges, const float2* edge_vals, float* t, uint32_t* feat, float* q,
-                          uint32_t* evals, size_t cand_bytes, int mode, const float* values, const MlpDev* mlp,
-                          float* feat_out, unsigned long long* counters, cudaStream_t s) {
-    if (!n) return cudaSuccess;
-    const uint32_t mlp_off = uint32_t((cand_bytes + 127) / 128 * 128);
-    const uint32_t list_off = mlp_off + (mode == REFINE_MLP ? uint32_t((sizeof(MlpSmem) + 127) / 128 * 128) : 0u);
-    const size_t smem = size_t(list_off) + size_t(3) * L.sub * L.sub * L.sub * 4 + 16;
-    auto kern = mode == REFINE_MLP ? k_refine<REFINE_MLP> : (mode == EDGE_FEATURES ? k_refine<EDGE_FEATURES>
-                                                                                 : k_refine<REFINE_PLAIN>);
+                          const uint32_t* rec, const uint32_t* ids, const uint32_t* edges, const float2* edge_vals,
+                          const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
+                          uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float* values,
+                          const MlpDev* mlp, float* feat_out, unsigned long long* counters, int sms,
+                          size_t smem_limit, cudaStream_t s, size_t* smem_out) {
+    auto al = [](size_t v) { return (v + 127) / 128 * 128; };
+    RefinePlan P;
+    P.cand_bytes = uint32_t(al(cand_bytes));
+    // MLP: weights (kept) then tiles and the first S candidates (per tile),
+    // the latter two in bytes the staging regions reuse.
+    const size_t keep = mode == REFINE_MLP ? al(offsetof(MlpSmem, x)) : 0;
+    const size_t tiles = mode == REFINE_MLP ? al(sizeof(MlpSmem) - offsetof(MlpSmem, x)) : 0;
+    P.stage_off = uint32_t(keep);
+    P.first_off = uint32_t(keep + tiles);
+    const size_t phase_a = mode == REFINE_PLAIN ? 0 : tiles + size_t(REFINE_WARPS) * REFINE_BATCH * FEATURE_SCAN * 16;
+    const size_t narrow = keep + std::max(phase_a, size_t(REFINE_WARPS) * P.cand_bytes);
+    const size_t wide = keep + std::max(phase_a, size_t(P.cand_bytes));
+    // One staging region per warp (an item per warp in flight, as many items
+    // per SM as regions fit) while four fit in a block, else one per block.
+    const bool use_wide = narrow > smem_limit;
+    const size_t smem = use_wide ? wide : narrow;
+    if (smem_out) *smem_out = smem;
+    if (!n_items) return cudaSuccess;
+    auto pick = [&](auto narrow_k, auto wide_k) { return use_wide ? wide_k : narrow_k; };
+    auto kern = mode == REFINE_MLP
+                    ? pick(k_refine<REFINE_MLP, false>, k_refine<REFINE_MLP, true>)
+                    : (mode == EDGE_FEATURES ? pick(k_refine<EDGE_FEATURES, false>, k_refine<EDGE_FEATURES, true>)
+                                             : pick(k_refine<REFINE_PLAIN, false>, k_refine<REFINE_PLAIN, true>));
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
+    // Resident CTAs per SM from the plain kernel's occupancy at this shared
+    // memory size (the same limits; the TMEM columns cap the MLP kernel).
+    auto occ = use_wide ? k_refine<REFINE_PLAIN, true> : k_refine<REFINE_PLAIN, false>;
+    e = cudaFuncSetAttribute(occ, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, occ, 32 * REFINE_WARPS, smem);
+    if (e != cudaSuccess) return e;
+    if (mode == REFINE_MLP) per_sm = std::min(per_sm, 8);  // 64 TMEM columns per CTA of the SM's 512
+    const uint32_t quads = (n_items + REFINE_WARPS - 1) / REFINE_WARPS;
+    const uint32_t grid = std::min<uint32_t>(quads, uint32_t(std::max(1, sms * std::max(per_sm, 1))));
+    P.batch = std::max<uint32_t>(1, std::min<uint32_t>(REFINE_BATCH, quads / (4 * grid)));
+    cudaMemsetAsync(&counters[CNT_QUEUE], 0, sizeof(unsigned long long), s);
     COUNT(1);
     MlpDev md = mlp ? *mlp : MlpDev{nullptr, nullptr, nullptr};
-    kern<<<n, 128, smem, s>>>(A, L, RC, keys, work, n, rec, ids, edge_off, edges, edge_vals, RefOut{t, feat, q, evals},
-                              values, md, feat_out, mlp_off, list_off, counters);
+    kern<<<grid, 32 * REFINE_WARPS, smem, s>>>(A, L, RC, keys, work, rec, ids, edges, edge_vals, item_off, item_edges,
+                                               n_items, RefOut{t, feat, q, evals}, values, md, feat_out, P, counters);
     return cudaGetLastError();
 }
 

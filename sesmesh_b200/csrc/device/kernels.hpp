@@ -29,7 +29,7 @@ __host__ __device__ inline size_t gather_smem_bytes(const GatherCaps& c) {
 // Device counters of one gather/sample pass.
 enum : int {
     CNT_IDS = 0, CNT_PACK = 1, CNT_MAXPACK = 2, CNT_OVERFLOW = 3, CNT_NOMEM = 4, CNT_TIMEOUT = 5, CNT_OPS = 6,
-    CNT_OWNED = 7, CNT_MAXNN = 8, CNT_MAXNS = 9, CNT_MAXNC = 10, CNT_MAXNV = 11, CNT_N = 16
+    CNT_OWNED = 7, CNT_MAXNN = 8, CNT_MAXNS = 9, CNT_MAXNC = 10, CNT_MAXNV = 11, CNT_MAXITEM = 12, CNT_QUEUE = 13, CNT_N = 16
 };
 constexpr uint32_t REC_NOMEM = 2;
 
@@ -51,11 +51,22 @@ struct RefineConsts {
 size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uint32_t nsb, uint32_t ncb);
 enum : int { REFINE_PLAIN = 0, REFINE_MLP = 1, EDGE_FEATURES = 2 };
 struct MlpDev;
+// Per refinable work item, its edge list (counts, exclusive offsets with the
+// total at item_off[n], edge indices); the largest count goes to
+// counters[CNT_MAXITEM].
+void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const uint32_t* rec, const uint32_t* edge_off,
+                       const uint32_t* edges, uint32_t* counts, uint32_t* item_off, uint32_t* item_edges,
+                       unsigned long long* tiles, unsigned long long* total, unsigned long long* counters,
+                       cudaStream_t s);
+// Persistent refinement (or feature pass) over the items' edge lists; grid
+// = SMs x resident CTAs.  *smem_out gets the shared memory it needs (also
+// when it does not launch, for n_items = 0).
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
-                          uint32_t n, const uint32_t* rec, const uint32_t* ids, const uint32_t* edge_off,
-                          const uint32_t* edges, const float2* edge_vals, float* t, uint32_t* feat, float* q,
-                          uint32_t* evals, size_t cand_bytes, int mode, const float* values, const MlpDev* mlp,
-                          float* feat_out, unsigned long long* counters, cudaStream_t s);
+                          const uint32_t* rec, const uint32_t* ids, const uint32_t* edges, const float2* edge_vals,
+                          const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
+                          uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float* values,
+                          const MlpDev* mlp, float* feat_out, unsigned long long* counters, int sms,
+                          size_t smem_limit, cudaStream_t s, size_t* smem_out);
 
 unsigned long long kernel_launches();
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);

@@ -32,27 +32,38 @@ struct MlpDev {
     const __nv_bfloat16* w2t;
 };
 
+// Weights, biases, TMEM slot and barrier first (they live across tiles),
+// then the per-tile input and hidden tiles (a caller may reuse those bytes
+// between tiles: offsetof(MlpSmem, x) is the persistent part's size).
 struct MlpSmem {
-    __nv_bfloat16 x[MLP_ROWS * MLP_IN];
-    __nv_bfloat16 a1[MLP_ROWS * MLP_H];
     __nv_bfloat16 w1[MLP_H * MLP_IN];
     __nv_bfloat16 w2[MLP_H * MLP_H];
     float b1[MLP_H], b2[MLP_H], w3[MLP_H];
     float b3;
     uint32_t tmem;
     alignas(8) uint64_t bar;
+    alignas(16) __nv_bfloat16 x[MLP_ROWS * MLP_IN];
+    __nv_bfloat16 a1[MLP_ROWS * MLP_H];
 };
 
-// GELU, tanh form, and its derivative (f32).
+// tanh on the special-function unit (one MUFU instruction, relative error
+// below 2^-10, far inside the BF16 rounding of the activations it feeds).
+__device__ __forceinline__ float tanh_sfu(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// GELU, tanh form, and its derivative (f32 arithmetic, SFU tanh).
 __device__ __forceinline__ float gelu(float z) {
     const float k = 0.7978845608028654f;
     float u = k * (z + 0.044715f * z * z * z);
-    return 0.5f * z * (1.0f + tanhf(u));
+    return 0.5f * z * (1.0f + tanh_sfu(u));
 }
 __device__ __forceinline__ float gelu_grad(float z) {
     const float k = 0.7978845608028654f;
     float u = k * (z + 0.044715f * z * z * z);
-    float th = tanhf(u);
+    float th = tanh_sfu(u);
     return 0.5f * (1.0f + th) + 0.5f * z * (1.0f - th * th) * k * (1.0f + 3.0f * 0.044715f * z * z);
 }
 

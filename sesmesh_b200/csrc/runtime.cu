@@ -694,27 +694,42 @@ static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* m
         return SMB_OK;
     }
     const size_t cand = size_t(b->max_pack) * 16 + 64;
-    const size_t smem = (cand + 127) / 128 * 128 + (mode == REFINE_MLP ? mlp_smem_bytes() : 0) +
-                        size_t(3) * r->L.sub * r->L.sub * r->L.sub * 4 + 16;
+    size_t smem = 0;
+    launch_refine(r->A, r->L, r->rc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
+                  nullptr, nullptr, nullptr, nullptr, cand, mode, nullptr, nullptr, nullptr, nullptr,
+                  d->info.multiprocessors, d->smem_optin, s, &smem);
     if (smem > size_t(d->smem_optin))
         return set_err(err, errlen, "a sub-block's candidates exceed shared memory for refinement"), SMB_ERR_MEMORY;
+    const uint32_t nw = b->n_work;
+    if ((rc = b->item_counts.reserve(size_t(nw) * 4, err, errlen)) ||
+        (rc = b->item_off.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
+        (rc = b->item_edges.reserve(ne * 4, err, errlen)) ||
+        (rc = b->tiles.reserve(size_t(scan_tiles_needed(nw)) * 8, err, errlen)))
+        return rc;
     cudaEventRecord(b->ev[4], s);
     CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
     if (mode == EDGE_FEATURES) CK(cudaMemsetAsync(b->e_x.p, 0, ne * 4 * 32, s));
-    CK(cudaMemsetAsync(b->counters.as<unsigned long long>() + CNT_TIMEOUT, 0, 8, s));
+    unsigned long long* cnt = b->counters.as<unsigned long long>();
+    CK(cudaMemsetAsync(cnt + CNT_TIMEOUT, 0, 8, s));
+    CK(cudaMemsetAsync(cnt + CNT_MAXITEM, 0, 8, s));
+    launch_item_edges(r->L, b->work.as<uint32_t>(), nw, b->rec.as<uint32_t>(), b->edge_off.as<uint32_t>(),
+                      b->edges.as<uint32_t>(), b->item_counts.as<uint32_t>(), b->item_off.as<uint32_t>(),
+                      b->item_edges.as<uint32_t>(), b->tiles.as<unsigned long long>(),
+                      b->totals.as<unsigned long long>() + 3, cnt, s);
     MlpDev md{nullptr, nullptr, nullptr};
     if (mlp) md = mlp_dev(mlp);
-    cudaError_t e = launch_refine(r->A, r->L, r->rc, r->keys + b->first, b->work.as<uint32_t>(), b->n_work,
-                                  b->rec.as<uint32_t>(), b->ids.as<uint32_t>(), b->edge_off.as<uint32_t>(),
-                                  b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->e_t.as<float>(),
-                                  b->e_feat.as<uint32_t>(), b->e_q.as<float>(), b->e_evals.as<uint32_t>(), cand, mode,
-                                  b->values.as<float>(), mode == REFINE_MLP ? &md : nullptr, b->e_x.as<float>(),
-                                  b->counters.as<unsigned long long>(), s);
+    cudaError_t e = launch_refine(r->A, r->L, r->rc, r->keys + b->first, b->work.as<uint32_t>(), b->rec.as<uint32_t>(),
+                                  b->ids.as<uint32_t>(), b->edges.as<uint32_t>(), b->edge_vals.as<float2>(),
+                                  b->item_off.as<uint32_t>(), b->item_edges.as<uint32_t>(), nw,
+                                  b->e_t.as<float>(), b->e_feat.as<uint32_t>(), b->e_q.as<float>(),
+                                  b->e_evals.as<uint32_t>(), cand, mode, b->values.as<float>(),
+                                  mode == REFINE_MLP ? &md : nullptr, b->e_x.as<float>(), cnt,
+                                  d->info.multiprocessors, d->smem_optin, s, nullptr);
     if (e != cudaSuccess) return set_err(err, errlen, "refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     cudaEventRecord(b->ev[5], s);
     CK(cudaStreamSynchronize(s));
     unsigned long long timeouts = 0;
-    CK(cudaMemcpy(&timeouts, b->counters.as<unsigned long long>() + CNT_TIMEOUT, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&timeouts, cnt + CNT_TIMEOUT, 8, cudaMemcpyDeviceToHost));
     if (timeouts) return set_err(err, errlen, "tensor-core wait timed out in %llu tiles", timeouts), SMB_ERR_CUDA;
     float t = 0;
     cudaEventElapsedTime(&t, b->ev[4], b->ev[5]);

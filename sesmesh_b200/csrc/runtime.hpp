@@ -75,12 +75,13 @@ struct smb_batch {
     smb::DBuf ids, pack, mc_counts, edge_off, tri_off, edges, edge_vals, tris;
     smb::DBuf e_t, e_feat, e_q, e_evals;  // fast-mode refinement results
     smb::DBuf e_x;                        // warm-start features (32 f32 per edge)
+    smb::DBuf item_counts, item_off, item_edges;  // per sampled sub-block edge lists
     smb::GatherCaps caps{192, 128, 384, 128};
     int gather_warps = 4;
     bool use_tma = true;
     cudaEvent_t ev[6] = {};
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
-                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x};
+                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &item_counts, &item_off, &item_edges};
     }
 };

@@ -133,7 +133,7 @@ def _features_np(arr, probe, h, brick, bricks, vals, mc, rec, ids, batch):
             m = np.array([x + 0.5 * (ax == 0), y + 0.5 * (ax == 1), z + 0.5 * (ax == 2)]) * h
             if j not in lists:
                 lists[j] = batch.lists(rec[j], ids)["s"]
-            sid = lists[j]
+            sid = lists[j][:32]  # FEATURE_SCAN
             origin = np.asarray(bricks[i], np.float64) * brick * h
             c = arr["center"][sid] - origin
             r = arr["expanded"][sid] - probe
