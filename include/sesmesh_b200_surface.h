@@ -83,6 +83,49 @@ int smb_surface_mesh(const smb_surface* s, float* positions, float* normals, uin
 size_t smb_surface_obj(smb_surface* s, char* out, size_t cap);
 int smb_surface_write_obj(smb_surface* s, const char* path, char* err, size_t errlen);
 
+/* Many structures in one device pass (no counterpart in the reference,
+ * which meshes one structure per compute_surface call, surface.rs:599-711):
+ * structures stay resident side by side, one classification pass covers
+ * them all, and the mesh stage runs as one captured CUDA graph whose
+ * kernels take (structure, brick) items from a device queue; fast mode,
+ * optionally with the learned warm start.  Each structure's mesh is the
+ * single-structure device path's at the same brick edge.  Buffers are
+ * sized from per-brick caps; a structure over a cap is meshed again on its
+ * own (counted in smb_multi_times.redone).  The autotuner picks the brick
+ * edge (8 or 16), the candidate caps (level 0 or 1) and the gather block
+ * shape (2 or 4 warps) by timing the device pass; a config with every
+ * field set skips it. */
+typedef struct smb_multi smb_multi;
+typedef struct {
+    uint32_t brick;        /* 0: tuned; else even, 4..32 */
+    uint32_t caps_level;   /* 0 or 1 (tuned when brick or gather_warps is 0) */
+    uint32_t gather_warps; /* 0: tuned; else 1, 2, 4 or 8 */
+} smb_multi_config;
+typedef struct {
+    size_t structures, redone, bricks, samples;
+    /* ms: arrangements and uploads (once), tuning (once), classification,
+     * device pass, copies back, host stages, structures redone, whole run */
+    double t_setup, t_tune, t_classify, t_device, t_d2h, t_host, t_redo, t_total;
+    int graph; /* the pass ran from a captured CUDA graph */
+} smb_multi_times;
+/* n structures: xyzr[i] holds counts[i] rows (x, y, z, r); params[i] its
+ * SES parameters (refine must be SMB_REFINE_FAST; brick_size is set by the
+ * batch). */
+int smb_multi_new(smb_device* dev, size_t n, const double* const* xyzr, const size_t* counts,
+                  const smb_surface_params* params, const smb_multi_config* cfg, smb_multi** out, char* err,
+                  size_t errlen);
+void smb_multi_free(smb_multi* m);
+int smb_multi_set_warm_start(smb_multi* m, const smb_mlp* mlp);
+/* Runs the autotuner now (smb_multi_run runs it first when needed). */
+int smb_multi_tune(smb_multi* m, char* err, size_t errlen);
+int smb_multi_config_get(const smb_multi* m, smb_multi_config* out);
+/* Meshes every structure; per-structure results and latencies (ms from the
+ * start of the run until that structure's mesh is complete) until the next
+ * run. */
+int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen);
+smb_surface* smb_multi_surface(smb_multi* m, size_t i);
+int smb_multi_latency(const smb_multi* m, double* ms);
+
 /* The host arrangement of an engine (views valid while it lives). */
 typedef struct {
     size_t n_spheres, n_contained, n_circles, n_vertices;

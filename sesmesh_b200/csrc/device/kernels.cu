@@ -104,11 +104,37 @@ __device__ __forceinline__ long long sat_floor(double v) {
     return (long long)f;
 }
 
+// The structure whose range [off[s], off[s + 1]) holds v (off ascending,
+// n + 1 entries).
+template <class T>
+__device__ __forceinline__ uint32_t structure_of(const T* off, uint32_t n, T v) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (off[mid] <= v) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 // lattice::touched_bricks (field/lattice.rs:105-163): every non-contained
 // sphere marks the bricks its ball of radius R + CLASSIFY_EPS overlaps, in a
 // dense flag grid over the bricks' bounding box.
-__global__ void k_mark_touched(DArr A, DLat L, BrickBox box, uint32_t* flags, int* err) {
+template <bool MANY>
+__global__ void k_mark_touched(DArr A0, DLat L0, BrickBox box0, uint32_t* flags0, int* err0, Scene S,
+                               uint32_t n_total) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t st = 0;
+    if constexpr (MANY) {
+        if (i >= n_total) return;
+        st = structure_of(S.sph_off, S.n_struct, i);
+        i -= S.sph_off[st];
+    }
+    const DArr& A = MANY ? S.arr[st] : A0;
+    const DLat& L = MANY ? S.lat[st] : L0;
+    const BrickBox& box = MANY ? S.box[st] : box0;
+    uint32_t* flags = MANY ? flags0 + S.flag_off[st] : flags0;
+    int* err = MANY ? S.err + st : err0;
     if (i >= A.n || A.status[i] == STATUS_CONTAINED) return;
     double4 c = A.sph[i];
     double r = c.w + CLASSIFY_EPS;
@@ -139,26 +165,41 @@ __device__ __forceinline__ void cell_key(const BrickBox& box, uint32_t cell, int
 
 // lattice::surface_bricks (field/lattice.rs:168-181): the exact f64 test at
 // each touched brick's centre, one warp per brick.
-__global__ void k_classify_bricks(DArr A, DLat L, BrickBox box, const uint32_t* touched, uint32_t n_touched,
-                                  uint32_t* surface) {
+template <bool MANY>
+__global__ void k_classify_bricks(DArr A0, DLat L0, BrickBox box0, const uint32_t* touched, uint32_t n_touched,
+                                  uint32_t* surface, Scene S) {
     uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (w >= n_touched) return;
-    uint32_t cell = touched[w];
+    const uint32_t flag = touched[w];
+    uint32_t st = 0, cell = flag;
+    if constexpr (MANY) {
+        st = structure_of(S.flag_off, S.n_struct, (unsigned long long)flag);
+        cell = uint32_t(flag - S.flag_off[st]);
+    }
+    const DArr& A = MANY ? S.arr[st] : A0;
+    const DLat& L = MANY ? S.lat[st] : L0;
+    const BrickBox& box = MANY ? S.box[st] : box0;
     int k[3];
     cell_key(box, cell, k);
     double bh = double(L.b);
     double cx = (double(k[0]) + 0.5) * bh * L.h, cy = (double(k[1]) + 0.5) * bh * L.h, cz = (double(k[2]) + 0.5) * bh * L.h;
     int s = uniform_sign_warp(A, cx, cy, cz, L.rho_brick, lane);
-    if (lane == 0) surface[cell] = s < 0 ? 1u : 0u;
+    if (lane == 0) surface[flag] = s < 0 ? 1u : 0u;
 }
 
-__global__ void k_cells_to_keys(BrickBox box, const uint32_t* cells, uint32_t n, int4* keys) {
+template <bool MANY>
+__global__ void k_cells_to_keys(BrickBox box0, const uint32_t* cells, uint32_t n, int4* keys, Scene S) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    uint32_t st = 0, cell = cells[i];
+    if constexpr (MANY) {
+        st = structure_of(S.flag_off, S.n_struct, (unsigned long long)cell);
+        cell = uint32_t(cell - S.flag_off[st]);
+    }
     int k[3];
-    cell_key(box, cells[i], k);
-    keys[i] = make_int4(k[0], k[1], k[2], 0);
+    cell_key(MANY ? S.box[st] : box0, cell, k);
+    keys[i] = make_int4(k[0], k[1], k[2], int(st));
 }
 
 // Owner of a brick sample (Engine::assign, field/kernel.rs:489-546): the
@@ -189,13 +230,16 @@ __device__ __forceinline__ int sample_owner(int x, int y, int z, int sub, const 
 // Engine::sub_states (field/kernel.rs:467-482): one warp per sub-block,
 // independent of the brick's other sub-blocks (the +-band values of samples
 // no sampled sub-block owns are written by the marching-cubes count pass).
-__global__ void __launch_bounds__(256) k_substates(DArr A, DLat L, const int4* keys, uint32_t n_bricks, uint32_t* rec,
-                                                   uint32_t* sampled) {
+template <bool MANY>
+__global__ void __launch_bounds__(256) k_substates(DArr A0, DLat L0, const int4* keys, uint32_t n_bricks, uint32_t* rec,
+                                                   uint32_t* sampled, Scene S) {
     const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (j >= n_bricks * 8) return;
     const uint32_t brick = j >> 3, w = j & 7;
     int4 key = keys[brick];
+    const DArr& A = MANY ? S.arr[key.w] : A0;
+    const DLat& L = MANY ? S.lat[key.w] : L0;
     double h = L.h, sub = double(L.sub), half = double(L.sub) * 0.5;
     double bx = double((long long)key.x * L.b) * h, by = double((long long)key.y * L.b) * h,
            bz = double((long long)key.z * L.b) * h;
@@ -259,12 +303,13 @@ __device__ __forceinline__ unsigned warp_inclusive_scan(unsigned v) {
 }
 
 
-__global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
-                         GatherCaps caps) {
+template <bool MANY>
+__global__ void k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
+                         GatherCaps caps, Scene S) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t item = blockIdx.x * (blockDim.x >> 5) + wib;
-    if (item >= n_work) return;
+    if (item >= (MANY ? uint32_t(*S.n_work) : n_work)) return;
     unsigned char* base = smem_raw + size_t(wib) * gather_smem_bytes(caps);
     double* s_key = reinterpret_cast<double*>(base);
     double* c_key = s_key + caps.s;
@@ -284,6 +329,8 @@ __global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work,
     const uint32_t brick = j >> 3, sb = j & 7;
     uint32_t* rec = O.rec + size_t(j) * REC_WORDS;
     const int4 key = keys[brick];
+    const DArr& A = MANY ? S.arr[key.w] : A0;
+    const DLat& L = MANY ? S.lat[key.w] : L0;
     // Sub-block centre as Engine::prepare_sub computes it (kernel.rs:575-583).
     const double h = L.h, sub = double(L.sub), half = double(L.sub) * 0.5;
     const double px = double((long long)key.x * L.b) * h, py = double((long long)key.y * L.b) * h,
@@ -299,6 +346,7 @@ __global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work,
             rec[R_FLAGS] |= bit;
             unsigned long long q = atomicAdd(&O.counters[bit == REC_OVERFLOW ? CNT_OVERFLOW : CNT_NOMEM], 1ull);
             if (bit == REC_OVERFLOW && O.retry) O.retry[q] = j;
+            if (O.fail) O.fail[key.w] = 1;
         }
     };
 
@@ -435,7 +483,8 @@ __global__ void k_gather(DArr A, DLat L, const int4* keys, const uint32_t* work,
     }
     ids_base = __shfl_sync(0xffffffffu, ids_base, 0);
     pack_base = __shfl_sync(0xffffffffu, pack_base, 0);
-    if (ids_base + ids_words > O.ids_cap || pack_base + units > O.pack_cap) return overflow(REC_NOMEM);
+    if (ids_base + ids_words > O.ids_cap || pack_base + units > O.pack_cap || units > O.unit_cap)
+        return overflow(REC_NOMEM);
 
     // CSR ids: near, S, s_off, s_blk, C, c_off, c_blk, V.
     uint32_t* ids = O.ids + ids_base;
@@ -566,15 +615,17 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 constexpr uint32_t BULK_CHUNK = 32768;            // bytes per bulk copy
 constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;     // bounded wait
 
-template <bool TMA, bool COUNT>
-__global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const uint32_t* work, uint32_t n_work,
+template <bool TMA, bool COUNT, bool MANY>
+__global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work,
                                                 const uint32_t* rec, const uint4* pack, float* values,
-                                                unsigned long long* counters) {
+                                                unsigned long long* counters, Scene SC) {
     extern __shared__ __align__(16) uint4 sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t sts[8];
+    if (MANY && blockIdx.x >= uint32_t(*SC.n_work)) return;
     const uint32_t j = work[blockIdx.x];
     const uint32_t brick = j >> 3, sb = j & 7;
+    const DLat& L = MANY ? SC.lat[keys[brick].w] : L0;
     const uint32_t* R = rec + size_t(j) * REC_WORDS;
     if (R[R_FLAGS] != 0) return;
     const int nn = int(R[R_NEAR]), n_in = int(R[R_INSIDE]), ns = int(R[R_S]), nc = int(R[R_C]), nv = int(R[R_V]);
@@ -722,10 +773,11 @@ __global__ void __launch_bounds__(128) k_sample(DLat L, const int4* keys, const 
 constexpr int MC_THREADS = 256;
 __constant__ uint8_t c_edge_lower[12] = {0, 2, 4, 6, 0, 1, 4, 5, 0, 1, 2, 3};
 
-template <bool FILL>
-__global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L, uint32_t n_bricks, float* values, const uint32_t* rec, uint32_t* counts,
+template <bool FILL, bool MANY>
+__global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L0, uint32_t n_bricks, float* values, const uint32_t* rec, uint32_t* counts,
                                                    const uint32_t* edge_off, const uint32_t* tri_off, uint32_t* edges,
-                                                   float2* edge_vals, uint32_t* tris) {
+                                                   float2* edge_vals, uint32_t* tris, const int4* keys,
+                                                   unsigned long long edge_cap, unsigned long long tri_cap, Scene S) {
     extern __shared__ float v[];
     __shared__ uint16_t t_off[257];
     __shared__ uint8_t t_edges[SMB_MC_TRIANGLES * 3];
@@ -733,6 +785,11 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L, uint32_t n_bricks, fl
     __shared__ uint32_t sts[8];
     const uint32_t brick = blockIdx.x;
     if (brick >= n_bricks) return;
+    const DLat& L = MANY ? S.lat[keys[brick].w] : L0;
+    if (FILL && (edge_off[brick + 1] > edge_cap || tri_off[brick + 1] > tri_cap)) {
+        if (MANY && threadIdx.x == 0) S.fail[keys[brick].w] = 1;
+        return;
+    }
     const int b = L.b, s = b + 1;
     float* src = values + size_t(brick) * L.spb;
     if (!FILL) {
@@ -974,18 +1031,24 @@ __device__ __forceinline__ float edge_features(const float* val, int b, float h,
 // sub-block, in the brick's (ascending) order.  Warp per item; FILL = false
 // counts (and records the largest count), FILL = true writes at item_off[i]
 // and the list's tail item_off[n] = *total.
-template <bool FILL>
-__global__ void __launch_bounds__(256) k_item_edges(const DLat L, const uint32_t* work, uint32_t n,
+template <bool FILL, bool MANY>
+__global__ void __launch_bounds__(256) k_item_edges(const DLat L, const uint32_t* work, uint32_t n_host,
                                                     const uint32_t* rec, const uint32_t* edge_off,
                                                     const uint32_t* edges, uint32_t* counts, uint32_t* item_off,
                                                     uint32_t* item_edges, const unsigned long long* total,
-                                                    unsigned long long* counters) {
+                                                    unsigned long long* counters, const int4* keys, Scene S) {
     const uint32_t lane = threadIdx.x & 31, i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t n = MANY ? uint32_t(*S.n_work) : n_host;
     if (FILL && blockIdx.x == 0 && threadIdx.x == 0) item_off[n] = uint32_t(*total);
-    if (i >= n) return;
+    if (i >= n) {
+        if (!FILL && MANY && lane == 0 && i < n_host) counts[i] = 0;  // the scan runs over n_host entries
+        return;
+    }
     const uint32_t j = work[i], brick = j >> 3, sb = j & 7;
     const uint32_t* R = rec + size_t(j) * REC_WORDS;
-    if (R[R_STATE] != ST_SAMPLE || R[R_FLAGS] != 0) {
+    // Many structures: a structure over a list or buffer limit is redone on
+    // its own, and its marching-cubes output may be incomplete.
+    if (R[R_STATE] != ST_SAMPLE || R[R_FLAGS] != 0 || (MANY && S.fail[keys[brick].w])) {
         if (!FILL && lane == 0) counts[i] = 0;
         return;
     }
@@ -1008,6 +1071,11 @@ __global__ void __launch_bounds__(256) k_item_edges(const DLat L, const uint32_t
         counts[i] = at;
         atomicMax(reinterpret_cast<unsigned int*>(&counters[CNT_MAXITEM]), at);
     }
+}
+
+// dst = the low 32 bits of a device total (the tail of an offset list).
+__global__ void k_put_total(uint32_t* dst, const unsigned long long* total) {
+    if (threadIdx.x == 0) *dst = uint32_t(*total);
 }
 
 // Brick-local frame of one brick: the origin (key * b - frame) * h as an f32
@@ -1286,12 +1354,13 @@ struct RefinePlan {
     uint32_t first_off;   // phase A: first S candidates, REFINE_WARPS x REFINE_BATCH x FEATURE_SCAN float4
 };
 
-template <int MODE, bool WIDE>
+template <int MODE, bool WIDE, bool MANY>
 __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
-    DArr A, DLat L, RefineConsts RC, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
+    DArr A0, DLat L0, RefineConsts RC0, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
     const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
-    uint32_t n_items, RefOut out, const float* values, MlpDev mlp, float* feat_out, RefinePlan P,
-    unsigned long long* counters) {
+    uint32_t n_host, RefOut out, const float* values, MlpDev mlp, float* feat_out, RefinePlan P,
+    unsigned long long* counters, Scene S) {
+    const uint32_t n_items = MANY ? uint32_t(*S.n_work) : n_host;
     extern __shared__ __align__(128) float4 rs[];
     __shared__ uint32_t sh_q, sh_next;
     __shared__ uint32_t sh_off[REFINE_WARPS * REFINE_BATCH + 1], sh_sbase[REFINE_WARPS * REFINE_BATCH],
@@ -1303,10 +1372,11 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
     float4* first_s = reinterpret_cast<float4*>(smem + P.first_off);  // per batch item, FEATURE_SCAN each
     unsigned char* mine = smem + P.stage_off + (WIDE ? 0 : size_t(warp) * P.cand_bytes);
     unsigned int* queue = reinterpret_cast<unsigned int*>(&counters[CNT_QUEUE]);
-    const float probe = L.probe32, band = L.band32, h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
-    const int b = L.b;
     const uint32_t n_quads = (n_items + REFINE_WARPS - 1) / REFINE_WARPS;
-    auto edge_geom = [&](uint32_t k, uint32_t& axis, int& ex, int& ey, int& ez, float& ax, float& ay, float& az) {
+    auto edge_geom = [&](const DLat& L, const RefineConsts& RC, uint32_t k, uint32_t& axis, int& ex, int& ey, int& ez,
+                         float& ax, float& ay, float& az) {
+        const int b = L.b;
+        const float h = RC.h_hi;
         const uint32_t code = edges[k], cell = code / 3;
         axis = code % 3;
         ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
@@ -1318,7 +1388,12 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
         const uint32_t a0 = item_off[i], a1 = item_off[i + 1];
         if (a0 == a1) return;
         const uint32_t j = work[i], brick = j >> 3;
-        const BrickFrame F = brick_frame(L, RC, keys[brick]);
+        const int4 key = keys[brick];
+        const DArr& A = MANY ? S.arr[key.w] : A0;
+        const DLat& L = MANY ? S.lat[key.w] : L0;
+        const RefineConsts& RC = MANY ? S.rc[key.w] : RC0;
+        const float probe = L.probe32, band = L.band32;
+        const BrickFrame F = brick_frame(L, RC, key);
         const uint32_t* R = rec + size_t(j) * REC_WORDS;
         if (WIDE) __syncthreads();
         else __syncwarp();
@@ -1330,7 +1405,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
             uint32_t axis;
             int ex, ey, ez;
             float ax, ay, az;
-            edge_geom(k, axis, ex, ey, ez, ax, ay, az);
+            edge_geom(L, RC, k, axis, ex, ey, ez, ax, ay, az);
             const float2 fv = edge_vals[k];
             const float t0 = MODE == REFINE_MLP ? out.t[k] : fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
             refine_edge_f32(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, k, out);
@@ -1372,7 +1447,11 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
             for (uint32_t x = threadIdx.x; x < ni * FEATURE_SCAN; x += blockDim.x) {
                 const uint32_t it = x / FEATURE_SCAN, c = x % FEATURE_SCAN;
                 if (int(c) >= sh_ns[it] || sh_off[it] == sh_off[it + 1]) continue;
-                const BrickFrame F = brick_frame(L, RC, keys[sh_brick[it]]);
+                const int4 key = keys[sh_brick[it]];
+                const DArr& A = MANY ? S.arr[key.w] : A0;
+                const DLat& L = MANY ? S.lat[key.w] : L0;
+                const RefineConsts& RC = MANY ? S.rc[key.w] : RC0;
+                const BrickFrame F = brick_frame(L, RC, key);
                 double4 sp = A.sph[ids[sh_sbase[it] + c]];
                 float lx, ly, lz;
                 to_local(L, F, sp.x, sp.y, sp.z, lx, ly, lz);
@@ -1395,13 +1474,17 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
                         else hi = mid;
                     }
                     k = item_edges[e];
+                    const int st = keys[sh_brick[lo]].w;
+                    const DLat& L = MANY ? S.lat[st] : L0;
+                    const RefineConsts& RC = MANY ? S.rc[st] : RC0;
                     uint32_t axis;
                     int ex, ey, ez;
                     float ax, ay, az;
-                    edge_geom(k, axis, ex, ey, ez, ax, ay, az);
+                    edge_geom(L, RC, k, axis, ex, ey, ez, ax, ay, az);
                     const float2 fv = edge_vals[k];
-                    t_c = edge_features(values + size_t(sh_brick[lo]) * L.spb, b, h, hd, probe, ex, ey, ez, ax, ay,
-                                        az, int(axis), fv.x, fv.y, first_s + lo * FEATURE_SCAN, sh_ns[lo], RC, f);
+                    t_c = edge_features(values + size_t(sh_brick[lo]) * L.spb, L.b, RC.h_hi, RC.h_hi + RC.h_lo,
+                                        L.probe32, ex, ey, ez, ax, ay, az, int(axis), fv.x, fv.y,
+                                        first_s + lo * FEATURE_SCAN, sh_ns[lo], RC, f);
                     t_lin = fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
                 }
                 if (MODE == EDGE_FEATURES) {
@@ -1467,59 +1550,85 @@ void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, 
 
 uint32_t scan_tiles_needed(uint32_t n) { return (n + SCAN_TILE - 1) / SCAN_TILE + 1; }
 
-void launch_mark_touched(const DArr& A, const DLat& L, const BrickBox& box, uint32_t* flags, int* err, cudaStream_t s) {
-    if (A.n) COUNT(1), k_mark_touched<<<(A.n + 127) / 128, 128, 0, s>>>(A, L, box, flags, err);
+void launch_mark_touched(const DArr& A, const DLat& L, const BrickBox& box, uint32_t* flags, int* err, cudaStream_t s,
+                         const Scene* many, uint32_t n_total) {
+    if (many) {
+        if (n_total) COUNT(1), k_mark_touched<true><<<(n_total + 127) / 128, 128, 0, s>>>(A, L, box, flags, err, *many,
+                                                                                          n_total);
+        return;
+    }
+    if (A.n) COUNT(1), k_mark_touched<false><<<(A.n + 127) / 128, 128, 0, s>>>(A, L, box, flags, err, Scene{}, 0);
 }
 
 void launch_classify_bricks(const DArr& A, const DLat& L, const BrickBox& box, const uint32_t* touched, uint32_t n,
-                            uint32_t* surface, cudaStream_t s) {
-    if (n) COUNT(1), k_classify_bricks<<<(n + 7) / 8, 256, 0, s>>>(A, L, box, touched, n, surface);
+                            uint32_t* surface, cudaStream_t s, const Scene* many) {
+    if (!n) return;
+    COUNT(1);
+    if (many) k_classify_bricks<true><<<(n + 7) / 8, 256, 0, s>>>(A, L, box, touched, n, surface, *many);
+    else k_classify_bricks<false><<<(n + 7) / 8, 256, 0, s>>>(A, L, box, touched, n, surface, Scene{});
 }
 
-void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n, int4* keys, cudaStream_t s) {
-    if (n) COUNT(1), k_cells_to_keys<<<(n + 255) / 256, 256, 0, s>>>(box, cells, n, keys);
+void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n, int4* keys, cudaStream_t s,
+                          const Scene* many) {
+    if (!n) return;
+    COUNT(1);
+    if (many) k_cells_to_keys<true><<<(n + 255) / 256, 256, 0, s>>>(box, cells, n, keys, *many);
+    else k_cells_to_keys<false><<<(n + 255) / 256, 256, 0, s>>>(box, cells, n, keys, Scene{});
 }
 
 void launch_substates(const DArr& A, const DLat& L, const int4* keys, uint32_t n, uint32_t* rec, uint32_t* sampled,
-                      cudaStream_t s) {
-    if (n) COUNT(1), k_substates<<<n, 256, 0, s>>>(A, L, keys, n, rec, sampled);
+                      cudaStream_t s, const Scene* many) {
+    if (!n) return;
+    COUNT(1);
+    if (many) k_substates<true><<<n, 256, 0, s>>>(A, L, keys, n, rec, sampled, *many);
+    else k_substates<false><<<n, 256, 0, s>>>(A, L, keys, n, rec, sampled, Scene{});
 }
 
 cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const uint32_t* work, uint32_t n,
-                          const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s) {
+                          const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s, const Scene* many) {
     if (!n) return cudaSuccess;
     size_t smem = gather_smem_bytes(caps) * size_t(warps);
-    cudaError_t e = cudaFuncSetAttribute(k_gather, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    auto kern = many ? k_gather<true> : k_gather<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     COUNT(1);
-    k_gather<<<(n + warps - 1) / warps, 32 * warps, smem, s>>>(A, L, keys, work, n, O, caps);
+    kern<<<(n + warps - 1) / warps, 32 * warps, smem, s>>>(A, L, keys, work, n, O, caps, many ? *many : Scene{});
     return cudaGetLastError();
 }
 
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
-                          bool count, cudaStream_t s) {
+                          bool count, cudaStream_t s, const Scene* many) {
     if (!n) return cudaSuccess;
     size_t smem = size_t(max_units) * 16;
-    auto kern = count ? k_sample<true, true> : (tma ? k_sample<true, false> : k_sample<false, false>);
+    auto kern = many ? k_sample<true, false, true>
+                     : (count ? k_sample<true, true, false>
+                              : (tma ? k_sample<true, false, false> : k_sample<false, false, false>));
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     COUNT(1);
-    kern<<<n, 128, smem, s>>>(L, keys, work, n, rec, pack, values, counters);
+    kern<<<n, 128, smem, s>>>(L, keys, work, n, rec, pack, values, counters, many ? *many : Scene{});
     return cudaGetLastError();
 }
 
 cudaError_t launch_mc(const DLat& L, uint32_t n, float* values, const uint32_t* rec, uint32_t* counts, const uint32_t* edge_off,
                       const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
-                      cudaStream_t s) {
+                      cudaStream_t s, const int4* keys, unsigned long long edge_cap, unsigned long long tri_cap,
+                      const Scene* many) {
     if (!n) return cudaSuccess;
     size_t smem = size_t(L.spb) * 4;
-    auto kern = fill ? k_mc<true> : k_mc<false>;
+    auto kern = many ? (fill ? k_mc<true, true> : k_mc<false, true>) : (fill ? k_mc<true, false> : k_mc<false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     COUNT(1);
-    kern<<<n, MC_THREADS, smem, s>>>(L, n, values, rec, counts, edge_off, tri_off, edges, edge_vals, tris);
+    kern<<<n, MC_THREADS, smem, s>>>(L, n, values, rec, counts, edge_off, tri_off, edges, edge_vals, tris, keys, edge_cap,
+                                     tri_cap, many ? *many : Scene{});
     return cudaGetLastError();
+}
+
+void launch_put_total(uint32_t* dst, const unsigned long long* total, cudaStream_t s) {
+    COUNT(1);
+    k_put_total<<<1, 32, 0, s>>>(dst, total);
 }
 
 size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uint32_t nsb, uint32_t ncb) {
@@ -1529,14 +1638,22 @@ size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uin
 void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const uint32_t* rec, const uint32_t* edge_off,
                        const uint32_t* edges, uint32_t* counts, uint32_t* item_off, uint32_t* item_edges,
                        unsigned long long* tiles, unsigned long long* total, unsigned long long* counters,
-                       cudaStream_t s) {
+                       cudaStream_t s, const Scene* many, const int4* keys) {
     const uint32_t blocks = (n * 32 + 255) / 256;
-    if (n) COUNT(1), k_item_edges<false><<<blocks, 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
-                                                                item_edges, total, counters);
+    const Scene sc = many ? *many : Scene{};
+    if (n) {
+        COUNT(1);
+        if (many) k_item_edges<false, true><<<blocks, 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
+                                                                 item_edges, total, counters, keys, sc);
+        else k_item_edges<false, false><<<blocks, 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
+                                                              item_edges, total, counters, keys, sc);
+    }
     launch_scan(counts, n, item_off, nullptr, tiles, total, s);
     COUNT(1);
-    k_item_edges<true><<<max(blocks, 1u), 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off, item_edges,
-                                                      total, counters);
+    if (many) k_item_edges<true, true><<<max(blocks, 1u), 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
+                                                                     item_edges, total, counters, keys, sc);
+    else k_item_edges<true, false><<<max(blocks, 1u), 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
+                                                                  item_edges, total, counters, keys, sc);
 }
 
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
@@ -1544,7 +1661,7 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
                           const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
                           uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float* values,
                           const MlpDev* mlp, float* feat_out, unsigned long long* counters, int sms,
-                          size_t smem_limit, cudaStream_t s, size_t* smem_out) {
+                          size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many) {
     auto al = [](size_t v) { return (v + 127) / 128 * 128; };
     RefinePlan P;
     P.cand_bytes = uint32_t(al(cand_bytes));
@@ -1564,15 +1681,19 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
     if (smem_out) *smem_out = smem;
     if (!n_items) return cudaSuccess;
     auto pick = [&](auto narrow_k, auto wide_k) { return use_wide ? wide_k : narrow_k; };
-    auto kern = mode == REFINE_MLP
-                    ? pick(k_refine<REFINE_MLP, false>, k_refine<REFINE_MLP, true>)
-                    : (mode == EDGE_FEATURES ? pick(k_refine<EDGE_FEATURES, false>, k_refine<EDGE_FEATURES, true>)
-                                             : pick(k_refine<REFINE_PLAIN, false>, k_refine<REFINE_PLAIN, true>));
+    auto kern = many ? (mode == REFINE_MLP ? pick(k_refine<REFINE_MLP, false, true>, k_refine<REFINE_MLP, true, true>)
+                                           : pick(k_refine<REFINE_PLAIN, false, true>,
+                                                  k_refine<REFINE_PLAIN, true, true>))
+                     : (mode == REFINE_MLP
+                            ? pick(k_refine<REFINE_MLP, false, false>, k_refine<REFINE_MLP, true, false>)
+                            : (mode == EDGE_FEATURES
+                                   ? pick(k_refine<EDGE_FEATURES, false, false>, k_refine<EDGE_FEATURES, true, false>)
+                                   : pick(k_refine<REFINE_PLAIN, false, false>, k_refine<REFINE_PLAIN, true, false>)));
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     // Resident CTAs per SM from the plain kernel's occupancy at this shared
     // memory size (the same limits; the TMEM columns cap the MLP kernel).
-    auto occ = use_wide ? k_refine<REFINE_PLAIN, true> : k_refine<REFINE_PLAIN, false>;
+    auto occ = use_wide ? k_refine<REFINE_PLAIN, true, false> : k_refine<REFINE_PLAIN, false, false>;
     e = cudaFuncSetAttribute(occ, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -1586,7 +1707,8 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
     COUNT(1);
     MlpDev md = mlp ? *mlp : MlpDev{nullptr, nullptr, nullptr};
     kern<<<grid, 32 * REFINE_WARPS, smem, s>>>(A, L, RC, keys, work, rec, ids, edges, edge_vals, item_off, item_edges,
-                                               n_items, RefOut{t, feat, q, evals}, values, md, feat_out, P, counters);
+                                               n_items, RefOut{t, feat, q, evals}, values, md, feat_out, P, counters,
+                                               many ? *many : Scene{});
     return cudaGetLastError();
 }
 

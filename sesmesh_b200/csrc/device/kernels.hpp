@@ -40,12 +40,31 @@ struct GatherOut {
     uint32_t* retry;  // sub-blocks whose lists exceeded the shared-memory caps
     unsigned long long* counters;
     unsigned long long ids_cap, pack_cap;
+    unsigned long long unit_cap;  // largest packed block of one sub-block
+    uint32_t* fail;               // per structure (many-structure runs), else null
 };
 
 // Fast-mode refinement constants (RefineRef, sesmesh-gpu batch.rs:133-150).
 struct RefineConsts {
     float h_hi, h_lo, tol;
     uint32_t max_iter, max_bisect;
+};
+
+// Many structures in one launch: per-structure descriptors, indexed by the
+// structure number each brick key carries in .w (int4 keys (x, y, z, s)).
+// Every structure's arrays are slices of shared device buffers and use
+// structure-local indices, so the kernels' bodies are those of one structure.
+struct Scene {
+    const DArr* arr;
+    const DLat* lat;
+    const RefineConsts* rc;
+    const BrickBox* box;                 // classification: each structure's brick box
+    const unsigned long long* flag_off;  // its first flag (n_struct + 1)
+    const uint32_t* sph_off;             // its first sphere (n_struct + 1)
+    uint32_t n_struct;
+    const unsigned long long* n_work;    // sampled sub-blocks, on the device (graph replays)
+    int* err;                            // per structure: classification errors
+    uint32_t* fail;                      // per structure: a list or buffer limit was exceeded
 };
 
 size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uint32_t nsb, uint32_t ncb);
@@ -57,7 +76,8 @@ struct MlpDev;
 void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const uint32_t* rec, const uint32_t* edge_off,
                        const uint32_t* edges, uint32_t* counts, uint32_t* item_off, uint32_t* item_edges,
                        unsigned long long* tiles, unsigned long long* total, unsigned long long* counters,
-                       cudaStream_t s);
+                       cudaStream_t s, const Scene* many = nullptr, const int4* keys = nullptr);
+void launch_put_total(uint32_t* dst, const unsigned long long* total, cudaStream_t s);
 // Persistent refinement (or feature pass) over the items' edge lists; grid
 // = SMs x resident CTAs.  *smem_out gets the shared memory it needs (also
 // when it does not launch, for n_items = 0).
@@ -66,26 +86,31 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
                           const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
                           uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float* values,
                           const MlpDev* mlp, float* feat_out, unsigned long long* counters, int sms,
-                          size_t smem_limit, cudaStream_t s, size_t* smem_out);
+                          size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many = nullptr);
 
 unsigned long long kernel_launches();
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);
 void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, unsigned long long* tiles,
                  unsigned long long* total, cudaStream_t s);
 uint32_t scan_tiles_needed(uint32_t n);
-void launch_mark_touched(const DArr& A, const DLat& L, const BrickBox& box, uint32_t* flags, int* err, cudaStream_t s);
+void launch_mark_touched(const DArr& A, const DLat& L, const BrickBox& box, uint32_t* flags, int* err, cudaStream_t s,
+                         const Scene* many = nullptr, uint32_t n_total = 0);
 void launch_classify_bricks(const DArr& A, const DLat& L, const BrickBox& box, const uint32_t* touched, uint32_t n,
-                            uint32_t* surface, cudaStream_t s);
-void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n, int4* keys, cudaStream_t s);
+                            uint32_t* surface, cudaStream_t s, const Scene* many = nullptr);
+void launch_cells_to_keys(const BrickBox& box, const uint32_t* cells, uint32_t n, int4* keys, cudaStream_t s,
+                          const Scene* many = nullptr);
 void launch_substates(const DArr& A, const DLat& L, const int4* keys, uint32_t n, uint32_t* rec, uint32_t* sampled,
-                      cudaStream_t s);
+                      cudaStream_t s, const Scene* many = nullptr);
 cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const uint32_t* work, uint32_t n,
-                          const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s);
+                          const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s,
+                          const Scene* many = nullptr);
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
-                          bool count, cudaStream_t s);
+                          bool count, cudaStream_t s, const Scene* many = nullptr);
 cudaError_t launch_mc(const DLat& L, uint32_t n, float* values, const uint32_t* rec, uint32_t* counts, const uint32_t* edge_off,
                       const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
-                      cudaStream_t s);
+                      cudaStream_t s, const int4* keys = nullptr,
+                      unsigned long long edge_cap = ~0ull, unsigned long long tri_cap = ~0ull,
+                      const Scene* many = nullptr);
 
 }  // namespace smb

@@ -19,8 +19,12 @@ int threads() {
     return h ? int(h) : 1;
 }
 
+static thread_local bool t_serial = false;
+SerialScope::SerialScope() : prev(t_serial) { t_serial = true; }
+SerialScope::~SerialScope() { t_serial = prev; }
+
 void parallel_for(size_t n, const std::function<void(size_t, int)>& f) {
-    size_t t = std::min<size_t>(size_t(threads()), n);
+    size_t t = t_serial ? 1 : std::min<size_t>(size_t(threads()), n);
     if (t <= 1) {
         for (size_t i = 0; i < n; i++) f(i, 0);
         return;

@@ -1,0 +1,54 @@
+// Host objects behind the opaque handles of include/sesmesh_b200_surface.h,
+// shared by the single-structure engine and the many-structure batch.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../../include/sesmesh_b200.h"
+#include "../../../include/sesmesh_b200_surface.h"
+#include "geom.hpp"
+#include "mesher.hpp"
+
+using smbh::Arrangement;
+using smbh::Component;
+using smbh::DeviceRefine;
+using smbh::Mesh;
+using smbh::MeshParams;
+
+struct smb_engine {
+    smb_device* dev = nullptr;
+    smb_surface_params params{};
+    Arrangement arr;
+    MeshParams mp;
+    smb_resident* res = nullptr;
+    smb_batch* batch = nullptr;
+    double t_geometry = 0, t_upload = 0;
+    // Host copies of the last device run.
+    std::vector<int32_t> keys;
+    std::vector<uint32_t> edge_off, edges, tri_off, tris;
+    std::vector<float> edge_vals, t, closest;
+    std::vector<uint32_t> feat, evals;
+    size_t touched = 0;
+    smb_batch_times times{};
+    double t_classify = 0;
+    const smb_mlp* warm = nullptr;  // warm start of fast-mode refinement
+    // Warm-start training rows of the last device run.
+    bool rows_ready = false;
+    std::vector<float> row_x, row_t;
+};
+
+struct smb_surface {
+    Mesh mesh;
+    std::vector<Component> comps;
+    smb_surface_stats stats{};
+    std::string obj;
+};
+
+
+// Host stages of one structure after its device run: placement of the
+// device's f32 roots (fast) or f64 refinement (exact), assembly,
+// validation, components and grouping; fills the statistics it can (sizes,
+// area, volume, evaluations, host stage times).  Error text or "".
+std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fast, const int32_t* keys, size_t nb,
+                           const uint32_t* edge_off, const uint32_t* edges, const float* edge_vals,
+                           const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s);

@@ -98,4 +98,12 @@ void set_threads(int n);
 int threads();
 void parallel_for(size_t n, const std::function<void(size_t, int)>& f);
 
+// While alive, parallel_for on this thread runs its loop in the calling
+// thread (for work that is itself one of many parallel tasks).
+struct SerialScope {
+    SerialScope();
+    ~SerialScope();
+    bool prev;
+};
+
 }  // namespace smbh

@@ -1,0 +1,628 @@
+// Many structures meshed in one device pass: the structures' arrangements
+// stay resident side by side, one classification pass covers every
+// structure's brick box, and the mesh stage (sub-block states, candidate
+// gather, sampling, marching cubes, fast-mode refinement) runs as one
+// captured CUDA graph whose kernels take their work from a device queue of
+// (structure, brick) items: every brick key carries its structure number,
+// and the kernels find that structure's arrangement, lattice and refinement
+// constants in per-structure descriptor arrays.  Buffers are sized from
+// per-brick caps chosen by an autotuner (brick edge, candidate caps, gather
+// block shape); a structure that meets a cap is flagged on the device and
+// meshed again on its own through the single-structure engine.
+//
+// sesmesh meshes one structure per compute_surface call (crates/sesmesh/
+// src/surface.rs:599-711); the per-structure results here are those of the
+// single-structure device path at the same brick edge (same kernels, same
+// arithmetic), with the host stages of crates/sesmesh/src/mesh/extract.rs:
+// 274-365 and 606-691 run per structure on the host threads.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+
+#include "../device/kernels.hpp"
+#include "../device/mlp.cuh"
+#include "../runtime.hpp"
+#include "engine.hpp"
+
+using namespace smb;
+using namespace smbh;
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+double ms_since(clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); }
+
+void set_err(char* err, size_t len, const char* fmt, ...) {
+    if (!err || !len) return;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(err, len, fmt, ap);
+    va_end(ap);
+}
+
+#define MCK(call)                                                                            \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            set_err(err, errlen, "%s: %s", #call, cudaGetErrorString(e_));                   \
+            return SMB_ERR_CUDA;                                                             \
+        }                                                                                    \
+    } while (0)
+
+// Candidate caps of one level: the gather's per-warp shared-memory lists,
+// the largest packed block of one sub-block (16-byte units; the sampler's
+// shared memory), and the list pools per sub-block of the batch.
+struct CapLevel {
+    GatherCaps caps;
+    uint32_t unit_cap;
+    uint32_t ids_per_sub, units_per_sub;
+};
+const CapLevel CAP_LEVELS[2] = {
+    {{192, 128, 384, 128}, 2048, 640, 320},
+    {{384, 256, 768, 256}, 8192, 1280, 640},
+};
+
+DLat lattice_for(const DLat& L0, int b) {
+    DLat L = L0;
+    L.b = b;
+    L.sub = b / 2;
+    L.spb = (b + 1) * (b + 1) * (b + 1);
+    L.rho_sub = 0.5 * std::sqrt(3.0) * double(L.sub) * L.h;  // kernel.rs:474
+    L.rho_brick = 0.5 * std::sqrt(3.0) * double(L.b) * L.h;  // lattice.rs:78-80
+    return L;
+}
+
+}  // namespace
+
+struct smb_multi {
+    smb_device* dev = nullptr;
+    std::vector<smb_engine*> eng;  // per structure: host arrangement, parameters, resident
+    const smb_mlp* warm = nullptr;
+    smb_multi_config cfg{};
+    bool tuned = false;
+    double t_setup = 0, t_tune = 0;
+    // Descriptors of the current brick edge.
+    int desc_brick = 0;
+    std::vector<DLat> lat;
+    std::vector<MeshParams> mp;
+    std::vector<BrickBox> box;
+    std::vector<unsigned long long> flag_off;
+    std::vector<uint32_t> sph_off;
+    DBuf d_arr, d_lat, d_rc, d_box, d_flag_off, d_sph_off, d_err, d_fail;
+    // Batch buffers.
+    DBuf flags, list, surf, cells, tiles, tot, keys, rec, sampled, work, values, counters, totals, ids, pack;
+    DBuf mc_counts, edge_off, tri_off, edges, edge_vals, tris, item_counts, item_off, item_edges;
+    DBuf e_t, e_feat, e_q, e_evals;
+    size_t edge_cap = 0, tri_cap = 0;
+    // Captured graph of the mesh-stage pass.
+    cudaGraphExec_t graph = nullptr;
+    size_t graph_bricks = 0;
+    smb_multi_config graph_cfg{};
+    const smb_mlp* graph_warm = nullptr;
+    bool graph_ok = true;
+    cudaEvent_t ev[2] = {};
+    // Results of the last run.
+    std::vector<std::unique_ptr<smb_surface>> out;
+    std::vector<double> latency;
+    std::vector<uint8_t> redone;
+    uint32_t n_bricks = 0;
+
+    std::vector<DBuf*> bufs() {
+        return {&d_arr, &d_lat, &d_rc, &d_box, &d_flag_off, &d_sph_off, &d_err, &d_fail, &flags, &list, &surf,
+                &cells, &tiles, &tot, &keys, &rec, &sampled, &work, &values, &counters, &totals, &ids, &pack,
+                &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &item_counts, &item_off, &item_edges,
+                &e_t, &e_feat, &e_q, &e_evals};
+    }
+    size_t n() const { return eng.size(); }
+};
+
+namespace {
+
+// Per-structure lattice, host mesh parameters, brick boxes and the device
+// descriptor arrays for brick edge b.
+int set_brick(smb_multi* m, int b, char* err, size_t errlen) {
+    if (m->desc_brick == b) return SMB_OK;
+    const size_t n = m->n();
+    m->lat.resize(n), m->mp.resize(n), m->box.resize(n);
+    m->flag_off.assign(n + 1, 0);
+    m->sph_off.assign(n + 1, 0);
+    std::vector<DArr> arr(n);
+    std::vector<RefineConsts> rc(n);
+    for (size_t i = 0; i < n; i++) {
+        smb_resident* r = m->eng[i]->res;
+        arr[i] = r->A;
+        rc[i] = r->rc;
+        m->lat[i] = lattice_for(r->L, b);
+        m->mp[i] = m->eng[i]->mp;
+        m->mp[i].b = b, m->mp[i].sub = b / 2;
+        // Box of the bricks any sphere can touch (as smb_classify).
+        const DLat& L = m->lat[i];
+        double rr = r->A.max_expanded + CLASSIFY_EPS, bh = double(L.b) * L.h, cells = 1;
+        for (int k = 0; k < 3; k++) {
+            double lo = std::floor((r->lo[k] - rr) / bh), hi = std::floor((r->hi[k] + rr) / bh);
+            if (!(std::fabs(lo) < double(KEY_BIAS) && std::fabs(hi) < double(KEY_BIAS)))
+                return set_err(err, errlen, "structure %zu: coordinates too far from the origin", i), SMB_ERR_RANGE;
+            m->box[i].lo[k] = (long long)lo;
+            m->box[i].n[k] = r->A.n ? uint32_t(hi - lo + 1) : 0;
+            cells *= double(m->box[i].n[k]);
+        }
+        m->flag_off[i + 1] = m->flag_off[i] + (unsigned long long)cells;
+        m->sph_off[i + 1] = m->sph_off[i] + r->A.n;
+    }
+    if (m->flag_off[n] >= (1ull << 31))
+        return set_err(err, errlen, "the structures' brick boxes hold %llu bricks, more than 2^31", m->flag_off[n]),
+               SMB_ERR_RANGE;
+    int rc_;
+    if ((rc_ = m->d_arr.reserve(n * sizeof(DArr), err, errlen)) ||
+        (rc_ = m->d_lat.reserve(n * sizeof(DLat), err, errlen)) ||
+        (rc_ = m->d_rc.reserve(n * sizeof(RefineConsts), err, errlen)) ||
+        (rc_ = m->d_box.reserve(n * sizeof(BrickBox), err, errlen)) ||
+        (rc_ = m->d_flag_off.reserve((n + 1) * 8, err, errlen)) ||
+        (rc_ = m->d_sph_off.reserve((n + 1) * 4, err, errlen)) || (rc_ = m->d_err.reserve(n * 4, err, errlen)) ||
+        (rc_ = m->d_fail.reserve(n * 4, err, errlen)))
+        return rc_;
+    cudaStream_t s = m->dev->stream;
+    MCK(cudaMemcpyAsync(m->d_arr.p, arr.data(), n * sizeof(DArr), cudaMemcpyHostToDevice, s));
+    MCK(cudaMemcpyAsync(m->d_lat.p, m->lat.data(), n * sizeof(DLat), cudaMemcpyHostToDevice, s));
+    MCK(cudaMemcpyAsync(m->d_rc.p, rc.data(), n * sizeof(RefineConsts), cudaMemcpyHostToDevice, s));
+    MCK(cudaMemcpyAsync(m->d_box.p, m->box.data(), n * sizeof(BrickBox), cudaMemcpyHostToDevice, s));
+    MCK(cudaMemcpyAsync(m->d_flag_off.p, m->flag_off.data(), (n + 1) * 8, cudaMemcpyHostToDevice, s));
+    MCK(cudaMemcpyAsync(m->d_sph_off.p, m->sph_off.data(), (n + 1) * 4, cudaMemcpyHostToDevice, s));
+    MCK(cudaStreamSynchronize(s));
+    m->desc_brick = b;
+    return SMB_OK;
+}
+
+Scene scene_of(smb_multi* m) {
+    Scene S{};
+    S.arr = m->d_arr.as<DArr>();
+    S.lat = m->d_lat.as<DLat>();
+    S.rc = m->d_rc.as<RefineConsts>();
+    S.box = m->d_box.as<BrickBox>();
+    S.flag_off = m->d_flag_off.as<unsigned long long>();
+    S.sph_off = m->d_sph_off.as<uint32_t>();
+    S.n_struct = uint32_t(m->n());
+    S.n_work = m->totals.as<unsigned long long>();
+    S.err = m->d_err.as<int>();
+    S.fail = m->d_fail.as<uint32_t>();
+    return S;
+}
+
+// Every structure's surface bricks in one pass (lattice::touched_bricks +
+// surface_bricks per structure); keys (x, y, z, structure) in structure
+// order, each structure's in packed-key order.
+int classify_all(smb_multi* m, char* err, size_t errlen) {
+    const size_t n = m->n();
+    cudaStream_t s = m->dev->stream;
+    const uint32_t nf = uint32_t(m->flag_off[n]);
+    int rc;
+    if ((rc = m->flags.reserve(size_t(nf) * 4 + 4, err, errlen)) || (rc = m->list.reserve(size_t(nf) * 4 + 4, err, errlen)) ||
+        (rc = m->surf.reserve(size_t(nf) * 4 + 4, err, errlen)) || (rc = m->cells.reserve(size_t(nf) * 4 + 4, err, errlen)) ||
+        (rc = m->tiles.reserve(size_t(scan_tiles_needed(std::max(nf, 8u))) * 8 + 64, err, errlen)) ||
+        (rc = m->tot.reserve(16, err, errlen)) || (rc = m->totals.reserve(64, err, errlen)))
+        return rc;
+    Scene S = scene_of(m);
+    MCK(cudaMemsetAsync(m->flags.p, 0, size_t(nf) * 4 + 4, s));
+    MCK(cudaMemsetAsync(m->surf.p, 0, size_t(nf) * 4 + 4, s));
+    MCK(cudaMemsetAsync(m->d_err.p, 0, n * 4, s));
+    launch_mark_touched(DArr{}, DLat{}, BrickBox{}, m->flags.as<uint32_t>(), nullptr, s, &S, m->sph_off[n]);
+    launch_scan(m->flags.as<uint32_t>(), nf, nullptr, m->list.as<uint32_t>(), m->tiles.as<unsigned long long>(),
+                m->tot.as<unsigned long long>(), s);
+    unsigned long long n_touched = 0;
+    std::vector<int> kerr(n);
+    MCK(cudaMemcpyAsync(&n_touched, m->tot.p, 8, cudaMemcpyDeviceToHost, s));
+    MCK(cudaMemcpyAsync(kerr.data(), m->d_err.p, n * 4, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < n; i++)
+        if (kerr[i]) return set_err(err, errlen, "structure %zu: coordinates too far from the origin", i), SMB_ERR_RANGE;
+    launch_classify_bricks(DArr{}, DLat{}, BrickBox{}, m->list.as<uint32_t>(), uint32_t(n_touched),
+                           m->surf.as<uint32_t>(), s, &S);
+    launch_scan(m->surf.as<uint32_t>(), nf, nullptr, m->cells.as<uint32_t>(), m->tiles.as<unsigned long long>(),
+                m->tot.as<unsigned long long>(), s);
+    unsigned long long n_surface = 0;
+    MCK(cudaMemcpyAsync(&n_surface, m->tot.p, 8, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+    if ((rc = m->keys.reserve(std::max<size_t>(n_surface, 1) * sizeof(int4), err, errlen))) return rc;
+    launch_cells_to_keys(BrickBox{}, m->cells.as<uint32_t>(), uint32_t(n_surface), m->keys.as<int4>(), s, &S);
+    m->n_bricks = uint32_t(n_surface);
+    return SMB_OK;
+}
+
+// Buffers of the mesh-stage pass for n_bricks surface bricks at the
+// configured caps.
+int reserve_pass(smb_multi* m, char* err, size_t errlen) {
+    const size_t nb = std::max<uint32_t>(m->n_bricks, 1), nsub = nb * 8;
+    const int b = m->cfg.brick;
+    const CapLevel& C = CAP_LEVELS[m->cfg.caps_level];
+    const size_t spb = size_t(b + 1) * (b + 1) * (b + 1);
+    m->edge_cap = std::min<size_t>(size_t(0xFFFFFFF0u), nb * size_t(3) * b * b);
+    m->tri_cap = std::min<size_t>(size_t(0xFFFFFFF0u), 2 * m->edge_cap);
+    int rc;
+    if ((rc = m->rec.reserve(nsub * REC_WORDS * 4, err, errlen)) || (rc = m->sampled.reserve(nsub * 4, err, errlen)) ||
+        (rc = m->work.reserve(nsub * 4, err, errlen)) || (rc = m->values.reserve(nb * spb * 4, err, errlen)) ||
+        (rc = m->tiles.reserve(size_t(scan_tiles_needed(uint32_t(nsub))) * 8 + 64, err, errlen)) ||
+        (rc = m->counters.reserve(CNT_N * 8, err, errlen)) ||
+        (rc = m->ids.reserve(nsub / 2 * C.ids_per_sub * 4, err, errlen)) ||
+        (rc = m->pack.reserve(nsub / 2 * C.units_per_sub * 16, err, errlen)) ||
+        (rc = m->mc_counts.reserve(nb * 8, err, errlen)) || (rc = m->edge_off.reserve(nb * 4 + 4, err, errlen)) ||
+        (rc = m->tri_off.reserve(nb * 4 + 4, err, errlen)) || (rc = m->edges.reserve(m->edge_cap * 4, err, errlen)) ||
+        (rc = m->edge_vals.reserve(m->edge_cap * 8, err, errlen)) ||
+        (rc = m->tris.reserve(m->tri_cap * 12, err, errlen)) || (rc = m->item_counts.reserve(nsub * 4, err, errlen)) ||
+        (rc = m->item_off.reserve(nsub * 4 + 4, err, errlen)) ||
+        (rc = m->item_edges.reserve(m->edge_cap * 4, err, errlen)) || (rc = m->e_t.reserve(m->edge_cap * 4, err, errlen)) ||
+        (rc = m->e_feat.reserve(m->edge_cap * 4, err, errlen)) || (rc = m->e_q.reserve(m->edge_cap * 12, err, errlen)) ||
+        (rc = m->e_evals.reserve(m->edge_cap * 4, err, errlen)))
+        return rc;
+    return SMB_OK;
+}
+
+// The mesh-stage pass over every structure's surface bricks, all sizes
+// fixed by n_bricks and the caps (no host synchronisation inside), as one
+// stream of launches: recorded once into a CUDA graph, then replayed.
+int enqueue_pass(smb_multi* m, char* err, size_t errlen) {
+    cudaStream_t s = m->dev->stream;
+    smb_device* d = m->dev;
+    const uint32_t nb = m->n_bricks, nsub = nb * 8;
+    const int b = m->cfg.brick;
+    const CapLevel& C = CAP_LEVELS[m->cfg.caps_level];
+    const size_t spb = size_t(b + 1) * (b + 1) * (b + 1);
+    Scene S = scene_of(m);
+    const int4* keys = m->keys.as<int4>();
+    unsigned long long* cnt = m->counters.as<unsigned long long>();
+    unsigned long long* tot = m->totals.as<unsigned long long>();
+    DLat L{};  // per-structure lattices come from the scene; b and spb are shared
+    L.b = b, L.sub = b / 2, L.spb = int(spb);
+    MCK(cudaMemsetAsync(cnt, 0, CNT_N * 8, s));
+    MCK(cudaMemsetAsync(m->d_fail.p, 0, m->n() * 4, s));
+    MCK(cudaMemsetAsync(m->values.p, 0, size_t(nb) * spb * 4, s));
+    launch_substates(DArr{}, DLat{}, keys, nb, m->rec.as<uint32_t>(), m->sampled.as<uint32_t>(), s, &S);
+    launch_scan(m->sampled.as<uint32_t>(), nsub, nullptr, m->work.as<uint32_t>(), m->tiles.as<unsigned long long>(),
+                tot, s);
+    GatherOut O{m->rec.as<uint32_t>(), m->ids.as<uint32_t>(), m->pack.as<uint4>(), nullptr, cnt,
+                m->ids.cap / 4, m->pack.cap / 16, C.unit_cap, m->d_fail.as<uint32_t>()};
+    cudaError_t e = launch_gather(DArr{}, DLat{}, keys, m->work.as<uint32_t>(), nsub, O, C.caps,
+                                  int(m->cfg.gather_warps), s, &S);
+    if (e != cudaSuccess) return set_err(err, errlen, "gather launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    e = launch_sample(DLat{}, keys, m->work.as<uint32_t>(), nsub, m->rec.as<uint32_t>(), m->pack.as<uint4>(),
+                      C.unit_cap, m->values.as<float>(), cnt, true, false, s, &S);
+    if (e != cudaSuccess) return set_err(err, errlen, "sample launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    e = launch_mc(L, nb, m->values.as<float>(), m->rec.as<uint32_t>(), m->mc_counts.as<uint32_t>(), nullptr, nullptr,
+                  nullptr, nullptr, nullptr, false, s, keys, ~0ull, ~0ull, &S);
+    if (e != cudaSuccess) return set_err(err, errlen, "mc launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    launch_scan(m->mc_counts.as<uint32_t>(), nb, m->edge_off.as<uint32_t>(), nullptr, m->tiles.as<unsigned long long>(),
+                tot + 1, s);
+    launch_scan(m->mc_counts.as<uint32_t>() + nb, nb, m->tri_off.as<uint32_t>(), nullptr,
+                m->tiles.as<unsigned long long>(), tot + 2, s);
+    launch_put_total(m->edge_off.as<uint32_t>() + nb, tot + 1, s);
+    launch_put_total(m->tri_off.as<uint32_t>() + nb, tot + 2, s);
+    e = launch_mc(L, nb, m->values.as<float>(), m->rec.as<uint32_t>(), nullptr, m->edge_off.as<uint32_t>(),
+                  m->tri_off.as<uint32_t>(), m->edges.as<uint32_t>(), m->edge_vals.as<float2>(), m->tris.as<uint32_t>(),
+                  true, s, keys, m->edge_cap, m->tri_cap, &S);
+    if (e != cudaSuccess) return set_err(err, errlen, "mc launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    launch_item_edges(L, m->work.as<uint32_t>(), nsub, m->rec.as<uint32_t>(), m->edge_off.as<uint32_t>(),
+                      m->edges.as<uint32_t>(), m->item_counts.as<uint32_t>(), m->item_off.as<uint32_t>(),
+                      m->item_edges.as<uint32_t>(), m->tiles.as<unsigned long long>(), tot + 3, cnt, s, &S, keys);
+    const int mode = m->warm ? REFINE_MLP : REFINE_PLAIN;
+    MlpDev md{nullptr, nullptr, nullptr};
+    if (m->warm) md = mlp_dev(m->warm);
+    const size_t cand = size_t(C.unit_cap) * 16 + 64;
+    e = launch_refine(DArr{}, DLat{}, RefineConsts{}, keys, m->work.as<uint32_t>(), m->rec.as<uint32_t>(),
+                      m->ids.as<uint32_t>(), m->edges.as<uint32_t>(), m->edge_vals.as<float2>(),
+                      m->item_off.as<uint32_t>(), m->item_edges.as<uint32_t>(), nsub, m->e_t.as<float>(),
+                      m->e_feat.as<uint32_t>(), m->e_q.as<float>(), m->e_evals.as<uint32_t>(), cand, mode,
+                      m->values.as<float>(), m->warm ? &md : nullptr, nullptr, cnt, d->info.multiprocessors,
+                      d->smem_optin, s, nullptr, &S);
+    if (e != cudaSuccess) return set_err(err, errlen, "refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    return SMB_OK;
+}
+
+// Runs the pass: from the captured graph when it matches the current sizes
+// and configuration, else records it (and replays it); direct launches if
+// recording is refused.
+int run_pass(smb_multi* m, float* device_ms, char* err, size_t errlen) {
+    cudaStream_t s = m->dev->stream;
+    int rc;
+    if ((rc = reserve_pass(m, err, errlen))) return rc;
+    const bool same = m->graph && m->graph_bricks == m->n_bricks && m->graph_cfg.brick == m->cfg.brick &&
+                      m->graph_cfg.caps_level == m->cfg.caps_level &&
+                      m->graph_cfg.gather_warps == m->cfg.gather_warps && m->graph_warm == m->warm;
+    if (!m->ev[0]) cudaEventCreate(&m->ev[0]), cudaEventCreate(&m->ev[1]);
+    if (!same && m->n_bricks) {
+        if (m->graph) cudaGraphExecDestroy(m->graph), m->graph = nullptr;
+        // One direct pass first: sets the kernels' attributes outside the
+        // recording and checks the launches.
+        MCK(cudaEventRecord(m->ev[0], s));
+        if ((rc = enqueue_pass(m, err, errlen))) return rc;
+        MCK(cudaEventRecord(m->ev[1], s));
+        MCK(cudaStreamSynchronize(s));
+        cudaGraph_t g = nullptr;
+        if (m->graph_ok && cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            char e2[256] = {0};
+            int prc = enqueue_pass(m, e2, sizeof e2);
+            cudaError_t ce = cudaStreamEndCapture(s, &g);
+            if (prc == SMB_OK && ce == cudaSuccess && g && cudaGraphInstantiate(&m->graph, g, 0) == cudaSuccess) {
+                m->graph_bricks = m->n_bricks;
+                m->graph_cfg = m->cfg;
+                m->graph_warm = m->warm;
+            } else {
+                m->graph = nullptr;
+                m->graph_ok = false;
+                cudaGetLastError();
+            }
+            if (g) cudaGraphDestroy(g);
+        }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]);
+        *device_ms = ms;
+        return SMB_OK;
+    }
+    MCK(cudaEventRecord(m->ev[0], s));
+    if (m->n_bricks) {
+        if (m->graph) MCK(cudaGraphLaunch(m->graph, s));
+        else if ((rc = enqueue_pass(m, err, errlen))) return rc;
+    }
+    MCK(cudaEventRecord(m->ev[1], s));
+    MCK(cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]);
+    *device_ms = ms;
+    return SMB_OK;
+}
+
+// Device part for the current configuration: classification and the pass;
+// *fails gets the number of structures over a cap.
+int device_run(smb_multi* m, double* classify_ms, float* device_ms, size_t* fails, char* err, size_t errlen) {
+    int rc;
+    if ((rc = set_brick(m, m->cfg.brick, err, errlen))) return rc;
+    auto t0 = clk::now();
+    if ((rc = classify_all(m, err, errlen))) return rc;
+    MCK(cudaStreamSynchronize(m->dev->stream));
+    *classify_ms = ms_since(t0);
+    if ((rc = run_pass(m, device_ms, err, errlen))) return rc;
+    std::vector<uint32_t> f(m->n());
+    MCK(cudaMemcpy(f.data(), m->d_fail.p, m->n() * 4, cudaMemcpyDeviceToHost));
+    unsigned long long t3[4] = {0, 0, 0, 0};
+    MCK(cudaMemcpy(t3, m->totals.p, 32, cudaMemcpyDeviceToHost));
+    size_t k = 0;
+    for (uint32_t v : f) k += v != 0;
+    *fails = k;
+    return SMB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int smb_multi_new(smb_device* dev, size_t n, const double* const* xyzr, const size_t* counts,
+                  const smb_surface_params* params, const smb_multi_config* cfg, smb_multi** out, char* err,
+                  size_t errlen) {
+    if (!dev || !out || (n && (!xyzr || !counts || !params))) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
+    *out = nullptr;
+    if (n == 0 || n >= (size_t(1) << 31)) return set_err(err, errlen, "structure count must be 1..2^31"), SMB_ERR_ARG;
+    smb_multi_config c = cfg ? *cfg : smb_multi_config{};
+    if (c.brick && (c.brick < 4 || c.brick > 32 || c.brick % 2))
+        return set_err(err, errlen, "brick must be 0 (tuned) or even and 4..32, got %u", c.brick), SMB_ERR_ARG;
+    if (c.caps_level > 1) return set_err(err, errlen, "caps level must be 0 or 1"), SMB_ERR_ARG;
+    if (c.gather_warps && c.gather_warps != 1 && c.gather_warps != 2 && c.gather_warps != 4 && c.gather_warps != 8)
+        return set_err(err, errlen, "gather warps must be 0 (tuned), 1, 2, 4 or 8"), SMB_ERR_ARG;
+    for (size_t i = 0; i < n; i++)
+        if (params[i].refine != SMB_REFINE_FAST)
+            return set_err(err, errlen, "structure %zu: the batch meshes in fast mode", i), SMB_ERR_ARG;
+    auto t0 = clk::now();
+    auto m = std::make_unique<smb_multi>();
+    m->dev = dev;
+    dev_retain(dev);
+    m->cfg = c;
+    m->tuned = c.brick != 0 && c.gather_warps != 0;
+    m->eng.assign(n, nullptr);
+    for (size_t i = 0; i < n; i++) {
+        smb_surface_params p = params[i];
+        p.brick_size = c.brick ? c.brick : 8;
+        int rc = smb_engine_new(dev, xyzr[i], counts[i], &p, &m->eng[i], err, errlen);
+        if (rc != SMB_OK) {
+            char tmp[512];
+            snprintf(tmp, sizeof tmp, "structure %zu: %s", i, err ? err : "");
+            set_err(err, errlen, "%s", tmp);
+            smb_multi_free(m.release());
+            return rc;
+        }
+    }
+    if (!m->cfg.gather_warps) m->cfg.gather_warps = 4;
+    if (!m->cfg.brick) m->cfg.brick = 8;
+    m->t_setup = ms_since(t0);
+    *out = m.release();
+    return SMB_OK;
+}
+
+void smb_multi_free(smb_multi* m) {
+    if (!m) return;
+    cudaSetDevice(m->dev->index);
+    cudaStreamSynchronize(m->dev->stream);
+    if (m->graph) cudaGraphExecDestroy(m->graph);
+    for (auto& ev : m->ev)
+        if (ev) cudaEventDestroy(ev);
+    for (DBuf* b : m->bufs()) b->release();
+    for (smb_engine* e : m->eng) smb_engine_free(e);
+    smb_device* d = m->dev;
+    delete m;
+    dev_release(d);
+}
+
+int smb_multi_set_warm_start(smb_multi* m, const smb_mlp* mlp) {
+    if (!m) return SMB_ERR_ARG;
+    m->warm = mlp;
+    for (smb_engine* e : m->eng) smb_engine_set_warm_start(e, mlp);
+    return SMB_OK;
+}
+
+int smb_multi_tune(smb_multi* m, char* err, size_t errlen) {
+    if (!m) return SMB_ERR_ARG;
+    if (cudaSetDevice(m->dev->index) != cudaSuccess) return set_err(err, errlen, "cudaSetDevice failed"), SMB_ERR_CUDA;
+    auto t0 = clk::now();
+    // Candidates: brick edge 8 or 16, candidate caps level 0 or 1, 2 or 4
+    // warps per gather block.  Score: device time of classification and
+    // pass, plus the single-structure cost of every structure over a cap
+    // (taken as the pass's time per structure, times four).
+    smb_multi_config best = m->cfg;
+    double best_score = 1e300;
+    const int bricks[2] = {8, 16};
+    const uint32_t warps[2] = {2, 4};
+    for (int b : bricks)
+        for (uint32_t lvl = 0; lvl < 2; lvl++)
+            for (uint32_t w : warps) {
+                m->cfg.brick = uint32_t(b), m->cfg.caps_level = lvl, m->cfg.gather_warps = w;
+                double cms = 0, score = 0;
+                float dms = 0;
+                size_t fails = 0;
+                int rc = device_run(m, &cms, &dms, &fails, err, errlen);
+                if (rc == SMB_OK) rc = run_pass(m, &dms, err, errlen);  // a replay, the steady-state time
+                if (rc != SMB_OK) continue;
+                score = cms + dms + 4.0 * (cms + dms) / double(m->n()) * double(fails);
+                if (score < best_score) best_score = score, best = m->cfg;
+            }
+    if (best_score >= 1e300) return set_err(err, errlen, "no configuration ran"), SMB_ERR_CUDA;
+    m->cfg = best;
+    m->tuned = true;
+    m->t_tune = ms_since(t0);
+    return SMB_OK;
+}
+
+int smb_multi_config_get(const smb_multi* m, smb_multi_config* out) {
+    if (!m || !out) return SMB_ERR_ARG;
+    *out = m->cfg;
+    return SMB_OK;
+}
+
+int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen) {
+    if (!m) return SMB_ERR_ARG;
+    if (cudaSetDevice(m->dev->index) != cudaSuccess) return set_err(err, errlen, "cudaSetDevice failed"), SMB_ERR_CUDA;
+    int rc;
+    if (!m->tuned && (rc = smb_multi_tune(m, err, errlen))) return rc;
+    auto t_start = clk::now();
+    double cms = 0;
+    float dms = 0;
+    size_t fails = 0;
+    if ((rc = device_run(m, &cms, &dms, &fails, err, errlen))) return rc;
+    // Results to the host.
+    auto t1 = clk::now();
+    const size_t n = m->n(), nb = m->n_bricks;
+    unsigned long long t3[4] = {0, 0, 0, 0};
+    MCK(cudaMemcpy(t3, m->totals.p, 32, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> fail(n);
+    MCK(cudaMemcpy(fail.data(), m->d_fail.p, n * 4, cudaMemcpyDeviceToHost));
+    const size_t ne = std::min<size_t>(t3[1], m->edge_cap), nt = std::min<size_t>(t3[2], m->tri_cap);
+    std::vector<int4> keys4(nb);
+    std::vector<uint32_t> eo(nb + 1, 0), to(nb + 1, 0), edges(ne), tris(3 * nt), feat(ne), evals(ne);
+    std::vector<float> ev(2 * ne), t(ne), q(3 * ne);
+    if (nb) {
+        MCK(cudaMemcpy(keys4.data(), m->keys.p, nb * sizeof(int4), cudaMemcpyDeviceToHost));
+        MCK(cudaMemcpy(eo.data(), m->edge_off.p, (nb + 1) * 4, cudaMemcpyDeviceToHost));
+        MCK(cudaMemcpy(to.data(), m->tri_off.p, (nb + 1) * 4, cudaMemcpyDeviceToHost));
+    }
+    if (ne) {
+        MCK(cudaMemcpy(edges.data(), m->edges.p, ne * 4, cudaMemcpyDeviceToHost));
+        MCK(cudaMemcpy(ev.data(), m->edge_vals.p, ne * 8, cudaMemcpyDeviceToHost));
+        MCK(cudaMemcpy(t.data(), m->e_t.p, ne * 4, cudaMemcpyDeviceToHost));
+        MCK(cudaMemcpy(feat.data(), m->e_feat.p, ne * 4, cudaMemcpyDeviceToHost));
+        MCK(cudaMemcpy(q.data(), m->e_q.p, ne * 12, cudaMemcpyDeviceToHost));
+        MCK(cudaMemcpy(evals.data(), m->e_evals.p, ne * 4, cudaMemcpyDeviceToHost));
+    }
+    if (nt) MCK(cudaMemcpy(tris.data(), m->tris.p, nt * 12, cudaMemcpyDeviceToHost));
+    double t_d2h = ms_since(t1);
+    // Brick ranges per structure (keys are in structure order).
+    std::vector<size_t> b0(n + 1, nb);
+    for (size_t i = nb; i-- > 0;) b0[size_t(keys4[i].w)] = i;
+    for (size_t i = n; i-- > 0;) b0[i] = std::min(b0[i], b0[i + 1]);
+    // Host stages per structure, on the host threads; a structure over a cap
+    // (or whose output runs past the edge or triangle buffers) is redone on
+    // its own afterwards.
+    auto t2 = clk::now();
+    m->out.clear();
+    m->out.resize(n);
+    m->latency.assign(n, 0.0);
+    m->redone.assign(n, 0);
+    std::vector<std::string> errs(n);
+    for (size_t i = 0; i < n; i++)
+        if (fail[i] || eo[b0[i + 1]] > ne || to[b0[i + 1]] > nt) m->redone[i] = 1;
+    parallel_for(n, [&](size_t i, int) {
+        if (m->redone[i]) return;
+        SerialScope serial;
+        const size_t lo = b0[i], hi = b0[i + 1], nbi = hi - lo;
+        std::vector<int32_t> k3(3 * nbi);
+        std::vector<uint32_t> leo(nbi + 1), lto(nbi + 1);
+        for (size_t j = 0; j < nbi; j++)
+            k3[3 * j] = keys4[lo + j].x, k3[3 * j + 1] = keys4[lo + j].y, k3[3 * j + 2] = keys4[lo + j].z;
+        for (size_t j = 0; j <= nbi; j++) leo[j] = eo[lo + j] - eo[lo], lto[j] = to[lo + j] - to[lo];
+        const size_t e0 = eo[lo], tr0 = to[lo];
+        auto s = std::make_unique<smb_surface>();
+        smb_engine* e = m->eng[i];
+        std::string msg = finish_surface(e->arr, m->mp[i], true, k3.data(), nbi, leo.data(), edges.data() + e0,
+                                         ev.data() + 2 * e0, lto.data(), tris.data() + 3 * tr0,
+                                         DeviceRefine{t.data() + e0, feat.data() + e0, q.data() + 3 * e0,
+                                                      evals.data() + e0},
+                                         *s);
+        if (!msg.empty()) {
+            errs[i] = msg;
+            return;
+        }
+        s->stats.t_geometry = e->t_geometry;
+        s->stats.t_upload = e->t_upload;
+        m->out[i] = std::move(s);
+        m->latency[i] = ms_since(t_start);
+    });
+    for (size_t i = 0; i < n; i++)
+        if (!errs[i].empty()) return set_err(err, errlen, "structure %zu: %s", i, errs[i].c_str()), SMB_ERR_STATE;
+    double t_host = ms_since(t2);
+    auto t3b = clk::now();
+    size_t n_redone = 0;
+    for (size_t i = 0; i < n; i++) {
+        if (!m->redone[i]) continue;
+        n_redone++;
+        smb_surface* s = nullptr;
+        smb_engine* e = m->eng[i];
+        // The engine meshes on its own, at the batch's brick edge, with
+        // retries on every cap.
+        e->res->L = m->lat[i];
+        e->mp = m->mp[i];
+        if ((rc = smb_engine_mesh(e, &s, err, errlen))) return rc;
+        m->out[i].reset(s);
+        m->latency[i] = ms_since(t_start);
+    }
+    double t_redo = ms_since(t3b);
+    if (times) {
+        smb_multi_times& T = *times;
+        T = smb_multi_times{};
+        T.structures = n;
+        T.redone = n_redone;
+        T.bricks = nb;
+        T.samples = size_t(nb) * size_t(m->cfg.brick + 1) * size_t(m->cfg.brick + 1) * size_t(m->cfg.brick + 1);
+        T.t_setup = m->t_setup;
+        T.t_tune = m->t_tune;
+        T.t_classify = cms;
+        T.t_device = dms;
+        T.t_d2h = t_d2h;
+        T.t_host = t_host;
+        T.t_redo = t_redo;
+        T.t_total = ms_since(t_start);
+        T.graph = m->graph != nullptr;
+    }
+    return SMB_OK;
+}
+
+smb_surface* smb_multi_surface(smb_multi* m, size_t i) {
+    if (!m || i >= m->out.size()) return nullptr;
+    return m->out[i].get();
+}
+
+int smb_multi_latency(const smb_multi* m, double* ms) {
+    if (!m || !ms) return SMB_ERR_ARG;
+    if (m->latency.size() != m->n()) return SMB_ERR_STATE;
+    std::copy(m->latency.begin(), m->latency.end(), ms);
+    return SMB_OK;
+}
+
+}  // extern "C"

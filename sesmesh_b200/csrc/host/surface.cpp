@@ -13,6 +13,7 @@
 #include "../../../include/sesmesh_b200_surface.h"
 #include "../runtime.hpp"
 #include "geom.hpp"
+#include "engine.hpp"
 #include "mesher.hpp"
 
 using namespace smbh;
@@ -32,34 +33,49 @@ void set_err(char* err, size_t len, const char* fmt, ...) {
 
 }  // namespace
 
-struct smb_engine {
-    smb_device* dev = nullptr;
-    smb_surface_params params{};
-    Arrangement arr;
-    MeshParams mp;
-    smb_resident* res = nullptr;
-    smb_batch* batch = nullptr;
-    double t_geometry = 0, t_upload = 0;
-    // Host copies of the last device run.
-    std::vector<int32_t> keys;
-    std::vector<uint32_t> edge_off, edges, tri_off, tris;
-    std::vector<float> edge_vals, t, closest;
-    std::vector<uint32_t> feat, evals;
-    size_t touched = 0;
-    smb_batch_times times{};
-    double t_classify = 0;
-    const smb_mlp* warm = nullptr;  // warm start of fast-mode refinement
-    // Warm-start training rows of the last device run.
-    bool rows_ready = false;
-    std::vector<float> row_x, row_t;
-};
-
-struct smb_surface {
-    Mesh mesh;
-    std::vector<Component> comps;
-    smb_surface_stats stats{};
-    std::string obj;
-};
+// Host stages of one structure after its device run: placement of the
+// device's f32 roots (fast) or f64 refinement (exact), assembly,
+// validation, components and grouping; fills the statistics it can (sizes,
+// area, volume, evaluations, host stage times).  Error text or "".
+std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fast, const int32_t* keys, size_t nb,
+                           const uint32_t* edge_off, const uint32_t* edges, const float* edge_vals,
+                           const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s) {
+    auto t1 = clk::now();
+    MeshOut mo;
+    if (fast) place_fast(arr, mp, keys, nb, edge_off, edges, edge_vals, dev, mo);
+    else refine_exact(arr, mp, keys, nb, edge_off, edges, edge_vals, mo);
+    double t_host = ms_since(t1);
+    auto t2 = clk::now();
+    Mesh& mesh = s.mesh;
+    std::string m = assemble(keys, nb, edge_off, edges, tri_off, tris, mesh);
+    if (!m.empty()) return m;
+    mesh.positions.swap(mo.positions);
+    mesh.normals.swap(mo.normals);
+    mesh.vertex_atom.swap(mo.atoms);
+    mesh.vertex_patch.swap(mo.patches);
+    double t_assemble = ms_since(t2);
+    auto t3 = clk::now();
+    EdgeUses uses;
+    size_t bad = defects(mesh, &uses);
+    if (bad) return "mesh failed validation (" + std::to_string(bad) + " defects)";
+    components_and_group(mesh, s.comps, &uses);
+    double t_measure = ms_since(t3);
+    smb_surface_stats& st = s.stats;
+    st.spheres = arr.n;
+    st.surface_bricks = nb;
+    st.samples = nb * size_t(mp.b + 1) * size_t(mp.b + 1) * size_t(mp.b + 1);
+    st.vertices = mesh.positions.size();
+    st.triangles = mesh.triangles.size();
+    st.components = s.comps.size();
+    for (auto& c : s.comps) st.area += c.area, st.volume += c.volume, st.euler += c.euler;
+    for (uint32_t v : mo.evals) st.refine_evaluations += v;
+    for (uint32_t v : mo.cpu_refined) st.refine_cpu_edges += v;
+    st.t_host_refine = t_host;
+    st.t_assemble = t_assemble;
+    st.t_measure = t_measure;
+    st.host_threads = threads();
+    return "";
+}
 
 extern "C" {
 
@@ -244,41 +260,13 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
             return set_err(err, errlen, "edge results copy"), rc;
     }
     double t_d2h = ms_since(t0);
-    auto t1 = clk::now();
-    MeshOut mo;
-    if (fast)
-        place_fast(e->arr, e->mp, e->keys.data(), nb, e->edge_off.data(), e->edges.data(), e->edge_vals.data(),
-                   DeviceRefine{e->t.data(), e->feat.data(), e->closest.data(), e->evals.data()}, mo);
-    else
-        refine_exact(e->arr, e->mp, e->keys.data(), nb, e->edge_off.data(), e->edges.data(), e->edge_vals.data(), mo);
-    double t_host = ms_since(t1);
-    auto t2 = clk::now();
     auto s = std::make_unique<smb_surface>();
-    Mesh& mesh = s->mesh;
-    std::string m = assemble(e->keys.data(), nb, e->edge_off.data(), e->edges.data(), e->tri_off.data(), e->tris.data(), mesh);
+    std::string m = finish_surface(e->arr, e->mp, fast, e->keys.data(), nb, e->edge_off.data(), e->edges.data(),
+                                   e->edge_vals.data(), e->tri_off.data(), e->tris.data(),
+                                   DeviceRefine{e->t.data(), e->feat.data(), e->closest.data(), e->evals.data()}, *s);
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_STATE;
-    mesh.positions.swap(mo.positions);
-    mesh.normals.swap(mo.normals);
-    mesh.vertex_atom.swap(mo.atoms);
-    mesh.vertex_patch.swap(mo.patches);
-    double t_assemble = ms_since(t2);
-    auto t3 = clk::now();
-    EdgeUses uses;
-    size_t bad = defects(mesh, &uses);
-    if (bad) return set_err(err, errlen, "mesh failed validation (%zu defects)", bad), SMB_ERR_STATE;
-    components_and_group(mesh, s->comps, &uses);
-    double t_measure = ms_since(t3);
     smb_surface_stats& st = s->stats;
-    st.spheres = e->arr.n;
     st.touched_bricks = e->touched;
-    st.surface_bricks = nb;
-    st.samples = nb * size_t(e->mp.b + 1) * size_t(e->mp.b + 1) * size_t(e->mp.b + 1);
-    st.vertices = mesh.positions.size();
-    st.triangles = mesh.triangles.size();
-    st.components = s->comps.size();
-    for (auto& c : s->comps) st.area += c.area, st.volume += c.volume, st.euler += c.euler;
-    for (uint32_t v : mo.evals) st.refine_evaluations += v;
-    for (uint32_t v : mo.cpu_refined) st.refine_cpu_edges += v;
     st.t_geometry = e->t_geometry;
     st.t_upload = e->t_upload;
     st.t_classify = e->t_classify;
@@ -288,11 +276,7 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
     st.t_mc = e->times.mc;
     st.t_device = e->t_classify + e->times.total;
     st.t_d2h = t_d2h;
-    st.t_host_refine = t_host;
-    st.t_assemble = t_assemble;
-    st.t_measure = t_measure;
-    st.t_mesh_stage = ms_since(t_all) - t_assemble - t_measure;
-    st.host_threads = threads();
+    st.t_mesh_stage = ms_since(t_all) - st.t_assemble - st.t_measure;
     *out = s.release();
     return SMB_OK;
 }

@@ -547,7 +547,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
             return rc;
         CK(cudaMemsetAsync(b->counters.p, 0, CNT_N * 8, s));
         GatherOut O{b->rec.as<uint32_t>(), b->ids.as<uint32_t>(), b->pack.as<uint4>(), b->retry_a.as<uint32_t>(),
-                    b->counters.as<unsigned long long>(), b->ids.cap / 4, b->pack.cap / 16};
+                    b->counters.as<unsigned long long>(), b->ids.cap / 4, b->pack.cap / 16, ~0ull, nullptr};
         cudaError_t e = launch_gather(r->A, L, keys, b->work.as<uint32_t>(), uint32_t(n_work), O, caps, b->gather_warps, s);
         if (e != cudaSuccess) return set_err(err, errlen, "gather launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
         CK(cudaMemcpyAsync(cnt, b->counters.p, CNT_N * 8, cudaMemcpyDeviceToHost, s));

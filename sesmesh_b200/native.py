@@ -83,6 +83,18 @@ class ArrangementInfo(C.Structure):
                 ("frame", C.c_int64 * 3)]
 
 
+class MultiConfig(C.Structure):
+    _fields_ = [("brick", C.c_uint32), ("caps_level", C.c_uint32), ("gather_warps", C.c_uint32)]
+
+
+MULTI_COUNTS = ["structures", "redone", "bricks", "samples"]
+MULTI_TIMES = ["t_setup", "t_tune", "t_classify", "t_device", "t_d2h", "t_host", "t_redo", "t_total"]
+
+
+class MultiTimes(C.Structure):
+    _fields_ = [(f, C.c_size_t) for f in MULTI_COUNTS] + [(f, C.c_double) for f in MULTI_TIMES] + [("graph", C.c_int)]
+
+
 class BatchInfo(C.Structure):
     _fields_ = [(f, C.c_size_t) for f in ("bricks", "sampled_subblocks", "ids_words", "max_pack_units", "edges",
                                           "triangles", "touched", "resident_bytes")] + \
@@ -146,6 +158,15 @@ SIGNATURES = {
     "smb_surface_mesh": (C.c_int, [_vp, _fp, _fp, _u32p, _u32p, C.POINTER(C.c_uint8), _u32p]),
     "smb_surface_obj": (_sz, [_vp, _cp, _sz]),
     "smb_surface_write_obj": (C.c_int, [_vp, _cp, _cp, _sz]),
+    "smb_multi_new": (C.c_int, [_vp, _sz, C.POINTER(C.POINTER(C.c_double)), C.POINTER(_sz),
+                                C.POINTER(SurfaceParams_), C.POINTER(MultiConfig), C.POINTER(_vp), _cp, _sz]),
+    "smb_multi_free": (None, [_vp]),
+    "smb_multi_set_warm_start": (C.c_int, [_vp, _vp]),
+    "smb_multi_tune": (C.c_int, [_vp, _cp, _sz]),
+    "smb_multi_config_get": (C.c_int, [_vp, C.POINTER(MultiConfig)]),
+    "smb_multi_run": (C.c_int, [_vp, C.POINTER(MultiTimes), _cp, _sz]),
+    "smb_multi_surface": (_vp, [_vp, _sz]),
+    "smb_multi_latency": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "smb_engine_arrangement": (C.c_int, [_vp, C.POINTER(ArrangementInfo)]),
     "smb_arrangement_build": (C.c_int, [C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_), C.POINTER(_vp), _cp,
                                         _sz]),

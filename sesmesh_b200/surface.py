@@ -65,8 +65,9 @@ class SurfaceParams:
 class SurfaceOutput:
     """Mesh, statistics (SurfaceStats + stage times in ms) and OBJ text."""
 
-    def __init__(self, h):
+    def __init__(self, h, owned=True):
         self._h = h
+        self._owned = owned
         st = native.SurfaceStats_()
         lib().smb_surface_stats_get(h, C.byref(st))
         self.stats = {name: getattr(st, name) for name, _ in st._fields_}
@@ -95,7 +96,8 @@ class SurfaceOutput:
 
     def close(self):
         if getattr(self, "_h", None):
-            lib().smb_surface_free(self._h)
+            if getattr(self, "_owned", True):
+                lib().smb_surface_free(self._h)
             self._h = None
 
     def __del__(self):
@@ -234,3 +236,70 @@ def host_arrangement(spheres, params=SurfaceParams()):
         return out
     finally:
         lib().smb_engine_free(h)
+
+
+class MultiBatch:
+    """Many structures meshed in one device pass (smb_multi_*): fast mode,
+    optionally with the learned warm start, the autotuned brick edge,
+    candidate caps and gather block shape unless `config` fixes them.
+
+    `structures` is a list of (spheres, SurfaceParams) pairs."""
+
+    def __init__(self, structures, config=None, warm=None, device=0):
+        self.dev = _device(device)
+        self._keep = [_spheres(sp) for sp, _ in structures]
+        n = len(self._keep)
+        ptrs = (C.POINTER(C.c_double) * n)(*[_p(a, C.c_double) for a in self._keep])
+        counts = (C.c_size_t * n)(*[len(a) for a in self._keep])
+        params = (native.SurfaceParams_ * n)(*[p.with_refine("fast")._c() for _, p in structures])
+        cfg = native.MultiConfig(*(config or (0, 0, 0)))
+        err = C.create_string_buffer(2048)
+        h = C.c_void_p()
+        _check(lib().smb_multi_new(self.dev.h, n, ptrs, counts, params, C.byref(cfg), C.byref(h), err, 2048), err)
+        self.h = h
+        self.n = n
+        self.warm = None
+        if warm is not None:
+            self.set_warm_start(warm)
+
+    def set_warm_start(self, mlp):
+        self.warm = mlp  # kept alive while the batch uses it
+        lib().smb_multi_set_warm_start(self.h, mlp.h if mlp is not None else None)
+
+    def tune(self):
+        err = C.create_string_buffer(1024)
+        _check(lib().smb_multi_tune(self.h, err, 1024), err)
+        return self.config()
+
+    def config(self):
+        c = native.MultiConfig()
+        lib().smb_multi_config_get(self.h, C.byref(c))
+        return dict(brick=c.brick, caps_level=c.caps_level, gather_warps=c.gather_warps)
+
+    def run(self):
+        """Meshes every structure; returns the run's counts and times (ms)."""
+        t = native.MultiTimes()
+        err = C.create_string_buffer(2048)
+        _check(lib().smb_multi_run(self.h, C.byref(t), err, 2048), err)
+        return {name: getattr(t, name) for name, _ in t._fields_}
+
+    def surface(self, i):
+        """Structure i's mesh of the last run (valid until the next run)."""
+        h = lib().smb_multi_surface(self.h, i)
+        if not h:
+            raise IndexError(i)
+        return SurfaceOutput(C.c_void_p(h), owned=False)
+
+    def latency(self):
+        out = np.zeros(self.n, np.float64)
+        lib().smb_multi_latency(self.h, _p(out, C.c_double))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().smb_multi_free(self.h)
+            self.h = None
+        self.warm = None
+
+    def __del__(self):
+        self.close()
