@@ -91,7 +91,10 @@ int smb_surface_write_obj(smb_surface* s, const char* path, char* err, size_t er
  * optionally with the learned warm start.  Each structure's mesh is the
  * single-structure device path's at the same brick edge.  Buffers are
  * sized from per-brick caps; a structure over a cap is meshed again on its
- * own (counted in smb_multi_times.redone).  The autotuner picks the brick
+ * own (counted in smb_multi_times.redone).  Structures are taken in groups
+ * whose buffers fit a third of the free device memory, one pass (one
+ * recorded graph) per group; the host stages of one group run while the
+ * device meshes the next.  The autotuner picks the brick
  * edge (8 or 16), the candidate caps (level 0 or 1) and the gather block
  * shape (2 or 4 warps) by timing the device pass; a config with every
  * field set skips it. */
@@ -106,7 +109,12 @@ typedef struct {
     /* ms: arrangements and uploads (once), tuning (once), classification,
      * device pass, copies back, host stages, structures redone, whole run */
     double t_setup, t_tune, t_classify, t_device, t_d2h, t_host, t_redo, t_total;
-    int graph; /* the pass ran from a captured CUDA graph */
+    int graph;     /* every pass ran from a captured CUDA graph */
+    size_t groups; /* passes: structures are grouped to fit the device buffers */
+    /* sub-blocks whose lists exceeded the shared-memory caps even on the
+     * retry with four times the caps, and that exceeded the list pools or
+     * the sampler's block cap (their structures are redone) */
+    unsigned long long over_lists, over_memory;
 } smb_multi_times;
 /* n structures: xyzr[i] holds counts[i] rows (x, y, z, r); params[i] its
  * SES parameters (refine must be SMB_REFINE_FAST; brick_size is set by the

@@ -303,13 +303,12 @@ __device__ __forceinline__ unsigned warp_inclusive_scan(unsigned v) {
 }
 
 
+// One warp: the lists of work item `item` (a sampled sub-block).
 template <bool MANY>
-__global__ void k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
-                         GatherCaps caps, Scene S) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const DLat& L0, const int4* keys,
+                                            const uint32_t* work, const GatherOut& O, const GatherCaps& caps,
+                                            const Scene& S, unsigned char* smem_raw) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const uint32_t item = blockIdx.x * (blockDim.x >> 5) + wib;
-    if (item >= (MANY ? uint32_t(*S.n_work) : n_work)) return;
     unsigned char* base = smem_raw + size_t(wib) * gather_smem_bytes(caps);
     double* s_key = reinterpret_cast<double*>(base);
     double* c_key = s_key + caps.s;
@@ -346,7 +345,9 @@ __global__ void k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* wor
             rec[R_FLAGS] |= bit;
             unsigned long long q = atomicAdd(&O.counters[bit == REC_OVERFLOW ? CNT_OVERFLOW : CNT_NOMEM], 1ull);
             if (bit == REC_OVERFLOW && O.retry) O.retry[q] = j;
-            if (O.fail) O.fail[key.w] = 1;
+            // Many structures: a structure is flagged unless a retry with
+            // larger caps follows.
+            if (O.fail && !(bit == REC_OVERFLOW && O.retry)) O.fail[key.w] = 1;
         }
     };
 
@@ -575,6 +576,18 @@ __global__ void k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* wor
         rec[R_PACK] = uint32_t(pack_base);
         rec[R_PACKLEN] = uint32_t(units);
     }
+}
+
+// Warp per work item, the grid striding over the items (many structures:
+// the item count is read on the device).
+template <bool MANY>
+__global__ void k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
+                         GatherCaps caps, Scene S) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t n = MANY ? uint32_t(*S.n_work) : n_work;
+    const uint32_t wpb = blockDim.x >> 5;
+    for (uint32_t item = blockIdx.x * wpb + (threadIdx.x >> 5); item < n; item += gridDim.x * wpb)
+        gather_item<MANY>(item, A0, L0, keys, work, O, caps, S, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -1071,6 +1084,11 @@ __global__ void __launch_bounds__(256) k_item_edges(const DLat L, const uint32_t
         counts[i] = at;
         atomicMax(reinterpret_cast<unsigned int*>(&counters[CNT_MAXITEM]), at);
     }
+}
+
+// *dst = *src (a device count kept before the kernel that reads it grows it).
+__global__ void k_copy_count(unsigned long long* dst, const unsigned long long* src) {
+    if (threadIdx.x == 0) *dst = *src;
 }
 
 // dst = the low 32 bits of a device total (the tail of an offset list).
@@ -1592,7 +1610,11 @@ cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const 
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     COUNT(1);
-    kern<<<(n + warps - 1) / warps, 32 * warps, smem, s>>>(A, L, keys, work, n, O, caps, many ? *many : Scene{});
+    // Many structures: n is an upper bound of the device count; the grid
+    // strides (a few waves of blocks, not one per possible item).
+    uint32_t blocks = (n + warps - 1) / warps;
+    if (many) blocks = std::min<uint32_t>(blocks, 148u * 32u);
+    kern<<<blocks, 32 * warps, smem, s>>>(A, L, keys, work, n, O, caps, many ? *many : Scene{});
     return cudaGetLastError();
 }
 
@@ -1624,6 +1646,11 @@ cudaError_t launch_mc(const DLat& L, uint32_t n, float* values, const uint32_t* 
     kern<<<n, MC_THREADS, smem, s>>>(L, n, values, rec, counts, edge_off, tri_off, edges, edge_vals, tris, keys, edge_cap,
                                      tri_cap, many ? *many : Scene{});
     return cudaGetLastError();
+}
+
+void launch_copy_count(unsigned long long* dst, const unsigned long long* src, cudaStream_t s) {
+    COUNT(1);
+    k_copy_count<<<1, 32, 0, s>>>(dst, src);
 }
 
 void launch_put_total(uint32_t* dst, const unsigned long long* total, cudaStream_t s) {

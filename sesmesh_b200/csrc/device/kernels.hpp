@@ -29,7 +29,7 @@ __host__ __device__ inline size_t gather_smem_bytes(const GatherCaps& c) {
 // Device counters of one gather/sample pass.
 enum : int {
     CNT_IDS = 0, CNT_PACK = 1, CNT_MAXPACK = 2, CNT_OVERFLOW = 3, CNT_NOMEM = 4, CNT_TIMEOUT = 5, CNT_OPS = 6,
-    CNT_OWNED = 7, CNT_MAXNN = 8, CNT_MAXNS = 9, CNT_MAXNC = 10, CNT_MAXNV = 11, CNT_MAXITEM = 12, CNT_QUEUE = 13, CNT_N = 16
+    CNT_OWNED = 7, CNT_MAXNN = 8, CNT_MAXNS = 9, CNT_MAXNC = 10, CNT_MAXNV = 11, CNT_MAXITEM = 12, CNT_QUEUE = 13, CNT_RETRY = 14, CNT_N = 16
 };
 constexpr uint32_t REC_NOMEM = 2;
 
@@ -78,6 +78,7 @@ void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const ui
                        unsigned long long* tiles, unsigned long long* total, unsigned long long* counters,
                        cudaStream_t s, const Scene* many = nullptr, const int4* keys = nullptr);
 void launch_put_total(uint32_t* dst, const unsigned long long* total, cudaStream_t s);
+void launch_copy_count(unsigned long long* dst, const unsigned long long* src, cudaStream_t s);
 // Persistent refinement (or feature pass) over the items' edge lists; grid
 // = SMs x resident CTAs.  *smem_out gets the shared memory it needs (also
 // when it does not launch, for n_items = 0).

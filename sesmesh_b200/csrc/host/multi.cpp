@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <thread>
 
 #include "../device/kernels.hpp"
 #include "../device/mlp.cuh"
@@ -76,7 +77,46 @@ DLat lattice_for(const DLat& L0, int b) {
     return L;
 }
 
+// Page-locked host memory that grows on demand (copies from the device run
+// at full link speed into it).
+struct Pinned {
+    void* p = nullptr;
+    size_t cap = 0;
+    bool reserve(size_t bytes) {
+        if (bytes <= cap) return true;
+        if (p) cudaFreeHost(p), p = nullptr, cap = 0;
+        size_t want = bytes + bytes / 4 + 4096;
+        if (cudaHostAlloc(&p, want, cudaHostAllocDefault) != cudaSuccess) return p = nullptr, false;
+        cap = want;
+        return true;
+    }
+    template <class T>
+    T* as() const {
+        return static_cast<T*>(p);
+    }
+    ~Pinned() {
+        if (p) cudaFreeHost(p);
+    }
+};
+
+// One group's results on the host.
+struct HostGroup {
+    size_t ne = 0, nt = 0;
+    Pinned eo, to, edges, tris, feat, evals, ev, t, q;
+};
+
 }  // namespace
+
+// Structures [s0, s1), surface bricks [k0, k1) of the keys, and the graph
+// recorded for that pass (with the configuration it was recorded for).
+struct Group {
+    size_t s0 = 0, s1 = 0, k0 = 0, k1 = 0;
+    cudaGraphExec_t graph = nullptr;
+    smb_multi_config cfg{};
+    const smb_mlp* warm = nullptr;
+    const void* keys = nullptr;
+    uint64_t gen = 0;
+};
 
 struct smb_multi {
     smb_device* dev = nullptr;
@@ -94,16 +134,20 @@ struct smb_multi {
     std::vector<uint32_t> sph_off;
     DBuf d_arr, d_lat, d_rc, d_box, d_flag_off, d_sph_off, d_err, d_fail;
     // Batch buffers.
-    DBuf flags, list, surf, cells, tiles, tot, keys, rec, sampled, work, values, counters, totals, ids, pack;
+    DBuf flags, list, surf, cells, tiles, tot, keys, rec, sampled, work, retry, values, counters, totals, ids, pack;
     DBuf mc_counts, edge_off, tri_off, edges, edge_vals, tris, item_counts, item_off, item_edges;
     DBuf e_t, e_feat, e_q, e_evals;
     size_t edge_cap = 0, tri_cap = 0;
-    // Captured graph of the mesh-stage pass.
-    cudaGraphExec_t graph = nullptr;
-    size_t graph_bricks = 0;
-    smb_multi_config graph_cfg{};
-    const smb_mlp* graph_warm = nullptr;
+    // Groups of structures, one pass (and one recorded graph) each.
+    std::vector<Group> groups;
+    size_t group_bricks = 0;
     bool graph_ok = true;
+    uint32_t unit_cap = 0;     // the sampler's block cap (units), raised to what a pass needed
+    smb_multi_config unit_cfg{};
+    uint64_t gen = 0;          // buffer generation (recorded graphs hold their buffers' addresses)
+    std::vector<int4> keys4;   // host copy of the keys
+    HostGroup* hosts = nullptr;  // two alternating sets of results on the host
+    std::vector<size_t> b0;    // first brick of each structure (n + 1)
     cudaEvent_t ev[2] = {};
     // Results of the last run.
     std::vector<std::unique_ptr<smb_surface>> out;
@@ -113,7 +157,7 @@ struct smb_multi {
 
     std::vector<DBuf*> bufs() {
         return {&d_arr, &d_lat, &d_rc, &d_box, &d_flag_off, &d_sph_off, &d_err, &d_fail, &flags, &list, &surf,
-                &cells, &tiles, &tot, &keys, &rec, &sampled, &work, &values, &counters, &totals, &ids, &pack,
+                &cells, &tiles, &tot, &keys, &rec, &sampled, &work, &retry, &values, &counters, &totals, &ids, &pack,
                 &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &item_counts, &item_off, &item_edges,
                 &e_t, &e_feat, &e_q, &e_evals};
     }
@@ -232,10 +276,47 @@ int classify_all(smb_multi* m, char* err, size_t errlen) {
     return SMB_OK;
 }
 
-// Buffers of the mesh-stage pass for n_bricks surface bricks at the
-// configured caps.
-int reserve_pass(smb_multi* m, char* err, size_t errlen) {
-    const size_t nb = std::max<uint32_t>(m->n_bricks, 1), nsub = nb * 8;
+// Device bytes one surface brick of a pass needs at the configured caps
+// (records, values, list pools, marching-cubes and refinement outputs).
+size_t bytes_per_brick(const smb_multi_config& c) {
+    const int b = int(c.brick);
+    const CapLevel& C = CAP_LEVELS[c.caps_level];
+    const size_t spb = size_t(b + 1) * (b + 1) * (b + 1), edges = size_t(3) * b * b;
+    return spb * 4 + 8 * (REC_WORDS * 4 + 12) + 4 * (size_t(C.ids_per_sub) * 4 + size_t(C.units_per_sub) * 16) +
+           edges * (4 + 8 + 4 + 4 + 4 + 12 + 4) + 2 * edges * 12 + 8;
+}
+
+// Structures in order, grouped so that each group's surface bricks fit the
+// pass buffers (a structure larger than that is a group of its own).
+void form_groups(smb_multi* m) {
+    const size_t n = m->n();
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t budget = std::max<size_t>(size_t(1) << 28, free_b / 3);
+    m->group_bricks = std::max<size_t>(4096, budget / bytes_per_brick(m->cfg));
+    std::vector<Group> g;
+    size_t s0 = 0;
+    while (s0 < n) {
+        size_t s1 = s0 + 1;
+        while (s1 < n && m->b0[s1 + 1] - m->b0[s0] <= m->group_bricks) s1++;
+        Group G;
+        G.s0 = s0, G.s1 = s1, G.k0 = m->b0[s0], G.k1 = m->b0[s1];
+        g.push_back(G);
+        s0 = s1;
+    }
+    // Keep recorded graphs whose group is unchanged.
+    for (Group& G : g)
+        for (Group& O : m->groups)
+            if (O.graph && O.s0 == G.s0 && O.s1 == G.s1 && O.k0 == G.k0 && O.k1 == G.k1) std::swap(G.graph, O.graph),
+                G.cfg = O.cfg, G.warm = O.warm, G.keys = O.keys, G.gen = O.gen;
+    for (Group& O : m->groups)
+        if (O.graph) cudaGraphExecDestroy(O.graph);
+    m->groups.swap(g);
+}
+
+// Buffers of one pass of up to max_nb surface bricks at the configured caps.
+int reserve_pass(smb_multi* m, size_t max_nb, char* err, size_t errlen) {
+    const size_t nb = std::max<size_t>(max_nb, 1), nsub = nb * 8;
     const int b = m->cfg.brick;
     const CapLevel& C = CAP_LEVELS[m->cfg.caps_level];
     const size_t spb = size_t(b + 1) * (b + 1) * (b + 1);
@@ -243,7 +324,8 @@ int reserve_pass(smb_multi* m, char* err, size_t errlen) {
     m->tri_cap = std::min<size_t>(size_t(0xFFFFFFF0u), 2 * m->edge_cap);
     int rc;
     if ((rc = m->rec.reserve(nsub * REC_WORDS * 4, err, errlen)) || (rc = m->sampled.reserve(nsub * 4, err, errlen)) ||
-        (rc = m->work.reserve(nsub * 4, err, errlen)) || (rc = m->values.reserve(nb * spb * 4, err, errlen)) ||
+        (rc = m->work.reserve(nsub * 4, err, errlen)) || (rc = m->retry.reserve(nsub * 4, err, errlen)) ||
+        (rc = m->values.reserve(nb * spb * 4, err, errlen)) ||
         (rc = m->tiles.reserve(size_t(scan_tiles_needed(uint32_t(nsub))) * 8 + 64, err, errlen)) ||
         (rc = m->counters.reserve(CNT_N * 8, err, errlen)) ||
         (rc = m->ids.reserve(nsub / 2 * C.ids_per_sub * 4, err, errlen)) ||
@@ -260,35 +342,48 @@ int reserve_pass(smb_multi* m, char* err, size_t errlen) {
     return SMB_OK;
 }
 
-// The mesh-stage pass over every structure's surface bricks, all sizes
-// fixed by n_bricks and the caps (no host synchronisation inside), as one
-// stream of launches: recorded once into a CUDA graph, then replayed.
-int enqueue_pass(smb_multi* m, char* err, size_t errlen) {
+// The mesh-stage pass over one group's surface bricks (keys [k0, k1)), all
+// sizes fixed (no host synchronisation inside), as one stream of launches:
+// recorded once into a CUDA graph, then replayed.
+int enqueue_pass(smb_multi* m, const Group& G, char* err, size_t errlen) {
     cudaStream_t s = m->dev->stream;
     smb_device* d = m->dev;
-    const uint32_t nb = m->n_bricks, nsub = nb * 8;
+    const uint32_t nb = uint32_t(G.k1 - G.k0), nsub = nb * 8;
     const int b = m->cfg.brick;
     const CapLevel& C = CAP_LEVELS[m->cfg.caps_level];
     const size_t spb = size_t(b + 1) * (b + 1) * (b + 1);
     Scene S = scene_of(m);
-    const int4* keys = m->keys.as<int4>();
+    const int4* keys = m->keys.as<int4>() + G.k0;
     unsigned long long* cnt = m->counters.as<unsigned long long>();
     unsigned long long* tot = m->totals.as<unsigned long long>();
     DLat L{};  // per-structure lattices come from the scene; b and spb are shared
     L.b = b, L.sub = b / 2, L.spb = int(spb);
     MCK(cudaMemsetAsync(cnt, 0, CNT_N * 8, s));
-    MCK(cudaMemsetAsync(m->d_fail.p, 0, m->n() * 4, s));
     MCK(cudaMemsetAsync(m->values.p, 0, size_t(nb) * spb * 4, s));
     launch_substates(DArr{}, DLat{}, keys, nb, m->rec.as<uint32_t>(), m->sampled.as<uint32_t>(), s, &S);
     launch_scan(m->sampled.as<uint32_t>(), nsub, nullptr, m->work.as<uint32_t>(), m->tiles.as<unsigned long long>(),
                 tot, s);
-    GatherOut O{m->rec.as<uint32_t>(), m->ids.as<uint32_t>(), m->pack.as<uint4>(), nullptr, cnt,
-                m->ids.cap / 4, m->pack.cap / 16, C.unit_cap, m->d_fail.as<uint32_t>()};
+    GatherOut O{m->rec.as<uint32_t>(), m->ids.as<uint32_t>(), m->pack.as<uint4>(), m->retry.as<uint32_t>(), cnt,
+                m->ids.cap / 4, m->pack.cap / 16, m->unit_cap, m->d_fail.as<uint32_t>()};
     cudaError_t e = launch_gather(DArr{}, DLat{}, keys, m->work.as<uint32_t>(), nsub, O, C.caps,
                                   int(m->cfg.gather_warps), s, &S);
     if (e != cudaSuccess) return set_err(err, errlen, "gather launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    // Sub-blocks over the shared-memory list caps: once more, a warp per
+    // block with four times the caps (the count is kept first: the retry
+    // pass counts its own overflows in the same counter).
+    {
+        GatherCaps big = C.caps;
+        big.near *= 4, big.s *= 4, big.c *= 4, big.v *= 4;
+        launch_copy_count(cnt + CNT_RETRY, cnt + CNT_OVERFLOW, s);
+        Scene R = S;
+        R.n_work = cnt + CNT_RETRY;
+        GatherOut O2 = O;
+        O2.retry = nullptr;
+        e = launch_gather(DArr{}, DLat{}, keys, m->retry.as<uint32_t>(), nsub, O2, big, 1, s, &R);
+        if (e != cudaSuccess) return set_err(err, errlen, "gather launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    }
     e = launch_sample(DLat{}, keys, m->work.as<uint32_t>(), nsub, m->rec.as<uint32_t>(), m->pack.as<uint4>(),
-                      C.unit_cap, m->values.as<float>(), cnt, true, false, s, &S);
+                      m->unit_cap, m->values.as<float>(), cnt, true, false, s, &S);
     if (e != cudaSuccess) return set_err(err, errlen, "sample launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     e = launch_mc(L, nb, m->values.as<float>(), m->rec.as<uint32_t>(), m->mc_counts.as<uint32_t>(), nullptr, nullptr,
                   nullptr, nullptr, nullptr, false, s, keys, ~0ull, ~0ull, &S);
@@ -309,7 +404,7 @@ int enqueue_pass(smb_multi* m, char* err, size_t errlen) {
     const int mode = m->warm ? REFINE_MLP : REFINE_PLAIN;
     MlpDev md{nullptr, nullptr, nullptr};
     if (m->warm) md = mlp_dev(m->warm);
-    const size_t cand = size_t(C.unit_cap) * 16 + 64;
+    const size_t cand = size_t(m->unit_cap) * 16 + 64;
     e = launch_refine(DArr{}, DLat{}, RefineConsts{}, keys, m->work.as<uint32_t>(), m->rec.as<uint32_t>(),
                       m->ids.as<uint32_t>(), m->edges.as<uint32_t>(), m->edge_vals.as<float2>(),
                       m->item_off.as<uint32_t>(), m->item_edges.as<uint32_t>(), nsub, m->e_t.as<float>(),
@@ -320,76 +415,131 @@ int enqueue_pass(smb_multi* m, char* err, size_t errlen) {
     return SMB_OK;
 }
 
-// Runs the pass: from the captured graph when it matches the current sizes
-// and configuration, else records it (and replays it); direct launches if
-// recording is refused.
-int run_pass(smb_multi* m, float* device_ms, char* err, size_t errlen) {
+// Runs one group's pass: from its recorded graph when that matches the
+// configuration, else directly once (setting the kernels' attributes) and
+// then records it; direct launches if recording is refused.
+int run_group(smb_multi* m, Group& G, float* device_ms, char* err, size_t errlen) {
     cudaStream_t s = m->dev->stream;
     int rc;
-    if ((rc = reserve_pass(m, err, errlen))) return rc;
-    const bool same = m->graph && m->graph_bricks == m->n_bricks && m->graph_cfg.brick == m->cfg.brick &&
-                      m->graph_cfg.caps_level == m->cfg.caps_level &&
-                      m->graph_cfg.gather_warps == m->cfg.gather_warps && m->graph_warm == m->warm;
     if (!m->ev[0]) cudaEventCreate(&m->ev[0]), cudaEventCreate(&m->ev[1]);
-    if (!same && m->n_bricks) {
-        if (m->graph) cudaGraphExecDestroy(m->graph), m->graph = nullptr;
-        // One direct pass first: sets the kernels' attributes outside the
-        // recording and checks the launches.
-        MCK(cudaEventRecord(m->ev[0], s));
-        if ((rc = enqueue_pass(m, err, errlen))) return rc;
-        MCK(cudaEventRecord(m->ev[1], s));
-        MCK(cudaStreamSynchronize(s));
+    *device_ms = 0;
+    if (G.k1 == G.k0) return SMB_OK;
+    const bool same = G.graph && G.cfg.brick == m->cfg.brick && G.cfg.caps_level == m->cfg.caps_level &&
+                      G.cfg.gather_warps == m->cfg.gather_warps && G.warm == m->warm && G.keys == m->keys.p &&
+                      G.gen == m->gen;
+    if (!same) {
+        if (G.graph) cudaGraphExecDestroy(G.graph), G.graph = nullptr;
+        // Direct passes: the first sets the kernels' attributes; when lists
+        // ran past the pools or the sampler's block cap, those grow to what
+        // the pass counted and the pass runs again (twice at most).
+        for (int attempt = 0;; attempt++) {
+            MCK(cudaEventRecord(m->ev[0], s));
+            if ((rc = enqueue_pass(m, G, err, errlen))) return rc;
+            MCK(cudaEventRecord(m->ev[1], s));
+            MCK(cudaStreamSynchronize(s));
+            unsigned long long c[CNT_N];
+            MCK(cudaMemcpy(c, m->counters.p, sizeof c, cudaMemcpyDeviceToHost));
+            if (!c[CNT_NOMEM] || attempt >= 2) break;
+            bool grow = false;
+            if (c[CNT_IDS] > m->ids.cap / 4) {
+                if ((rc = m->ids.reserve(size_t(c[CNT_IDS]) * 4, err, errlen))) return rc;
+                grow = true;
+            }
+            if (c[CNT_PACK] > m->pack.cap / 16) {
+                if ((rc = m->pack.reserve(size_t(c[CNT_PACK]) * 16, err, errlen))) return rc;
+                grow = true;
+            }
+            const unsigned long long unit_limit = (m->dev->smem_optin - 64) / 16;
+            if (c[CNT_MAXPACK] > m->unit_cap && c[CNT_MAXPACK] <= unit_limit) {
+                m->unit_cap = uint32_t(c[CNT_MAXPACK]);
+                grow = true;
+            }
+            if (!grow) break;
+            m->gen++;
+            MCK(cudaMemsetAsync(m->d_fail.as<uint32_t>() + G.s0, 0, (G.s1 - G.s0) * 4, s));
+        }
         cudaGraph_t g = nullptr;
         if (m->graph_ok && cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
             char e2[256] = {0};
-            int prc = enqueue_pass(m, e2, sizeof e2);
+            int prc = enqueue_pass(m, G, e2, sizeof e2);
             cudaError_t ce = cudaStreamEndCapture(s, &g);
-            if (prc == SMB_OK && ce == cudaSuccess && g && cudaGraphInstantiate(&m->graph, g, 0) == cudaSuccess) {
-                m->graph_bricks = m->n_bricks;
-                m->graph_cfg = m->cfg;
-                m->graph_warm = m->warm;
+            if (prc == SMB_OK && ce == cudaSuccess && g && cudaGraphInstantiate(&G.graph, g, 0) == cudaSuccess) {
+                G.cfg = m->cfg, G.warm = m->warm, G.keys = m->keys.p, G.gen = m->gen;
             } else {
-                m->graph = nullptr;
+                G.graph = nullptr;
                 m->graph_ok = false;
                 cudaGetLastError();
             }
             if (g) cudaGraphDestroy(g);
         }
-        float ms = 0;
-        cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]);
-        *device_ms = ms;
+        cudaEventElapsedTime(device_ms, m->ev[0], m->ev[1]);
         return SMB_OK;
     }
     MCK(cudaEventRecord(m->ev[0], s));
-    if (m->n_bricks) {
-        if (m->graph) MCK(cudaGraphLaunch(m->graph, s));
-        else if ((rc = enqueue_pass(m, err, errlen))) return rc;
-    }
+    MCK(cudaGraphLaunch(G.graph, s));
     MCK(cudaEventRecord(m->ev[1], s));
     MCK(cudaStreamSynchronize(s));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, m->ev[0], m->ev[1]);
-    *device_ms = ms;
+    cudaEventElapsedTime(device_ms, m->ev[0], m->ev[1]);
     return SMB_OK;
 }
 
-// Device part for the current configuration: classification and the pass;
-// *fails gets the number of structures over a cap.
-int device_run(smb_multi* m, double* classify_ms, float* device_ms, size_t* fails, char* err, size_t errlen) {
+// Classification of every structure, brick ranges and groups, buffers.
+int prepare_run(smb_multi* m, double* classify_ms, char* err, size_t errlen) {
     int rc;
     if ((rc = set_brick(m, m->cfg.brick, err, errlen))) return rc;
     auto t0 = clk::now();
     if ((rc = classify_all(m, err, errlen))) return rc;
-    MCK(cudaStreamSynchronize(m->dev->stream));
+    const size_t n = m->n(), nb = m->n_bricks;
+    m->keys4.resize(nb);
+    if (nb) MCK(cudaMemcpy(m->keys4.data(), m->keys.p, nb * sizeof(int4), cudaMemcpyDeviceToHost));
     *classify_ms = ms_since(t0);
-    if ((rc = run_pass(m, device_ms, err, errlen))) return rc;
-    std::vector<uint32_t> f(m->n());
-    MCK(cudaMemcpy(f.data(), m->d_fail.p, m->n() * 4, cudaMemcpyDeviceToHost));
+    m->b0.assign(n + 1, nb);
+    for (size_t i = nb; i-- > 0;) m->b0[size_t(m->keys4[i].w)] = i;
+    for (size_t i = n; i-- > 0;) m->b0[i] = std::min(m->b0[i], m->b0[i + 1]);
+    form_groups(m);
+    const smb_multi_config& c = m->cfg;
+    if (!m->unit_cap || c.brick != m->unit_cfg.brick || c.caps_level != m->unit_cfg.caps_level) {
+        m->unit_cap = CAP_LEVELS[c.caps_level].unit_cap;
+        m->unit_cfg = c;
+        m->gen++;
+    }
+    size_t max_nb = 0;
+    for (const Group& G : m->groups) max_nb = std::max(max_nb, G.k1 - G.k0);
+    if ((rc = reserve_pass(m, max_nb, err, errlen))) return rc;
+    MCK(cudaMemsetAsync(m->d_fail.p, 0, n * 4, m->dev->stream));
+    return SMB_OK;
+}
+
+int fetch_group(smb_multi* m, const Group& G, HostGroup& H, char* err, size_t errlen) {
+    const size_t nb = G.k1 - G.k0;
+    cudaStream_t s = m->dev->stream;
+    H.ne = H.nt = 0;
+    if (!H.eo.reserve((nb + 1) * 4) || !H.to.reserve((nb + 1) * 4))
+        return set_err(err, errlen, "page-locked host memory"), SMB_ERR_MEMORY;
+    if (!nb) {
+        H.eo.as<uint32_t>()[0] = H.to.as<uint32_t>()[0] = 0;
+        return SMB_OK;
+    }
     unsigned long long t3[4] = {0, 0, 0, 0};
     MCK(cudaMemcpy(t3, m->totals.p, 32, cudaMemcpyDeviceToHost));
-    size_t k = 0;
-    for (uint32_t v : f) k += v != 0;
-    *fails = k;
+    H.ne = std::min<size_t>(t3[1], m->edge_cap), H.nt = std::min<size_t>(t3[2], m->tri_cap);
+    const size_t ne = H.ne, nt = H.nt;
+    if (!H.edges.reserve(ne * 4 + 4) || !H.tris.reserve(nt * 12 + 4) || !H.feat.reserve(ne * 4 + 4) ||
+        !H.evals.reserve(ne * 4 + 4) || !H.ev.reserve(ne * 8 + 8) || !H.t.reserve(ne * 4 + 4) ||
+        !H.q.reserve(ne * 12 + 12))
+        return set_err(err, errlen, "page-locked host memory"), SMB_ERR_MEMORY;
+    MCK(cudaMemcpyAsync(H.eo.p, m->edge_off.p, (nb + 1) * 4, cudaMemcpyDeviceToHost, s));
+    MCK(cudaMemcpyAsync(H.to.p, m->tri_off.p, (nb + 1) * 4, cudaMemcpyDeviceToHost, s));
+    if (ne) {
+        MCK(cudaMemcpyAsync(H.edges.p, m->edges.p, ne * 4, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(H.ev.p, m->edge_vals.p, ne * 8, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(H.t.p, m->e_t.p, ne * 4, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(H.feat.p, m->e_feat.p, ne * 4, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(H.q.p, m->e_q.p, ne * 12, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(H.evals.p, m->e_evals.p, ne * 4, cudaMemcpyDeviceToHost, s));
+    }
+    if (nt) MCK(cudaMemcpyAsync(H.tris.p, m->tris.p, nt * 12, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
     return SMB_OK;
 }
 
@@ -442,10 +592,12 @@ void smb_multi_free(smb_multi* m) {
     if (!m) return;
     cudaSetDevice(m->dev->index);
     cudaStreamSynchronize(m->dev->stream);
-    if (m->graph) cudaGraphExecDestroy(m->graph);
+    for (Group& G : m->groups)
+        if (G.graph) cudaGraphExecDestroy(G.graph);
     for (auto& ev : m->ev)
         if (ev) cudaEventDestroy(ev);
     for (DBuf* b : m->bufs()) b->release();
+    delete[] m->hosts;
     for (smb_engine* e : m->eng) smb_engine_free(e);
     smb_device* d = m->dev;
     delete m;
@@ -464,27 +616,37 @@ int smb_multi_tune(smb_multi* m, char* err, size_t errlen) {
     if (cudaSetDevice(m->dev->index) != cudaSuccess) return set_err(err, errlen, "cudaSetDevice failed"), SMB_ERR_CUDA;
     auto t0 = clk::now();
     // Candidates: brick edge 8 or 16, candidate caps level 0 or 1, 2 or 4
-    // warps per gather block.  Score: device time of classification and
-    // pass, plus the single-structure cost of every structure over a cap
-    // (taken as the pass's time per structure, times four).
+    // warps per gather block.  Each runs the device part over every group
+    // (first pass of a configuration, so recording included); score: its
+    // time plus classification plus the single-structure cost of the
+    // structures over a cap (their share of the pass, times four).
     smb_multi_config best = m->cfg;
     double best_score = 1e300;
+    std::string last;
     const int bricks[2] = {8, 16};
     const uint32_t warps[2] = {2, 4};
     for (int b : bricks)
         for (uint32_t lvl = 0; lvl < 2; lvl++)
             for (uint32_t w : warps) {
                 m->cfg.brick = uint32_t(b), m->cfg.caps_level = lvl, m->cfg.gather_warps = w;
-                double cms = 0, score = 0;
+                double cms = 0, dev = 0;
                 float dms = 0;
-                size_t fails = 0;
-                int rc = device_run(m, &cms, &dms, &fails, err, errlen);
-                if (rc == SMB_OK) rc = run_pass(m, &dms, err, errlen);  // a replay, the steady-state time
-                if (rc != SMB_OK) continue;
-                score = cms + dms + 4.0 * (cms + dms) / double(m->n()) * double(fails);
+                int rc = prepare_run(m, &cms, err, errlen);
+                for (size_t gi = 0; rc == SMB_OK && gi < m->groups.size(); gi++)
+                    rc = run_group(m, m->groups[gi], &dms, err, errlen), dev += dms;
+                if (rc != SMB_OK) {
+                    last = err ? err : "";
+                    continue;
+                }
+                std::vector<uint32_t> f(m->n());
+                if (cudaMemcpy(f.data(), m->d_fail.p, m->n() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) continue;
+                const double all = double(std::max<uint32_t>(m->n_bricks, 1));
+                double fails = 0;
+                for (size_t i = 0; i < m->n(); i++) fails += f[i] ? double(m->b0[i + 1] - m->b0[i]) : 0.0;
+                double score = cms + dev + 4.0 * dev * fails / all;
                 if (score < best_score) best_score = score, best = m->cfg;
             }
-    if (best_score >= 1e300) return set_err(err, errlen, "no configuration ran"), SMB_ERR_CUDA;
+    if (best_score >= 1e300) return set_err(err, errlen, "no configuration ran: %s", last.c_str()), SMB_ERR_CUDA;
     m->cfg = best;
     m->tuned = true;
     m->t_tune = ms_since(t0);
@@ -504,79 +666,100 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
     if (!m->tuned && (rc = smb_multi_tune(m, err, errlen))) return rc;
     auto t_start = clk::now();
     double cms = 0;
-    float dms = 0;
-    size_t fails = 0;
-    if ((rc = device_run(m, &cms, &dms, &fails, err, errlen))) return rc;
-    // Results to the host.
-    auto t1 = clk::now();
-    const size_t n = m->n(), nb = m->n_bricks;
-    unsigned long long t3[4] = {0, 0, 0, 0};
-    MCK(cudaMemcpy(t3, m->totals.p, 32, cudaMemcpyDeviceToHost));
-    std::vector<uint32_t> fail(n);
-    MCK(cudaMemcpy(fail.data(), m->d_fail.p, n * 4, cudaMemcpyDeviceToHost));
-    const size_t ne = std::min<size_t>(t3[1], m->edge_cap), nt = std::min<size_t>(t3[2], m->tri_cap);
-    std::vector<int4> keys4(nb);
-    std::vector<uint32_t> eo(nb + 1, 0), to(nb + 1, 0), edges(ne), tris(3 * nt), feat(ne), evals(ne);
-    std::vector<float> ev(2 * ne), t(ne), q(3 * ne);
-    if (nb) {
-        MCK(cudaMemcpy(keys4.data(), m->keys.p, nb * sizeof(int4), cudaMemcpyDeviceToHost));
-        MCK(cudaMemcpy(eo.data(), m->edge_off.p, (nb + 1) * 4, cudaMemcpyDeviceToHost));
-        MCK(cudaMemcpy(to.data(), m->tri_off.p, (nb + 1) * 4, cudaMemcpyDeviceToHost));
-    }
-    if (ne) {
-        MCK(cudaMemcpy(edges.data(), m->edges.p, ne * 4, cudaMemcpyDeviceToHost));
-        MCK(cudaMemcpy(ev.data(), m->edge_vals.p, ne * 8, cudaMemcpyDeviceToHost));
-        MCK(cudaMemcpy(t.data(), m->e_t.p, ne * 4, cudaMemcpyDeviceToHost));
-        MCK(cudaMemcpy(feat.data(), m->e_feat.p, ne * 4, cudaMemcpyDeviceToHost));
-        MCK(cudaMemcpy(q.data(), m->e_q.p, ne * 12, cudaMemcpyDeviceToHost));
-        MCK(cudaMemcpy(evals.data(), m->e_evals.p, ne * 4, cudaMemcpyDeviceToHost));
-    }
-    if (nt) MCK(cudaMemcpy(tris.data(), m->tris.p, nt * 12, cudaMemcpyDeviceToHost));
-    double t_d2h = ms_since(t1);
-    // Brick ranges per structure (keys are in structure order).
-    std::vector<size_t> b0(n + 1, nb);
-    for (size_t i = nb; i-- > 0;) b0[size_t(keys4[i].w)] = i;
-    for (size_t i = n; i-- > 0;) b0[i] = std::min(b0[i], b0[i + 1]);
-    // Host stages per structure, on the host threads; a structure over a cap
-    // (or whose output runs past the edge or triangle buffers) is redone on
-    // its own afterwards.
-    auto t2 = clk::now();
+    if ((rc = prepare_run(m, &cms, err, errlen))) return rc;
+    const size_t n = m->n();
     m->out.clear();
     m->out.resize(n);
     m->latency.assign(n, 0.0);
     m->redone.assign(n, 0);
     std::vector<std::string> errs(n);
-    for (size_t i = 0; i < n; i++)
-        if (fail[i] || eo[b0[i + 1]] > ne || to[b0[i + 1]] > nt) m->redone[i] = 1;
-    parallel_for(n, [&](size_t i, int) {
-        if (m->redone[i]) return;
-        SerialScope serial;
-        const size_t lo = b0[i], hi = b0[i + 1], nbi = hi - lo;
-        std::vector<int32_t> k3(3 * nbi);
-        std::vector<uint32_t> leo(nbi + 1), lto(nbi + 1);
-        for (size_t j = 0; j < nbi; j++)
-            k3[3 * j] = keys4[lo + j].x, k3[3 * j + 1] = keys4[lo + j].y, k3[3 * j + 2] = keys4[lo + j].z;
-        for (size_t j = 0; j <= nbi; j++) leo[j] = eo[lo + j] - eo[lo], lto[j] = to[lo + j] - to[lo];
-        const size_t e0 = eo[lo], tr0 = to[lo];
-        auto s = std::make_unique<smb_surface>();
-        smb_engine* e = m->eng[i];
-        std::string msg = finish_surface(e->arr, m->mp[i], true, k3.data(), nbi, leo.data(), edges.data() + e0,
-                                         ev.data() + 2 * e0, lto.data(), tris.data() + 3 * tr0,
-                                         DeviceRefine{t.data() + e0, feat.data() + e0, q.data() + 3 * e0,
-                                                      evals.data() + e0},
-                                         *s);
-        if (!msg.empty()) {
-            errs[i] = msg;
-            return;
+    double t_device = 0, t_d2h = 0;
+    unsigned long long over_lists = 0, over_memory = 0;
+    bool graphs = true;
+    // Group by group: the device pass of group g + 1 runs while the host
+    // threads finish group g (results in two alternating page-locked sets).
+    if (!m->hosts) m->hosts = new HostGroup[2];
+    HostGroup* hosts = m->hosts;
+    std::thread worker;
+    auto t_host0 = clk::now();
+    double t_host = 0;
+    for (size_t gi = 0; gi < m->groups.size(); gi++) {
+        Group& G = m->groups[gi];
+        float dms = 0;
+        if ((rc = run_group(m, G, &dms, err, errlen))) {
+            if (worker.joinable()) worker.join();
+            return rc;
         }
-        s->stats.t_geometry = e->t_geometry;
-        s->stats.t_upload = e->t_upload;
-        m->out[i] = std::move(s);
-        m->latency[i] = ms_since(t_start);
-    });
+        graphs = graphs && (G.graph != nullptr || G.k1 == G.k0);
+        t_device += dms;
+        auto t1 = clk::now();
+        std::vector<uint32_t> fail(n);
+        HostGroup& Hc = hosts[gi % 2];
+        if ((rc = fetch_group(m, G, Hc, err, errlen)) ||
+            cudaMemcpy(fail.data(), m->d_fail.p, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+            if (worker.joinable()) worker.join();
+            return rc ? rc : (set_err(err, errlen, "copy of the failure flags failed"), SMB_ERR_CUDA);
+        }
+        t_d2h += ms_since(t1);
+        unsigned long long c[CNT_N];
+        if (cudaMemcpy(c, m->counters.p, sizeof c, cudaMemcpyDeviceToHost) == cudaSuccess) {
+            over_lists += c[CNT_OVERFLOW] - c[CNT_RETRY];  // after the retry pass
+            over_memory += c[CNT_NOMEM];
+        }
+        for (size_t i = G.s0; i < G.s1; i++) {
+            const size_t hi = m->b0[i + 1] - G.k0;
+            if (fail[i] || Hc.eo.as<uint32_t>()[hi] > Hc.ne || Hc.to.as<uint32_t>()[hi] > Hc.nt) m->redone[i] = 1;
+        }
+        if (worker.joinable()) worker.join();
+        worker = std::thread([m, gi, hosts, &errs, t_start] {
+            const Group& G = m->groups[gi];
+            const HostGroup& H = hosts[gi % 2];
+            const uint32_t* eo = H.eo.as<uint32_t>();
+            const uint32_t* to = H.to.as<uint32_t>();
+            auto one = [&](size_t i) {
+                const size_t lo = m->b0[i] - G.k0, hi = m->b0[i + 1] - G.k0, nbi = hi - lo;
+                std::vector<int32_t> k3(3 * nbi);
+                std::vector<uint32_t> leo(nbi + 1), lto(nbi + 1);
+                for (size_t j = 0; j < nbi; j++) {
+                    const int4& k = m->keys4[G.k0 + lo + j];
+                    k3[3 * j] = k.x, k3[3 * j + 1] = k.y, k3[3 * j + 2] = k.z;
+                }
+                for (size_t j = 0; j <= nbi; j++) leo[j] = eo[lo + j] - eo[lo], lto[j] = to[lo + j] - to[lo];
+                const size_t e0 = eo[lo], tr0 = to[lo];
+                auto s = std::make_unique<smb_surface>();
+                smb_engine* e = m->eng[i];
+                std::string msg = finish_surface(
+                    e->arr, m->mp[i], true, k3.data(), nbi, leo.data(), H.edges.as<uint32_t>() + e0,
+                    H.ev.as<float>() + 2 * e0, lto.data(), H.tris.as<uint32_t>() + 3 * tr0,
+                    DeviceRefine{H.t.as<float>() + e0, H.feat.as<uint32_t>() + e0, H.q.as<float>() + 3 * e0,
+                                 H.evals.as<uint32_t>() + e0},
+                    *s);
+                if (!msg.empty()) {
+                    errs[i] = msg;
+                    return;
+                }
+                s->stats.t_geometry = e->t_geometry;
+                s->stats.t_upload = e->t_upload;
+                m->out[i] = std::move(s);
+                m->latency[i] = ms_since(t_start);
+            };
+            // One host thread per structure, the largest first (longest
+            // processing time first keeps the threads evenly loaded).
+            std::vector<size_t> order;
+            for (size_t i = G.s0; i < G.s1; i++)
+                if (!m->redone[i]) order.push_back(i);
+            auto edges_of = [&](size_t i) { return eo[m->b0[i + 1] - G.k0] - eo[m->b0[i] - G.k0]; };
+            std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return edges_of(a) > edges_of(b); });
+            parallel_for(order.size(), [&](size_t k, int) {
+                SerialScope serial;
+                one(order[k]);
+            });
+        });
+    }
+    if (worker.joinable()) worker.join();
+    t_host = ms_since(t_host0) - t_device - t_d2h;
     for (size_t i = 0; i < n; i++)
         if (!errs[i].empty()) return set_err(err, errlen, "structure %zu: %s", i, errs[i].c_str()), SMB_ERR_STATE;
-    double t_host = ms_since(t2);
     auto t3b = clk::now();
     size_t n_redone = 0;
     for (size_t i = 0; i < n; i++) {
@@ -598,17 +781,20 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
         T = smb_multi_times{};
         T.structures = n;
         T.redone = n_redone;
-        T.bricks = nb;
-        T.samples = size_t(nb) * size_t(m->cfg.brick + 1) * size_t(m->cfg.brick + 1) * size_t(m->cfg.brick + 1);
+        T.bricks = m->n_bricks;
+        T.samples = size_t(m->n_bricks) * size_t(m->cfg.brick + 1) * size_t(m->cfg.brick + 1) * size_t(m->cfg.brick + 1);
         T.t_setup = m->t_setup;
         T.t_tune = m->t_tune;
         T.t_classify = cms;
-        T.t_device = dms;
+        T.t_device = t_device;
         T.t_d2h = t_d2h;
         T.t_host = t_host;
         T.t_redo = t_redo;
         T.t_total = ms_since(t_start);
-        T.graph = m->graph != nullptr;
+        T.graph = graphs ? 1 : 0;
+        T.groups = m->groups.size();
+        T.over_lists = over_lists;
+        T.over_memory = over_memory;
     }
     return SMB_OK;
 }

@@ -92,7 +92,9 @@ MULTI_TIMES = ["t_setup", "t_tune", "t_classify", "t_device", "t_d2h", "t_host",
 
 
 class MultiTimes(C.Structure):
-    _fields_ = [(f, C.c_size_t) for f in MULTI_COUNTS] + [(f, C.c_double) for f in MULTI_TIMES] + [("graph", C.c_int)]
+    _fields_ = [(f, C.c_size_t) for f in MULTI_COUNTS] + [(f, C.c_double) for f in MULTI_TIMES] + \
+               [("graph", C.c_int), ("groups", C.c_size_t), ("over_lists", C.c_ulonglong),
+                ("over_memory", C.c_ulonglong)]
 
 
 class BatchInfo(C.Structure):
