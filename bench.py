@@ -47,11 +47,13 @@ def args_():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="rings58800", choices=["rings58800", "globule330", "shell2400k"])
+    p.add_argument("--workload", default="rings58800",
+                   choices=["rings58800", "globule330", "shell2400k", "batch512"])
     p.add_argument("--refine", default=None, choices=[None, "exact", "fast"])
     p.add_argument("--spacing", type=float, default=None, help="override the workload's grid spacing")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-fast", action="store_true", help="skip the fast-mode (plain vs warm start) leg")
     return p.parse_args()
 
 
@@ -140,10 +142,50 @@ def cpu_leg(w, budget_s=20.0):
     return eng, sample, spb, k, len(bricks)
 
 
+def run_reference_batch(a):
+    """The CPU restatement on every 16th structure of the batch (each one's
+    mesh stage: classification, sampling, marching cubes, f64 refinement;
+    the reference's CPU fast mode is its exact mode): structures/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from sesmesh_b200 import workloads
+    O.build()
+    items = workloads.batch512()[::16]
+    engs = []
+    for it in items:
+        e = O.Engine(it["spheres"], it["probe"], it["spacing"], 10)
+        engs.append((e, e.classify()[0]))
+    for _ in range(max(1, a.warmup)):
+        engs[0][0].mesh_sample(engs[0][1])
+    times = []
+    for _ in range(a.steps):
+        t = 0.0
+        for e, bricks in engs:
+            t0 = time.perf_counter()
+            if len(bricks):
+                e.mesh_sample(bricks)
+            t += time.perf_counter() - t0
+        times.append(t)
+    value = len(engs) / float(np.mean(times))
+    line = {
+        "impl": "reference", "metric": "structures/s (batched SES meshes, fast mode + learned warm start)",
+        "value": value, "unit": "structures/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+        "config": {"workload": "batch512 (every 16th structure: %d)" % len(engs)},
+        "cpu_baseline": {"value": value, "unit": "structures/s", "cores": O.threads(), "kind": "port",
+                         "sample": "every 16th of the 512 structures, whole mesh stage each"},
+        "e2e": {"value": value, "unit": "structures/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if a.workload == "batch512":
+        return run_reference_batch(a)
     w = workload(a.workload, a.refine, a.spacing)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
@@ -278,6 +320,8 @@ def run_ours(a):
         "gpu_launches": int(launches),
         "clocks": clk,
     }
+    if rank == 0 and world == 1 and not a.no_fast and w["refine"] == "exact":
+        line["fast_mode"] = fast_leg(w, params, st, grid_points)
     if rank == 0 and world == 1 and not a.no_cpu:
         ceng, sample, spb_, k, nb = cpu_leg(w)
         t, _ = ceng.mesh_sample(sample)
@@ -286,10 +330,147 @@ def run_ours(a):
                                 "kind": "port",
                                 "sample": "every %d-th of %d surface bricks (%d bricks, %.1f s): CPU oracle evaluate + "
                                           "mesh_brick (exact f64 refinement)" % (k, nb, len(sample), t)}
+        # The same restatement on one core, on a smaller sample.
+        cores = O.threads()
+        O.set_threads(1)
+        one = sample[:: max(1, 4 * cores)]
+        t1, _ = ceng.mesh_sample(one)
+        O.set_threads(cores)
+        line["cpu_baseline_one_core"] = {"value": len(one) * spb_ / t1 / 1e6, "unit": "Mgridpts/s", "cores": 1,
+                                         "kind": "port", "sample": "%d surface bricks (%.1f s)" % (len(one), t1)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     del out
     eng.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def fast_leg(w, params, exact_stats, grid_points, reps=2):
+    """Fast mode on the same workload, plain f32 refinement against the
+    learned warm start: end to end through the engine (arrangement, upload,
+    device stage, copies, host placement, assembly, measure), device
+    refinement time, field evaluations per edge, area and volume against
+    exact mode, and vertex |F| from the exact f64 field on a sample of
+    vertices."""
+    from sesmesh_b200 import native
+    from sesmesh_b200 import surface as S
+    from sesmesh_b200 import warm_start
+    fp = params.with_refine("fast")
+    out = {}
+    for mode in ("plain", "warm"):
+        e2e, dev_refine = [], []
+        st = None
+        for r in range(reps + 1):
+            t0 = time.perf_counter()
+            eng = S.SurfaceEngine(w["spheres"], fp)
+            mlp = None
+            if mode == "warm":
+                mlp = native.Mlp(eng.dev, warm_start.load())
+                eng.set_warm_start(mlp)
+            mesh = eng.mesh()
+            ms = 1e3 * (time.perf_counter() - t0)
+            if r:  # the first is a warm-up
+                e2e.append(ms)
+            st = mesh.stats
+            t = eng.run_device()
+            dev_refine.append(t["total"] - t["substates"] - t["gather"] - t["sample"] - t["mc"])
+            if r == reps:
+                pos = mesh.positions
+                pick = pos[:: max(1, len(pos) // 200000)].astype(np.float64)
+                f = np.abs(eng.field(pick))
+            mesh.close()
+            eng.close()
+        e2e_ms = float(np.mean(e2e))
+        out[mode] = {
+            "e2e_ms_per_mesh": e2e_ms, "e2e_Mgridpts_s": grid_points / (e2e_ms / 1e3) / 1e6,
+            "device_refine_ms": float(np.median(dev_refine)),
+            "evaluations": int(st["refine_evaluations"]), "edges": int(st["vertices"]),
+            "evaluations_per_edge": st["refine_evaluations"] / max(1, st["vertices"]),
+            "cpu_refined_edges": int(st["refine_cpu_edges"]),
+            "area_rel_vs_exact": abs(st["area"] - exact_stats["area"]) / abs(exact_stats["area"]),
+            "volume_rel_vs_exact": abs(st["volume"] - exact_stats["volume"]) / abs(exact_stats["volume"]),
+            "vertex_F_max": float(f.max()) if len(f) else 0.0,
+            "vertex_F_rms": float(np.sqrt(np.mean(f * f))) if len(f) else 0.0,
+            "vertex_F_sample": int(len(f)),
+            "stages_ms": {k: st[k] for k in ("t_geometry", "t_upload", "t_device", "t_d2h", "t_host_refine",
+                                             "t_assemble", "t_measure")},
+        }
+    p, q = out["plain"], out["warm"]
+    out["warm_vs_plain"] = {"e2e_speedup": p["e2e_ms_per_mesh"] / q["e2e_ms_per_mesh"],
+                            "device_refine_speedup": p["device_refine_ms"] / max(q["device_refine_ms"], 1e-9),
+                            "evaluations_saved": 1.0 - q["evaluations"] / max(1, p["evaluations"])}
+    return out
+
+
+def run_batch(a):
+    """Config: 512 seeded structures in one device pass per group (fast mode,
+    learned warm start, autotuned brick edge, caps and gather block)."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from sesmesh_b200 import native, warm_start, workloads
+    from sesmesh_b200 import surface as S
+    items = workloads.batch512()
+    structs = [(it["spheres"], S.SurfaceParams.ses(it["probe"]).with_spacing(it["spacing"])) for it in items]
+    b = S.MultiBatch(structs, device=local)
+    mlp = native.Mlp(b.dev, warm_start.load())
+    b.set_warm_start(mlp)
+    cfg = b.tune()
+    for _ in range(max(3, a.warmup)):
+        b.run()
+    clocks = Clocks(local)
+    runs, lats = [], []
+    for _ in range(a.steps):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = b.run()
+        r["wall_ms"] = 1e3 * (time.perf_counter() - t0)
+        runs.append(r)
+        lats.append(b.latency())
+    clk = clocks.stop()
+    wall = float(np.mean([r["wall_ms"] for r in runs]))
+    t = torch.tensor([wall], dtype=torch.float64, device=dev)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    wall = float(t.item())
+    lat = np.concatenate(lats)
+    last = runs[-1]
+    line = {
+        "metric": "structures/s (batched SES meshes, fast mode + learned warm start)",
+        "value": world * len(items) / (wall / 1e3), "unit": "structures/s", "n_gpus": world, "steps": a.steps,
+        "warmup": max(3, a.warmup), "ms_per_step": wall, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+        "config": {"workload": "batch512: 512 globules, atoms log-uniform 20-5000, probe U(1.2, 1.4), "
+                               "spacing in {0.1, 0.25, 0.5} A", "atoms": int(sum(len(it["spheres"]) for it in items)),
+                   "tuned": cfg, "groups": int(last["groups"]), "graph": bool(last["graph"]),
+                   "parallelism": "replicas x%d" % world},
+        "grid_Mpts_s": world * last["samples"] / (wall / 1e3) / 1e6,
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "stages_ms": {k: float(np.mean([r[k] for r in runs])) for k in ("t_classify", "t_device", "t_d2h", "t_host",
+                                                                         "t_redo", "t_total")},
+        "once_ms": {"t_setup": last["t_setup"], "t_tune": last["t_tune"]},
+        "bricks": int(last["bricks"]), "samples": int(last["samples"]), "redone": int(last["redone"]),
+        "e2e": {"value": world * len(items) / (wall / 1e3), "unit": "structures/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": None},
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -325,6 +506,8 @@ def main():
     a = args_()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "batch512":
+        run_batch(a)
     else:
         run_ours(a)
 

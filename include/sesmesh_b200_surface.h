@@ -55,6 +55,12 @@ void smb_engine_free(smb_engine* e);
 int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size_t errlen);
 size_t smb_engine_bricks(const smb_engine* e);
 int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen);
+/* The exact SES field (f64) at n points (3 doubles each), on the host
+ * threads: SesField::value (field/point.rs:496-738) wherever |F| is below
+ * the refinement band sqrt(3) h 1.01 (the candidates of the point, as the
+ * refinement evaluates them), clamped to -band beyond it inside.  For the
+ * distance of mesh vertices to the surface. */
+int smb_engine_field(const smb_engine* e, const double* points, size_t n, double* values);
 /* The engine's device batch (sizes, counters, operation counts). */
 smb_batch* smb_engine_batch(smb_engine* e);
 /* Learned warm start of fast mode (no counterpart in the reference): the

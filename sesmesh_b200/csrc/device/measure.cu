@@ -1,0 +1,535 @@
+// Validation, components, area and volume, and triangle grouping of an
+// assembled mesh on the device: validate_with, components_with,
+// triangle_area_volume and group_by_component (crates/sesmesh/src/mesh/
+// mod.rs:91-330, 638-700; mesh/post.rs:14-32), with the host mesher's
+// results bit for bit (host/mesher.cpp defects, components_and_group):
+//   * defects: non-finite positions, normals not of unit length, triangle
+//     indices out of range (then nothing else is counted), repeated or zero-
+//     area triangles, undirected edges not used exactly once in each
+//     direction, duplicate triangles;
+//   * union-find linking the larger root to the smaller, so every root is
+//     its component's smallest vertex whatever the order of the links;
+//     components numbered by their root;
+//   * area and volume in f64 (the first vertex as origin) summed per
+//     component within fixed 16,384-triangle chunks in triangle order, then
+//     over the chunks in chunk order: the host's operations in the host's
+//     order;
+//   * Euler characteristic from the distinct undirected edges;
+//   * triangles regrouped by component, relative order kept.
+// Edges and duplicate triangles are found with open-addressing hash tables
+// in HBM (linear probing, half full at most); the order-dependent parts
+// (the sums, the regrouping) follow the host's order exactly.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "../host/mesher.hpp"
+#include "../runtime.hpp"
+#include "kernels.hpp"
+#include "measure.hpp"
+
+namespace smb {
+namespace {
+
+constexpr uint64_t EMPTY = ~0ull;
+constexpr uint32_t SUM_CHUNK = 1u << 14;  // triangles per area/volume chunk, as the host
+constexpr int CHUNK_COMPS = 16;           // components one chunk may hold on the device
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser
+    x ^= x >> 30;
+    x *= 0xbf58476d1ce4e5b9ull;
+    x ^= x >> 27;
+    x *= 0x94d049bb133111ebull;
+    return x ^ (x >> 31);
+}
+
+__device__ __forceinline__ void block_add(unsigned long long* dst, unsigned long long v) {
+    // Warp sums, one atomic per warp.
+    for (int o = 16; o; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+__global__ void k_vertex_checks(const float* pos, const float* nrm, uint32_t nv, unsigned long long* bad) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long b = 0;
+    if (v < nv) {
+        const float* p = pos + 3 * size_t(v);
+        if (!(isfinite(p[0]) && isfinite(p[1]) && isfinite(p[2]))) b++;
+        if (nrm) {
+            const float* q = nrm + 3 * size_t(v);
+            float len2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+            if (!(isfinite(q[0]) && isfinite(q[1]) && isfinite(q[2]) && fabsf(len2 - 1.0f) < 1e-3f)) b++;
+        }
+    }
+    block_add(bad, b);
+}
+
+__device__ __forceinline__ void area_volume(const float* pos, const uint32_t* t, const double o[3], double& a,
+                                            double& v) {
+    double p[3][3];
+    for (int q = 0; q < 3; q++)
+        for (int k = 0; k < 3; k++) p[q][k] = double(pos[3 * size_t(t[q]) + k]) - o[k];
+    double e1[3] = {p[1][0] - p[0][0], p[1][1] - p[0][1], p[1][2] - p[0][2]};
+    double e2[3] = {p[2][0] - p[0][0], p[2][1] - p[0][1], p[2][2] - p[0][2]};
+    double c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+    a = 0.5 * sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+    double x[3] = {p[1][1] * p[2][2] - p[1][2] * p[2][1], p[1][2] * p[2][0] - p[1][0] * p[2][2],
+                   p[1][0] * p[2][1] - p[1][1] * p[2][0]};
+    v = (p[0][0] * x[0] + p[0][1] * x[1] + p[0][2] * x[2]) / 6.0;
+}
+
+__global__ void k_index_checks(const uint32_t* tris, uint32_t nt, uint32_t nv, unsigned long long* oob) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long b = 0;
+    if (t < nt) {
+        const uint32_t* T = tris + 3 * size_t(t);
+        b = (T[0] >= nv || T[1] >= nv || T[2] >= nv) ? 1 : 0;
+    }
+    block_add(oob, b);
+}
+
+__global__ void k_triangle_checks(const float* pos, const uint32_t* tris, uint32_t nt, unsigned long long* bad) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long b = 0;
+    if (t < nt) {
+        const uint32_t* T = tris + 3 * size_t(t);
+        double o[3] = {double(pos[0]), double(pos[1]), double(pos[2])};
+        double a, v;
+        area_volume(pos, T, o, a, v);
+        b = (T[0] == T[1] || T[1] == T[2] || T[0] == T[2] || a == 0.0) ? 1 : 0;
+    }
+    block_add(bad, b);
+}
+
+// Undirected edge (lo, hi) of every triangle side a -> b: counts of uses
+// a < b (low half) and a > b (high half).
+__global__ void k_edge_insert(const uint32_t* tris, uint32_t nt, unsigned long long* keys, unsigned long long* cnt,
+                              uint64_t mask) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const uint32_t* T = tris + 3 * size_t(t);
+    for (int k = 0; k < 3; k++) {
+        uint32_t a = T[k], b = T[(k + 1) % 3];
+        uint64_t key = (uint64_t(min(a, b)) << 32) | max(a, b);
+        for (uint64_t s = mix64(key) & mask, probes = 0; probes <= mask; s = (s + 1) & mask, probes++) {
+            unsigned long long prev = atomicCAS(&keys[s], EMPTY, key);
+            if (prev == EMPTY || prev == key) {
+                atomicAdd(&cnt[s], a < b ? 1ull : (1ull << 32));
+                break;
+            }
+        }
+    }
+}
+
+__global__ void k_edge_check(const unsigned long long* keys, const unsigned long long* cnt, uint64_t cap,
+                             unsigned long long* bad) {
+    uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    unsigned long long b = 0;
+    if (s < cap && keys[s] != EMPTY) b = (cnt[s] == ((1ull << 32) | 1ull)) ? 0 : 1;
+    block_add(bad, b);
+}
+
+// Duplicate triangles (equal vertex sets): the first of each set takes a
+// slot, every later one counts.
+__global__ void k_duplicates(const uint32_t* tris, uint32_t nt, uint32_t* slots, uint64_t mask,
+                             unsigned long long* bad) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long b = 0;
+    if (t < nt) {
+        const uint32_t* T = tris + 3 * size_t(t);
+        uint32_t a0 = T[0], a1 = T[1], a2 = T[2], x;
+        if (a0 > a1) x = a0, a0 = a1, a1 = x;
+        if (a1 > a2) x = a1, a1 = a2, a2 = x;
+        if (a0 > a1) x = a0, a0 = a1, a1 = x;
+        uint64_t h = mix64((uint64_t(a0) << 32 | a1) ^ mix64(a2));
+        for (uint64_t s = h & mask, probes = 0; probes <= mask; s = (s + 1) & mask, probes++) {
+            uint32_t prev = atomicCAS(&slots[s], 0u, t + 1);
+            if (prev == 0) break;
+            const uint32_t* U = tris + 3 * size_t(prev - 1);
+            uint32_t b0 = U[0], b1 = U[1], b2 = U[2];
+            if (b0 > b1) x = b0, b0 = b1, b1 = x;
+            if (b1 > b2) x = b1, b1 = b2, b2 = x;
+            if (b0 > b1) x = b0, b0 = b1, b1 = x;
+            if (a0 == b0 && a1 == b1 && a2 == b2) {
+                b = 1;
+                break;
+            }
+        }
+    }
+    block_add(bad, b);
+}
+
+// Parent pointers are read from L2 (__ldcg): other blocks change them with
+// atomics, and a stale L1 copy could make a root look like a root forever.
+// Links only ever lower a parent, so every retry makes progress; the loops
+// are bounded all the same and report a failure (the host then measures).
+constexpr uint32_t UF_LIMIT = 1u << 22;
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x, unsigned long long* fail) {
+    for (uint32_t it = 0; it < UF_LIMIT; it++) {
+        uint32_t p = __ldcg(parent + x);
+        if (p == x) return x;
+        uint32_t g = __ldcg(parent + p);
+        if (g != p) atomicCAS(&parent[x], p, g);
+        x = g;
+    }
+    atomicAdd(fail, 1ull);
+    return x;
+}
+
+__device__ __forceinline__ void uf_unite(uint32_t* parent, uint32_t a, uint32_t b, unsigned long long* fail) {
+    for (uint32_t it = 0; it < UF_LIMIT; it++) {
+        uint32_t ra = uf_find(parent, a, fail), rb = uf_find(parent, b, fail);
+        if (ra == rb) return;
+        uint32_t lo = min(ra, rb), hi = max(ra, rb);
+        if (atomicCAS(&parent[hi], hi, lo) == hi) return;
+    }
+    atomicAdd(fail, 1ull);
+}
+
+__global__ void k_uf_init(uint32_t* parent, uint32_t nv) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < nv) parent[v] = v;
+}
+
+__global__ void k_uf_link(const uint32_t* tris, uint32_t nt, uint32_t* parent, unsigned long long* fail) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const uint32_t* T = tris + 3 * size_t(t);
+    uf_unite(parent, T[0], T[1], fail);
+    uf_unite(parent, T[0], T[2], fail);
+}
+
+// Roots (a component's smallest vertex) and the root flags for numbering.
+__global__ void k_uf_roots(uint32_t* parent, uint32_t nv, uint32_t* is_root, unsigned long long* fail) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    uint32_t r = uf_find(parent, v, fail);
+    is_root[v] = r == v ? 1u : 0u;
+}
+
+__global__ void k_component_ids(const uint32_t* parent, const uint32_t* cid_of_root, uint32_t nv, uint32_t* id,
+                                unsigned long long* comp_vertices) {
+    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    uint32_t r = parent[v];
+    for (uint32_t it = 0; it < UF_LIMIT && parent[r] != r; it++) r = parent[r];
+    uint32_t c = cid_of_root[r];
+    id[v] = c;
+    atomicAdd(&comp_vertices[c], 1ull);
+}
+
+// Per chunk of SUM_CHUNK triangles, in order: each component's triangle
+// count and area and volume partial sums (sequential, the host's order).
+struct Partial {
+    uint32_t comp, chunk;
+    unsigned long long t;
+    double a, v;
+};
+
+__global__ void k_chunk_partials(const float* pos, const uint32_t* tris, uint32_t nt, const uint32_t* id,
+                                 Partial* out, unsigned long long* n_out, unsigned long long* overflow) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n_chunks = (nt + SUM_CHUNK - 1) / SUM_CHUNK;
+    if (c >= n_chunks) return;
+    double o[3] = {double(pos[0]), double(pos[1]), double(pos[2])};
+    Partial acc[CHUNK_COMPS];
+    int na = 0;
+    const uint32_t t1 = min(nt, (c + 1) * SUM_CHUNK);
+    for (uint32_t t = c * SUM_CHUNK; t < t1; t++) {
+        const uint32_t* T = tris + 3 * size_t(t);
+        uint32_t comp = id[T[0]];
+        double a, v;
+        area_volume(pos, T, o, a, v);
+        int e = -1;
+        for (int q = 0; q < na; q++)
+            if (acc[q].comp == comp) {
+                e = q;
+                break;
+            }
+        if (e < 0) {
+            if (na == CHUNK_COMPS) {
+                atomicAdd(overflow, 1ull);
+                return;
+            }
+            e = na++;
+            acc[e] = Partial{comp, c, 0ull, 0.0, 0.0};
+        }
+        acc[e].t++, acc[e].a += a, acc[e].v += v;
+    }
+    unsigned long long base = atomicAdd(n_out, (unsigned long long)na);
+    for (int q = 0; q < na; q++) out[base + q] = acc[q];
+}
+
+__global__ void k_iota(uint32_t* v, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+// key[i] = the chunk (by_comp = false) or component of partial idx[i].
+__global__ void k_part_keys(const Partial* parts, const uint32_t* idx, uint32_t n, uint32_t* key, bool by_comp) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) key[i] = by_comp ? parts[idx[i]].comp : parts[idx[i]].chunk;
+}
+
+// Partials sorted by (component, chunk): each component sums its chunks in
+// chunk order (the host's order).
+__global__ void k_component_sums(const Partial* parts, const uint32_t* sorted_idx, uint32_t n_parts,
+                                 const uint32_t* first, uint32_t n_comp, unsigned long long* tris_out, double* area,
+                                 double* volume) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_comp) return;
+    unsigned long long t = 0;
+    double a = 0.0, v = 0.0;
+    for (uint32_t i = first[c]; i < first[c + 1]; i++) {
+        const Partial& p = parts[sorted_idx[i]];
+        t += p.t, a += p.a, v += p.v;
+    }
+    tris_out[c] = t, area[c] = a, volume[c] = v;
+}
+
+__global__ void k_first_of_component(const uint32_t* sorted_comp, uint32_t n, uint32_t* first, uint32_t n_comp) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    // first[c] = the first sorted index with component >= c.
+    uint32_t lo = i == 0 ? 0 : sorted_comp[i - 1] + 1, hi = i == n ? n_comp : sorted_comp[i];
+    for (uint32_t c = lo; c <= hi && c <= n_comp; c++) first[c] = i;
+}
+
+__global__ void k_euler_edges(const unsigned long long* keys, uint64_t cap, const uint32_t* id,
+                              unsigned long long* comp_edges) {
+    uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (s >= cap || keys[s] == EMPTY) return;
+    atomicAdd(&comp_edges[id[uint32_t(keys[s] >> 32)]], 1ull);
+}
+
+__global__ void k_triangle_keys(const uint32_t* tris, uint32_t nt, const uint32_t* id, uint32_t* key,
+                                uint32_t* idx) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    key[t] = id[tris[3 * size_t(t)]];
+    idx[t] = t;
+}
+
+__global__ void k_gather_triangles(const uint32_t* tris, const uint32_t* idx, uint32_t nt, uint32_t* out) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    const uint32_t* T = tris + 3 * size_t(idx[t]);
+    uint32_t* U = out + 3 * size_t(t);
+    U[0] = T[0], U[1] = T[1], U[2] = T[2];
+}
+
+uint64_t pow2_at_least(uint64_t v) {
+    uint64_t p = 1024;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+unsigned bits_for(uint32_t n) {
+    unsigned b = 1;
+    while (b < 32 && (uint64_t(1) << b) <= n) b++;
+    return b;
+}
+
+#define MCK(call)                                                                          \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            if (msg) *msg = std::string(#call) + ": " + cudaGetErrorString(e_);            \
+            return false;                                                                  \
+        }                                                                                  \
+    } while (0)
+
+}  // namespace
+
+void MeasureScratch::release() {
+    for (DBuf* b : {&pos, &nrm, &tris, &tris_out, &keys, &cnt, &dup, &parent, &flag, &cid, &id, &counters, &comp_v,
+                    &comp_t, &comp_e, &area, &volume, &parts, &pkey, &pidx, &pkey2, &pidx2, &first, &tkey, &tidx,
+                    &tkey2, &tidx2, &tiles, &cub})
+        b->release();
+}
+
+bool measure_on_device(smb_device* d, smbh::Mesh& m, std::vector<smbh::Component>& comps, size_t* bad,
+                       MeasureScratch& S, std::string* msg) {
+    using smbh::Component;
+    cudaStream_t s = d->stream;
+    const size_t nv = m.positions.size(), nt = m.triangles.size();
+    if (nv >= (size_t(1) << 31) || nt >= (size_t(1) << 31)) {
+        if (msg) *msg = "mesh too large for the device measure";
+        return false;
+    }
+    char e[256];
+    auto R = [&](DBuf& b, size_t bytes) { return b.reserve(std::max<size_t>(bytes, 16), e, sizeof e) == 0; };
+    const uint64_t ecap = pow2_at_least(uint64_t(nt) * 3 + 16), dcap = pow2_at_least(uint64_t(nt) * 2 + 16);
+    const uint32_t n_chunks = uint32_t((nt + SUM_CHUNK - 1) / SUM_CHUNK);
+    const size_t max_parts = size_t(n_chunks) * CHUNK_COMPS;
+    if (!R(S.pos, nv * 12) || !R(S.nrm, nv * 12) || !R(S.tris, nt * 12) || !R(S.tris_out, nt * 12) ||
+        !R(S.keys, ecap * 8) || !R(S.cnt, ecap * 8) || !R(S.dup, dcap * 4) || !R(S.parent, nv * 4) ||
+        !R(S.flag, nv * 4) || !R(S.cid, nv * 4) || !R(S.id, nv * 4) || !R(S.counters, 64) ||
+        !R(S.parts, max_parts * sizeof(Partial)) || !R(S.pkey, max_parts * 4) || !R(S.pidx, max_parts * 4) ||
+        !R(S.pkey2, max_parts * 4) || !R(S.pidx2, max_parts * 4) || !R(S.tkey, nt * 4) || !R(S.tidx, nt * 4) ||
+        !R(S.tkey2, nt * 4) || !R(S.tidx2, nt * 4) || !R(S.tiles, size_t(scan_tiles_needed(uint32_t(nv))) * 8 + 64)) {
+        if (msg) *msg = std::string("device memory for the measure: ") + e;
+        return false;
+    }
+    unsigned long long* cnt = S.counters.as<unsigned long long>();  // 0 bad, 1 oob, 2 parts, 3 overflow, 4 comps, 5 union-find
+    MCK(cudaMemsetAsync(cnt, 0, 64, s));
+    MCK(cudaMemcpyAsync(S.pos.p, m.positions.data(), nv * 12, cudaMemcpyHostToDevice, s));
+    const bool normals = !m.normals.empty();
+    if (normals) MCK(cudaMemcpyAsync(S.nrm.p, m.normals.data(), nv * 12, cudaMemcpyHostToDevice, s));
+    MCK(cudaMemcpyAsync(S.tris.p, m.triangles.data(), nt * 12, cudaMemcpyHostToDevice, s));
+    const float* pos = S.pos.as<float>();
+    const uint32_t* tris = S.tris.as<uint32_t>();
+    auto blocks = [](uint64_t n) { return unsigned((n + 255) / 256); };
+    if (nv) k_vertex_checks<<<blocks(nv), 256, 0, s>>>(pos, normals ? S.nrm.as<float>() : nullptr, uint32_t(nv), cnt);
+    if (nt) k_index_checks<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), uint32_t(nv), cnt + 1);
+    unsigned long long c2[2];
+    MCK(cudaMemcpyAsync(c2, cnt, 16, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+    if (c2[1]) {  // indices out of range: the host counts one defect more and stops there
+        *bad = size_t(c2[0] + 1);
+        return true;
+    }
+    if (nt) {
+        k_triangle_checks<<<blocks(nt), 256, 0, s>>>(pos, tris, uint32_t(nt), cnt);
+        MCK(cudaMemsetAsync(S.keys.p, 0xFF, ecap * 8, s));
+        MCK(cudaMemsetAsync(S.cnt.p, 0, ecap * 8, s));
+        MCK(cudaMemsetAsync(S.dup.p, 0, dcap * 4, s));
+        k_edge_insert<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), S.keys.as<unsigned long long>(),
+                                                 S.cnt.as<unsigned long long>(), ecap - 1);
+        k_edge_check<<<blocks(ecap), 256, 0, s>>>(S.keys.as<unsigned long long>(), S.cnt.as<unsigned long long>(), ecap,
+                                                  cnt);
+        k_duplicates<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), S.dup.as<uint32_t>(), dcap - 1, cnt);
+    }
+    unsigned long long nbad = 0;
+    MCK(cudaMemcpyAsync(&nbad, cnt, 8, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+    *bad = size_t(nbad);
+    if (nbad) return true;
+    // Components.
+    uint32_t* parent = S.parent.as<uint32_t>();
+    if (nv) {
+        k_uf_init<<<blocks(nv), 256, 0, s>>>(parent, uint32_t(nv));
+        if (nt) k_uf_link<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), parent, cnt + 5);
+        k_uf_roots<<<blocks(nv), 256, 0, s>>>(parent, uint32_t(nv), S.flag.as<uint32_t>(), cnt + 5);
+        launch_scan(S.flag.as<uint32_t>(), uint32_t(nv), S.cid.as<uint32_t>(), nullptr,
+                    S.tiles.as<unsigned long long>(), cnt + 4, s);
+    }
+    unsigned long long n_comp = 0, uf_fail = 0;
+    MCK(cudaMemcpyAsync(&n_comp, cnt + 4, 8, cudaMemcpyDeviceToHost, s));
+    MCK(cudaMemcpyAsync(&uf_fail, cnt + 5, 8, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+    if (uf_fail) {
+        if (msg) *msg = "union-find gave up";
+        return false;
+    }
+    const uint32_t nc = uint32_t(n_comp);
+    if (!R(S.comp_v, size_t(nc) * 8) || !R(S.comp_t, size_t(nc) * 8) || !R(S.comp_e, size_t(nc) * 8) ||
+        !R(S.area, size_t(nc) * 8) || !R(S.volume, size_t(nc) * 8) || !R(S.first, (size_t(nc) + 1) * 4)) {
+        if (msg) *msg = std::string("device memory for the measure: ") + e;
+        return false;
+    }
+    MCK(cudaMemsetAsync(S.comp_v.p, 0, size_t(nc) * 8 + 8, s));
+    MCK(cudaMemsetAsync(S.comp_e.p, 0, size_t(nc) * 8 + 8, s));
+    uint32_t* id = S.id.as<uint32_t>();
+    if (nv) k_component_ids<<<blocks(nv), 256, 0, s>>>(parent, S.cid.as<uint32_t>(), uint32_t(nv), id,
+                                                       S.comp_v.as<unsigned long long>());
+    if (nt)
+        k_euler_edges<<<blocks(ecap), 256, 0, s>>>(S.keys.as<unsigned long long>(), ecap, id,
+                                                   S.comp_e.as<unsigned long long>());
+    // Area and volume: chunk partials, stably sorted by component (the
+    // partials of one component stay in chunk order after a stable sort by
+    // chunk, then by component).
+    unsigned long long n_parts = 0, overflow = 0;
+    if (nt) {
+        k_chunk_partials<<<blocks(n_chunks), 256, 0, s>>>(pos, tris, uint32_t(nt), id, S.parts.as<Partial>(), cnt + 2,
+                                                          cnt + 3);
+        MCK(cudaMemcpyAsync(&n_parts, cnt + 2, 8, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(&overflow, cnt + 3, 8, cudaMemcpyDeviceToHost, s));
+        MCK(cudaStreamSynchronize(s));
+        if (overflow) {
+            if (msg) *msg = "a triangle chunk holds more components than the device measure keeps";
+            return false;
+        }
+    }
+    const uint32_t np = uint32_t(n_parts);
+    auto sort_pairs = [&](const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout, uint32_t n,
+                          unsigned bits) -> bool {
+        size_t tmp = 0;
+        if (cub::DeviceRadixSort::SortPairs(nullptr, tmp, kin, kout, vin, vout, int(n), 0, int(bits), s) !=
+            cudaSuccess)
+            return false;
+        if (!R(S.cub, tmp)) return false;
+        return cub::DeviceRadixSort::SortPairs(S.cub.p, tmp, kin, kout, vin, vout, int(n), 0, int(bits), s) ==
+               cudaSuccess;
+    };
+    if (np) {
+        // Partials by chunk, then stably by component: each component's
+        // partials in chunk order.
+        Partial* parts = S.parts.as<Partial>();
+        k_iota<<<blocks(np), 256, 0, s>>>(S.pidx.as<uint32_t>(), np);
+        k_part_keys<<<blocks(np), 256, 0, s>>>(parts, S.pidx.as<uint32_t>(), np, S.pkey2.as<uint32_t>(), false);
+        if (!sort_pairs(S.pkey2.as<uint32_t>(), S.pkey.as<uint32_t>(), S.pidx.as<uint32_t>(), S.pidx2.as<uint32_t>(),
+                        np, bits_for(n_chunks))) {
+            if (msg) *msg = "partial sort failed";
+            return false;
+        }
+        k_part_keys<<<blocks(np), 256, 0, s>>>(parts, S.pidx2.as<uint32_t>(), np, S.pkey2.as<uint32_t>(), true);
+        if (!sort_pairs(S.pkey2.as<uint32_t>(), S.pkey.as<uint32_t>(), S.pidx2.as<uint32_t>(), S.pidx.as<uint32_t>(),
+                        np, bits_for(nc))) {
+            if (msg) *msg = "partial sort failed";
+            return false;
+        }
+        k_first_of_component<<<blocks(uint64_t(np) + 1), 256, 0, s>>>(S.pkey.as<uint32_t>(), np,
+                                                                        S.first.as<uint32_t>(), nc);
+        k_component_sums<<<blocks(nc), 256, 0, s>>>(parts, S.pidx.as<uint32_t>(), np, S.first.as<uint32_t>(), nc,
+                                                    S.comp_t.as<unsigned long long>(), S.area.as<double>(),
+                                                    S.volume.as<double>());
+    } else if (nc) {
+        MCK(cudaMemsetAsync(S.comp_t.p, 0, size_t(nc) * 8, s));
+        MCK(cudaMemsetAsync(S.area.p, 0, size_t(nc) * 8, s));
+        MCK(cudaMemsetAsync(S.volume.p, 0, size_t(nc) * 8, s));
+    }
+    // Triangles regrouped by component, relative order kept.
+    if (nt) {
+        k_triangle_keys<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), id, S.tkey.as<uint32_t>(), S.tidx.as<uint32_t>());
+        if (!sort_pairs(S.tkey.as<uint32_t>(), S.tkey2.as<uint32_t>(), S.tidx.as<uint32_t>(), S.tidx2.as<uint32_t>(),
+                        uint32_t(nt), bits_for(nc))) {
+            if (msg) *msg = "triangle sort failed";
+            return false;
+        }
+        k_gather_triangles<<<blocks(nt), 256, 0, s>>>(tris, S.tidx2.as<uint32_t>(), uint32_t(nt),
+                                                      S.tris_out.as<uint32_t>());
+    }
+    // Results to the host.
+    std::vector<unsigned long long> cv(nc), ct(nc), ce(nc);
+    std::vector<double> ca(nc), cvol(nc);
+    m.vertex_component.resize(nv);
+    if (nc) {
+        MCK(cudaMemcpyAsync(cv.data(), S.comp_v.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(ct.data(), S.comp_t.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(ce.data(), S.comp_e.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(ca.data(), S.area.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
+        MCK(cudaMemcpyAsync(cvol.data(), S.volume.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
+    }
+    if (nv) MCK(cudaMemcpyAsync(m.vertex_component.data(), id, nv * 4, cudaMemcpyDeviceToHost, s));
+    if (nt) MCK(cudaMemcpyAsync(m.triangles.data(), S.tris_out.p, nt * 12, cudaMemcpyDeviceToHost, s));
+    MCK(cudaStreamSynchronize(s));
+    comps.assign(nc, Component());
+    size_t start = 0;
+    for (uint32_t c = 0; c < nc; c++) {
+        Component& C = comps[c];
+        C.vertices = size_t(cv[c]);
+        C.triangles = size_t(ct[c]);
+        C.area = ca[c];
+        C.volume = cvol[c];
+        C.euler = int64_t(cv[c]) - int64_t(ce[c]) + int64_t(ct[c]);
+        C.first_triangle = start;
+        start += C.triangles;
+    }
+    return true;
+}
+
+}  // namespace smb

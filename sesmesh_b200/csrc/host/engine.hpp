@@ -6,6 +6,7 @@
 
 #include "../../../include/sesmesh_b200.h"
 #include "../../../include/sesmesh_b200_surface.h"
+#include "../device/measure.hpp"
 #include "geom.hpp"
 #include "mesher.hpp"
 
@@ -32,6 +33,7 @@ struct smb_engine {
     smb_batch_times times{};
     double t_classify = 0;
     const smb_mlp* warm = nullptr;  // warm start of fast-mode refinement
+    smb::MeasureScratch measure;    // device buffers of the validation and measure
     // Warm-start training rows of the last device run.
     bool rows_ready = false;
     std::vector<float> row_x, row_t;
@@ -48,7 +50,10 @@ struct smb_surface {
 // Host stages of one structure after its device run: placement of the
 // device's f32 roots (fast) or f64 refinement (exact), assembly,
 // validation, components and grouping; fills the statistics it can (sizes,
-// area, volume, evaluations, host stage times).  Error text or "".
+// area, volume, evaluations, host stage times).  With a device, the
+// validation and measure run there (same results), else on the host
+// threads.  Error text or "".
 std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fast, const int32_t* keys, size_t nb,
                            const uint32_t* edge_off, const uint32_t* edges, const float* edge_vals,
-                           const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s);
+                           const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s,
+                           smb_device* device = nullptr, smb::MeasureScratch* scratch = nullptr);

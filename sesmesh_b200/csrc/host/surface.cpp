@@ -39,7 +39,8 @@ void set_err(char* err, size_t len, const char* fmt, ...) {
 // area, volume, evaluations, host stage times).  Error text or "".
 std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fast, const int32_t* keys, size_t nb,
                            const uint32_t* edge_off, const uint32_t* edges, const float* edge_vals,
-                           const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s) {
+                           const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s,
+                           smb_device* device, smb::MeasureScratch* scratch) {
     auto t1 = clk::now();
     MeshOut mo;
     if (fast) place_fast(arr, mp, keys, nb, edge_off, edges, edge_vals, dev, mo);
@@ -55,10 +56,21 @@ std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fa
     mesh.vertex_patch.swap(mo.patches);
     double t_assemble = ms_since(t2);
     auto t3 = clk::now();
-    EdgeUses uses;
-    size_t bad = defects(mesh, &uses);
-    if (bad) return "mesh failed validation (" + std::to_string(bad) + " defects)";
-    components_and_group(mesh, s.comps, &uses);
+    bool measured = false;
+    if (device && scratch) {
+        size_t bad = 0;
+        std::string why;
+        if (smb::measure_on_device(device, mesh, s.comps, &bad, *scratch, &why)) {
+            if (bad) return "mesh failed validation (" + std::to_string(bad) + " defects)";
+            measured = true;
+        }
+    }
+    if (!measured) {
+        EdgeUses uses;
+        size_t bad = defects(mesh, &uses);
+        if (bad) return "mesh failed validation (" + std::to_string(bad) + " defects)";
+        components_and_group(mesh, s.comps, &uses);
+    }
     double t_measure = ms_since(t3);
     smb_surface_stats& st = s.stats;
     st.spheres = arr.n;
@@ -263,7 +275,8 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
     auto s = std::make_unique<smb_surface>();
     std::string m = finish_surface(e->arr, e->mp, fast, e->keys.data(), nb, e->edge_off.data(), e->edges.data(),
                                    e->edge_vals.data(), e->tri_off.data(), e->tris.data(),
-                                   DeviceRefine{e->t.data(), e->feat.data(), e->closest.data(), e->evals.data()}, *s);
+                                   DeviceRefine{e->t.data(), e->feat.data(), e->closest.data(), e->evals.data()}, *s,
+                                   e->dev, &e->measure);
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_STATE;
     smb_surface_stats& st = s->stats;
     st.touched_bricks = e->touched;
@@ -278,6 +291,23 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
     st.t_d2h = t_d2h;
     st.t_mesh_stage = ms_since(t_all) - st.t_assemble - st.t_measure;
     *out = s.release();
+    return SMB_OK;
+}
+
+int smb_engine_field(const smb_engine* e, const double* points, size_t n, double* values) {
+    if (!e || (n && (!points || !values))) return SMB_ERR_ARG;
+    const double band = e->mp.band;
+    // The refinement's evaluation (field/point.rs:496-738): the candidates of
+    // the point (a ball of radius 0), then the exact f64 field, which equals
+    // SesField::value within the band.
+    parallel_for((n + 255) / 256, [&](size_t c, int) {
+        Local l;
+        for (size_t i = c * 256; i < std::min(n, (c + 1) * 256); i++) {
+            V3 x = V3::at(points + 3 * i);
+            gather_local(e->arr, x, 0.0, band, l);
+            values[i] = eval_local(e->arr, x, band, l).value;
+        }
+    });
     return SMB_OK;
 }
 

@@ -178,6 +178,14 @@ class SurfaceEngine:
         _check(lib().smb_engine_mesh(self.h, C.byref(h), err, 1024), err)
         return SurfaceOutput(h)
 
+    def field(self, points):
+        """The exact f64 SES field at points (n, 3), host threads."""
+        p = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+        out = np.zeros(len(p))
+        _check(lib().smb_engine_field(self.h, _p(p, C.c_double), len(p), _p(out, C.c_double)),
+               C.create_string_buffer(8))
+        return out
+
     def set_warm_start(self, mlp):
         """Start fast-mode refinement from `mlp` (a native.Mlp on this
         engine's device; None: the linear guess)."""

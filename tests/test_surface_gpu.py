@@ -103,3 +103,22 @@ def test_empty_input_gives_an_empty_mesh():
     from sesmesh_b200 import surface as S
     out = S.compute_surface(np.zeros((0, 4)), S.SurfaceParams.ses(1.4))
     assert out.stats["triangles"] == 0 and out.stats["components"] == 0
+
+
+def test_engine_field_equals_oracle_field():
+    """smb_engine_field (the exact f64 field on the host, used for vertex
+    distances) gives the CPU back end's SesField::value bit for bit within
+    the refinement band around the surface, where it is defined."""
+    from sesmesh_b200 import surface as S, workloads
+    g = workloads.globule330()
+    eng = S.SurfaceEngine(g["spheres"], S.SurfaceParams.ses(1.4).with_spacing(0.5))
+    rng = np.random.default_rng(7)
+    verts = eng.mesh().positions.astype(np.float64)
+    pts = verts[::7] + rng.uniform(-0.3, 0.3, size=(len(verts[::7]), 3))
+    got = eng.field(pts)
+    want = O.Engine(g["spheres"], 1.4, 0.5).field(pts)
+    eng.close()
+    band = np.sqrt(3.0) * 0.5 * 1.01
+    near = np.abs(want) < 0.9 * band
+    assert near.sum() > 1000
+    assert np.array_equal(got[near].view(np.uint64), want[near].view(np.uint64))
