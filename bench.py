@@ -48,7 +48,7 @@ def args_():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="rings58800",
-                   choices=["rings58800", "globule330", "shell2400k", "batch512"])
+                   choices=["rings58800", "globule330", "globule2800", "shell2400k", "batch512"])
     p.add_argument("--refine", default=None, choices=[None, "exact", "fast"])
     p.add_argument("--spacing", type=float, default=None, help="override the workload's grid spacing")
     p.add_argument("--e2e-steps", type=int, default=2)
@@ -60,7 +60,7 @@ def args_():
 def workload(name, refine=None, spacing=None):
     from sesmesh_b200 import workloads
     w = {"rings58800": workloads.rings58800, "globule330": workloads.globule330,
-         "shell2400k": workloads.shell2400k}[name]()
+         "globule2800": workloads.globule2800, "shell2400k": workloads.shell2400k}[name]()
     if refine:
         w["refine"] = refine
     if spacing:

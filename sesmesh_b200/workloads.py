@@ -55,6 +55,13 @@ def rings58800(seed=58800, per=2800, spacing=0.25, refine="exact"):
                 copies=21, per_copy=per, ring_z=RING_Z, ring_r=RING_R)
 
 
+def globule2800(seed=58800, spacing=0.25, refine="exact"):
+    """One copy of the rings58800 unit (2,800 spheres): the profiling case."""
+    r = rings58800(seed)
+    return dict(name="globule2800", spheres=r["spheres"][:2800], probe=1.4, spacing=spacing, brick=10,
+                refine=refine)
+
+
 def shell2400k(seed=2400, per=40000, refine="exact"):
     out = np.zeros((60 * per, 4))
     m = native.synth().smb_synth_icosahedral(seed, per, 0.0, 380.0, _p(out))
