@@ -255,3 +255,110 @@ def push_fixed(x, prec):
     buf = C.create_string_buffer(600)
     n = lib().orc_push_fixed(C.c_float(x), prec, buf, 600)
     return buf.raw[:n].decode()
+
+
+# ---- the reference's own CUDA kernels (oracle/_ref, built by `make ref-gpu`) ----
+_REFGPU = None
+
+
+class _RefInput(C.Structure):
+    _fields_ = [("n_spheres", C.c_uint), ("n_circles", C.c_uint), ("n_vertices", C.c_uint),
+                ("sphere", C.c_void_p), ("status", C.c_void_p), ("nb_off", C.c_void_p), ("nb_items", C.c_void_p),
+                ("nb_items_len", C.c_uint), ("circle", C.c_void_p), ("cb_off", C.c_void_p),
+                ("cb_items", C.c_void_p), ("cb_items_len", C.c_uint), ("vertex", C.c_void_p),
+                ("grid_f", C.c_void_p), ("grid_dims", C.c_void_p), ("grid_starts", C.c_void_p * 3),
+                ("grid_items", C.c_void_p * 3), ("grid_n_items", C.c_uint * 3),
+                ("max_expanded", C.c_float), ("rho_max", C.c_float), ("probe", C.c_float), ("band", C.c_float),
+                ("cutoff2", C.c_float), ("rho", C.c_float), ("reach", C.c_float), ("margin", C.c_float),
+                ("slack", C.c_float), ("cutoffc2", C.c_float), ("h", C.c_float), ("b", C.c_uint),
+                ("sub", C.c_uint), ("bricks", C.c_void_p), ("n_bricks", C.c_uint)]
+
+
+class _RefTimes(C.Structure):
+    _fields_ = [("count_ms", C.c_double), ("scan_ms", C.c_double), ("fill_ms", C.c_double),
+                ("sample_ms", C.c_double), ("total_ms", C.c_double), ("ids", C.c_ulonglong)]
+
+
+def ref_gpu_path():
+    return os.path.join(_HERE, "_ref", "libsesmesh_refgpu.so")
+
+
+def ref_gpu_available():
+    return os.path.exists(ref_gpu_path())
+
+
+def ref_gpu_run(eng, bricks, spacing, brick, probe, reps=3):
+    """Sample values of the given surface bricks from the reference's own
+    CUDA kernels (count, host scan, fill, sample, as cuda::Resident::run)
+    with the inputs gpu.rs builds for them, and the best time of each pass
+    over `reps` runs (the first a warm-up): ((n, (b+1)^3) f32, times)."""
+    global _REFGPU
+    if _REFGPU is None:
+        L = C.CDLL(ref_gpu_path())
+        L.refgpu_run.restype = C.c_int
+        L.refgpu_run.argtypes = [C.POINTER(_RefInput), C.c_int, C.POINTER(C.c_float), C.POINTER(_RefTimes)]
+        _REFGPU = L
+    i = eng.info
+    h, b = float(spacing), int(brick)
+    sub = b // 2
+    frame = np.array([i["frame_x"], i["frame_y"], i["frame_z"]], np.int64)
+    fo = frame.astype(np.float64) * h                               # lattice.rs:62-64
+    a = eng.arrangement()
+    sph = a["spheres"]
+    n = len(sph)
+    r32 = sph[:, 3].astype(np.float32)
+    rt = np.maximum(r32 - np.float32(2e-5), np.float32(0))           # kernel.rs:42 INSIDE_TOL
+    sphere = np.stack([(sph[:, 0] - fo[0]).astype(np.float32), (sph[:, 1] - fo[1]).astype(np.float32),
+                       (sph[:, 2] - fo[2]).astype(np.float32), r32, r32 * r32, rt * rt,
+                       sph[:, 4].astype(np.float32)]).astype(np.float32).copy()
+    status = np.ascontiguousarray(a["status"], np.uint32)
+    nb_off, nb_items = eng.csr(0)
+    cb_off, cb_items = eng.csr(1)
+    circ = a["circles"]
+    nc = len(circ)
+    if nc:
+        c = circ[:, 2:12].copy()
+        c[:, 0:3] -= fo
+        circle = np.ascontiguousarray(c.T.astype(np.float32))
+    else:
+        circle = np.zeros((10, 1), np.float32)
+    vert = a["vertices"]
+    nv = len(vert)
+    vertex = np.ascontiguousarray((vert[:, :3] - fo).T.astype(np.float32)) if nv else np.zeros((3, 1), np.float32)
+    grids = [eng.grid(g) for g in range(3)]
+    grid_f = np.array([[*(gr["origin"] - fo), gr["cell"]] for gr in grids], np.float64).astype(np.float32)
+    grid_dims = np.array([gr["dims"] for gr in grids], np.uint32)
+    # batch_params (field/gpu.rs:369-400).
+    band = float(i["band"])
+    rho = 0.5 * np.sqrt(3.0) * sub * h
+    reach = probe + band + rho
+    margin = rho + 2e-3                                              # CLASSIFY_EPS
+    cutoffc = np.float32(probe + margin + 2e-3)
+    cutoff = np.float32(probe + band)
+    m = np.float32(min(max(float(i["coord_max"]), 1.0), 1e6))
+    ulp = np.nextafter(m, np.float32(np.inf)) - m
+    slack = np.float32(1e-3) + np.float32(16.0) * ulp
+    bk = np.asarray(bricks, np.int64).reshape(-1, 3) * b - frame      # frame_origins (gpu.rs:403-414)
+    bk = np.ascontiguousarray(bk, np.int32)
+    keep = [sphere, status, nb_off, nb_items, circle, cb_off, cb_items, vertex, grid_f, grid_dims, bk]
+    ri = _RefInput()
+    ri.n_spheres, ri.n_circles, ri.n_vertices = n, nc, nv
+    ri.sphere, ri.status = sphere.ctypes.data, status.ctypes.data
+    ri.nb_off, ri.nb_items, ri.nb_items_len = nb_off.ctypes.data, nb_items.ctypes.data, len(nb_items)
+    ri.circle, ri.cb_off, ri.cb_items, ri.cb_items_len = circle.ctypes.data, cb_off.ctypes.data, \
+        cb_items.ctypes.data, len(cb_items)
+    ri.vertex, ri.grid_f, ri.grid_dims = vertex.ctypes.data, grid_f.ctypes.data, grid_dims.ctypes.data
+    for g, gr in enumerate(grids):
+        keep += [gr["starts"], gr["items"]]
+        ri.grid_starts[g], ri.grid_items[g], ri.grid_n_items[g] = gr["starts"].ctypes.data, \
+            gr["items"].ctypes.data, len(gr["items"])
+    ri.max_expanded, ri.rho_max = float(i["max_expanded"]), float(i["rho_max"])
+    ri.probe, ri.band, ri.cutoff2, ri.rho = probe, band, float(cutoff * cutoff), rho
+    ri.reach, ri.margin, ri.slack, ri.cutoffc2, ri.h = reach, margin, float(slack), float(cutoffc * cutoffc), h
+    ri.b, ri.sub, ri.bricks, ri.n_bricks = b, sub, bk.ctypes.data, len(bk)
+    out = np.zeros((len(bk), (b + 1) ** 3), np.float32)
+    t = _RefTimes()
+    rc = _REFGPU.refgpu_run(C.byref(ri), int(reps), _p(out, C.c_float), C.byref(t))
+    if rc:
+        raise RuntimeError("reference kernels failed (%d)" % rc)
+    return out, {name: getattr(t, name) for name, _ in t._fields_}
