@@ -268,9 +268,9 @@ def run_ours(a):
     mean_ms = max_over_ranks(float(np.mean(step_ms)))
     value = world * grid_points / (mean_ms / 1e3) / 1e6
     stage = {k: float(np.mean([p[k] for p in parts])) for k in ("classify", "substates", "gather", "sample", "mc")}
-    if w["refine"] == "fast":
-        stage["refine"] = float(np.mean([p["total"] - p["substates"] - p["gather"] - p["sample"] - p["mc"]
-                                         for p in parts]))
+    # Vertex refinement on the device: f32 in fast mode, f64 in exact mode.
+    stage["refine"] = float(np.mean([p["total"] - p["substates"] - p["gather"] - p["sample"] - p["mc"]
+                                     for p in parts]))
     dominant = max(stage, key=stage.get)
 
     # End to end through the public API, host arrays in, mesh out.
@@ -290,8 +290,9 @@ def run_ours(a):
     info = eng.batch_info()
     h2d = int(info["resident_bytes"])
     d2h = int(n_bricks * 16 + (n_bricks + 1) * 8 + st["vertices"] * 12 + st["triangles"] * 12)
-    if w["refine"] == "fast":
-        d2h += int(st["vertices"] * 24)
+    # Per edge: t, feature, closest point, evaluations (fast); position,
+    # normal, atom, patch, t, evaluations (exact, refined on the device).
+    d2h += int(st["vertices"] * (24 if w["refine"] == "fast" else 37))
 
     pk, pk_kind = peaks()
     ops, owned = eng.count_ops()

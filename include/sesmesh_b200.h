@@ -177,12 +177,41 @@ int smb_refine(smb_resident* res, smb_batch* batch, double* ms, char* err, size_
  * converged (DeviceBatch::edge_*, batch.rs:222-232). */
 int smb_batch_edges(const smb_batch* batch, float* t, uint32_t* feat, float* closest, uint32_t* evals);
 
+/* Exact mode on the device (additive: the reference refines exact-mode
+ * vertices on the host, extract::mesh_brick, mesh/extract.rs:146-219 with
+ * vertex :425-535 and attributes :553-597).  Uploads the tables the vertex
+ * attributes read: the input index of each sphere (orig, n_spheres), the
+ * atom pair of each circle (2 per circle) and the atom triple of each SAS
+ * vertex (3 per vertex), in the resident arrangement's order, and the edge
+ * clamp t_min (extract.rs:47-51). */
+int smb_resident_set_exact(smb_resident* res, const uint32_t* orig, const uint32_t* circle_ij, size_t n_circles,
+                           const uint32_t* vertex_atoms, size_t n_vertices, double t_min, char* err, size_t errlen);
+/* Refines the crossing edges of the last run in f64 on the device: for each
+ * sampled sub-block the candidates of its ball (SesField::gather_local,
+ * field/point.rs:496-582), then extract::vertex's Newton / Illinois /
+ * bisection search and the vertex attributes, operation by operation as the
+ * CPU does them, so every vertex equals the CPU's.  Edges left to the host
+ * (evals = 0 in smb_batch_vertices): those whose last evaluation is solvent
+ * or beyond the band, and those of a sub-block whose lists exceed a block's
+ * shared memory.  *ms gets the device time. */
+int smb_refine_exact(smb_resident* res, smb_batch* batch, double* ms, char* err, size_t errlen);
+/* Results of smb_refine_exact per marching-cubes edge: position and normal
+ * (3 f32 each), input atom index, patch (0 sphere, 1 circle, 2 vertex),
+ * root parameter before the clamp, evaluations (0: not refined on the
+ * device).  Null pointers are skipped. */
+int smb_batch_vertices(const smb_batch* batch, float* positions, float* normals, uint32_t* atoms, uint8_t* patches,
+                       float* t, uint32_t* evals);
+/* Shared memory per warp for one sub-block's f64 lists in smb_refine_exact
+ * (1 KiB..48 KiB; default 18 KiB); larger sub-blocks take a whole block. */
+int smb_batch_set_exact_region(smb_batch* batch, size_t bytes);
+
 /* Sizes and times of the last run of a batch (diagnostics; BatchTimes and
  * DeviceBatch::bytes, batch.rs:118-129, 233). */
 typedef struct {
     size_t bricks, sampled_subblocks, ids_words, max_pack_units, edges, triangles, touched, resident_bytes;
     unsigned long long pack_units;
     double classify_ms;
+    size_t exact_block_items;  /* smb_refine_exact: sub-blocks refined by a whole block (lists over a warp's share) */
 } smb_batch_info;
 int smb_batch_info_get(const smb_batch* batch, smb_batch_info* out);
 /* Re-runs the sampling pass of the last run counting its f32 arithmetic

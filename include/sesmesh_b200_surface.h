@@ -2,10 +2,10 @@
  * sesmesh_b200 — host API of the mesh stage with the B200 back end: the
  * counterpart of compute_surface / SurfaceEngine with Backend::Cuda
  * (crates/sesmesh/src/surface.rs:599-711) for the SES, refine exact or fast.
- * The host keeps what sesmesh keeps on the CPU (arrangement, f64 root
- * refinement in exact mode, assembly, validation, components, OBJ); the
- * device runs classification, gather, sampling, marching cubes and, in fast
- * mode, f32 refinement through include/sesmesh_b200.h.
+ * The host keeps the arrangement, assembly and OBJ output; the device runs
+ * classification, gather, sampling, marching cubes, the vertex refinement
+ * (f64 in exact mode, f32 in fast mode), validation and measure through
+ * include/sesmesh_b200.h.
  */
 #ifndef SESMESH_B200_SURFACE_H
 #define SESMESH_B200_SURFACE_H
@@ -61,6 +61,11 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen);
  * refinement evaluates them), clamped to -band beyond it inside.  For the
  * distance of mesh vertices to the surface. */
 int smb_engine_field(const smb_engine* e, const double* points, size_t n, double* values);
+/* Exact mode: vertex refinement in f64 on the device (smb_refine_exact;
+ * the default, on = 1) or on the host threads (on = 0, as the reference).
+ * Both give the same mesh bytes; edges the device leaves are refined on the
+ * host either way (stats.refine_cpu_edges). */
+int smb_engine_set_exact_device(smb_engine* e, int on);
 /* The engine's device batch (sizes, counters, operation counts). */
 smb_batch* smb_engine_batch(smb_engine* e);
 /* Learned warm start of fast mode (no counterpart in the reference): the

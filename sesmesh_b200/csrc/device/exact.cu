@@ -1,0 +1,581 @@
+// Exact mode's vertex refinement on the device, in f64.  Per sampled
+// sub-block: the candidates of its ball (SesField::gather_local,
+// crates/sesmesh/src/field/point.rs:496-582, with the pruning keys of the
+// host restatement), then per crossing edge whose lower sample lies in the
+// sub-block the root search (extract::vertex, crates/sesmesh/src/mesh/
+// extract.rs:425-535, eval_local point.rs:686-738, gradient extract.rs:
+// 539-549) and the vertex attributes (attributes, extract.rs:553-597).
+//
+// Every f64 expression keeps the CPU's operation order (the library is
+// built without FMA contraction; f64 division and square root are IEEE), so
+// positions, normals, atoms, patches, root parameters and evaluation counts
+// equal host/mesher.cpp refine_edge's bit for bit.  The candidate lists
+// are sets sorted by unique keys (near by index, S by (lb, index), C by
+// (distance, index), V by (distance, index)) and the inside test is an
+// any-of, so collecting them in a different order gives the same lists.
+//
+// Two edges stay with the host, marked evals = 0: an edge whose last
+// evaluation is solvent or beyond the band (its attributes search the
+// whole sphere grid), and the edges of a sub-block whose lists do not fit
+// the shared memory of a whole block.
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.hpp"
+
+namespace smb {
+
+namespace {
+
+constexpr double X_EPS = 1e-9;    // blocker tolerance (point.rs:422-476)
+constexpr double X_TOL = 1e-5;    // extract.rs:35
+constexpr int X_MAX_ITER = 8;     // extract.rs:29
+constexpr int X_MAX_BISECT = 64;  // extract.rs:33
+constexpr double X_PRUNE = 1e-9;  // margin of the candidates' pruning keys
+constexpr uint32_t XF_SOLVENT = 0, XF_BEYOND = 1, XF_SPHERE = 2, XF_CIRCLE = 3, XF_VERTEX = 4;
+constexpr int X_WARPS = 4;
+
+// List sizes of one ball.
+struct XCounts {
+    uint32_t nn, ni, ns, nc, nv;
+};
+
+// One ball's lists in shared memory.  near: ascending sphere index, with
+// (centre, R); blockers are positions in it.  t_key / t_id: unsorted
+// scratch of the list being built; the blocker lists take its place once
+// the lists are sorted.
+struct XView {
+    uint32_t* near_id;
+    double4* near_c;
+    double4* in_c;
+    double4* s_c;
+    double* s_key;
+    uint32_t *s_id, *s_off, *s_blk;
+    double4 *c_m, *c_u;  // (centre, radius), (axis, e1.x)
+    double* c_key;
+    uint32_t *c_id, *c_off, *c_blk;
+    double4* v_p;
+    double* v_key;
+    uint32_t* v_id;
+    double* t_key;
+    uint32_t* t_id;
+    uint32_t nn, ni, ns, nc, nv;
+};
+
+__device__ __forceinline__ size_t xal(size_t v) { return (v + 15) & ~size_t(15); }
+
+// Lays one ball's lists out from `base`; *tail gets the offset where the
+// scratch (and later the blocker lists) start.  Returns the bytes the lists
+// and the scratch take.
+__device__ __forceinline__ size_t x_layout(const XCounts& c, unsigned char* base, XView& v, size_t* tail) {
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base + o;
+        o = xal(o + bytes);
+        return p;
+    };
+    v.near_c = reinterpret_cast<double4*>(take(size_t(c.nn) * 32));
+    v.in_c = reinterpret_cast<double4*>(take(size_t(c.ni) * 32));
+    v.s_c = reinterpret_cast<double4*>(take(size_t(c.ns) * 32));
+    v.c_m = reinterpret_cast<double4*>(take(size_t(c.nc) * 32));
+    v.c_u = reinterpret_cast<double4*>(take(size_t(c.nc) * 32));
+    v.v_p = reinterpret_cast<double4*>(take(size_t(c.nv) * 32));
+    v.s_key = reinterpret_cast<double*>(take(size_t(c.ns) * 8));
+    v.c_key = reinterpret_cast<double*>(take(size_t(c.nc) * 8));
+    v.v_key = reinterpret_cast<double*>(take(size_t(c.nv) * 8));
+    v.near_id = reinterpret_cast<uint32_t*>(take(size_t(c.nn) * 4));
+    v.s_id = reinterpret_cast<uint32_t*>(take(size_t(c.ns) * 4));
+    v.s_off = reinterpret_cast<uint32_t*>(take(size_t(c.ns + 1) * 4));
+    v.c_id = reinterpret_cast<uint32_t*>(take(size_t(c.nc) * 4));
+    v.c_off = reinterpret_cast<uint32_t*>(take(size_t(c.nc + 1) * 4));
+    v.v_id = reinterpret_cast<uint32_t*>(take(size_t(c.nv) * 4));
+    *tail = o;
+    const uint32_t tk = max(c.ns, max(c.nc, c.nv)), ti = max(c.nn + c.ns, max(c.nc, c.nv));
+    v.t_key = reinterpret_cast<double*>(take(size_t(tk) * 8));
+    v.t_id = reinterpret_cast<uint32_t*>(take(size_t(ti) * 4));
+    v.nn = c.nn, v.ni = c.ni, v.ns = c.ns, v.nc = c.nc, v.nv = c.nv;
+    return o;
+}
+
+template <bool WIDE>
+__device__ __forceinline__ void x_sync() {
+    if (WIDE) __syncthreads();
+    else __syncwarp();
+}
+
+// Threads tid, tid + T, ... visit the items of the cells overlapping the
+// cube of half-size r around (x, y, z) (geom/cells.rs:113-130).
+template <class F>
+__device__ __forceinline__ void x_for_near(const DGrid& g, double x, double y, double z, double r, uint32_t tid,
+                                           uint32_t T, F&& f) {
+    CellBox bx = cell_box(g, x, y, z, r);
+    for (uint32_t zc = bx.z0; zc <= bx.z1; zc++)
+        for (uint32_t yc = bx.y0; yc <= bx.y1; yc++) {
+            size_t row = (size_t(zc) * g.dy + yc) * g.dx;
+            uint32_t a = g.starts[row + bx.x0], e = g.starts[row + bx.x1 + 1];
+            for (uint32_t i = a + tid; i < e; i += T) f(g.items[i]);
+        }
+}
+
+// Position of id in the ascending near list, or -1.
+__device__ __forceinline__ int x_find(const uint32_t* ids, uint32_t n, uint32_t id) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (ids[mid] < id) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < n && ids[lo] == id) ? int(lo) : -1;
+}
+
+// Blocker rows of the n sorted candidates kept to near spheres: counts
+// into off[1..n] ...
+__device__ __forceinline__ void x_blocker_counts(const XView& v, const uint32_t* ids, uint32_t n,
+                                                 const uint32_t* row_off, const uint32_t* row_items, uint32_t* off,
+                                                 uint32_t tid, uint32_t T) {
+    for (uint32_t i = tid; i < n; i += T) {
+        const uint32_t k = ids[i];
+        uint32_t c = 0;
+        for (uint32_t p = row_off[k], e = row_off[k + 1]; p < e; p++) c += x_find(v.near_id, v.nn, row_items[p]) >= 0;
+        off[i + 1] = c;
+    }
+}
+
+// ... then, with off scanned, the near-list positions into blk.
+__device__ __forceinline__ void x_blocker_fill(const XView& v, const uint32_t* ids, uint32_t n,
+                                               const uint32_t* row_off, const uint32_t* row_items,
+                                               const uint32_t* off, uint32_t* blk, uint32_t tid, uint32_t T) {
+    for (uint32_t i = tid; i < n; i += T) {
+        const uint32_t k = ids[i];
+        uint32_t at = off[i];
+        for (uint32_t p = row_off[k], e = row_off[k + 1]; p < e; p++) {
+            int pos = x_find(v.near_id, v.nn, row_items[p]);
+            if (pos >= 0) blk[at++] = uint32_t(pos);
+        }
+    }
+}
+
+// Rank of (key, id) among n scratch pairs in (key, id) order.
+__device__ __forceinline__ uint32_t x_rank(const double* keys, const uint32_t* ids, uint32_t n, double key,
+                                           uint32_t id) {
+    uint32_t r = 0;
+    for (uint32_t q = 0; q < n; q++) {
+        const double kq = keys[q];
+        r += (kq < key || (kq == key && ids[q] < id)) ? 1u : 0u;
+    }
+    return r;
+}
+
+// gather_local of sub-block j's ball into `base` (cap bytes) with threads
+// tid of T; false when the lists do not fit.  cnt: 8 shared counters.
+template <bool WIDE>
+__device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsigned char* base, size_t cap,
+                       uint32_t* cnt, uint32_t tid, uint32_t T, XView& v) {
+    const int b = L.b, sub = L.sub, sb = int(j & 7);
+    const double h = L.h, subd = double(sub);
+    // local_of (extract.rs:165-177, 195-206): ball centre and radius.
+    const double bx = double((long long)key.x * b) * h, by = double((long long)key.y * b) * h,
+                 bz = double((long long)key.z * b) * h;
+    const double cx = bx + (double((sb & 1) * sub) + 0.5 * subd) * h;
+    const double cy = by + (double(((sb >> 1) & 1) * sub) + 0.5 * subd) * h;
+    const double cz = bz + (double((sb >> 2) * sub) + 0.5 * subd) * h;
+    const double rho = 0.5 * sqrt(3.0) * subd * h * (1.0 + 1e-9) + 1e-9;
+    const double reach = A.probe + L.band + rho;
+    x_sync<WIDE>();
+    if (tid < 8) cnt[tid] = 0;
+    x_sync<WIDE>();
+    // Sizes.
+    x_for_near(A.gs, cx, cy, cz, reach + A.max_expanded, tid, T, [&](uint32_t k) {
+        const uint32_t st = A.status[k];
+        if (st == STATUS_CONTAINED) return;
+        const double4 c = A.sph[k];
+        const double d = dist3(cx, cy, cz, c.x, c.y, c.z);
+        if (d < c.w + reach) atomicAdd(&cnt[0], 1u);
+        if (d < c.w + rho) atomicAdd(&cnt[1], 1u);
+        if (st == STATUS_EXPOSED && fabs(d - c.w) <= reach) atomicAdd(&cnt[2], 1u);
+    });
+    x_for_near(A.gc, cx, cy, cz, reach + A.rho_max, tid, T, [&](uint32_t ci) {
+        if (circle_reach_dist(A, cx, cy, cz, ci) <= reach) atomicAdd(&cnt[3], 1u);
+    });
+    x_for_near(A.gv, cx, cy, cz, reach, tid, T, [&](uint32_t vi) {
+        const double4 p = A.vert[vi];
+        if (dist3(cx, cy, cz, p.x, p.y, p.z) <= reach) atomicAdd(&cnt[4], 1u);
+    });
+    x_sync<WIDE>();
+    const XCounts c{cnt[0], cnt[1], cnt[2], cnt[3], cnt[4]};
+    size_t tail = 0;
+    const size_t need = x_layout(c, base, v, &tail);
+    x_sync<WIDE>();
+    if (need > cap) return false;
+    if (tid < 8) cnt[tid] = 0;
+    x_sync<WIDE>();
+    // Spheres: near (scratch ids), inside (direct), S (scratch pairs).
+    x_for_near(A.gs, cx, cy, cz, reach + A.max_expanded, tid, T, [&](uint32_t k) {
+        const uint32_t st = A.status[k];
+        if (st == STATUS_CONTAINED) return;
+        const double4 s = A.sph[k];
+        const double d = dist3(cx, cy, cz, s.x, s.y, s.z);
+        if (d < s.w + reach) v.t_id[atomicAdd(&cnt[0], 1u)] = k;
+        if (d < s.w + rho) v.in_c[atomicAdd(&cnt[1], 1u)] = s;
+        const double lb = fabs(d - s.w);
+        if (st == STATUS_EXPOSED && lb <= reach) {
+            const uint32_t p = atomicAdd(&cnt[2], 1u);
+            v.t_key[p] = lb;
+            v.t_id[c.nn + p] = k;
+        }
+    });
+    x_sync<WIDE>();
+    for (uint32_t i = tid; i < c.nn; i += T) {
+        const uint32_t id = v.t_id[i];
+        uint32_t r = 0;
+        for (uint32_t q = 0; q < c.nn; q++) r += v.t_id[q] < id ? 1u : 0u;
+        v.near_id[r] = id;
+        v.near_c[r] = A.sph[id];
+    }
+    for (uint32_t i = tid; i < c.ns; i += T) {
+        const double lb = v.t_key[i];
+        const uint32_t k = v.t_id[c.nn + i];
+        const uint32_t r = x_rank(v.t_key, v.t_id + c.nn, c.ns, lb, k);
+        v.s_id[r] = k;
+        v.s_key[r] = lb - rho - X_PRUNE;
+        v.s_c[r] = A.sph[k];
+    }
+    // Circles.
+    x_sync<WIDE>();
+    x_for_near(A.gc, cx, cy, cz, reach + A.rho_max, tid, T, [&](uint32_t ci) {
+        const double d = circle_reach_dist(A, cx, cy, cz, ci);
+        if (d <= reach) {
+            const uint32_t p = atomicAdd(&cnt[3], 1u);
+            v.t_key[p] = d;
+            v.t_id[p] = ci;
+        }
+    });
+    x_sync<WIDE>();
+    for (uint32_t i = tid; i < c.nc; i += T) {
+        const double d = v.t_key[i];
+        const uint32_t ci = v.t_id[i];
+        const uint32_t r = x_rank(v.t_key, v.t_id, c.nc, d, ci);
+        const double* C = A.circ + 12 * size_t(ci);
+        v.c_id[r] = ci;
+        v.c_key[r] = d - rho - X_PRUNE;
+        v.c_m[r] = make_double4(C[0], C[1], C[2], C[9]);
+        v.c_u[r] = make_double4(C[3], C[4], C[5], C[6]);
+    }
+    x_sync<WIDE>();
+    // SAS vertices.
+    x_for_near(A.gv, cx, cy, cz, reach, tid, T, [&](uint32_t vi) {
+        const double4 p = A.vert[vi];
+        const double d = dist3(cx, cy, cz, p.x, p.y, p.z);
+        if (d <= reach) {
+            const uint32_t q = atomicAdd(&cnt[4], 1u);
+            v.t_key[q] = d;
+            v.t_id[q] = vi;
+        }
+    });
+    x_sync<WIDE>();
+    for (uint32_t i = tid; i < c.nv; i += T) {
+        const double d = v.t_key[i];
+        const uint32_t vi = v.t_id[i];
+        const uint32_t r = x_rank(v.t_key, v.t_id, c.nv, d, vi);
+        v.v_id[r] = vi;
+        v.v_key[r] = d - rho - X_PRUNE;
+        v.v_p[r] = A.vert[vi];
+    }
+    // Blockers, kept to near spheres, in the scratch's place.
+    x_blocker_counts(v, v.s_id, c.ns, A.nb_off, A.nb_items, v.s_off, tid, T);
+    x_blocker_counts(v, v.c_id, c.nc, A.cb_off, A.cb_items, v.c_off, tid, T);
+    x_sync<WIDE>();
+    if (tid == 0) {
+        v.s_off[0] = 0;
+        for (uint32_t i = 1; i <= c.ns; i++) v.s_off[i] += v.s_off[i - 1];
+    }
+    if (tid == T - 1) {
+        v.c_off[0] = 0;
+        for (uint32_t i = 1; i <= c.nc; i++) v.c_off[i] += v.c_off[i - 1];
+    }
+    x_sync<WIDE>();
+    const size_t nsb = v.s_off[c.ns], ncb = v.c_off[c.nc];
+    v.s_blk = reinterpret_cast<uint32_t*>(base + tail);
+    v.c_blk = reinterpret_cast<uint32_t*>(base + xal(tail + nsb * 4));
+    if (xal(tail + nsb * 4) + ncb * 4 > cap) return false;
+    x_blocker_fill(v, v.s_id, c.ns, A.nb_off, A.nb_items, v.s_off, v.s_blk, tid, T);
+    x_blocker_fill(v, v.c_id, c.nc, A.cb_off, A.cb_items, v.c_off, v.c_blk, tid, T);
+    x_sync<WIDE>();
+    return true;
+}
+
+struct XEval {
+    double value, qx, qy, qz;
+    uint32_t kind, id;
+};
+
+// eval_local (point.rs:686-738) against the ball's lists: value, feature and
+// closest point.
+__device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, double probe, double band, double x, double y, double z) {
+    XEval e;
+    e.qx = x, e.qy = y, e.qz = z, e.id = 0;
+    bool inside = false;
+    for (uint32_t k = 0; k < v.ni; k++) {
+        const double4 c = v.in_c[k];
+        if (dist3(x, y, z, c.x, c.y, c.z) < c.w) {
+            inside = true;
+            break;
+        }
+    }
+    if (!inside) {
+        e.value = probe, e.kind = XF_SOLVENT;
+        return e;
+    }
+    double best = probe + band;
+    e.kind = XF_BEYOND;
+    for (uint32_t i = 0; i < v.ns && v.s_key[i] < best; i++) {
+        const double4 c = v.s_c[i];
+        const double vx = x - c.x, vy = y - c.y, vz = z - c.z;
+        const double len = sqrt(vx * vx + vy * vy + vz * vz);
+        const double lb = fabs(len - c.w);
+        if (lb >= best || len < 1e-12) continue;
+        const double s = c.w / len;
+        const double qx = c.x + vx * s, qy = c.y + vy * s, qz = c.z + vz * s;
+        bool free = true;
+        for (uint32_t p = v.s_off[i], pe = v.s_off[i + 1]; p < pe; p++) {
+            const double4 k = v.near_c[v.s_blk[p]];
+            if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - X_EPS)) {
+                free = false;
+                break;
+            }
+        }
+        if (free) best = lb, e.kind = XF_SPHERE, e.id = v.s_id[i], e.qx = qx, e.qy = qy, e.qz = qz;
+    }
+    for (uint32_t i = 0; i < v.nc && v.c_key[i] < best; i++) {
+        const double4 m = v.c_m[i], u = v.c_u[i];
+        const double yx = x - m.x, yy = y - m.y, yz = z - m.z;
+        const double along = yx * u.x + yy * u.y + yz * u.z;
+        const double wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
+        const double wl = sqrt(wx * wx + wy * wy + wz * wz);
+        const double dist = sqrt(along * along + (wl - m.w) * (wl - m.w));
+        if (dist >= best) continue;
+        double dx, dy, dz;
+        if (wl > 1e-12) {
+            dx = wx / wl, dy = wy / wl, dz = wz / wl;
+        } else {  // on the axis: e1 (A.circ words 6..8)
+            const double* C = circ + 12 * size_t(v.c_id[i]);
+            dx = u.w, dy = C[7], dz = C[8];
+        }
+        const double qx = m.x + dx * m.w, qy = m.y + dy * m.w, qz = m.z + dz * m.w;
+        bool free = true;
+        for (uint32_t p = v.c_off[i], pe = v.c_off[i + 1]; p < pe; p++) {
+            const double4 k = v.near_c[v.c_blk[p]];
+            if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - X_EPS)) {
+                free = false;
+                break;
+            }
+        }
+        if (free) best = dist, e.kind = XF_CIRCLE, e.id = v.c_id[i], e.qx = qx, e.qy = qy, e.qz = qz;
+    }
+    for (uint32_t i = 0; i < v.nv && v.v_key[i] < best; i++) {
+        const double4 p = v.v_p[i];
+        const double d = dist3(x, y, z, p.x, p.y, p.z);
+        if (d < best) best = d, e.kind = XF_VERTEX, e.id = v.v_id[i], e.qx = p.x, e.qy = p.y, e.qz = p.z;
+    }
+    e.value = probe - best;
+    return e;
+}
+
+__device__ __forceinline__ double x_clamp(double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// The atom nearest to p among ids (extract.rs:566-576): its input index.
+__device__ __forceinline__ uint32_t x_nearest(const DArr& A, const ExactAttr& X, const uint32_t* ids, int n, double px,
+                                              double py, double pz) {
+    double best = __longlong_as_double(0x7ff0000000000000LL);
+    uint32_t bi = ids[0];
+    for (int q = 0; q < n; q++) {
+        const double4 c = A.sph[ids[q]];
+        const double d = dist3(px, py, pz, c.x, c.y, c.z) - A.rvdw[ids[q]];
+        if (d < best) best = d, bi = ids[q];
+    }
+    return X.orig[bi];
+}
+
+// extract::vertex of edge k (exact mode) and its attributes; leaves evals[k]
+// = 0 when the last evaluation is solvent or beyond.
+__device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat& L, const ExactAttr& X, int4 key, uint32_t k,
+                       uint32_t code, float2 fv, const ExactOut& out) {
+    const int b = L.b;
+    const double h = L.h;
+    const uint32_t cell = code / 3, axis = code % 3;
+    const long long ix = (long long)key.x * b + (long long)(cell % uint32_t(b)),
+                    iy = (long long)key.y * b + (long long)((cell / uint32_t(b)) % uint32_t(b)),
+                    iz = (long long)key.z * b + (long long)(cell / uint32_t(b * b));
+    const double pax = double(ix) * h, pay = double(iy) * h, paz = double(iz) * h;
+    const double pbx = double(ix + (axis == 0)) * h, pby = double(iy + (axis == 1)) * h,
+                 pbz = double(iz + (axis == 2)) * h;
+    const double fa = double(fv.x), fb = double(fv.y);
+    const double dx = pbx - pax, dy = pby - pay, dz = pbz - paz;
+    const double probe = A.probe, band = L.band;
+    double t = x_clamp(fa / (fa - fb), 0.0, 1.0);
+    XEval last;
+    double t0 = 0.0, g0 = fa, t1 = 1.0, g1 = fb;
+    int side = 0;
+    bool converged = false;
+    uint32_t evals = 0;
+    for (int it = 0; it < X_MAX_ITER; it++) {
+        const double x = pax + dx * t, y = pay + dy * t, z = paz + dz * t;
+        const XEval e = x_eval(v, A.circ, probe, band, x, y, z);
+        evals++;
+        last = e;
+        const double g = e.value;
+        if (fabs(g) <= X_TOL) {
+            converged = true;
+            break;
+        }
+        if ((g < 0.0) == (g0 < 0.0)) {
+            t0 = t, g0 = g;
+            if (side == -1) g1 *= 0.5;
+            side = -1;
+        } else {
+            t1 = t, g1 = g;
+            if (side == 1) g0 *= 0.5;
+            side = 1;
+        }
+        double slope = 0.0;
+        if (e.kind != XF_SOLVENT && e.kind != XF_BEYOND) {
+            const double wx = e.qx - x, wy = e.qy - y, wz = e.qz - z;
+            const double len = sqrt(wx * wx + wy * wy + wz * wz);
+            if (len > 1e-12) slope = (wx / len) * dx + (wy / len) * dy + (wz / len) * dz;
+        }
+        const double newton = t - g / slope;
+        if (fabs(slope) > 1e-3 * sqrt(dx * dx + dy * dy + dz * dz) && newton > t0 && newton < t1) {
+            t = newton;
+        } else {
+            const double s = (t0 * g1 - t1 * g0) / (g1 - g0);
+            t = (isfinite(s) && s > t0 && s < t1) ? s : 0.5 * (t0 + t1);
+        }
+    }
+    if (!converged) {
+        const double len = sqrt(dx * dx + dy * dy + dz * dz);
+        const bool neg0 = g0 < 0.0;
+        for (int it = 0; it < X_MAX_BISECT; it++) {
+            t = 0.5 * (t0 + t1);
+            const XEval e = x_eval(v, A.circ, probe, band, pax + dx * t, pay + dy * t, paz + dz * t);
+            evals++;
+            last = e;
+            if (fabs(e.value) <= X_TOL || (t1 - t0) * len <= 2.0 * X_TOL) break;
+            if ((e.value < 0.0) == neg0) t0 = t;
+            else t1 = t;
+        }
+    }
+    if (last.kind == XF_SOLVENT || last.kind == XF_BEYOND) return;
+    const double ct = x_clamp(t, X.t_min, 1.0 - X.t_min);
+    const double px = pax + dx * ct, py = pay + dy * ct, pz = paz + dz * ct;
+    double nx = last.qx - px, ny = last.qy - py, nz = last.qz - pz;
+    const double nl = sqrt(nx * nx + ny * ny + nz * nz);
+    if (nl > 1e-9) {
+        nx = nx / nl, ny = ny / nl, nz = nz / nl;
+    } else {
+        double ox = dx, oy = dy, oz = dz;
+        if (!(fa < 0.0)) ox = dx * -1.0, oy = dy * -1.0, oz = dz * -1.0;
+        const double on = sqrt(ox * ox + oy * oy + oz * oz);
+        nx = ox / on, ny = oy / on, nz = oz / on;
+    }
+    uint32_t atom, patch;
+    if (last.kind == XF_SPHERE) atom = X.orig[last.id], patch = 0;
+    else if (last.kind == XF_CIRCLE) atom = x_nearest(A, X, X.circle_ij + 2 * size_t(last.id), 2, px, py, pz), patch = 1;
+    else atom = x_nearest(A, X, X.vertex_atoms + 3 * size_t(last.id), 3, px, py, pz), patch = 2;
+    out.pos[3 * size_t(k)] = float(px), out.pos[3 * size_t(k) + 1] = float(py), out.pos[3 * size_t(k) + 2] = float(pz);
+    out.nrm[3 * size_t(k)] = float(nx), out.nrm[3 * size_t(k) + 1] = float(ny), out.nrm[3 * size_t(k) + 2] = float(nz);
+    out.atom[k] = atom;
+    out.patch[k] = uint8_t(patch);
+    out.t[k] = float(t);
+    out.evals[k] = evals;
+}
+
+// Persistent CTAs of X_WARPS warps.  Narrow (WIDE = false): each warp claims
+// work items from counters[CNT_QUEUE], builds the item's ball in its own
+// region of `region` bytes and refines the item's edges lane per edge; an
+// item whose lists do not fit goes to ovf (ovf[0] = count).  WIDE: each CTA
+// claims the overflowed items from counters[CNT_XQUEUE] and works on one at
+// a time with all its threads and all its dynamic shared memory.
+template <bool WIDE>
+__global__ void __launch_bounds__(32 * X_WARPS, 1) k_refine_exact(DArr A, DLat L, ExactAttr X, const int4* keys,
+                                                               const uint32_t* work, const uint32_t* edges,
+                                                               const float2* edge_vals, const uint32_t* item_off,
+                                                               const uint32_t* item_edges, uint32_t n_items,
+                                                               ExactOut out, size_t region, uint32_t* ovf,
+                                                               unsigned long long* counters) {
+    extern __shared__ __align__(16) unsigned char xs[];
+    __shared__ uint32_t sh_cnt[X_WARPS][8];
+    __shared__ uint32_t sh_item;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t tid = WIDE ? threadIdx.x : lane, T = WIDE ? blockDim.x : 32u;
+    unsigned char* mine = xs + (WIDE ? size_t(0) : size_t(warp) * region);
+    uint32_t* cnt = sh_cnt[WIDE ? 0 : warp];
+    unsigned int* queue = reinterpret_cast<unsigned int*>(&counters[WIDE ? CNT_XQUEUE : CNT_QUEUE]);
+    const uint32_t n_ovf = WIDE ? ovf[0] : 0u;
+    for (;;) {
+        uint32_t i;
+        if constexpr (WIDE) {
+            __syncthreads();
+            if (threadIdx.x == 0) sh_item = atomicAdd(queue, 1u);
+            __syncthreads();
+            if (sh_item >= n_ovf) break;
+            i = ovf[1 + sh_item];
+        } else {
+            i = 0;
+            if (lane == 0) i = atomicAdd(queue, 1u);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= n_items) break;
+        }
+        const uint32_t a0 = item_off[i], a1 = item_off[i + 1];
+        if (a0 == a1) continue;
+        const uint32_t j = work[i];
+        const int4 key = keys[j >> 3];
+        XView v;
+        if (!x_ball<WIDE>(A, L, key, j, mine, region, cnt, tid, T, v)) {
+            if (!WIDE && lane == 0) ovf[1 + atomicAdd(&ovf[0], 1u)] = i;
+            continue;
+        }
+        for (uint32_t e = a0 + tid; e < a1; e += T) {
+            const uint32_t k = item_edges[e];
+            x_edge(v, A, L, X, key, k, edges[k], edge_vals[k], out);
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
+                                const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
+                                const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
+                                const ExactOut& out, uint32_t* ovf, unsigned long long* counters, int sms,
+                                size_t smem_limit, size_t region, cudaStream_t s) {
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(&counters[CNT_QUEUE], 0, 8, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(&counters[CNT_XQUEUE], 0, 8, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(ovf, 0, 4, s)) != cudaSuccess) return e;
+    if (!n_items) return cudaSuccess;
+    region = (region + 15) & ~size_t(15);
+    const size_t narrow = size_t(X_WARPS) * region;
+    auto kn = k_refine_exact<false>;
+    auto kw = k_refine_exact<true>;
+    if ((e = cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(narrow))) != cudaSuccess)
+        return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kn, 32 * X_WARPS, narrow)) != cudaSuccess)
+        return e;
+    const uint32_t warps = (n_items + X_WARPS - 1) / X_WARPS;
+    const uint32_t grid = std::min<uint32_t>(warps, uint32_t(sms * std::max(per_sm, 1)));
+    count_launches(2);
+    kn<<<grid, 32 * X_WARPS, narrow, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
+                                          region, ovf, counters);
+    // The overflowed items: one CTA per SM, all of the CTA's shared memory.
+    cudaFuncAttributes fa{};
+    if ((e = cudaFuncGetAttributes(&fa, kw)) != cudaSuccess) return e;
+    const size_t wide = (smem_limit > fa.sharedSizeBytes ? smem_limit - fa.sharedSizeBytes : 0) & ~size_t(15);
+    if ((e = cudaFuncSetAttribute(kw, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wide))) != cudaSuccess)
+        return e;
+    kw<<<uint32_t(std::max(sms, 1)), 32 * X_WARPS, wide, s>>>(A, L, X, keys, work, edges, edge_vals, item_off,
+                                                              item_edges, n_items, out, wide, ovf, counters);
+    return cudaGetLastError();
+}
+
+}  // namespace smb

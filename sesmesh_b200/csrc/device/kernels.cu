@@ -1546,6 +1546,7 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
 // Host launchers.  Each counts the kernels it launches.
 static std::atomic<unsigned long long> g_launches{0};
 unsigned long long kernel_launches() { return g_launches.load(); }
+void count_launches(unsigned long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 #define COUNT(n) g_launches.fetch_add(n, std::memory_order_relaxed)
 
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s) {

@@ -29,7 +29,7 @@ __host__ __device__ inline size_t gather_smem_bytes(const GatherCaps& c) {
 // Device counters of one gather/sample pass.
 enum : int {
     CNT_IDS = 0, CNT_PACK = 1, CNT_MAXPACK = 2, CNT_OVERFLOW = 3, CNT_NOMEM = 4, CNT_TIMEOUT = 5, CNT_OPS = 6,
-    CNT_OWNED = 7, CNT_MAXNN = 8, CNT_MAXNS = 9, CNT_MAXNC = 10, CNT_MAXNV = 11, CNT_MAXITEM = 12, CNT_QUEUE = 13, CNT_RETRY = 14, CNT_N = 16
+    CNT_OWNED = 7, CNT_MAXNN = 8, CNT_MAXNS = 9, CNT_MAXNC = 10, CNT_MAXNV = 11, CNT_MAXITEM = 12, CNT_QUEUE = 13, CNT_RETRY = 14, CNT_XQUEUE = 15, CNT_N = 16
 };
 constexpr uint32_t REC_NOMEM = 2;
 
@@ -90,6 +90,36 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
                           size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many = nullptr);
 
 unsigned long long kernel_launches();
+void count_launches(unsigned long long n);
+
+// Exact mode on the device (exact.cu): the vertex attribute tables (input
+// index per sphere, atom pair per circle, atom triple per SAS vertex) and
+// the edge clamp t_min (extract.rs:47-51).
+struct ExactAttr {
+    const uint32_t* orig;
+    const uint32_t* circle_ij;
+    const uint32_t* vertex_atoms;
+    double t_min;
+};
+// Per edge: position and normal (3 f32 each), input atom, patch, root
+// parameter before the clamp, evaluations (0: left to the host).
+struct ExactOut {
+    float* pos;
+    float* nrm;
+    uint32_t* atom;
+    uint8_t* patch;
+    float* t;
+    uint32_t* evals;
+};
+// f64 refinement of the work items' edge lists (k_item_edges): a warp per
+// item with `region` bytes of shared memory for the item's candidate lists,
+// then the items that did not fit (ovf: count then items, n_items + 1
+// words) with a CTA each.
+cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
+                                const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
+                                const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
+                                const ExactOut& out, uint32_t* ovf, unsigned long long* counters, int sms,
+                                size_t smem_limit, size_t region, cudaStream_t s);
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);
 void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, unsigned long long* tiles,
                  unsigned long long* total, cudaStream_t s);

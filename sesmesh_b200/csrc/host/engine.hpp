@@ -33,6 +33,9 @@ struct smb_engine {
     smb_batch_times times{};
     double t_classify = 0;
     const smb_mlp* warm = nullptr;  // warm start of fast-mode refinement
+    bool exact_device = true;       // exact mode: f64 refinement on the device (else on the host threads)
+    smbh::MeshOut exact_out;        // its vertices, at their edge index
+    std::vector<uint32_t> exact_evals;
     smb::MeasureScratch measure;    // device buffers of the validation and measure
     // Warm-start training rows of the last device run.
     bool rows_ready = false;
@@ -52,8 +55,11 @@ struct smb_surface {
 // validation, components and grouping; fills the statistics it can (sizes,
 // area, volume, evaluations, host stage times).  With a device, the
 // validation and measure run there (same results), else on the host
-// threads.  Error text or "".
+// threads.  Exact mode with the device's f64 vertices: `exact` holds them
+// (consumed) and exact_evals their evaluation counts (0: refined here).
+// Error text or "".
 std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fast, const int32_t* keys, size_t nb,
                            const uint32_t* edge_off, const uint32_t* edges, const float* edge_vals,
                            const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s,
-                           smb_device* device = nullptr, smb::MeasureScratch* scratch = nullptr);
+                           smb_device* device = nullptr, smb::MeasureScratch* scratch = nullptr,
+                           smbh::MeshOut* exact = nullptr, const uint32_t* exact_evals = nullptr);

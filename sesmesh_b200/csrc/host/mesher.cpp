@@ -380,6 +380,31 @@ void place_fast(const Arrangement& A, const MeshParams& P, const int32_t* keys, 
     });
 }
 
+void place_exact(const Arrangement& A, const MeshParams& P, const int32_t* keys, size_t n, const uint32_t* edge_off,
+                 const uint32_t* edges, const float* vals, const uint32_t* dev_evals, MeshOut& out) {
+    resize(out, edge_off[n], n);
+    const size_t chunk = 64;
+    parallel_for((n + chunk - 1) / chunk, [&](size_t c, int) {
+        Local locals[8];
+        for (size_t i = c * chunk; i < std::min(n, (c + 1) * chunk); i++) {
+            bool have[8] = {false};
+            uint32_t evals = 0, cpu = 0;
+            for (uint32_t k = edge_off[i]; k < edge_off[i + 1]; k++) {
+                if (dev_evals[k]) {
+                    evals += dev_evals[k];
+                    continue;
+                }
+                EdgeGeom g = edge_geom(P, keys + 3 * i, edges[k]);
+                if (!have[g.sb]) local_of(A, P, keys + 3 * i, g.sb, locals[g.sb]), have[g.sb] = true;
+                put(out, k, refine_edge(A, P, g.pa, g.pb, double(vals[2 * k]), double(vals[2 * k + 1]), locals[g.sb], evals));
+                cpu++;
+            }
+            out.evals[i] = evals;
+            out.cpu_refined[i] = cpu;
+        }
+    });
+}
+
 static uint64_t pack_key(int32_t x, int32_t y, int32_t z) {  // lattice.rs:93-96
     const int64_t bias = int64_t(1) << 20;
     return uint64_t(int64_t(x) + bias) | (uint64_t(int64_t(y) + bias) << 21) | (uint64_t(int64_t(z) + bias) << 42);

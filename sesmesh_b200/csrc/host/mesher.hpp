@@ -77,6 +77,13 @@ struct DeviceRefine {
 void place_fast(const Arrangement& A, const MeshParams& P, const int32_t* keys, size_t n, const uint32_t* edge_off,
                 const uint32_t* edges, const float* edge_vals, const DeviceRefine& dev, MeshOut& out);
 
+// Exact mode with the device's f64 vertices (smb_refine_exact): out holds
+// them at their edge index (positions, normals, atoms, patches, t); edges
+// with dev_evals[k] = 0 are refined here as in refine_exact.  Per-brick
+// evaluations and host-refined edge counts are filled.
+void place_exact(const Arrangement& A, const MeshParams& P, const int32_t* keys, size_t n, const uint32_t* edge_off,
+                 const uint32_t* edges, const float* edge_vals, const uint32_t* dev_evals, MeshOut& out);
+
 struct Mesh {
     std::vector<std::array<float, 3>> positions, normals;
     std::vector<std::array<uint32_t, 3>> triangles;

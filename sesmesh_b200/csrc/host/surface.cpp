@@ -40,11 +40,19 @@ void set_err(char* err, size_t len, const char* fmt, ...) {
 std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fast, const int32_t* keys, size_t nb,
                            const uint32_t* edge_off, const uint32_t* edges, const float* edge_vals,
                            const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s,
-                           smb_device* device, smb::MeasureScratch* scratch) {
+                           smb_device* device, smb::MeasureScratch* scratch, MeshOut* exact,
+                           const uint32_t* exact_evals) {
     auto t1 = clk::now();
     MeshOut mo;
-    if (fast) place_fast(arr, mp, keys, nb, edge_off, edges, edge_vals, dev, mo);
-    else refine_exact(arr, mp, keys, nb, edge_off, edges, edge_vals, mo);
+    if (fast) {
+        place_fast(arr, mp, keys, nb, edge_off, edges, edge_vals, dev, mo);
+    } else if (exact && exact_evals) {
+        mo.positions.swap(exact->positions), mo.normals.swap(exact->normals), mo.atoms.swap(exact->atoms);
+        mo.patches.swap(exact->patches), mo.t.swap(exact->t);
+        place_exact(arr, mp, keys, nb, edge_off, edges, edge_vals, exact_evals, mo);
+    } else {
+        refine_exact(arr, mp, keys, nb, edge_off, edges, edge_vals, mo);
+    }
     double t_host = ms_since(t1);
     auto t2 = clk::now();
     Mesh& mesh = s.mesh;
@@ -186,6 +194,10 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
     if (p->refine == SMB_REFINE_FAST) {
         rc = smb_resident_set_refinement(e->res, err, errlen);
         if (rc != SMB_OK) return rc;
+    } else {
+        rc = smb_resident_set_exact(e->res, A.orig.data(), A.circle_ij.data(), A.n_circles(), A.vertex_atoms.data(),
+                                    A.n_vertices(), P.t_min, err, errlen);
+        if (rc != SMB_OK) return rc;
     }
     e->t_upload = ms_since(t1);
     *out = e.release();
@@ -219,6 +231,10 @@ int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size
         rc = e->warm ? smb_refine_warm(e->res, e->batch, e->warm, &ms, err, errlen)
                      : smb_refine(e->res, e->batch, &ms, err, errlen);
         if (rc != SMB_OK) return rc;
+        t.total += ms;
+    } else if (e->exact_device) {
+        double ms = 0;
+        if ((rc = smb_refine_exact(e->res, e->batch, &ms, err, errlen)) != SMB_OK) return rc;
         t.total += ms;
     }
     e->times = t;
@@ -271,12 +287,22 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
         if ((rc = smb_batch_edges(e->batch, e->t.data(), e->feat.data(), e->closest.data(), e->evals.data())) != SMB_OK)
             return set_err(err, errlen, "edge results copy"), rc;
     }
+    const bool exact_dev = !fast && e->exact_device;
+    if (exact_dev && ne) {
+        smbh::MeshOut& x = e->exact_out;
+        x.positions.resize(ne), x.normals.resize(ne), x.atoms.resize(ne), x.patches.resize(ne), x.t.resize(ne);
+        e->exact_evals.resize(ne);
+        if ((rc = smb_batch_vertices(e->batch, x.positions.data()->data(), x.normals.data()->data(), x.atoms.data(),
+                                     x.patches.data(), x.t.data(), e->exact_evals.data())) != SMB_OK)
+            return set_err(err, errlen, "vertex copy"), rc;
+    }
     double t_d2h = ms_since(t0);
     auto s = std::make_unique<smb_surface>();
     std::string m = finish_surface(e->arr, e->mp, fast, e->keys.data(), nb, e->edge_off.data(), e->edges.data(),
                                    e->edge_vals.data(), e->tri_off.data(), e->tris.data(),
                                    DeviceRefine{e->t.data(), e->feat.data(), e->closest.data(), e->evals.data()}, *s,
-                                   e->dev, &e->measure);
+                                   e->dev, &e->measure, exact_dev && ne ? &e->exact_out : nullptr,
+                                   exact_dev && ne ? e->exact_evals.data() : nullptr);
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_STATE;
     smb_surface_stats& st = s->stats;
     st.touched_bricks = e->touched;
@@ -308,6 +334,12 @@ int smb_engine_field(const smb_engine* e, const double* points, size_t n, double
             values[i] = eval_local(e->arr, x, band, l).value;
         }
     });
+    return SMB_OK;
+}
+
+int smb_engine_set_exact_device(smb_engine* e, int on) {
+    if (!e) return SMB_ERR_ARG;
+    e->exact_device = on != 0;
     return SMB_OK;
 }
 

@@ -507,6 +507,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     b->n = uint32_t(count);
     b->first = first;
     b->refined = false;
+    b->refined_exact = false;
     b->n_work = 0;
     b->n_edges = b->n_tris = 0;
     b->ids_words = 0;
@@ -685,6 +686,7 @@ static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* m
         return rc;
     if (mode == EDGE_FEATURES && (rc = b->e_x.reserve(ne * 4 * 32, err, errlen))) return rc;
     b->refined = false;
+    b->refined_exact = false;
     if (ms) *ms = 0;
     if (ne == 0 || b->n_work == 0) {
         if (ne) CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
@@ -763,6 +765,114 @@ int smb_batch_edge_features(smb_resident* r, smb_batch* b, float* features, uint
     return SMB_OK;
 }
 
+int smb_resident_set_exact(smb_resident* r, const uint32_t* orig, const uint32_t* circle_ij, size_t n_circles,
+                           const uint32_t* vertex_atoms, size_t n_vertices, double t_min, char* err, size_t errlen) {
+    if (!r) return set_err(err, errlen, "null resident"), SMB_ERR_ARG;
+    const size_t n = r->A.n;
+    if ((n && !orig) || (n_circles && !circle_ij) || (n_vertices && !vertex_atoms))
+        return set_err(err, errlen, "missing attribute tables"), SMB_ERR_ARG;
+    if (n_circles != r->A.nc || n_vertices != r->A.nv)
+        return set_err(err, errlen, "attribute tables do not match the arrangement (%zu circles, %zu vertices)",
+                       size_t(r->A.nc), size_t(r->A.nv)),
+               SMB_ERR_ARG;
+    for (size_t i = 0; i < 2 * n_circles; i++)
+        if (circle_ij[i] >= n) return set_err(err, errlen, "circle atom out of range"), SMB_ERR_ARG;
+    for (size_t i = 0; i < 3 * n_vertices; i++)
+        if (vertex_atoms[i] >= n) return set_err(err, errlen, "vertex atom out of range"), SMB_ERR_ARG;
+    if (!(t_min >= 0.0 && t_min < 0.5)) return set_err(err, errlen, "t_min must be in [0, 0.5)"), SMB_ERR_ARG;
+    smb_device* d = r->dev;
+    CK(cudaSetDevice(d->index));
+    const void* src[3] = {orig, circle_ij, vertex_atoms};
+    const size_t bytes[3] = {n * 4, n_circles * 8, n_vertices * 12};
+    const uint32_t* dst[3] = {nullptr, nullptr, nullptr};
+    for (int k = 0; k < 3; k++) {
+        void* p = nullptr;
+        int rc = dev_alloc(&p, bytes[k], &r->owned, &r->bytes, err, errlen);
+        if (rc != SMB_OK) return rc;
+        if (bytes[k]) CK(cudaMemcpyAsync(p, src[k], bytes[k], cudaMemcpyHostToDevice, d->stream));
+        dst[k] = static_cast<const uint32_t*>(p);
+    }
+    CK(cudaStreamSynchronize(d->stream));
+    r->xa = ExactAttr{dst[0], dst[1], dst[2], t_min};
+    r->exact_ready = true;
+    return SMB_OK;
+}
+
+int smb_refine_exact(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errlen) {
+    if (!r || !b || b->res != r) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
+    if (!r->exact_ready) return set_err(err, errlen, "smb_resident_set_exact must run first"), SMB_ERR_STATE;
+    smb_device* d = r->dev;
+    CK(cudaSetDevice(d->index));
+    cudaStream_t s = d->stream;
+    const size_t ne = b->n_edges;
+    const uint32_t nw = b->n_work;
+    int rc;
+    if ((rc = b->x_pos.reserve(ne * 12, err, errlen)) || (rc = b->x_nrm.reserve(ne * 12, err, errlen)) ||
+        (rc = b->x_atom.reserve(ne * 4, err, errlen)) || (rc = b->x_patch.reserve(ne, err, errlen)) ||
+        (rc = b->e_t.reserve(ne * 4, err, errlen)) || (rc = b->e_evals.reserve(ne * 4, err, errlen)) ||
+        (rc = b->x_ovf.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
+        (rc = b->item_counts.reserve(size_t(nw) * 4, err, errlen)) ||
+        (rc = b->item_off.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
+        (rc = b->item_edges.reserve(ne * 4, err, errlen)) ||
+        (rc = b->tiles.reserve(size_t(scan_tiles_needed(nw)) * 8, err, errlen)))
+        return rc;
+    b->refined_exact = false;
+    b->refined = false;
+    if (ms) *ms = 0;
+    cudaEventRecord(b->ev[4], s);
+    if (ne) CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
+    if (ne && nw) {
+        unsigned long long* cnt = b->counters.as<unsigned long long>();
+        CK(cudaMemsetAsync(cnt + CNT_MAXITEM, 0, 8, s));
+        launch_item_edges(r->L, b->work.as<uint32_t>(), nw, b->rec.as<uint32_t>(), b->edge_off.as<uint32_t>(),
+                          b->edges.as<uint32_t>(), b->item_counts.as<uint32_t>(), b->item_off.as<uint32_t>(),
+                          b->item_edges.as<uint32_t>(), b->tiles.as<unsigned long long>(),
+                          b->totals.as<unsigned long long>() + 3, cnt, s);
+        ExactOut out{b->x_pos.as<float>(), b->x_nrm.as<float>(), b->x_atom.as<uint32_t>(), b->x_patch.as<uint8_t>(),
+                     b->e_t.as<float>(), b->e_evals.as<uint32_t>()};
+        cudaError_t e = launch_refine_exact(r->A, r->L, r->xa, r->keys + b->first, b->work.as<uint32_t>(),
+                                            b->edges.as<uint32_t>(), b->edge_vals.as<float2>(),
+                                            b->item_off.as<uint32_t>(), b->item_edges.as<uint32_t>(), nw, out,
+                                            b->x_ovf.as<uint32_t>(), cnt, d->info.multiprocessors, d->smem_optin,
+                                            b->x_region, s);
+        if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    }
+    cudaEventRecord(b->ev[5], s);
+    CK(cudaStreamSynchronize(s));
+    float t = 0;
+    cudaEventElapsedTime(&t, b->ev[4], b->ev[5]);
+    if (ms) *ms = t;
+    uint32_t n_block = 0;
+    if (ne && nw) CK(cudaMemcpy(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost));
+    b->x_block_items = n_block;
+    b->refined_exact = true;
+    return SMB_OK;
+}
+
+int smb_batch_vertices(const smb_batch* b, float* positions, float* normals, uint32_t* atoms, uint8_t* patches,
+                       float* t, uint32_t* evals) {
+    if (!b || !b->refined_exact) return SMB_ERR_STATE;
+    cudaSetDevice(b->res->dev->index);
+    const size_t ne = b->n_edges;
+    if (!ne) return SMB_OK;
+    cudaStream_t s = b->res->dev->stream;
+    bool ok = true;
+    if (positions) ok &= cudaMemcpyAsync(positions, b->x_pos.p, ne * 12, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    if (normals) ok &= cudaMemcpyAsync(normals, b->x_nrm.p, ne * 12, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    if (atoms) ok &= cudaMemcpyAsync(atoms, b->x_atom.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    if (patches) ok &= cudaMemcpyAsync(patches, b->x_patch.p, ne, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    if (t) ok &= cudaMemcpyAsync(t, b->e_t.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    if (evals) ok &= cudaMemcpyAsync(evals, b->e_evals.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    ok &= cudaStreamSynchronize(s) == cudaSuccess;
+    return ok ? SMB_OK : SMB_ERR_CUDA;
+}
+
+int smb_batch_set_exact_region(smb_batch* b, size_t bytes) {
+    if (!b || bytes < 1024 || bytes > 48 * 1024) return SMB_ERR_ARG;
+    b->x_region = bytes;
+    return SMB_OK;
+}
+
 int smb_batch_edges(const smb_batch* b, float* t, uint32_t* feat, float* closest, uint32_t* evals) {
     if (!b || !b->refined) return SMB_ERR_STATE;
     cudaSetDevice(b->res->dev->index);
@@ -797,6 +907,7 @@ int smb_batch_info_get(const smb_batch* b, smb_batch_info* out) {
         if (cudaMemcpy(c, b->counters.p, sizeof c, cudaMemcpyDeviceToHost) != cudaSuccess) return SMB_ERR_CUDA;
     }
     out->pack_units = c[CNT_PACK];
+    out->exact_block_items = b->x_block_items;
     return SMB_OK;
 }
 

@@ -61,6 +61,8 @@ struct smb_resident {
     float classify_ms = 0;
     smb::RefineConsts rc{};
     bool refine_ready = false;
+    smb::ExactAttr xa{};  // exact mode on the device (smb_resident_set_exact)
+    bool exact_ready = false;
     std::atomic<int> refs{0};  // batches made on this resident
     std::atomic<bool> freed{false}, gone{false};
 };
@@ -76,12 +78,17 @@ struct smb_batch {
     smb::DBuf e_t, e_feat, e_q, e_evals;  // fast-mode refinement results
     smb::DBuf e_x;                        // warm-start features (32 f32 per edge)
     smb::DBuf item_counts, item_off, item_edges;  // per sampled sub-block edge lists
+    smb::DBuf x_pos, x_nrm, x_atom, x_patch, x_ovf;  // exact mode on the device: vertices, overflowed items
+    bool refined_exact = false;
+    size_t x_block_items = 0;  // items of the last exact pass refined by a whole block
+    size_t x_region = 18432;  // shared-memory bytes per warp for one sub-block's f64 candidate lists
     smb::GatherCaps caps{192, 128, 384, 128};
     int gather_warps = 4;
     bool use_tma = true;
     cudaEvent_t ev[6] = {};
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
-                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &item_counts, &item_off, &item_edges};
+                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &item_counts, &item_off, &item_edges,
+                &x_pos, &x_nrm, &x_atom, &x_patch, &x_ovf};
     }
 };

@@ -100,7 +100,7 @@ class MultiTimes(C.Structure):
 class BatchInfo(C.Structure):
     _fields_ = [(f, C.c_size_t) for f in ("bricks", "sampled_subblocks", "ids_words", "max_pack_units", "edges",
                                           "triangles", "touched", "resident_bytes")] + \
-               [("pack_units", C.c_ulonglong), ("classify_ms", C.c_double)]
+               [("pack_units", C.c_ulonglong), ("classify_ms", C.c_double), ("exact_block_items", C.c_size_t)]
 
 
 # Every entry point of include/*.h with its ctypes signature.
@@ -131,6 +131,10 @@ SIGNATURES = {
     "smb_batch_edges": (C.c_int, [_vp, _fp, _u32p, _fp, _u32p]),
     "smb_refine_warm": (C.c_int, [_vp, _vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
     "smb_batch_edge_features": (C.c_int, [_vp, _vp, _fp, C.POINTER(C.c_uint8), _cp, _sz]),
+    "smb_resident_set_exact": (C.c_int, [_vp, _u32p, _u32p, _sz, _u32p, _sz, C.c_double, _cp, _sz]),
+    "smb_refine_exact": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
+    "smb_batch_vertices": (C.c_int, [_vp, _fp, _fp, _u32p, C.POINTER(C.c_uint8), _fp, _u32p]),
+    "smb_batch_set_exact_region": (C.c_int, [_vp, _sz]),
     "smb_kernel_launches": (C.c_ulonglong, []),
     "smb_batch_info_get": (C.c_int, [_vp, C.POINTER(BatchInfo)]),
     "smb_batch_count_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _cp, _sz]),
@@ -154,6 +158,7 @@ SIGNATURES = {
     "smb_engine_bricks": (_sz, [_vp]),
     "smb_engine_mesh": (C.c_int, [_vp, C.POINTER(_vp), _cp, _sz]),
     "smb_engine_set_warm_start": (C.c_int, [_vp, _vp]),
+    "smb_engine_set_exact_device": (C.c_int, [_vp, C.c_int]),
     "smb_engine_field": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(C.c_double)]),
     "smb_engine_warm_start_rows": (C.c_int, [_vp, _fp, _fp, _sz, C.POINTER(_sz), _cp, _sz]),
     "smb_surface_free": (None, [_vp]),
@@ -406,6 +411,42 @@ class Batch:
         else:
             _check(lib().smb_refine_warm(self.res.h, self.h, mlp.h, C.byref(ms), err, 1024), err)
         return ms.value
+
+    def refine_exact(self, orig, circle_ij, vertex_atoms, t_min, region=None):
+        """Exact-mode f64 refinement of the last run's crossing edges on the
+        device (smb_resident_set_exact with the attribute tables, then
+        smb_refine_exact); device ms."""
+        err = C.create_string_buffer(1024)
+        orig = np.ascontiguousarray(orig, np.uint32)
+        cij = np.ascontiguousarray(circle_ij, np.uint32).reshape(-1)
+        va = np.ascontiguousarray(vertex_atoms, np.uint32).reshape(-1)
+        _check(lib().smb_resident_set_exact(self.res.h, _p(orig, C.c_uint32), _p(cij, C.c_uint32), len(cij) // 2,
+                                            _p(va, C.c_uint32), len(va) // 3, float(t_min), err, 1024), err)
+        if region is not None:
+            if lib().smb_batch_set_exact_region(self.h, int(region)) != SMB_OK:
+                raise ValueError("exact region must be 1 KiB..48 KiB, got %d" % region)
+        ms = C.c_double(0)
+        _check(lib().smb_refine_exact(self.res.h, self.h, C.byref(ms), err, 1024), err)
+        return ms.value
+
+    def vertices(self):
+        """Per crossing edge after refine_exact: positions (n, 3), normals
+        (n, 3), atoms, patches, t, evaluations (0: left to the host)."""
+        ne, nt = _sz(0), _sz(0)
+        lib().smb_batch_mc_counts(self.h, C.byref(ne), C.byref(nt))
+        n = max(ne.value, 1)
+        pos = np.zeros((n, 3), np.float32)
+        nrm = np.zeros((n, 3), np.float32)
+        atom = np.zeros(n, np.uint32)
+        patch = np.zeros(n, np.uint8)
+        t = np.zeros(n, np.float32)
+        ev = np.zeros(n, np.uint32)
+        rc = lib().smb_batch_vertices(self.h, _p(pos, C.c_float), _p(nrm, C.c_float), _p(atom, C.c_uint32),
+                                      _p(patch, C.c_uint8), _p(t, C.c_float), _p(ev, C.c_uint32))
+        if rc != SMB_OK:
+            raise SmbError(rc, "smb_batch_vertices")
+        k = ne.value
+        return pos[:k], nrm[:k], atom[:k], patch[:k], t[:k], ev[:k]
 
     def edges(self):
         """Per crossing edge: t, feature, closest point, evaluations (bit 31:

@@ -186,6 +186,11 @@ class SurfaceEngine:
                C.create_string_buffer(8))
         return out
 
+    def set_exact_on_device(self, on=True):
+        """Exact mode: refine vertices in f64 on the device (default) or on
+        the host threads (as the reference); the mesh bytes are the same."""
+        lib().smb_engine_set_exact_device(self.h, 1 if on else 0)
+
     def set_warm_start(self, mlp):
         """Start fast-mode refinement from `mlp` (a native.Mlp on this
         engine's device; None: the linear guess)."""

@@ -1,0 +1,78 @@
+"""Exact mode with the f64 vertex refinement on the device (smb_refine_exact).
+
+The device restates the host's exact refinement operation by operation, so
+the mesh must be byte-identical whichever side refines: OBJ bytes, counts,
+area, volume and evaluation counts are compared for equality with the
+host-refined mesh (and, through test_surface_gpu.py, with the CPU oracle).
+The device must refine nearly every edge itself, and its whole-block path
+(taken by sub-blocks whose lists exceed a warp's share of shared memory)
+must give the same vertices as the warp path.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from helpers import random_chain
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    from sesmesh_b200 import workloads
+    out = []
+    for seed, n in ((5, 40), (11, 60)):
+        s, p = random_chain(seed, n)
+        out.append(("chain%d" % seed, s, p, 0.3))
+    g = workloads.globule330()
+    out.append(("globule330@0.5", g["spheres"], 1.4, 0.5))
+    out.append(("globule330@0.25", g["spheres"], 1.4, 0.25))
+    out.append(("globule330@1", g["spheres"], 1.4, 1.0))
+    u = workloads.globule2800()
+    out.append(("globule2800@0.25", u["spheres"], 1.4, 0.25))
+    out.append(("one sphere", np.array([[0.3, -0.2, 0.1, 1.7]]), 1.4, 0.25))
+    out.append(("stall4", np.array([[42.580, -79.518, -23.569, 1.52], [45.767, -76.655, -20.023, 1.7],
+                                    [46.735, -77.095, -22.324, 1.7], [45.949, -76.134, -21.455, 1.7]]), 1.4, 0.25))
+    return out
+
+
+def _mesh(spheres, probe, h, on_device, region=None, brick=10):
+    from sesmesh_b200 import surface as S
+    from sesmesh_b200.native import lib
+    eng = S.SurfaceEngine(spheres, S.SurfaceParams.ses(probe).with_spacing(h).with_brick_size(brick))
+    eng.set_exact_on_device(on_device)
+    if region is not None:
+        assert lib().smb_batch_set_exact_region(lib().smb_engine_batch(eng.h), C.c_size_t(region)) == 0
+    out = eng.mesh()
+    res = (out.obj(), dict(out.stats))
+    out.close()
+    eng.close()
+    return res
+
+
+KEYS = ("vertices", "triangles", "components", "surface_bricks", "area", "volume", "euler", "refine_evaluations")
+
+
+@pytest.mark.parametrize("case", _cases(), ids=lambda c: c[0])
+def test_device_exact_equals_host_exact(case):
+    name, spheres, probe, h = case
+    obj_d, st_d = _mesh(spheres, probe, h, True)
+    obj_h, st_h = _mesh(spheres, probe, h, False)
+    for k in KEYS:
+        assert st_d[k] == st_h[k], (k, st_d[k], st_h[k])
+    assert obj_d == obj_h
+    assert st_h["refine_cpu_edges"] == 0
+    # The host refines only the edges the device leaves to it.
+    if st_d["vertices"] > 1000:
+        assert st_d["refine_cpu_edges"] < 0.01 * st_d["vertices"], st_d["refine_cpu_edges"]
+
+
+@pytest.mark.parametrize("brick", [10, 16])
+def test_block_path_equals_warp_path(brick):
+    from sesmesh_b200 import workloads
+    g = workloads.globule330()
+    obj_w, st_w = _mesh(g["spheres"], 1.4, 0.35, True, brick=brick)
+    obj_b, st_b = _mesh(g["spheres"], 1.4, 0.35, True, region=1024, brick=brick)
+    for k in KEYS + ("refine_cpu_edges",):
+        assert st_w[k] == st_b[k], (k, st_w[k], st_b[k])
+    assert obj_w == obj_b
