@@ -290,9 +290,12 @@ def run_ours(a):
     info = eng.batch_info()
     h2d = int(info["resident_bytes"])
     d2h = int(n_bricks * 16 + (n_bricks + 1) * 8 + st["vertices"] * 12 + st["triangles"] * 12)
-    # Per edge: t, feature, closest point, evaluations (fast); position,
-    # normal, atom, patch, t, evaluations (exact, refined on the device).
-    d2h += int(st["vertices"] * (24 if w["refine"] == "fast" else 37))
+    if w["refine"] == "fast":
+        d2h += int(st["vertices"] * 24)  # per edge: t, feature, closest point, evaluations
+    else:
+        # Exact mode finished on the device: the finished mesh alone (position,
+        # normal, atom, component, patch per vertex; triangles) and 16 B of totals.
+        d2h = int(st["vertices"] * 33 + st["triangles"] * 12 + 16)
 
     pk, pk_kind = peaks()
     ops, owned = eng.count_ops()

@@ -89,6 +89,11 @@ int smb_surface_stats_get(const smb_surface* s, smb_surface_stats* out);
 /* Mesh arrays (Mesh, mesh/mod.rs:48-67), triangles grouped by component. */
 int smb_surface_mesh(const smb_surface* s, float* positions, float* normals, uint32_t* triangles, uint32_t* atoms,
                      uint8_t* patches, uint32_t* components);
+/* The same arrays without a copy: pointers into the surface, valid until
+ * smb_surface_free (null for empty arrays). */
+int smb_surface_arrays(const smb_surface* s, const float** positions, const float** normals,
+                       const uint32_t** triangles, const uint32_t** atoms, const uint8_t** patches,
+                       const uint32_t** components);
 /* OBJ bytes with the default options (export/obj.rs:37-73): returns the
  * length, copies at most cap bytes. */
 size_t smb_surface_obj(smb_surface* s, char* out, size_t cap);

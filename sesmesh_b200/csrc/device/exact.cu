@@ -541,7 +541,35 @@ __global__ void __launch_bounds__(32 * X_WARPS, 1) k_refine_exact(DArr A, DLat L
     }
 }
 
+// Sum of the edges' evaluation counts and the number of edges left to the
+// host (evals = 0): out[0], out[1].
+__global__ void k_exact_summary(const uint32_t* evals, size_t n, unsigned long long* out) {
+    unsigned long long sum = 0, zero = 0;
+    for (size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x; k < n; k += size_t(gridDim.x) * blockDim.x) {
+        const uint32_t e = evals[k];
+        sum += e;
+        zero += e == 0;
+    }
+    for (int o = 16; o; o >>= 1) {
+        sum += __shfl_down_sync(0xffffffffu, sum, o);
+        zero += __shfl_down_sync(0xffffffffu, zero, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (sum) atomicAdd(&out[0], sum);
+        if (zero) atomicAdd(&out[1], zero);
+    }
+}
+
 }  // namespace
+
+cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long long* out, int sms, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, 16, s);
+    if (e != cudaSuccess || !n) return e;
+    const size_t want = (n + 255) / 256;
+    count_launches(1);
+    k_exact_summary<<<unsigned(std::min<size_t>(want, size_t(sms) * 8)), 256, 0, s>>>(evals, n, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                 const uint32_t* work, const uint32_t* edges, const float2* edge_vals,

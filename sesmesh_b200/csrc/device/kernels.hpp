@@ -115,6 +115,8 @@ struct ExactOut {
 // item with `region` bytes of shared memory for the item's candidate lists,
 // then the items that did not fit (ovf: count then items, n_items + 1
 // words) with a CTA each.
+// out[0] = sum of evals[0..n), out[1] = how many are 0.
+cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long long* out, int sms, cudaStream_t s);
 cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                 const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,

@@ -22,7 +22,9 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "../host/mesher.hpp"
@@ -327,6 +329,76 @@ uint64_t pow2_at_least(uint64_t v) {
     return p;
 }
 
+// extract::assemble (mesh/extract.rs:606-691) on the device.  Packed brick
+// keys (lattice.rs:93-96): the bricks must be in ascending packed order.
+__device__ __forceinline__ unsigned long long pack_key(long long x, long long y, long long z) {
+    const long long bias = 1ll << 20;
+    return (unsigned long long)(x + bias) | ((unsigned long long)(y + bias) << 21) |
+           ((unsigned long long)(z + bias) << 42);
+}
+
+__global__ void k_packed_keys(const int4* keys, uint32_t n, unsigned long long* packed, unsigned long long* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 k = keys[i];
+    packed[i] = pack_key(k.x, k.y, k.z);
+    if (i > 0) {
+        const int4 p = keys[i - 1];
+        if (pack_key(k.x, k.y, k.z) <= pack_key(p.x, p.y, p.z)) atomicOr(err, 4ull);
+    }
+}
+
+// Thread per triangle: each corner's (neighbour code, edge id) reference
+// resolved to the global vertex index edge_off[target] + position of the
+// edge in the target brick's (ascending) edge list.  err |= 1: a reference
+// to a missing brick; 2: to an edge without vertex.
+__global__ void k_assemble(const unsigned long long* packed, const int4* keys, uint32_t n, const uint32_t* edge_off,
+                           const uint32_t* edges, const uint32_t* tri_off, const uint32_t* refs, uint32_t nt,
+                           uint32_t* tris, unsigned long long* err) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    uint32_t lo = 0, hi = n;  // the brick holding triangle t: tri_off[lo] <= t < tri_off[lo + 1]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (tri_off[mid] <= t) lo = mid;
+        else hi = mid;
+    }
+    const int4 key = keys[lo];
+    for (int c = 0; c < 3; c++) {
+        const uint32_t r = refs[3 * size_t(t) + c], code = r >> 28, id = r & ((1u << 28) - 1);
+        uint32_t tb = lo;
+        if (code) {
+            const unsigned long long want = pack_key((long long)key.x + (code & 1), (long long)key.y + ((code >> 1) & 1),
+                                                     (long long)key.z + ((code >> 2) & 1));
+            uint32_t a = 0, b = n;
+            while (a < b) {
+                const uint32_t mid = (a + b) >> 1;
+                if (packed[mid] < want) a = mid + 1;
+                else b = mid;
+            }
+            if (a == n || packed[a] != want) {
+                atomicOr(err, 1ull);
+                tris[3 * size_t(t) + c] = 0;
+                continue;
+            }
+            tb = a;
+        }
+        uint32_t a = edge_off[tb], b = edge_off[tb + 1];
+        const uint32_t e1 = b;
+        while (a < b) {
+            const uint32_t mid = (a + b) >> 1;
+            if (edges[mid] < id) a = mid + 1;
+            else b = mid;
+        }
+        if (a == e1 || edges[a] != id) {
+            atomicOr(err, 2ull);
+            tris[3 * size_t(t) + c] = 0;
+            continue;
+        }
+        tris[3 * size_t(t) + c] = a;
+    }
+}
+
 unsigned bits_for(uint32_t n) {
     unsigned b = 1;
     while (b < 32 && (uint64_t(1) << b) <= n) b++;
@@ -347,15 +419,22 @@ unsigned bits_for(uint32_t n) {
 void MeasureScratch::release() {
     for (DBuf* b : {&pos, &nrm, &tris, &tris_out, &keys, &cnt, &dup, &parent, &flag, &cid, &id, &counters, &comp_v,
                     &comp_t, &comp_e, &area, &volume, &parts, &pkey, &pidx, &pkey2, &pidx2, &first, &tkey, &tidx,
-                    &tkey2, &tidx2, &tiles, &cub})
+                    &tkey2, &tidx2, &tiles, &cub, &packed, &err})
         b->release();
+    pinned_free(host);
+    host = nullptr;
+    host_cap = 0;
 }
 
-bool measure_on_device(smb_device* d, smbh::Mesh& m, std::vector<smbh::Component>& comps, size_t* bad,
-                       MeasureScratch& S, std::string* msg) {
+// The measure of a mesh already on the device (pos, nrm: 3 f32 per vertex,
+// nrm may be null; tris: 3 u32 per triangle).  Results: comps, *bad, and,
+// when there are no defects, each vertex's component into host_comp and the
+// regrouped triangles into host_tris (nv and 3 nt words on the host).
+static bool measure_core(smb_device* d, const float* pos, const float* nrm, const uint32_t* tris, size_t nv,
+                         size_t nt, std::vector<smbh::Component>& comps, size_t* bad, MeasureScratch& S,
+                         std::string* msg, uint32_t* host_comp, uint32_t* host_tris) {
     using smbh::Component;
     cudaStream_t s = d->stream;
-    const size_t nv = m.positions.size(), nt = m.triangles.size();
     if (nv >= (size_t(1) << 31) || nt >= (size_t(1) << 31)) {
         if (msg) *msg = "mesh too large for the device measure";
         return false;
@@ -365,7 +444,7 @@ bool measure_on_device(smb_device* d, smbh::Mesh& m, std::vector<smbh::Component
     const uint64_t ecap = pow2_at_least(uint64_t(nt) * 3 + 16), dcap = pow2_at_least(uint64_t(nt) * 2 + 16);
     const uint32_t n_chunks = uint32_t((nt + SUM_CHUNK - 1) / SUM_CHUNK);
     const size_t max_parts = size_t(n_chunks) * CHUNK_COMPS;
-    if (!R(S.pos, nv * 12) || !R(S.nrm, nv * 12) || !R(S.tris, nt * 12) || !R(S.tris_out, nt * 12) ||
+    if (!R(S.tris_out, nt * 12) ||
         !R(S.keys, ecap * 8) || !R(S.cnt, ecap * 8) || !R(S.dup, dcap * 4) || !R(S.parent, nv * 4) ||
         !R(S.flag, nv * 4) || !R(S.cid, nv * 4) || !R(S.id, nv * 4) || !R(S.counters, 64) ||
         !R(S.parts, max_parts * sizeof(Partial)) || !R(S.pkey, max_parts * 4) || !R(S.pidx, max_parts * 4) ||
@@ -376,14 +455,8 @@ bool measure_on_device(smb_device* d, smbh::Mesh& m, std::vector<smbh::Component
     }
     unsigned long long* cnt = S.counters.as<unsigned long long>();  // 0 bad, 1 oob, 2 parts, 3 overflow, 4 comps, 5 union-find
     MCK(cudaMemsetAsync(cnt, 0, 64, s));
-    MCK(cudaMemcpyAsync(S.pos.p, m.positions.data(), nv * 12, cudaMemcpyHostToDevice, s));
-    const bool normals = !m.normals.empty();
-    if (normals) MCK(cudaMemcpyAsync(S.nrm.p, m.normals.data(), nv * 12, cudaMemcpyHostToDevice, s));
-    MCK(cudaMemcpyAsync(S.tris.p, m.triangles.data(), nt * 12, cudaMemcpyHostToDevice, s));
-    const float* pos = S.pos.as<float>();
-    const uint32_t* tris = S.tris.as<uint32_t>();
     auto blocks = [](uint64_t n) { return unsigned((n + 255) / 256); };
-    if (nv) k_vertex_checks<<<blocks(nv), 256, 0, s>>>(pos, normals ? S.nrm.as<float>() : nullptr, uint32_t(nv), cnt);
+    if (nv) k_vertex_checks<<<blocks(nv), 256, 0, s>>>(pos, nrm, uint32_t(nv), cnt);
     if (nt) k_index_checks<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), uint32_t(nv), cnt + 1);
     unsigned long long c2[2];
     MCK(cudaMemcpyAsync(c2, cnt, 16, cudaMemcpyDeviceToHost, s));
@@ -506,7 +579,6 @@ bool measure_on_device(smb_device* d, smbh::Mesh& m, std::vector<smbh::Component
     // Results to the host.
     std::vector<unsigned long long> cv(nc), ct(nc), ce(nc);
     std::vector<double> ca(nc), cvol(nc);
-    m.vertex_component.resize(nv);
     if (nc) {
         MCK(cudaMemcpyAsync(cv.data(), S.comp_v.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
         MCK(cudaMemcpyAsync(ct.data(), S.comp_t.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
@@ -514,8 +586,8 @@ bool measure_on_device(smb_device* d, smbh::Mesh& m, std::vector<smbh::Component
         MCK(cudaMemcpyAsync(ca.data(), S.area.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
         MCK(cudaMemcpyAsync(cvol.data(), S.volume.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
     }
-    if (nv) MCK(cudaMemcpyAsync(m.vertex_component.data(), id, nv * 4, cudaMemcpyDeviceToHost, s));
-    if (nt) MCK(cudaMemcpyAsync(m.triangles.data(), S.tris_out.p, nt * 12, cudaMemcpyDeviceToHost, s));
+    if (nv) MCK(cudaMemcpyAsync(host_comp, id, nv * 4, cudaMemcpyDeviceToHost, s));
+    if (nt) MCK(cudaMemcpyAsync(host_tris, S.tris_out.p, nt * 12, cudaMemcpyDeviceToHost, s));
     MCK(cudaStreamSynchronize(s));
     comps.assign(nc, Component());
     size_t start = 0;
@@ -530,6 +602,131 @@ bool measure_on_device(smb_device* d, smbh::Mesh& m, std::vector<smbh::Component
         start += C.triangles;
     }
     return true;
+}
+
+bool measure_on_device(smb_device* d, smbh::Mesh& m, std::vector<smbh::Component>& comps, size_t* bad,
+                       MeasureScratch& S, std::string* msg) {
+    cudaStream_t s = d->stream;
+    const size_t nv = m.positions.size(), nt = m.triangles.size();
+    char e[256];
+    auto R = [&](DBuf& b, size_t bytes) { return b.reserve(std::max<size_t>(bytes, 16), e, sizeof e) == 0; };
+    if (!R(S.pos, nv * 12) || !R(S.nrm, nv * 12) || !R(S.tris, nt * 12)) {
+        if (msg) *msg = std::string("device memory for the measure: ") + e;
+        return false;
+    }
+    MCK(cudaMemcpyAsync(S.pos.p, m.positions.data(), nv * 12, cudaMemcpyHostToDevice, s));
+    const bool normals = !m.normals.empty();
+    if (normals) MCK(cudaMemcpyAsync(S.nrm.p, m.normals.data(), nv * 12, cudaMemcpyHostToDevice, s));
+    MCK(cudaMemcpyAsync(S.tris.p, m.triangles.data(), nt * 12, cudaMemcpyHostToDevice, s));
+    m.vertex_component.resize(nv);
+    return measure_core(d, S.pos.as<float>(), normals ? S.nrm.as<float>() : nullptr, S.tris.as<uint32_t>(), nv, nt,
+                        comps, bad, S, msg, m.vertex_component.data(), reinterpret_cast<uint32_t*>(m.triangles.data()));
+}
+
+void* MeasureScratch::staging(size_t bytes) {
+    if (bytes <= host_cap) return host;
+    pinned_free(host);
+    host_cap = 0;
+    const size_t want = bytes + bytes / 4;
+    host = pinned_alloc(want);
+    if (host) host_cap = want;
+    return host;
+}
+
+int finish_on_device(smb_device* d, const DeviceMesh& in, smbh::Mesh& m, std::vector<smbh::Component>& comps,
+                     size_t* bad, MeasureScratch& S, std::string* msg, double* ms_assemble, double* ms_copy) {
+    cudaStream_t s = d->stream;
+    const size_t nv = in.n_edges, nt = in.n_tris;
+    if (nv >= (size_t(1) << 31) || nt >= (size_t(1) << 31) || in.n_bricks == 0) {
+        if (msg) *msg = "mesh too large (or empty) for the device path";
+        return 1;
+    }
+    char e[256];
+    auto R = [&](DBuf& b, size_t bytes) { return b.reserve(std::max<size_t>(bytes, 16), e, sizeof e) == 0; };
+    if (!R(S.packed, size_t(in.n_bricks) * 8) || !R(S.tris, nt * 12) || !R(S.err, 16)) {
+        if (msg) *msg = std::string("device memory for the assembly: ") + e;
+        return 1;
+    }
+    const size_t stage = nv * 33 + nt * 12;
+    unsigned char* H = static_cast<unsigned char*>(S.staging(stage));
+    if (!H) {
+        if (msg) *msg = "page-locked staging memory";
+        return 1;
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    auto blocks = [](uint64_t n) { return unsigned((n + 255) / 256); };
+    unsigned long long* err = S.err.as<unsigned long long>();
+    if (cudaMemsetAsync(err, 0, 8, s) != cudaSuccess) return 1;
+    k_packed_keys<<<blocks(in.n_bricks), 256, 0, s>>>(in.keys, uint32_t(in.n_bricks), S.packed.as<unsigned long long>(),
+                                                      err);
+    if (nt)
+        k_assemble<<<blocks(nt), 256, 0, s>>>(S.packed.as<unsigned long long>(), in.keys, uint32_t(in.n_bricks),
+                                              in.edge_off, in.edges, in.tri_off, in.tri_refs, uint32_t(nt),
+                                              S.tris.as<uint32_t>(), err);
+    count_launches(nt ? 2 : 1);
+    unsigned long long ferr = 0;
+    if (cudaMemcpyAsync(&ferr, err, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        if (msg) *msg = "device assembly failed";
+        return 1;
+    }
+    if (ms_assemble) *ms_assemble = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (ferr) {
+        if (msg)
+            *msg = (ferr & 4) ? "bricks are not in packed-key order"
+                   : (ferr & 1) ? "triangle references an edge of a missing brick"
+                                : "triangle references an edge without vertex";
+        return 2;
+    }
+    // Staging layout: positions, normals (12 B each), atoms, components
+    // (4 B), patches (1 B) per vertex, then the triangles.
+    unsigned char* h_pos = H;
+    unsigned char* h_nrm = h_pos + nv * 12;
+    unsigned char* h_atom = h_nrm + nv * 12;
+    unsigned char* h_comp = h_atom + nv * 4;
+    unsigned char* h_patch = h_comp + nv * 4;
+    unsigned char* h_tris = h_patch + nv;
+    auto d2h = [&](void* dst, const void* src, size_t bytes) {
+        return !bytes || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    };
+    // The vertex arrays go back while the measure runs (same stream: after
+    // the assembly, before the measure's own copies).
+    if (!d2h(h_pos, in.pos, nv * 12) || !d2h(h_nrm, in.nrm, nv * 12) || !d2h(h_atom, in.atoms, nv * 4) ||
+        !d2h(h_patch, in.patches, nv)) {
+        if (msg) *msg = "vertex copy";
+        return 1;
+    }
+    if (!measure_core(d, in.pos, in.nrm, S.tris.as<uint32_t>(), nv, nt, comps, bad, S, msg,
+                      reinterpret_cast<uint32_t*>(h_comp), reinterpret_cast<uint32_t*>(h_tris)))
+        return 1;
+    if (*bad) return 0;
+    // Staging to the mesh arrays, in parallel.
+    auto t1 = std::chrono::steady_clock::now();
+    m.positions.resize(nv);
+    m.normals.resize(nv);
+    m.vertex_atom.resize(nv);
+    m.vertex_component.resize(nv);
+    m.vertex_patch.resize(nv);
+    m.triangles.resize(nt);
+    struct Part {
+        void* dst;
+        const void* src;
+        size_t bytes;
+    };
+    const Part parts[6] = {{m.positions.data(), h_pos, nv * 12},     {m.normals.data(), h_nrm, nv * 12},
+                           {m.vertex_atom.data(), h_atom, nv * 4},   {m.vertex_component.data(), h_comp, nv * 4},
+                           {m.vertex_patch.data(), h_patch, nv},     {m.triangles.data(), h_tris, nt * 12}};
+    constexpr size_t PIECE = size_t(4) << 20;
+    std::vector<std::pair<int, size_t>> pieces;
+    for (int k = 0; k < 6; k++)
+        for (size_t o = 0; o < parts[k].bytes; o += PIECE) pieces.push_back({k, o});
+    smbh::parallel_for(pieces.size(), [&](size_t i, int) {
+        const Part& P = parts[pieces[i].first];
+        const size_t o = pieces[i].second, n = std::min(PIECE, P.bytes - o);
+        std::memcpy(static_cast<unsigned char*>(P.dst) + o, static_cast<const unsigned char*>(P.src) + o, n);
+    });
+    if (ms_copy) *ms_copy = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    return 0;
 }
 
 }  // namespace smb

@@ -12,10 +12,38 @@ namespace smb {
 // Device buffers of the measure, kept between meshes.
 struct MeasureScratch {
     DBuf pos, nrm, tris, tris_out, keys, cnt, dup, parent, flag, cid, id, counters, comp_v, comp_t, comp_e, area,
-        volume, parts, pkey, pidx, pkey2, pidx2, first, tkey, tidx, tkey2, tidx2, tiles, cub;
+        volume, parts, pkey, pidx, pkey2, pidx2, first, tkey, tidx, tkey2, tidx2, tiles, cub, packed, err;
+    void* host = nullptr;  // page-locked staging of the results
+    size_t host_cap = 0;
+    void* staging(size_t bytes);  // null when page-locked memory cannot be had
     void release();
     ~MeasureScratch() { release(); }
 };
+
+// A mesh stage's results on the device: brick keys (packed-key order),
+// marching-cubes edge lists and triangle references, and one vertex per
+// edge (position, normal, input atom, patch).
+struct DeviceMesh {
+    const int4* keys;
+    size_t n_bricks;
+    const uint32_t *edge_off, *edges, *tri_off, *tri_refs;
+    size_t n_edges, n_tris;
+    const float *pos, *nrm;
+    const uint32_t* atoms;
+    const uint8_t* patches;
+};
+
+// Assembly (extract::assemble, mesh/extract.rs:606-691), validation,
+// components, area/volume and grouping of a mesh whose vertices are on the
+// device, then the finished mesh into m through page-locked staging: the
+// host's assemble, defects and components_and_group results bit for bit.
+// *ms_assemble and *ms_copy get the assembly's time and the time of the
+// copies from the staging into m.
+// 0: done (*bad defects; m and comps filled when there are none); 1: the
+// device could not (*msg; the caller finishes on the host); 2: the
+// assembly failed (*msg is the host assembly's error text).
+int finish_on_device(smb_device* d, const DeviceMesh& in, smbh::Mesh& m, std::vector<smbh::Component>& comps,
+                     size_t* bad, MeasureScratch& S, std::string* msg, double* ms_assemble, double* ms_copy);
 
 // The mesh's defects (*bad); when there are none, its components (area,
 // volume, Euler characteristic, first triangle), m.vertex_component and

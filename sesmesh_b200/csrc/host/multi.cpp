@@ -84,9 +84,9 @@ struct Pinned {
     size_t cap = 0;
     bool reserve(size_t bytes) {
         if (bytes <= cap) return true;
-        if (p) cudaFreeHost(p), p = nullptr, cap = 0;
+        smb::pinned_free(p), p = nullptr, cap = 0;
         size_t want = bytes + bytes / 4 + 4096;
-        if (cudaHostAlloc(&p, want, cudaHostAllocDefault) != cudaSuccess) return p = nullptr, false;
+        if (!(p = smb::pinned_alloc(want))) return false;
         cap = want;
         return true;
     }
@@ -94,9 +94,7 @@ struct Pinned {
     T* as() const {
         return static_cast<T*>(p);
     }
-    ~Pinned() {
-        if (p) cudaFreeHost(p);
-    }
+    ~Pinned() { smb::pinned_free(p); }
 };
 
 // One group's results on the host.

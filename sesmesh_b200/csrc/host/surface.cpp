@@ -269,6 +269,57 @@ static int fetch_mc(smb_engine* e, char* err, size_t errlen) {
     return SMB_OK;
 }
 
+// Exact mode with every vertex refined on the device: assembly, validation,
+// measure and grouping there too, and the finished mesh back once.
+// SMB_OK, or an error code; *fallback when the device could not and the
+// host stages should run instead.
+static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long evals, bool* fallback,
+                               double* ms_d2h, char* err, size_t errlen) {
+    *fallback = false;
+    const smb_batch* b = e->batch;
+    smb::DeviceMesh in{};
+    in.keys = e->res->keys + b->first;
+    in.n_bricks = b->n;
+    in.edge_off = b->edge_off.as<uint32_t>();
+    in.edges = b->edges.as<uint32_t>();
+    in.tri_off = b->tri_off.as<uint32_t>();
+    in.tri_refs = b->tris.as<uint32_t>();
+    in.n_edges = b->n_edges;
+    in.n_tris = b->n_tris;
+    in.pos = b->x_pos.as<float>();
+    in.nrm = b->x_nrm.as<float>();
+    in.atoms = b->x_atom.as<uint32_t>();
+    in.patches = b->x_patch.as<uint8_t>();
+    auto t0 = clk::now();
+    size_t bad = 0;
+    std::string msg;
+    double ms_asm = 0, ms_copy = 0;
+    int r = smb::finish_on_device(e->dev, in, s.mesh, s.comps, &bad, e->measure, &msg, &ms_asm, &ms_copy);
+    if (r == 1) {
+        *fallback = true;
+        return SMB_OK;
+    }
+    if (r == 2) return set_err(err, errlen, "%s", msg.c_str()), SMB_ERR_STATE;
+    if (bad) return set_err(err, errlen, "mesh failed validation (%zu defects)", bad), SMB_ERR_STATE;
+    const MeshParams& mp = e->mp;
+    smb_surface_stats& st = s.stats;
+    st.spheres = e->arr.n;
+    st.surface_bricks = b->n;
+    st.samples = size_t(b->n) * size_t(mp.b + 1) * size_t(mp.b + 1) * size_t(mp.b + 1);
+    st.vertices = s.mesh.positions.size();
+    st.triangles = s.mesh.triangles.size();
+    st.components = s.comps.size();
+    for (auto& c : s.comps) st.area += c.area, st.volume += c.volume, st.euler += c.euler;
+    st.refine_evaluations = evals;
+    st.refine_cpu_edges = 0;
+    st.t_host_refine = 0;
+    st.t_assemble = ms_asm;
+    st.t_measure = ms_since(t0) - ms_asm - ms_copy;
+    st.host_threads = threads();
+    *ms_d2h = ms_copy;
+    return SMB_OK;
+}
+
 // Whole mesh stage and the stages after it: device part, results to the
 // host, f64 refinement (exact) or placement (fast), assembly, validation,
 // components and grouping.
@@ -278,6 +329,35 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
     auto t_all = clk::now();
     int rc = smb_engine_run_device(e, nullptr, err, errlen);
     if (rc != SMB_OK) return rc;
+    auto fill_times = [&](smb_surface_stats& st, double t_d2h) {
+        st.touched_bricks = e->touched;
+        st.t_geometry = e->t_geometry;
+        st.t_upload = e->t_upload;
+        st.t_classify = e->t_classify;
+        st.t_substates = e->times.substates;
+        st.t_gather = e->times.gather;
+        st.t_sample = e->times.sample;
+        st.t_mc = e->times.mc;
+        st.t_device = e->t_classify + e->times.total;
+        st.t_d2h = t_d2h;
+        st.t_mesh_stage = ms_since(t_all) - st.t_assemble - st.t_measure;
+    };
+    if (e->params.refine != SMB_REFINE_FAST && e->exact_device && e->res->n_bricks) {
+        unsigned long long evals = 0, host_edges = 0;
+        if ((rc = smb_batch_exact_summary(e->batch, &evals, &host_edges)) != SMB_OK)
+            return set_err(err, errlen, "exact refinement summary failed"), rc;
+        if (host_edges == 0) {
+            auto s = std::make_unique<smb_surface>();
+            bool fallback = false;
+            double ms_d2h = 0;
+            if ((rc = finish_exact_device(e, *s, evals, &fallback, &ms_d2h, err, errlen)) != SMB_OK) return rc;
+            if (!fallback) {
+                fill_times(s->stats, ms_d2h);
+                *out = s.release();
+                return SMB_OK;
+            }
+        }
+    }
     auto t0 = clk::now();
     if ((rc = fetch_mc(e, err, errlen)) != SMB_OK) return rc;
     size_t nb = e->res->n_bricks, ne = e->edges.size();
@@ -304,18 +384,7 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
                                    e->dev, &e->measure, exact_dev && ne ? &e->exact_out : nullptr,
                                    exact_dev && ne ? e->exact_evals.data() : nullptr);
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_STATE;
-    smb_surface_stats& st = s->stats;
-    st.touched_bricks = e->touched;
-    st.t_geometry = e->t_geometry;
-    st.t_upload = e->t_upload;
-    st.t_classify = e->t_classify;
-    st.t_substates = e->times.substates;
-    st.t_gather = e->times.gather;
-    st.t_sample = e->times.sample;
-    st.t_mc = e->times.mc;
-    st.t_device = e->t_classify + e->times.total;
-    st.t_d2h = t_d2h;
-    st.t_mesh_stage = ms_since(t_all) - st.t_assemble - st.t_measure;
+    fill_times(s->stats, t_d2h);
     *out = s.release();
     return SMB_OK;
 }
@@ -411,6 +480,19 @@ int smb_surface_mesh(const smb_surface* s, float* pos, float* nrm, uint32_t* tri
     if (patches && !m.vertex_patch.empty()) std::memcpy(patches, m.vertex_patch.data(), m.vertex_patch.size());
     if (components && !m.vertex_component.empty())
         std::memcpy(components, m.vertex_component.data(), m.vertex_component.size() * 4);
+    return SMB_OK;
+}
+
+int smb_surface_arrays(const smb_surface* s, const float** pos, const float** nrm, const uint32_t** tris,
+                       const uint32_t** atoms, const uint8_t** patches, const uint32_t** components) {
+    if (!s) return SMB_ERR_ARG;
+    const Mesh& m = s->mesh;
+    if (pos) *pos = m.positions.empty() ? nullptr : m.positions.data()->data();
+    if (nrm) *nrm = m.normals.empty() ? nullptr : m.normals.data()->data();
+    if (tris) *tris = m.triangles.empty() ? nullptr : m.triangles.data()->data();
+    if (atoms) *atoms = m.vertex_atom.empty() ? nullptr : m.vertex_atom.data();
+    if (patches) *patches = m.vertex_patch.empty() ? nullptr : m.vertex_patch.data();
+    if (components) *components = m.vertex_component.empty() ? nullptr : m.vertex_component.data();
     return SMB_OK;
 }
 

@@ -11,7 +11,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/sesmesh_b200.h"
@@ -68,10 +71,187 @@ void selftest_ref(float x, float y, uint32_t out[12]) {
 
 namespace smb {
 
+// Device memory cache.  Blocks a library object frees stay with the process
+// and are handed to the next allocation of a similar size on the same
+// device, so engines made one after another (compute_surface calls) do not
+// pay cudaMalloc / cudaFree for their multi-GB buffers each time.  A free
+// synchronizes the device first, as cudaFree does, so no queued kernel
+// still uses a block when it is handed out again.  An allocation that fails
+// releases the device's cached blocks and retries; the cache is released
+// when the last handle of a device closes.
+namespace {
+constexpr int MAX_DEVICES = 64;
+struct MemCache {
+    std::mutex m;
+    std::multimap<size_t, void*> free_blocks[MAX_DEVICES];
+    std::unordered_map<void*, std::pair<int, size_t>> live;  // block -> (device, bytes)
+    int open[MAX_DEVICES] = {};
+};
+MemCache& mem_cache() {
+    static MemCache* c = new MemCache();  // kept to process exit: frees may run in static destructors
+    return *c;
+}
+}  // namespace
+
+void mem_trim(int dev) {
+    if (dev < 0 || dev >= MAX_DEVICES) return;
+    MemCache& C = mem_cache();
+    std::vector<void*> blocks;
+    {
+        std::lock_guard<std::mutex> g(C.m);
+        for (auto& kv : C.free_blocks[dev]) blocks.push_back(kv.second);
+        C.free_blocks[dev].clear();
+    }
+    if (blocks.empty()) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(dev);
+    for (void* b : blocks) cudaFree(b);
+    cudaSetDevice(cur);
+}
+
+cudaError_t mem_alloc(void** p, size_t bytes) {
+    *p = nullptr;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    MemCache& C = mem_cache();
+    if (dev >= 0 && dev < MAX_DEVICES) {
+        std::lock_guard<std::mutex> g(C.m);
+        auto& fb = C.free_blocks[dev];
+        auto it = fb.lower_bound(bytes);
+        if (it != fb.end() && it->first <= 2 * bytes + (size_t(1) << 20)) {
+            *p = it->second;
+            C.live[*p] = {dev, it->first};
+            fb.erase(it);
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        mem_trim(dev);
+        e = cudaMalloc(p, bytes);
+    }
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return e;
+    }
+    std::lock_guard<std::mutex> g(C.m);
+    C.live[*p] = {dev, bytes};
+    return cudaSuccess;
+}
+
+void mem_free(void* p) {
+    if (!p) return;
+    MemCache& C = mem_cache();
+    std::pair<int, size_t> info{-1, 0};
+    {
+        std::lock_guard<std::mutex> g(C.m);
+        auto it = C.live.find(p);
+        if (it != C.live.end()) info = it->second, C.live.erase(it);
+    }
+    if (info.first < 0 || info.first >= MAX_DEVICES) {
+        cudaFree(p);
+        return;
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != info.first) cudaSetDevice(info.first);
+    cudaDeviceSynchronize();
+    if (cur != info.first) cudaSetDevice(cur);
+    std::lock_guard<std::mutex> g(C.m);
+    C.free_blocks[info.first].emplace(info.second, p);
+}
+
+// Page-locked host memory through a cache of the same kind (no device
+// synchronization needed: callers free staging only after their copies
+// completed).  Released when the last device handle closes.
+namespace {
+struct HostCache {
+    std::mutex m;
+    std::multimap<size_t, void*> free_blocks;
+    std::unordered_map<void*, size_t> live;
+};
+HostCache& host_cache() {
+    static HostCache* c = new HostCache();
+    return *c;
+}
+void host_trim() {
+    std::vector<void*> blocks;
+    {
+        std::lock_guard<std::mutex> g(host_cache().m);
+        for (auto& kv : host_cache().free_blocks) blocks.push_back(kv.second);
+        host_cache().free_blocks.clear();
+    }
+    for (void* b : blocks) cudaFreeHost(b);
+}
+}  // namespace
+
+void* pinned_alloc(size_t bytes) {
+    HostCache& C = host_cache();
+    {
+        std::lock_guard<std::mutex> g(C.m);
+        auto it = C.free_blocks.lower_bound(bytes);
+        if (it != C.free_blocks.end() && it->first <= 2 * bytes + (size_t(1) << 20)) {
+            void* p = it->second;
+            C.live[p] = it->first;
+            C.free_blocks.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        host_trim();
+        if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+    }
+    std::lock_guard<std::mutex> g(C.m);
+    C.live[p] = bytes;
+    return p;
+}
+
+void pinned_free(void* p) {
+    if (!p) return;
+    HostCache& C = host_cache();
+    std::lock_guard<std::mutex> g(C.m);
+    auto it = C.live.find(p);
+    if (it == C.live.end()) {
+        cudaFreeHost(p);
+        return;
+    }
+    C.free_blocks.emplace(it->second, p);
+    C.live.erase(it);
+}
+
+void mem_device_open(int dev) {
+    if (dev < 0 || dev >= MAX_DEVICES) return;
+    std::lock_guard<std::mutex> g(mem_cache().m);
+    mem_cache().open[dev]++;
+}
+
+void mem_device_close(int dev) {
+    if (dev < 0 || dev >= MAX_DEVICES) return;
+    bool last;
+    {
+        std::lock_guard<std::mutex> g(mem_cache().m);
+        last = --mem_cache().open[dev] <= 0;
+    }
+    if (last) mem_trim(dev);
+    bool none = true;
+    {
+        std::lock_guard<std::mutex> g(mem_cache().m);
+        for (int k = 0; k < MAX_DEVICES; k++) none &= mem_cache().open[k] <= 0;
+    }
+    if (none) host_trim();
+}
+
 int dev_alloc(void** p, size_t bytes, std::vector<void*>* owned, size_t* total, char* err, size_t errlen) {
     *p = nullptr;
     if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = mem_alloc(p, bytes);
     if (e != cudaSuccess) {
         set_err(err, errlen, "cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
         *p = nullptr;
@@ -85,11 +265,11 @@ int dev_alloc(void** p, size_t bytes, std::vector<void*>* owned, size_t* total, 
 // Grows a batch buffer to at least `bytes` (contents discarded).
 int DBuf::reserve(size_t bytes, char* err, size_t errlen) {
     if (bytes <= cap) return SMB_OK;
-    if (p) cudaFree(p);
+    if (p) mem_free(p);
     p = nullptr;
     cap = 0;
     size_t want = bytes + bytes / 4 + 256;
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = mem_alloc(&p, want);
     if (e != cudaSuccess) {
         set_err(err, errlen, "cudaMalloc(%zu bytes) failed: %s", want, cudaGetErrorString(e));
         p = nullptr;
@@ -100,7 +280,7 @@ int DBuf::reserve(size_t bytes, char* err, size_t errlen) {
 }
 
 void DBuf::release() {
-    if (p) cudaFree(p);
+    if (p) mem_free(p);
     p = nullptr;
     cap = 0;
 }
@@ -109,6 +289,7 @@ static void destroy_device(smb_device* d) {
     if (d->gone.exchange(true)) return;
     cudaSetDevice(d->index);
     if (d->stream) cudaStreamDestroy(d->stream);
+    mem_device_close(d->index);
     delete d;
 }
 
@@ -154,6 +335,7 @@ int smb_open(int index, smb_device** out, char* err, size_t errlen) {
         set_err(err, errlen, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
         return SMB_ERR_CUDA;
     }
+    mem_device_open(index);
     int rc = smb_self_test(d, 4096, err, errlen);
     if (rc != SMB_OK) {
         smb_close(d);
@@ -360,8 +542,8 @@ static void destroy_resident(smb_resident* r) {
     smb_device* d = r->dev;
     cudaSetDevice(d->index);
     cudaStreamSynchronize(d->stream);
-    for (void* p : r->owned) cudaFree(p);
-    if (r->keys) cudaFree(r->keys);
+    for (void* p : r->owned) mem_free(p);
+    if (r->keys) mem_free(r->keys);
     delete r;
     dev_release(d);
 }
@@ -380,7 +562,7 @@ int smb_classify(smb_resident* r, size_t* touched, size_t* surface, char* err, s
     CK(cudaSetDevice(d->index));
     cudaStream_t s = d->stream;
     const DLat& L = r->L;
-    if (r->keys) cudaFree(r->keys);
+    if (r->keys) mem_free(r->keys);
     r->keys = nullptr;
     r->n_bricks = 0;
     r->classified = false;
@@ -444,7 +626,7 @@ int smb_classify(smb_resident* r, size_t* touched, size_t* surface, char* err, s
     unsigned long long n_surface = 0;
     cudaMemcpyAsync(&n_surface, tot.p, 8, cudaMemcpyDeviceToHost, s);
     e = cudaStreamSynchronize(s);
-    if (e == cudaSuccess && n_surface) e = cudaMalloc(&r->keys, n_surface * sizeof(int4));
+    if (e == cudaSuccess && n_surface) e = mem_alloc(reinterpret_cast<void**>(&r->keys), n_surface * sizeof(int4));
     if (e == cudaSuccess) launch_cells_to_keys(box, cells.as<uint32_t>(), uint32_t(n_surface), r->keys, s);
     cudaEventRecord(e1, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -810,7 +992,7 @@ int smb_refine_exact(smb_resident* r, smb_batch* b, double* ms, char* err, size_
     if ((rc = b->x_pos.reserve(ne * 12, err, errlen)) || (rc = b->x_nrm.reserve(ne * 12, err, errlen)) ||
         (rc = b->x_atom.reserve(ne * 4, err, errlen)) || (rc = b->x_patch.reserve(ne, err, errlen)) ||
         (rc = b->e_t.reserve(ne * 4, err, errlen)) || (rc = b->e_evals.reserve(ne * 4, err, errlen)) ||
-        (rc = b->x_ovf.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
+        (rc = b->x_ovf.reserve(size_t(nw) * 4 + 4, err, errlen)) || (rc = b->x_sum.reserve(16, err, errlen)) ||
         (rc = b->item_counts.reserve(size_t(nw) * 4, err, errlen)) ||
         (rc = b->item_off.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
         (rc = b->item_edges.reserve(ne * 4, err, errlen)) ||
@@ -865,6 +1047,24 @@ int smb_batch_vertices(const smb_batch* b, float* positions, float* normals, uin
     if (evals) ok &= cudaMemcpyAsync(evals, b->e_evals.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
     ok &= cudaStreamSynchronize(s) == cudaSuccess;
     return ok ? SMB_OK : SMB_ERR_CUDA;
+}
+
+int smb_batch_exact_summary(const smb_batch* b, unsigned long long* evaluations, unsigned long long* host_edges) {
+    if (!b || !b->refined_exact) return SMB_ERR_STATE;
+    smb_device* d = b->res->dev;
+    if (cudaSetDevice(d->index) != cudaSuccess) return SMB_ERR_CUDA;
+    unsigned long long out[2] = {0, 0};
+    if (b->n_edges) {
+        unsigned long long* sum = b->x_sum.as<unsigned long long>();
+        if (!sum || launch_exact_summary(b->e_evals.as<uint32_t>(), b->n_edges, sum, d->info.multiprocessors,
+                                         d->stream) != cudaSuccess ||
+            cudaMemcpyAsync(out, sum, 16, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess ||
+            cudaStreamSynchronize(d->stream) != cudaSuccess)
+            return SMB_ERR_CUDA;
+    }
+    if (evaluations) *evaluations = out[0];
+    if (host_edges) *host_edges = out[1];
+    return SMB_OK;
 }
 
 int smb_batch_set_exact_region(smb_batch* b, size_t bytes) {

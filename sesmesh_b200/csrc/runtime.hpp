@@ -24,6 +24,18 @@ struct DBuf {
 
 int dev_alloc(void** p, size_t bytes, std::vector<void*>* owned, size_t* total, char* err, size_t errlen);
 
+// Device memory through the process-wide cache (runtime.cu): mem_free
+// synchronizes the device and keeps the block for the next mem_alloc of a
+// similar size on that device; mem_trim returns a device's cached blocks.
+cudaError_t mem_alloc(void** p, size_t bytes);
+void mem_free(void* p);
+void mem_trim(int device);
+void mem_device_open(int device);
+// Page-locked host memory through a process-wide cache (null on failure).
+void* pinned_alloc(size_t bytes);
+void pinned_free(void* p);
+void mem_device_close(int device);
+
 // Handle lifetimes: a device stays open while residents or MLPs made on it
 // live, a resident while batches made on it live, whatever order the caller
 // frees them in (a garbage-collected host may finalize them in any order).
@@ -78,7 +90,7 @@ struct smb_batch {
     smb::DBuf e_t, e_feat, e_q, e_evals;  // fast-mode refinement results
     smb::DBuf e_x;                        // warm-start features (32 f32 per edge)
     smb::DBuf item_counts, item_off, item_edges;  // per sampled sub-block edge lists
-    smb::DBuf x_pos, x_nrm, x_atom, x_patch, x_ovf;  // exact mode on the device: vertices, overflowed items
+    smb::DBuf x_pos, x_nrm, x_atom, x_patch, x_ovf, x_sum;  // exact mode on the device: vertices, overflowed items, summary
     bool refined_exact = false;
     size_t x_block_items = 0;  // items of the last exact pass refined by a whole block
     size_t x_region = 18432;  // shared-memory bytes per warp for one sub-block's f64 candidate lists
@@ -89,6 +101,6 @@ struct smb_batch {
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
                 &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &item_counts, &item_off, &item_edges,
-                &x_pos, &x_nrm, &x_atom, &x_patch, &x_ovf};
+                &x_pos, &x_nrm, &x_atom, &x_patch, &x_ovf, &x_sum};
     }
 };

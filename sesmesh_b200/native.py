@@ -135,6 +135,7 @@ SIGNATURES = {
     "smb_refine_exact": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
     "smb_batch_vertices": (C.c_int, [_vp, _fp, _fp, _u32p, C.POINTER(C.c_uint8), _fp, _u32p]),
     "smb_batch_set_exact_region": (C.c_int, [_vp, _sz]),
+    "smb_batch_exact_summary": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong)]),
     "smb_kernel_launches": (C.c_ulonglong, []),
     "smb_batch_info_get": (C.c_int, [_vp, C.POINTER(BatchInfo)]),
     "smb_batch_count_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _cp, _sz]),
@@ -162,6 +163,7 @@ SIGNATURES = {
     "smb_engine_field": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(C.c_double)]),
     "smb_engine_warm_start_rows": (C.c_int, [_vp, _fp, _fp, _sz, C.POINTER(_sz), _cp, _sz]),
     "smb_surface_free": (None, [_vp]),
+    "smb_surface_arrays": (C.c_int, [_vp] + [C.POINTER(_vp)] * 6),
     "smb_surface_stats_get": (C.c_int, [_vp, C.POINTER(SurfaceStats_)]),
     "smb_surface_mesh": (C.c_int, [_vp, _fp, _fp, _u32p, _u32p, C.POINTER(C.c_uint8), _u32p]),
     "smb_surface_obj": (_sz, [_vp, _cp, _sz]),

@@ -62,26 +62,72 @@ class SurfaceParams:
         return p
 
 
+class _SurfaceHandle:
+    """Owns one smb_surface; freed when the output and every array view of
+    it are gone."""
+
+    def __init__(self, h, owned):
+        self.h = h
+        self.owned = owned
+
+    def __del__(self):
+        if self.owned and self.h:
+            lib().smb_surface_free(self.h)
+            self.h = None
+
+
 class SurfaceOutput:
-    """Mesh, statistics (SurfaceStats + stage times in ms) and OBJ text."""
+    """Mesh, statistics (SurfaceStats + stage times in ms) and OBJ text.
+    The mesh arrays are read-only views of the library's mesh (no copy) for
+    outputs this object owns, copies otherwise."""
+
+    _ARRAYS = (("positions", C.c_float, np.float32, 3), ("normals", C.c_float, np.float32, 3),
+               ("triangles", C.c_uint32, np.uint32, 3), ("vertex_atom", C.c_uint32, np.uint32, 0),
+               ("vertex_patch", C.c_uint8, np.uint8, 0), ("vertex_component", C.c_uint32, np.uint32, 0))
 
     def __init__(self, h, owned=True):
+        self._keep = _SurfaceHandle(h, owned)
         self._h = h
         self._owned = owned
         st = native.SurfaceStats_()
         lib().smb_surface_stats_get(h, C.byref(st))
         self.stats = {name: getattr(st, name) for name, _ in st._fields_}
-        nv, nt = st.vertices, st.triangles
-        self.positions = np.zeros((nv, 3), np.float32)
-        self.normals = np.zeros((nv, 3), np.float32)
-        self.triangles = np.zeros((nt, 3), np.uint32)
-        self.vertex_atom = np.zeros(nv, np.uint32)
-        self.vertex_patch = np.zeros(nv, np.uint8)
-        self.vertex_component = np.zeros(nv, np.uint32)
-        if nv:
-            lib().smb_surface_mesh(h, _p(self.positions, C.c_float), _p(self.normals, C.c_float),
-                                   _p(self.triangles, C.c_uint32), _p(self.vertex_atom, C.c_uint32),
-                                   _p(self.vertex_patch, C.c_uint8), _p(self.vertex_component, C.c_uint32))
+        self._arrays = None
+        if not owned:
+            self._arrays = {k: v.copy() for k, v in self._views().items()}
+
+    def _views(self):
+        nv, nt = self.stats["vertices"], self.stats["triangles"]
+        ptrs = [C.c_void_p() for _ in self._ARRAYS]
+        lib().smb_surface_arrays(self._h, *[C.byref(q) for q in ptrs])
+        out = {}
+        for (name, ct, dt, width), q in zip(self._ARRAYS, ptrs):
+            rows = nt if name == "triangles" else nv
+            shape = (rows, width) if width else (rows,)
+            n = rows * max(width, 1)
+            if not n or not q.value:
+                out[name] = np.zeros(shape, dt)
+                continue
+            buf = (ct * n).from_address(q.value)
+            buf.keeper = self._keep  # the mesh lives while any view does
+            a = np.frombuffer(buf, dtype=dt).reshape(shape)
+            a.flags.writeable = False
+            out[name] = a
+        return out
+
+    def _array(self, name):
+        if self._arrays is None:
+            if self._h is None:
+                raise ValueError("surface closed")
+            self._arrays = self._views()
+        return self._arrays[name]
+
+    positions = property(lambda self: self._array("positions"))
+    normals = property(lambda self: self._array("normals"))
+    triangles = property(lambda self: self._array("triangles"))
+    vertex_atom = property(lambda self: self._array("vertex_atom"))
+    vertex_patch = property(lambda self: self._array("vertex_patch"))
+    vertex_component = property(lambda self: self._array("vertex_component"))
 
     def obj(self):
         """OBJ bytes with the default options (export/obj.rs:37-73)."""
@@ -95,10 +141,9 @@ class SurfaceOutput:
         _check(lib().smb_surface_write_obj(self._h, path.encode(), err, 512), err)
 
     def close(self):
-        if getattr(self, "_h", None):
-            if getattr(self, "_owned", True):
-                lib().smb_surface_free(self._h)
-            self._h = None
+        """Drops this object's hold on the mesh (views already taken keep it)."""
+        self._h = None
+        self._keep = None
 
     def __del__(self):
         self.close()
