@@ -633,8 +633,10 @@ void* MeasureScratch::staging(size_t bytes) {
     return host;
 }
 
-int finish_on_device(smb_device* d, const DeviceMesh& in, smbh::Mesh& m, std::vector<smbh::Component>& comps,
-                     size_t* bad, MeasureScratch& S, std::string* msg, double* ms_assemble, double* ms_copy) {
+int finish_on_device(smb_device* d, const DeviceMesh& in, smbh::MeshRef* out, void** block,
+                     std::vector<smbh::Component>& comps, size_t* bad, MeasureScratch& S, std::string* msg,
+                     double* ms_assemble) {
+    *block = nullptr;
     cudaStream_t s = d->stream;
     const size_t nv = in.n_edges, nt = in.n_tris;
     if (nv >= (size_t(1) << 31) || nt >= (size_t(1) << 31) || in.n_bricks == 0) {
@@ -700,32 +702,16 @@ int finish_on_device(smb_device* d, const DeviceMesh& in, smbh::Mesh& m, std::ve
                       reinterpret_cast<uint32_t*>(h_comp), reinterpret_cast<uint32_t*>(h_tris)))
         return 1;
     if (*bad) return 0;
-    // Staging to the mesh arrays, in parallel.
-    auto t1 = std::chrono::steady_clock::now();
-    m.positions.resize(nv);
-    m.normals.resize(nv);
-    m.vertex_atom.resize(nv);
-    m.vertex_component.resize(nv);
-    m.vertex_patch.resize(nv);
-    m.triangles.resize(nt);
-    struct Part {
-        void* dst;
-        const void* src;
-        size_t bytes;
-    };
-    const Part parts[6] = {{m.positions.data(), h_pos, nv * 12},     {m.normals.data(), h_nrm, nv * 12},
-                           {m.vertex_atom.data(), h_atom, nv * 4},   {m.vertex_component.data(), h_comp, nv * 4},
-                           {m.vertex_patch.data(), h_patch, nv},     {m.triangles.data(), h_tris, nt * 12}};
-    constexpr size_t PIECE = size_t(4) << 20;
-    std::vector<std::pair<int, size_t>> pieces;
-    for (int k = 0; k < 6; k++)
-        for (size_t o = 0; o < parts[k].bytes; o += PIECE) pieces.push_back({k, o});
-    smbh::parallel_for(pieces.size(), [&](size_t i, int) {
-        const Part& P = parts[pieces[i].first];
-        const size_t o = pieces[i].second, n = std::min(PIECE, P.bytes - o);
-        std::memcpy(static_cast<unsigned char*>(P.dst) + o, static_cast<const unsigned char*>(P.src) + o, n);
-    });
-    if (ms_copy) *ms_copy = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
+    // The staging block becomes the mesh's storage.
+    out->pos = reinterpret_cast<const float*>(h_pos);
+    out->nrm = reinterpret_cast<const float*>(h_nrm);
+    out->atom = reinterpret_cast<const uint32_t*>(h_atom);
+    out->comp = reinterpret_cast<const uint32_t*>(h_comp);
+    out->patch = reinterpret_cast<const uint8_t*>(h_patch);
+    out->tris = reinterpret_cast<const uint32_t*>(h_tris);
+    out->nv = nv, out->nt = nt;
+    *block = S.host;
+    S.host = nullptr, S.host_cap = 0;
     return 0;
 }
 

@@ -35,15 +35,17 @@ struct DeviceMesh {
 
 // Assembly (extract::assemble, mesh/extract.rs:606-691), validation,
 // components, area/volume and grouping of a mesh whose vertices are on the
-// device, then the finished mesh into m through page-locked staging: the
+// device, then the finished mesh back into one page-locked block: the
 // host's assemble, defects and components_and_group results bit for bit.
-// *ms_assemble and *ms_copy get the assembly's time and the time of the
-// copies from the staging into m.
-// 0: done (*bad defects; m and comps filled when there are none); 1: the
+// On success with no defects *block is that block (the caller releases it
+// with pinned_free) and *out points into it.  *ms_assemble gets the
+// assembly's time.
+// 0: done (*bad defects; *out, *block and comps filled when there are none); 1: the
 // device could not (*msg; the caller finishes on the host); 2: the
 // assembly failed (*msg is the host assembly's error text).
-int finish_on_device(smb_device* d, const DeviceMesh& in, smbh::Mesh& m, std::vector<smbh::Component>& comps,
-                     size_t* bad, MeasureScratch& S, std::string* msg, double* ms_assemble, double* ms_copy);
+int finish_on_device(smb_device* d, const DeviceMesh& in, smbh::MeshRef* out, void** block,
+                     std::vector<smbh::Component>& comps, size_t* bad, MeasureScratch& S, std::string* msg,
+                     double* ms_assemble);
 
 // The mesh's defects (*bad); when there are none, its components (area,
 // volume, Euler characteristic, first triangle), m.vertex_component and

@@ -7,6 +7,7 @@
 #include "../../../include/sesmesh_b200.h"
 #include "../../../include/sesmesh_b200_surface.h"
 #include "../device/measure.hpp"
+#include "../runtime.hpp"
 #include "geom.hpp"
 #include "mesher.hpp"
 
@@ -47,6 +48,15 @@ struct smb_surface {
     std::vector<Component> comps;
     smb_surface_stats stats{};
     std::string obj;
+    // A mesh finished on the device stays in the page-locked block its
+    // results came back in (view points into it); else view is of mesh.
+    void* block = nullptr;
+    smbh::MeshRef view;
+    smbh::MeshRef ref() const { return block ? view : smbh::MeshRef::of(mesh); }
+    smb_surface() = default;
+    smb_surface(const smb_surface&) = delete;
+    smb_surface& operator=(const smb_surface&) = delete;
+    ~smb_surface() { smb::pinned_free(block); }
 };
 
 

@@ -698,28 +698,28 @@ void push_fixed(std::string& buf, float x, int prec) {
 }
 
 // export/obj.rs:144-236, default options: header, object "ses", v, vn, f a//a.
-std::string obj_text(const Mesh& m, int precision, bool normals) {
-    normals = normals && !m.normals.empty();
-    const size_t nv = m.positions.size(), nt = m.triangles.size();
+std::string obj_text(const MeshRef& m, int precision, bool normals) {
+    normals = normals && m.nrm;
+    const size_t nv = m.nv, nt = m.nt;
     const size_t CH = 1 << 15;
-    auto vec_lines = [&](const std::vector<std::array<float, 3>>& data, const char* tag, std::vector<std::string>& out) {
-        out.assign((data.size() + CH - 1) / CH, std::string());
+    auto vec_lines = [&](const float* data, const char* tag, std::vector<std::string>& out) {
+        out.assign((nv + CH - 1) / CH, std::string());
         parallel_for(out.size(), [&](size_t c, int) {
             std::string& s = out[c];
             s.reserve(CH * 32);
-            for (size_t i = c * CH; i < std::min(data.size(), (c + 1) * CH); i++) {
+            for (size_t i = c * CH; i < std::min(nv, (c + 1) * CH); i++) {
                 s += tag;
                 for (int k = 0; k < 3; k++) {
                     if (k) s.push_back(' ');
-                    push_fixed(s, data[i][k], precision);
+                    push_fixed(s, data[3 * i + k], precision);
                 }
                 s.push_back('\n');
             }
         });
     };
     std::vector<std::string> v, vn, f;
-    vec_lines(m.positions, "v ", v);
-    if (normals) vec_lines(m.normals, "vn ", vn);
+    vec_lines(m.pos, "v ", v);
+    if (normals) vec_lines(m.nrm, "vn ", vn);
     f.assign((nt + CH - 1) / CH, std::string());
     parallel_for(f.size(), [&](size_t c, int) {
         std::string& s = f[c];
@@ -728,7 +728,7 @@ std::string obj_text(const Mesh& m, int precision, bool normals) {
         for (size_t t = c * CH; t < std::min(nt, (c + 1) * CH); t++) {
             s.push_back('f');
             for (int k = 0; k < 3; k++) {
-                int len = std::snprintf(num, sizeof num, "%llu", (unsigned long long)(uint64_t(m.triangles[t][k]) + 1));
+                int len = std::snprintf(num, sizeof num, "%llu", (unsigned long long)(uint64_t(m.tris[3 * t + k]) + 1));
                 s.push_back(' ');
                 s.append(num, size_t(len));
                 if (normals) s += "//", s.append(num, size_t(len));
@@ -744,7 +744,6 @@ std::string obj_text(const Mesh& m, int precision, bool normals) {
     out += "# sesmesh 1.3.2\no ses\n";
     for (auto* part : {&v, &vn, &f})
         for (auto& s : *part) out += s;
-    (void)nv;
     return out;
 }
 

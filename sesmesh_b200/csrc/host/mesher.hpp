@@ -116,7 +116,32 @@ struct EdgeUses {
 size_t defects(const Mesh& m, EdgeUses* keep = nullptr);
 // components_with + group_by_component (mesh/mod.rs:185-297, post.rs:14-32).
 void components_and_group(Mesh& m, std::vector<Component>& comps, const EdgeUses* uses = nullptr);
-std::string obj_text(const Mesh& m, int precision = 4, bool normals = true);
+// Read-only arrays of a finished mesh, wherever they are stored.
+struct MeshRef {
+    const float* pos = nullptr;      // 3 per vertex
+    const float* nrm = nullptr;      // 3 per vertex, or null
+    const uint32_t* tris = nullptr;  // 3 per triangle
+    const uint32_t* atom = nullptr;
+    const uint8_t* patch = nullptr;
+    const uint32_t* comp = nullptr;
+    size_t nv = 0, nt = 0;
+    static MeshRef of(const Mesh& m) {
+        MeshRef r;
+        r.nv = m.positions.size(), r.nt = m.triangles.size();
+        r.pos = r.nv ? m.positions.data()->data() : nullptr;
+        r.nrm = m.normals.empty() ? nullptr : m.normals.data()->data();
+        r.tris = r.nt ? m.triangles.data()->data() : nullptr;
+        r.atom = m.vertex_atom.empty() ? nullptr : m.vertex_atom.data();
+        r.patch = m.vertex_patch.empty() ? nullptr : m.vertex_patch.data();
+        r.comp = m.vertex_component.empty() ? nullptr : m.vertex_component.data();
+        return r;
+    }
+};
+
+std::string obj_text(const MeshRef& m, int precision = 4, bool normals = true);
+inline std::string obj_text(const Mesh& m, int precision = 4, bool normals = true) {
+    return obj_text(MeshRef::of(m), precision, normals);
+}
 void push_fixed(std::string& buf, float x, int prec);
 
 }  // namespace smbh

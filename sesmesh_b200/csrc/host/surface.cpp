@@ -293,8 +293,8 @@ static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long
     auto t0 = clk::now();
     size_t bad = 0;
     std::string msg;
-    double ms_asm = 0, ms_copy = 0;
-    int r = smb::finish_on_device(e->dev, in, s.mesh, s.comps, &bad, e->measure, &msg, &ms_asm, &ms_copy);
+    double ms_asm = 0;
+    int r = smb::finish_on_device(e->dev, in, &s.view, &s.block, s.comps, &bad, e->measure, &msg, &ms_asm);
     if (r == 1) {
         *fallback = true;
         return SMB_OK;
@@ -306,17 +306,17 @@ static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long
     st.spheres = e->arr.n;
     st.surface_bricks = b->n;
     st.samples = size_t(b->n) * size_t(mp.b + 1) * size_t(mp.b + 1) * size_t(mp.b + 1);
-    st.vertices = s.mesh.positions.size();
-    st.triangles = s.mesh.triangles.size();
+    st.vertices = s.view.nv;
+    st.triangles = s.view.nt;
     st.components = s.comps.size();
     for (auto& c : s.comps) st.area += c.area, st.volume += c.volume, st.euler += c.euler;
     st.refine_evaluations = evals;
     st.refine_cpu_edges = 0;
     st.t_host_refine = 0;
     st.t_assemble = ms_asm;
-    st.t_measure = ms_since(t0) - ms_asm - ms_copy;
+    st.t_measure = ms_since(t0) - ms_asm;
     st.host_threads = threads();
-    *ms_d2h = ms_copy;
+    *ms_d2h = 0;  // the copies back overlap the measure
     return SMB_OK;
 }
 
@@ -472,40 +472,42 @@ int smb_surface_stats_get(const smb_surface* s, smb_surface_stats* out) {
 int smb_surface_mesh(const smb_surface* s, float* pos, float* nrm, uint32_t* tris, uint32_t* atoms, uint8_t* patches,
                      uint32_t* components) {
     if (!s) return SMB_ERR_ARG;
-    const Mesh& m = s->mesh;
-    if (pos && !m.positions.empty()) std::memcpy(pos, m.positions.data(), m.positions.size() * 12);
-    if (nrm && !m.normals.empty()) std::memcpy(nrm, m.normals.data(), m.normals.size() * 12);
-    if (tris && !m.triangles.empty()) std::memcpy(tris, m.triangles.data(), m.triangles.size() * 12);
-    if (atoms && !m.vertex_atom.empty()) std::memcpy(atoms, m.vertex_atom.data(), m.vertex_atom.size() * 4);
-    if (patches && !m.vertex_patch.empty()) std::memcpy(patches, m.vertex_patch.data(), m.vertex_patch.size());
-    if (components && !m.vertex_component.empty())
-        std::memcpy(components, m.vertex_component.data(), m.vertex_component.size() * 4);
+    const smbh::MeshRef m = s->ref();
+    auto copy = [](void* dst, const void* src, size_t bytes) {
+        if (dst && src && bytes) std::memcpy(dst, src, bytes);
+    };
+    copy(pos, m.pos, m.nv * 12);
+    copy(nrm, m.nrm, m.nv * 12);
+    copy(tris, m.tris, m.nt * 12);
+    copy(atoms, m.atom, m.nv * 4);
+    copy(patches, m.patch, m.nv);
+    copy(components, m.comp, m.nv * 4);
     return SMB_OK;
 }
 
 int smb_surface_arrays(const smb_surface* s, const float** pos, const float** nrm, const uint32_t** tris,
                        const uint32_t** atoms, const uint8_t** patches, const uint32_t** components) {
     if (!s) return SMB_ERR_ARG;
-    const Mesh& m = s->mesh;
-    if (pos) *pos = m.positions.empty() ? nullptr : m.positions.data()->data();
-    if (nrm) *nrm = m.normals.empty() ? nullptr : m.normals.data()->data();
-    if (tris) *tris = m.triangles.empty() ? nullptr : m.triangles.data()->data();
-    if (atoms) *atoms = m.vertex_atom.empty() ? nullptr : m.vertex_atom.data();
-    if (patches) *patches = m.vertex_patch.empty() ? nullptr : m.vertex_patch.data();
-    if (components) *components = m.vertex_component.empty() ? nullptr : m.vertex_component.data();
+    const smbh::MeshRef m = s->ref();
+    if (pos) *pos = m.nv ? m.pos : nullptr;
+    if (nrm) *nrm = m.nv ? m.nrm : nullptr;
+    if (tris) *tris = m.nt ? m.tris : nullptr;
+    if (atoms) *atoms = m.nv ? m.atom : nullptr;
+    if (patches) *patches = m.nv ? m.patch : nullptr;
+    if (components) *components = m.nv ? m.comp : nullptr;
     return SMB_OK;
 }
 
 size_t smb_surface_obj(smb_surface* s, char* out, size_t cap) {
     if (!s) return 0;
-    if (s->obj.empty()) s->obj = obj_text(s->mesh);
+    if (s->obj.empty()) s->obj = obj_text(s->ref());
     if (out) std::memcpy(out, s->obj.data(), s->obj.size() < cap ? s->obj.size() : cap);
     return s->obj.size();
 }
 
 int smb_surface_write_obj(smb_surface* s, const char* path, char* err, size_t errlen) {
     if (!s || !path) return SMB_ERR_ARG;
-    if (s->obj.empty()) s->obj = obj_text(s->mesh);
+    if (s->obj.empty()) s->obj = obj_text(s->ref());
     FILE* f = std::fopen(path, "wb");
     if (!f) return set_err(err, errlen, "cannot open %s", path), SMB_ERR_ARG;
     size_t w = std::fwrite(s->obj.data(), 1, s->obj.size(), f);
