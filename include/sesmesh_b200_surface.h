@@ -150,14 +150,22 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
 smb_surface* smb_multi_surface(smb_multi* m, size_t i);
 int smb_multi_latency(const smb_multi* m, double* ms);
 
-/* The host arrangement of an engine (views valid while it lives). */
+/* The host arrangement of an engine (views valid while it lives; an
+ * arrangement built on the device is copied to the host on first use).
+ * built_on_device: 1 when the device built it. */
 typedef struct {
     size_t n_spheres, n_contained, n_circles, n_vertices;
     const double *center, *expanded, *circle, *vertex;
     const uint32_t *status, *orig, *circle_ij, *vertex_atoms, *nb_off, *nb_items, *cb_off, *cb_items;
     double max_expanded, rho_max, band, t_min;
     int64_t frame[3];
+    int built_on_device;
 } smb_arrangement_info;
+/* Inputs of at least n spheres get their arrangement built on the device
+ * (geom/arrangement.rs:246-770 with the host build's values bit for bit;
+ * the host builds it when the device declines).  Process-wide; default
+ * 16384; 0 = always, SIZE_MAX = never. */
+void smb_set_device_arrangement_min(size_t n);
 int smb_engine_arrangement(const smb_engine* e, smb_arrangement_info* out);
 /* Builds only the host arrangement (no device; smb_engine_arrangement). */
 int smb_arrangement_build(const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out, char* err,

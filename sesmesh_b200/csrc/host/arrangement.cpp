@@ -202,7 +202,7 @@ struct SpherePart {
 
 }  // namespace
 
-std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arrangement& A) {
+std::string check_spheres(const double* xyzr, size_t ns, double probe) {
     if (!(std::isfinite(probe) && probe > 0.0)) return "probe radius must be finite and > 0 for the SES";
     for (size_t i = 0; i < ns; i++) {
         const double* s = xyzr + 4 * i;
@@ -210,6 +210,12 @@ std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arran
             return "sphere " + std::to_string(i) + " has a non-finite centre";
         if (!(std::isfinite(s[3]) && s[3] >= 0.0)) return "sphere " + std::to_string(i) + " has an invalid radius";
     }
+    return "";
+}
+
+std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arrangement& A) {
+    std::string bad = check_spheres(xyzr, ns, probe);
+    if (!bad.empty()) return bad;
     A = Arrangement();
     A.probe = probe;
     std::vector<uint32_t> active;

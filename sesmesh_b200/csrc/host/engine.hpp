@@ -7,6 +7,7 @@
 #include "../../../include/sesmesh_b200.h"
 #include "../../../include/sesmesh_b200_surface.h"
 #include "../device/measure.hpp"
+#include "../device/sas.hpp"
 #include "../runtime.hpp"
 #include "geom.hpp"
 #include "mesher.hpp"
@@ -20,7 +21,10 @@ using smbh::MeshParams;
 struct smb_engine {
     smb_device* dev = nullptr;
     smb_surface_params params{};
-    Arrangement arr;
+    Arrangement arr;           // the host arrangement (of a device-built one: copied on first use)
+    bool arr_ready = true;     // arr holds the arrangement
+    smb::DevArrangement darr;  // the device-built arrangement's descriptors (its buffers belong to res)
+    size_t n_spheres = 0;      // spheres with r > 0
     MeshParams mp;
     smb_resident* res = nullptr;
     smb_batch* batch = nullptr;
@@ -42,6 +46,10 @@ struct smb_engine {
     bool rows_ready = false;
     std::vector<float> row_x, row_t;
 };
+
+// The engine's host arrangement (copied from the device on first use when
+// the device built it).
+const Arrangement& host_arrangement(smb_engine* e);
 
 struct smb_surface {
     Mesh mesh;

@@ -93,6 +93,8 @@ struct Arrangement {
 
 // Builds the SES arrangement of n spheres (x, y, z, r rows); error text or "".
 std::string build_arrangement(const double* xyzr, size_t n, double probe, Arrangement& out);
+// The input checks of build_arrangement alone; error text or "".
+std::string check_spheres(const double* xyzr, size_t n, double probe);
 
 void set_threads(int n);
 int threads();

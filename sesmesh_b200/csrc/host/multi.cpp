@@ -727,7 +727,7 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
                 auto s = std::make_unique<smb_surface>();
                 smb_engine* e = m->eng[i];
                 std::string msg = finish_surface(
-                    e->arr, m->mp[i], true, k3.data(), nbi, leo.data(), H.edges.as<uint32_t>() + e0,
+                    host_arrangement(e), m->mp[i], true, k3.data(), nbi, leo.data(), H.edges.as<uint32_t>() + e0,
                     H.ev.as<float>() + 2 * e0, lto.data(), H.tris.as<uint32_t>() + 3 * tr0,
                     DeviceRefine{H.t.as<float>() + e0, H.feat.as<uint32_t>() + e0, H.q.as<float>() + 3 * e0,
                                  H.evals.as<uint32_t>() + e0},

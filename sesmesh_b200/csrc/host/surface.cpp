@@ -97,7 +97,19 @@ std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fa
     return "";
 }
 
+static size_t g_device_arrangement_min = 16384;
+
+const Arrangement& host_arrangement(smb_engine* e) {
+    if (!e->arr_ready) {
+        smb::arrangement_to_host(e->darr, e->arr);
+        e->arr_ready = true;
+    }
+    return e->arr;
+}
+
 extern "C" {
+
+void smb_set_device_arrangement_min(size_t n) { g_device_arrangement_min = n; }
 
 int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out,
                    char* err, size_t errlen) {
@@ -115,15 +127,34 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
     e->dev = dev;
     e->params = *p;
     auto t0 = clk::now();
-    std::string m = build_arrangement(xyzr, n, p->probe_radius, e->arr);
+    std::string m = check_spheres(xyzr, n, p->probe_radius);
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
+    // The arrangement: on the device for large inputs (the host builds it
+    // when the device declines), else on the host threads.
+    bool on_device = false;
+    if (n >= g_device_arrangement_min) {
+        std::string why;
+        on_device = smb::build_arrangement_device(dev, xyzr, n, p->probe_radius, e->darr, &why) == 0;
+    }
+    if (!on_device) {
+        m = build_arrangement(xyzr, n, p->probe_radius, e->arr);
+        if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
+    }
+    e->arr_ready = !on_device;
     const Arrangement& A = e->arr;
+    const double max_expanded = on_device ? e->darr.A.max_expanded : A.max_expanded;
+    e->n_spheres = on_device ? e->darr.n : A.n;
     // Engine::new (field/kernel.rs:204-271).
     V3 center;
     double half = 0.0;
-    if (A.n) {
-        V3 lo = A.c(0), hi = lo;
-        for (size_t i = 0; i < A.n; i++) lo = lo.lo(A.c(uint32_t(i))), hi = hi.hi(A.c(uint32_t(i)));
+    if (e->n_spheres) {
+        V3 lo, hi;
+        if (on_device) {
+            lo = V3::at(e->darr.lo), hi = V3::at(e->darr.hi);
+        } else {
+            lo = A.c(0), hi = lo;
+            for (size_t i = 0; i < A.n; i++) lo = lo.lo(A.c(uint32_t(i))), hi = hi.hi(A.c(uint32_t(i)));
+        }
         V3 d = hi - lo;
         center = (lo + hi) * 0.5;
         half = 0.5 * std::fmax(std::fmax(d.x, d.y), d.z);
@@ -135,14 +166,14 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
     P.frame[0] = to_i64(std::round(center.x / P.h));
     P.frame[1] = to_i64(std::round(center.y / P.h));
     P.frame[2] = to_i64(std::round(center.z / P.h));
-    double reach = half + 2.0 * A.max_expanded + 2.0 * p->probe_radius + 4.0 * double(P.b) * P.h;
+    double reach = half + 2.0 * max_expanded + 2.0 * p->probe_radius + 4.0 * double(P.b) * P.h;
     P.f32_ok = reach < 2000.0 && reach / P.h < double(1u << 23);
     if (!P.f32_ok)
         return set_err(err, errlen, "extent beyond the f32 frame (%g A): the device path does not take it", reach),
                SMB_ERR_RANGE;
     P.band = std::sqrt(3.0) * P.h * 1.01;
     P.coord_max = std::fmax(std::fmax(std::fabs(center.x), std::fabs(center.y)), std::fabs(center.z)) + half +
-                  A.max_expanded + p->probe_radius + 2.0 * P.band;
+                  max_expanded + p->probe_radius + 2.0 * P.band;
     {  // edge_clamp (extract.rs:47-51)
         double cm = P.coord_max < 1.0 ? 1.0 : (P.coord_max > double(3.4028234663852886e38f) / 4.0 ? double(3.4028234663852886e38f) / 4.0 : P.coord_max);
         float mf = float(cm), nx;
@@ -154,8 +185,28 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
         P.t_min = tm < 1e-4 ? 1e-4 : (tm > 0.25 ? 0.25 : tm);
     }
     e->t_geometry = ms_since(t0);
-    // Upload (Resident::new).
     auto t1 = clk::now();
+    smb_lattice_ref lat{};
+    lat.spacing = P.h;
+    lat.brick = uint32_t(P.b);
+    for (int k = 0; k < 3; k++) lat.frame[k] = P.frame[k];
+    lat.band = P.band;
+    int rc;
+    if (on_device) {  // the resident takes over the device-built arrangement
+        rc = smb::resident_from_device(dev, e->darr, &lat, &e->res, err, errlen);
+        if (rc != SMB_OK) return e->darr.release(), rc;
+        rc = smb_batch_new(e->res, &e->batch, err, errlen);
+        if (rc != SMB_OK) return rc;
+        if (p->refine == SMB_REFINE_FAST) {
+            if ((rc = smb_resident_set_refinement(e->res, err, errlen)) != SMB_OK) return rc;
+        } else {
+            smb::resident_set_exact_tmin(e->res, P.t_min);
+        }
+        e->t_upload = ms_since(t1);
+        *out = e.release();
+        return SMB_OK;
+    }
+    // Upload (Resident::new).
     smb_arrangement_ref r{};
     r.n_spheres = A.n;
     r.center = A.center.data();
@@ -182,12 +233,7 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
     r.max_expanded = A.max_expanded;
     r.rho_max = A.rho_max;
     r.probe = A.probe;
-    smb_lattice_ref lat{};
-    lat.spacing = P.h;
-    lat.brick = uint32_t(P.b);
-    for (int k = 0; k < 3; k++) lat.frame[k] = P.frame[k];
-    lat.band = P.band;
-    int rc = smb_resident_new(dev, &r, &lat, &e->res, err, errlen);
+    rc = smb_resident_new(dev, &r, &lat, &e->res, err, errlen);
     if (rc != SMB_OK) return rc;
     rc = smb_batch_new(e->res, &e->batch, err, errlen);
     if (rc != SMB_OK) return rc;
@@ -303,7 +349,7 @@ static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long
     if (bad) return set_err(err, errlen, "mesh failed validation (%zu defects)", bad), SMB_ERR_STATE;
     const MeshParams& mp = e->mp;
     smb_surface_stats& st = s.stats;
-    st.spheres = e->arr.n;
+    st.spheres = e->n_spheres;
     st.surface_bricks = b->n;
     st.samples = size_t(b->n) * size_t(mp.b + 1) * size_t(mp.b + 1) * size_t(mp.b + 1);
     st.vertices = s.view.nv;
@@ -378,7 +424,7 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
     }
     double t_d2h = ms_since(t0);
     auto s = std::make_unique<smb_surface>();
-    std::string m = finish_surface(e->arr, e->mp, fast, e->keys.data(), nb, e->edge_off.data(), e->edges.data(),
+    std::string m = finish_surface(host_arrangement(e), e->mp, fast, e->keys.data(), nb, e->edge_off.data(), e->edges.data(),
                                    e->edge_vals.data(), e->tri_off.data(), e->tris.data(),
                                    DeviceRefine{e->t.data(), e->feat.data(), e->closest.data(), e->evals.data()}, *s,
                                    e->dev, &e->measure, exact_dev && ne ? &e->exact_out : nullptr,
@@ -392,6 +438,7 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
 int smb_engine_field(const smb_engine* e, const double* points, size_t n, double* values) {
     if (!e || (n && (!points || !values))) return SMB_ERR_ARG;
     const double band = e->mp.band;
+    const Arrangement& A = host_arrangement(const_cast<smb_engine*>(e));
     // The refinement's evaluation (field/point.rs:496-738): the candidates of
     // the point (a ball of radius 0), then the exact f64 field, which equals
     // SesField::value within the band.
@@ -399,8 +446,8 @@ int smb_engine_field(const smb_engine* e, const double* points, size_t n, double
         Local l;
         for (size_t i = c * 256; i < std::min(n, (c + 1) * 256); i++) {
             V3 x = V3::at(points + 3 * i);
-            gather_local(e->arr, x, 0.0, band, l);
-            values[i] = eval_local(e->arr, x, band, l).value;
+            gather_local(A, x, 0.0, band, l);
+            values[i] = eval_local(A, x, band, l).value;
         }
     });
     return SMB_OK;
@@ -431,7 +478,7 @@ int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, si
         std::vector<uint8_t> covered(ne);
         if ((rc = smb_batch_edge_features(e->res, e->batch, x.data(), covered.data(), err, errlen)) != SMB_OK) return rc;
         MeshOut mo;
-        refine_exact(e->arr, e->mp, e->keys.data(), e->res->n_bricks, e->edge_off.data(), e->edges.data(),
+        refine_exact(host_arrangement(e), e->mp, e->keys.data(), e->res->n_bricks, e->edge_off.data(), e->edges.data(),
                      e->edge_vals.data(), mo);
         e->row_x.clear(), e->row_t.clear();
         for (size_t k = 0; k < ne; k++) {
@@ -519,7 +566,8 @@ int smb_surface_write_obj(smb_surface* s, const char* path, char* err, size_t er
 // The host arrangement of an engine (tests compare it with the oracle's).
 int smb_engine_arrangement(const smb_engine* e, smb_arrangement_info* out) {
     if (!e || !out) return SMB_ERR_ARG;
-    const Arrangement& A = e->arr;
+    const Arrangement& A = host_arrangement(const_cast<smb_engine*>(e));
+    out->built_on_device = e->darr.A.sph != nullptr;
     out->n_spheres = A.n;
     out->n_contained = A.n_contained;
     out->n_circles = A.n_circles();

@@ -20,6 +20,7 @@
 #include "../../include/sesmesh_b200.h"
 #include "device/kernels.hpp"
 #include "device/mlp.cuh"
+#include "device/sas.hpp"
 #include "runtime.hpp"
 
 using namespace smb;
@@ -406,6 +407,24 @@ static bool csr_ok(const uint32_t* off, size_t rows, size_t items) {
     return off[rows] == items;
 }
 
+// Lattice constants, computed here in the CPU's f64 operation order.
+static void set_lattice(DLat& L, const smb_lattice_ref* lat, double probe) {
+    L.h = lat->spacing;
+    L.b = int(lat->brick);
+    L.sub = L.b / 2;
+    L.spb = (L.b + 1) * (L.b + 1) * (L.b + 1);
+    for (int k = 0; k < 3; k++) L.frame[k] = (long long)lat->frame[k];
+    L.fx = double(lat->frame[0]) * L.h, L.fy = double(lat->frame[1]) * L.h, L.fz = double(lat->frame[2]) * L.h;
+    L.band = lat->band;
+    L.rho_sub = 0.5 * std::sqrt(3.0) * double(L.sub) * L.h;   // kernel.rs:474
+    L.rho_brick = 0.5 * std::sqrt(3.0) * double(L.b) * L.h;   // lattice.rs:78-80
+    L.h32 = float(L.h);
+    L.band32 = float(L.band);
+    L.probe32 = float(probe);
+    float cutoff = float(probe + L.band);                      // kernel.rs:425
+    L.cutoff2 = cutoff * cutoff;
+}
+
 int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_lattice_ref* lat, smb_resident** out,
                      char* err, size_t errlen) {
     if (!d || !a || !lat || !out) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
@@ -512,22 +531,7 @@ int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_latt
         D.items = static_cast<const uint32_t*>(p);
     }
     A.max_expanded = a->max_expanded, A.rho_max = a->rho_max, A.probe = a->probe;
-    // Lattice constants, computed here in the CPU's f64 operation order.
-    DLat& L = r->L;
-    L.h = lat->spacing;
-    L.b = int(lat->brick);
-    L.sub = L.b / 2;
-    L.spb = (L.b + 1) * (L.b + 1) * (L.b + 1);
-    for (int k = 0; k < 3; k++) L.frame[k] = (long long)lat->frame[k];
-    L.fx = double(lat->frame[0]) * L.h, L.fy = double(lat->frame[1]) * L.h, L.fz = double(lat->frame[2]) * L.h;
-    L.band = lat->band;
-    L.rho_sub = 0.5 * std::sqrt(3.0) * double(L.sub) * L.h;   // kernel.rs:474
-    L.rho_brick = 0.5 * std::sqrt(3.0) * double(L.b) * L.h;   // lattice.rs:78-80
-    L.h32 = float(L.h);
-    L.band32 = float(L.band);
-    L.probe32 = float(a->probe);
-    float cutoff = float(a->probe + L.band);                   // kernel.rs:425
-    L.cutoff2 = cutoff * cutoff;
+    set_lattice(r->L, lat, a->probe);
     cudaError_t e = cudaStreamSynchronize(d->stream);
     if (e != cudaSuccess) {
         set_err(err, errlen, "upload failed: %s", cudaGetErrorString(e));
@@ -946,6 +950,41 @@ int smb_batch_edge_features(smb_resident* r, smb_batch* b, float* features, uint
     }
     return SMB_OK;
 }
+
+}  // extern "C"
+
+namespace smb {
+
+int resident_from_device(smb_device* d, DevArrangement& D, const smb_lattice_ref* lat, smb_resident** out, char* err,
+                         size_t errlen) {
+    if (!d || !lat || !out) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
+    *out = nullptr;
+    if (lat->brick < 4 || lat->brick > 32 || lat->brick % 2)
+        return set_err(err, errlen, "brick must be even and 4..32, got %u", lat->brick), SMB_ERR_ARG;
+    if (!(lat->spacing >= 0.01) || !std::isfinite(lat->spacing))
+        return set_err(err, errlen, "grid spacing must be at least 0.01"), SMB_ERR_ARG;
+    auto* r = new smb_resident();
+    r->dev = d;
+    dev_retain(d);
+    r->A = D.A;
+    r->owned.swap(D.owned);
+    r->bytes = D.bytes;
+    D.bytes = 0;
+    for (int k = 0; k < 3; k++) r->lo[k] = D.lo[k], r->hi[k] = D.hi[k];
+    set_lattice(r->L, lat, D.A.probe);
+    r->xa = ExactAttr{D.orig, D.circle_ij, D.vertex_atoms, 0.0};
+    *out = r;
+    return SMB_OK;
+}
+
+void resident_set_exact_tmin(smb_resident* r, double t_min) {
+    r->xa.t_min = t_min;
+    r->exact_ready = true;
+}
+
+}  // namespace smb
+
+extern "C" {
 
 int smb_resident_set_exact(smb_resident* r, const uint32_t* orig, const uint32_t* circle_ij, size_t n_circles,
                            const uint32_t* vertex_atoms, size_t n_vertices, double t_min, char* err, size_t errlen) {

@@ -80,7 +80,7 @@ class ArrangementInfo(C.Structure):
                 ("nb_off", C.POINTER(C.c_uint32)), ("nb_items", C.POINTER(C.c_uint32)),
                 ("cb_off", C.POINTER(C.c_uint32)), ("cb_items", C.POINTER(C.c_uint32)),
                 ("max_expanded", C.c_double), ("rho_max", C.c_double), ("band", C.c_double), ("t_min", C.c_double),
-                ("frame", C.c_int64 * 3)]
+                ("frame", C.c_int64 * 3), ("built_on_device", C.c_int)]
 
 
 class MultiConfig(C.Structure):
@@ -178,6 +178,7 @@ SIGNATURES = {
     "smb_multi_surface": (_vp, [_vp, _sz]),
     "smb_multi_latency": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "smb_engine_arrangement": (C.c_int, [_vp, C.POINTER(ArrangementInfo)]),
+    "smb_set_device_arrangement_min": (None, [_sz]),
     "smb_arrangement_build": (C.c_int, [C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_), C.POINTER(_vp), _cp,
                                         _sz]),
 }

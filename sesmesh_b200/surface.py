@@ -264,6 +264,30 @@ class SurfaceEngine:
         self.close()
 
 
+def _arrangement_arrays(h):
+    info = native.ArrangementInfo()
+    lib().smb_engine_arrangement(h, C.byref(info))
+    n, nc, nv = info.n_spheres, info.n_circles, info.n_vertices
+
+    def arr(ptr, count, dt):
+        if count == 0:
+            return np.zeros(0, dt)
+        return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt).copy()
+
+    out = dict(center=arr(info.center, 3 * n, np.float64).reshape(-1, 3),
+               expanded=arr(info.expanded, n, np.float64), status=arr(info.status, n, np.uint32),
+               orig=arr(info.orig, n, np.uint32), circle=arr(info.circle, 10 * nc, np.float64).reshape(-1, 10),
+               circle_ij=arr(info.circle_ij, 2 * nc, np.uint32).reshape(-1, 2),
+               vertex=arr(info.vertex, 3 * nv, np.float64).reshape(-1, 3),
+               vertex_atoms=arr(info.vertex_atoms, 3 * nv, np.uint32).reshape(-1, 3),
+               nb_off=arr(info.nb_off, n + 1, np.uint32), cb_off=arr(info.cb_off, nc + 1, np.uint32),
+               n_contained=info.n_contained, max_expanded=info.max_expanded, rho_max=info.rho_max,
+               built_on_device=bool(info.built_on_device))
+    out["nb_items"] = arr(info.nb_items, int(out["nb_off"][-1]), np.uint32)
+    out["cb_items"] = arr(info.cb_items, int(out["cb_off"][-1]), np.uint32)
+    return out
+
+
 def host_arrangement(spheres, params=SurfaceParams()):
     """The host-built arrangement (no device), as numpy copies."""
     s = _spheres(spheres)
@@ -272,28 +296,21 @@ def host_arrangement(spheres, params=SurfaceParams()):
     p = params._c()
     _check(lib().smb_arrangement_build(_p(s, C.c_double), len(s), C.byref(p), C.byref(h), err, 1024), err)
     try:
-        info = native.ArrangementInfo()
-        lib().smb_engine_arrangement(h, C.byref(info))
-        n, nc, nv = info.n_spheres, info.n_circles, info.n_vertices
-
-        def arr(ptr, count, dt):
-            if count == 0:
-                return np.zeros(0, dt)
-            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt).copy()
-
-        out = dict(center=arr(info.center, 3 * n, np.float64).reshape(-1, 3),
-                   expanded=arr(info.expanded, n, np.float64), status=arr(info.status, n, np.uint32),
-                   orig=arr(info.orig, n, np.uint32), circle=arr(info.circle, 10 * nc, np.float64).reshape(-1, 10),
-                   circle_ij=arr(info.circle_ij, 2 * nc, np.uint32).reshape(-1, 2),
-                   vertex=arr(info.vertex, 3 * nv, np.float64).reshape(-1, 3),
-                   vertex_atoms=arr(info.vertex_atoms, 3 * nv, np.uint32).reshape(-1, 3),
-                   nb_off=arr(info.nb_off, n + 1, np.uint32), cb_off=arr(info.cb_off, nc + 1, np.uint32),
-                   n_contained=info.n_contained, max_expanded=info.max_expanded, rho_max=info.rho_max)
-        out["nb_items"] = arr(info.nb_items, int(out["nb_off"][-1]), np.uint32)
-        out["cb_items"] = arr(info.cb_items, int(out["cb_off"][-1]), np.uint32)
-        return out
+        return _arrangement_arrays(h)
     finally:
         lib().smb_engine_free(h)
+
+
+def set_device_arrangement_min(n):
+    """Inputs of at least n spheres get their arrangement built on the
+    device (process-wide; 0 = always, None = never)."""
+    lib().smb_set_device_arrangement_min(C.c_size_t(2 ** 64 - 1 if n is None else int(n)))
+
+
+def engine_arrangement(engine):
+    """An engine's arrangement (copied from the device when the device built
+    it), as numpy copies; built_on_device tells which."""
+    return _arrangement_arrays(engine.h)
 
 
 class MultiBatch:
