@@ -201,9 +201,18 @@ int smb_refine_exact(smb_resident* res, smb_batch* batch, double* ms, char* err,
  * device).  Null pointers are skipped. */
 int smb_batch_vertices(const smb_batch* batch, float* positions, float* normals, uint32_t* atoms, uint8_t* patches,
                        float* t, uint32_t* evals);
-/* Over the edges of the last smb_refine_exact: the total evaluation count
- * and the number of edges left to the host (evals = 0). */
-int smb_batch_exact_summary(const smb_batch* batch, unsigned long long* evaluations, unsigned long long* host_edges);
+/* Fast mode's vertex placement on the device (mesh_brick_device,
+ * mesh/extract.rs:274-365; additive, the reference places on the host):
+ * after smb_refine, every edge the f32 refinement converged on is placed at
+ * pa + d clamp(t) with the exact attributes of its feature, and every other
+ * edge is refined exactly as smb_refine_exact does.  Needs
+ * smb_resident_set_exact.  Results through smb_batch_vertices. */
+int smb_place_fast(smb_resident* res, smb_batch* batch, double* ms, char* err, size_t errlen);
+/* Over the vertices of the last smb_refine_exact / smb_place_fast: the total
+ * evaluation count, the number of edges left to the host (evals = 0) and
+ * the number of edges the exact refinement took. */
+int smb_batch_exact_summary(const smb_batch* batch, unsigned long long* evaluations, unsigned long long* host_edges,
+                            unsigned long long* exact_edges);
 /* Shared memory per warp for one sub-block's f64 lists in smb_refine_exact
  * (1 KiB..48 KiB; default 18 KiB); larger sub-blocks take a whole block. */
 int smb_batch_set_exact_region(smb_batch* batch, size_t bytes);

@@ -396,8 +396,53 @@ __device__ __forceinline__ uint32_t x_nearest(const DArr& A, const ExactAttr& X,
     return X.orig[bi];
 }
 
-// extract::vertex of edge k (exact mode) and its attributes; leaves evals[k]
-// = 0 when the last evaluation is solvent or beyond.
+// sphere_eval (point.rs:742-757): the non-contained sphere with the lowest
+// |p - c| - R below cutoff, in cell-scan order (first on ties); -1: none.
+__device__ long long x_sphere_eval(const DArr& A, double px, double py, double pz, double cutoff) {
+    double best = cutoff;
+    long long bi = -1;
+    const CellBox bx = cell_box(A.gs, px, py, pz, cutoff + A.max_expanded);
+    for (uint32_t zc = bx.z0; zc <= bx.z1; zc++)
+        for (uint32_t yc = bx.y0; yc <= bx.y1; yc++) {
+            const size_t row = (size_t(zc) * A.gs.dy + yc) * A.gs.dx;
+            for (uint32_t i = A.gs.starts[row + bx.x0], e = A.gs.starts[row + bx.x1 + 1]; i < e; i++) {
+                const uint32_t k = A.gs.items[i];
+                if (A.status[k] == STATUS_CONTAINED) continue;
+                const double4 c = A.sph[k];
+                const double v = dist3(px, py, pz, c.x, c.y, c.z) - c.w;
+                if (v < best) best = v, bi = k;
+            }
+        }
+    return bi;
+}
+
+// extract::attributes (extract.rs:553-597) of a vertex at p on the edge
+// (pa, pa + d) whose last evaluation had feature (kind, id) and closest
+// point q: normal, patch, input atom.
+__device__ void x_attributes(const DArr& A, const DLat& L, const ExactAttr& X, uint32_t kind, uint32_t id, double qx,
+                             double qy, double qz, double px, double py, double pz, double dx, double dy, double dz,
+                             double fa, double& nx, double& ny, double& nz, uint32_t& atom, uint32_t& patch) {
+    double ox = dx, oy = dy, oz = dz;
+    if (!(fa < 0.0)) ox = dx * -1.0, oy = dy * -1.0, oz = dz * -1.0;
+    const double on = sqrt(ox * ox + oy * oy + oz * oz);
+    ox = ox / on, oy = oy / on, oz = oz / on;
+    if (kind == XF_SPHERE || kind == XF_CIRCLE || kind == XF_VERTEX) {
+        nx = qx - px, ny = qy - py, nz = qz - pz;
+        const double nl = sqrt(nx * nx + ny * ny + nz * nz);
+        if (nl > 1e-9) nx = nx / nl, ny = ny / nl, nz = nz / nl;
+        else nx = ox, ny = oy, nz = oz;
+        if (kind == XF_SPHERE) atom = X.orig[id], patch = 0;
+        else if (kind == XF_CIRCLE) atom = x_nearest(A, X, X.circle_ij + 2 * size_t(id), 2, px, py, pz), patch = 1;
+        else atom = x_nearest(A, X, X.vertex_atoms + 3 * size_t(id), 3, px, py, pz), patch = 2;
+        return;
+    }
+    nx = ox, ny = oy, nz = oz;
+    patch = 0;
+    const long long bi = x_sphere_eval(A, px, py, pz, A.probe + L.band + 8.0);
+    atom = bi < 0 ? 0u : X.orig[bi];
+}
+
+// extract::vertex of edge k (exact mode) and its attributes.
 __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat& L, const ExactAttr& X, int4 key, uint32_t k,
                        uint32_t code, float2 fv, const ExactOut& out) {
     const int b = L.b;
@@ -464,23 +509,12 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
             else t1 = t;
         }
     }
-    if (last.kind == XF_SOLVENT || last.kind == XF_BEYOND) return;
     const double ct = x_clamp(t, X.t_min, 1.0 - X.t_min);
     const double px = pax + dx * ct, py = pay + dy * ct, pz = paz + dz * ct;
-    double nx = last.qx - px, ny = last.qy - py, nz = last.qz - pz;
-    const double nl = sqrt(nx * nx + ny * ny + nz * nz);
-    if (nl > 1e-9) {
-        nx = nx / nl, ny = ny / nl, nz = nz / nl;
-    } else {
-        double ox = dx, oy = dy, oz = dz;
-        if (!(fa < 0.0)) ox = dx * -1.0, oy = dy * -1.0, oz = dz * -1.0;
-        const double on = sqrt(ox * ox + oy * oy + oz * oz);
-        nx = ox / on, ny = oy / on, nz = oz / on;
-    }
+    double nx, ny, nz;
     uint32_t atom, patch;
-    if (last.kind == XF_SPHERE) atom = X.orig[last.id], patch = 0;
-    else if (last.kind == XF_CIRCLE) atom = x_nearest(A, X, X.circle_ij + 2 * size_t(last.id), 2, px, py, pz), patch = 1;
-    else atom = x_nearest(A, X, X.vertex_atoms + 3 * size_t(last.id), 3, px, py, pz), patch = 2;
+    x_attributes(A, L, X, last.kind, last.id, last.qx, last.qy, last.qz, px, py, pz, dx, dy, dz, fa, nx, ny, nz, atom,
+                 patch);
     out.pos[3 * size_t(k)] = float(px), out.pos[3 * size_t(k) + 1] = float(py), out.pos[3 * size_t(k) + 2] = float(pz);
     out.nrm[3 * size_t(k)] = float(nx), out.nrm[3 * size_t(k) + 1] = float(ny), out.nrm[3 * size_t(k) + 2] = float(nz);
     out.atom[k] = atom;
@@ -560,7 +594,84 @@ __global__ void k_exact_summary(const uint32_t* evals, size_t n, unsigned long l
     }
 }
 
+// mesh_brick_device (extract.rs:274-365) on the device: each edge the f32
+// refinement converged on (t in [0, 1], a valid feature) is placed at
+// pa + d clamp(t) with the exact attributes of its feature and closest
+// point (brick origin + the f32 offset); every other edge is marked in
+// need[] for the exact refinement.  counters[0] += the marked edges.
+__global__ void k_place_fast(DArr A, DLat L, ExactAttr X, const int4* keys, uint32_t n_bricks,
+                             const uint32_t* edge_off, const uint32_t* edges, const float2* edge_vals, size_t n_edges,
+                             const float* t_in, const uint32_t* feat, const float* q, const uint32_t* ev_in,
+                             ExactOut out, uint8_t* need, unsigned long long* marked) {
+    const size_t k = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    unsigned long long mine = 0;
+    if (k < n_edges) {
+        const uint32_t ev = ev_in[k];
+        const double t = double(t_in[k]);
+        const uint32_t kind = feat[k] >> 29, id = feat[k] & ((1u << 29) - 1);
+        bool ok = (ev & 0x80000000u) && t >= 0.0 && t <= 1.0;
+        if (ok) {
+            if (kind == XF_SPHERE) ok = id < A.n;
+            else if (kind == XF_CIRCLE) ok = id < A.nc;
+            else if (kind == XF_VERTEX) ok = id < A.nv;
+            else ok = kind == XF_SOLVENT || kind == XF_BEYOND;
+        }
+        if (!ok) {
+            need[k] = 1;
+            out.evals[k] = 0;
+            mine = 1;
+        } else {
+            need[k] = 0;
+            uint32_t lo = 0, hi = n_bricks;  // the brick of edge k: edge_off[lo] <= k < edge_off[lo + 1]
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (edge_off[mid] <= k) lo = mid;
+                else hi = mid;
+            }
+            const int4 key = keys[lo];
+            const int b = L.b;
+            const double h = L.h;
+            const uint32_t code = edges[k], cell = code / 3, axis = code % 3;
+            const long long ix = (long long)key.x * b + (long long)(cell % uint32_t(b)),
+                            iy = (long long)key.y * b + (long long)((cell / uint32_t(b)) % uint32_t(b)),
+                            iz = (long long)key.z * b + (long long)(cell / uint32_t(b * b));
+            const double pax = double(ix) * h, pay = double(iy) * h, paz = double(iz) * h;
+            const double dx = double(ix + (axis == 0)) * h - pax, dy = double(iy + (axis == 1)) * h - pay,
+                         dz = double(iz + (axis == 2)) * h - paz;
+            const double ct = x_clamp(t, X.t_min, 1.0 - X.t_min);
+            const double px = pax + dx * ct, py = pay + dy * ct, pz = paz + dz * ct;
+            const double bx = double((long long)key.x * b) * h, by = double((long long)key.y * b) * h,
+                         bz = double((long long)key.z * b) * h;
+            const double qx = bx + double(q[3 * k]), qy = by + double(q[3 * k + 1]), qz = bz + double(q[3 * k + 2]);
+            double nx, ny, nz;
+            uint32_t atom, patch;
+            x_attributes(A, L, X, kind, id, qx, qy, qz, px, py, pz, dx, dy, dz, double(edge_vals[k].x), nx, ny, nz,
+                         atom, patch);
+            out.pos[3 * k] = float(px), out.pos[3 * k + 1] = float(py), out.pos[3 * k + 2] = float(pz);
+            out.nrm[3 * k] = float(nx), out.nrm[3 * k + 1] = float(ny), out.nrm[3 * k + 2] = float(nz);
+            out.atom[k] = atom;
+            out.patch[k] = uint8_t(patch);
+            out.t[k] = t_in[k];
+            out.evals[k] = ev & 0x7fffffffu;
+        }
+    }
+    for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, o);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(marked, mine);
+}
+
 }  // namespace
+
+cudaError_t launch_place_fast(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys, uint32_t n_bricks,
+                              const uint32_t* edge_off, const uint32_t* edges, const float2* edge_vals, size_t n_edges,
+                              const float* t, const uint32_t* feat, const float* q, const uint32_t* evals,
+                              const ExactOut& out, uint8_t* need, unsigned long long* marked, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(marked, 0, 8, s);
+    if (e != cudaSuccess || !n_edges) return e;
+    count_launches(1);
+    k_place_fast<<<unsigned((n_edges + 255) / 256), 256, 0, s>>>(A, L, X, keys, n_bricks, edge_off, edges, edge_vals,
+                                                                  n_edges, t, feat, q, evals, out, need, marked);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long long* out, int sms, cudaStream_t s) {
     cudaError_t e = cudaMemsetAsync(out, 0, 16, s);

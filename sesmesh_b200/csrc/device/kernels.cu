@@ -1039,9 +1039,10 @@ __device__ __forceinline__ float edge_features(const float* val, int b, float h,
     return t_c;
 }
 
-// Sub-block edge lists for refinement: per work item (a sampled sub-block
-// without flags), its brick's crossing edges whose lower sample lies in the
-// sub-block, in the brick's (ascending) order.  Warp per item; FILL = false
+// Sub-block edge lists for refinement: per work item (a sampled sub-block;
+// without flags unless any_flags: the f32 refinement stages the sampler's
+// lists, which a flagged sub-block lacks), its brick's crossing edges whose
+// lower sample lies in the sub-block, in the brick's (ascending) order.  Warp per item; FILL = false
 // counts (and records the largest count), FILL = true writes at item_off[i]
 // and the list's tail item_off[n] = *total.
 template <bool FILL, bool MANY>
@@ -1049,7 +1050,8 @@ __global__ void __launch_bounds__(256) k_item_edges(const DLat L, const uint32_t
                                                     const uint32_t* rec, const uint32_t* edge_off,
                                                     const uint32_t* edges, uint32_t* counts, uint32_t* item_off,
                                                     uint32_t* item_edges, const unsigned long long* total,
-                                                    unsigned long long* counters, const int4* keys, Scene S) {
+                                                    unsigned long long* counters, const int4* keys, Scene S,
+                                                    const uint8_t* mask, bool any_flags) {
     const uint32_t lane = threadIdx.x & 31, i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t n = MANY ? uint32_t(*S.n_work) : n_host;
     if (FILL && blockIdx.x == 0 && threadIdx.x == 0) item_off[n] = uint32_t(*total);
@@ -1061,7 +1063,7 @@ __global__ void __launch_bounds__(256) k_item_edges(const DLat L, const uint32_t
     const uint32_t* R = rec + size_t(j) * REC_WORDS;
     // Many structures: a structure over a list or buffer limit is redone on
     // its own, and its marching-cubes output may be incomplete.
-    if (R[R_STATE] != ST_SAMPLE || R[R_FLAGS] != 0 || (MANY && S.fail[keys[brick].w])) {
+    if (R[R_STATE] != ST_SAMPLE || (R[R_FLAGS] != 0 && !any_flags) || (MANY && S.fail[keys[brick].w])) {
         if (!FILL && lane == 0) counts[i] = 0;
         return;
     }
@@ -1074,7 +1076,7 @@ __global__ void __launch_bounds__(256) k_item_edges(const DLat L, const uint32_t
         if (k < e1) {
             const uint32_t cell = edges[k] / 3;
             const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
-            mine = uint32_t(min(ex / sub, 1) + 2 * min(ey / sub, 1) + 4 * min(ez / sub, 1)) == sb;
+            mine = uint32_t(min(ex / sub, 1) + 2 * min(ey / sub, 1) + 4 * min(ez / sub, 1)) == sb && (!mask || mask[k]);
         }
         const uint32_t m = __ballot_sync(0xffffffffu, mine);
         if (FILL && mine) item_edges[at + __popc(m & ((1u << lane) - 1u))] = k;
@@ -1666,22 +1668,22 @@ size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uin
 void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const uint32_t* rec, const uint32_t* edge_off,
                        const uint32_t* edges, uint32_t* counts, uint32_t* item_off, uint32_t* item_edges,
                        unsigned long long* tiles, unsigned long long* total, unsigned long long* counters,
-                       cudaStream_t s, const Scene* many, const int4* keys) {
+                       cudaStream_t s, const Scene* many, const int4* keys, const uint8_t* mask, bool all_items) {
     const uint32_t blocks = (n * 32 + 255) / 256;
     const Scene sc = many ? *many : Scene{};
     if (n) {
         COUNT(1);
         if (many) k_item_edges<false, true><<<blocks, 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
-                                                                 item_edges, total, counters, keys, sc);
+                                                                 item_edges, total, counters, keys, sc, mask, mask != nullptr || all_items);
         else k_item_edges<false, false><<<blocks, 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
-                                                              item_edges, total, counters, keys, sc);
+                                                              item_edges, total, counters, keys, sc, mask, mask != nullptr || all_items);
     }
     launch_scan(counts, n, item_off, nullptr, tiles, total, s);
     COUNT(1);
     if (many) k_item_edges<true, true><<<max(blocks, 1u), 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
-                                                                     item_edges, total, counters, keys, sc);
+                                                                     item_edges, total, counters, keys, sc, mask, mask != nullptr || all_items);
     else k_item_edges<true, false><<<max(blocks, 1u), 256, 0, s>>>(L, work, n, rec, edge_off, edges, counts, item_off,
-                                                                  item_edges, total, counters, keys, sc);
+                                                                  item_edges, total, counters, keys, sc, mask, mask != nullptr || all_items);
 }
 
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,

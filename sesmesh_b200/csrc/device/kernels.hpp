@@ -72,11 +72,14 @@ enum : int { REFINE_PLAIN = 0, REFINE_MLP = 1, EDGE_FEATURES = 2 };
 struct MlpDev;
 // Per refinable work item, its edge list (counts, exclusive offsets with the
 // total at item_off[n], edge indices); the largest count goes to
-// counters[CNT_MAXITEM].
+// counters[CNT_MAXITEM].  With a mask, only the edges k with mask[k] != 0.
+// Flagged sub-blocks (sampler lists over their caps) are left out unless
+// all_items or a mask is given (the exact refinement builds its own lists).
 void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const uint32_t* rec, const uint32_t* edge_off,
                        const uint32_t* edges, uint32_t* counts, uint32_t* item_off, uint32_t* item_edges,
                        unsigned long long* tiles, unsigned long long* total, unsigned long long* counters,
-                       cudaStream_t s, const Scene* many = nullptr, const int4* keys = nullptr);
+                       cudaStream_t s, const Scene* many = nullptr, const int4* keys = nullptr,
+                       const uint8_t* mask = nullptr, bool all_items = false);
 void launch_put_total(uint32_t* dst, const unsigned long long* total, cudaStream_t s);
 void launch_copy_count(unsigned long long* dst, const unsigned long long* src, cudaStream_t s);
 // Persistent refinement (or feature pass) over the items' edge lists; grid
@@ -115,6 +118,13 @@ struct ExactOut {
 // item with `region` bytes of shared memory for the item's candidate lists,
 // then the items that did not fit (ovf: count then items, n_items + 1
 // words) with a CTA each.
+// Fast mode's placement on the device (mesh_brick_device, extract.rs:274-365):
+// converged edges placed with their exact attributes into out; need[k] = 1
+// (and *marked counts them) for the edges the exact refinement must take.
+cudaError_t launch_place_fast(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys, uint32_t n_bricks,
+                              const uint32_t* edge_off, const uint32_t* edges, const float2* edge_vals, size_t n_edges,
+                              const float* t, const uint32_t* feat, const float* q, const uint32_t* evals,
+                              const ExactOut& out, uint8_t* need, unsigned long long* marked, cudaStream_t s);
 // out[0] = sum of evals[0..n), out[1] = how many are 0.
 cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long long* out, int sms, cudaStream_t s);
 cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,

@@ -197,11 +197,9 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
         if (rc != SMB_OK) return e->darr.release(), rc;
         rc = smb_batch_new(e->res, &e->batch, err, errlen);
         if (rc != SMB_OK) return rc;
-        if (p->refine == SMB_REFINE_FAST) {
-            if ((rc = smb_resident_set_refinement(e->res, err, errlen)) != SMB_OK) return rc;
-        } else {
-            smb::resident_set_exact_tmin(e->res, P.t_min);
-        }
+        if (p->refine == SMB_REFINE_FAST && (rc = smb_resident_set_refinement(e->res, err, errlen)) != SMB_OK)
+            return rc;
+        smb::resident_set_exact_tmin(e->res, P.t_min);
         e->t_upload = ms_since(t1);
         *out = e.release();
         return SMB_OK;
@@ -237,14 +235,10 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
     if (rc != SMB_OK) return rc;
     rc = smb_batch_new(e->res, &e->batch, err, errlen);
     if (rc != SMB_OK) return rc;
-    if (p->refine == SMB_REFINE_FAST) {
-        rc = smb_resident_set_refinement(e->res, err, errlen);
-        if (rc != SMB_OK) return rc;
-    } else {
-        rc = smb_resident_set_exact(e->res, A.orig.data(), A.circle_ij.data(), A.n_circles(), A.vertex_atoms.data(),
-                                    A.n_vertices(), P.t_min, err, errlen);
-        if (rc != SMB_OK) return rc;
-    }
+    if (p->refine == SMB_REFINE_FAST && (rc = smb_resident_set_refinement(e->res, err, errlen)) != SMB_OK) return rc;
+    rc = smb_resident_set_exact(e->res, A.orig.data(), A.circle_ij.data(), A.n_circles(), A.vertex_atoms.data(),
+                                A.n_vertices(), P.t_min, err, errlen);
+    if (rc != SMB_OK) return rc;
     e->t_upload = ms_since(t1);
     *out = e.release();
     return SMB_OK;
@@ -278,6 +272,10 @@ int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size
                      : smb_refine(e->res, e->batch, &ms, err, errlen);
         if (rc != SMB_OK) return rc;
         t.total += ms;
+        if (e->exact_device) {
+            if ((rc = smb_place_fast(e->res, e->batch, &ms, err, errlen)) != SMB_OK) return rc;
+            t.total += ms;
+        }
     } else if (e->exact_device) {
         double ms = 0;
         if ((rc = smb_refine_exact(e->res, e->batch, &ms, err, errlen)) != SMB_OK) return rc;
@@ -319,8 +317,8 @@ static int fetch_mc(smb_engine* e, char* err, size_t errlen) {
 // measure and grouping there too, and the finished mesh back once.
 // SMB_OK, or an error code; *fallback when the device could not and the
 // host stages should run instead.
-static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long evals, bool* fallback,
-                               double* ms_d2h, char* err, size_t errlen) {
+static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long evals, unsigned long long cpu_edges,
+                               bool* fallback, double* ms_d2h, char* err, size_t errlen) {
     *fallback = false;
     const smb_batch* b = e->batch;
     smb::DeviceMesh in{};
@@ -357,7 +355,7 @@ static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long
     st.components = s.comps.size();
     for (auto& c : s.comps) st.area += c.area, st.volume += c.volume, st.euler += c.euler;
     st.refine_evaluations = evals;
-    st.refine_cpu_edges = 0;
+    st.refine_cpu_edges = cpu_edges;
     st.t_host_refine = 0;
     st.t_assemble = ms_asm;
     st.t_measure = ms_since(t0) - ms_asm;
@@ -388,15 +386,16 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
         st.t_d2h = t_d2h;
         st.t_mesh_stage = ms_since(t_all) - st.t_assemble - st.t_measure;
     };
-    if (e->params.refine != SMB_REFINE_FAST && e->exact_device && e->res->n_bricks) {
-        unsigned long long evals = 0, host_edges = 0;
-        if ((rc = smb_batch_exact_summary(e->batch, &evals, &host_edges)) != SMB_OK)
-            return set_err(err, errlen, "exact refinement summary failed"), rc;
+    if (e->exact_device && e->res->n_bricks) {
+        unsigned long long evals = 0, host_edges = 0, exact_edges = 0;
+        if ((rc = smb_batch_exact_summary(e->batch, &evals, &host_edges, &exact_edges)) != SMB_OK)
+            return set_err(err, errlen, "vertex summary failed"), rc;
         if (host_edges == 0) {
             auto s = std::make_unique<smb_surface>();
             bool fallback = false;
             double ms_d2h = 0;
-            if ((rc = finish_exact_device(e, *s, evals, &fallback, &ms_d2h, err, errlen)) != SMB_OK) return rc;
+            const unsigned long long cpu = e->params.refine == SMB_REFINE_FAST ? exact_edges : 0;
+            if ((rc = finish_exact_device(e, *s, evals, cpu, &fallback, &ms_d2h, err, errlen)) != SMB_OK) return rc;
             if (!fallback) {
                 fill_times(s->stats, ms_d2h);
                 *out = s.release();

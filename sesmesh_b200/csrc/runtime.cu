@@ -1019,53 +1019,108 @@ int smb_resident_set_exact(smb_resident* r, const uint32_t* orig, const uint32_t
     return SMB_OK;
 }
 
+// The exact refinement of the last run's crossing edges (mask: only the
+// edges k with mask[k] != 0; their results into the vertex buffers).
+static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* err, size_t errlen) {
+    smb_device* d = r->dev;
+    cudaStream_t s = d->stream;
+    const size_t ne = b->n_edges;
+    const uint32_t nw = b->n_work;
+    int rc;
+    if ((rc = b->x_ovf.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
+        (rc = b->item_counts.reserve(size_t(nw) * 4, err, errlen)) ||
+        (rc = b->item_off.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
+        (rc = b->item_edges.reserve(ne * 4, err, errlen)) ||
+        (rc = b->tiles.reserve(size_t(scan_tiles_needed(nw)) * 8, err, errlen)))
+        return rc;
+    b->x_block_items = 0;
+    if (!ne || !nw) return SMB_OK;
+    unsigned long long* cnt = b->counters.as<unsigned long long>();
+    CK(cudaMemsetAsync(cnt + CNT_MAXITEM, 0, 8, s));
+    launch_item_edges(r->L, b->work.as<uint32_t>(), nw, b->rec.as<uint32_t>(), b->edge_off.as<uint32_t>(),
+                      b->edges.as<uint32_t>(), b->item_counts.as<uint32_t>(), b->item_off.as<uint32_t>(),
+                      b->item_edges.as<uint32_t>(), b->tiles.as<unsigned long long>(),
+                      b->totals.as<unsigned long long>() + 3, cnt, s, nullptr, nullptr, mask, true);
+    ExactOut out{b->x_pos.as<float>(), b->x_nrm.as<float>(), b->x_atom.as<uint32_t>(), b->x_patch.as<uint8_t>(),
+                 b->x_t.as<float>(), b->x_evals.as<uint32_t>()};
+    cudaError_t e = launch_refine_exact(r->A, r->L, r->xa, r->keys + b->first, b->work.as<uint32_t>(),
+                                        b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->item_off.as<uint32_t>(),
+                                        b->item_edges.as<uint32_t>(), nw, out, b->x_ovf.as<uint32_t>(), cnt,
+                                        d->info.multiprocessors, d->smem_optin, b->x_region, s);
+    if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    uint32_t n_block = 0;
+    CK(cudaMemcpyAsync(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    b->x_block_items = n_block;
+    return SMB_OK;
+}
+
+static int reserve_vertices(smb_batch* b, char* err, size_t errlen) {
+    const size_t ne = b->n_edges;
+    int rc;
+    if ((rc = b->x_pos.reserve(ne * 12, err, errlen)) || (rc = b->x_nrm.reserve(ne * 12, err, errlen)) ||
+        (rc = b->x_atom.reserve(ne * 4, err, errlen)) || (rc = b->x_patch.reserve(ne, err, errlen)) ||
+        (rc = b->x_t.reserve(ne * 4, err, errlen)) || (rc = b->x_evals.reserve(ne * 4, err, errlen)) ||
+        (rc = b->x_sum.reserve(16, err, errlen)))
+        return rc;
+    return SMB_OK;
+}
+
 int smb_refine_exact(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errlen) {
     if (!r || !b || b->res != r) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
     if (!r->exact_ready) return set_err(err, errlen, "smb_resident_set_exact must run first"), SMB_ERR_STATE;
     smb_device* d = r->dev;
     CK(cudaSetDevice(d->index));
     cudaStream_t s = d->stream;
-    const size_t ne = b->n_edges;
-    const uint32_t nw = b->n_work;
     int rc;
-    if ((rc = b->x_pos.reserve(ne * 12, err, errlen)) || (rc = b->x_nrm.reserve(ne * 12, err, errlen)) ||
-        (rc = b->x_atom.reserve(ne * 4, err, errlen)) || (rc = b->x_patch.reserve(ne, err, errlen)) ||
-        (rc = b->e_t.reserve(ne * 4, err, errlen)) || (rc = b->e_evals.reserve(ne * 4, err, errlen)) ||
-        (rc = b->x_ovf.reserve(size_t(nw) * 4 + 4, err, errlen)) || (rc = b->x_sum.reserve(16, err, errlen)) ||
-        (rc = b->item_counts.reserve(size_t(nw) * 4, err, errlen)) ||
-        (rc = b->item_off.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
-        (rc = b->item_edges.reserve(ne * 4, err, errlen)) ||
-        (rc = b->tiles.reserve(size_t(scan_tiles_needed(nw)) * 8, err, errlen)))
-        return rc;
+    if ((rc = reserve_vertices(b, err, errlen))) return rc;
     b->refined_exact = false;
     b->refined = false;
+    b->x_exact_edges = b->n_edges;
     if (ms) *ms = 0;
     cudaEventRecord(b->ev[4], s);
-    if (ne) CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
-    if (ne && nw) {
-        unsigned long long* cnt = b->counters.as<unsigned long long>();
-        CK(cudaMemsetAsync(cnt + CNT_MAXITEM, 0, 8, s));
-        launch_item_edges(r->L, b->work.as<uint32_t>(), nw, b->rec.as<uint32_t>(), b->edge_off.as<uint32_t>(),
-                          b->edges.as<uint32_t>(), b->item_counts.as<uint32_t>(), b->item_off.as<uint32_t>(),
-                          b->item_edges.as<uint32_t>(), b->tiles.as<unsigned long long>(),
-                          b->totals.as<unsigned long long>() + 3, cnt, s);
-        ExactOut out{b->x_pos.as<float>(), b->x_nrm.as<float>(), b->x_atom.as<uint32_t>(), b->x_patch.as<uint8_t>(),
-                     b->e_t.as<float>(), b->e_evals.as<uint32_t>()};
-        cudaError_t e = launch_refine_exact(r->A, r->L, r->xa, r->keys + b->first, b->work.as<uint32_t>(),
-                                            b->edges.as<uint32_t>(), b->edge_vals.as<float2>(),
-                                            b->item_off.as<uint32_t>(), b->item_edges.as<uint32_t>(), nw, out,
-                                            b->x_ovf.as<uint32_t>(), cnt, d->info.multiprocessors, d->smem_optin,
-                                            b->x_region, s);
-        if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
-    }
+    if (b->n_edges) CK(cudaMemsetAsync(b->x_evals.p, 0, b->n_edges * 4, s));
+    if ((rc = exact_pass(r, b, nullptr, err, errlen))) return rc;
     cudaEventRecord(b->ev[5], s);
     CK(cudaStreamSynchronize(s));
     float t = 0;
     cudaEventElapsedTime(&t, b->ev[4], b->ev[5]);
     if (ms) *ms = t;
-    uint32_t n_block = 0;
-    if (ne && nw) CK(cudaMemcpy(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost));
-    b->x_block_items = n_block;
+    b->refined_exact = true;
+    return SMB_OK;
+}
+
+int smb_place_fast(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errlen) {
+    if (!r || !b || b->res != r) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
+    if (!b->refined) return set_err(err, errlen, "smb_refine must run first"), SMB_ERR_STATE;
+    if (!r->exact_ready) return set_err(err, errlen, "smb_resident_set_exact must run first"), SMB_ERR_STATE;
+    smb_device* d = r->dev;
+    CK(cudaSetDevice(d->index));
+    cudaStream_t s = d->stream;
+    const size_t ne = b->n_edges;
+    int rc;
+    if ((rc = reserve_vertices(b, err, errlen)) || (rc = b->x_mask.reserve(ne, err, errlen))) return rc;
+    b->refined_exact = false;
+    if (ms) *ms = 0;
+    cudaEventRecord(b->ev[4], s);
+    ExactOut out{b->x_pos.as<float>(), b->x_nrm.as<float>(), b->x_atom.as<uint32_t>(), b->x_patch.as<uint8_t>(),
+                 b->x_t.as<float>(), b->x_evals.as<uint32_t>()};
+    unsigned long long* marked = b->x_sum.as<unsigned long long>();
+    cudaError_t e = launch_place_fast(r->A, r->L, r->xa, r->keys + b->first, b->n, b->edge_off.as<uint32_t>(),
+                                      b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), ne, b->e_t.as<float>(),
+                                      b->e_feat.as<uint32_t>(), b->e_q.as<float>(), b->e_evals.as<uint32_t>(), out,
+                                      b->x_mask.as<uint8_t>(), marked, s);
+    if (e != cudaSuccess) return set_err(err, errlen, "placement launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    unsigned long long n_marked = 0;
+    CK(cudaMemcpyAsync(&n_marked, marked, 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    b->x_exact_edges = size_t(n_marked);
+    if (n_marked && (rc = exact_pass(r, b, b->x_mask.as<uint8_t>(), err, errlen))) return rc;
+    cudaEventRecord(b->ev[5], s);
+    CK(cudaStreamSynchronize(s));
+    float t = 0;
+    cudaEventElapsedTime(&t, b->ev[4], b->ev[5]);
+    if (ms) *ms = t;
     b->refined_exact = true;
     return SMB_OK;
 }
@@ -1082,20 +1137,21 @@ int smb_batch_vertices(const smb_batch* b, float* positions, float* normals, uin
     if (normals) ok &= cudaMemcpyAsync(normals, b->x_nrm.p, ne * 12, cudaMemcpyDeviceToHost, s) == cudaSuccess;
     if (atoms) ok &= cudaMemcpyAsync(atoms, b->x_atom.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
     if (patches) ok &= cudaMemcpyAsync(patches, b->x_patch.p, ne, cudaMemcpyDeviceToHost, s) == cudaSuccess;
-    if (t) ok &= cudaMemcpyAsync(t, b->e_t.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
-    if (evals) ok &= cudaMemcpyAsync(evals, b->e_evals.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    if (t) ok &= cudaMemcpyAsync(t, b->x_t.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+    if (evals) ok &= cudaMemcpyAsync(evals, b->x_evals.p, ne * 4, cudaMemcpyDeviceToHost, s) == cudaSuccess;
     ok &= cudaStreamSynchronize(s) == cudaSuccess;
     return ok ? SMB_OK : SMB_ERR_CUDA;
 }
 
-int smb_batch_exact_summary(const smb_batch* b, unsigned long long* evaluations, unsigned long long* host_edges) {
+int smb_batch_exact_summary(const smb_batch* b, unsigned long long* evaluations, unsigned long long* host_edges,
+                            unsigned long long* exact_edges) {
     if (!b || !b->refined_exact) return SMB_ERR_STATE;
     smb_device* d = b->res->dev;
     if (cudaSetDevice(d->index) != cudaSuccess) return SMB_ERR_CUDA;
     unsigned long long out[2] = {0, 0};
     if (b->n_edges) {
         unsigned long long* sum = b->x_sum.as<unsigned long long>();
-        if (!sum || launch_exact_summary(b->e_evals.as<uint32_t>(), b->n_edges, sum, d->info.multiprocessors,
+        if (!sum || launch_exact_summary(b->x_evals.as<uint32_t>(), b->n_edges, sum, d->info.multiprocessors,
                                          d->stream) != cudaSuccess ||
             cudaMemcpyAsync(out, sum, 16, cudaMemcpyDeviceToHost, d->stream) != cudaSuccess ||
             cudaStreamSynchronize(d->stream) != cudaSuccess)
@@ -1103,6 +1159,7 @@ int smb_batch_exact_summary(const smb_batch* b, unsigned long long* evaluations,
     }
     if (evaluations) *evaluations = out[0];
     if (host_edges) *host_edges = out[1];
+    if (exact_edges) *exact_edges = b->x_exact_edges;
     return SMB_OK;
 }
 

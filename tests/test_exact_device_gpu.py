@@ -1,4 +1,5 @@
-"""Exact mode with the f64 vertex refinement on the device (smb_refine_exact).
+"""Vertex refinement, placement and the mesh's finish on the device
+(smb_refine_exact in exact mode, smb_place_fast in fast mode).
 
 The device restates the host's exact refinement operation by operation, so
 the mesh must be byte-identical whichever side refines: OBJ bytes, counts,
@@ -6,7 +7,10 @@ area, volume and evaluation counts are compared for equality with the
 host-refined mesh (and, through test_surface_gpu.py, with the CPU oracle).
 The device must refine nearly every edge itself, and its whole-block path
 (taken by sub-blocks whose lists exceed a warp's share of shared memory)
-must give the same vertices as the warp path.
+must give the same vertices as the warp path.  In fast mode the device's
+placement of the f32 roots (and exact refinement of the edges they do not
+settle) must equal the host placement byte for byte, with and without the
+learned warm start.
 """
 import ctypes as C
 
@@ -36,10 +40,13 @@ def _cases():
     return out
 
 
-def _mesh(spheres, probe, h, on_device, region=None, brick=10):
+def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", warm=None):
     from sesmesh_b200 import surface as S
     from sesmesh_b200.native import lib
-    eng = S.SurfaceEngine(spheres, S.SurfaceParams.ses(probe).with_spacing(h).with_brick_size(brick))
+    eng = S.SurfaceEngine(spheres, S.SurfaceParams.ses(probe).with_spacing(h).with_brick_size(brick)
+                          .with_refine(refine))
+    if warm is not None:
+        eng.set_warm_start(warm)
     eng.set_exact_on_device(on_device)
     if region is not None:
         assert lib().smb_batch_set_exact_region(lib().smb_engine_batch(eng.h), C.c_size_t(region)) == 0
@@ -76,3 +83,26 @@ def test_block_path_equals_warp_path(brick):
     for k in KEYS + ("refine_cpu_edges",):
         assert st_w[k] == st_b[k], (k, st_w[k], st_b[k])
     assert obj_w == obj_b
+
+
+@pytest.mark.parametrize("case", [c for c in _cases() if c[0] in ("chain5", "globule330@0.5", "globule2800@0.25",
+                                                                   "globule330@1", "stall4")], ids=lambda c: c[0])
+def test_fast_device_placement_equals_host(case):
+    name, spheres, probe, h = case
+    obj_d, st_d = _mesh(spheres, probe, h, True, refine="fast")
+    obj_h, st_h = _mesh(spheres, probe, h, False, refine="fast")
+    for k in KEYS + ("refine_cpu_edges",):
+        assert st_d[k] == st_h[k], (k, st_d[k], st_h[k])
+    assert obj_d == obj_h
+
+
+def test_fast_device_placement_with_warm_start_equals_host():
+    from sesmesh_b200 import native, warm_start, workloads
+    from sesmesh_b200 import surface as S
+    g = workloads.globule2800()
+    mlp = native.Mlp(S._device(0), warm_start.load())
+    obj_d, st_d = _mesh(g["spheres"], 1.4, 0.25, True, refine="fast", warm=mlp)
+    obj_h, st_h = _mesh(g["spheres"], 1.4, 0.25, False, refine="fast", warm=mlp)
+    for k in KEYS + ("refine_cpu_edges",):
+        assert st_d[k] == st_h[k], (k, st_d[k], st_h[k])
+    assert obj_d == obj_h
