@@ -61,11 +61,15 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen);
  * refinement evaluates them), clamped to -band beyond it inside.  For the
  * distance of mesh vertices to the surface. */
 int smb_engine_field(const smb_engine* e, const double* points, size_t n, double* values);
-/* Exact mode: vertex refinement in f64 on the device (smb_refine_exact;
- * the default, on = 1) or on the host threads (on = 0, as the reference).
- * Both give the same mesh bytes; edges the device leaves are refined on the
- * host either way (stats.refine_cpu_edges). */
+/* Vertex refinement (exact mode, smb_refine_exact) and placement (fast
+ * mode, smb_place_fast) on the device, then assembly, validation, measure
+ * and grouping there too (the default, on = 1); or all of these on the
+ * host threads (on = 0, as the reference).  Both give the same mesh bytes;
+ * a mesh with edges the device leaves is finished on the host. */
 int smb_engine_set_exact_device(smb_engine* e, int on);
+/* Why the engine's last mesh was finished on the host threads rather than
+ * on the device ("" when it was not; valid until the next mesh). */
+const char* smb_engine_note(const smb_engine* e);
 /* The engine's device batch (sizes, counters, operation counts). */
 smb_batch* smb_engine_batch(smb_engine* e);
 /* Learned warm start of fast mode (no counterpart in the reference): the

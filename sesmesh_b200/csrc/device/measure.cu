@@ -37,7 +37,6 @@ namespace {
 
 constexpr uint64_t EMPTY = ~0ull;
 constexpr uint32_t SUM_CHUNK = 1u << 14;  // triangles per area/volume chunk, as the host
-constexpr int CHUNK_COMPS = 16;           // components one chunk may hold on the device
 
 __device__ __forceinline__ uint64_t mix64(uint64_t x) {  // splitmix64 finaliser
     x ^= x >> 30;
@@ -231,53 +230,37 @@ struct Partial {
     double a, v;
 };
 
-__global__ void k_chunk_partials(const float* pos, const uint32_t* tris, uint32_t nt, const uint32_t* id,
-                                 Partial* out, unsigned long long* n_out, unsigned long long* overflow) {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n_chunks = (nt + SUM_CHUNK - 1) / SUM_CHUNK;
-    if (c >= n_chunks) return;
-    double o[3] = {double(pos[0]), double(pos[1]), double(pos[2])};
-    Partial acc[CHUNK_COMPS];
-    int na = 0;
-    const uint32_t t1 = min(nt, (c + 1) * SUM_CHUNK);
-    for (uint32_t t = c * SUM_CHUNK; t < t1; t++) {
-        const uint32_t* T = tris + 3 * size_t(t);
-        uint32_t comp = id[T[0]];
+// Segments of the triangles sorted by component (stably: triangle order
+// within a component): a new segment where the component or the 16,384-
+// triangle chunk changes.  flag[p] = 1 at a segment's first position.
+__global__ void k_segment_flags(const uint32_t* comp, const uint32_t* perm, uint32_t nt, uint32_t* flag) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nt) return;
+    flag[p] = (p == 0 || comp[p] != comp[p - 1] || (perm[p] / SUM_CHUNK) != (perm[p - 1] / SUM_CHUNK)) ? 1u : 0u;
+}
+
+// Thread per segment: its triangles' area and volume summed in triangle
+// order (one (component, chunk) partial of the host's sums).
+__global__ void k_segment_partials(const float* pos, const uint32_t* tris, const uint32_t* comp,
+                                   const uint32_t* perm, uint32_t nt, const uint32_t* start, uint32_t n_seg,
+                                   Partial* out, uint32_t* seg_comp) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_seg) return;
+    const double o[3] = {double(pos[0]), double(pos[1]), double(pos[2])};
+    const uint32_t p0 = start[s], p1 = s + 1 < n_seg ? start[s + 1] : nt;
+    Partial acc{comp[p0], perm[p0] / SUM_CHUNK, 0ull, 0.0, 0.0};
+    for (uint32_t p = p0; p < p1; p++) {
         double a, v;
-        area_volume(pos, T, o, a, v);
-        int e = -1;
-        for (int q = 0; q < na; q++)
-            if (acc[q].comp == comp) {
-                e = q;
-                break;
-            }
-        if (e < 0) {
-            if (na == CHUNK_COMPS) {
-                atomicAdd(overflow, 1ull);
-                return;
-            }
-            e = na++;
-            acc[e] = Partial{comp, c, 0ull, 0.0, 0.0};
-        }
-        acc[e].t++, acc[e].a += a, acc[e].v += v;
+        area_volume(pos, tris + 3 * size_t(perm[p]), o, a, v);
+        acc.t++, acc.a += a, acc.v += v;
     }
-    unsigned long long base = atomicAdd(n_out, (unsigned long long)na);
-    for (int q = 0; q < na; q++) out[base + q] = acc[q];
+    out[s] = acc;
+    seg_comp[s] = acc.comp;
 }
 
-__global__ void k_iota(uint32_t* v, uint32_t n) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) v[i] = i;
-}
-
-// key[i] = the chunk (by_comp = false) or component of partial idx[i].
-__global__ void k_part_keys(const Partial* parts, const uint32_t* idx, uint32_t n, uint32_t* key, bool by_comp) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) key[i] = by_comp ? parts[idx[i]].comp : parts[idx[i]].chunk;
-}
-
-// Partials sorted by (component, chunk): each component sums its chunks in
-// chunk order (the host's order).
+// Partials in (component, chunk) order (sorted_idx: their order, or null
+// for the identity): each component sums its chunks in chunk order (the
+// host's order).
 __global__ void k_component_sums(const Partial* parts, const uint32_t* sorted_idx, uint32_t n_parts,
                                  const uint32_t* first, uint32_t n_comp, unsigned long long* tris_out, double* area,
                                  double* volume) {
@@ -286,7 +269,7 @@ __global__ void k_component_sums(const Partial* parts, const uint32_t* sorted_id
     unsigned long long t = 0;
     double a = 0.0, v = 0.0;
     for (uint32_t i = first[c]; i < first[c + 1]; i++) {
-        const Partial& p = parts[sorted_idx[i]];
+        const Partial& p = parts[sorted_idx ? sorted_idx[i] : i];
         t += p.t, a += p.a, v += p.v;
     }
     tris_out[c] = t, area[c] = a, volume[c] = v;
@@ -442,14 +425,11 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
     char e[256];
     auto R = [&](DBuf& b, size_t bytes) { return b.reserve(std::max<size_t>(bytes, 16), e, sizeof e) == 0; };
     const uint64_t ecap = pow2_at_least(uint64_t(nt) * 3 + 16), dcap = pow2_at_least(uint64_t(nt) * 2 + 16);
-    const uint32_t n_chunks = uint32_t((nt + SUM_CHUNK - 1) / SUM_CHUNK);
-    const size_t max_parts = size_t(n_chunks) * CHUNK_COMPS;
     if (!R(S.tris_out, nt * 12) ||
         !R(S.keys, ecap * 8) || !R(S.cnt, ecap * 8) || !R(S.dup, dcap * 4) || !R(S.parent, nv * 4) ||
         !R(S.flag, nv * 4) || !R(S.cid, nv * 4) || !R(S.id, nv * 4) || !R(S.counters, 64) ||
-        !R(S.parts, max_parts * sizeof(Partial)) || !R(S.pkey, max_parts * 4) || !R(S.pidx, max_parts * 4) ||
-        !R(S.pkey2, max_parts * 4) || !R(S.pidx2, max_parts * 4) || !R(S.tkey, nt * 4) || !R(S.tidx, nt * 4) ||
-        !R(S.tkey2, nt * 4) || !R(S.tidx2, nt * 4) || !R(S.tiles, size_t(scan_tiles_needed(uint32_t(nv))) * 8 + 64)) {
+        !R(S.tkey, nt * 4) || !R(S.tidx, nt * 4) ||
+        !R(S.tkey2, nt * 4) || !R(S.tidx2, nt * 4) || !R(S.tiles, size_t(scan_tiles_needed(uint32_t(std::max(nv, nt)))) * 8 + 64)) {
         if (msg) *msg = std::string("device memory for the measure: ") + e;
         return false;
     }
@@ -512,22 +492,6 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
     if (nt)
         k_euler_edges<<<blocks(ecap), 256, 0, s>>>(S.keys.as<unsigned long long>(), ecap, id,
                                                    S.comp_e.as<unsigned long long>());
-    // Area and volume: chunk partials, stably sorted by component (the
-    // partials of one component stay in chunk order after a stable sort by
-    // chunk, then by component).
-    unsigned long long n_parts = 0, overflow = 0;
-    if (nt) {
-        k_chunk_partials<<<blocks(n_chunks), 256, 0, s>>>(pos, tris, uint32_t(nt), id, S.parts.as<Partial>(), cnt + 2,
-                                                          cnt + 3);
-        MCK(cudaMemcpyAsync(&n_parts, cnt + 2, 8, cudaMemcpyDeviceToHost, s));
-        MCK(cudaMemcpyAsync(&overflow, cnt + 3, 8, cudaMemcpyDeviceToHost, s));
-        MCK(cudaStreamSynchronize(s));
-        if (overflow) {
-            if (msg) *msg = "a triangle chunk holds more components than the device measure keeps";
-            return false;
-        }
-    }
-    const uint32_t np = uint32_t(n_parts);
     auto sort_pairs = [&](const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout, uint32_t n,
                           unsigned bits) -> bool {
         size_t tmp = 0;
@@ -538,26 +502,42 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         return cub::DeviceRadixSort::SortPairs(S.cub.p, tmp, kin, kout, vin, vout, int(n), 0, int(bits), s) ==
                cudaSuccess;
     };
+    // Triangles stably sorted by component: the regrouping's order, and the
+    // segments of the area/volume sums.
+    if (nt) {
+        k_triangle_keys<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), id, S.tkey.as<uint32_t>(), S.tidx.as<uint32_t>());
+        if (!sort_pairs(S.tkey.as<uint32_t>(), S.tkey2.as<uint32_t>(), S.tidx.as<uint32_t>(), S.tidx2.as<uint32_t>(),
+                        uint32_t(nt), bits_for(nc))) {
+            if (msg) *msg = "triangle sort failed";
+            return false;
+        }
+    }
+    // Area and volume: one partial per (component, 16,384-triangle chunk)
+    // summed in triangle order, then each component's partials in chunk
+    // order (the host's operations in the host's order).  The sorted
+    // triangles list the segments in (component, chunk) order.
+    unsigned long long n_seg = 0;
+    if (nt) {
+        uint32_t* flag = S.tkey.as<uint32_t>();   // free once sorted
+        uint32_t* start = S.tidx.as<uint32_t>();  // idem
+        k_segment_flags<<<blocks(nt), 256, 0, s>>>(S.tkey2.as<uint32_t>(), S.tidx2.as<uint32_t>(), uint32_t(nt), flag);
+        launch_scan(flag, uint32_t(nt), nullptr, start, S.tiles.as<unsigned long long>(), cnt + 2, s);
+        MCK(cudaMemcpyAsync(&n_seg, cnt + 2, 8, cudaMemcpyDeviceToHost, s));
+        MCK(cudaStreamSynchronize(s));
+    }
+    const uint32_t np = uint32_t(n_seg);
     if (np) {
-        // Partials by chunk, then stably by component: each component's
-        // partials in chunk order.
+        if (!R(S.parts, size_t(np) * sizeof(Partial)) || !R(S.pkey, size_t(np) * 4)) {
+            if (msg) *msg = std::string("device memory for the measure: ") + e;
+            return false;
+        }
         Partial* parts = S.parts.as<Partial>();
-        k_iota<<<blocks(np), 256, 0, s>>>(S.pidx.as<uint32_t>(), np);
-        k_part_keys<<<blocks(np), 256, 0, s>>>(parts, S.pidx.as<uint32_t>(), np, S.pkey2.as<uint32_t>(), false);
-        if (!sort_pairs(S.pkey2.as<uint32_t>(), S.pkey.as<uint32_t>(), S.pidx.as<uint32_t>(), S.pidx2.as<uint32_t>(),
-                        np, bits_for(n_chunks))) {
-            if (msg) *msg = "partial sort failed";
-            return false;
-        }
-        k_part_keys<<<blocks(np), 256, 0, s>>>(parts, S.pidx2.as<uint32_t>(), np, S.pkey2.as<uint32_t>(), true);
-        if (!sort_pairs(S.pkey2.as<uint32_t>(), S.pkey.as<uint32_t>(), S.pidx2.as<uint32_t>(), S.pidx.as<uint32_t>(),
-                        np, bits_for(nc))) {
-            if (msg) *msg = "partial sort failed";
-            return false;
-        }
+        k_segment_partials<<<blocks(np), 256, 0, s>>>(pos, tris, S.tkey2.as<uint32_t>(), S.tidx2.as<uint32_t>(),
+                                                      uint32_t(nt), S.tidx.as<uint32_t>(), np, parts,
+                                                      S.pkey.as<uint32_t>());
         k_first_of_component<<<blocks(uint64_t(np) + 1), 256, 0, s>>>(S.pkey.as<uint32_t>(), np,
                                                                         S.first.as<uint32_t>(), nc);
-        k_component_sums<<<blocks(nc), 256, 0, s>>>(parts, S.pidx.as<uint32_t>(), np, S.first.as<uint32_t>(), nc,
+        k_component_sums<<<blocks(nc), 256, 0, s>>>(parts, nullptr, np, S.first.as<uint32_t>(), nc,
                                                     S.comp_t.as<unsigned long long>(), S.area.as<double>(),
                                                     S.volume.as<double>());
     } else if (nc) {
@@ -566,16 +546,9 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         MCK(cudaMemsetAsync(S.volume.p, 0, size_t(nc) * 8, s));
     }
     // Triangles regrouped by component, relative order kept.
-    if (nt) {
-        k_triangle_keys<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), id, S.tkey.as<uint32_t>(), S.tidx.as<uint32_t>());
-        if (!sort_pairs(S.tkey.as<uint32_t>(), S.tkey2.as<uint32_t>(), S.tidx.as<uint32_t>(), S.tidx2.as<uint32_t>(),
-                        uint32_t(nt), bits_for(nc))) {
-            if (msg) *msg = "triangle sort failed";
-            return false;
-        }
+    if (nt)
         k_gather_triangles<<<blocks(nt), 256, 0, s>>>(tris, S.tidx2.as<uint32_t>(), uint32_t(nt),
                                                       S.tris_out.as<uint32_t>());
-    }
     // Results to the host.
     std::vector<unsigned long long> cv(nc), ct(nc), ce(nc);
     std::vector<double> ca(nc), cvol(nc);

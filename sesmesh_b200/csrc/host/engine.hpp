@@ -40,6 +40,7 @@ struct smb_engine {
     const smb_mlp* warm = nullptr;  // warm start of fast-mode refinement
     bool exact_device = true;       // exact mode: f64 refinement on the device (else on the host threads)
     smbh::MeshOut exact_out;        // its vertices, at their edge index
+    std::string note;               // why the last mesh was finished on the host, if it was
     std::vector<uint32_t> exact_evals;
     smb::MeasureScratch measure;    // device buffers of the validation and measure
     // Warm-start training rows of the last device run.

@@ -341,6 +341,7 @@ static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long
     int r = smb::finish_on_device(e->dev, in, &s.view, &s.block, s.comps, &bad, e->measure, &msg, &ms_asm);
     if (r == 1) {
         *fallback = true;
+        e->note = "device finish declined: " + msg;
         return SMB_OK;
     }
     if (r == 2) return set_err(err, errlen, "%s", msg.c_str()), SMB_ERR_STATE;
@@ -386,10 +387,12 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
         st.t_d2h = t_d2h;
         st.t_mesh_stage = ms_since(t_all) - st.t_assemble - st.t_measure;
     };
+    e->note.clear();
     if (e->exact_device && e->res->n_bricks) {
         unsigned long long evals = 0, host_edges = 0, exact_edges = 0;
         if ((rc = smb_batch_exact_summary(e->batch, &evals, &host_edges, &exact_edges)) != SMB_OK)
             return set_err(err, errlen, "vertex summary failed"), rc;
+        if (host_edges) e->note = std::to_string(host_edges) + " edges left to the host";
         if (host_edges == 0) {
             auto s = std::make_unique<smb_surface>();
             bool fallback = false;
@@ -451,6 +454,8 @@ int smb_engine_field(const smb_engine* e, const double* points, size_t n, double
     });
     return SMB_OK;
 }
+
+const char* smb_engine_note(const smb_engine* e) { return e ? e->note.c_str() : ""; }
 
 int smb_engine_set_exact_device(smb_engine* e, int on) {
     if (!e) return SMB_ERR_ARG;

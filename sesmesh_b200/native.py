@@ -162,6 +162,7 @@ SIGNATURES = {
     "smb_engine_mesh": (C.c_int, [_vp, C.POINTER(_vp), _cp, _sz]),
     "smb_engine_set_warm_start": (C.c_int, [_vp, _vp]),
     "smb_engine_set_exact_device": (C.c_int, [_vp, C.c_int]),
+    "smb_engine_note": (C.c_char_p, [_vp]),
     "smb_engine_field": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(C.c_double)]),
     "smb_engine_warm_start_rows": (C.c_int, [_vp, _fp, _fp, _sz, C.POINTER(_sz), _cp, _sz]),
     "smb_surface_free": (None, [_vp]),

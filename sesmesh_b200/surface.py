@@ -231,6 +231,10 @@ class SurfaceEngine:
                C.create_string_buffer(8))
         return out
 
+    def note(self):
+        """Why the last mesh was finished on the host ("" when it was not)."""
+        return lib().smb_engine_note(self.h).decode()
+
     def set_exact_on_device(self, on=True):
         """Exact mode: refine vertices in f64 on the device (default) or on
         the host threads (as the reference); the mesh bytes are the same."""
