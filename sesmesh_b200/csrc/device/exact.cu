@@ -34,6 +34,7 @@ constexpr int X_MAX_BISECT = 64;  // extract.rs:33
 constexpr double X_PRUNE = 1e-9;  // margin of the candidates' pruning keys
 constexpr uint32_t XF_SOLVENT = 0, XF_BEYOND = 1, XF_SPHERE = 2, XF_CIRCLE = 3, XF_VERTEX = 4;
 constexpr int X_WARPS = 4;
+constexpr size_t EXACT_SLAB = size_t(256) << 10;  // bytes of a warp's global list region
 
 // List sizes of one ball.
 struct XCounts {
@@ -523,52 +524,48 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
     out.evals[k] = evals;
 }
 
-// Persistent CTAs of X_WARPS warps.  Narrow (WIDE = false): each warp claims
-// work items from counters[CNT_QUEUE], builds the item's ball in its own
-// region of `region` bytes and refines the item's edges lane per edge; an
-// item whose lists do not fit goes to ovf (ovf[0] = count).  WIDE: each CTA
-// claims the overflowed items from counters[CNT_XQUEUE] and works on one at
-// a time with all its threads and all its dynamic shared memory.
-template <bool WIDE>
+// Persistent CTAs of X_WARPS warps; each warp claims a work item, builds
+// the item's ball in its own region and refines the item's edges lane per
+// edge.  SLAB = false: the region is `region` bytes of shared memory, items
+// come from counters[CNT_QUEUE] over all items, and an item whose lists do
+// not fit goes to ovf (ovf[0] = count, then the items).  SLAB = true: the
+// region is `region` bytes of a global slab per warp (read back through
+// L1), items come from ovf through counters[CNT_XQUEUE], and an item that
+// does not fit either stays with the host (*left counts them).
+template <bool SLAB>
 __global__ void __launch_bounds__(32 * X_WARPS, 1) k_refine_exact(DArr A, DLat L, ExactAttr X, const int4* keys,
                                                                const uint32_t* work, const uint32_t* edges,
                                                                const float2* edge_vals, const uint32_t* item_off,
                                                                const uint32_t* item_edges, uint32_t n_items,
                                                                ExactOut out, size_t region, uint32_t* ovf,
+                                                               unsigned char* slab, unsigned int* left,
                                                                unsigned long long* counters) {
     extern __shared__ __align__(16) unsigned char xs[];
     __shared__ uint32_t sh_cnt[X_WARPS][8];
-    __shared__ uint32_t sh_item;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t tid = WIDE ? threadIdx.x : lane, T = WIDE ? blockDim.x : 32u;
-    unsigned char* mine = xs + (WIDE ? size_t(0) : size_t(warp) * region);
-    uint32_t* cnt = sh_cnt[WIDE ? 0 : warp];
-    unsigned int* queue = reinterpret_cast<unsigned int*>(&counters[WIDE ? CNT_XQUEUE : CNT_QUEUE]);
-    const uint32_t n_ovf = WIDE ? ovf[0] : 0u;
+    unsigned char* mine = SLAB ? slab + (size_t(blockIdx.x) * X_WARPS + warp) * region : xs + size_t(warp) * region;
+    uint32_t* cnt = sh_cnt[warp];
+    unsigned int* queue = reinterpret_cast<unsigned int*>(&counters[SLAB ? CNT_XQUEUE : CNT_QUEUE]);
+    const uint32_t n_claim = SLAB ? ovf[0] : n_items;
     for (;;) {
-        uint32_t i;
-        if constexpr (WIDE) {
-            __syncthreads();
-            if (threadIdx.x == 0) sh_item = atomicAdd(queue, 1u);
-            __syncthreads();
-            if (sh_item >= n_ovf) break;
-            i = ovf[1 + sh_item];
-        } else {
-            i = 0;
-            if (lane == 0) i = atomicAdd(queue, 1u);
-            i = __shfl_sync(0xffffffffu, i, 0);
-            if (i >= n_items) break;
-        }
+        uint32_t q = 0;
+        if (lane == 0) q = atomicAdd(queue, 1u);
+        q = __shfl_sync(0xffffffffu, q, 0);
+        if (q >= n_claim) break;
+        const uint32_t i = SLAB ? ovf[1 + q] : q;
         const uint32_t a0 = item_off[i], a1 = item_off[i + 1];
         if (a0 == a1) continue;
         const uint32_t j = work[i];
         const int4 key = keys[j >> 3];
         XView v;
-        if (!x_ball<WIDE>(A, L, key, j, mine, region, cnt, tid, T, v)) {
-            if (!WIDE && lane == 0) ovf[1 + atomicAdd(&ovf[0], 1u)] = i;
+        if (!x_ball<false>(A, L, key, j, mine, region, cnt, lane, 32u, v)) {
+            if (lane == 0) {
+                if (SLAB) atomicAdd(left, 1u);
+                else ovf[1 + atomicAdd(&ovf[0], 1u)] = i;
+            }
             continue;
         }
-        for (uint32_t e = a0 + tid; e < a1; e += T) {
+        for (uint32_t e = a0 + lane; e < a1; e += 32) {
             const uint32_t k = item_edges[e];
             x_edge(v, A, L, X, key, k, edges[k], edge_vals[k], out);
         }
@@ -682,20 +679,26 @@ cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long 
     return cudaGetLastError();
 }
 
+size_t exact_slab_bytes(int sms) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_exact<true>, 32 * X_WARPS, 0);
+    return size_t(std::max(sms, 1)) * size_t(std::max(per_sm, 1)) * X_WARPS * EXACT_SLAB;
+}
+
 cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                 const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
-                                const ExactOut& out, uint32_t* ovf, unsigned long long* counters, int sms,
-                                size_t smem_limit, size_t region, cudaStream_t s) {
+                                const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
+                                unsigned long long* counters, int sms, size_t region, cudaStream_t s) {
     cudaError_t e;
     if ((e = cudaMemsetAsync(&counters[CNT_QUEUE], 0, 8, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&counters[CNT_XQUEUE], 0, 8, s)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(ovf, 0, 4, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(ovf, 0, 8, s)) != cudaSuccess) return e;
     if (!n_items) return cudaSuccess;
     region = (region + 15) & ~size_t(15);
     const size_t narrow = size_t(X_WARPS) * region;
     auto kn = k_refine_exact<false>;
-    auto kw = k_refine_exact<true>;
+    auto kg = k_refine_exact<true>;
     if ((e = cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(narrow))) != cudaSuccess)
         return e;
     int per_sm = 0;
@@ -704,16 +707,18 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
     const uint32_t warps = (n_items + X_WARPS - 1) / X_WARPS;
     const uint32_t grid = std::min<uint32_t>(warps, uint32_t(sms * std::max(per_sm, 1)));
     count_launches(2);
+    // ovf[0]: items over the shared region, ovf[1..]: those items; the word
+    // after the list counts the items over a slab (left to the host).
+    unsigned int* left = reinterpret_cast<unsigned int*>(ovf) + 1 + n_items;
+    if ((e = cudaMemsetAsync(left, 0, 4, s)) != cudaSuccess) return e;
     kn<<<grid, 32 * X_WARPS, narrow, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                          region, ovf, counters);
-    // The overflowed items: one CTA per SM, all of the CTA's shared memory.
-    cudaFuncAttributes fa{};
-    if ((e = cudaFuncGetAttributes(&fa, kw)) != cudaSuccess) return e;
-    const size_t wide = (smem_limit > fa.sharedSizeBytes ? smem_limit - fa.sharedSizeBytes : 0) & ~size_t(15);
-    if ((e = cudaFuncSetAttribute(kw, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wide))) != cudaSuccess)
-        return e;
-    kw<<<uint32_t(std::max(sms, 1)), 32 * X_WARPS, wide, s>>>(A, L, X, keys, work, edges, edge_vals, item_off,
-                                                              item_edges, n_items, out, wide, ovf, counters);
+                                          region, ovf, nullptr, left, counters);
+    // The overflowed items: a warp each, lists in a global slab.
+    const uint32_t slabs = uint32_t(slab_bytes / EXACT_SLAB);
+    const uint32_t grid_g = std::max<uint32_t>(1, slabs / X_WARPS);
+    if (!slab || !grid_g) return cudaErrorInvalidValue;
+    kg<<<grid_g, 32 * X_WARPS, 0, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
+                                       EXACT_SLAB, ovf, slab, left, counters);
     return cudaGetLastError();
 }
 

@@ -114,10 +114,6 @@ struct ExactOut {
     float* t;
     uint32_t* evals;
 };
-// f64 refinement of the work items' edge lists (k_item_edges): a warp per
-// item with `region` bytes of shared memory for the item's candidate lists,
-// then the items that did not fit (ovf: count then items, n_items + 1
-// words) with a CTA each.
 // Fast mode's placement on the device (mesh_brick_device, extract.rs:274-365):
 // converged edges placed with their exact attributes into out; need[k] = 1
 // (and *marked counts them) for the edges the exact refinement must take.
@@ -127,11 +123,18 @@ cudaError_t launch_place_fast(const DArr& A, const DLat& L, const ExactAttr& X, 
                               const ExactOut& out, uint8_t* need, unsigned long long* marked, cudaStream_t s);
 // out[0] = sum of evals[0..n), out[1] = how many are 0.
 cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long long* out, int sms, cudaStream_t s);
+// f64 refinement of the work items' edge lists (k_item_edges): a warp per
+// item with `region` bytes of shared memory for the item's candidate lists,
+// then the items that did not fit with a warp each and a 256 KiB list slab
+// in global memory (slab: exact_slab_bytes(sms) bytes).  ovf: n_items + 2
+// words (overflow count, items, then the count of items over a slab, whose
+// edges keep evals = 0).
+size_t exact_slab_bytes(int sms);
 cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                 const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
-                                const ExactOut& out, uint32_t* ovf, unsigned long long* counters, int sms,
-                                size_t smem_limit, size_t region, cudaStream_t s);
+                                const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
+                                unsigned long long* counters, int sms, size_t region, cudaStream_t s);
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);
 void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, unsigned long long* tiles,
                  unsigned long long* total, cudaStream_t s);

@@ -1027,7 +1027,8 @@ static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* 
     const size_t ne = b->n_edges;
     const uint32_t nw = b->n_work;
     int rc;
-    if ((rc = b->x_ovf.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
+    const size_t slab = exact_slab_bytes(d->info.multiprocessors);
+    if ((rc = b->x_ovf.reserve(size_t(nw) * 4 + 8, err, errlen)) || (rc = b->x_slab.reserve(slab, err, errlen)) ||
         (rc = b->item_counts.reserve(size_t(nw) * 4, err, errlen)) ||
         (rc = b->item_off.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
         (rc = b->item_edges.reserve(ne * 4, err, errlen)) ||
@@ -1045,8 +1046,9 @@ static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* 
                  b->x_t.as<float>(), b->x_evals.as<uint32_t>()};
     cudaError_t e = launch_refine_exact(r->A, r->L, r->xa, r->keys + b->first, b->work.as<uint32_t>(),
                                         b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->item_off.as<uint32_t>(),
-                                        b->item_edges.as<uint32_t>(), nw, out, b->x_ovf.as<uint32_t>(), cnt,
-                                        d->info.multiprocessors, d->smem_optin, b->x_region, s);
+                                        b->item_edges.as<uint32_t>(), nw, out, b->x_ovf.as<uint32_t>(),
+                                        b->x_slab.as<unsigned char>(), slab, cnt, d->info.multiprocessors,
+                                        b->x_region, s);
     if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     uint32_t n_block = 0;
     CK(cudaMemcpyAsync(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost, s));

@@ -92,7 +92,7 @@ struct smb_batch {
     smb::DBuf item_counts, item_off, item_edges;  // per sampled sub-block edge lists
     // Vertices refined or placed on the device: position, normal, atom, patch,
     // t, evaluations; overflowed items, summary words, fast-mode exact mask.
-    smb::DBuf x_pos, x_nrm, x_atom, x_patch, x_t, x_evals, x_ovf, x_sum, x_mask;
+    smb::DBuf x_pos, x_nrm, x_atom, x_patch, x_t, x_evals, x_ovf, x_sum, x_mask, x_slab;
     bool refined_exact = false;
     size_t x_exact_edges = 0;  // edges the exact refinement took in the last pass
     size_t x_block_items = 0;  // items of the last exact pass refined by a whole block
@@ -104,6 +104,6 @@ struct smb_batch {
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
                 &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &item_counts, &item_off, &item_edges,
-                &x_pos, &x_nrm, &x_atom, &x_patch, &x_t, &x_evals, &x_ovf, &x_sum, &x_mask};
+                &x_pos, &x_nrm, &x_atom, &x_patch, &x_t, &x_evals, &x_ovf, &x_sum, &x_mask, &x_slab};
     }
 };
