@@ -39,6 +39,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # FP32 lanes x SMs x max clock, one operation per lane per cycle: the bound
 # of kernels that may not contract multiply-adds (bit-exact f32).
 FP32_NOFMA_TOPS = 148 * 128 * 1.965e9 / 1e12
+FP64_NOFMA_TOPS = 148 * 64 * 1.965e9 / 1e12
 
 
 def args_():
@@ -275,7 +276,12 @@ def run_ours(a):
 
     # End to end through the public API, host arrays in, mesh out.
     e2e_ms, st = [], None
-    out = S.compute_surface(w["spheres"], params) if a.e2e_steps else None  # warm-up
+    # Warm-up: two calls, so that the timed calls find the memory a previous
+    # result still holds and the one the call before released in the caches
+    # (the steady state of a caller that keeps its last result).
+    out = None
+    for _ in range(2 if a.e2e_steps else 0):
+        out = S.compute_surface(w["spheres"], params)
     for _ in range(a.e2e_steps):
         barrier()
         t0 = time.perf_counter()
@@ -299,7 +305,10 @@ def run_ours(a):
 
     pk, pk_kind = peaks()
     ops, owned = eng.count_ops()
-    roof = roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks)
+    xops = eng.count_exact_ops() if w["refine"] == "exact" else 0
+    roof = roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops)
+    if roof.get("kernel") == "k_refine_exact":
+        roof["evaluations"] = int(st["refine_evaluations"])
     line = {
         "metric": "Mgridpts/s (SES mesh stage)", "value": value, "unit": "Mgridpts/s", "n_gpus": world,
         "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": mean_ms, "higher_is_better": True,
@@ -480,11 +489,19 @@ def run_batch(a):
         dist.destroy_process_group()
 
 
-def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks):
+def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops=0):
     """Roofline of the dominant kernel (per-unit counts in DESIGN.md)."""
     ms = stage[dominant]
     hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
     spb = (w["brick"] + 1) ** 3
+    if dominant == "refine" and xops:
+        achieved = xops / (ms / 1e3) / 1e12
+        return {"kernel": "k_refine_exact", "bound": "fp64", "achieved": achieved, "peak": FP64_NOFMA_TOPS,
+                "unit": "Tops/s", "frac": achieved / FP64_NOFMA_TOPS, "traffic": None,
+                "peak_source": "nominal: 148 SMs x 64 FP64 lanes x 1965 MHz, one op per lane-cycle "
+                               "(no FMA contraction, bit-exact f64; sqrt and division counted as one op)",
+                "algorithmic_ops": xops, "ms": ms,
+                "sampler": roofline("sample", stage, info, ops, owned, w, pk, pk_kind, n_bricks)}
     if dominant == "sample":
         achieved = ops / (ms / 1e3) / 1e12
         return {"kernel": "k_sample", "bound": "fp32", "achieved": achieved, "peak": FP32_NOFMA_TOPS,

@@ -213,6 +213,10 @@ int smb_place_fast(smb_resident* res, smb_batch* batch, double* ms, char* err, s
  * the number of edges the exact refinement took. */
 int smb_batch_exact_summary(const smb_batch* batch, unsigned long long* evaluations, unsigned long long* host_edges,
                             unsigned long long* exact_edges);
+/* Re-runs the last smb_refine_exact counting the f64 arithmetic operations
+ * of its field evaluations (the algorithmic count of its roofline; sqrt and
+ * division one each; vertices are rewritten identically). */
+int smb_batch_count_exact_ops(smb_batch* batch, unsigned long long* ops, char* err, size_t errlen);
 /* Shared memory per warp for one sub-block's f64 lists in smb_refine_exact
  * (1 KiB..48 KiB; default 18 KiB); larger sub-blocks take a whole block. */
 int smb_batch_set_exact_region(smb_batch* batch, size_t bytes);

@@ -311,13 +311,21 @@ struct XEval {
 };
 
 // eval_local (point.rs:686-738) against the ball's lists: value, feature and
-// closest point.
-__device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, double probe, double band, double x, double y, double z) {
+// closest point.  COUNT: adds the f64 arithmetic operations executed to ops
+// (sqrt and division one each; compares, selects, fabs not counted): 9 per
+// inside sphere tested; if inside, 1, then 10 per S candidate visited (+7
+// for the projection, +10 per blocker tested), 26 per C candidate (+9 or +6,
+// +10 per blocker), 9 per SAS vertex, 1 final.
+template <bool COUNT = false>
+__device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, double probe, double band, double x,
+                                        double y, double z, unsigned long long* ops = nullptr) {
     XEval e;
     e.qx = x, e.qy = y, e.qz = z, e.id = 0;
     bool inside = false;
+    unsigned long long n_ops = 0;
     for (uint32_t k = 0; k < v.ni; k++) {
         const double4 c = v.in_c[k];
+        if (COUNT) n_ops += 9;
         if (dist3(x, y, z, c.x, c.y, c.z) < c.w) {
             inside = true;
             break;
@@ -325,21 +333,26 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
     }
     if (!inside) {
         e.value = probe, e.kind = XF_SOLVENT;
+        if (COUNT) *ops += n_ops;
         return e;
     }
     double best = probe + band;
+    if (COUNT) n_ops += 1;
     e.kind = XF_BEYOND;
     for (uint32_t i = 0; i < v.ns && v.s_key[i] < best; i++) {
         const double4 c = v.s_c[i];
         const double vx = x - c.x, vy = y - c.y, vz = z - c.z;
         const double len = sqrt(vx * vx + vy * vy + vz * vz);
         const double lb = fabs(len - c.w);
+        if (COUNT) n_ops += 10;
         if (lb >= best || len < 1e-12) continue;
         const double s = c.w / len;
         const double qx = c.x + vx * s, qy = c.y + vy * s, qz = c.z + vz * s;
+        if (COUNT) n_ops += 7;
         bool free = true;
         for (uint32_t p = v.s_off[i], pe = v.s_off[i + 1]; p < pe; p++) {
             const double4 k = v.near_c[v.s_blk[p]];
+            if (COUNT) n_ops += 10;
             if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - X_EPS)) {
                 free = false;
                 break;
@@ -354,18 +367,22 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
         const double wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
         const double wl = sqrt(wx * wx + wy * wy + wz * wz);
         const double dist = sqrt(along * along + (wl - m.w) * (wl - m.w));
+        if (COUNT) n_ops += 26;
         if (dist >= best) continue;
         double dx, dy, dz;
         if (wl > 1e-12) {
             dx = wx / wl, dy = wy / wl, dz = wz / wl;
+            if (COUNT) n_ops += 3;
         } else {  // on the axis: e1 (A.circ words 6..8)
             const double* C = circ + 12 * size_t(v.c_id[i]);
             dx = u.w, dy = C[7], dz = C[8];
         }
         const double qx = m.x + dx * m.w, qy = m.y + dy * m.w, qz = m.z + dz * m.w;
+        if (COUNT) n_ops += 6;
         bool free = true;
         for (uint32_t p = v.c_off[i], pe = v.c_off[i + 1]; p < pe; p++) {
             const double4 k = v.near_c[v.c_blk[p]];
+            if (COUNT) n_ops += 10;
             if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - X_EPS)) {
                 free = false;
                 break;
@@ -376,8 +393,10 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
     for (uint32_t i = 0; i < v.nv && v.v_key[i] < best; i++) {
         const double4 p = v.v_p[i];
         const double d = dist3(x, y, z, p.x, p.y, p.z);
+        if (COUNT) n_ops += 9;
         if (d < best) best = d, e.kind = XF_VERTEX, e.id = v.v_id[i], e.qx = p.x, e.qy = p.y, e.qz = p.z;
     }
+    if (COUNT) *ops += n_ops + 1;
     e.value = probe - best;
     return e;
 }
@@ -444,8 +463,9 @@ __device__ void x_attributes(const DArr& A, const DLat& L, const ExactAttr& X, u
 }
 
 // extract::vertex of edge k (exact mode) and its attributes.
+template <bool COUNT = false>
 __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat& L, const ExactAttr& X, int4 key, uint32_t k,
-                       uint32_t code, float2 fv, const ExactOut& out) {
+                       uint32_t code, float2 fv, const ExactOut& out, unsigned long long* ops = nullptr) {
     const int b = L.b;
     const double h = L.h;
     const uint32_t cell = code / 3, axis = code % 3;
@@ -466,7 +486,7 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
     uint32_t evals = 0;
     for (int it = 0; it < X_MAX_ITER; it++) {
         const double x = pax + dx * t, y = pay + dy * t, z = paz + dz * t;
-        const XEval e = x_eval(v, A.circ, probe, band, x, y, z);
+        const XEval e = x_eval<COUNT>(v, A.circ, probe, band, x, y, z, ops);
         evals++;
         last = e;
         const double g = e.value;
@@ -502,7 +522,7 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
         const bool neg0 = g0 < 0.0;
         for (int it = 0; it < X_MAX_BISECT; it++) {
             t = 0.5 * (t0 + t1);
-            const XEval e = x_eval(v, A.circ, probe, band, pax + dx * t, pay + dy * t, paz + dz * t);
+            const XEval e = x_eval<COUNT>(v, A.circ, probe, band, pax + dx * t, pay + dy * t, paz + dz * t, ops);
             evals++;
             last = e;
             if (fabs(e.value) <= X_TOL || (t1 - t0) * len <= 2.0 * X_TOL) break;
@@ -532,7 +552,7 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
 // region is `region` bytes of a global slab per warp (read back through
 // L1), items come from ovf through counters[CNT_XQUEUE], and an item that
 // does not fit either stays with the host (*left counts them).
-template <bool SLAB>
+template <bool SLAB, bool COUNT = false>
 __global__ void __launch_bounds__(32 * X_WARPS, 1) k_refine_exact(DArr A, DLat L, ExactAttr X, const int4* keys,
                                                                const uint32_t* work, const uint32_t* edges,
                                                                const float2* edge_vals, const uint32_t* item_off,
@@ -547,6 +567,7 @@ __global__ void __launch_bounds__(32 * X_WARPS, 1) k_refine_exact(DArr A, DLat L
     uint32_t* cnt = sh_cnt[warp];
     unsigned int* queue = reinterpret_cast<unsigned int*>(&counters[SLAB ? CNT_XQUEUE : CNT_QUEUE]);
     const uint32_t n_claim = SLAB ? ovf[0] : n_items;
+    unsigned long long ops = 0;
     for (;;) {
         uint32_t q = 0;
         if (lane == 0) q = atomicAdd(queue, 1u);
@@ -567,8 +588,12 @@ __global__ void __launch_bounds__(32 * X_WARPS, 1) k_refine_exact(DArr A, DLat L
         }
         for (uint32_t e = a0 + lane; e < a1; e += 32) {
             const uint32_t k = item_edges[e];
-            x_edge(v, A, L, X, key, k, edges[k], edge_vals[k], out);
+            x_edge<COUNT>(v, A, L, X, key, k, edges[k], edge_vals[k], out, &ops);
         }
+    }
+    if (COUNT) {
+        for (int o = 16; o; o >>= 1) ops += __shfl_down_sync(0xffffffffu, ops, o);
+        if (lane == 0 && ops) atomicAdd(&counters[CNT_OPS], ops);
     }
 }
 
@@ -679,6 +704,13 @@ cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long 
     return cudaGetLastError();
 }
 
+template <bool COUNT>
+static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
+                                       const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
+                                       const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
+                                       const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
+                                       unsigned long long* counters, int sms, size_t region, cudaStream_t s);
+
 size_t exact_slab_bytes(int sms) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_refine_exact<true>, 32 * X_WARPS, 0);
@@ -689,7 +721,23 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
                                 const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                 const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
-                                unsigned long long* counters, int sms, size_t region, cudaStream_t s) {
+                                unsigned long long* counters, int sms, size_t region, cudaStream_t s, bool count) {
+    if (count) {
+        cudaError_t e = cudaMemsetAsync(&counters[CNT_OPS], 0, 8, s);
+        if (e != cudaSuccess) return e;
+        return launch_exact_levels<true>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
+                                         ovf, slab, slab_bytes, counters, sms, region, s);
+    }
+    return launch_exact_levels<false>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out, ovf,
+                                      slab, slab_bytes, counters, sms, region, s);
+}
+
+template <bool COUNT>
+static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
+                                       const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
+                                       const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
+                                       const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
+                                       unsigned long long* counters, int sms, size_t region, cudaStream_t s) {
     cudaError_t e;
     if ((e = cudaMemsetAsync(&counters[CNT_QUEUE], 0, 8, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&counters[CNT_XQUEUE], 0, 8, s)) != cudaSuccess) return e;
@@ -697,8 +745,8 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
     if (!n_items) return cudaSuccess;
     region = (region + 15) & ~size_t(15);
     const size_t narrow = size_t(X_WARPS) * region;
-    auto kn = k_refine_exact<false>;
-    auto kg = k_refine_exact<true>;
+    auto kn = k_refine_exact<false, COUNT>;
+    auto kg = k_refine_exact<true, COUNT>;
     if ((e = cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(narrow))) != cudaSuccess)
         return e;
     int per_sm = 0;

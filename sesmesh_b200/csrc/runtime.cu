@@ -1021,7 +1021,8 @@ int smb_resident_set_exact(smb_resident* r, const uint32_t* orig, const uint32_t
 
 // The exact refinement of the last run's crossing edges (mask: only the
 // edges k with mask[k] != 0; their results into the vertex buffers).
-static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* err, size_t errlen) {
+static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* err, size_t errlen,
+                      bool count = false) {
     smb_device* d = r->dev;
     cudaStream_t s = d->stream;
     const size_t ne = b->n_edges;
@@ -1048,7 +1049,7 @@ static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* 
                                         b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->item_off.as<uint32_t>(),
                                         b->item_edges.as<uint32_t>(), nw, out, b->x_ovf.as<uint32_t>(),
                                         b->x_slab.as<unsigned char>(), slab, cnt, d->info.multiprocessors,
-                                        b->x_region, s);
+                                        b->x_region, s, count);
     if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     uint32_t n_block = 0;
     CK(cudaMemcpyAsync(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost, s));
@@ -1089,6 +1090,18 @@ int smb_refine_exact(smb_resident* r, smb_batch* b, double* ms, char* err, size_
     cudaEventElapsedTime(&t, b->ev[4], b->ev[5]);
     if (ms) *ms = t;
     b->refined_exact = true;
+    return SMB_OK;
+}
+
+int smb_batch_count_exact_ops(smb_batch* b, unsigned long long* ops, char* err, size_t errlen) {
+    if (!b || !ops) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
+    smb_resident* r = b->res;
+    if (!b->refined_exact || b->x_exact_edges != b->n_edges)
+        return set_err(err, errlen, "smb_refine_exact must run first"), SMB_ERR_STATE;
+    CK(cudaSetDevice(r->dev->index));
+    int rc = exact_pass(r, b, nullptr, err, errlen, true);
+    if (rc) return rc;
+    CK(cudaMemcpy(ops, b->counters.as<unsigned long long>() + CNT_OPS, 8, cudaMemcpyDeviceToHost));
     return SMB_OK;
 }
 

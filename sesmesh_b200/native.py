@@ -138,6 +138,7 @@ SIGNATURES = {
     "smb_batch_exact_summary": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
                                           C.POINTER(C.c_ulonglong)]),
     "smb_place_fast": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
+    "smb_batch_count_exact_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), _cp, _sz]),
     "smb_kernel_launches": (C.c_ulonglong, []),
     "smb_batch_info_get": (C.c_int, [_vp, C.POINTER(BatchInfo)]),
     "smb_batch_count_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _cp, _sz]),

@@ -209,6 +209,15 @@ class SurfaceEngine:
         lib().smb_batch_info_get(b, C.byref(i))
         return {name: getattr(i, name) for name, _ in i._fields_}
 
+    def count_exact_ops(self):
+        """f64 operations of the last run's exact refinement (its field
+        evaluations), counted by re-running it."""
+        b = lib().smb_engine_batch(self.h)
+        err = C.create_string_buffer(1024)
+        ops = C.c_ulonglong(0)
+        _check(lib().smb_batch_count_exact_ops(b, C.byref(ops), err, 1024), err)
+        return ops.value
+
     def count_ops(self):
         """f32 operations and evaluated samples of the last run's sampling pass."""
         b = lib().smb_engine_batch(self.h)
