@@ -310,6 +310,29 @@ struct XEval {
     uint32_t kind, id;
 };
 
+// Comparisons of a correctly rounded square root with a positive threshold
+// T, decided from the square when it is clear of T^2: t2 = fl(T T) is within
+// 2^-53 of T^2, so d2 >= fl(t2 (1 + 2^-49)) gives sqrt(d2) >= T (1 + 6 2^-53)
+// and fl(sqrt(d2)) > T; d2 <= fl(t2 (1 - 2^-49)) gives fl(sqrt(d2)) < T.
+// Only in between is the square root taken.  The results are those of
+// fl(sqrt(d2)) >= T and fl(sqrt(d2)) < T exactly (NaN: false for both).
+__device__ __forceinline__ bool sqrt_ge(double d2, double T) {
+    const double t2 = T * T;
+    if (d2 >= t2 * (1.0 + 0x1p-49)) return true;
+    if (d2 <= t2 * (1.0 - 0x1p-49)) return false;
+    return sqrt(d2) >= T;
+}
+__device__ __forceinline__ bool sqrt_lt(double d2, double T) {
+    const double t2 = T * T;
+    if (d2 <= t2 * (1.0 - 0x1p-49)) return true;
+    if (d2 >= t2 * (1.0 + 0x1p-49)) return false;
+    return sqrt(d2) < T;
+}
+__device__ __forceinline__ double sq3(double ax, double ay, double az, double bx, double by, double bz) {
+    const double dx = ax - bx, dy = ay - by, dz = az - bz;
+    return dx * dx + dy * dy + dz * dz;
+}
+
 // eval_local (point.rs:686-738) against the ball's lists: value, feature and
 // closest point.  COUNT: adds the f64 arithmetic operations executed to ops
 // (sqrt and division one each; compares, selects, fabs not counted): 9 per
@@ -326,7 +349,7 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
     for (uint32_t k = 0; k < v.ni; k++) {
         const double4 c = v.in_c[k];
         if (COUNT) n_ops += 9;
-        if (dist3(x, y, z, c.x, c.y, c.z) < c.w) {
+        if (sqrt_lt(sq3(x, y, z, c.x, c.y, c.z), c.w)) {
             inside = true;
             break;
         }
@@ -353,7 +376,7 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
         for (uint32_t p = v.s_off[i], pe = v.s_off[i + 1]; p < pe; p++) {
             const double4 k = v.near_c[v.s_blk[p]];
             if (COUNT) n_ops += 10;
-            if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - X_EPS)) {
+            if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - X_EPS)) {
                 free = false;
                 break;
             }
@@ -366,9 +389,10 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
         const double along = yx * u.x + yy * u.y + yz * u.z;
         const double wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
         const double wl = sqrt(wx * wx + wy * wy + wz * wz);
-        const double dist = sqrt(along * along + (wl - m.w) * (wl - m.w));
+        const double dist2 = along * along + (wl - m.w) * (wl - m.w);
         if (COUNT) n_ops += 26;
-        if (dist >= best) continue;
+        if (sqrt_ge(dist2, best)) continue;
+        const double dist = sqrt(dist2);
         double dx, dy, dz;
         if (wl > 1e-12) {
             dx = wx / wl, dy = wy / wl, dz = wz / wl;
@@ -383,7 +407,7 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
         for (uint32_t p = v.c_off[i], pe = v.c_off[i + 1]; p < pe; p++) {
             const double4 k = v.near_c[v.c_blk[p]];
             if (COUNT) n_ops += 10;
-            if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - X_EPS)) {
+            if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - X_EPS)) {
                 free = false;
                 break;
             }
@@ -392,9 +416,10 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
     }
     for (uint32_t i = 0; i < v.nv && v.v_key[i] < best; i++) {
         const double4 p = v.v_p[i];
-        const double d = dist3(x, y, z, p.x, p.y, p.z);
+        const double d2 = sq3(x, y, z, p.x, p.y, p.z);
         if (COUNT) n_ops += 9;
-        if (d < best) best = d, e.kind = XF_VERTEX, e.id = v.v_id[i], e.qx = p.x, e.qy = p.y, e.qz = p.z;
+        if (!sqrt_lt(d2, best)) continue;
+        best = sqrt(d2), e.kind = XF_VERTEX, e.id = v.v_id[i], e.qx = p.x, e.qy = p.y, e.qz = p.z;
     }
     if (COUNT) *ops += n_ops + 1;
     e.value = probe - best;

@@ -52,6 +52,16 @@ __device__ __forceinline__ void block_add(unsigned long long* dst, unsigned long
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
 }
 
+// base[key] += 1 for the active threads of a warp, one atomic per distinct
+// key (the counts of a large component's members come from one address).
+// All threads of the warp call it.
+__device__ __forceinline__ void add_by_key(unsigned long long* base, uint32_t key, bool active) {
+    const unsigned m = __ballot_sync(0xffffffffu, active);
+    if (!active) return;
+    const unsigned peers = __match_any_sync(m, key);
+    if (int(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&base[key], (unsigned long long)__popc(peers));
+}
+
 __global__ void k_vertex_checks(const float* pos, const float* nrm, uint32_t nv, unsigned long long* bad) {
     uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long b = 0;
@@ -213,13 +223,15 @@ __global__ void k_uf_roots(uint32_t* parent, uint32_t nv, uint32_t* is_root, uns
 
 __global__ void k_component_ids(const uint32_t* parent, const uint32_t* cid_of_root, uint32_t nv, uint32_t* id,
                                 unsigned long long* comp_vertices) {
-    uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= nv) return;
-    uint32_t r = parent[v];
-    for (uint32_t it = 0; it < UF_LIMIT && parent[r] != r; it++) r = parent[r];
-    uint32_t c = cid_of_root[r];
-    id[v] = c;
-    atomicAdd(&comp_vertices[c], 1ull);
+    const uint32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t c = 0;
+    if (v < nv) {
+        uint32_t r = parent[v];
+        for (uint32_t it = 0; it < UF_LIMIT && parent[r] != r; it++) r = parent[r];
+        c = cid_of_root[r];
+        id[v] = c;
+    }
+    add_by_key(comp_vertices, c, v < nv);
 }
 
 // Per chunk of SUM_CHUNK triangles, in order: each component's triangle
@@ -239,21 +251,27 @@ __global__ void k_segment_flags(const uint32_t* comp, const uint32_t* perm, uint
     flag[p] = (p == 0 || comp[p] != comp[p - 1] || (perm[p] / SUM_CHUNK) != (perm[p - 1] / SUM_CHUNK)) ? 1u : 0u;
 }
 
+// Area and volume of each triangle, in the component-sorted order.
+__global__ void k_triangle_area_volume(const float* pos, const uint32_t* tris, const uint32_t* perm, uint32_t nt,
+                                       double* ta, double* tv) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nt) return;
+    const double o[3] = {double(pos[0]), double(pos[1]), double(pos[2])};
+    double a, v;
+    area_volume(pos, tris + 3 * size_t(perm[p]), o, a, v);
+    ta[p] = a, tv[p] = v;
+}
+
 // Thread per segment: its triangles' area and volume summed in triangle
 // order (one (component, chunk) partial of the host's sums).
-__global__ void k_segment_partials(const float* pos, const uint32_t* tris, const uint32_t* comp,
-                                   const uint32_t* perm, uint32_t nt, const uint32_t* start, uint32_t n_seg,
-                                   Partial* out, uint32_t* seg_comp) {
+__global__ void k_segment_partials(const double* ta, const double* tv, const uint32_t* comp, const uint32_t* perm,
+                                   uint32_t nt, const uint32_t* start, uint32_t n_seg, Partial* out,
+                                   uint32_t* seg_comp) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n_seg) return;
-    const double o[3] = {double(pos[0]), double(pos[1]), double(pos[2])};
     const uint32_t p0 = start[s], p1 = s + 1 < n_seg ? start[s + 1] : nt;
     Partial acc{comp[p0], perm[p0] / SUM_CHUNK, 0ull, 0.0, 0.0};
-    for (uint32_t p = p0; p < p1; p++) {
-        double a, v;
-        area_volume(pos, tris + 3 * size_t(perm[p]), o, a, v);
-        acc.t++, acc.a += a, acc.v += v;
-    }
+    for (uint32_t p = p0; p < p1; p++) acc.t++, acc.a += ta[p], acc.v += tv[p];
     out[s] = acc;
     seg_comp[s] = acc.comp;
 }
@@ -285,9 +303,9 @@ __global__ void k_first_of_component(const uint32_t* sorted_comp, uint32_t n, ui
 
 __global__ void k_euler_edges(const unsigned long long* keys, uint64_t cap, const uint32_t* id,
                               unsigned long long* comp_edges) {
-    uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (s >= cap || keys[s] == EMPTY) return;
-    atomicAdd(&comp_edges[id[uint32_t(keys[s] >> 32)]], 1ull);
+    const uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const bool active = s < cap && keys[s] != EMPTY;
+    add_by_key(comp_edges, active ? id[uint32_t(keys[s] >> 32)] : 0u, active);
 }
 
 __global__ void k_triangle_keys(const uint32_t* tris, uint32_t nt, const uint32_t* id, uint32_t* key,
@@ -402,7 +420,7 @@ unsigned bits_for(uint32_t n) {
 void MeasureScratch::release() {
     for (DBuf* b : {&pos, &nrm, &tris, &tris_out, &keys, &cnt, &dup, &parent, &flag, &cid, &id, &counters, &comp_v,
                     &comp_t, &comp_e, &area, &volume, &parts, &pkey, &pidx, &pkey2, &pidx2, &first, &tkey, &tidx,
-                    &tkey2, &tidx2, &tiles, &cub, &packed, &err})
+                    &tkey2, &tidx2, &tiles, &cub, &packed, &err, &tri_a, &tri_v})
         b->release();
     pinned_free(host);
     host = nullptr;
@@ -527,14 +545,17 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
     }
     const uint32_t np = uint32_t(n_seg);
     if (np) {
-        if (!R(S.parts, size_t(np) * sizeof(Partial)) || !R(S.pkey, size_t(np) * 4)) {
+        if (!R(S.parts, size_t(np) * sizeof(Partial)) || !R(S.pkey, size_t(np) * 4) || !R(S.tri_a, nt * 8) ||
+            !R(S.tri_v, nt * 8)) {
             if (msg) *msg = std::string("device memory for the measure: ") + e;
             return false;
         }
         Partial* parts = S.parts.as<Partial>();
-        k_segment_partials<<<blocks(np), 256, 0, s>>>(pos, tris, S.tkey2.as<uint32_t>(), S.tidx2.as<uint32_t>(),
-                                                      uint32_t(nt), S.tidx.as<uint32_t>(), np, parts,
-                                                      S.pkey.as<uint32_t>());
+        k_triangle_area_volume<<<blocks(nt), 256, 0, s>>>(pos, tris, S.tidx2.as<uint32_t>(), uint32_t(nt),
+                                                          S.tri_a.as<double>(), S.tri_v.as<double>());
+        k_segment_partials<<<blocks(np), 256, 0, s>>>(S.tri_a.as<double>(), S.tri_v.as<double>(),
+                                                      S.tkey2.as<uint32_t>(), S.tidx2.as<uint32_t>(), uint32_t(nt),
+                                                      S.tidx.as<uint32_t>(), np, parts, S.pkey.as<uint32_t>());
         k_first_of_component<<<blocks(uint64_t(np) + 1), 256, 0, s>>>(S.pkey.as<uint32_t>(), np,
                                                                         S.first.as<uint32_t>(), nc);
         k_component_sums<<<blocks(nc), 256, 0, s>>>(parts, nullptr, np, S.first.as<uint32_t>(), nc,

@@ -12,7 +12,8 @@ namespace smb {
 // Device buffers of the measure, kept between meshes.
 struct MeasureScratch {
     DBuf pos, nrm, tris, tris_out, keys, cnt, dup, parent, flag, cid, id, counters, comp_v, comp_t, comp_e, area,
-        volume, parts, pkey, pidx, pkey2, pidx2, first, tkey, tidx, tkey2, tidx2, tiles, cub, packed, err;
+        volume, parts, pkey, pidx, pkey2, pidx2, first, tkey, tidx, tkey2, tidx2, tiles, cub, packed, err, tri_a,
+        tri_v;
     void* host = nullptr;  // page-locked staging of the results
     size_t host_cap = 0;
     void* staging(size_t bytes);  // null when page-locked memory cannot be had
