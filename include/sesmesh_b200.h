@@ -218,7 +218,7 @@ int smb_batch_exact_summary(const smb_batch* batch, unsigned long long* evaluati
  * division one each; vertices are rewritten identically). */
 int smb_batch_count_exact_ops(smb_batch* batch, unsigned long long* ops, char* err, size_t errlen);
 /* Shared memory per warp for one sub-block's f64 lists in smb_refine_exact
- * (1 KiB..48 KiB; default 18 KiB); larger sub-blocks take a whole block. */
+ * (1 KiB..48 KiB; default 13 KiB); larger sub-blocks go to warps with global list slabs. */
 int smb_batch_set_exact_region(smb_batch* batch, size_t bytes);
 
 /* Sizes and times of the last run of a batch (diagnostics; BatchTimes and

@@ -14,10 +14,8 @@
 // (distance, index), V by (distance, index)) and the inside test is an
 // any-of, so collecting them in a different order gives the same lists.
 //
-// Two edges stay with the host, marked evals = 0: an edge whose last
-// evaluation is solvent or beyond the band (its attributes search the
-// whole sphere grid), and the edges of a sub-block whose lists do not fit
-// the shared memory of a whole block.
+// Edges stay with the host (marked evals = 0) only when their sub-block's
+// lists exceed a warp's 256 KiB global slab.
 #include <algorithm>
 
 #include "common.cuh"
@@ -578,7 +576,7 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
 // L1), items come from ovf through counters[CNT_XQUEUE], and an item that
 // does not fit either stays with the host (*left counts them).
 template <bool SLAB, bool COUNT = false>
-__global__ void __launch_bounds__(32 * X_WARPS, 1) k_refine_exact(DArr A, DLat L, ExactAttr X, const int4* keys,
+__global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L, ExactAttr X, const int4* keys,
                                                                const uint32_t* work, const uint32_t* edges,
                                                                const float2* edge_vals, const uint32_t* item_off,
                                                                const uint32_t* item_edges, uint32_t n_items,

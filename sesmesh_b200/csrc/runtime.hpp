@@ -96,7 +96,7 @@ struct smb_batch {
     bool refined_exact = false;
     size_t x_exact_edges = 0;  // edges the exact refinement took in the last pass
     size_t x_block_items = 0;  // items of the last exact pass refined by a whole block
-    size_t x_region = 18432;  // shared-memory bytes per warp for one sub-block's f64 candidate lists
+    size_t x_region = 13312;  // shared-memory bytes per warp for one sub-block's f64 candidate lists
     smb::GatherCaps caps{192, 128, 384, 128};
     int gather_warps = 4;
     bool use_tma = true;
