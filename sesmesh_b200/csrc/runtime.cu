@@ -666,6 +666,12 @@ int smb_batch_new(smb_resident* r, smb_batch** out, char* err, size_t errlen) {
     b->res = r;
     r->refs.fetch_add(1);
     for (auto& ev : b->ev) cudaEventCreate(&ev);
+    {
+        smb_device* d = r->dev;
+        std::lock_guard<std::mutex> g(d->hint_mu);
+        if (d->hint.warps && d->hint.b == r->L.b && d->hint.h == r->L.h && d->hint.probe == r->A.probe)
+            b->caps = d->hint.caps, b->gather_warps = d->hint.warps;
+    }
     *out = b;
     return SMB_OK;
 }
@@ -786,6 +792,9 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
         if (per <= size_t(d->smem_optin)) {
             b->caps = next;
             b->gather_warps = int(std::max<size_t>(1, std::min<size_t>(8, size_t(65536) / per)));
+            std::lock_guard<std::mutex> g(d->hint_mu);
+            d->hint.h = L.h, d->hint.b = L.b, d->hint.probe = r->A.probe;
+            d->hint.caps = b->caps, d->hint.warps = b->gather_warps;
         }
     }
     cudaEventRecord(b->ev[2], s);

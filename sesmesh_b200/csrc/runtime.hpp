@@ -1,6 +1,7 @@
 // Internal state behind the opaque handles of include/sesmesh_b200.h.
 #pragma once
 #include <atomic>
+#include <mutex>
 #include <cstddef>
 #include <cstdint>
 #include <vector>
@@ -57,6 +58,15 @@ struct smb_device {
     size_t smem_optin = 0;
     std::atomic<int> refs{0};
     std::atomic<bool> closed{false}, gone{false};
+    // Gather caps and block shape the last batch with these lattice and probe
+    // values settled on; new batches with the same values start from them.
+    std::mutex hint_mu;
+    struct CapsHint {
+        double h = 0, probe = 0;
+        int b = 0;
+        smb::GatherCaps caps{};
+        int warps = 0;
+    } hint;
 };
 
 struct smb_resident {
