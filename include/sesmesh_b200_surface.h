@@ -151,6 +151,11 @@ int smb_multi_config_get(const smb_multi* m, smb_multi_config* out);
  * start of the run until that structure's mesh is complete) until the next
  * run. */
 int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen);
+/* Each structure's placement, assembly, validation and measure on the
+ * device after its group's pass (on = 1, the default; results then live in
+ * page-locked memory until the next run), or on the host threads while the
+ * device meshes the next group (on = 0).  Same mesh bytes either way. */
+int smb_multi_set_device_finish(smb_multi* m, int on);
 smb_surface* smb_multi_surface(smb_multi* m, size_t i);
 int smb_multi_latency(const smb_multi* m, double* ms);
 

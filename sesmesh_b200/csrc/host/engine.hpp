@@ -82,3 +82,12 @@ std::string finish_surface(const Arrangement& arr, const MeshParams& mp, bool fa
                            const uint32_t* tri_off, const uint32_t* tris, const DeviceRefine& dev, smb_surface& s,
                            smb_device* device = nullptr, smb::MeasureScratch* scratch = nullptr,
                            smbh::MeshOut* exact = nullptr, const uint32_t* exact_evals = nullptr);
+
+// The engine's batch, with every vertex on the device (smb_refine_exact or
+// smb_place_fast ran and left no edge to the host), assembled, validated,
+// measured and grouped on the device into s (surface.cpp).  evals: the
+// vertices' evaluation count; cpu_edges: the statistic refine_cpu_edges.
+// SMB_OK or an error code; *fallback when the device declined (the host
+// stages must finish the mesh).
+int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long evals, unsigned long long cpu_edges,
+                        bool* fallback, double* ms_d2h, char* err, size_t errlen);

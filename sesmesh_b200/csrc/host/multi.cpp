@@ -146,6 +146,7 @@ struct smb_multi {
     std::vector<int4> keys4;   // host copy of the keys
     HostGroup* hosts = nullptr;  // two alternating sets of results on the host
     std::vector<size_t> b0;    // first brick of each structure (n + 1)
+    bool device_finish = true; // place, refine and finish each structure on the device
     cudaEvent_t ev[2] = {};
     // Results of the last run.
     std::vector<std::unique_ptr<smb_surface>> out;
@@ -508,7 +509,7 @@ int prepare_run(smb_multi* m, double* classify_ms, char* err, size_t errlen) {
     return SMB_OK;
 }
 
-int fetch_group(smb_multi* m, const Group& G, HostGroup& H, char* err, size_t errlen) {
+int fetch_group(smb_multi* m, const Group& G, HostGroup& H, char* err, size_t errlen, bool full = true) {
     const size_t nb = G.k1 - G.k0;
     cudaStream_t s = m->dev->stream;
     H.ne = H.nt = 0;
@@ -528,6 +529,10 @@ int fetch_group(smb_multi* m, const Group& G, HostGroup& H, char* err, size_t er
         return set_err(err, errlen, "page-locked host memory"), SMB_ERR_MEMORY;
     MCK(cudaMemcpyAsync(H.eo.p, m->edge_off.p, (nb + 1) * 4, cudaMemcpyDeviceToHost, s));
     MCK(cudaMemcpyAsync(H.to.p, m->tri_off.p, (nb + 1) * 4, cudaMemcpyDeviceToHost, s));
+    if (!full) {
+        MCK(cudaStreamSynchronize(s));
+        return SMB_OK;
+    }
     if (ne) {
         MCK(cudaMemcpyAsync(H.edges.p, m->edges.p, ne * 4, cudaMemcpyDeviceToHost, s));
         MCK(cudaMemcpyAsync(H.ev.p, m->edge_vals.p, ne * 8, cudaMemcpyDeviceToHost, s));
@@ -651,11 +656,120 @@ int smb_multi_tune(smb_multi* m, char* err, size_t errlen) {
     return SMB_OK;
 }
 
+int smb_multi_set_device_finish(smb_multi* m, int on) {
+    if (!m) return SMB_ERR_ARG;
+    m->device_finish = on != 0;
+    return SMB_OK;
+}
+
 int smb_multi_config_get(const smb_multi* m, smb_multi_config* out) {
     if (!m || !out) return SMB_ERR_ARG;
     *out = m->cfg;
     return SMB_OK;
 }
+
+namespace {
+
+__global__ void k_rebase(uint32_t* dst, const uint32_t* src, size_t n, uint32_t delta) {
+    const size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i < n) dst[i] = src[i] + delta;
+}
+
+// Structure i of group G finished on the device: its slice of the group's
+// results (bricks, sub-block records, work items, marching-cubes lists, f32
+// roots) is copied into its engine's own batch in the single-structure
+// layout (offsets rebased to the slice), then placed (smb_place_fast: the
+// converged roots with their exact attributes, the rest refined exactly),
+// assembled, validated and measured there.  work: the group's work list on
+// the host.  *fallback when the device left the structure to the host.
+int finish_structure_device(smb_multi* m, const Group& G, size_t i, const uint32_t* eo, const uint32_t* to,
+                            const uint32_t* work, size_t n_work, smb_surface& s, bool* fallback, char* err,
+                            size_t errlen) {
+    *fallback = false;
+    smb_engine* e = m->eng[i];
+    smb_resident* r = e->res;
+    smb_batch* b = e->batch;
+    cudaStream_t st = m->dev->stream;
+    const size_t lo = m->b0[i] - G.k0, hi = m->b0[i + 1] - G.k0, nb = hi - lo;
+    const uint32_t e0 = eo[lo], e1 = eo[hi], t0 = to[lo], t1 = to[hi];
+    const size_t ne = e1 - e0, nt = t1 - t0;
+    const uint32_t* w0 = std::lower_bound(work, work + n_work, uint32_t(8 * lo));
+    const uint32_t* w1 = std::lower_bound(work, work + n_work, uint32_t(8 * hi));
+    const size_t nw = size_t(w1 - w0), wo = size_t(w0 - work);
+    r->L = m->lat[i];
+    e->mp = m->mp[i];
+    if (r->keys) mem_free(r->keys);
+    r->keys = nullptr;
+    if (nb && mem_alloc(reinterpret_cast<void**>(&r->keys), nb * sizeof(int4)) != cudaSuccess)
+        return set_err(err, errlen, "device memory for structure %zu", i), SMB_ERR_MEMORY;
+    r->n_bricks = uint32_t(nb);
+    r->classified = true;
+    int rc;
+    if ((rc = b->rec.reserve(std::max<size_t>(nb, 1) * 8 * REC_WORDS * 4, err, errlen)) ||
+        (rc = b->work.reserve(std::max<size_t>(nw, 1) * 4, err, errlen)) ||
+        (rc = b->edge_off.reserve((nb + 1) * 4, err, errlen)) || (rc = b->tri_off.reserve((nb + 1) * 4, err, errlen)) ||
+        (rc = b->edges.reserve(std::max<size_t>(ne, 1) * 4, err, errlen)) ||
+        (rc = b->edge_vals.reserve(std::max<size_t>(ne, 1) * 8, err, errlen)) ||
+        (rc = b->tris.reserve(std::max<size_t>(nt, 1) * 12, err, errlen)) ||
+        (rc = b->e_t.reserve(std::max<size_t>(ne, 1) * 4, err, errlen)) ||
+        (rc = b->e_feat.reserve(std::max<size_t>(ne, 1) * 4, err, errlen)) ||
+        (rc = b->e_q.reserve(std::max<size_t>(ne, 1) * 12, err, errlen)) ||
+        (rc = b->e_evals.reserve(std::max<size_t>(ne, 1) * 4, err, errlen)) ||
+        (rc = b->totals.reserve(64, err, errlen)) || (rc = b->counters.reserve(CNT_N * 8, err, errlen)))
+        return rc;
+    auto d2d = [&](void* dst, const void* src, size_t bytes) {
+        return !bytes || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, st) == cudaSuccess;
+    };
+    auto rebase = [&](uint32_t* dst, const uint32_t* src, size_t n, uint32_t delta) {
+        if (n) k_rebase<<<unsigned((n + 255) / 256), 256, 0, st>>>(dst, src, n, delta);
+        return cudaGetLastError() == cudaSuccess;
+    };
+    const size_t sub0 = 8 * lo;
+    if (!d2d(r->keys, m->keys.as<int4>() + G.k0 + lo, nb * sizeof(int4)) ||
+        !d2d(b->rec.p, m->rec.as<uint32_t>() + sub0 * REC_WORDS, nb * 8 * REC_WORDS * 4) ||
+        !rebase(b->work.as<uint32_t>(), m->work.as<uint32_t>() + wo, nw, uint32_t(0) - uint32_t(sub0)) ||
+        !rebase(b->edge_off.as<uint32_t>(), m->edge_off.as<uint32_t>() + lo, nb + 1, uint32_t(0) - e0) ||
+        !rebase(b->tri_off.as<uint32_t>(), m->tri_off.as<uint32_t>() + lo, nb + 1, uint32_t(0) - t0) ||
+        !d2d(b->edges.p, m->edges.as<uint32_t>() + e0, ne * 4) ||
+        !d2d(b->edge_vals.p, m->edge_vals.as<float2>() + e0, ne * 8) ||
+        !d2d(b->tris.p, m->tris.as<uint32_t>() + 3 * size_t(t0), nt * 12) ||
+        !d2d(b->e_t.p, m->e_t.as<float>() + e0, ne * 4) || !d2d(b->e_feat.p, m->e_feat.as<uint32_t>() + e0, ne * 4) ||
+        !d2d(b->e_q.p, m->e_q.as<float>() + 3 * size_t(e0), ne * 12) ||
+        !d2d(b->e_evals.p, m->e_evals.as<uint32_t>() + e0, ne * 4))
+        return set_err(err, errlen, "copy of structure %zu's results failed", i), SMB_ERR_CUDA;
+    count_launches(3);
+    b->first = 0;
+    b->n = uint32_t(nb);
+    b->n_work = uint32_t(nw);
+    b->n_edges = ne;
+    b->n_tris = nt;
+    b->refined = true;
+    b->refined_exact = false;
+    // The engine's buffers go back to the memory cache afterwards: the next
+    // structure takes them from there (one structure's worth held at a time).
+    auto release = [&](int code) {
+        for (DBuf* x : b->bufs()) x->release();
+        e->measure.release();
+        mem_free(r->keys);
+        r->keys = nullptr;
+        r->n_bricks = 0;
+        b->refined = b->refined_exact = false;
+        return code;
+    };
+    double ms = 0;
+    if ((rc = smb_place_fast(r, b, &ms, err, errlen)) != SMB_OK) return release(rc);
+    unsigned long long evals = 0, host_edges = 0, exact_edges = 0;
+    if ((rc = smb_batch_exact_summary(b, &evals, &host_edges, &exact_edges)) != SMB_OK)
+        return release((set_err(err, errlen, "vertex summary failed"), rc));
+    if (host_edges || !nb) {
+        *fallback = true;
+        return release(SMB_OK);
+    }
+    double ms_d2h = 0;
+    return release(finish_exact_device(e, s, evals, exact_edges, fallback, &ms_d2h, err, errlen));
+}
+
+}  // namespace
 
 int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen) {
     if (!m) return SMB_ERR_ARG;
@@ -671,7 +785,7 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
     m->latency.assign(n, 0.0);
     m->redone.assign(n, 0);
     std::vector<std::string> errs(n);
-    double t_device = 0, t_d2h = 0;
+    double t_device = 0, t_d2h = 0, t_finish = 0;
     unsigned long long over_lists = 0, over_memory = 0;
     bool graphs = true;
     // Group by group: the device pass of group g + 1 runs while the host
@@ -693,7 +807,7 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
         auto t1 = clk::now();
         std::vector<uint32_t> fail(n);
         HostGroup& Hc = hosts[gi % 2];
-        if ((rc = fetch_group(m, G, Hc, err, errlen)) ||
+        if ((rc = fetch_group(m, G, Hc, err, errlen, !m->device_finish)) ||
             cudaMemcpy(fail.data(), m->d_fail.p, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
             if (worker.joinable()) worker.join();
             return rc ? rc : (set_err(err, errlen, "copy of the failure flags failed"), SMB_ERR_CUDA);
@@ -708,8 +822,55 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
             const size_t hi = m->b0[i + 1] - G.k0;
             if (fail[i] || Hc.eo.as<uint32_t>()[hi] > Hc.ne || Hc.to.as<uint32_t>()[hi] > Hc.nt) m->redone[i] = 1;
         }
+        // On the device: each structure placed, refined where the f32 search
+        // left edges, assembled and measured; those it declines (host[i])
+        // are finished on the host threads below.
+        std::vector<uint8_t> host(n, m->device_finish ? 0 : 1);
+        if (m->device_finish) {
+            auto t2 = clk::now();
+            std::vector<uint32_t> work;
+            unsigned long long nw = 0;
+            if (G.k1 > G.k0) {
+                if (cudaMemcpy(&nw, m->totals.p, 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                    if (worker.joinable()) worker.join();
+                    return set_err(err, errlen, "copy of the work count failed"), SMB_ERR_CUDA;
+                }
+                work.resize(size_t(nw));
+                if (nw && cudaMemcpy(work.data(), m->work.p, size_t(nw) * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                    if (worker.joinable()) worker.join();
+                    return set_err(err, errlen, "copy of the work list failed"), SMB_ERR_CUDA;
+                }
+            }
+            for (size_t i = G.s0; i < G.s1; i++) {
+                if (m->redone[i]) continue;
+                auto s = std::make_unique<smb_surface>();
+                bool fallback = false;
+                if ((rc = finish_structure_device(m, G, i, Hc.eo.as<uint32_t>(), Hc.to.as<uint32_t>(), work.data(),
+                                                  work.size(), *s, &fallback, err, errlen))) {
+                    if (worker.joinable()) worker.join();
+                    return rc;
+                }
+                if (fallback) {
+                    host[i] = 1;
+                    continue;
+                }
+                s->stats.t_geometry = m->eng[i]->t_geometry;
+                s->stats.t_upload = m->eng[i]->t_upload;
+                m->out[i] = std::move(s);
+                m->latency[i] = ms_since(t_start);
+            }
+            t_finish += ms_since(t2);
+            bool any = false;
+            for (size_t i = G.s0; i < G.s1; i++) any = any || (host[i] && !m->redone[i]);
+            if (any) {  // the host threads need the group's lists
+                if (worker.joinable()) worker.join();
+                auto t3 = clk::now();
+                if ((rc = fetch_group(m, G, Hc, err, errlen, true))) return rc;
+                t_d2h += ms_since(t3);
+            }
+        }
         if (worker.joinable()) worker.join();
-        worker = std::thread([m, gi, hosts, &errs, t_start] {
+        worker = std::thread([m, gi, hosts, &errs, t_start, host] {
             const Group& G = m->groups[gi];
             const HostGroup& H = hosts[gi % 2];
             const uint32_t* eo = H.eo.as<uint32_t>();
@@ -745,7 +906,7 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
             // processing time first keeps the threads evenly loaded).
             std::vector<size_t> order;
             for (size_t i = G.s0; i < G.s1; i++)
-                if (!m->redone[i]) order.push_back(i);
+                if (!m->redone[i] && host[i]) order.push_back(i);
             auto edges_of = [&](size_t i) { return eo[m->b0[i + 1] - G.k0] - eo[m->b0[i] - G.k0]; };
             std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return edges_of(a) > edges_of(b); });
             parallel_for(order.size(), [&](size_t k, int) {
@@ -755,7 +916,7 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
         });
     }
     if (worker.joinable()) worker.join();
-    t_host = ms_since(t_host0) - t_device - t_d2h;
+    t_host = ms_since(t_host0) - t_device - t_d2h - t_finish;
     for (size_t i = 0; i < n; i++)
         if (!errs[i].empty()) return set_err(err, errlen, "structure %zu: %s", i, errs[i].c_str()), SMB_ERR_STATE;
     auto t3b = clk::now();
@@ -784,7 +945,7 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
         T.t_setup = m->t_setup;
         T.t_tune = m->t_tune;
         T.t_classify = cms;
-        T.t_device = t_device;
+        T.t_device = t_device + t_finish;
         T.t_d2h = t_d2h;
         T.t_host = t_host;
         T.t_redo = t_redo;

@@ -313,12 +313,14 @@ static int fetch_mc(smb_engine* e, char* err, size_t errlen) {
     return SMB_OK;
 }
 
+}  // extern "C"
+
 // Exact mode with every vertex refined on the device: assembly, validation,
 // measure and grouping there too, and the finished mesh back once.
 // SMB_OK, or an error code; *fallback when the device could not and the
 // host stages should run instead.
-static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long evals, unsigned long long cpu_edges,
-                               bool* fallback, double* ms_d2h, char* err, size_t errlen) {
+int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long evals, unsigned long long cpu_edges,
+                        bool* fallback, double* ms_d2h, char* err, size_t errlen) {
     *fallback = false;
     const smb_batch* b = e->batch;
     smb::DeviceMesh in{};
@@ -364,6 +366,9 @@ static int finish_exact_device(smb_engine* e, smb_surface& s, unsigned long long
     *ms_d2h = 0;  // the copies back overlap the measure
     return SMB_OK;
 }
+
+extern "C" {
+
 
 // Whole mesh stage and the stages after it: device part, results to the
 // host, f64 refinement (exact) or placement (fast), assembly, validation,

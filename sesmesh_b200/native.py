@@ -178,6 +178,7 @@ SIGNATURES = {
     "smb_multi_set_warm_start": (C.c_int, [_vp, _vp]),
     "smb_multi_tune": (C.c_int, [_vp, _cp, _sz]),
     "smb_multi_config_get": (C.c_int, [_vp, C.POINTER(MultiConfig)]),
+    "smb_multi_set_device_finish": (C.c_int, [_vp, C.c_int]),
     "smb_multi_run": (C.c_int, [_vp, C.POINTER(MultiTimes), _cp, _sz]),
     "smb_multi_surface": (_vp, [_vp, _sz]),
     "smb_multi_latency": (C.c_int, [_vp, C.POINTER(C.c_double)]),

@@ -354,6 +354,10 @@ class MultiBatch:
         self.warm = mlp  # kept alive while the batch uses it
         lib().smb_multi_set_warm_start(self.h, mlp.h if mlp is not None else None)
 
+    def set_device_finish(self, on=True):
+        """Finish each structure on the device (default) or on the host threads."""
+        lib().smb_multi_set_device_finish(self.h, 1 if on else 0)
+
     def tune(self):
         err = C.create_string_buffer(1024)
         _check(lib().smb_multi_tune(self.h, err, 1024), err)

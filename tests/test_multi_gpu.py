@@ -6,7 +6,8 @@ item, so the OBJ bytes and statistics are compared for equality, with the
 linear start and with the learned warm start.  The tuned configuration must
 give the single path's meshes at the brick edge it chose, the pass must run
 from a captured CUDA graph once recorded, and every structure must report a
-latency within the run.
+latency within the run; finishing each structure on the device and on the
+host threads gives the same bytes.
 """
 import numpy as np
 import pytest
@@ -77,3 +78,20 @@ def test_tuned_batch_equals_single_structure_path():
     assert t["structures"] == len(structs)
     _check(b, structs, cfg["brick"])
     b.close()
+
+
+def test_device_finish_equals_host_finish():
+    from sesmesh_b200 import surface as S
+    structs = _structures()
+    outs = []
+    for on in (True, False):
+        b = S.MultiBatch(structs, config=(10, 0, 4))
+        b.set_device_finish(on)
+        t = b.run()
+        assert t["structures"] == len(structs) and t["redone"] == 0
+        outs.append([(b.surface(i).obj(), b.surface(i).stats) for i in range(len(structs))])
+        b.close()
+    for (obj_d, st_d), (obj_h, st_h) in zip(*outs):
+        for k in ("vertices", "triangles", "components", "area", "volume", "refine_evaluations", "refine_cpu_edges"):
+            assert st_d[k] == st_h[k], (k, st_d[k], st_h[k])
+        assert obj_d == obj_h
