@@ -417,11 +417,11 @@ unsigned bits_for(uint32_t n) {
 
 }  // namespace
 
-void MeasureScratch::release() {
+void MeasureScratch::release(bool synced) {
     for (DBuf* b : {&pos, &nrm, &tris, &tris_out, &keys, &cnt, &dup, &parent, &flag, &cid, &id, &counters, &comp_v,
                     &comp_t, &comp_e, &area, &volume, &parts, &pkey, &pidx, &pkey2, &pidx2, &first, &tkey, &tidx,
                     &tkey2, &tidx2, &tiles, &cub, &packed, &err, &tri_a, &tri_v})
-        b->release();
+        synced ? b->release_synced() : b->release();
     pinned_free(host);
     host = nullptr;
     host_cap = 0;

@@ -17,7 +17,7 @@ struct MeasureScratch {
     void* host = nullptr;  // page-locked staging of the results
     size_t host_cap = 0;
     void* staging(size_t bytes);  // null when page-locked memory cannot be had
-    void release();
+    void release(bool synced = false);  // synced: the device has finished every use of them
     ~MeasureScratch() { release(); }
 };
 

@@ -748,9 +748,10 @@ int finish_structure_device(smb_multi* m, const Group& G, size_t i, const uint32
     // The engine's buffers go back to the memory cache afterwards: the next
     // structure takes them from there (one structure's worth held at a time).
     auto release = [&](int code) {
-        for (DBuf* x : b->bufs()) x->release();
-        e->measure.release();
-        mem_free(r->keys);
+        cudaDeviceSynchronize();
+        for (DBuf* x : b->bufs()) x->release_synced();
+        e->measure.release(true);
+        mem_free_synced(r->keys);
         r->keys = nullptr;
         r->n_bricks = 0;
         b->refined = b->refined_exact = false;

@@ -142,6 +142,19 @@ cudaError_t mem_alloc(void** p, size_t bytes) {
     return cudaSuccess;
 }
 
+void mem_free_synced(void* p) {
+    if (!p) return;
+    MemCache& C = mem_cache();
+    std::lock_guard<std::mutex> g(C.m);
+    auto it = C.live.find(p);
+    if (it == C.live.end()) {
+        cudaFree(p);
+        return;
+    }
+    C.free_blocks[it->second.first].emplace(it->second.second, p);
+    C.live.erase(it);
+}
+
 void mem_free(void* p) {
     if (!p) return;
     MemCache& C = mem_cache();
@@ -278,6 +291,12 @@ int DBuf::reserve(size_t bytes, char* err, size_t errlen) {
     }
     cap = want;
     return SMB_OK;
+}
+
+void DBuf::release_synced() {
+    if (p) mem_free_synced(p);
+    p = nullptr;
+    cap = 0;
 }
 
 void DBuf::release() {

@@ -17,6 +17,7 @@ struct DBuf {
     size_t cap = 0;
     int reserve(size_t bytes, char* err, size_t errlen);
     void release();
+    void release_synced();  // the device has finished every use of it (no synchronize here)
     template <class T>
     T* as() const {
         return static_cast<T*>(p);
@@ -30,6 +31,8 @@ int dev_alloc(void** p, size_t bytes, std::vector<void*>* owned, size_t* total, 
 // similar size on that device; mem_trim returns a device's cached blocks.
 cudaError_t mem_alloc(void** p, size_t bytes);
 void mem_free(void* p);
+// mem_free for a block the device has finished with (the caller synchronized).
+void mem_free_synced(void* p);
 void mem_trim(int device);
 void mem_device_open(int device);
 // Page-locked host memory through a process-wide cache (null on failure).
