@@ -37,6 +37,9 @@ struct DGrid {
     const uint32_t* items;
 };
 
+// DArr::pad flags.
+constexpr uint32_t DARR_ROWS_SORTED = 1;  // every neighbour row and circle-blocker list ascends
+
 // The resident arrangement, internal (Morton) sphere order.
 struct DArr {
     uint32_t n, nc, nv, pad;

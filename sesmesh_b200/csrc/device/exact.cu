@@ -128,14 +128,28 @@ __device__ __forceinline__ int x_find(const uint32_t* ids, uint32_t n, uint32_t 
 }
 
 // Blocker rows of the n sorted candidates kept to near spheres: counts
-// into off[1..n] ...
+// into off[1..n] ...  Rows that ascend (sorted: the arrangement's rows and
+// circle-blocker lists do) are merged with the ascending near list; other
+// rows are searched entry by entry.  Either way the kept entries keep their
+// row order.
 __device__ __forceinline__ void x_blocker_counts(const XView& v, const uint32_t* ids, uint32_t n,
                                                  const uint32_t* row_off, const uint32_t* row_items, uint32_t* off,
-                                                 uint32_t tid, uint32_t T) {
+                                                 bool sorted, uint32_t tid, uint32_t T) {
     for (uint32_t i = tid; i < n; i += T) {
         const uint32_t k = ids[i];
         uint32_t c = 0;
-        for (uint32_t p = row_off[k], e = row_off[k + 1]; p < e; p++) c += x_find(v.near_id, v.nn, row_items[p]) >= 0;
+        if (sorted) {
+            uint32_t p = row_off[k], pe = row_off[k + 1], q = 0;
+            while (p < pe && q < v.nn) {
+                const uint32_t x = row_items[p], y = v.near_id[q];
+                c += x == y;
+                p += x <= y;
+                q += y <= x;
+            }
+        } else {
+            for (uint32_t p = row_off[k], e = row_off[k + 1]; p < e; p++)
+                c += x_find(v.near_id, v.nn, row_items[p]) >= 0;
+        }
         off[i + 1] = c;
     }
 }
@@ -143,15 +157,51 @@ __device__ __forceinline__ void x_blocker_counts(const XView& v, const uint32_t*
 // ... then, with off scanned, the near-list positions into blk.
 __device__ __forceinline__ void x_blocker_fill(const XView& v, const uint32_t* ids, uint32_t n,
                                                const uint32_t* row_off, const uint32_t* row_items,
-                                               const uint32_t* off, uint32_t* blk, uint32_t tid, uint32_t T) {
+                                               const uint32_t* off, uint32_t* blk, bool sorted, uint32_t tid,
+                                               uint32_t T) {
     for (uint32_t i = tid; i < n; i += T) {
         const uint32_t k = ids[i];
         uint32_t at = off[i];
-        for (uint32_t p = row_off[k], e = row_off[k + 1]; p < e; p++) {
-            int pos = x_find(v.near_id, v.nn, row_items[p]);
-            if (pos >= 0) blk[at++] = uint32_t(pos);
+        if (sorted) {
+            uint32_t p = row_off[k], pe = row_off[k + 1], q = 0;
+            while (p < pe && q < v.nn) {
+                const uint32_t x = row_items[p], y = v.near_id[q];
+                if (x == y) blk[at++] = q;
+                p += x <= y;
+                q += y <= x;
+            }
+        } else {
+            for (uint32_t p = row_off[k], e = row_off[k + 1]; p < e; p++) {
+                int pos = x_find(v.near_id, v.nn, row_items[p]);
+                if (pos >= 0) blk[at++] = uint32_t(pos);
+            }
         }
     }
+}
+
+// off[0] = 0 and off[1..n] turned into their inclusive prefix sums, by the
+// warp (lanes over chunks of 32) or, in a block, by one thread.
+template <bool WIDE>
+__device__ __forceinline__ void x_offsets(uint32_t* off, uint32_t n, uint32_t tid) {
+    if (WIDE) {
+        if (tid == 0) {
+            off[0] = 0;
+            for (uint32_t i = 1; i <= n; i++) off[i] += off[i - 1];
+        }
+        return;
+    }
+    uint32_t carry = 0;
+    for (uint32_t b = 0; b < n; b += 32) {
+        const uint32_t i = b + tid + 1;
+        uint32_t x = i <= n ? off[i] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (int(tid) >= o) x += y;
+        }
+        if (i <= n) off[i] = carry + x;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+    }
+    if (tid == 0) off[0] = 0;
 }
 
 // Rank of (key, id) among n scratch pairs in (key, id) order.
@@ -281,24 +331,19 @@ __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsig
         v.v_p[r] = A.vert[vi];
     }
     // Blockers, kept to near spheres, in the scratch's place.
-    x_blocker_counts(v, v.s_id, c.ns, A.nb_off, A.nb_items, v.s_off, tid, T);
-    x_blocker_counts(v, v.c_id, c.nc, A.cb_off, A.cb_items, v.c_off, tid, T);
+    const bool sorted = A.pad & DARR_ROWS_SORTED;
+    x_blocker_counts(v, v.s_id, c.ns, A.nb_off, A.nb_items, v.s_off, sorted, tid, T);
+    x_blocker_counts(v, v.c_id, c.nc, A.cb_off, A.cb_items, v.c_off, sorted, tid, T);
     x_sync<WIDE>();
-    if (tid == 0) {
-        v.s_off[0] = 0;
-        for (uint32_t i = 1; i <= c.ns; i++) v.s_off[i] += v.s_off[i - 1];
-    }
-    if (tid == T - 1) {
-        v.c_off[0] = 0;
-        for (uint32_t i = 1; i <= c.nc; i++) v.c_off[i] += v.c_off[i - 1];
-    }
+    x_offsets<WIDE>(v.s_off, c.ns, tid);
+    x_offsets<WIDE>(v.c_off, c.nc, tid);
     x_sync<WIDE>();
     const size_t nsb = v.s_off[c.ns], ncb = v.c_off[c.nc];
     v.s_blk = reinterpret_cast<uint32_t*>(base + tail);
     v.c_blk = reinterpret_cast<uint32_t*>(base + xal(tail + nsb * 4));
     if (xal(tail + nsb * 4) + ncb * 4 > cap) return false;
-    x_blocker_fill(v, v.s_id, c.ns, A.nb_off, A.nb_items, v.s_off, v.s_blk, tid, T);
-    x_blocker_fill(v, v.c_id, c.nc, A.cb_off, A.cb_items, v.c_off, v.c_blk, tid, T);
+    x_blocker_fill(v, v.s_id, c.ns, A.nb_off, A.nb_items, v.s_off, v.s_blk, sorted, tid, T);
+    x_blocker_fill(v, v.c_id, c.nc, A.cb_off, A.cb_items, v.c_off, v.c_blk, sorted, tid, T);
     x_sync<WIDE>();
     return true;
 }

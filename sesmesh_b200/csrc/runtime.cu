@@ -517,6 +517,16 @@ int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_latt
     };
     DArr& A = r->A;
     A.n = uint32_t(n), A.nc = uint32_t(nc), A.nv = uint32_t(nv);
+    {  // rows that ascend let the exact refinement merge instead of search
+        bool sorted = true;
+        for (size_t i = 0; i < n && sorted; i++)
+            for (uint32_t p = a->nb_off[i] + 1; p < a->nb_off[i + 1] && sorted; p++)
+                sorted = a->nb_items[p - 1] < a->nb_items[p];
+        for (size_t c = 0; c < nc && sorted; c++)
+            for (uint32_t p = a->cb_off[c] + 1; p < a->cb_off[c + 1] && sorted; p++)
+                sorted = a->cb_items[p - 1] < a->cb_items[p];
+        A.pad = sorted ? DARR_ROWS_SORTED : 0u;
+    }
     void* p;
     if ((rc = up(&p, sph.data(), sph.size() * 8)) != SMB_OK) return fail(rc);
     A.sph = static_cast<const double4*>(p);
