@@ -59,6 +59,7 @@ struct XView {
     double* t_key;
     uint32_t* t_id;
     uint32_t nn, ni, ns, nc, nv;
+    double cx, cy, cz, rho;  // the ball
 };
 
 __device__ __forceinline__ size_t xal(size_t v) { return (v + 15) & ~size_t(15); }
@@ -230,6 +231,7 @@ __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsig
     const double cz = bz + (double((sb >> 2) * sub) + 0.5 * subd) * h;
     const double rho = 0.5 * sqrt(3.0) * subd * h * (1.0 + 1e-9) + 1e-9;
     const double reach = A.probe + L.band + rho;
+    v.cx = cx, v.cy = cy, v.cz = cz, v.rho = rho;
     x_sync<WIDE>();
     if (tid < 8) cnt[tid] = 0;
     x_sync<WIDE>();
@@ -405,7 +407,15 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
     double best = probe + band;
     if (COUNT) n_ops += 1;
     e.kind = XF_BEYOND;
-    for (uint32_t i = 0; i < v.ns && v.s_key[i] < best; i++) {
+    // Pruning at this point: a candidate's value here is at least its value
+    // at the ball's centre minus |x - centre| (each is 1-Lipschitz), so with
+    // slack = rho - |x - centre| (less a 1e-12 rounding margin, at least 0)
+    // the keys (centre value - rho - 1e-9, ascending) can stop a loop at
+    // best - slack instead of best: every candidate skipped could not go
+    // below best, so the result is the unpruned one.
+    const double ddx = x - v.cx, ddy = y - v.cy, ddz = z - v.cz;
+    const double slack = fmax(v.rho - sqrt(ddx * ddx + ddy * ddy + ddz * ddz) - 1e-12, 0.0);
+    for (uint32_t i = 0; i < v.ns && v.s_key[i] < best - slack; i++) {
         const double4 c = v.s_c[i];
         const double vx = x - c.x, vy = y - c.y, vz = z - c.z;
         const double len = sqrt(vx * vx + vy * vy + vz * vz);
@@ -426,7 +436,7 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
         }
         if (free) best = lb, e.kind = XF_SPHERE, e.id = v.s_id[i], e.qx = qx, e.qy = qy, e.qz = qz;
     }
-    for (uint32_t i = 0; i < v.nc && v.c_key[i] < best; i++) {
+    for (uint32_t i = 0; i < v.nc && v.c_key[i] < best - slack; i++) {
         const double4 m = v.c_m[i], u = v.c_u[i];
         const double yx = x - m.x, yy = y - m.y, yz = z - m.z;
         const double along = yx * u.x + yy * u.y + yz * u.z;
@@ -457,7 +467,7 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
         }
         if (free) best = dist, e.kind = XF_CIRCLE, e.id = v.c_id[i], e.qx = qx, e.qy = qy, e.qz = qz;
     }
-    for (uint32_t i = 0; i < v.nv && v.v_key[i] < best; i++) {
+    for (uint32_t i = 0; i < v.nv && v.v_key[i] < best - slack; i++) {
         const double4 p = v.v_p[i];
         const double d2 = sq3(x, y, z, p.x, p.y, p.z);
         if (COUNT) n_ops += 9;
