@@ -1130,13 +1130,19 @@ struct RefStage {
     const float4 *nearA, *nearT, *S, *C, *V;
     const uint32_t *s_id, *s_off, *s_blk, *c_off, *c_blk;
     int n_in, ns, nc, nv;
+    // Pruning keys (each candidate's value at the sub-block's centre, less
+    // rho and a 1e-3 A margin; C keys in C[3 i + 2].w): s_key null when the
+    // region has no room for the S keys (then neither list is pruned).
+    const float* s_key;
+    float cx, cy, cz, rho;
 };
 
 // One warp (BLOCK = false) or the whole block: stages work item j's
 // candidates at `base` and returns the view (ends with a warp / block barrier).
 template <bool BLOCK>
 __device__ RefStage stage_candidates(const DArr& A, const DLat& L, const BrickFrame& F, const uint32_t* R,
-                                     const uint32_t* ids, unsigned char* base) {
+                                     const uint32_t* ids, unsigned char* base, size_t cap, float cx, float cy,
+                                     float cz, float rho) {
     const int lane = BLOCK ? int(threadIdx.x) : int(threadIdx.x & 31), step = BLOCK ? int(blockDim.x) : 32;
     const int nn = int(R[R_NEAR]), n_in = int(R[R_INSIDE]), ns = int(R[R_S]), nc = int(R[R_C]), nv = int(R[R_V]);
     const int nsb = int(R[R_SBLK]), ncb = int(R[R_CBLK]);
@@ -1158,6 +1164,8 @@ __device__ RefStage stage_candidates(const DArr& A, const DLat& L, const BrickFr
     uint32_t* s_blk = s_off + ns + 1;
     uint32_t* c_off = s_blk + nsb;
     uint32_t* c_blk = c_off + nc + 1;
+    float* s_key = reinterpret_cast<float*>(c_blk + ncb);
+    const bool keyed = size_t(reinterpret_cast<unsigned char*>(s_key + ns) - base) <= cap;
     for (int i = lane; i < nn; i += step) {
         double4 c = A.sph[l_near[i]];
         float x, y, z;
@@ -1183,6 +1191,11 @@ __device__ RefStage stage_candidates(const DArr& A, const DLat& L, const BrickFr
             }
         S[i] = nearA[pos];
         s_id[i] = k;
+        if (keyed) {
+            const float4 c = nearA[pos];
+            const float dx = cx - c.x, dy = cy - c.y, dz = cz - c.z;
+            s_key[i] = fabsf(sqrtf(dx * dx + dy * dy + dz * dz) - c.w) - rho - 1e-3f;
+        }
     }
     for (int i = lane; i < nc; i += step) {
         const double* c = A.circ + 12 * size_t(l_c[i]);
@@ -1190,7 +1203,16 @@ __device__ RefStage stage_candidates(const DArr& A, const DLat& L, const BrickFr
         to_local(L, F, c[0], c[1], c[2], x, y, z);
         C[3 * i] = make_float4(x, y, z, float(c[9]));
         C[3 * i + 1] = make_float4(float(c[3]), float(c[4]), float(c[5]), float(c[6]));
-        C[3 * i + 2] = make_float4(float(c[7]), float(c[8]), __int_as_float(int(l_c[i])), 0.0f);
+        float key = 0.0f;
+        {
+            const float ux = float(c[3]), uy = float(c[4]), uz = float(c[5]);
+            const float yx = cx - x, yy = cy - y, yz = cz - z;
+            const float along = yx * ux + yy * uy + yz * uz;
+            const float wx = yx - ux * along, wy = yy - uy * along, wz = yz - uz * along;
+            const float wl = sqrtf(wx * wx + wy * wy + wz * wz), tt = wl - float(c[9]);
+            key = sqrtf(along * along + tt * tt) - rho - 1e-3f;
+        }
+        C[3 * i + 2] = make_float4(float(c[7]), float(c[8]), __int_as_float(int(l_c[i])), key);
     }
     for (int i = lane; i < nv; i += step) {
         double4 p = A.vert[l_v[i]];
@@ -1200,7 +1222,8 @@ __device__ RefStage stage_candidates(const DArr& A, const DLat& L, const BrickFr
     }
     if (BLOCK) __syncthreads();
     else __syncwarp();
-    return RefStage{nearA, nearT, S, C, V, s_id, s_off, s_blk, c_off, c_blk, n_in, ns, nc, nv};
+    return RefStage{nearA, nearT, S,  C,  V,  s_id, s_off, s_blk, c_off, c_blk, n_in, ns, nc, nv,
+                    keyed ? s_key : nullptr, cx, cy, cz, rho};
 }
 
 struct Eval {
@@ -1225,7 +1248,19 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
     }
     float best = probe + band;
     e.feat = 1u << FEAT_SHIFT_D;
+    // Pruning: a candidate's value here is at least its value at the centre
+    // minus |x - centre| (1-Lipschitz), the lists ascend in that centre value
+    // (the gather's order), and the keys hold it less rho and a 1e-3 A margin
+    // (far above f32 rounding): a loop stops once a key reaches best - slack,
+    // slack = rho - |x - centre|, since no later candidate can go below best.
+    const bool pruned = st.s_key != nullptr;
+    float slack = 0.0f;
+    if (pruned) {
+        const float qx = x - st.cx, qy = y - st.cy, qz = z - st.cz;
+        slack = fmaxf(st.rho - sqrtf(qx * qx + qy * qy + qz * qz) - 1e-5f, 0.0f);
+    }
     for (int i = 0; i < st.ns; i++) {
+        if (pruned && st.s_key[i] >= best - slack) break;
         float4 c = st.S[i];
         const uint32_t k = st.s_id[i];
         const float cx = c.x, cy = c.y, cz = c.z, rr = c.w;
@@ -1245,6 +1280,7 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
     }
     for (int i = 0; i < st.nc; i++) {
         float4 m = st.C[3 * i], u = st.C[3 * i + 1], w2 = st.C[3 * i + 2];
+        if (pruned && w2.w >= best - slack) break;
         float yx = x - m.x, yy = y - m.y, yz = z - m.z;
         float along = yx * u.x + yy * u.y + yz * u.z;
         float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
@@ -1417,8 +1453,13 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
         const uint32_t* R = rec + size_t(j) * REC_WORDS;
         if (WIDE) __syncthreads();
         else __syncwarp();
-        const RefStage st = WIDE ? stage_candidates<true>(A, L, F, R, ids, mine)
-                                 : stage_candidates<false>(A, L, F, R, ids, mine);
+        const int sb = int(j & 7), sub = L.sub;
+        const float h32 = float(L.h), half = 0.5f * float(sub);
+        const float ccx = (float((sb & 1) * sub) + half) * h32, ccy = (float(((sb >> 1) & 1) * sub) + half) * h32,
+                    ccz = (float((sb >> 2) * sub) + half) * h32;
+        const float crho = float(L.rho_sub) * 1.000001f + 1e-6f;
+        const RefStage st = WIDE ? stage_candidates<true>(A, L, F, R, ids, mine, P.cand_bytes, ccx, ccy, ccz, crho)
+                                 : stage_candidates<false>(A, L, F, R, ids, mine, P.cand_bytes, ccx, ccy, ccz, crho);
         const uint32_t step = WIDE ? blockDim.x : 32u;
         for (uint32_t e = a0 + (WIDE ? threadIdx.x : lane); e < a1; e += step) {
             const uint32_t k = item_edges[e];
