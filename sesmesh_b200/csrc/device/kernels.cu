@@ -1231,15 +1231,44 @@ struct Eval {
     uint32_t feat;
 };
 
-// eval_local in f32, brick-local (sesmesh.cuh eval_point semantics).
-__device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float band, float x, float y, float z) {
+// eval_local in f32, brick-local (sesmesh.cuh eval_point semantics), by a
+// group of RG lanes that all hold the same point: the lanes take RG
+// candidates of a list at a time and the group keeps the least value, the
+// earliest candidate on ties (a candidate replaces the best only when
+// strictly smaller, in list order, as one lane walking the list would), so
+// the result does not depend on RG.  gl: the lane's place in the group, gm:
+// the group's lanes.  RG = 1 is one lane per point.
+
+// The group's least (v, i), lexicographic.
+template <int RG>
+__device__ __forceinline__ void group_argmin(uint32_t gm, float& v, int& i) {
+#pragma unroll
+    for (int o = RG / 2; o; o >>= 1) {
+        const float v2 = __shfl_xor_sync(gm, v, o);
+        const int i2 = __shfl_xor_sync(gm, i, o);
+        if (v2 < v || (v2 == v && i2 < i)) v = v2, i = i2;
+    }
+}
+
+template <int RG>
+__device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float band, float x, float y, float z,
+                                         int gl, uint32_t gm) {
+    static_assert(RG == 1 || RG == 8 || RG == 32, "groups of 1, 8 or 32 lanes");
     Eval e;
     e.qx = x, e.qy = y, e.qz = z;
     bool inside = false;
-    for (int k = 0; k < st.n_in && !inside; k++) {
-        float4 a = st.nearA[k];
-        float dx = x - a.x, dy = y - a.y, dz = z - a.z;
-        inside = sqrtf(dx * dx + dy * dy + dz * dz) < a.w;
+    for (int k0 = 0; k0 < st.n_in; k0 += RG) {
+        const int k = k0 + gl;
+        bool in = false;
+        if (k < st.n_in) {
+            float4 a = st.nearA[k];
+            float dx = x - a.x, dy = y - a.y, dz = z - a.z;
+            in = sqrtf(dx * dx + dy * dy + dz * dz) < a.w;
+        }
+        if (__any_sync(gm, in)) {
+            inside = true;
+            break;
+        }
     }
     if (!inside) {
         e.value = probe;
@@ -1252,62 +1281,98 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
     // minus |x - centre| (1-Lipschitz), the lists ascend in that centre value
     // (the gather's order), and the keys hold it less rho and a 1e-3 A margin
     // (far above f32 rounding): a loop stops once a key reaches best - slack,
-    // slack = rho - |x - centre|, since no later candidate can go below best.
+    // slack = rho - |x - centre|, since no later candidate can go below best;
+    // a lane skips a candidate whose key does.
     const bool pruned = st.s_key != nullptr;
     float slack = 0.0f;
     if (pruned) {
         const float qx = x - st.cx, qy = y - st.cy, qz = z - st.cz;
         slack = fmaxf(st.rho - sqrtf(qx * qx + qy * qy + qz * qz) - 1e-5f, 0.0f);
     }
-    for (int i = 0; i < st.ns; i++) {
-        if (pruned && st.s_key[i] >= best - slack) break;
-        float4 c = st.S[i];
-        const uint32_t k = st.s_id[i];
-        const float cx = c.x, cy = c.y, cz = c.z, rr = c.w;
-        float dx = x - cx, dy = y - cy, dz = z - cz;
-        float len = sqrtf(dx * dx + dy * dy + dz * dz);
-        float lb = fabsf(len - rr);
-        if (lb >= best || len < 1e-12f) continue;
-        float sc = rr / len;
-        float qx = cx + dx * sc, qy = cy + dy * sc, qz = cz + dz * sc;
-        bool free = true;
-        for (uint32_t p = st.s_off[i], e2 = st.s_off[i + 1]; p < e2 && free; p++) {
-            float4 t = st.nearT[st.s_blk[p]];
-            float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
-            free = ex * ex + ey * ey + ez * ez >= t.w;
+    const int g0 = int(threadIdx.x & 31) & ~(RG - 1);  // the group's first lane
+    for (int i0 = 0; i0 < st.ns; i0 += RG) {
+        if (pruned && st.s_key[i0] >= best - slack) break;
+        const int i = i0 + gl;
+        float v = INFINITY, qx = 0.0f, qy = 0.0f, qz = 0.0f;
+        if (i < st.ns && !(pruned && st.s_key[i] >= best - slack)) {
+            float4 c = st.S[i];
+            const float cx = c.x, cy = c.y, cz = c.z, rr = c.w;
+            float dx = x - cx, dy = y - cy, dz = z - cz;
+            float len = sqrtf(dx * dx + dy * dy + dz * dz);
+            float lb = fabsf(len - rr);
+            if (!(lb >= best || len < 1e-12f)) {
+                float sc = rr / len;
+                qx = cx + dx * sc, qy = cy + dy * sc, qz = cz + dz * sc;
+                bool free = true;
+                for (uint32_t p = st.s_off[i], e2 = st.s_off[i + 1]; p < e2 && free; p++) {
+                    float4 t = st.nearT[st.s_blk[p]];
+                    float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
+                    free = ex * ex + ey * ey + ez * ez >= t.w;
+                }
+                if (free) v = lb;
+            }
         }
-        if (free) best = lb, e.feat = (2u << FEAT_SHIFT_D) | k, e.qx = qx, e.qy = qy, e.qz = qz;
+        int w = i;
+        group_argmin<RG>(gm, v, w);
+        if (v < best) {
+            const int src = g0 + (w - i0);
+            best = v;
+            e.feat = (2u << FEAT_SHIFT_D) | st.s_id[w];
+            e.qx = __shfl_sync(gm, qx, src), e.qy = __shfl_sync(gm, qy, src), e.qz = __shfl_sync(gm, qz, src);
+        }
     }
-    for (int i = 0; i < st.nc; i++) {
-        float4 m = st.C[3 * i], u = st.C[3 * i + 1], w2 = st.C[3 * i + 2];
-        if (pruned && w2.w >= best - slack) break;
-        float yx = x - m.x, yy = y - m.y, yz = z - m.z;
-        float along = yx * u.x + yy * u.y + yz * u.z;
-        float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
-        float wl = sqrtf(wx * wx + wy * wy + wz * wz);
-        float tt = wl - m.w;
-        float dist = sqrtf(along * along + tt * tt);
-        if (dist >= best) continue;
-        float qx, qy, qz;
-        if (wl > 1e-12f) {
-            qx = m.x + (wx / wl) * m.w, qy = m.y + (wy / wl) * m.w, qz = m.z + (wz / wl) * m.w;
-        } else {
-            qx = m.x + u.w * m.w, qy = m.y + w2.x * m.w, qz = m.z + w2.y * m.w;
+    for (int i0 = 0; i0 < st.nc; i0 += RG) {
+        if (pruned && st.C[3 * i0 + 2].w >= best - slack) break;
+        const int i = i0 + gl;
+        float v = INFINITY, qx = 0.0f, qy = 0.0f, qz = 0.0f;
+        if (i < st.nc) {
+            float4 m = st.C[3 * i], u = st.C[3 * i + 1], w2 = st.C[3 * i + 2];
+            if (!(pruned && w2.w >= best - slack)) {
+                float yx = x - m.x, yy = y - m.y, yz = z - m.z;
+                float along = yx * u.x + yy * u.y + yz * u.z;
+                float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
+                float wl = sqrtf(wx * wx + wy * wy + wz * wz);
+                float tt = wl - m.w;
+                float dist = sqrtf(along * along + tt * tt);
+                if (!(dist >= best)) {
+                    if (wl > 1e-12f) {
+                        qx = m.x + (wx / wl) * m.w, qy = m.y + (wy / wl) * m.w, qz = m.z + (wz / wl) * m.w;
+                    } else {
+                        qx = m.x + u.w * m.w, qy = m.y + w2.x * m.w, qz = m.z + w2.y * m.w;
+                    }
+                    bool free = true;
+                    for (uint32_t p = st.c_off[i], e2 = st.c_off[i + 1]; p < e2 && free; p++) {
+                        float4 t = st.nearT[st.c_blk[p]];
+                        float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
+                        free = ex * ex + ey * ey + ez * ez >= t.w;
+                    }
+                    if (free) v = dist;
+                }
+            }
         }
-        bool free = true;
-        for (uint32_t p = st.c_off[i], e2 = st.c_off[i + 1]; p < e2 && free; p++) {
-            float4 t = st.nearT[st.c_blk[p]];
-            float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
-            free = ex * ex + ey * ey + ez * ez >= t.w;
+        int w = i;
+        group_argmin<RG>(gm, v, w);
+        if (v < best) {
+            const int src = g0 + (w - i0);
+            best = v;
+            e.feat = (3u << FEAT_SHIFT_D) | uint32_t(__float_as_int(st.C[3 * w + 2].z));
+            e.qx = __shfl_sync(gm, qx, src), e.qy = __shfl_sync(gm, qy, src), e.qz = __shfl_sync(gm, qz, src);
         }
-        if (free)
-            best = dist, e.feat = (3u << FEAT_SHIFT_D) | uint32_t(__float_as_int(w2.z)), e.qx = qx, e.qy = qy, e.qz = qz;
     }
-    for (int i = 0; i < st.nv; i++) {
-        float4 p = st.V[i];
-        float dx = x - p.x, dy = y - p.y, dz = z - p.z;
-        float d = sqrtf(dx * dx + dy * dy + dz * dz);
-        if (d < best) best = d, e.feat = (4u << FEAT_SHIFT_D) | uint32_t(__float_as_int(p.w)), e.qx = p.x, e.qy = p.y, e.qz = p.z;
+    for (int i0 = 0; i0 < st.nv; i0 += RG) {
+        const int i = i0 + gl;
+        float v = INFINITY;
+        if (i < st.nv) {
+            float4 p = st.V[i];
+            float dx = x - p.x, dy = y - p.y, dz = z - p.z;
+            v = sqrtf(dx * dx + dy * dy + dz * dz);
+        }
+        int w = i;
+        group_argmin<RG>(gm, v, w);
+        if (v < best) {
+            const float4 p = st.V[w];
+            best = v, e.feat = (4u << FEAT_SHIFT_D) | uint32_t(__float_as_int(p.w)), e.qx = p.x, e.qy = p.y, e.qz = p.z;
+        }
     }
     e.value = probe - best;
     return e;
@@ -1316,9 +1381,10 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
 // The f32 root search of one crossing edge (extract.rs:425-535 iteration:
 // Newton with the Illinois bracket for MAX_ITER evaluations, then
 // bisection), from t_start; writes edge k's outputs.
+template <int RG>
 __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const RefineConsts& RC, float probe, float band,
                                                 float ax, float ay, float az, uint32_t axis, float fa, float fb,
-                                                float t_start, uint32_t k, const RefOut& out) {
+                                                float t_start, uint32_t k, const RefOut& out, int gl, uint32_t gm) {
     const float h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
     float t = t_start;
     float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
@@ -1329,7 +1395,7 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
     last.feat = 1u << FEAT_SHIFT_D, last.qx = last.qy = last.qz = 0.0f, last.value = 0.0f;
     for (uint32_t it = 0; it < RC.max_iter; it++) {
         float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
-        Eval e = eval_f32(st, probe, band, x, y, z);
+        Eval e = eval_f32<RG>(st, probe, band, x, y, z, gl, gm);
         evals++;
         last = e;
         float gv = e.value;
@@ -1366,7 +1432,7 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
         for (uint32_t it = 0; it < RC.max_bisect; it++) {
             t = 0.5f * (t0 + t1);
             float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
-            Eval e = eval_f32(st, probe, band, x, y, z);
+            Eval e = eval_f32<RG>(st, probe, band, x, y, z, gl, gm);
             evals++;
             last = e;
             if (fabsf(e.value) <= RC.tol || (t1 - t0) * hd <= 2.0f * RC.tol) break;
@@ -1374,6 +1440,7 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
             else t1 = t;
         }
     }
+    if (gl) return;
     out.t[k] = t;
     out.feat[k] = last.feat;
     out.q[3 * size_t(k)] = last.qx, out.q[3 * size_t(k) + 1] = last.qy, out.q[3 * size_t(k) + 2] = last.qz;
@@ -1383,8 +1450,9 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
 // Fast-mode refinement over the work items' edge lists (k_item_edges).
 // Work is claimed from a queue (counters[CNT_QUEUE]) by persistent CTAs:
 //   REFINE_PLAIN:  each warp claims items and refines the item's edges from
-//                  the linear guess (the reference's fast mode), lane per
-//                  edge, candidates staged in the warp's shared region;
+//                  the linear guess (the reference's fast mode), a group
+//                  of RG lanes per edge, candidates staged in the warp's
+//                  shared region;
 //   REFINE_MLP:    each CTA claims REFINE_BATCH quads of REFINE_WARPS items.
 //                  Phase A: the batch's edges, packed densely in 128-row
 //                  tiles (thread r holds row r), get their features and one
@@ -1410,12 +1478,12 @@ struct RefinePlan {
     uint32_t first_off;   // phase A: first S candidates, REFINE_WARPS x REFINE_BATCH x FEATURE_SCAN float4
 };
 
-template <int MODE, bool WIDE, bool MANY>
+template <int MODE, bool WIDE, bool MANY, int RG>
 __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
     DArr A0, DLat L0, RefineConsts RC0, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
     const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
     uint32_t n_host, RefOut out, const float* values, MlpDev mlp, float* feat_out, RefinePlan P,
-    unsigned long long* counters, Scene S) {
+    unsigned long long* counters, Scene S, uint32_t* ovf, const uint32_t* list) {
     const uint32_t n_items = MANY ? uint32_t(*S.n_work) : n_host;
     extern __shared__ __align__(128) float4 rs[];
     __shared__ uint32_t sh_q, sh_next;
@@ -1451,6 +1519,16 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
         const float probe = L.probe32, band = L.band32;
         const BrickFrame F = brick_frame(L, RC, key);
         const uint32_t* R = rec + size_t(j) * REC_WORDS;
+        if (!WIDE && ovf) {
+            // A sub-block whose candidates outgrow this warp's region goes
+            // to the list the whole-block pass takes after this one.
+            const size_t nn = R[R_NEAR], ns = R[R_S], nc = R[R_C], nv = R[R_V];
+            const size_t need = (2 * nn + ns + 3 * nc + nv) * 16 + (2 * ns + 1 + R[R_SBLK] + nc + 1 + R[R_CBLK]) * 4;
+            if (need > P.cand_bytes) {
+                if (lane == 0) ovf[1 + atomicAdd(ovf, 1u)] = i;
+                return;
+            }
+        }
         if (WIDE) __syncthreads();
         else __syncwarp();
         const int sb = int(j & 7), sub = L.sub;
@@ -1460,8 +1538,10 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
         const float crho = float(L.rho_sub) * 1.000001f + 1e-6f;
         const RefStage st = WIDE ? stage_candidates<true>(A, L, F, R, ids, mine, P.cand_bytes, ccx, ccy, ccz, crho)
                                  : stage_candidates<false>(A, L, F, R, ids, mine, P.cand_bytes, ccx, ccy, ccz, crho);
-        const uint32_t step = WIDE ? blockDim.x : 32u;
-        for (uint32_t e = a0 + (WIDE ? threadIdx.x : lane); e < a1; e += step) {
+        // A group of RG lanes per edge.
+        const uint32_t step = (WIDE ? blockDim.x : 32u) / RG, gl = lane % RG;
+        const uint32_t gm = (0xffffffffu >> (32 - RG)) << (lane & ~uint32_t(RG - 1));
+        for (uint32_t e = a0 + (WIDE ? threadIdx.x : lane) / RG; e < a1; e += step) {
             const uint32_t k = item_edges[e];
             uint32_t axis;
             int ex, ey, ez;
@@ -1469,9 +1549,24 @@ __global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
             edge_geom(L, RC, k, axis, ex, ey, ez, ax, ay, az);
             const float2 fv = edge_vals[k];
             const float t0 = MODE == REFINE_MLP ? out.t[k] : fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
-            refine_edge_f32(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, k, out);
+            refine_edge_f32<RG>(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, k, out, int(gl), gm);
         }
     };
+    if constexpr (MODE == REFINE_PLAIN && WIDE) {
+        if (list) {
+            // The sub-blocks the per-warp pass listed, one per block at a time.
+            const uint32_t n = *list;
+            for (;;) {
+                __syncthreads();
+                if (threadIdx.x == 0) sh_q = atomicAdd(queue, 1u);
+                __syncthreads();
+                const uint32_t q = sh_q;
+                if (q >= n) break;
+                refine_item(list[1 + q]);
+            }
+            return;
+        }
+    }
     if constexpr (MODE == REFINE_PLAIN && !WIDE) {
         for (;;) {
             uint32_t i = 0;
@@ -1732,7 +1827,8 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
                           const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
                           uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float* values,
                           const MlpDev* mlp, float* feat_out, unsigned long long* counters, int sms,
-                          size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many) {
+                          size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many, uint32_t* ovf,
+                          size_t region, int group) {
     auto al = [](size_t v) { return (v + 127) / 128 * 128; };
     RefinePlan P;
     P.cand_bytes = uint32_t(al(cand_bytes));
@@ -1747,40 +1843,68 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
     const size_t wide = keep + std::max(phase_a, size_t(P.cand_bytes));
     // One staging region per warp (an item per warp in flight, as many items
     // per SM as regions fit) while four fit in a block, else one per block.
+    // The plain single-structure pass instead keeps per-warp regions of the
+    // size asked for (default: two blocks of four to an SM) and hands the
+    // sub-blocks that outgrow them to a whole-block pass over a list.
     const bool use_wide = narrow > smem_limit;
+    size_t small = region ? region / 128 * 128 : (smem_limit / 2 - 1024) / REFINE_WARPS / 128 * 128;
+    small = std::max<size_t>(std::min(small, size_t(P.cand_bytes)), 128);
+    const bool split = mode == REFINE_PLAIN && !many && ovf && (use_wide || small < P.cand_bytes);
     const size_t smem = use_wide ? wide : narrow;
     if (smem_out) *smem_out = smem;
     if (!n_items) return cudaSuccess;
-    auto pick = [&](auto narrow_k, auto wide_k) { return use_wide ? wide_k : narrow_k; };
-    auto kern = many ? (mode == REFINE_MLP ? pick(k_refine<REFINE_MLP, false, true>, k_refine<REFINE_MLP, true, true>)
-                                           : pick(k_refine<REFINE_PLAIN, false, true>,
-                                                  k_refine<REFINE_PLAIN, true, true>))
-                     : (mode == REFINE_MLP
-                            ? pick(k_refine<REFINE_MLP, false, false>, k_refine<REFINE_MLP, true, false>)
-                            : (mode == EDGE_FEATURES
-                                   ? pick(k_refine<EDGE_FEATURES, false, false>, k_refine<EDGE_FEATURES, true, false>)
-                                   : pick(k_refine<REFINE_PLAIN, false, false>, k_refine<REFINE_PLAIN, true, false>)));
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    // Resident CTAs per SM from the plain kernel's occupancy at this shared
-    // memory size (the same limits; the TMEM columns cap the MLP kernel).
-    auto occ = use_wide ? k_refine<REFINE_PLAIN, true, false> : k_refine<REFINE_PLAIN, false, false>;
-    e = cudaFuncSetAttribute(occ, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, occ, 32 * REFINE_WARPS, smem);
-    if (e != cudaSuccess) return e;
-    if (mode == REFINE_MLP) per_sm = std::min(per_sm, 8);  // 64 TMEM columns per CTA of the SM's 512
-    const uint32_t quads = (n_items + REFINE_WARPS - 1) / REFINE_WARPS;
-    const uint32_t grid = std::min<uint32_t>(quads, uint32_t(std::max(1, sms * std::max(per_sm, 1))));
-    P.batch = std::max<uint32_t>(1, std::min<uint32_t>(REFINE_BATCH, quads / (4 * grid)));
-    cudaMemsetAsync(&counters[CNT_QUEUE], 0, sizeof(unsigned long long), s);
-    COUNT(1);
     MlpDev md = mlp ? *mlp : MlpDev{nullptr, nullptr, nullptr};
-    kern<<<grid, 32 * REFINE_WARPS, smem, s>>>(A, L, RC, keys, work, rec, ids, edges, edge_vals, item_off, item_edges,
-                                               n_items, RefOut{t, feat, q, evals}, values, md, feat_out, P, counters,
-                                               many ? *many : Scene{});
-    return cudaGetLastError();
+    // Launches kern with `bytes` of shared memory on as many CTAs as stay
+    // resident (the plain kernel of that width sets the occupancy; the TMEM
+    // columns cap the MLP kernel).
+    auto run = [&](auto kern, auto occ, const RefinePlan& PL, size_t bytes, uint32_t* o, const uint32_t* list,
+                   uint32_t units) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(occ, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+        if (e != cudaSuccess) return e;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, occ, 32 * REFINE_WARPS, bytes);
+        if (e != cudaSuccess) return e;
+        if (mode == REFINE_MLP) per_sm = std::min(per_sm, 8);  // 64 TMEM columns per CTA of the SM's 512
+        const uint32_t grid = std::min<uint32_t>(units, uint32_t(std::max(1, sms * std::max(per_sm, 1))));
+        RefinePlan Q = PL;
+        Q.batch = std::max<uint32_t>(1, std::min<uint32_t>(REFINE_BATCH, units / (4 * grid)));
+        cudaMemsetAsync(&counters[CNT_QUEUE], 0, sizeof(unsigned long long), s);
+        COUNT(1);
+        kern<<<grid, 32 * REFINE_WARPS, bytes, s>>>(A, L, RC, keys, work, rec, ids, edges, edge_vals, item_off,
+                                                     item_edges, n_items, RefOut{t, feat, q, evals}, values, md,
+                                                     feat_out, Q, counters, many ? *many : Scene{}, o, list);
+        return cudaGetLastError();
+    };
+    const uint32_t quads = (n_items + REFINE_WARPS - 1) / REFINE_WARPS;
+    const bool g32 = group == 32;
+    if (split) {
+        RefinePlan PS = P;
+        PS.cand_bytes = uint32_t(small);
+        cudaError_t e = cudaMemsetAsync(ovf, 0, 4, s);
+        if (e != cudaSuccess) return e;
+        auto kn = g32 ? k_refine<REFINE_PLAIN, false, false, 32> : k_refine<REFINE_PLAIN, false, false, 8>;
+        auto kw = g32 ? k_refine<REFINE_PLAIN, true, false, 32> : k_refine<REFINE_PLAIN, true, false, 8>;
+        e = run(kn, kn, PS, size_t(REFINE_WARPS) * small, ovf, nullptr, quads);
+        if (e != cudaSuccess) return e;
+        return run(kw, kw, P, wide, nullptr, ovf, n_items);
+    }
+    // Groups of lanes per edge: one lane in the many-structure pass (short
+    // lists, few evaluations after the warm start), else 8 or 32 as asked.
+    auto pick = [&](auto narrow_k, auto wide_k) { return use_wide ? wide_k : narrow_k; };
+    auto kern =
+        many ? (mode == REFINE_MLP ? pick(k_refine<REFINE_MLP, false, true, 1>, k_refine<REFINE_MLP, true, true, 1>)
+                                   : pick(k_refine<REFINE_PLAIN, false, true, 1>, k_refine<REFINE_PLAIN, true, true, 1>))
+        : mode == REFINE_MLP
+            ? (g32 ? pick(k_refine<REFINE_MLP, false, false, 32>, k_refine<REFINE_MLP, true, false, 32>)
+                   : pick(k_refine<REFINE_MLP, false, false, 8>, k_refine<REFINE_MLP, true, false, 8>))
+        : mode == EDGE_FEATURES
+            ? pick(k_refine<EDGE_FEATURES, false, false, 8>, k_refine<EDGE_FEATURES, true, false, 8>)
+            : (g32 ? pick(k_refine<REFINE_PLAIN, false, false, 32>, k_refine<REFINE_PLAIN, true, false, 32>)
+                   : pick(k_refine<REFINE_PLAIN, false, false, 8>, k_refine<REFINE_PLAIN, true, false, 8>));
+    auto occ = use_wide ? k_refine<REFINE_PLAIN, true, false, 8> : k_refine<REFINE_PLAIN, false, false, 8>;
+    return run(kern, occ, P, smem, nullptr, nullptr, quads);
 }
 
 }  // namespace smb

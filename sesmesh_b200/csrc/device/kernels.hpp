@@ -84,13 +84,19 @@ void launch_put_total(uint32_t* dst, const unsigned long long* total, cudaStream
 void launch_copy_count(unsigned long long* dst, const unsigned long long* src, cudaStream_t s);
 // Persistent refinement (or feature pass) over the items' edge lists; grid
 // = SMs x resident CTAs.  *smem_out gets the shared memory it needs (also
-// when it does not launch, for n_items = 0).
+// when it does not launch, for n_items = 0).  With ovf (n_items + 1 words)
+// the plain single-structure pass runs per-warp regions of `region` bytes
+// (0: an eighth of smem_limit, two blocks to an SM) where four regions for the largest sub-block
+// would not fit or `region` is smaller, then a whole-block pass over the
+// sub-blocks that outgrow them.  group: lanes per edge in the single-
+// structure passes, 8 or 32 (32 pays for long candidate lists).
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
                           const uint32_t* rec, const uint32_t* ids, const uint32_t* edges, const float2* edge_vals,
                           const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
                           uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float* values,
                           const MlpDev* mlp, float* feat_out, unsigned long long* counters, int sms,
-                          size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many = nullptr);
+                          size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many = nullptr,
+                          uint32_t* ovf = nullptr, size_t region = 0, int group = 8);
 
 unsigned long long kernel_launches();
 void count_launches(unsigned long long n);

@@ -811,6 +811,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     }
     b->ids_words = size_t(cnt[CNT_IDS]);
     b->max_pack = uint32_t(cnt[CNT_MAXPACK]);
+    b->pack_units = cnt[CNT_PACK];
     {
         // Caps for the next run of this batch: the list sizes seen, with an
         // eighth to spare, rounded to 16; warps per block so that a block's
@@ -891,6 +892,13 @@ int smb_resident_set_refinement(smb_resident* r, char* err, size_t errlen) {
     return SMB_OK;
 }
 
+// Lanes per edge in the f32 refinement: a warp when the sub-blocks' lists
+// average 16 KiB or more (the lane loops over them diverge most), else 8.
+static int refine_group(const smb_batch* b) {
+    if (b->r_group) return b->r_group;
+    return b->n_work && double(b->pack_units) * 16.0 >= 16384.0 * double(b->n_work) ? 32 : 8;
+}
+
 // One refinement-kernel pass over the sampled sub-blocks of the last run:
 // plain (linear start), warm (MLP start) or the feature pass (features of
 // each covered edge into e_x, evals = 1 marks it covered).
@@ -930,7 +938,8 @@ static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* m
     if ((rc = b->item_counts.reserve(size_t(nw) * 4, err, errlen)) ||
         (rc = b->item_off.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
         (rc = b->item_edges.reserve(ne * 4, err, errlen)) ||
-        (rc = b->tiles.reserve(size_t(scan_tiles_needed(nw)) * 8, err, errlen)))
+        (rc = b->tiles.reserve(size_t(scan_tiles_needed(nw)) * 8, err, errlen)) ||
+        (mode == REFINE_PLAIN && (rc = b->x_ovf.reserve(size_t(nw) * 4 + 8, err, errlen))))
         return rc;
     cudaEventRecord(b->ev[4], s);
     CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
@@ -950,7 +959,9 @@ static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* m
                                   b->e_t.as<float>(), b->e_feat.as<uint32_t>(), b->e_q.as<float>(),
                                   b->e_evals.as<uint32_t>(), cand, mode, b->values.as<float>(),
                                   mode == REFINE_MLP ? &md : nullptr, b->e_x.as<float>(), cnt,
-                                  d->info.multiprocessors, d->smem_optin, s, nullptr);
+                                  d->info.multiprocessors, d->smem_optin, s, nullptr, nullptr,
+                                  mode == REFINE_PLAIN ? b->x_ovf.as<uint32_t>() : nullptr, b->r_region,
+                                  refine_group(b));
     if (e != cudaSuccess) return set_err(err, errlen, "refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     cudaEventRecord(b->ev[5], s);
     CK(cudaStreamSynchronize(s));
@@ -1213,6 +1224,18 @@ int smb_batch_exact_summary(const smb_batch* b, unsigned long long* evaluations,
     if (evaluations) *evaluations = out[0];
     if (host_edges) *host_edges = out[1];
     if (exact_edges) *exact_edges = b->x_exact_edges;
+    return SMB_OK;
+}
+
+int smb_batch_set_refine_region(smb_batch* b, size_t bytes) {
+    if (!b || (bytes && (bytes < 1024 || bytes > 56 * 1024))) return SMB_ERR_ARG;
+    b->r_region = bytes;
+    return SMB_OK;
+}
+
+int smb_batch_set_refine_group(smb_batch* b, int lanes) {
+    if (!b || (lanes != 0 && lanes != 8 && lanes != 32)) return SMB_ERR_ARG;
+    b->r_group = lanes;
     return SMB_OK;
 }
 

@@ -135,6 +135,8 @@ SIGNATURES = {
     "smb_refine_exact": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
     "smb_batch_vertices": (C.c_int, [_vp, _fp, _fp, _u32p, C.POINTER(C.c_uint8), _fp, _u32p]),
     "smb_batch_set_exact_region": (C.c_int, [_vp, _sz]),
+    "smb_batch_set_refine_region": (C.c_int, [_vp, _sz]),
+    "smb_batch_set_refine_group": (C.c_int, [_vp, C.c_int]),
     "smb_batch_exact_summary": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
                                           C.POINTER(C.c_ulonglong)]),
     "smb_place_fast": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
@@ -408,11 +410,16 @@ class Batch:
         _check(lib().smb_batch_count_ops(self.h, C.byref(ops), C.byref(n), err, 1024), err)
         return ops.value, n.value
 
-    def refine(self, mlp=None):
+    def refine(self, mlp=None, region=None):
         """Fast-mode f32 refinement of the last run's crossing edges on the
-        device (smb_refine; smb_refine_warm with an Mlp); device ms."""
+        device (smb_refine; smb_refine_warm with an Mlp); device ms.  region:
+        per-warp bytes when four whole regions do not fit (0: an eighth of
+        the SM's shared memory)."""
         err = C.create_string_buffer(1024)
         lib().smb_resident_set_refinement(self.res.h, err, 1024)
+        if region is not None:
+            if lib().smb_batch_set_refine_region(self.h, int(region)) != SMB_OK:
+                raise ValueError("refine region must be 0 or 1 KiB..56 KiB, got %d" % region)
         ms = C.c_double(0)
         if mlp is None:
             _check(lib().smb_refine(self.res.h, self.h, C.byref(ms), err, 1024), err)

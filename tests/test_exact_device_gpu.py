@@ -10,7 +10,10 @@ The device must refine nearly every edge itself, and its whole-block path
 must give the same vertices as the warp path.  In fast mode the device's
 placement of the f32 roots (and exact refinement of the edges they do not
 settle) must equal the host placement byte for byte, with and without the
-learned warm start.
+learned warm start.  The f32 refinement's second pass (whole blocks for
+the sub-blocks whose lists outgrow a warp's region) must give the same mesh
+as one pass with regions for every sub-block, and groups of 8 or 32 lanes
+per edge the same mesh as each other.
 """
 import ctypes as C
 
@@ -40,7 +43,8 @@ def _cases():
     return out
 
 
-def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", warm=None):
+def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", warm=None, refine_region=None,
+          refine_group=None):
     from sesmesh_b200 import surface as S
     from sesmesh_b200.native import lib
     eng = S.SurfaceEngine(spheres, S.SurfaceParams.ses(probe).with_spacing(h).with_brick_size(brick)
@@ -50,6 +54,10 @@ def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", w
     eng.set_exact_on_device(on_device)
     if region is not None:
         assert lib().smb_batch_set_exact_region(lib().smb_engine_batch(eng.h), C.c_size_t(region)) == 0
+    if refine_region is not None:
+        assert lib().smb_batch_set_refine_region(lib().smb_engine_batch(eng.h), C.c_size_t(refine_region)) == 0
+    if refine_group is not None:
+        assert lib().smb_batch_set_refine_group(lib().smb_engine_batch(eng.h), refine_group) == 0
     out = eng.mesh()
     res = (out.obj(), dict(out.stats))
     out.close()
@@ -106,3 +114,16 @@ def test_fast_device_placement_with_warm_start_equals_host():
     for k in KEYS + ("refine_cpu_edges",):
         assert st_d[k] == st_h[k], (k, st_d[k], st_h[k])
     assert obj_d == obj_h
+
+
+@pytest.mark.parametrize("variant", [dict(refine_region=2048), dict(refine_group=32),
+                                     dict(refine_group=32, refine_region=4096)], ids=str)
+@pytest.mark.parametrize("case", [c for c in _cases() if c[0] in ("globule330@0.5", "globule2800@0.25")],
+                         ids=lambda c: c[0])
+def test_fast_refine_variants_give_one_mesh(case, variant):
+    name, spheres, probe, h = case
+    obj_1, st_1 = _mesh(spheres, probe, h, True, refine="fast", refine_group=8)
+    obj_2, st_2 = _mesh(spheres, probe, h, True, refine="fast", **variant)
+    for k in KEYS + ("refine_cpu_edges",):
+        assert st_1[k] == st_2[k], (k, st_1[k], st_2[k])
+    assert obj_1 == obj_2
