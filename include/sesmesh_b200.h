@@ -229,6 +229,10 @@ int smb_batch_set_refine_region(smb_batch* batch, size_t bytes);
  * smb_refine_warm: 8 or 32 (0, the default: 32 when the sub-blocks' lists
  * average 16 KiB or more, else 8).  The roots do not depend on it. */
 int smb_batch_set_refine_group(smb_batch* batch, int lanes);
+/* Lanes per edge in smb_refine_exact and the exact pass of smb_place_fast:
+ * 1, 8 or 32 (0, the default: 32 when the sub-blocks' lists average 16 KiB
+ * or more, else 1).  The vertices do not depend on it. */
+int smb_batch_set_exact_group(smb_batch* batch, int lanes);
 
 /* Sizes and times of the last run of a batch (diagnostics; BatchTimes and
  * DeviceBatch::bytes, batch.rs:118-129, 233). */

@@ -479,6 +479,138 @@ __device__ __forceinline__ XEval x_eval(const XView& v, const double* circ, doub
     return e;
 }
 
+// x_eval by a group of RG lanes that all hold the same point: the lanes
+// take RG candidates of a list at a time (each skipping one whose key
+// reaches best - slack) and the group keeps the least value, the earliest
+// candidate on ties; a candidate replaces the best only when strictly
+// smaller, as in x_eval's walk, so the result is x_eval's.  gl: the lane's
+// place in the group, gm: the group's lanes.
+template <int RG>
+__device__ __forceinline__ void x_argmin(uint32_t gm, double& v, int& i) {
+#pragma unroll
+    for (int o = RG / 2; o; o >>= 1) {
+        const double v2 = __shfl_xor_sync(gm, v, o);
+        const int i2 = __shfl_xor_sync(gm, i, o);
+        if (v2 < v || (v2 == v && i2 < i)) v = v2, i = i2;
+    }
+}
+
+template <int RG>
+__device__ __forceinline__ XEval x_eval_group(const XView& v, const double* circ, double probe, double band, double x,
+                                              double y, double z, int gl, uint32_t gm) {
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+    XEval e;
+    e.qx = x, e.qy = y, e.qz = z, e.id = 0;
+    bool inside = false;
+    for (uint32_t k0 = 0; k0 < v.ni; k0 += RG) {
+        const uint32_t k = k0 + gl;
+        bool in = false;
+        if (k < v.ni) {
+            const double4 c = v.in_c[k];
+            in = sqrt_lt(sq3(x, y, z, c.x, c.y, c.z), c.w);
+        }
+        if (__any_sync(gm, in)) {
+            inside = true;
+            break;
+        }
+    }
+    if (!inside) {
+        e.value = probe, e.kind = XF_SOLVENT;
+        return e;
+    }
+    double best = probe + band;
+    e.kind = XF_BEYOND;
+    const double ddx = x - v.cx, ddy = y - v.cy, ddz = z - v.cz;
+    const double slack = fmax(v.rho - sqrt(ddx * ddx + ddy * ddy + ddz * ddz) - 1e-12, 0.0);
+    const int g0 = int(threadIdx.x & 31) & ~(RG - 1);
+    for (uint32_t i0 = 0; i0 < v.ns && v.s_key[i0] < best - slack; i0 += RG) {
+        const uint32_t i = i0 + gl;
+        double val = inf, qx = 0.0, qy = 0.0, qz = 0.0;
+        if (i < v.ns && v.s_key[i] < best - slack) {
+            const double4 c = v.s_c[i];
+            const double vx = x - c.x, vy = y - c.y, vz = z - c.z;
+            const double len = sqrt(vx * vx + vy * vy + vz * vz);
+            const double lb = fabs(len - c.w);
+            if (!(lb >= best || len < 1e-12)) {
+                const double s = c.w / len;
+                qx = c.x + vx * s, qy = c.y + vy * s, qz = c.z + vz * s;
+                bool free = true;
+                for (uint32_t p = v.s_off[i], pe = v.s_off[i + 1]; p < pe; p++) {
+                    const double4 k = v.near_c[v.s_blk[p]];
+                    if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - X_EPS)) {
+                        free = false;
+                        break;
+                    }
+                }
+                if (free) val = lb;
+            }
+        }
+        int w = int(i);
+        x_argmin<RG>(gm, val, w);
+        if (val < best) {
+            const int src = g0 + (w - int(i0));
+            best = val, e.kind = XF_SPHERE, e.id = v.s_id[w];
+            e.qx = __shfl_sync(gm, qx, src), e.qy = __shfl_sync(gm, qy, src), e.qz = __shfl_sync(gm, qz, src);
+        }
+    }
+    for (uint32_t i0 = 0; i0 < v.nc && v.c_key[i0] < best - slack; i0 += RG) {
+        const uint32_t i = i0 + gl;
+        double val = inf, qx = 0.0, qy = 0.0, qz = 0.0;
+        if (i < v.nc && v.c_key[i] < best - slack) {
+            const double4 m = v.c_m[i], u = v.c_u[i];
+            const double yx = x - m.x, yy = y - m.y, yz = z - m.z;
+            const double along = yx * u.x + yy * u.y + yz * u.z;
+            const double wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
+            const double wl = sqrt(wx * wx + wy * wy + wz * wz);
+            const double dist2 = along * along + (wl - m.w) * (wl - m.w);
+            if (!sqrt_ge(dist2, best)) {
+                const double dist = sqrt(dist2);
+                double dx, dy, dz;
+                if (wl > 1e-12) {
+                    dx = wx / wl, dy = wy / wl, dz = wz / wl;
+                } else {  // on the axis: e1 (A.circ words 6..8)
+                    const double* C = circ + 12 * size_t(v.c_id[i]);
+                    dx = u.w, dy = C[7], dz = C[8];
+                }
+                qx = m.x + dx * m.w, qy = m.y + dy * m.w, qz = m.z + dz * m.w;
+                bool free = true;
+                for (uint32_t p = v.c_off[i], pe = v.c_off[i + 1]; p < pe; p++) {
+                    const double4 k = v.near_c[v.c_blk[p]];
+                    if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - X_EPS)) {
+                        free = false;
+                        break;
+                    }
+                }
+                if (free) val = dist;
+            }
+        }
+        int w = int(i);
+        x_argmin<RG>(gm, val, w);
+        if (val < best) {
+            const int src = g0 + (w - int(i0));
+            best = val, e.kind = XF_CIRCLE, e.id = v.c_id[w];
+            e.qx = __shfl_sync(gm, qx, src), e.qy = __shfl_sync(gm, qy, src), e.qz = __shfl_sync(gm, qz, src);
+        }
+    }
+    for (uint32_t i0 = 0; i0 < v.nv && v.v_key[i0] < best - slack; i0 += RG) {
+        const uint32_t i = i0 + gl;
+        double val = inf;
+        if (i < v.nv && v.v_key[i] < best - slack) {
+            const double4 p = v.v_p[i];
+            const double d2 = sq3(x, y, z, p.x, p.y, p.z);
+            if (sqrt_lt(d2, best)) val = sqrt(d2);
+        }
+        int w = int(i);
+        x_argmin<RG>(gm, val, w);
+        if (val < best) {
+            const double4 p = v.v_p[w];
+            best = val, e.kind = XF_VERTEX, e.id = v.v_id[w], e.qx = p.x, e.qy = p.y, e.qz = p.z;
+        }
+    }
+    e.value = probe - best;
+    return e;
+}
+
 __device__ __forceinline__ double x_clamp(double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 // The atom nearest to p among ids (extract.rs:566-576): its input index.
@@ -540,10 +672,13 @@ __device__ void x_attributes(const DArr& A, const DLat& L, const ExactAttr& X, u
     atom = bi < 0 ? 0u : X.orig[bi];
 }
 
-// extract::vertex of edge k (exact mode) and its attributes.
-template <bool COUNT = false>
+// extract::vertex of edge k (exact mode) and its attributes; RG > 1: by a
+// group of RG lanes (x_eval_group), the group's first lane placing it.
+template <bool COUNT = false, int RG = 1>
 __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat& L, const ExactAttr& X, int4 key, uint32_t k,
-                       uint32_t code, float2 fv, const ExactOut& out, unsigned long long* ops = nullptr) {
+                       uint32_t code, float2 fv, const ExactOut& out, unsigned long long* ops = nullptr, int gl = 0,
+                       uint32_t gm = 0xffffffffu) {
+    static_assert(RG == 1 || !COUNT, "operations are counted one lane per edge");
     const int b = L.b;
     const double h = L.h;
     const uint32_t cell = code / 3, axis = code % 3;
@@ -564,7 +699,8 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
     uint32_t evals = 0;
     for (int it = 0; it < X_MAX_ITER; it++) {
         const double x = pax + dx * t, y = pay + dy * t, z = paz + dz * t;
-        const XEval e = x_eval<COUNT>(v, A.circ, probe, band, x, y, z, ops);
+        const XEval e = RG == 1 ? x_eval<COUNT>(v, A.circ, probe, band, x, y, z, ops)
+                                : x_eval_group<RG>(v, A.circ, probe, band, x, y, z, gl, gm);
         evals++;
         last = e;
         const double g = e.value;
@@ -600,7 +736,9 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
         const bool neg0 = g0 < 0.0;
         for (int it = 0; it < X_MAX_BISECT; it++) {
             t = 0.5 * (t0 + t1);
-            const XEval e = x_eval<COUNT>(v, A.circ, probe, band, pax + dx * t, pay + dy * t, paz + dz * t, ops);
+            const double x = pax + dx * t, y = pay + dy * t, z = paz + dz * t;
+            const XEval e = RG == 1 ? x_eval<COUNT>(v, A.circ, probe, band, x, y, z, ops)
+                                    : x_eval_group<RG>(v, A.circ, probe, band, x, y, z, gl, gm);
             evals++;
             last = e;
             if (fabs(e.value) <= X_TOL || (t1 - t0) * len <= 2.0 * X_TOL) break;
@@ -608,6 +746,7 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
             else t1 = t;
         }
     }
+    if (gl) return;
     const double ct = x_clamp(t, X.t_min, 1.0 - X.t_min);
     const double px = pax + dx * ct, py = pay + dy * ct, pz = paz + dz * ct;
     double nx, ny, nz;
@@ -629,8 +768,9 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
 // not fit goes to ovf (ovf[0] = count, then the items).  SLAB = true: the
 // region is `region` bytes of a global slab per warp (read back through
 // L1), items come from ovf through counters[CNT_XQUEUE], and an item that
-// does not fit either stays with the host (*left counts them).
-template <bool SLAB, bool COUNT = false>
+// does not fit either stays with the host (*left counts them).  RG > 1: a
+// group of RG lanes per edge instead of a lane.
+template <bool SLAB, bool COUNT = false, int RG = 1>
 __global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L, ExactAttr X, const int4* keys,
                                                                const uint32_t* work, const uint32_t* edges,
                                                                const float2* edge_vals, const uint32_t* item_off,
@@ -664,9 +804,10 @@ __global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L
             }
             continue;
         }
-        for (uint32_t e = a0 + lane; e < a1; e += 32) {
+        const uint32_t gm = (0xffffffffu >> (32 - RG)) << (lane & ~uint32_t(RG - 1));
+        for (uint32_t e = a0 + lane / RG; e < a1; e += 32 / RG) {
             const uint32_t k = item_edges[e];
-            x_edge<COUNT>(v, A, L, X, key, k, edges[k], edge_vals[k], out, &ops);
+            x_edge<COUNT, RG>(v, A, L, X, key, k, edges[k], edge_vals[k], out, &ops, int(lane % RG), gm);
         }
     }
     if (COUNT) {
@@ -782,7 +923,7 @@ cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long 
     return cudaGetLastError();
 }
 
-template <bool COUNT>
+template <bool COUNT, int RG>
 static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                        const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
@@ -799,18 +940,25 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
                                 const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                 const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
-                                unsigned long long* counters, int sms, size_t region, cudaStream_t s, bool count) {
+                                unsigned long long* counters, int sms, size_t region, cudaStream_t s, bool count,
+                                int group) {
     if (count) {
         cudaError_t e = cudaMemsetAsync(&counters[CNT_OPS], 0, 8, s);
         if (e != cudaSuccess) return e;
-        return launch_exact_levels<true>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                         ovf, slab, slab_bytes, counters, sms, region, s);
+        return launch_exact_levels<true, 1>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
+                                            out, ovf, slab, slab_bytes, counters, sms, region, s);
     }
-    return launch_exact_levels<false>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out, ovf,
-                                      slab, slab_bytes, counters, sms, region, s);
+    if (group == 32)
+        return launch_exact_levels<false, 32>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
+                                              out, ovf, slab, slab_bytes, counters, sms, region, s);
+    if (group == 8)
+        return launch_exact_levels<false, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
+                                             out, ovf, slab, slab_bytes, counters, sms, region, s);
+    return launch_exact_levels<false, 1>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
+                                         ovf, slab, slab_bytes, counters, sms, region, s);
 }
 
-template <bool COUNT>
+template <bool COUNT, int RG>
 static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                        const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
@@ -823,8 +971,8 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
     if (!n_items) return cudaSuccess;
     region = (region + 15) & ~size_t(15);
     const size_t narrow = size_t(X_WARPS) * region;
-    auto kn = k_refine_exact<false, COUNT>;
-    auto kg = k_refine_exact<true, COUNT>;
+    auto kn = k_refine_exact<false, COUNT, RG>;
+    auto kg = k_refine_exact<true, COUNT, RG>;
     if ((e = cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(narrow))) != cudaSuccess)
         return e;
     int per_sm = 0;

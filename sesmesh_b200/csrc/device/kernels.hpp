@@ -142,7 +142,7 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                 const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                 unsigned long long* counters, int sms, size_t region, cudaStream_t s,
-                                bool count = false);
+                                bool count = false, int group = 1);
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);
 void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, unsigned long long* tiles,
                  unsigned long long* total, cudaStream_t s);

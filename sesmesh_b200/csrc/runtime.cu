@@ -899,6 +899,14 @@ static int refine_group(const smb_batch* b) {
     return b->n_work && double(b->pack_units) * 16.0 >= 16384.0 * double(b->n_work) ? 32 : 8;
 }
 
+// Lanes per edge in the exact refinement: a warp for lists of 16 KiB or
+// more on average, else a lane (short f64 lists gain less from groups than
+// the edges lose from running one at a time).
+static int exact_group(const smb_batch* b) {
+    if (b->x_group) return b->x_group;
+    return refine_group(b) == 32 ? 32 : 1;
+}
+
 // One refinement-kernel pass over the sampled sub-blocks of the last run:
 // plain (linear start), warm (MLP start) or the feature pass (features of
 // each covered edge into e_x, evals = 1 marks it covered).
@@ -1098,7 +1106,7 @@ static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* 
                                         b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->item_off.as<uint32_t>(),
                                         b->item_edges.as<uint32_t>(), nw, out, b->x_ovf.as<uint32_t>(),
                                         b->x_slab.as<unsigned char>(), slab, cnt, d->info.multiprocessors,
-                                        b->x_region, s, count);
+                                        b->x_region, s, count, exact_group(b));
     if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     uint32_t n_block = 0;
     CK(cudaMemcpyAsync(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost, s));
@@ -1230,6 +1238,12 @@ int smb_batch_exact_summary(const smb_batch* b, unsigned long long* evaluations,
 int smb_batch_set_refine_region(smb_batch* b, size_t bytes) {
     if (!b || (bytes && (bytes < 1024 || bytes > 56 * 1024))) return SMB_ERR_ARG;
     b->r_region = bytes;
+    return SMB_OK;
+}
+
+int smb_batch_set_exact_group(smb_batch* b, int lanes) {
+    if (!b || (lanes != 0 && lanes != 1 && lanes != 8 && lanes != 32)) return SMB_ERR_ARG;
+    b->x_group = lanes;
     return SMB_OK;
 }
 

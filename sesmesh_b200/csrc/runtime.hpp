@@ -110,6 +110,7 @@ struct smb_batch {
     size_t x_exact_edges = 0;  // edges the exact refinement took in the last pass
     size_t x_block_items = 0;  // items of the last exact pass refined by a whole block
     size_t x_region = 13312;  // shared-memory bytes per warp for one sub-block's f64 candidate lists
+    int x_group = 0;  // smb_refine_exact: lanes per edge (0: by the lists' mean size)
     int r_group = 0;  // smb_refine: lanes per edge (0: by the lists' mean size)
     unsigned long long pack_units = 0;  // the last run's list units (16 bytes each)
     size_t r_region = 0;  // smb_refine: bytes per warp's f32 region when four whole ones do not fit (0: an eighth of the SM's)

@@ -13,7 +13,8 @@ settle) must equal the host placement byte for byte, with and without the
 learned warm start.  The f32 refinement's second pass (whole blocks for
 the sub-blocks whose lists outgrow a warp's region) must give the same mesh
 as one pass with regions for every sub-block, and groups of 8 or 32 lanes
-per edge the same mesh as each other.
+per edge the same mesh as each other; so must 1, 8 or 32 lanes per edge in
+the exact refinement, in shared memory and in the global slabs.
 """
 import ctypes as C
 
@@ -44,7 +45,7 @@ def _cases():
 
 
 def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", warm=None, refine_region=None,
-          refine_group=None):
+          refine_group=None, exact_group=None):
     from sesmesh_b200 import surface as S
     from sesmesh_b200.native import lib
     eng = S.SurfaceEngine(spheres, S.SurfaceParams.ses(probe).with_spacing(h).with_brick_size(brick)
@@ -58,6 +59,8 @@ def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", w
         assert lib().smb_batch_set_refine_region(lib().smb_engine_batch(eng.h), C.c_size_t(refine_region)) == 0
     if refine_group is not None:
         assert lib().smb_batch_set_refine_group(lib().smb_engine_batch(eng.h), refine_group) == 0
+    if exact_group is not None:
+        assert lib().smb_batch_set_exact_group(lib().smb_engine_batch(eng.h), exact_group) == 0
     out = eng.mesh()
     res = (out.obj(), dict(out.stats))
     out.close()
@@ -124,6 +127,19 @@ def test_fast_refine_variants_give_one_mesh(case, variant):
     name, spheres, probe, h = case
     obj_1, st_1 = _mesh(spheres, probe, h, True, refine="fast", refine_group=8)
     obj_2, st_2 = _mesh(spheres, probe, h, True, refine="fast", **variant)
+    for k in KEYS + ("refine_cpu_edges",):
+        assert st_1[k] == st_2[k], (k, st_1[k], st_2[k])
+    assert obj_1 == obj_2
+
+
+@pytest.mark.parametrize("group", [8, 32])
+@pytest.mark.parametrize("region", [None, 1024], ids=["shared", "slab"])
+@pytest.mark.parametrize("case", [c for c in _cases() if c[0] in ("chain5", "globule330@0.5", "globule2800@0.25",
+                                                                   "stall4")], ids=lambda c: c[0])
+def test_exact_groups_give_one_mesh(case, region, group):
+    name, spheres, probe, h = case
+    obj_1, st_1 = _mesh(spheres, probe, h, True, region=region, exact_group=1)
+    obj_2, st_2 = _mesh(spheres, probe, h, True, region=region, exact_group=group)
     for k in KEYS + ("refine_cpu_edges",):
         assert st_1[k] == st_2[k], (k, st_1[k], st_2[k])
     assert obj_1 == obj_2
