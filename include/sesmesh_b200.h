@@ -233,6 +233,10 @@ int smb_batch_set_refine_group(smb_batch* batch, int lanes);
  * 1, 8 or 32 (0, the default: 32 when the sub-blocks' lists average 16 KiB
  * or more, else 1).  The vertices do not depend on it. */
 int smb_batch_set_exact_group(smb_batch* batch, int lanes);
+/* Shared memory of each sampling CTA in a first pass over the sub-blocks
+ * whose packed lists fit it (>= 1 KiB; 0, the default: 56 KiB); the others
+ * run in a second pass with room for the largest. */
+int smb_batch_set_sample_region(smb_batch* batch, size_t bytes);
 
 /* Sizes and times of the last run of a batch (diagnostics; BatchTimes and
  * DeviceBatch::bytes, batch.rs:118-129, 233). */

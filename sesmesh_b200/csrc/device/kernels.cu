@@ -628,15 +628,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 constexpr uint32_t BULK_CHUNK = 32768;            // bytes per bulk copy
 constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;     // bounded wait
 
-template <bool TMA, bool COUNT, bool MANY>
+// list (single structure): blocks whose packed block exceeds limit_units
+// append their index to list (list[0] = count) and return; LIST: block b
+// samples the list's b-th entry (none past the count).
+template <bool TMA, bool COUNT, bool MANY, bool LIST = false>
 __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work,
                                                 const uint32_t* rec, const uint4* pack, float* values,
-                                                unsigned long long* counters, Scene SC) {
+                                                unsigned long long* counters, Scene SC, uint32_t limit_units,
+                                                uint32_t* list) {
     extern __shared__ __align__(16) uint4 sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t sts[8];
     if (MANY && blockIdx.x >= uint32_t(*SC.n_work)) return;
-    const uint32_t j = work[blockIdx.x];
+    if (LIST && blockIdx.x >= list[0]) return;
+    const uint32_t slot = LIST ? list[1 + blockIdx.x] : blockIdx.x;
+    const uint32_t j = work[slot];
     const uint32_t brick = j >> 3, sb = j & 7;
     const DLat& L = MANY ? SC.lat[keys[brick].w] : L0;
     const uint32_t* R = rec + size_t(j) * REC_WORDS;
@@ -644,6 +650,10 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
     const int nn = int(R[R_NEAR]), n_in = int(R[R_INSIDE]), ns = int(R[R_S]), nc = int(R[R_C]), nv = int(R[R_V]);
     const int nsb = int(R[R_SBLK]);
     const uint32_t units = R[R_PACKLEN];
+    if (!LIST && list && units > limit_units) {
+        if (threadIdx.x == 0) list[1 + atomicAdd(list, 1u)] = slot;
+        return;
+    }
     const uint4* src = pack + R[R_PACK];
     if (threadIdx.x < 8) sts[threadIdx.x] = rec[(size_t(brick) * 8 + threadIdx.x) * REC_WORDS + R_STATE];
     if (TMA) {
@@ -1759,16 +1769,29 @@ cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const 
 
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
-                          bool count, cudaStream_t s, const Scene* many) {
+                          bool count, cudaStream_t s, const Scene* many, uint32_t* list, size_t small) {
     if (!n) return cudaSuccess;
     size_t smem = size_t(max_units) * 16;
     auto kern = many ? k_sample<true, false, true>
                      : (count ? k_sample<true, true, false>
                               : (tma ? k_sample<true, false, false> : k_sample<false, false, false>));
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    // Shared memory for the largest block on every CTA can leave an SM a
+    // few CTAs: the blocks up to `small` bytes run first with that much,
+    // the rest after them with all of it.
+    const bool split = list && !many && !count && tma && small >= 16 && smem > small;
+    const size_t first = split ? small / 16 * 16 : smem;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(first));
     if (e != cudaSuccess) return e;
+    if (split && (e = cudaMemsetAsync(list, 0, 4, s)) != cudaSuccess) return e;
     COUNT(1);
-    kern<<<n, 128, smem, s>>>(L, keys, work, n, rec, pack, values, counters, many ? *many : Scene{});
+    kern<<<n, 128, first, s>>>(L, keys, work, n, rec, pack, values, counters, many ? *many : Scene{},
+                               uint32_t(first / 16), split ? list : nullptr);
+    if (!split) return cudaGetLastError();
+    auto rest = k_sample<true, false, false, true>;
+    if ((e = cudaFuncSetAttribute(rest, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) != cudaSuccess)
+        return e;
+    COUNT(1);
+    rest<<<n, 128, smem, s>>>(L, keys, work, n, rec, pack, values, counters, Scene{}, 0, list);
     return cudaGetLastError();
 }
 

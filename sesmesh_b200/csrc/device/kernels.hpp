@@ -158,9 +158,13 @@ void launch_substates(const DArr& A, const DLat& L, const int4* keys, uint32_t n
 cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const uint32_t* work, uint32_t n,
                           const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s,
                           const Scene* many = nullptr);
+// One CTA per sampled sub-block with the largest packed block's bytes of
+// shared memory; with list (n + 1 words) and small, two passes: the blocks
+// of up to small bytes with small bytes each, then the others.
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
-                          bool count, cudaStream_t s, const Scene* many = nullptr);
+                          bool count, cudaStream_t s, const Scene* many = nullptr, uint32_t* list = nullptr,
+                          size_t small = 0);
 cudaError_t launch_mc(const DLat& L, uint32_t n, float* values, const uint32_t* rec, uint32_t* counts, const uint32_t* edge_off,
                       const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
                       cudaStream_t s, const int4* keys = nullptr,

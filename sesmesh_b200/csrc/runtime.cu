@@ -833,9 +833,13 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     if (size_t(b->max_pack) * 16 > size_t(d->smem_optin))
         return set_err(err, errlen, "a sub-block's candidates (%u x 16 bytes) exceed shared memory", b->max_pack),
                SMB_ERR_MEMORY;
+    const size_t small = b->s_region ? b->s_region : SAMPLE_REGION;
+    if (size_t(b->max_pack) * 16 > small && (rc = b->s_list.reserve(size_t(n_work) * 4 + 4, err, errlen)))
+        return rc;
     cudaError_t e = launch_sample(L, keys, b->work.as<uint32_t>(), uint32_t(n_work), b->rec.as<uint32_t>(),
                                   b->pack.as<uint4>(), b->max_pack, b->values.as<float>(),
-                                  b->counters.as<unsigned long long>(), b->use_tma, false, s);
+                                  b->counters.as<unsigned long long>(), b->use_tma, false, s, nullptr,
+                                  size_t(b->max_pack) * 16 > small ? b->s_list.as<uint32_t>() : nullptr, small);
     if (e != cudaSuccess) return set_err(err, errlen, "sample launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     cudaEventRecord(b->ev[3], s);
 
@@ -1238,6 +1242,12 @@ int smb_batch_exact_summary(const smb_batch* b, unsigned long long* evaluations,
 int smb_batch_set_refine_region(smb_batch* b, size_t bytes) {
     if (!b || (bytes && (bytes < 1024 || bytes > 56 * 1024))) return SMB_ERR_ARG;
     b->r_region = bytes;
+    return SMB_OK;
+}
+
+int smb_batch_set_sample_region(smb_batch* b, size_t bytes) {
+    if (!b || (bytes && bytes < 1024)) return SMB_ERR_ARG;
+    b->s_region = bytes;
     return SMB_OK;
 }
 

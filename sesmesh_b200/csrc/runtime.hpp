@@ -92,6 +92,10 @@ struct smb_resident {
     std::atomic<bool> freed{false}, gone{false};
 };
 
+// Shared memory of the sampling's first-pass CTAs (sub-blocks whose packed
+// lists are larger wait for a second pass with room for the largest).
+constexpr size_t SAMPLE_REGION = 56 * 1024;
+
 struct smb_batch {
     smb_resident* res = nullptr;
     uint32_t n = 0, n_work = 0, max_pack = 0;
@@ -110,6 +114,8 @@ struct smb_batch {
     size_t x_exact_edges = 0;  // edges the exact refinement took in the last pass
     size_t x_block_items = 0;  // items of the last exact pass refined by a whole block
     size_t x_region = 13312;  // shared-memory bytes per warp for one sub-block's f64 candidate lists
+    size_t s_region = 0;  // sampling: shared memory of the first pass's CTAs (0: SAMPLE_REGION)
+    smb::DBuf s_list;     // sampling: the sub-blocks left to the second pass
     int x_group = 0;  // smb_refine_exact: lanes per edge (0: by the lists' mean size)
     int r_group = 0;  // smb_refine: lanes per edge (0: by the lists' mean size)
     unsigned long long pack_units = 0;  // the last run's list units (16 bytes each)
@@ -121,6 +127,6 @@ struct smb_batch {
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
                 &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &item_counts, &item_off, &item_edges,
-                &x_pos, &x_nrm, &x_atom, &x_patch, &x_t, &x_evals, &x_ovf, &x_sum, &x_mask, &x_slab};
+                &x_pos, &x_nrm, &x_atom, &x_patch, &x_t, &x_evals, &x_ovf, &x_sum, &x_mask, &x_slab, &s_list};
     }
 };

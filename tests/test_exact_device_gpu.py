@@ -14,7 +14,8 @@ learned warm start.  The f32 refinement's second pass (whole blocks for
 the sub-blocks whose lists outgrow a warp's region) must give the same mesh
 as one pass with regions for every sub-block, and groups of 8 or 32 lanes
 per edge the same mesh as each other; so must 1, 8 or 32 lanes per edge in
-the exact refinement, in shared memory and in the global slabs.
+the exact refinement, in shared memory and in the global slabs, and the
+sampling's second pass (sub-blocks over the first pass's shared memory).
 """
 import ctypes as C
 
@@ -45,7 +46,7 @@ def _cases():
 
 
 def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", warm=None, refine_region=None,
-          refine_group=None, exact_group=None):
+          refine_group=None, exact_group=None, sample_region=None):
     from sesmesh_b200 import surface as S
     from sesmesh_b200.native import lib
     eng = S.SurfaceEngine(spheres, S.SurfaceParams.ses(probe).with_spacing(h).with_brick_size(brick)
@@ -61,6 +62,8 @@ def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", w
         assert lib().smb_batch_set_refine_group(lib().smb_engine_batch(eng.h), refine_group) == 0
     if exact_group is not None:
         assert lib().smb_batch_set_exact_group(lib().smb_engine_batch(eng.h), exact_group) == 0
+    if sample_region is not None:
+        assert lib().smb_batch_set_sample_region(lib().smb_engine_batch(eng.h), C.c_size_t(sample_region)) == 0
     out = eng.mesh()
     res = (out.obj(), dict(out.stats))
     out.close()
@@ -120,7 +123,7 @@ def test_fast_device_placement_with_warm_start_equals_host():
 
 
 @pytest.mark.parametrize("variant", [dict(refine_region=2048), dict(refine_group=32),
-                                     dict(refine_group=32, refine_region=4096)], ids=str)
+                                     dict(refine_group=32, refine_region=4096), dict(sample_region=2048)], ids=str)
 @pytest.mark.parametrize("case", [c for c in _cases() if c[0] in ("globule330@0.5", "globule2800@0.25")],
                          ids=lambda c: c[0])
 def test_fast_refine_variants_give_one_mesh(case, variant):
