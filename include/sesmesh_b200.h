@@ -231,7 +231,8 @@ int smb_batch_set_refine_region(smb_batch* batch, size_t bytes);
 int smb_batch_set_refine_group(smb_batch* batch, int lanes);
 /* Lanes per edge in smb_refine_exact and the exact pass of smb_place_fast:
  * 1, 8 or 32 (0, the default: 32 when the sub-blocks' lists average 16 KiB
- * or more, else 1).  The vertices do not depend on it. */
+ * or more, else 1); the pass over sub-blocks with global list slabs takes
+ * at least 8.  The vertices do not depend on it. */
 int smb_batch_set_exact_group(smb_batch* batch, int lanes);
 /* Shared memory of each sampling CTA in a first pass over the sub-blocks
  * whose packed lists fit it (>= 1 KiB; 0, the default: 56 KiB); the others

@@ -923,7 +923,7 @@ cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long 
     return cudaGetLastError();
 }
 
-template <bool COUNT, int RG>
+template <bool COUNT, int RG, int RGS>
 static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                        const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
@@ -945,20 +945,21 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
     if (count) {
         cudaError_t e = cudaMemsetAsync(&counters[CNT_OPS], 0, 8, s);
         if (e != cudaSuccess) return e;
-        return launch_exact_levels<true, 1>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                            out, ovf, slab, slab_bytes, counters, sms, region, s);
+        return launch_exact_levels<true, 1, 1>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges,
+                                               n_items, out, ovf, slab, slab_bytes, counters, sms, region, s);
     }
+    // The slab pass takes the largest lists: at least 8 lanes per edge.
     if (group == 32)
-        return launch_exact_levels<false, 32>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                              out, ovf, slab, slab_bytes, counters, sms, region, s);
+        return launch_exact_levels<false, 32, 32>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges,
+                                                  n_items, out, ovf, slab, slab_bytes, counters, sms, region, s);
     if (group == 8)
-        return launch_exact_levels<false, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                             out, ovf, slab, slab_bytes, counters, sms, region, s);
-    return launch_exact_levels<false, 1>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                         ovf, slab, slab_bytes, counters, sms, region, s);
+        return launch_exact_levels<false, 8, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
+                                                out, ovf, slab, slab_bytes, counters, sms, region, s);
+    return launch_exact_levels<false, 1, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
+                                            out, ovf, slab, slab_bytes, counters, sms, region, s);
 }
 
-template <bool COUNT, int RG>
+template <bool COUNT, int RG, int RGS>
 static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                        const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
@@ -972,7 +973,7 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
     region = (region + 15) & ~size_t(15);
     const size_t narrow = size_t(X_WARPS) * region;
     auto kn = k_refine_exact<false, COUNT, RG>;
-    auto kg = k_refine_exact<true, COUNT, RG>;
+    auto kg = k_refine_exact<true, COUNT, RGS>;
     if ((e = cudaFuncSetAttribute(kn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(narrow))) != cudaSuccess)
         return e;
     int per_sm = 0;

@@ -682,11 +682,32 @@ int finish_on_device(smb_device* d, const DeviceMesh& in, smbh::MeshRef* out, vo
     unsigned char* h_comp = h_atom + nv * 4;
     unsigned char* h_patch = h_comp + nv * 4;
     unsigned char* h_tris = h_patch + nv;
+    // The vertex arrays go back on the copy stream while the measure's
+    // kernels run on the main one (the copies wait for everything the main
+    // stream has queued so far); every return below waits for them.
+    cudaStream_t cs = d->copy ? d->copy : s;
+    struct Join {
+        cudaStream_t c;
+        ~Join() {
+            if (c) cudaStreamSynchronize(c);
+        }
+    } join{cs != s ? cs : nullptr};
+    if (cs != s) {
+        cudaEvent_t ready;
+        if (cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess) {
+            if (msg) *msg = "copy event";
+            return 1;
+        }
+        const bool ok = cudaEventRecord(ready, s) == cudaSuccess && cudaStreamWaitEvent(cs, ready, 0) == cudaSuccess;
+        cudaEventDestroy(ready);
+        if (!ok) {
+            if (msg) *msg = "copy event";
+            return 1;
+        }
+    }
     auto d2h = [&](void* dst, const void* src, size_t bytes) {
-        return !bytes || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+        return !bytes || cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, cs) == cudaSuccess;
     };
-    // The vertex arrays go back while the measure runs (same stream: after
-    // the assembly, before the measure's own copies).
     if (!d2h(h_pos, in.pos, nv * 12) || !d2h(h_nrm, in.nrm, nv * 12) || !d2h(h_atom, in.atoms, nv * 4) ||
         !d2h(h_patch, in.patches, nv)) {
         if (msg) *msg = "vertex copy";

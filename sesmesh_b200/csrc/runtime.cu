@@ -309,6 +309,7 @@ static void destroy_device(smb_device* d) {
     if (d->gone.exchange(true)) return;
     cudaSetDevice(d->index);
     if (d->stream) cudaStreamDestroy(d->stream);
+    if (d->copy) cudaStreamDestroy(d->copy);
     mem_device_close(d->index);
     delete d;
 }
@@ -350,7 +351,9 @@ int smb_open(int index, smb_device** out, char* err, size_t errlen) {
     d->info.memory = prop.totalGlobalMem;
     d->smem_optin = prop.sharedMemPerBlockOptin;
     e = cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d->copy, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
+        if (d->stream) cudaStreamDestroy(d->stream);
         delete d;
         set_err(err, errlen, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
         return SMB_ERR_CUDA;

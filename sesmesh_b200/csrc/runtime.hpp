@@ -57,6 +57,7 @@ size_t mlp_smem_bytes();
 struct smb_device {
     int index = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy = nullptr;  // device-to-host copies that overlap the main stream's kernels
     smb_device_info info{};
     size_t smem_optin = 0;
     std::atomic<int> refs{0};
