@@ -52,13 +52,15 @@ def args_():
                    choices=["rings58800", "globule330", "globule2800", "shell2400k", "batch512"])
     p.add_argument("--refine", default=None, choices=[None, "exact", "fast"])
     p.add_argument("--spacing", type=float, default=None, help="override the workload's grid spacing")
+    p.add_argument("--spheres", type=int, default=None,
+                   help="keep the workload's first N spheres (smaller cases of the same kind, for ncu captures)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-fast", action="store_true", help="skip the fast-mode (plain vs warm start) leg")
     return p.parse_args()
 
 
-def workload(name, refine=None, spacing=None):
+def workload(name, refine=None, spacing=None, spheres=None):
     from sesmesh_b200 import workloads
     w = {"rings58800": workloads.rings58800, "globule330": workloads.globule330,
          "globule2800": workloads.globule2800, "shell2400k": workloads.shell2400k}[name]()
@@ -66,6 +68,9 @@ def workload(name, refine=None, spacing=None):
         w["refine"] = refine
     if spacing:
         w["spacing"] = spacing
+    if spheres and spheres < len(w["spheres"]):
+        w["spheres"] = w["spheres"][:spheres]
+        w["name"] = "%s[:%d]" % (w["name"], spheres)
     return w
 
 
@@ -187,7 +192,7 @@ def run_reference(a):
         return
     if a.workload == "batch512":
         return run_reference_batch(a)
-    w = workload(a.workload, a.refine, a.spacing)
+    w = workload(a.workload, a.refine, a.spacing, a.spheres)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     eng, sample, spb, k, nb = cpu_leg(w, budget_s=6.0)
@@ -241,7 +246,7 @@ def run_ours(a):
 
     from sesmesh_b200 import native
     from sesmesh_b200 import surface as S
-    w = workload(a.workload, a.refine, a.spacing)
+    w = workload(a.workload, a.refine, a.spacing, a.spheres)
     params = S.SurfaceParams.ses(w["probe"]).with_spacing(w["spacing"]).with_brick_size(w["brick"]).with_refine(
         w["refine"])
     params = S.SurfaceParams(**{**params.__dict__, "device": local})

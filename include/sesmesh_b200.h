@@ -235,7 +235,7 @@ int smb_batch_set_refine_group(smb_batch* batch, int lanes);
  * at least 8.  The vertices do not depend on it. */
 int smb_batch_set_exact_group(smb_batch* batch, int lanes);
 /* Shared memory of each sampling CTA in a first pass over the sub-blocks
- * whose packed lists fit it (>= 1 KiB; 0, the default: 56 KiB); the others
+ * whose packed lists fit it (>= 1 KiB; 0, the default: 55 KiB); the others
  * run in a second pass with room for the largest. */
 int smb_batch_set_sample_region(smb_batch* batch, size_t bytes);
 

@@ -1475,6 +1475,11 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
 // WIDE: candidates too large for a region per warp; the CTA refines one
 // item at a time with all its threads.
 constexpr int REFINE_WARPS = 4;
+// Warps of a block in the plain pass over the listed sub-blocks (those over
+// a warp's region): the block's warps take one sub-block's edges.
+#ifndef WIDE_LIST_WARPS
+#define WIDE_LIST_WARPS 16
+#endif
 // Most quads a CTA claims at once: phase A for all of them, then phase B
 // with the warps claiming the batch's items one by one (a barrier per batch,
 // not per quad, so warps with quick items do not wait for slow ones).  Small
@@ -1488,8 +1493,8 @@ struct RefinePlan {
     uint32_t first_off;   // phase A: first S candidates, REFINE_WARPS x REFINE_BATCH x FEATURE_SCAN float4
 };
 
-template <int MODE, bool WIDE, bool MANY, int RG>
-__global__ void __launch_bounds__(32 * REFINE_WARPS) k_refine(
+template <int MODE, bool WIDE, bool MANY, int RG, int NT = 32 * REFINE_WARPS>
+__global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
     DArr A0, DLat L0, RefineConsts RC0, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
     const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
     uint32_t n_host, RefOut out, const float* values, MlpDev mlp, float* feat_out, RefinePlan P,
@@ -1881,13 +1886,13 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
     // resident (the plain kernel of that width sets the occupancy; the TMEM
     // columns cap the MLP kernel).
     auto run = [&](auto kern, auto occ, const RefinePlan& PL, size_t bytes, uint32_t* o, const uint32_t* list,
-                   uint32_t units) -> cudaError_t {
+                   uint32_t units, int threads = 32 * REFINE_WARPS) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(occ, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (e != cudaSuccess) return e;
         int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, occ, 32 * REFINE_WARPS, bytes);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, occ, threads, bytes);
         if (e != cudaSuccess) return e;
         if (mode == REFINE_MLP) per_sm = std::min(per_sm, 8);  // 64 TMEM columns per CTA of the SM's 512
         const uint32_t grid = std::min<uint32_t>(units, uint32_t(std::max(1, sms * std::max(per_sm, 1))));
@@ -1895,7 +1900,7 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
         Q.batch = std::max<uint32_t>(1, std::min<uint32_t>(REFINE_BATCH, units / (4 * grid)));
         cudaMemsetAsync(&counters[CNT_QUEUE], 0, sizeof(unsigned long long), s);
         COUNT(1);
-        kern<<<grid, 32 * REFINE_WARPS, bytes, s>>>(A, L, RC, keys, work, rec, ids, edges, edge_vals, item_off,
+        kern<<<grid, threads, bytes, s>>>(A, L, RC, keys, work, rec, ids, edges, edge_vals, item_off,
                                                      item_edges, n_items, RefOut{t, feat, q, evals}, values, md,
                                                      feat_out, Q, counters, many ? *many : Scene{}, o, list);
         return cudaGetLastError();
@@ -1908,10 +1913,12 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
         cudaError_t e = cudaMemsetAsync(ovf, 0, 4, s);
         if (e != cudaSuccess) return e;
         auto kn = g32 ? k_refine<REFINE_PLAIN, false, false, 32> : k_refine<REFINE_PLAIN, false, false, 8>;
-        auto kw = g32 ? k_refine<REFINE_PLAIN, true, false, 32> : k_refine<REFINE_PLAIN, true, false, 8>;
+        // The list pass: WIDE_LIST_WARPS warps share each sub-block's lists.
+        auto kw = g32 ? k_refine<REFINE_PLAIN, true, false, 32, 32 * WIDE_LIST_WARPS>
+                      : k_refine<REFINE_PLAIN, true, false, 8, 32 * WIDE_LIST_WARPS>;
         e = run(kn, kn, PS, size_t(REFINE_WARPS) * small, ovf, nullptr, quads);
         if (e != cudaSuccess) return e;
-        return run(kw, kw, P, wide, nullptr, ovf, n_items);
+        return run(kw, kw, P, wide, nullptr, ovf, n_items, 32 * WIDE_LIST_WARPS);
     }
     // Groups of lanes per edge: one lane in the many-structure pass (short
     // lists, few evaluations after the warm start), else 8 or 32 as asked.

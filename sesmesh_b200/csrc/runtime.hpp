@@ -94,8 +94,9 @@ struct smb_resident {
 };
 
 // Shared memory of the sampling's first-pass CTAs (sub-blocks whose packed
-// lists are larger wait for a second pass with room for the largest).
-constexpr size_t SAMPLE_REGION = 56 * 1024;
+// lists are larger wait for a second pass with room for the largest): four
+// CTAs fit an SM's 228 KiB with their 1 KiB reserve and static bytes.
+constexpr size_t SAMPLE_REGION = 55 * 1024;
 
 struct smb_batch {
     smb_resident* res = nullptr;
