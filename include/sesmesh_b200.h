@@ -246,6 +246,8 @@ typedef struct {
     unsigned long long pack_units;
     double classify_ms;
     size_t exact_block_items;  /* smb_refine_exact: sub-blocks refined by a whole block (lists over a warp's share) */
+    uint32_t gather_caps[4];   /* the gather's per-warp list caps (near, S, C, V) for the next run */
+    uint32_t gather_warps;     /* warps per gather block for the next run */
 } smb_batch_info;
 int smb_batch_info_get(const smb_batch* batch, smb_batch_info* out);
 /* Re-runs the sampling pass of the last run counting its f32 arithmetic

@@ -104,17 +104,53 @@ __device__ __forceinline__ double warp_min(double v) {
     return v;
 }
 
-// Lanes stride over the items of each row of the box: every item of the box
-// is visited once, by some lane.
+// The items of a box's rows as one sequence in the rows' order (z, then y,
+// then the row's cells from x0 to x1), visited by a warp in chunks of 32
+// consecutive items: f(valid, item) on every lane, lane l holding the
+// chunk's l-th item (valid false past the end).  The row bounds of 32 rows
+// are loaded at once and the rows' items flattened by a prefix sum, so a
+// box costs a dependent load round per 32 rows and one per 32 items rather
+// than one per row.
+template <class F>
+__device__ __forceinline__ void warp_box_items(const DGrid& g, const CellBox& bx, int lane, F&& f) {
+    const uint32_t ny = bx.y1 - bx.y0 + 1, nrows = ny * (bx.z1 - bx.z0 + 1);
+    for (uint32_t r0 = 0; r0 < nrows; r0 += 32) {
+        const uint32_t rr = r0 + uint32_t(lane);
+        uint32_t a = 0, cnt = 0;
+        if (rr < nrows) {
+            const size_t row = (size_t(bx.z0 + rr / ny) * g.dy + (bx.y0 + rr % ny)) * g.dx;
+            a = g.starts[row + bx.x0];
+            cnt = g.starts[row + bx.x1 + 1] - a;
+        }
+        uint32_t inc = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31), excl = inc - cnt;
+        for (uint32_t b = 0; b < total; b += 32) {
+            const uint32_t t = b + uint32_t(lane);
+            // The row holding item t: the last lane q with excl_q <= t
+            // (excl ascends; such a row is not empty while t < total).
+            int q = 0;
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+                const uint32_t e = __shfl_sync(0xffffffffu, excl, q + step);
+                if (e <= t) q += step;
+            }
+            const uint32_t aq = __shfl_sync(0xffffffffu, a, q), eq = __shfl_sync(0xffffffffu, excl, q);
+            const bool valid = t < total;
+            f(valid, valid ? g.items[aq + (t - eq)] : 0u);
+        }
+    }
+}
+
+// Every item of the box visited once, by some lane of the warp.
 template <class F>
 __device__ __forceinline__ void warp_for_near(const DGrid& g, double x, double y, double z, double r, int lane, F&& f) {
-    CellBox bx = cell_box(g, x, y, z, r);
-    for (uint32_t zc = bx.z0; zc <= bx.z1; zc++)
-        for (uint32_t yc = bx.y0; yc <= bx.y1; yc++) {
-            size_t row = (size_t(zc) * g.dy + yc) * g.dx;
-            uint32_t a = g.starts[row + bx.x0], e = g.starts[row + bx.x1 + 1];
-            for (uint32_t i = a + lane; i < e; i += 32) f(g.items[i]);
-        }
+    warp_box_items(g, cell_box(g, x, y, z, r), lane, [&](bool valid, uint32_t k) {
+        if (valid) f(k);
+    });
 }
 
 // SesField::try_sphere_with (field/point.rs:422-444): the candidate's

@@ -109,6 +109,12 @@ template <class F>
 __device__ __forceinline__ void x_for_near(const DGrid& g, double x, double y, double z, double r, uint32_t tid,
                                            uint32_t T, F&& f) {
     CellBox bx = cell_box(g, x, y, z, r);
+    if (T == 32) {  // a warp: the rows flattened (warp_box_items)
+        warp_box_items(g, bx, int(tid), [&](bool valid, uint32_t k) {
+            if (valid) f(k);
+        });
+        return;
+    }
     for (uint32_t zc = bx.z0; zc <= bx.z1; zc++)
         for (uint32_t yc = bx.y0; yc <= bx.y1; yc++) {
             size_t row = (size_t(zc) * g.dy + yc) * g.dx;

@@ -270,27 +270,21 @@ __device__ __forceinline__ int warp_append(bool p, int& count) {
 // sees the items in scan order.
 template <class F>
 __device__ __forceinline__ void warp_scan_box(const DGrid& g, double x, double y, double z, double r, int lane, F&& f) {
-    CellBox bx = cell_box(g, x, y, z, r);
-    for (uint32_t zc = bx.z0; zc <= bx.z1; zc++)
-        for (uint32_t yc = bx.y0; yc <= bx.y1; yc++) {
-            size_t row = (size_t(zc) * g.dy + yc) * g.dx;
-            uint32_t a = g.starts[row + bx.x0], e = g.starts[row + bx.x1 + 1];
-            for (uint32_t b = a; b < e; b += 32) {
-                uint32_t i = b + lane;
-                bool valid = i < e;
-                f(valid, valid ? g.items[i] : 0u);
-            }
-        }
+    warp_box_items(g, cell_box(g, x, y, z, r), lane, f);
 }
 
-__device__ __forceinline__ int lookup_local(const uint32_t* sorted_ids, const uint32_t* sorted_loc, int n, uint32_t id) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (sorted_ids[mid] < id) lo = mid + 1;
-        else hi = mid;
+// Open-addressing table of a sub-block's near spheres: 2^bits 16-bit slots
+// holding near-list positions (0xFFFF empty), at most half of them used, so
+// a lookup ends at the sphere's slot or at an empty one.
+__device__ __forceinline__ uint32_t near_hash(uint32_t id, uint32_t bits) { return (id * 0x9E3779B1u) >> (32 - bits); }
+
+__device__ __forceinline__ int lookup_near(const uint16_t* tab, uint32_t bits, const uint32_t* near_ids, uint32_t id) {
+    const uint32_t mask = (1u << bits) - 1;
+    for (uint32_t h = near_hash(id, bits);; h = (h + 1) & mask) {
+        const uint32_t l = tab[h];
+        if (l == 0xFFFFu) return -1;
+        if (near_ids[l] == id) return int(l);
     }
-    return (lo < n && sorted_ids[lo] == id) ? int(sorted_loc[lo]) : -1;
 }
 
 __device__ __forceinline__ unsigned warp_inclusive_scan(unsigned v) {
@@ -313,9 +307,11 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
     double* s_key = reinterpret_cast<double*>(base);
     double* c_key = s_key + caps.s;
     uint32_t* near_ids = reinterpret_cast<uint32_t*>(c_key + caps.c);
-    uint32_t* sorted_ids = near_ids + caps.near;
-    uint32_t* sorted_loc = sorted_ids + caps.near;
-    uint32_t* s_id = sorted_loc + caps.near;
+    // The near table takes the 2 caps.near words after the near ids: 2^bits
+    // >= 2 caps.near 16-bit slots.
+    uint16_t* near_tab = reinterpret_cast<uint16_t*>(near_ids + caps.near);
+    const uint32_t tab_bits = 31u - uint32_t(__clz(4 * caps.near));
+    uint32_t* s_id = near_ids + 3 * caps.near;
     uint32_t* s_loc = s_id + caps.s;
     uint32_t* s_perm = s_loc + caps.s;
     uint32_t* s_off = s_perm + caps.s;
@@ -370,14 +366,16 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
     if (lane == 0) atomicMax(&O.counters[CNT_MAXNN], (unsigned long long)nn);
     if (nn > caps.near) return overflow(REC_OVERFLOW);
     __syncwarp();
-    // Sorted copy of the near ids for blocker lookups.
+    // The near table for blocker lookups (positions in the near list).
+    for (uint32_t i = lane; i < (1u << tab_bits); i += 32) near_tab[i] = 0xFFFFu;
+    __syncwarp();
     for (int i = lane; i < nn; i += 32) {
-        uint32_t id = near_ids[i];
-        int rank = 0;
-        for (int q = 0; q < nn; q++) rank += near_ids[q] < id;
-        sorted_ids[rank] = id;
-        sorted_loc[rank] = uint32_t(i);
+        const uint32_t mask = (1u << tab_bits) - 1;
+        uint32_t h = near_hash(near_ids[i], tab_bits);
+        while (atomicCAS(&near_tab[h], (unsigned short)0xFFFFu, (unsigned short)i) != (unsigned short)0xFFFFu)
+            h = (h + 1) & mask;  // ends: at most half of the slots are taken
     }
+    __syncwarp();
     // Class S candidates among the near spheres.
     int ns = 0;
     for (int b0 = 0; b0 < nn; b0 += 32) {
@@ -447,7 +445,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         if (r < ns) {
             uint32_t k = s_id[s_perm[r]];
             for (uint32_t p = A.nb_off[k], e = A.nb_off[k + 1]; p < e; p++)
-                cnt += lookup_local(sorted_ids, sorted_loc, nn, A.nb_items[p]) >= 0;
+                cnt += lookup_near(near_tab, tab_bits, near_ids, A.nb_items[p]) >= 0;
         }
         unsigned inc = warp_inclusive_scan(cnt);
         if (r < ns) s_off[r + 1] = run + inc;
@@ -462,7 +460,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         if (r < nc) {
             uint32_t ci = c_id[c_perm[r]];
             for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++)
-                cnt += lookup_local(sorted_ids, sorted_loc, nn, A.cb_items[p]) >= 0;
+                cnt += lookup_near(near_tab, tab_bits, near_ids, A.cb_items[p]) >= 0;
         }
         unsigned inc = warp_inclusive_scan(cnt);
         if (r < nc) c_off[r + 1] = run + inc;
@@ -540,7 +538,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         p_s[r] = make_float4(float(c.x - L.fx), float(c.y - L.fy), float(c.z - L.fz), float(c.w));
         uint32_t o = s_off[r];
         for (uint32_t p = A.nb_off[k], e = A.nb_off[k + 1]; p < e; p++) {
-            int l = lookup_local(sorted_ids, sorted_loc, nn, A.nb_items[p]);
+            int l = lookup_near(near_tab, tab_bits, near_ids, A.nb_items[p]);
             if (l >= 0) w_sblk[o] = uint32_t(l), p_sblk[o] = uint32_t(l), o++;
         }
     }
@@ -554,7 +552,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         p_c[3 * r + 2] = make_float4(float(c[7]), float(c[8]), 0.0f, 0.0f);
         uint32_t o = c_off[r];
         for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++) {
-            int l = lookup_local(sorted_ids, sorted_loc, nn, A.cb_items[p]);
+            int l = lookup_near(near_tab, tab_bits, near_ids, A.cb_items[p]);
             if (l >= 0) w_cblk[o] = uint32_t(l), p_cblk[o] = uint32_t(l), o++;
         }
     }

@@ -822,6 +822,12 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
         auto up = [](unsigned long long v) { return std::max(32, int((v + v / 8 + 16 + 15) / 16 * 16)); };
         GatherCaps next{up(cnt[CNT_MAXNN]), up(cnt[CNT_MAXNS]), up(cnt[CNT_MAXNC]), up(cnt[CNT_MAXNV])};
         size_t per = gather_smem_bytes(next);
+        if (GATHER_WARP_BUDGET && per > GATHER_WARP_BUDGET) {
+            const double f = double(GATHER_WARP_BUDGET) / double(per);
+            auto dn = [f](int v) { return std::max(32, int(double(v) * f) / 16 * 16); };
+            next = GatherCaps{dn(next.near), dn(next.s), dn(next.c), dn(next.v)};
+            per = gather_smem_bytes(next);
+        }
         if (per <= size_t(d->smem_optin)) {
             b->caps = next;
             b->gather_warps = int(std::max<size_t>(1, std::min<size_t>(8, size_t(65536) / per)));
@@ -1307,6 +1313,9 @@ int smb_batch_info_get(const smb_batch* b, smb_batch_info* out) {
     }
     out->pack_units = c[CNT_PACK];
     out->exact_block_items = b->x_block_items;
+    out->gather_caps[0] = uint32_t(b->caps.near), out->gather_caps[1] = uint32_t(b->caps.s);
+    out->gather_caps[2] = uint32_t(b->caps.c), out->gather_caps[3] = uint32_t(b->caps.v);
+    out->gather_warps = uint32_t(b->gather_warps);
     return SMB_OK;
 }
 

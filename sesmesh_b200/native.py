@@ -100,7 +100,8 @@ class MultiTimes(C.Structure):
 class BatchInfo(C.Structure):
     _fields_ = [(f, C.c_size_t) for f in ("bricks", "sampled_subblocks", "ids_words", "max_pack_units", "edges",
                                           "triangles", "touched", "resident_bytes")] + \
-               [("pack_units", C.c_ulonglong), ("classify_ms", C.c_double), ("exact_block_items", C.c_size_t)]
+               [("pack_units", C.c_ulonglong), ("classify_ms", C.c_double), ("exact_block_items", C.c_size_t),
+                ("gather_caps", C.c_uint32 * 4), ("gather_warps", C.c_uint32)]
 
 
 # Every entry point of include/*.h with its ctypes signature.
