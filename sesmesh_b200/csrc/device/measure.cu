@@ -425,6 +425,13 @@ void MeasureScratch::release(bool synced) {
     pinned_free(host);
     host = nullptr;
     host_cap = 0;
+    pinned_free(words);
+    words = nullptr;
+}
+
+// The first n counters into page-locked host words, by the device itself.
+__global__ void k_read_words(const unsigned long long* src, unsigned long long* dst, int n) {
+    if (int(threadIdx.x) < n) dst[threadIdx.x] = src[threadIdx.x];
 }
 
 // The measure of a mesh already on the device (pos, nrm: 3 f32 per vertex,
@@ -453,14 +460,26 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
     }
     unsigned long long* cnt = S.counters.as<unsigned long long>();  // 0 bad, 1 oob, 2 parts, 3 overflow, 4 comps, 5 union-find
     MCK(cudaMemsetAsync(cnt, 0, 64, s));
+    if (!S.words && !(S.words = static_cast<unsigned long long*>(pinned_alloc(64)))) {
+        if (msg) *msg = "page-locked counter words";
+        return false;
+    }
+    // Counters 0..7 to the host once the main stream gets here (a kernel
+    // writes them: a copy would wait behind the vertex copies).
+    volatile unsigned long long* W = S.words;
+    auto pull = [&]() -> bool {
+        k_read_words<<<1, 32, 0, s>>>(cnt, S.words, 8);
+        return cudaStreamSynchronize(s) == cudaSuccess;
+    };
     auto blocks = [](uint64_t n) { return unsigned((n + 255) / 256); };
     if (nv) k_vertex_checks<<<blocks(nv), 256, 0, s>>>(pos, nrm, uint32_t(nv), cnt);
     if (nt) k_index_checks<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), uint32_t(nv), cnt + 1);
-    unsigned long long c2[2];
-    MCK(cudaMemcpyAsync(c2, cnt, 16, cudaMemcpyDeviceToHost, s));
-    MCK(cudaStreamSynchronize(s));
-    if (c2[1]) {  // indices out of range: the host counts one defect more and stops there
-        *bad = size_t(c2[0] + 1);
+    if (!pull()) {
+        if (msg) *msg = "measure checks";
+        return false;
+    }
+    if (W[1]) {  // indices out of range: the host counts one defect more and stops there
+        *bad = size_t(W[0] + 1);
         return true;
     }
     if (nt) {
@@ -474,9 +493,11 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
                                                   cnt);
         k_duplicates<<<blocks(nt), 256, 0, s>>>(tris, uint32_t(nt), S.dup.as<uint32_t>(), dcap - 1, cnt);
     }
-    unsigned long long nbad = 0;
-    MCK(cudaMemcpyAsync(&nbad, cnt, 8, cudaMemcpyDeviceToHost, s));
-    MCK(cudaStreamSynchronize(s));
+    if (!pull()) {
+        if (msg) *msg = "measure checks";
+        return false;
+    }
+    const unsigned long long nbad = W[0];
     *bad = size_t(nbad);
     if (nbad) return true;
     // Components.
@@ -488,10 +509,11 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         launch_scan(S.flag.as<uint32_t>(), uint32_t(nv), S.cid.as<uint32_t>(), nullptr,
                     S.tiles.as<unsigned long long>(), cnt + 4, s);
     }
-    unsigned long long n_comp = 0, uf_fail = 0;
-    MCK(cudaMemcpyAsync(&n_comp, cnt + 4, 8, cudaMemcpyDeviceToHost, s));
-    MCK(cudaMemcpyAsync(&uf_fail, cnt + 5, 8, cudaMemcpyDeviceToHost, s));
-    MCK(cudaStreamSynchronize(s));
+    if (!pull()) {
+        if (msg) *msg = "measure components";
+        return false;
+    }
+    const unsigned long long n_comp = W[4], uf_fail = W[5];
     if (uf_fail) {
         if (msg) *msg = "union-find gave up";
         return false;
@@ -507,6 +529,31 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
     uint32_t* id = S.id.as<uint32_t>();
     if (nv) k_component_ids<<<blocks(nv), 256, 0, s>>>(parent, S.cid.as<uint32_t>(), uint32_t(nv), id,
                                                        S.comp_v.as<unsigned long long>());
+    // Arrays that are final go back on the copy stream while the main one
+    // computes the rest; the end of this function waits for both.
+    cudaStream_t cs = d->copy ? d->copy : s;
+    auto to_host = [&](void* dst, const void* src, size_t bytes) -> bool {
+        if (!bytes) return true;
+        if (cs != s) {
+            cudaEvent_t ready;
+            if (cudaEventCreateWithFlags(&ready, cudaEventDisableTiming) != cudaSuccess) return false;
+            const bool ok =
+                cudaEventRecord(ready, s) == cudaSuccess && cudaStreamWaitEvent(cs, ready, 0) == cudaSuccess;
+            cudaEventDestroy(ready);
+            if (!ok) return false;
+        }
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, cs) == cudaSuccess;
+    };
+    struct Join {
+        cudaStream_t c;
+        ~Join() {
+            if (c) cudaStreamSynchronize(c);
+        }
+    } join{cs != s ? cs : nullptr};
+    if (nv && !to_host(host_comp, id, nv * 4)) {
+        if (msg) *msg = "component copy";
+        return false;
+    }
     if (nt)
         k_euler_edges<<<blocks(ecap), 256, 0, s>>>(S.keys.as<unsigned long long>(), ecap, id,
                                                    S.comp_e.as<unsigned long long>());
@@ -529,6 +576,13 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
             if (msg) *msg = "triangle sort failed";
             return false;
         }
+        // Triangles regrouped by component, relative order kept.
+        k_gather_triangles<<<blocks(nt), 256, 0, s>>>(tris, S.tidx2.as<uint32_t>(), uint32_t(nt),
+                                                      S.tris_out.as<uint32_t>());
+        if (!to_host(host_tris, S.tris_out.p, nt * 12)) {
+            if (msg) *msg = "triangle copy";
+            return false;
+        }
     }
     // Area and volume: one partial per (component, 16,384-triangle chunk)
     // summed in triangle order, then each component's partials in chunk
@@ -540,8 +594,11 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         uint32_t* start = S.tidx.as<uint32_t>();  // idem
         k_segment_flags<<<blocks(nt), 256, 0, s>>>(S.tkey2.as<uint32_t>(), S.tidx2.as<uint32_t>(), uint32_t(nt), flag);
         launch_scan(flag, uint32_t(nt), nullptr, start, S.tiles.as<unsigned long long>(), cnt + 2, s);
-        MCK(cudaMemcpyAsync(&n_seg, cnt + 2, 8, cudaMemcpyDeviceToHost, s));
-        MCK(cudaStreamSynchronize(s));
+        if (!pull()) {
+            if (msg) *msg = "measure segments";
+            return false;
+        }
+        n_seg = W[2];
     }
     const uint32_t np = uint32_t(n_seg);
     if (np) {
@@ -566,10 +623,6 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         MCK(cudaMemsetAsync(S.area.p, 0, size_t(nc) * 8, s));
         MCK(cudaMemsetAsync(S.volume.p, 0, size_t(nc) * 8, s));
     }
-    // Triangles regrouped by component, relative order kept.
-    if (nt)
-        k_gather_triangles<<<blocks(nt), 256, 0, s>>>(tris, S.tidx2.as<uint32_t>(), uint32_t(nt),
-                                                      S.tris_out.as<uint32_t>());
     // Results to the host.
     std::vector<unsigned long long> cv(nc), ct(nc), ce(nc);
     std::vector<double> ca(nc), cvol(nc);
@@ -580,8 +633,6 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         MCK(cudaMemcpyAsync(ca.data(), S.area.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
         MCK(cudaMemcpyAsync(cvol.data(), S.volume.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
     }
-    if (nv) MCK(cudaMemcpyAsync(host_comp, id, nv * 4, cudaMemcpyDeviceToHost, s));
-    if (nt) MCK(cudaMemcpyAsync(host_tris, S.tris_out.p, nt * 12, cudaMemcpyDeviceToHost, s));
     MCK(cudaStreamSynchronize(s));
     comps.assign(nc, Component());
     size_t start = 0;

@@ -16,6 +16,9 @@ struct MeasureScratch {
         tri_v;
     void* host = nullptr;  // page-locked staging of the results
     size_t host_cap = 0;
+    // Page-locked words the device writes counters into directly: reading
+    // them does not queue behind large copies on the device's copy engines.
+    unsigned long long* words = nullptr;
     void* staging(size_t bytes);  // null when page-locked memory cannot be had
     void release(bool synced = false);  // synced: the device has finished every use of them
     ~MeasureScratch() { release(); }
