@@ -288,15 +288,20 @@ __device__ __forceinline__ double wrap_tau(double a) {  // f64::rem_euclid(TAU)
     return r < 0.0 ? r + S_TWO_PI : r;
 }
 
+// A circle's blocked spans: start and end parameters and the blocking
+// sphere (its cut points are recomputed where needed, which keeps each
+// thread's local memory small).
 struct Spans {
-    double start[MAX_SPANS], end[MAX_SPANS], en[MAX_SPANS][2], lv[MAX_SPANS][2];
+    double start[MAX_SPANS], end[MAX_SPANS];
     uint32_t sphere[MAX_SPANS];
     uint8_t ord[MAX_SPANS];
     int n;
 };
 
 // any_exposed (arrangement.rs:340-405): 1 exposed, 0 buried, -1 declined.
-__device__ int any_exposed(Spans& S) {
+// Runs keep the span that opened them (its start and entry point) and the
+// span that gave their end (its exit point).
+__device__ int any_exposed(Spans& S, const Circle& C, const double4* sph) {
     if (S.n == 0) return 1;
     for (int a = 0; a < S.n; a++) S.ord[a] = uint8_t(a);
     auto less = [&](int a, int b) {
@@ -313,33 +318,38 @@ __device__ int any_exposed(Spans& S) {
         S.ord[b] = v;
     }
     // Runs, in place of nothing: at most n of them.
-    double rs[MAX_SPANS], re[MAX_SPANS], ren[MAX_SPANS][2], rlv[MAX_SPANS][2];
+    double re[MAX_SPANS];
+    uint8_t first[MAX_SPANS], last[MAX_SPANS];
     int m = 0;
     for (int a = 0; a < S.n; a++) {
         const int s = S.ord[a];
         if (m > 0 && S.start[s] <= re[m - 1]) {
-            if (S.end[s] > re[m - 1]) re[m - 1] = S.end[s], rlv[m - 1][0] = S.lv[s][0], rlv[m - 1][1] = S.lv[s][1];
+            if (S.end[s] > re[m - 1]) re[m - 1] = S.end[s], last[m - 1] = uint8_t(s);
         } else {
-            rs[m] = S.start[s], re[m] = S.end[s];
-            ren[m][0] = S.en[s][0], ren[m][1] = S.en[s][1], rlv[m][0] = S.lv[s][0], rlv[m][1] = S.lv[s][1];
+            re[m] = S.end[s], first[m] = uint8_t(s), last[m] = uint8_t(s);
             m++;
         }
     }
     int b0 = 0;  // runs[b0 .. m)
     while (m - b0 > 1) {
-        const double fs = rs[b0], fe = re[b0], flv0 = rlv[b0][0], flv1 = rlv[b0][1];
+        const double fs = S.start[first[b0]], fe = re[b0];
         const int l = m - 1;
         if (re[l] - S_PERIOD < fs) break;
-        if (fe + S_PERIOD > re[l]) re[l] = fe + S_PERIOD, rlv[l][0] = flv0, rlv[l][1] = flv1;
+        if (fe + S_PERIOD > re[l]) re[l] = fe + S_PERIOD, last[l] = last[b0];
         b0++;
     }
     const int cnt = m - b0;
     for (int k = 0; k < cnt; k++) {
         const int cur = b0 + k, nxt = b0 + (k + 1) % cnt;
-        const double next_start = k + 1 < cnt ? rs[nxt] : rs[nxt] + S_PERIOD;
+        const double ns = S.start[first[nxt]];
+        const double next_start = k + 1 < cnt ? ns : ns + S_PERIOD;
         if (next_start - re[cur] > S_PSEUDO_EPS) {
-            const double a0 = wrap_tau(atan2(rlv[cur][1], rlv[cur][0]));
-            const double a1 = atan2(ren[nxt][1], ren[nxt][0]);
+            double en[2], lv[2], en2[2], lv2[2];
+            const double4 sc = sph[S.sphere[last[cur]]], sn = sph[S.sphere[first[nxt]]];
+            cut(C, xyz(sc), sc.w, en, lv);
+            cut(C, xyz(sn), sn.w, en2, lv2);
+            const double a0 = wrap_tau(atan2(lv[1], lv[0]));
+            const double a1 = atan2(en2[1], en2[0]);
             const double w = wrap_tau(a1 - a0);
             if (w < S_ANG_EPS + S_ANG_MARGIN || w > S_TWO_PI - S_ANG_MARGIN) return -1;
             if (w > S_ANG_EPS) return 1;
@@ -409,9 +419,8 @@ __global__ void __launch_bounds__(128) k_circles(const double4* sph, size_t n, c
         S.end[a] = diamond(lv[0], lv[1]);
         if (S.end[a] <= S.start[a]) S.end[a] += S_PERIOD;
         S.sphere[a] = k;
-        S.en[a][0] = en[0], S.en[a][1] = en[1], S.lv[a][0] = lv[0], S.lv[a][1] = lv[1];
     }
-    const int ex = any_exposed(S);
+    const int ex = any_exposed(S, C, sph);
     if (ex < 0) {
         atomicOr(decline, DECLINE_ANGLE);
         return zero();
