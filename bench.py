@@ -13,7 +13,8 @@ Workload (N=1): rings58800 -- 58,800 spheres (21 copies of a seeded
 * e2e -- the same metric through the public API (compute_surface from host
   sphere arrays): host arrangement, upload, device stage, copies back, host
   f64 refinement, assembly, validation, components; wall clock.
-* roofline -- the dominant kernel against its bound.
+* roofline -- the dominant kernel against its bound: counted operations of
+  its evaluations per launch over the launch's CUDA-event time.
 * cpu_baseline -- the CPU oracle (C++ restatement of sesmesh's CPU back end)
   meshing a sample of the same bricks on all host cores.
 
@@ -495,7 +496,8 @@ def run_batch(a):
 
 
 def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops=0):
-    """Roofline of the dominant kernel (per-unit counts in DESIGN.md)."""
+    """Roofline of the dominant kernel: its counted operations (or bytes) per
+    launch over the launch's device time, against the matching peak."""
     ms = stage[dominant]
     hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
     spb = (w["brick"] + 1) ** 3

@@ -338,7 +338,7 @@ int smb_open(int index, smb_device** out, char* err, size_t errlen) {
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, index));
     if (prop.major < 10) {
-        set_err(err, errlen, "device %d (%s) is sm_%d%d; this build targets sm_100a", index, prop.name, prop.major,
+        set_err(err, errlen, "device %d (%s) is sm_%d%d; the library is built for sm_100a", index, prop.name, prop.major,
                 prop.minor);
         return SMB_ERR_NODEVICE;
     }
@@ -822,12 +822,6 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
         auto up = [](unsigned long long v) { return std::max(32, int((v + v / 8 + 16 + 15) / 16 * 16)); };
         GatherCaps next{up(cnt[CNT_MAXNN]), up(cnt[CNT_MAXNS]), up(cnt[CNT_MAXNC]), up(cnt[CNT_MAXNV])};
         size_t per = gather_smem_bytes(next);
-        if (GATHER_WARP_BUDGET && per > GATHER_WARP_BUDGET) {
-            const double f = double(GATHER_WARP_BUDGET) / double(per);
-            auto dn = [f](int v) { return std::max(32, int(double(v) * f) / 16 * 16); };
-            next = GatherCaps{dn(next.near), dn(next.s), dn(next.c), dn(next.v)};
-            per = gather_smem_bytes(next);
-        }
         if (per <= size_t(d->smem_optin)) {
             b->caps = next;
             b->gather_warps = int(std::max<size_t>(1, std::min<size_t>(8, size_t(65536) / per)));

@@ -93,13 +93,6 @@ struct smb_resident {
     std::atomic<bool> freed{false}, gone{false};
 };
 
-// Most shared memory a gather warp's list scratch takes in the first pass of
-// a run (0: the largest lists of the last run); sub-blocks over it go to the
-// retry passes with larger caps.
-#ifndef GATHER_WARP_BUDGET
-#define GATHER_WARP_BUDGET 0
-#endif
-
 // Shared memory of the sampling's first-pass CTAs (sub-blocks whose packed
 // lists are larger wait for a second pass with room for the largest): four
 // CTAs fit an SM's 228 KiB with their 1 KiB reserve and static bytes.
