@@ -1499,7 +1499,7 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
     unsigned long long* counters, Scene S, uint32_t* ovf, const uint32_t* list) {
     const uint32_t n_items = MANY ? uint32_t(*S.n_work) : n_host;
     extern __shared__ __align__(128) float4 rs[];
-    __shared__ uint32_t sh_q, sh_next;
+    __shared__ uint32_t sh_q, sh_next, sh_edge;
     __shared__ uint32_t sh_off[REFINE_WARPS * REFINE_BATCH + 1], sh_sbase[REFINE_WARPS * REFINE_BATCH],
         sh_brick[REFINE_WARPS * REFINE_BATCH];
     __shared__ int sh_ns[REFINE_WARPS * REFINE_BATCH];
@@ -1542,8 +1542,12 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
                 return;
             }
         }
-        if (WIDE) __syncthreads();
-        else __syncwarp();
+        if (WIDE) {
+            __syncthreads();
+            if (threadIdx.x == 0) sh_edge = a0;  // read after the staging's barrier
+        } else {
+            __syncwarp();
+        }
         const int sb = int(j & 7), sub = L.sub;
         const float h32 = float(L.h), half = 0.5f * float(sub);
         const float ccx = (float((sb & 1) * sub) + half) * h32, ccy = (float(((sb >> 1) & 1) * sub) + half) * h32,
@@ -1554,7 +1558,7 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
         // A group of RG lanes per edge.
         const uint32_t step = (WIDE ? blockDim.x : 32u) / RG, gl = lane % RG;
         const uint32_t gm = (0xffffffffu >> (32 - RG)) << (lane & ~uint32_t(RG - 1));
-        for (uint32_t e = a0 + (WIDE ? threadIdx.x : lane) / RG; e < a1; e += step) {
+        auto edge = [&](uint32_t e) {
             const uint32_t k = item_edges[e];
             uint32_t axis;
             int ex, ey, ez;
@@ -1563,6 +1567,20 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
             const float2 fv = edge_vals[k];
             const float t0 = MODE == REFINE_MLP ? out.t[k] : fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
             refine_edge_f32<RG>(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, k, out, int(gl), gm);
+        };
+        if (WIDE) {
+            // The block's groups claim the edges one at a time (their
+            // evaluation counts differ).
+            const uint32_t leader = lane & ~uint32_t(RG - 1);
+            for (;;) {
+                uint32_t e = 0;
+                if (gl == 0) e = atomicAdd(&sh_edge, 1u);
+                e = __shfl_sync(gm, e, leader);
+                if (e >= a1) break;
+                edge(e);
+            }
+        } else {
+            for (uint32_t e = a0 + lane / RG; e < a1; e += step) edge(e);
         }
     };
     if constexpr (MODE == REFINE_PLAIN && WIDE) {
