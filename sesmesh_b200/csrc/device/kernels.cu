@@ -1499,7 +1499,7 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
     unsigned long long* counters, Scene S, uint32_t* ovf, const uint32_t* list) {
     const uint32_t n_items = MANY ? uint32_t(*S.n_work) : n_host;
     extern __shared__ __align__(128) float4 rs[];
-    __shared__ uint32_t sh_q, sh_next, sh_edge;
+    __shared__ uint32_t sh_q, sh_next, sh_edge, sh_wedge[REFINE_WARPS];
     __shared__ uint32_t sh_off[REFINE_WARPS * REFINE_BATCH + 1], sh_sbase[REFINE_WARPS * REFINE_BATCH],
         sh_brick[REFINE_WARPS * REFINE_BATCH];
     __shared__ int sh_ns[REFINE_WARPS * REFINE_BATCH];
@@ -1547,6 +1547,7 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
             if (threadIdx.x == 0) sh_edge = a0;  // read after the staging's barrier
         } else {
             __syncwarp();
+            if (lane == 0) sh_wedge[warp] = a0;
         }
         const int sb = int(j & 7), sub = L.sub;
         const float h32 = float(L.h), half = 0.5f * float(sub);
@@ -1568,13 +1569,14 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
             const float t0 = MODE == REFINE_MLP ? out.t[k] : fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
             refine_edge_f32<RG>(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, k, out, int(gl), gm);
         };
-        if (WIDE) {
-            // The block's groups claim the edges one at a time (their
-            // evaluation counts differ).
+        if (WIDE || RG < 32) {
+            // The block's (warp's) groups claim the edges one at a time
+            // (their evaluation counts differ).
+            uint32_t* next = WIDE ? &sh_edge : &sh_wedge[warp];
             const uint32_t leader = lane & ~uint32_t(RG - 1);
             for (;;) {
                 uint32_t e = 0;
-                if (gl == 0) e = atomicAdd(&sh_edge, 1u);
+                if (gl == 0) e = atomicAdd(next, 1u);
                 e = __shfl_sync(gm, e, leader);
                 if (e >= a1) break;
                 edge(e);
