@@ -264,16 +264,34 @@ __global__ void k_triangle_area_volume(const float* pos, const uint32_t* tris, c
 
 // Thread per segment: its triangles' area and volume summed in triangle
 // order (one (component, chunk) partial of the host's sums).
-__global__ void k_segment_partials(const double* ta, const double* tv, const uint32_t* comp, const uint32_t* perm,
-                                   uint32_t nt, const uint32_t* start, uint32_t n_seg, Partial* out,
-                                   uint32_t* seg_comp) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+constexpr int SEG_WARPS = 4;     // warps (segments) per block of k_segment_partials
+constexpr uint32_t SEG_STAGE = 256;  // values per array a warp stages at a time
+
+// A warp per (component, chunk) segment: the lanes stage the segment's
+// per-triangle areas and volumes in shared memory, coalesced, and lane 0
+// sums them in triangle order (the host's order of additions).
+__global__ void __launch_bounds__(32 * SEG_WARPS) k_segment_partials(const double* ta, const double* tv,
+                                                                   const uint32_t* comp, const uint32_t* perm,
+                                                                   uint32_t nt, const uint32_t* start, uint32_t n_seg,
+                                                                   Partial* out, uint32_t* seg_comp) {
+    __shared__ double sa[SEG_WARPS][SEG_STAGE], sv[SEG_WARPS][SEG_STAGE];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t s = blockIdx.x * SEG_WARPS + warp;
     if (s >= n_seg) return;
     const uint32_t p0 = start[s], p1 = s + 1 < n_seg ? start[s + 1] : nt;
-    Partial acc{comp[p0], perm[p0] / SUM_CHUNK, 0ull, 0.0, 0.0};
-    for (uint32_t p = p0; p < p1; p++) acc.t++, acc.a += ta[p], acc.v += tv[p];
-    out[s] = acc;
-    seg_comp[s] = acc.comp;
+    double a = 0.0, v = 0.0;
+    for (uint32_t base = p0; base < p1; base += SEG_STAGE) {
+        const uint32_t cnt = min(SEG_STAGE, p1 - base);
+        for (uint32_t u = lane; u < cnt; u += 32) sa[warp][u] = ta[base + u], sv[warp][u] = tv[base + u];
+        __syncwarp();
+        if (lane == 0)
+            for (uint32_t u = 0; u < cnt; u++) a += sa[warp][u], v += sv[warp][u];
+        __syncwarp();
+    }
+    if (lane == 0) {
+        out[s] = Partial{comp[p0], perm[p0] / SUM_CHUNK, (unsigned long long)(p1 - p0), a, v};
+        seg_comp[s] = comp[p0];
+    }
 }
 
 // Partials in (component, chunk) order (sorted_idx: their order, or null
@@ -610,7 +628,8 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         Partial* parts = S.parts.as<Partial>();
         k_triangle_area_volume<<<blocks(nt), 256, 0, s>>>(pos, tris, S.tidx2.as<uint32_t>(), uint32_t(nt),
                                                           S.tri_a.as<double>(), S.tri_v.as<double>());
-        k_segment_partials<<<blocks(np), 256, 0, s>>>(S.tri_a.as<double>(), S.tri_v.as<double>(),
+        k_segment_partials<<<(np + SEG_WARPS - 1) / SEG_WARPS, 32 * SEG_WARPS, 0, s>>>(
+            S.tri_a.as<double>(), S.tri_v.as<double>(),
                                                       S.tkey2.as<uint32_t>(), S.tidx2.as<uint32_t>(), uint32_t(nt),
                                                       S.tidx.as<uint32_t>(), np, parts, S.pkey.as<uint32_t>());
         k_first_of_component<<<blocks(uint64_t(np) + 1), 256, 0, s>>>(S.pkey.as<uint32_t>(), np,
