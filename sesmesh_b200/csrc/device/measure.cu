@@ -319,13 +319,6 @@ __global__ void k_first_of_component(const uint32_t* sorted_comp, uint32_t n, ui
     for (uint32_t c = lo; c <= hi && c <= n_comp; c++) first[c] = i;
 }
 
-__global__ void k_euler_edges(const unsigned long long* keys, uint64_t cap, const uint32_t* id,
-                              unsigned long long* comp_edges) {
-    const uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const bool active = s < cap && keys[s] != EMPTY;
-    add_by_key(comp_edges, active ? id[uint32_t(keys[s] >> 32)] : 0u, active);
-}
-
 __global__ void k_triangle_keys(const uint32_t* tris, uint32_t nt, const uint32_t* id, uint32_t* key,
                                 uint32_t* idx) {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -437,7 +430,7 @@ unsigned bits_for(uint32_t n) {
 
 void MeasureScratch::release(bool synced) {
     for (DBuf* b : {&pos, &nrm, &tris, &tris_out, &keys, &cnt, &dup, &parent, &flag, &cid, &id, &counters, &comp_v,
-                    &comp_t, &comp_e, &area, &volume, &parts, &pkey, &pidx, &pkey2, &pidx2, &first, &tkey, &tidx,
+                    &comp_t, &area, &volume, &parts, &pkey, &pidx, &pkey2, &pidx2, &first, &tkey, &tidx,
                     &tkey2, &tidx2, &tiles, &cub, &packed, &err, &tri_a, &tri_v})
         synced ? b->release_synced() : b->release();
     pinned_free(host);
@@ -537,13 +530,12 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         return false;
     }
     const uint32_t nc = uint32_t(n_comp);
-    if (!R(S.comp_v, size_t(nc) * 8) || !R(S.comp_t, size_t(nc) * 8) || !R(S.comp_e, size_t(nc) * 8) ||
+    if (!R(S.comp_v, size_t(nc) * 8) || !R(S.comp_t, size_t(nc) * 8) ||
         !R(S.area, size_t(nc) * 8) || !R(S.volume, size_t(nc) * 8) || !R(S.first, (size_t(nc) + 1) * 4)) {
         if (msg) *msg = std::string("device memory for the measure: ") + e;
         return false;
     }
     MCK(cudaMemsetAsync(S.comp_v.p, 0, size_t(nc) * 8 + 8, s));
-    MCK(cudaMemsetAsync(S.comp_e.p, 0, size_t(nc) * 8 + 8, s));
     uint32_t* id = S.id.as<uint32_t>();
     if (nv) k_component_ids<<<blocks(nv), 256, 0, s>>>(parent, S.cid.as<uint32_t>(), uint32_t(nv), id,
                                                        S.comp_v.as<unsigned long long>());
@@ -572,9 +564,6 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         if (msg) *msg = "component copy";
         return false;
     }
-    if (nt)
-        k_euler_edges<<<blocks(ecap), 256, 0, s>>>(S.keys.as<unsigned long long>(), ecap, id,
-                                                   S.comp_e.as<unsigned long long>());
     auto sort_pairs = [&](const uint32_t* kin, uint32_t* kout, const uint32_t* vin, uint32_t* vout, uint32_t n,
                           unsigned bits) -> bool {
         size_t tmp = 0;
@@ -643,12 +632,11 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         MCK(cudaMemsetAsync(S.volume.p, 0, size_t(nc) * 8, s));
     }
     // Results to the host.
-    std::vector<unsigned long long> cv(nc), ct(nc), ce(nc);
+    std::vector<unsigned long long> cv(nc), ct(nc);
     std::vector<double> ca(nc), cvol(nc);
     if (nc) {
         MCK(cudaMemcpyAsync(cv.data(), S.comp_v.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
         MCK(cudaMemcpyAsync(ct.data(), S.comp_t.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
-        MCK(cudaMemcpyAsync(ce.data(), S.comp_e.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
         MCK(cudaMemcpyAsync(ca.data(), S.area.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
         MCK(cudaMemcpyAsync(cvol.data(), S.volume.p, size_t(nc) * 8, cudaMemcpyDeviceToHost, s));
     }
@@ -661,7 +649,10 @@ static bool measure_core(smb_device* d, const float* pos, const float* nrm, cons
         C.triangles = size_t(ct[c]);
         C.area = ca[c];
         C.volume = cvol[c];
-        C.euler = int64_t(cv[c]) - int64_t(ce[c]) + int64_t(ct[c]);
+        // The mesh passed the edge check: every edge is used once in each
+        // direction, by two triangles of one component, so the component has
+        // 3 T / 2 distinct edges.
+        C.euler = int64_t(cv[c]) - int64_t(3 * ct[c] / 2) + int64_t(ct[c]);
         C.first_triangle = start;
         start += C.triangles;
     }

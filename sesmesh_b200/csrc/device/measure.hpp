@@ -11,7 +11,7 @@ namespace smb {
 
 // Device buffers of the measure, kept between meshes.
 struct MeasureScratch {
-    DBuf pos, nrm, tris, tris_out, keys, cnt, dup, parent, flag, cid, id, counters, comp_v, comp_t, comp_e, area,
+    DBuf pos, nrm, tris, tris_out, keys, cnt, dup, parent, flag, cid, id, counters, comp_v, comp_t, area,
         volume, parts, pkey, pidx, pkey2, pidx2, first, tkey, tidx, tkey2, tidx2, tiles, cub, packed, err, tri_a,
         tri_v;
     void* host = nullptr;  // page-locked staging of the results
