@@ -224,9 +224,16 @@ __device__ __forceinline__ uint32_t x_rank(const double* keys, const uint32_t* i
 
 // gather_local of sub-block j's ball into `base` (cap bytes) with threads
 // tid of T; false when the lists do not fit.  cnt: 8 shared counters.
+// hint: the gather's record of the sub-block, or null.  Its list sizes are
+// those of a ball a hair smaller (the gather's rho has no margins), so with
+// a few entries more they bound this ball's sizes and the counting pass is
+// skipped; a list that outgrows them after all sends the ball back to the
+// counting pass.
+constexpr uint32_t X_HINT_SLACK = 4;
+
 template <bool WIDE>
 __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsigned char* base, size_t cap,
-                       uint32_t* cnt, uint32_t tid, uint32_t T, XView& v) {
+                       uint32_t* cnt, uint32_t tid, uint32_t T, XView& v, const uint32_t* hint = nullptr) {
     const int b = L.b, sub = L.sub, sb = int(j & 7);
     const double h = L.h, subd = double(sub);
     // local_of (extract.rs:165-177, 195-206): ball centre and radius.
@@ -238,122 +245,171 @@ __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsig
     const double rho = 0.5 * sqrt(3.0) * subd * h * (1.0 + 1e-9) + 1e-9;
     const double reach = A.probe + L.band + rho;
     v.cx = cx, v.cy = cy, v.cz = cz, v.rho = rho;
-    x_sync<WIDE>();
-    if (tid < 8) cnt[tid] = 0;
-    x_sync<WIDE>();
-    // Sizes.
-    x_for_near(A.gs, cx, cy, cz, reach + A.max_expanded, tid, T, [&](uint32_t k) {
-        const uint32_t st = A.status[k];
-        if (st == STATUS_CONTAINED) return;
-        const double4 c = A.sph[k];
-        const double d = dist3(cx, cy, cz, c.x, c.y, c.z);
-        if (d < c.w + reach) atomicAdd(&cnt[0], 1u);
-        if (d < c.w + rho) atomicAdd(&cnt[1], 1u);
-        if (st == STATUS_EXPOSED && fabs(d - c.w) <= reach) atomicAdd(&cnt[2], 1u);
-    });
-    x_for_near(A.gc, cx, cy, cz, reach + A.rho_max, tid, T, [&](uint32_t ci) {
-        if (circle_reach_dist(A, cx, cy, cz, ci) <= reach) atomicAdd(&cnt[3], 1u);
-    });
-    x_for_near(A.gv, cx, cy, cz, reach, tid, T, [&](uint32_t vi) {
-        const double4 p = A.vert[vi];
-        if (dist3(cx, cy, cz, p.x, p.y, p.z) <= reach) atomicAdd(&cnt[4], 1u);
-    });
-    x_sync<WIDE>();
-    const XCounts c{cnt[0], cnt[1], cnt[2], cnt[3], cnt[4]};
-    size_t tail = 0;
-    const size_t need = x_layout(c, base, v, &tail);
-    x_sync<WIDE>();
-    if (need > cap) return false;
-    if (tid < 8) cnt[tid] = 0;
-    x_sync<WIDE>();
-    // Spheres: near (scratch ids), inside (direct), S (scratch pairs).
-    x_for_near(A.gs, cx, cy, cz, reach + A.max_expanded, tid, T, [&](uint32_t k) {
-        const uint32_t st = A.status[k];
-        if (st == STATUS_CONTAINED) return;
-        const double4 s = A.sph[k];
-        const double d = dist3(cx, cy, cz, s.x, s.y, s.z);
-        if (d < s.w + reach) v.t_id[atomicAdd(&cnt[0], 1u)] = k;
-        if (d < s.w + rho) v.in_c[atomicAdd(&cnt[1], 1u)] = s;
-        const double lb = fabs(d - s.w);
-        if (st == STATUS_EXPOSED && lb <= reach) {
-            const uint32_t p = atomicAdd(&cnt[2], 1u);
-            v.t_key[p] = lb;
-            v.t_id[c.nn + p] = k;
+    bool hinted = hint && hint[R_FLAGS] == 0;
+    // Two attempts at most: hinted (when there is a hint), then counted.
+    for (;;) {
+        XCounts c;
+        if (hinted) {
+            c = XCounts{hint[R_NEAR] + X_HINT_SLACK, hint[R_INSIDE] + X_HINT_SLACK, hint[R_S] + X_HINT_SLACK,
+                        hint[R_C] + X_HINT_SLACK, hint[R_V] + X_HINT_SLACK};
+        } else {
+            x_sync<WIDE>();
+            if (tid < 8) cnt[tid] = 0;
+            x_sync<WIDE>();
+            // Sizes.
+            x_for_near(A.gs, cx, cy, cz, reach + A.max_expanded, tid, T, [&](uint32_t k) {
+                const uint32_t st = A.status[k];
+                if (st == STATUS_CONTAINED) return;
+                const double4 c = A.sph[k];
+                const double d = dist3(cx, cy, cz, c.x, c.y, c.z);
+                if (d < c.w + reach) atomicAdd(&cnt[0], 1u);
+                if (d < c.w + rho) atomicAdd(&cnt[1], 1u);
+                if (st == STATUS_EXPOSED && fabs(d - c.w) <= reach) atomicAdd(&cnt[2], 1u);
+            });
+            x_for_near(A.gc, cx, cy, cz, reach + A.rho_max, tid, T, [&](uint32_t ci) {
+                if (circle_reach_dist(A, cx, cy, cz, ci) <= reach) atomicAdd(&cnt[3], 1u);
+            });
+            x_for_near(A.gv, cx, cy, cz, reach, tid, T, [&](uint32_t vi) {
+                const double4 p = A.vert[vi];
+                if (dist3(cx, cy, cz, p.x, p.y, p.z) <= reach) atomicAdd(&cnt[4], 1u);
+            });
+            x_sync<WIDE>();
+            c = XCounts{cnt[0], cnt[1], cnt[2], cnt[3], cnt[4]};
         }
-    });
-    x_sync<WIDE>();
-    for (uint32_t i = tid; i < c.nn; i += T) {
-        const uint32_t id = v.t_id[i];
-        uint32_t r = 0;
-        for (uint32_t q = 0; q < c.nn; q++) r += v.t_id[q] < id ? 1u : 0u;
-        v.near_id[r] = id;
-        v.near_c[r] = A.sph[id];
-    }
-    for (uint32_t i = tid; i < c.ns; i += T) {
-        const double lb = v.t_key[i];
-        const uint32_t k = v.t_id[c.nn + i];
-        const uint32_t r = x_rank(v.t_key, v.t_id + c.nn, c.ns, lb, k);
-        v.s_id[r] = k;
-        v.s_key[r] = lb - rho - X_PRUNE;
-        v.s_c[r] = A.sph[k];
-    }
-    // Circles.
-    x_sync<WIDE>();
-    x_for_near(A.gc, cx, cy, cz, reach + A.rho_max, tid, T, [&](uint32_t ci) {
-        const double d = circle_reach_dist(A, cx, cy, cz, ci);
-        if (d <= reach) {
-            const uint32_t p = atomicAdd(&cnt[3], 1u);
-            v.t_key[p] = d;
-            v.t_id[p] = ci;
+        size_t tail = 0;
+        const size_t need = x_layout(c, base, v, &tail);
+        x_sync<WIDE>();
+        if (need > cap) {
+            if (hinted) {
+                hinted = false;
+                continue;
+            }
+            return false;
         }
-    });
-    x_sync<WIDE>();
-    for (uint32_t i = tid; i < c.nc; i += T) {
-        const double d = v.t_key[i];
-        const uint32_t ci = v.t_id[i];
-        const uint32_t r = x_rank(v.t_key, v.t_id, c.nc, d, ci);
-        const double* C = A.circ + 12 * size_t(ci);
-        v.c_id[r] = ci;
-        v.c_key[r] = d - rho - X_PRUNE;
-        v.c_m[r] = make_double4(C[0], C[1], C[2], C[9]);
-        v.c_u[r] = make_double4(C[3], C[4], C[5], C[6]);
-    }
-    x_sync<WIDE>();
-    // SAS vertices.
-    x_for_near(A.gv, cx, cy, cz, reach, tid, T, [&](uint32_t vi) {
-        const double4 p = A.vert[vi];
-        const double d = dist3(cx, cy, cz, p.x, p.y, p.z);
-        if (d <= reach) {
-            const uint32_t q = atomicAdd(&cnt[4], 1u);
-            v.t_key[q] = d;
-            v.t_id[q] = vi;
+        if (tid < 8) cnt[tid] = 0;
+        x_sync<WIDE>();
+        // Spheres: near (scratch ids), inside (direct), S (scratch pairs).
+        // Writes stay within the laid-out sizes; cnt[5] flags a list that
+        // went past them (only a hinted attempt can), which sends the ball
+        // to the counted attempt.
+        x_for_near(A.gs, cx, cy, cz, reach + A.max_expanded, tid, T, [&](uint32_t k) {
+            const uint32_t st = A.status[k];
+            if (st == STATUS_CONTAINED) return;
+            const double4 s = A.sph[k];
+            const double d = dist3(cx, cy, cz, s.x, s.y, s.z);
+            if (d < s.w + reach) {
+                const uint32_t p = atomicAdd(&cnt[0], 1u);
+                if (p < c.nn) v.t_id[p] = k;
+                else cnt[5] = 1;
+            }
+            if (d < s.w + rho) {
+                const uint32_t p = atomicAdd(&cnt[1], 1u);
+                if (p < c.ni) v.in_c[p] = s;
+                else cnt[5] = 1;
+            }
+            const double lb = fabs(d - s.w);
+            if (st == STATUS_EXPOSED && lb <= reach) {
+                const uint32_t p = atomicAdd(&cnt[2], 1u);
+                if (p < c.ns) v.t_key[p] = lb, v.t_id[c.nn + p] = k;
+                else cnt[5] = 1;
+            }
+        });
+        x_sync<WIDE>();
+        if (cnt[5]) {
+            hinted = false;
+            continue;
         }
-    });
-    x_sync<WIDE>();
-    for (uint32_t i = tid; i < c.nv; i += T) {
-        const double d = v.t_key[i];
-        const uint32_t vi = v.t_id[i];
-        const uint32_t r = x_rank(v.t_key, v.t_id, c.nv, d, vi);
-        v.v_id[r] = vi;
-        v.v_key[r] = d - rho - X_PRUNE;
-        v.v_p[r] = A.vert[vi];
+        const uint32_t nn = cnt[0], ni = cnt[1], ns = cnt[2];
+        for (uint32_t i = tid; i < nn; i += T) {
+            const uint32_t id = v.t_id[i];
+            uint32_t r = 0;
+            for (uint32_t q = 0; q < nn; q++) r += v.t_id[q] < id ? 1u : 0u;
+            v.near_id[r] = id;
+            v.near_c[r] = A.sph[id];
+        }
+        for (uint32_t i = tid; i < ns; i += T) {
+            const double lb = v.t_key[i];
+            const uint32_t k = v.t_id[c.nn + i];
+            const uint32_t r = x_rank(v.t_key, v.t_id + c.nn, ns, lb, k);
+            v.s_id[r] = k;
+            v.s_key[r] = lb - rho - X_PRUNE;
+            v.s_c[r] = A.sph[k];
+        }
+        // Circles.
+        x_sync<WIDE>();
+        x_for_near(A.gc, cx, cy, cz, reach + A.rho_max, tid, T, [&](uint32_t ci) {
+            const double d = circle_reach_dist(A, cx, cy, cz, ci);
+            if (d <= reach) {
+                const uint32_t p = atomicAdd(&cnt[3], 1u);
+                if (p < c.nc) v.t_key[p] = d, v.t_id[p] = ci;
+                else cnt[5] = 1;
+            }
+        });
+        x_sync<WIDE>();
+        if (cnt[5]) {
+            hinted = false;
+            continue;
+        }
+        const uint32_t nc = cnt[3];
+        for (uint32_t i = tid; i < nc; i += T) {
+            const double d = v.t_key[i];
+            const uint32_t ci = v.t_id[i];
+            const uint32_t r = x_rank(v.t_key, v.t_id, nc, d, ci);
+            const double* C = A.circ + 12 * size_t(ci);
+            v.c_id[r] = ci;
+            v.c_key[r] = d - rho - X_PRUNE;
+            v.c_m[r] = make_double4(C[0], C[1], C[2], C[9]);
+            v.c_u[r] = make_double4(C[3], C[4], C[5], C[6]);
+        }
+        x_sync<WIDE>();
+        // SAS vertices.
+        x_for_near(A.gv, cx, cy, cz, reach, tid, T, [&](uint32_t vi) {
+            const double4 p = A.vert[vi];
+            const double d = dist3(cx, cy, cz, p.x, p.y, p.z);
+            if (d <= reach) {
+                const uint32_t q = atomicAdd(&cnt[4], 1u);
+                if (q < c.nv) v.t_key[q] = d, v.t_id[q] = vi;
+                else cnt[5] = 1;
+            }
+        });
+        x_sync<WIDE>();
+        if (cnt[5]) {
+            hinted = false;
+            continue;
+        }
+        const uint32_t nv = cnt[4];
+        for (uint32_t i = tid; i < nv; i += T) {
+            const double d = v.t_key[i];
+            const uint32_t vi = v.t_id[i];
+            const uint32_t r = x_rank(v.t_key, v.t_id, nv, d, vi);
+            v.v_id[r] = vi;
+            v.v_key[r] = d - rho - X_PRUNE;
+            v.v_p[r] = A.vert[vi];
+        }
+        v.nn = nn, v.ni = ni, v.ns = ns, v.nc = nc, v.nv = nv;
+        // Blockers, kept to near spheres, in the scratch's place.
+        const bool sorted = A.pad & DARR_ROWS_SORTED;
+        x_blocker_counts(v, v.s_id, ns, A.nb_off, A.nb_items, v.s_off, sorted, tid, T);
+        x_blocker_counts(v, v.c_id, nc, A.cb_off, A.cb_items, v.c_off, sorted, tid, T);
+        x_sync<WIDE>();
+        x_offsets<WIDE>(v.s_off, ns, tid);
+        x_offsets<WIDE>(v.c_off, nc, tid);
+        x_sync<WIDE>();
+        const size_t nsb = v.s_off[ns], ncb = v.c_off[nc];
+        v.s_blk = reinterpret_cast<uint32_t*>(base + tail);
+        v.c_blk = reinterpret_cast<uint32_t*>(base + xal(tail + nsb * 4));
+        if (xal(tail + nsb * 4) + ncb * 4 > cap) {
+            if (hinted) {  // the laid-out bounds took the room: lay out the counted sizes
+                hinted = false;
+                continue;
+            }
+            return false;
+        }
+        x_blocker_fill(v, v.s_id, ns, A.nb_off, A.nb_items, v.s_off, v.s_blk, sorted, tid, T);
+        x_blocker_fill(v, v.c_id, nc, A.cb_off, A.cb_items, v.c_off, v.c_blk, sorted, tid, T);
+        x_sync<WIDE>();
+        return true;
     }
-    // Blockers, kept to near spheres, in the scratch's place.
-    const bool sorted = A.pad & DARR_ROWS_SORTED;
-    x_blocker_counts(v, v.s_id, c.ns, A.nb_off, A.nb_items, v.s_off, sorted, tid, T);
-    x_blocker_counts(v, v.c_id, c.nc, A.cb_off, A.cb_items, v.c_off, sorted, tid, T);
-    x_sync<WIDE>();
-    x_offsets<WIDE>(v.s_off, c.ns, tid);
-    x_offsets<WIDE>(v.c_off, c.nc, tid);
-    x_sync<WIDE>();
-    const size_t nsb = v.s_off[c.ns], ncb = v.c_off[c.nc];
-    v.s_blk = reinterpret_cast<uint32_t*>(base + tail);
-    v.c_blk = reinterpret_cast<uint32_t*>(base + xal(tail + nsb * 4));
-    if (xal(tail + nsb * 4) + ncb * 4 > cap) return false;
-    x_blocker_fill(v, v.s_id, c.ns, A.nb_off, A.nb_items, v.s_off, v.s_blk, sorted, tid, T);
-    x_blocker_fill(v, v.c_id, c.nc, A.cb_off, A.cb_items, v.c_off, v.c_blk, sorted, tid, T);
-    x_sync<WIDE>();
-    return true;
 }
 
 struct XEval {
@@ -783,7 +839,7 @@ __global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L
                                                                const uint32_t* item_edges, uint32_t n_items,
                                                                ExactOut out, size_t region, uint32_t* ovf,
                                                                unsigned char* slab, unsigned int* left,
-                                                               unsigned long long* counters) {
+                                                               unsigned long long* counters, const uint32_t* rec) {
     extern __shared__ __align__(16) unsigned char xs[];
     __shared__ uint32_t sh_cnt[X_WARPS][8];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -803,7 +859,8 @@ __global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L
         const uint32_t j = work[i];
         const int4 key = keys[j >> 3];
         XView v;
-        if (!x_ball<false>(A, L, key, j, mine, region, cnt, lane, 32u, v)) {
+        if (!x_ball<false>(A, L, key, j, mine, region, cnt, lane, 32u, v,
+                           rec ? rec + size_t(j) * REC_WORDS : nullptr)) {
             if (lane == 0) {
                 if (SLAB) atomicAdd(left, 1u);
                 else ovf[1 + atomicAdd(&ovf[0], 1u)] = i;
@@ -934,7 +991,8 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
                                        const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                        const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
-                                       unsigned long long* counters, int sms, size_t region, cudaStream_t s);
+                                       unsigned long long* counters, int sms, size_t region, cudaStream_t s,
+                                       const uint32_t* rec);
 
 size_t exact_slab_bytes(int sms) {
     int per_sm = 0;
@@ -947,22 +1005,22 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                 const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                 unsigned long long* counters, int sms, size_t region, cudaStream_t s, bool count,
-                                int group) {
+                                int group, const uint32_t* rec) {
     if (count) {
         cudaError_t e = cudaMemsetAsync(&counters[CNT_OPS], 0, 8, s);
         if (e != cudaSuccess) return e;
         return launch_exact_levels<true, 1, 1>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges,
-                                               n_items, out, ovf, slab, slab_bytes, counters, sms, region, s);
+                                               n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec);
     }
     // The slab pass takes the largest lists: at least 8 lanes per edge.
     if (group == 32)
         return launch_exact_levels<false, 32, 32>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges,
-                                                  n_items, out, ovf, slab, slab_bytes, counters, sms, region, s);
+                                                  n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec);
     if (group == 8)
         return launch_exact_levels<false, 8, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                                out, ovf, slab, slab_bytes, counters, sms, region, s);
+                                                out, ovf, slab, slab_bytes, counters, sms, region, s, rec);
     return launch_exact_levels<false, 1, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                            out, ovf, slab, slab_bytes, counters, sms, region, s);
+                                            out, ovf, slab, slab_bytes, counters, sms, region, s, rec);
 }
 
 template <bool COUNT, int RG, int RGS>
@@ -970,7 +1028,8 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
                                        const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                        const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
-                                       unsigned long long* counters, int sms, size_t region, cudaStream_t s) {
+                                       unsigned long long* counters, int sms, size_t region, cudaStream_t s,
+                                       const uint32_t* rec) {
     cudaError_t e;
     if ((e = cudaMemsetAsync(&counters[CNT_QUEUE], 0, 8, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&counters[CNT_XQUEUE], 0, 8, s)) != cudaSuccess) return e;
@@ -993,13 +1052,13 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
     unsigned int* left = reinterpret_cast<unsigned int*>(ovf) + 1 + n_items;
     if ((e = cudaMemsetAsync(left, 0, 4, s)) != cudaSuccess) return e;
     kn<<<grid, 32 * X_WARPS, narrow, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                          region, ovf, nullptr, left, counters);
+                                          region, ovf, nullptr, left, counters, rec);
     // The overflowed items: a warp each, lists in a global slab.
     const uint32_t slabs = uint32_t(slab_bytes / EXACT_SLAB);
     const uint32_t grid_g = std::max<uint32_t>(1, slabs / X_WARPS);
     if (!slab || !grid_g) return cudaErrorInvalidValue;
     kg<<<grid_g, 32 * X_WARPS, 0, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                       EXACT_SLAB, ovf, slab, left, counters);
+                                       EXACT_SLAB, ovf, slab, left, counters, rec);
     return cudaGetLastError();
 }
 
