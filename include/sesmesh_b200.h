@@ -234,6 +234,11 @@ int smb_batch_set_refine_group(smb_batch* batch, int lanes);
  * or more, else 1); the pass over sub-blocks with global list slabs takes
  * at least 8.  The vertices do not depend on it. */
 int smb_batch_set_exact_group(smb_batch* batch, int lanes);
+/* smb_refine_exact lays each sub-block's lists out from the gather's list
+ * sizes (1, the default), counts them first (0), or takes bounds one short
+ * of the gather's (2: every sub-block goes through the recount, for tests).
+ * The vertices do not depend on it. */
+int smb_batch_set_exact_hint(smb_batch* batch, int mode);
 /* Shared memory of each sampling CTA in a first pass over the sub-blocks
  * whose packed lists fit it (>= 1 KiB; 0, the default: 55 KiB); the others
  * run in a second pass with room for the largest. */

@@ -229,11 +229,14 @@ __device__ __forceinline__ uint32_t x_rank(const double* keys, const uint32_t* i
 // a few entries more they bound this ball's sizes and the counting pass is
 // skipped; a list that outgrows them after all sends the ball back to the
 // counting pass.
-constexpr uint32_t X_HINT_SLACK = 4;
+// slack: entries added to each hinted size (X_HINT_SLACK; 0 with the
+// bounds one short, which sends every ball through the counted layout).
+constexpr int X_HINT_SLACK = 4;
 
 template <bool WIDE>
 __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsigned char* base, size_t cap,
-                       uint32_t* cnt, uint32_t tid, uint32_t T, XView& v, const uint32_t* hint = nullptr) {
+                       uint32_t* cnt, uint32_t tid, uint32_t T, XView& v, const uint32_t* hint = nullptr,
+                       int slack = X_HINT_SLACK) {
     const int b = L.b, sub = L.sub, sb = int(j & 7);
     const double h = L.h, subd = double(sub);
     // local_of (extract.rs:165-177, 195-206): ball centre and radius.
@@ -250,8 +253,9 @@ __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsig
     for (;;) {
         XCounts c;
         if (hinted) {
-            c = XCounts{hint[R_NEAR] + X_HINT_SLACK, hint[R_INSIDE] + X_HINT_SLACK, hint[R_S] + X_HINT_SLACK,
-                        hint[R_C] + X_HINT_SLACK, hint[R_V] + X_HINT_SLACK};
+            auto bound = [&](uint32_t n) { return slack > 0 ? n + uint32_t(slack) : (n ? n - 1 : 0u); };
+            c = XCounts{bound(hint[R_NEAR]), bound(hint[R_INSIDE]), bound(hint[R_S]), bound(hint[R_C]),
+                        bound(hint[R_V])};
         } else {
             x_sync<WIDE>();
             if (tid < 8) cnt[tid] = 0;
@@ -839,7 +843,8 @@ __global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L
                                                                const uint32_t* item_edges, uint32_t n_items,
                                                                ExactOut out, size_t region, uint32_t* ovf,
                                                                unsigned char* slab, unsigned int* left,
-                                                               unsigned long long* counters, const uint32_t* rec) {
+                                                               unsigned long long* counters, const uint32_t* rec,
+                                                               int slack) {
     extern __shared__ __align__(16) unsigned char xs[];
     __shared__ uint32_t sh_cnt[X_WARPS][8];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -860,7 +865,7 @@ __global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L
         const int4 key = keys[j >> 3];
         XView v;
         if (!x_ball<false>(A, L, key, j, mine, region, cnt, lane, 32u, v,
-                           rec ? rec + size_t(j) * REC_WORDS : nullptr)) {
+                           rec ? rec + size_t(j) * REC_WORDS : nullptr, slack)) {
             if (lane == 0) {
                 if (SLAB) atomicAdd(left, 1u);
                 else ovf[1 + atomicAdd(&ovf[0], 1u)] = i;
@@ -992,7 +997,7 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                        const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                        unsigned long long* counters, int sms, size_t region, cudaStream_t s,
-                                       const uint32_t* rec);
+                                       const uint32_t* rec, int slack);
 
 size_t exact_slab_bytes(int sms) {
     int per_sm = 0;
@@ -1005,22 +1010,24 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                 const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                 unsigned long long* counters, int sms, size_t region, cudaStream_t s, bool count,
-                                int group, const uint32_t* rec) {
+                                int group, const uint32_t* rec, int hint) {
+    const int slack = hint == 2 ? 0 : X_HINT_SLACK;
+    if (hint == 0) rec = nullptr;
     if (count) {
         cudaError_t e = cudaMemsetAsync(&counters[CNT_OPS], 0, 8, s);
         if (e != cudaSuccess) return e;
         return launch_exact_levels<true, 1, 1>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges,
-                                               n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec);
+                                               n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack);
     }
     // The slab pass takes the largest lists: at least 8 lanes per edge.
     if (group == 32)
         return launch_exact_levels<false, 32, 32>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges,
-                                                  n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec);
+                                                  n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack);
     if (group == 8)
         return launch_exact_levels<false, 8, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                                out, ovf, slab, slab_bytes, counters, sms, region, s, rec);
+                                                out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack);
     return launch_exact_levels<false, 1, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                            out, ovf, slab, slab_bytes, counters, sms, region, s, rec);
+                                            out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack);
 }
 
 template <bool COUNT, int RG, int RGS>
@@ -1029,7 +1036,7 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                        const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                        unsigned long long* counters, int sms, size_t region, cudaStream_t s,
-                                       const uint32_t* rec) {
+                                       const uint32_t* rec, int slack) {
     cudaError_t e;
     if ((e = cudaMemsetAsync(&counters[CNT_QUEUE], 0, 8, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&counters[CNT_XQUEUE], 0, 8, s)) != cudaSuccess) return e;
@@ -1052,13 +1059,13 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
     unsigned int* left = reinterpret_cast<unsigned int*>(ovf) + 1 + n_items;
     if ((e = cudaMemsetAsync(left, 0, 4, s)) != cudaSuccess) return e;
     kn<<<grid, 32 * X_WARPS, narrow, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                          region, ovf, nullptr, left, counters, rec);
+                                          region, ovf, nullptr, left, counters, rec, slack);
     // The overflowed items: a warp each, lists in a global slab.
     const uint32_t slabs = uint32_t(slab_bytes / EXACT_SLAB);
     const uint32_t grid_g = std::max<uint32_t>(1, slabs / X_WARPS);
     if (!slab || !grid_g) return cudaErrorInvalidValue;
     kg<<<grid_g, 32 * X_WARPS, 0, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                       EXACT_SLAB, ovf, slab, left, counters, rec);
+                                       EXACT_SLAB, ovf, slab, left, counters, rec, slack);
     return cudaGetLastError();
 }
 

@@ -1113,7 +1113,7 @@ static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* 
                                         b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->item_off.as<uint32_t>(),
                                         b->item_edges.as<uint32_t>(), nw, out, b->x_ovf.as<uint32_t>(),
                                         b->x_slab.as<unsigned char>(), slab, cnt, d->info.multiprocessors,
-                                        b->x_region, s, count, exact_group(b), b->rec.as<uint32_t>());
+                                        b->x_region, s, count, exact_group(b), b->rec.as<uint32_t>(), b->x_hint);
     if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     uint32_t n_block = 0;
     CK(cudaMemcpyAsync(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost, s));
@@ -1251,6 +1251,12 @@ int smb_batch_set_refine_region(smb_batch* b, size_t bytes) {
 int smb_batch_set_sample_region(smb_batch* b, size_t bytes) {
     if (!b || (bytes && bytes < 1024)) return SMB_ERR_ARG;
     b->s_region = bytes;
+    return SMB_OK;
+}
+
+int smb_batch_set_exact_hint(smb_batch* b, int mode) {
+    if (!b || mode < 0 || mode > 2) return SMB_ERR_ARG;
+    b->x_hint = mode;
     return SMB_OK;
 }
 

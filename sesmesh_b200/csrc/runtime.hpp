@@ -118,6 +118,7 @@ struct smb_batch {
     size_t x_region = 13312;  // shared-memory bytes per warp for one sub-block's f64 candidate lists
     size_t s_region = 0;  // sampling: shared memory of the first pass's CTAs (0: SAMPLE_REGION)
     smb::DBuf s_list;     // sampling: the sub-blocks left to the second pass
+    int x_hint = 1;   // smb_refine_exact: list sizes from the gather's records (0 off, 2 one short)
     int x_group = 0;  // smb_refine_exact: lanes per edge (0: by the lists' mean size)
     int r_group = 0;  // smb_refine: lanes per edge (0: by the lists' mean size)
     unsigned long long pack_units = 0;  // the last run's list units (16 bytes each)

@@ -139,6 +139,7 @@ SIGNATURES = {
     "smb_batch_set_refine_region": (C.c_int, [_vp, _sz]),
     "smb_batch_set_refine_group": (C.c_int, [_vp, C.c_int]),
     "smb_batch_set_exact_group": (C.c_int, [_vp, C.c_int]),
+    "smb_batch_set_exact_hint": (C.c_int, [_vp, C.c_int]),
     "smb_batch_set_sample_region": (C.c_int, [_vp, _sz]),
     "smb_batch_exact_summary": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong),
                                           C.POINTER(C.c_ulonglong)]),

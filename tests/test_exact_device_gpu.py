@@ -46,7 +46,7 @@ def _cases():
 
 
 def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", warm=None, refine_region=None,
-          refine_group=None, exact_group=None, sample_region=None):
+          refine_group=None, exact_group=None, sample_region=None, exact_hint=None):
     from sesmesh_b200 import surface as S
     from sesmesh_b200.native import lib
     eng = S.SurfaceEngine(spheres, S.SurfaceParams.ses(probe).with_spacing(h).with_brick_size(brick)
@@ -62,6 +62,8 @@ def _mesh(spheres, probe, h, on_device, region=None, brick=10, refine="exact", w
         assert lib().smb_batch_set_refine_group(lib().smb_engine_batch(eng.h), refine_group) == 0
     if exact_group is not None:
         assert lib().smb_batch_set_exact_group(lib().smb_engine_batch(eng.h), exact_group) == 0
+    if exact_hint is not None:
+        assert lib().smb_batch_set_exact_hint(lib().smb_engine_batch(eng.h), exact_hint) == 0
     if sample_region is not None:
         assert lib().smb_batch_set_sample_region(lib().smb_engine_batch(eng.h), C.c_size_t(sample_region)) == 0
     out = eng.mesh()
@@ -143,6 +145,19 @@ def test_exact_groups_give_one_mesh(case, region, group):
     name, spheres, probe, h = case
     obj_1, st_1 = _mesh(spheres, probe, h, True, region=region, exact_group=1)
     obj_2, st_2 = _mesh(spheres, probe, h, True, region=region, exact_group=group)
+    for k in KEYS + ("refine_cpu_edges",):
+        assert st_1[k] == st_2[k], (k, st_1[k], st_2[k])
+    assert obj_1 == obj_2
+
+
+@pytest.mark.parametrize("hint", [0, 2])
+@pytest.mark.parametrize("region", [None, 1024], ids=["shared", "slab"])
+@pytest.mark.parametrize("case", [c for c in _cases() if c[0] in ("chain5", "globule330@0.5", "globule2800@0.25",
+                                                                   "stall4")], ids=lambda c: c[0])
+def test_exact_list_layouts_give_one_mesh(case, region, hint):
+    name, spheres, probe, h = case
+    obj_1, st_1 = _mesh(spheres, probe, h, True, region=region)
+    obj_2, st_2 = _mesh(spheres, probe, h, True, region=region, exact_hint=hint)
     for k in KEYS + ("refine_cpu_edges",):
         assert st_1[k] == st_2[k], (k, st_1[k], st_2[k])
     assert obj_1 == obj_2
