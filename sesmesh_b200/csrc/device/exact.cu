@@ -233,10 +233,97 @@ __device__ __forceinline__ uint32_t x_rank(const double* keys, const uint32_t* i
 // bounds one short, which sends every ball through the counted layout).
 constexpr int X_HINT_SLACK = 4;
 
+// Blocker rows of the ball's S and C candidates kept to its near spheres,
+// laid out from `tail`; false when they do not fit in cap.
+template <bool WIDE>
+__device__ bool x_blockers(const DArr& A, unsigned char* base, size_t cap, size_t tail, uint32_t tid, uint32_t T,
+                           XView& v) {
+    const bool sorted = A.pad & DARR_ROWS_SORTED;
+    x_blocker_counts(v, v.s_id, v.ns, A.nb_off, A.nb_items, v.s_off, sorted, tid, T);
+    x_blocker_counts(v, v.c_id, v.nc, A.cb_off, A.cb_items, v.c_off, sorted, tid, T);
+    x_sync<WIDE>();
+    x_offsets<WIDE>(v.s_off, v.ns, tid);
+    x_offsets<WIDE>(v.c_off, v.nc, tid);
+    x_sync<WIDE>();
+    const size_t nsb = v.s_off[v.ns], ncb = v.c_off[v.nc];
+    v.s_blk = reinterpret_cast<uint32_t*>(base + tail);
+    v.c_blk = reinterpret_cast<uint32_t*>(base + xal(tail + nsb * 4));
+    if (xal(tail + nsb * 4) + ncb * 4 > cap) return false;
+    x_blocker_fill(v, v.s_id, v.ns, A.nb_off, A.nb_items, v.s_off, v.s_blk, sorted, tid, T);
+    x_blocker_fill(v, v.c_id, v.nc, A.cb_off, A.cb_items, v.c_off, v.c_blk, sorted, tid, T);
+    x_sync<WIDE>();
+    return true;
+}
+
+// The ball's lists straight from the gather's candidate ids (ids: the
+// sub-block's CSR words, hint its record), for a sub-block whose gather
+// found no candidate on which the two balls disagree: the sets are then
+// equal, S and C come in the same (key, index) order, the near list's
+// first R_INSIDE entries are the inside spheres; near is re-sorted by index
+// and V by (distance, index).  False when they do not fit in cap.
+template <bool WIDE>
+__device__ bool x_ball_from_ids(const DArr& A, double cx, double cy, double cz, double rho, unsigned char* base,
+                                size_t cap, uint32_t tid, uint32_t T, XView& v, const uint32_t* hint,
+                                const uint32_t* ids) {
+    const XCounts c{hint[R_NEAR], hint[R_INSIDE], hint[R_S], hint[R_C], hint[R_V]};
+    size_t tail = 0;
+    const size_t need = x_layout(c, base, v, &tail);
+    x_sync<WIDE>();
+    if (need > cap) return false;
+    const uint32_t* l_near = ids;
+    const uint32_t* l_s = l_near + c.nn;
+    const uint32_t* l_c = l_s + c.ns + (c.ns + 1) + hint[R_SBLK];
+    const uint32_t* l_v = l_c + c.nc + (c.nc + 1) + hint[R_CBLK];
+    for (uint32_t i = tid; i < c.nn; i += T) v.t_id[i] = l_near[i];
+    for (uint32_t i = tid; i < c.ni; i += T) v.in_c[i] = A.sph[l_near[i]];
+    for (uint32_t i = tid; i < c.ns; i += T) {
+        const uint32_t k = l_s[i];
+        const double4 s = A.sph[k];
+        v.s_id[i] = k;
+        v.s_key[i] = fabs(dist3(cx, cy, cz, s.x, s.y, s.z) - s.w) - rho - X_PRUNE;
+        v.s_c[i] = s;
+    }
+    for (uint32_t i = tid; i < c.nc; i += T) {
+        const uint32_t ci = l_c[i];
+        const double* C = A.circ + 12 * size_t(ci);
+        v.c_id[i] = ci;
+        v.c_key[i] = circle_reach_dist(A, cx, cy, cz, ci) - rho - X_PRUNE;
+        v.c_m[i] = make_double4(C[0], C[1], C[2], C[9]);
+        v.c_u[i] = make_double4(C[3], C[4], C[5], C[6]);
+    }
+    x_sync<WIDE>();
+    for (uint32_t i = tid; i < c.nn; i += T) {
+        const uint32_t id = v.t_id[i];
+        uint32_t r = 0;
+        for (uint32_t q = 0; q < c.nn; q++) r += v.t_id[q] < id ? 1u : 0u;
+        v.near_id[r] = id;
+        v.near_c[r] = A.sph[id];
+    }
+    x_sync<WIDE>();
+    // V: (distance, index) pairs in the scratch (the near ids are placed).
+    for (uint32_t i = tid; i < c.nv; i += T) {
+        const uint32_t vi = l_v[i];
+        const double4 p = A.vert[vi];
+        v.t_key[i] = dist3(cx, cy, cz, p.x, p.y, p.z);
+        v.t_id[i] = vi;
+    }
+    x_sync<WIDE>();
+    for (uint32_t i = tid; i < c.nv; i += T) {
+        const double d = v.t_key[i];
+        const uint32_t vi = v.t_id[i];
+        const uint32_t r = x_rank(v.t_key, v.t_id, c.nv, d, vi);
+        v.v_id[r] = vi;
+        v.v_key[r] = d - rho - X_PRUNE;
+        v.v_p[r] = A.vert[vi];
+    }
+    x_sync<WIDE>();
+    return x_blockers<WIDE>(A, base, cap, tail, tid, T, v);
+}
+
 template <bool WIDE>
 __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsigned char* base, size_t cap,
                        uint32_t* cnt, uint32_t tid, uint32_t T, XView& v, const uint32_t* hint = nullptr,
-                       int slack = X_HINT_SLACK) {
+                       int slack = X_HINT_SLACK, const uint32_t* ids = nullptr, const uint8_t* window = nullptr) {
     const int b = L.b, sub = L.sub, sb = int(j & 7);
     const double h = L.h, subd = double(sub);
     // local_of (extract.rs:165-177, 195-206): ball centre and radius.
@@ -249,6 +336,8 @@ __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsig
     const double reach = A.probe + L.band + rho;
     v.cx = cx, v.cy = cy, v.cz = cz, v.rho = rho;
     bool hinted = hint && hint[R_FLAGS] == 0;
+    if (hinted && ids && window && window[j] == 0 && slack > 0)
+        return x_ball_from_ids<WIDE>(A, cx, cy, cz, rho, base, cap, tid, T, v, hint, ids + hint[R_IDS]);
     // Two attempts at most: hinted (when there is a hint), then counted.
     for (;;) {
         XCounts c;
@@ -392,27 +481,9 @@ __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsig
         }
         v.nn = nn, v.ni = ni, v.ns = ns, v.nc = nc, v.nv = nv;
         // Blockers, kept to near spheres, in the scratch's place.
-        const bool sorted = A.pad & DARR_ROWS_SORTED;
-        x_blocker_counts(v, v.s_id, ns, A.nb_off, A.nb_items, v.s_off, sorted, tid, T);
-        x_blocker_counts(v, v.c_id, nc, A.cb_off, A.cb_items, v.c_off, sorted, tid, T);
-        x_sync<WIDE>();
-        x_offsets<WIDE>(v.s_off, ns, tid);
-        x_offsets<WIDE>(v.c_off, nc, tid);
-        x_sync<WIDE>();
-        const size_t nsb = v.s_off[ns], ncb = v.c_off[nc];
-        v.s_blk = reinterpret_cast<uint32_t*>(base + tail);
-        v.c_blk = reinterpret_cast<uint32_t*>(base + xal(tail + nsb * 4));
-        if (xal(tail + nsb * 4) + ncb * 4 > cap) {
-            if (hinted) {  // the laid-out bounds took the room: lay out the counted sizes
-                hinted = false;
-                continue;
-            }
-            return false;
-        }
-        x_blocker_fill(v, v.s_id, ns, A.nb_off, A.nb_items, v.s_off, v.s_blk, sorted, tid, T);
-        x_blocker_fill(v, v.c_id, nc, A.cb_off, A.cb_items, v.c_off, v.c_blk, sorted, tid, T);
-        x_sync<WIDE>();
-        return true;
+        if (x_blockers<WIDE>(A, base, cap, tail, tid, T, v)) return true;
+        if (!hinted) return false;
+        hinted = false;  // the laid-out bounds took the room: lay out the counted sizes
     }
 }
 
@@ -844,7 +915,8 @@ __global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L
                                                                ExactOut out, size_t region, uint32_t* ovf,
                                                                unsigned char* slab, unsigned int* left,
                                                                unsigned long long* counters, const uint32_t* rec,
-                                                               int slack) {
+                                                               int slack, const uint32_t* gids,
+                                                               const uint8_t* window) {
     extern __shared__ __align__(16) unsigned char xs[];
     __shared__ uint32_t sh_cnt[X_WARPS][8];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -865,7 +937,7 @@ __global__ void __launch_bounds__(32 * X_WARPS, 4) k_refine_exact(DArr A, DLat L
         const int4 key = keys[j >> 3];
         XView v;
         if (!x_ball<false>(A, L, key, j, mine, region, cnt, lane, 32u, v,
-                           rec ? rec + size_t(j) * REC_WORDS : nullptr, slack)) {
+                           rec ? rec + size_t(j) * REC_WORDS : nullptr, slack, gids, window)) {
             if (lane == 0) {
                 if (SLAB) atomicAdd(left, 1u);
                 else ovf[1 + atomicAdd(&ovf[0], 1u)] = i;
@@ -997,7 +1069,8 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                        const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                        unsigned long long* counters, int sms, size_t region, cudaStream_t s,
-                                       const uint32_t* rec, int slack);
+                                       const uint32_t* rec, int slack, const uint32_t* gids,
+                                       const uint8_t* window);
 
 size_t exact_slab_bytes(int sms) {
     int per_sm = 0;
@@ -1010,24 +1083,25 @@ cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                 const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                 unsigned long long* counters, int sms, size_t region, cudaStream_t s, bool count,
-                                int group, const uint32_t* rec, int hint) {
+                                int group, const uint32_t* rec, int hint, const uint32_t* gids,
+                                const uint8_t* window) {
     const int slack = hint == 2 ? 0 : X_HINT_SLACK;
     if (hint == 0) rec = nullptr;
     if (count) {
         cudaError_t e = cudaMemsetAsync(&counters[CNT_OPS], 0, 8, s);
         if (e != cudaSuccess) return e;
         return launch_exact_levels<true, 1, 1>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges,
-                                               n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack);
+                                               n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack, gids, window);
     }
     // The slab pass takes the largest lists: at least 8 lanes per edge.
     if (group == 32)
         return launch_exact_levels<false, 32, 32>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges,
-                                                  n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack);
+                                                  n_items, out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack, gids, window);
     if (group == 8)
         return launch_exact_levels<false, 8, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                                out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack);
+                                                out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack, gids, window);
     return launch_exact_levels<false, 1, 8>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items,
-                                            out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack);
+                                            out, ovf, slab, slab_bytes, counters, sms, region, s, rec, slack, gids, window);
 }
 
 template <bool COUNT, int RG, int RGS>
@@ -1036,7 +1110,8 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
                                        const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                        const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                        unsigned long long* counters, int sms, size_t region, cudaStream_t s,
-                                       const uint32_t* rec, int slack) {
+                                       const uint32_t* rec, int slack, const uint32_t* gids,
+                                       const uint8_t* window) {
     cudaError_t e;
     if ((e = cudaMemsetAsync(&counters[CNT_QUEUE], 0, 8, s)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(&counters[CNT_XQUEUE], 0, 8, s)) != cudaSuccess) return e;
@@ -1059,13 +1134,13 @@ static cudaError_t launch_exact_levels(const DArr& A, const DLat& L, const Exact
     unsigned int* left = reinterpret_cast<unsigned int*>(ovf) + 1 + n_items;
     if ((e = cudaMemsetAsync(left, 0, 4, s)) != cudaSuccess) return e;
     kn<<<grid, 32 * X_WARPS, narrow, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                          region, ovf, nullptr, left, counters, rec, slack);
+                                          region, ovf, nullptr, left, counters, rec, slack, gids, window);
     // The overflowed items: a warp each, lists in a global slab.
     const uint32_t slabs = uint32_t(slab_bytes / EXACT_SLAB);
     const uint32_t grid_g = std::max<uint32_t>(1, slabs / X_WARPS);
     if (!slab || !grid_g) return cudaErrorInvalidValue;
     kg<<<grid_g, 32 * X_WARPS, 0, s>>>(A, L, X, keys, work, edges, edge_vals, item_off, item_edges, n_items, out,
-                                       EXACT_SLAB, ovf, slab, left, counters, rec, slack);
+                                       EXACT_SLAB, ovf, slab, left, counters, rec, slack, gids, window);
     return cudaGetLastError();
 }
 

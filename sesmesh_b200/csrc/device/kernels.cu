@@ -334,6 +334,17 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
                  bz = pz + (double((sb >> 2) & 1) * sub + half) * h;
     const double rho = L.rho_sub;
     const double reach = A.probe + L.band + rho;
+    // The exact refinement's ball (exact.cu x_ball: rho with a relative and
+    // an absolute 1e-9 margin).  With O.window the scans cover its larger
+    // boxes (the extra cells hold nothing this ball keeps, so the lists and
+    // their order do not change) and each candidate is also tested against
+    // it; a disagreement marks the sub-block.
+    const bool win = O.window != nullptr;
+    const double rho_x = 0.5 * sqrt(3.0) * sub * h * (1.0 + 1e-9) + 1e-9;
+    const double reach_x = A.probe + L.band + rho_x;
+    const double r_sph = win ? reach_x + A.max_expanded : reach + A.max_expanded;
+    const double r_circ = win ? reach_x + A.rho_max : reach + A.rho_max, r_vert = win ? reach_x : reach;
+    bool differ = false;
 
     if (lane == 0) rec[R_FLAGS] = 0;
     auto overflow = [&](uint32_t bit) {
@@ -350,13 +361,20 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
     // Near spheres, two passes (gather_near).
     int nn = 0, n_in = 0;
     for (int pass = 0; pass < 2; pass++) {
-        warp_scan_box(A.gs, bx, by, bz, reach + A.max_expanded, lane, [&](bool valid, uint32_t k) {
+        warp_scan_box(A.gs, bx, by, bz, r_sph, lane, [&](bool valid, uint32_t k) {
             bool keep = false;
             if (valid && A.status[k] != STATUS_CONTAINED) {
                 double4 c = A.sph[k];
                 double d = dist3(bx, by, bz, c.x, c.y, c.z);
                 bool contains = d < c.w + rho;
-                keep = !(d >= c.w + reach) && (contains == (pass == 0));
+                const bool near = !(d >= c.w + reach);
+                keep = near && (contains == (pass == 0));
+                if (win && pass == 0) {
+                    const bool exposed = A.status[k] == STATUS_EXPOSED;
+                    const double lb = fabs(d - c.w);
+                    differ |= (d < c.w + reach_x) != near || (d < c.w + rho_x) != contains ||
+                              (exposed && lb <= reach_x) != (exposed && near && lb <= reach);
+                }
             }
             int pos = warp_append(keep, nn);
             if (pos >= 0 && pos < caps.near) near_ids[pos] = k;
@@ -396,19 +414,22 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
     }
     // Class C candidates.
     int nc = 0;
-    warp_scan_box(A.gc, bx, by, bz, reach + A.rho_max, lane, [&](bool valid, uint32_t ci) {
+    warp_scan_box(A.gc, bx, by, bz, r_circ, lane, [&](bool valid, uint32_t ci) {
         double d = valid ? circle_reach_dist(A, bx, by, bz, ci) : 0.0;
         bool p = valid && d <= reach;
+        if (win && valid) differ |= (d <= reach_x) != p;
         int pos = warp_append(p, nc);
         if (pos >= 0 && pos < caps.c) c_key[pos] = d, c_id[pos] = ci;
     });
     // Class V, cell-scan order.
     int nv = 0;
-    warp_scan_box(A.gv, bx, by, bz, reach, lane, [&](bool valid, uint32_t vi) {
+    warp_scan_box(A.gv, bx, by, bz, r_vert, lane, [&](bool valid, uint32_t vi) {
         bool p = false;
         if (valid) {
             double4 q = A.vert[vi];
-            p = dist3(bx, by, bz, q.x, q.y, q.z) <= reach;
+            const double d = dist3(bx, by, bz, q.x, q.y, q.z);
+            p = d <= reach;
+            if (win) differ |= (d <= reach_x) != p;
         }
         int pos = warp_append(p, nv);
         if (pos >= 0 && pos < caps.v) v_id[pos] = vi;
@@ -562,7 +583,9 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         double4 q = A.vert[vi];
         p_v[i] = make_float4(float(q.x - L.fx), float(q.y - L.fy), float(q.z - L.fz), 0.0f);
     }
+    const bool any_differ = __any_sync(0xffffffffu, differ);
     if (lane == 0) {
+        if (win) O.window[j] = any_differ ? 1 : 0;
         rec[R_IDS] = uint32_t(ids_base);
         rec[R_INSIDE] = uint32_t(n_in);
         rec[R_NEAR] = uint32_t(nn);
@@ -579,7 +602,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
 // Warp per work item, the grid striding over the items (many structures:
 // the item count is read on the device).
 template <bool MANY>
-__global__ void k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
+__global__ void __launch_bounds__(256, MANY ? 2 : 3) k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
                          GatherCaps caps, Scene S) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t n = MANY ? uint32_t(*S.n_work) : n_work;

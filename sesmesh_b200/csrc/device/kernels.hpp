@@ -42,6 +42,10 @@ struct GatherOut {
     unsigned long long ids_cap, pack_cap;
     unsigned long long unit_cap;  // largest packed block of one sub-block
     uint32_t* fail;               // per structure (many-structure runs), else null
+    // Per sub-block (null: not kept): 1 when some candidate passes the
+    // exact refinement's ball test (rho with its margins) but not the
+    // gather's or the other way round, else 0.
+    uint8_t* window = nullptr;
 };
 
 // Fast-mode refinement constants (RefineRef, sesmesh-gpu batch.rs:133-150).
@@ -138,13 +142,16 @@ cudaError_t launch_exact_summary(const uint32_t* evals, size_t n, unsigned long 
 // of the field evaluations (x_eval's rules).  rec: the gather's records of
 // the sub-blocks (their list sizes bound each ball's), or null; hint 0: do
 // not use them, 2: bounds one short (every ball through the counted layout).
+// gids, window: the gather's candidate ids and its per-sub-block marks
+// (GatherOut::window); an unmarked sub-block takes its lists from the ids.
 size_t exact_slab_bytes(int sms);
 cudaError_t launch_refine_exact(const DArr& A, const DLat& L, const ExactAttr& X, const int4* keys,
                                 const uint32_t* work, const uint32_t* edges, const float2* edge_vals,
                                 const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items,
                                 const ExactOut& out, uint32_t* ovf, unsigned char* slab, size_t slab_bytes,
                                 unsigned long long* counters, int sms, size_t region, cudaStream_t s,
-                                bool count = false, int group = 1, const uint32_t* rec = nullptr, int hint = 1);
+                                bool count = false, int group = 1, const uint32_t* rec = nullptr, int hint = 1,
+                                const uint32_t* gids = nullptr, const uint8_t* window = nullptr);
 void launch_selftest(const float* a, const float* b, uint32_t* out, uint32_t n, cudaStream_t s);
 void launch_scan(const uint32_t* in, uint32_t n, uint32_t* out, uint32_t* keep, unsigned long long* tiles,
                  unsigned long long* total, cudaStream_t s);

@@ -749,7 +749,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
         (rc = b->tiles.reserve(size_t(scan_tiles_needed(uint32_t(nsub))) * 8, err, errlen)) ||
         (rc = b->totals.reserve(64, err, errlen)) || (rc = b->counters.reserve(CNT_N * 8, err, errlen)) ||
         (rc = b->mc_counts.reserve(count * 8, err, errlen)) || (rc = b->edge_off.reserve(count * 4 + 4, err, errlen)) ||
-        (rc = b->tri_off.reserve(count * 4 + 4, err, errlen)))
+        (rc = b->tri_off.reserve(count * 4 + 4, err, errlen)) || (rc = b->x_window.reserve(nsub, err, errlen)))
         return rc;
     cudaEventRecord(b->ev[0], s);
     launch_substates(r->A, L, keys, uint32_t(count), b->rec.as<uint32_t>(), b->sampled.as<uint32_t>(), s);
@@ -772,7 +772,8 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
             return rc;
         CK(cudaMemsetAsync(b->counters.p, 0, CNT_N * 8, s));
         GatherOut O{b->rec.as<uint32_t>(), b->ids.as<uint32_t>(), b->pack.as<uint4>(), b->retry_a.as<uint32_t>(),
-                    b->counters.as<unsigned long long>(), b->ids.cap / 4, b->pack.cap / 16, ~0ull, nullptr};
+                    b->counters.as<unsigned long long>(), b->ids.cap / 4, b->pack.cap / 16, ~0ull, nullptr,
+                    b->x_window.as<uint8_t>()};
         cudaError_t e = launch_gather(r->A, L, keys, b->work.as<uint32_t>(), uint32_t(n_work), O, caps, b->gather_warps, s);
         if (e != cudaSuccess) return set_err(err, errlen, "gather launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
         CK(cudaMemcpyAsync(cnt, b->counters.p, CNT_N * 8, cudaMemcpyDeviceToHost, s));
@@ -1113,7 +1114,8 @@ static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* 
                                         b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->item_off.as<uint32_t>(),
                                         b->item_edges.as<uint32_t>(), nw, out, b->x_ovf.as<uint32_t>(),
                                         b->x_slab.as<unsigned char>(), slab, cnt, d->info.multiprocessors,
-                                        b->x_region, s, count, exact_group(b), b->rec.as<uint32_t>(), b->x_hint);
+                                        b->x_region, s, count, exact_group(b), b->rec.as<uint32_t>(), b->x_hint,
+                                        b->ids.as<uint32_t>(), b->x_window.as<uint8_t>());
     if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     uint32_t n_block = 0;
     CK(cudaMemcpyAsync(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost, s));

@@ -112,6 +112,7 @@ struct smb_batch {
     // Vertices refined or placed on the device: position, normal, atom, patch,
     // t, evaluations; overflowed items, summary words, fast-mode exact mask.
     smb::DBuf x_pos, x_nrm, x_atom, x_patch, x_t, x_evals, x_ovf, x_sum, x_mask, x_slab;
+    smb::DBuf x_window;  // per sub-block: the gather's and the exact ball's tests disagree somewhere
     bool refined_exact = false;
     size_t x_exact_edges = 0;  // edges the exact refinement took in the last pass
     size_t x_block_items = 0;  // items of the last exact pass refined by a whole block
@@ -130,6 +131,6 @@ struct smb_batch {
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
                 &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &item_counts, &item_off, &item_edges,
-                &x_pos, &x_nrm, &x_atom, &x_patch, &x_t, &x_evals, &x_ovf, &x_sum, &x_mask, &x_slab, &s_list};
+                &x_pos, &x_nrm, &x_atom, &x_patch, &x_t, &x_evals, &x_ovf, &x_sum, &x_mask, &x_slab, &s_list, &x_window};
     }
 };
