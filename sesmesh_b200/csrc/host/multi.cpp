@@ -739,6 +739,7 @@ int finish_structure_device(smb_multi* m, const Group& G, size_t i, const uint32
         return set_err(err, errlen, "copy of structure %zu's results failed", i), SMB_ERR_CUDA;
     count_launches(3);
     b->first = 0;
+    b->window_ok = false;  // the slice brings records, not the gather's ids or marks
     b->n = uint32_t(nb);
     b->n_work = uint32_t(nw);
     b->n_edges = ne;

@@ -741,6 +741,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     }
     const int4* keys = r->keys + first;
     const size_t nsub = count * 8;
+    b->window_ok = false;
     int rc;
     if ((rc = b->rec.reserve(nsub * REC_WORDS * 4, err, errlen)) || (rc = b->sampled.reserve(nsub * 4, err, errlen)) ||
         (rc = b->work.reserve(nsub * 4, err, errlen)) || (rc = b->retry_a.reserve(nsub * 4, err, errlen)) ||
@@ -814,6 +815,7 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
         break;
     }
     b->ids_words = size_t(cnt[CNT_IDS]);
+    b->window_ok = true;
     b->max_pack = uint32_t(cnt[CNT_MAXPACK]);
     b->pack_units = cnt[CNT_PACK];
     {
@@ -1115,7 +1117,8 @@ static int exact_pass(smb_resident* r, smb_batch* b, const uint8_t* mask, char* 
                                         b->item_edges.as<uint32_t>(), nw, out, b->x_ovf.as<uint32_t>(),
                                         b->x_slab.as<unsigned char>(), slab, cnt, d->info.multiprocessors,
                                         b->x_region, s, count, exact_group(b), b->rec.as<uint32_t>(), b->x_hint,
-                                        b->ids.as<uint32_t>(), b->x_window.as<uint8_t>());
+                                        b->window_ok ? b->ids.as<uint32_t>() : nullptr,
+                                        b->window_ok ? b->x_window.as<uint8_t>() : nullptr);
     if (e != cudaSuccess) return set_err(err, errlen, "exact refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     uint32_t n_block = 0;
     CK(cudaMemcpyAsync(&n_block, b->x_ovf.p, 4, cudaMemcpyDeviceToHost, s));

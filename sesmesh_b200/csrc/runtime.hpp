@@ -113,6 +113,7 @@ struct smb_batch {
     // t, evaluations; overflowed items, summary words, fast-mode exact mask.
     smb::DBuf x_pos, x_nrm, x_atom, x_patch, x_t, x_evals, x_ovf, x_sum, x_mask, x_slab;
     smb::DBuf x_window;  // per sub-block: the gather's and the exact ball's tests disagree somewhere
+    bool window_ok = false;  // x_window and ids are this batch's last gather's (smb_run)
     bool refined_exact = false;
     size_t x_exact_edges = 0;  // edges the exact refinement took in the last pass
     size_t x_block_items = 0;  // items of the last exact pass refined by a whole block
