@@ -8,11 +8,14 @@ Workload (N=1): rings58800 -- 58,800 spheres (21 copies of a seeded
 * value -- device mesh-stage throughput in Mgridpts/s (grid points =
   surface bricks x (b+1)^3, as sesmesh counts samples) with the arrangement
   resident in HBM: brick classification, sub-block states, candidate gather,
-  field sampling and marching-cubes compaction, timed with CUDA events on the
-  library's stream; L2 flushed (256 MiB write) before every step.
+  field sampling, marching-cubes compaction and the vertex refinement (f64
+  in exact mode), timed with CUDA events on the library's stream; L2
+  flushed (256 MiB write) before every step.
 * e2e -- the same metric through the public API (compute_surface from host
-  sphere arrays): host arrangement, upload, device stage, copies back, host
-  f64 refinement, assembly, validation, components; wall clock.
+  sphere arrays): the arrangement (on the device for 16,384 spheres or
+  more), the device stage, the mesh's assembly, validation, components,
+  area and volume on the device, and the finished mesh copied back to
+  page-locked host memory; wall clock.
 * roofline -- the dominant kernel against its bound: counted operations of
   its evaluations per launch over the launch's CUDA-event time.
 * cpu_baseline -- the CPU oracle (C++ restatement of sesmesh's CPU back end)
