@@ -316,24 +316,31 @@ int smb_batch_edge_features(smb_resident* res, smb_batch* batch, float* features
 /* Marching cubes (the last pass of smb_run) over caller-owned device
  * buffers, with no device allocation at all.  This entry point has no
  * counterpart in the reference: it serves callers that cannot allocate
- * device memory while they mesh (code inside a CUDA stream capture, loops
- * under a fixed device-memory budget, hosts whose allocator belongs to
- * another framework).  Its scratch (per-brick counts, scan tiles, totals;
- * 528 KiB) is one static device array that every GPU loading the library
- * holds until exit; at most SMB_MC_NOALLOC_MAX_BRICKS bricks per call, more
- * are rejected with SMB_ERR_ARG.
+ * device memory while they mesh, such as services that reserve a fixed
+ * device-memory budget up front and must not grow it while serving, and
+ * hosts whose device memory belongs to another framework's caching
+ * allocator (a cudaMalloc beside it can fail once that allocator holds the
+ * free memory).  Its scratch (per-brick counts, scan tiles, totals;
+ * 524,832 bytes = 512.5 KiB) is one static device array that every GPU
+ * loading the library holds until exit; at most SMB_MC_NOALLOC_MAX_BRICKS
+ * bricks per call, more are rejected with SMB_ERR_ARG before any work.
  *   values:  (b+1)^3 floats per brick, as smb_batch_values returns them (the
  *            +-band samples are rewritten in place with the same values);
  *   records: SMB_REC_WORDS words per sub-block, as smb_batch_records;
  *   outputs: edge_off and tri_off (n_bricks + 1), edges (edges_cap),
  *            edge_vals (2 * edges_cap floats), tris (3 * tris_cap), encoded as
- *            smb_batch_mc; *n_edges and *n_tris get the totals (also when the
- *            buffers are too small: then SMB_ERR_MEMORY and nothing else is
- *            written).
- * All pointers but n_edges and n_tris are device pointers.  The first call
+ *            smb_batch_mc; *n_edges and *n_tris get the totals.
+ * When the totals exceed edges_cap / tris_cap (or reach 2^32, past the
+ * 32-bit offsets) the call returns SMB_ERR_MEMORY with the totals reported;
+ * by then it has written edge_off[0..n_bricks-1], tri_off[0..n_bricks-1]
+ * and the +-band samples of values, and nothing else.
+ * All pointers but n_edges and n_tris are device pointers.  The call runs
+ * on the resident's device stream and returns once its work there has
+ * finished; the caller's current device is left as it was.  The first call
  * on a device looks the scratch address up (cudaGetSymbolAddress); make it
- * before any stream capture.  Calls share the scratch: calls that overlap
- * on the GPU (other threads, other streams) race. */
+ * before any stream capture.  Calls share the scratch and it keeps the last
+ * call's contents: calls that overlap on the GPU (other threads, other
+ * streams) race. */
 #define SMB_MC_NOALLOC_MAX_BRICKS 65536
 int smb_mc_noalloc(const smb_resident* res, float* values, const uint32_t* records, size_t n_bricks,
                    uint32_t* edge_off, uint32_t* edges, float* edge_vals, size_t edges_cap, uint32_t* tri_off,

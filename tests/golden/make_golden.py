@@ -87,4 +87,9 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get("SESMESH_REFERENCE"):
+        main(os.environ["SESMESH_REFERENCE"])
+    else:
+        sys.exit("usage: make_golden.py REFERENCE_TREE (or set SESMESH_REFERENCE)")
