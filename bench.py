@@ -61,6 +61,8 @@ def args_():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-fast", action="store_true", help="skip the fast-mode (plain vs warm start) leg")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the shell2400k and batch512 blocks of the default line")
     return p.parse_args()
 
 
@@ -303,7 +305,9 @@ def run_ours(a):
                                                           "t_assemble", "t_measure", "t_total")}
     e2e_mean = max_over_ranks(float(np.mean(e2e_ms)) if e2e_ms else float("nan"))
     info = eng.batch_info()
-    h2d = int(info["resident_bytes"])
+    # Host to device: the sphere rows when the device builds the arrangement,
+    # else the uploaded arrangement (what the engine copied, counted by it).
+    h2d = int(st["upload_bytes"]) if out is not None else 0
     d2h = int(n_bricks * 16 + (n_bricks + 1) * 8 + st["vertices"] * 12 + st["triangles"] * 12)
     if w["refine"] == "fast":
         d2h += int(st["vertices"] * 24)  # per edge: t, feature, closest point, evaluations
@@ -337,13 +341,17 @@ def run_ours(a):
                                                  "t_assemble", "t_measure", "t_total")},
                 "mesh": {"vertices": st["vertices"], "triangles": st["triangles"], "area": st["area"],
                          "volume": st["volume"], "refine_evaluations": st["refine_evaluations"],
-                         "refine_cpu_edges": st["refine_cpu_edges"]}},
+                         "refine_cpu_edges": st["refine_cpu_edges"]},
+                "fallbacks": fallbacks(st)},
         "roofline": roof,
         "gpu_launches": int(launches),
         "clocks": clk,
     }
     if rank == 0 and world == 1 and not a.no_fast and w["refine"] == "exact":
         line["fast_mode"] = fast_leg(w, params, st, grid_points)
+    if rank == 0 and world == 1 and not a.no_configs and a.workload == "rings58800" and not a.spheres:
+        line["shell2400k"] = shell_leg(dev)
+        line["batch512"] = batch_leg(dev)
     if rank == 0 and world == 1 and not a.no_cpu:
         ceng, sample, spb_, k, nb = cpu_leg(w)
         t, _ = ceng.mesh_sample(sample)
@@ -423,6 +431,105 @@ def fast_leg(w, params, exact_stats, grid_points, reps=2):
     out["warm_vs_plain"] = {"e2e_speedup": p["e2e_ms_per_mesh"] / q["e2e_ms_per_mesh"],
                             "device_refine_speedup": p["device_refine_ms"] / max(q["device_refine_ms"], 1e-9),
                             "evaluations_saved": 1.0 - q["evaluations"] / max(1, p["evaluations"])}
+    return out
+
+
+def fallbacks(st):
+    """Work the device path handed to the host: the arrangement (1 built on
+    the device, 0 on the host below the device threshold, 2 the device
+    declined), meshes finished on the host, edges refined on the host."""
+    return {"arrangement_where": int(st["arrangement_where"]), "finished_on_host": int(st["finished_on_host"]),
+            "refine_cpu_edges": int(st["refine_cpu_edges"])}
+
+
+def shell_leg(dev, reps=2):
+    """The 2.4 M-sphere icosahedral shell at 1 A (60 x 40,000 spheres on a
+    380 A sphere), probe 1.4 A: exact and fast mode (plain f32 and the
+    learned warm start) end to end through compute_surface / the engine
+    (host sphere rows in, finished mesh in host memory out; wall clock,
+    first call a warm-up), and the device stage with the arrangement
+    resident (CUDA events, L2 flushed)."""
+    import torch
+    from sesmesh_b200 import native, warm_start
+    from sesmesh_b200 import surface as S
+    w = workload("shell2400k")
+    base = S.SurfaceParams.ses(w["probe"]).with_spacing(w["spacing"]).with_brick_size(w["brick"])
+    out = {"workload": describe(w)}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    for mode in ("exact", "fast", "fast+warm"):
+        p = base.with_refine("fast" if mode.startswith("fast") else "exact")
+        times, st = [], None
+        for r in range(reps + 1):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            eng = S.SurfaceEngine(w["spheres"], p)
+            if mode == "fast+warm":
+                eng.set_warm_start(native.Mlp(eng.dev, warm_start.load()))
+            mesh = eng.mesh()
+            torch.cuda.synchronize(dev)
+            ms = 1e3 * (time.perf_counter() - t0)
+            if r:
+                times.append(ms)
+            st = mesh.stats
+            if r == reps:
+                dev_ms = []
+                for _ in range(3):
+                    flush.zero_()
+                    torch.cuda.synchronize(dev)
+                    t = eng.run_device()
+                    dev_ms.append(eng.batch_info()["classify_ms"] + t["total"])
+            mesh.close()
+            eng.close()
+        gp = st["samples"]
+        e2e = float(np.mean(times))
+        out[mode] = {"e2e_ms_per_mesh": e2e, "e2e_Mgridpts_s": gp / (e2e / 1e3) / 1e6,
+                     "device_ms": float(np.median(dev_ms)), "device_Mgridpts_s": gp / (np.median(dev_ms) / 1e3) / 1e6,
+                     "stages_ms": {k: st[k] for k in ("t_geometry", "t_upload", "t_device", "t_assemble", "t_measure")},
+                     "vertices": int(st["vertices"]), "triangles": int(st["triangles"]),
+                     "refine_evaluations": int(st["refine_evaluations"]), "area": st["area"], "volume": st["volume"],
+                     "fallbacks": fallbacks(st)}
+    ex = out["exact"]
+    for mode in ("fast", "fast+warm"):
+        out[mode]["area_rel_vs_exact"] = abs(out[mode]["area"] - ex["area"]) / abs(ex["area"])
+        out[mode]["volume_rel_vs_exact"] = abs(out[mode]["volume"] - ex["volume"]) / abs(ex["volume"])
+    out["cpu_baseline"] = ("not run here: the oracle's single-threaded arrangement of 2.4 M spheres alone takes "
+                           "minutes; bench.py --workload shell2400k --impl reference times its mesh stage")
+    return out
+
+
+def batch_leg(dev, steps=2):
+    """The 512-structure batch (fast mode, learned warm start, autotuned):
+    structures/s over whole runs (wall clock; arrangements resident), p50/p99
+    per-structure latency, structures redone alone."""
+    import torch
+    from sesmesh_b200 import native, warm_start, workloads
+    from sesmesh_b200 import surface as S
+    items = workloads.batch512()
+    structs = [(it["spheres"], S.SurfaceParams.ses(it["probe"]).with_spacing(it["spacing"])) for it in items]
+    b = S.MultiBatch(structs)
+    b.set_warm_start(native.Mlp(b.dev, warm_start.load()))
+    cfg = b.tune()
+    b.run()
+    runs, lats = [], []
+    for _ in range(steps):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = b.run()
+        r["wall_ms"] = 1e3 * (time.perf_counter() - t0)
+        runs.append(r)
+        lats.append(b.latency())
+    wall = float(np.mean([r["wall_ms"] for r in runs]))
+    lat = np.concatenate(lats)
+    last = runs[-1]
+    out = {"workload": "batch512: 512 globules, atoms log-uniform 20-5000, probe U(1.2, 1.4), spacing in "
+                       "{0.1, 0.25, 0.5} A, fast mode + learned warm start",
+           "structures_per_s": len(items) / (wall / 1e3), "ms_per_batch": wall,
+           "grid_Mpts_s": last["samples"] / (wall / 1e3) / 1e6,
+           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+           "tuned": cfg, "groups": int(last["groups"]), "graph": bool(last["graph"]),
+           "redone": int(last["redone"]), "over_lists": int(last["over_lists"]), "over_memory": int(last["over_memory"]),
+           "once_ms": {"t_setup": last["t_setup"], "t_tune": last["t_tune"]}}
+    b.close()
     return out
 
 

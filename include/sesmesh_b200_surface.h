@@ -40,6 +40,15 @@ typedef struct {
     double t_geometry, t_upload, t_classify, t_substates, t_gather, t_sample, t_mc, t_device, t_d2h, t_host_refine,
         t_mesh_stage, t_assemble, t_measure, t_total;
     int host_threads;
+    /* Where the work ran.  arrangement_where: 1 the device built the
+     * arrangement, 0 the host did (input below the device threshold), 2 the
+     * device declined and the host built it.  finished_on_host: 1 when the
+     * device path was on but the mesh was finished on the host threads
+     * (smb_engine_note says why).  upload_bytes: bytes copied host to device
+     * for the arrangement (the sphere rows when the device builds it, else
+     * the uploaded arrangement). */
+    int arrangement_where, finished_on_host;
+    uint64_t upload_bytes;
 } smb_surface_stats;
 
 typedef struct smb_engine smb_engine;

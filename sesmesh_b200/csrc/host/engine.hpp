@@ -29,6 +29,8 @@ struct smb_engine {
     smb_resident* res = nullptr;
     smb_batch* batch = nullptr;
     double t_geometry = 0, t_upload = 0;
+    int arr_where = 0;          // smb_surface_stats::arrangement_where
+    uint64_t upload_bytes = 0;  // bytes copied host to device for the arrangement
     // Host copies of the last device run.
     std::vector<int32_t> keys;
     std::vector<uint32_t> edge_off, edges, tri_off, tris;

@@ -141,6 +141,7 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
         if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
     }
     e->arr_ready = !on_device;
+    e->arr_where = on_device ? 1 : (n >= g_device_arrangement_min ? 2 : 0);
     const Arrangement& A = e->arr;
     const double max_expanded = on_device ? e->darr.A.max_expanded : A.max_expanded;
     e->n_spheres = on_device ? e->darr.n : A.n;
@@ -201,6 +202,7 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
             return rc;
         smb::resident_set_exact_tmin(e->res, P.t_min);
         e->t_upload = ms_since(t1);
+        e->upload_bytes = uint64_t(n) * 32;
         *out = e.release();
         return SMB_OK;
     }
@@ -240,6 +242,7 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
                                 A.n_vertices(), P.t_min, err, errlen);
     if (rc != SMB_OK) return rc;
     e->t_upload = ms_since(t1);
+    e->upload_bytes = smb_resident_bytes(e->res);
     *out = e.release();
     return SMB_OK;
 }
@@ -391,6 +394,9 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
         st.t_device = e->t_classify + e->times.total;
         st.t_d2h = t_d2h;
         st.t_mesh_stage = ms_since(t_all) - st.t_assemble - st.t_measure;
+        st.arrangement_where = e->arr_where;
+        st.finished_on_host = e->exact_device && !e->note.empty();
+        st.upload_bytes = e->upload_bytes;
     };
     e->note.clear();
     if (e->exact_device && e->res->n_bricks) {

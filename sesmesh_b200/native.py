@@ -68,7 +68,8 @@ class SurfaceStats_(C.Structure):
     _fields_ = ([(f, C.c_size_t) for f in STAT_FIELDS] + [("area", C.c_double), ("volume", C.c_double),
                                                            ("euler", C.c_int64), ("refine_evaluations", C.c_uint64),
                                                            ("refine_cpu_edges", C.c_uint64)]
-                + [(f, C.c_double) for f in TIME_FIELDS] + [("host_threads", C.c_int)])
+                + [(f, C.c_double) for f in TIME_FIELDS] + [("host_threads", C.c_int)]
+                + [("arrangement_where", C.c_int), ("finished_on_host", C.c_int), ("upload_bytes", C.c_uint64)])
 
 
 class ArrangementInfo(C.Structure):

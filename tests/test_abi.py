@@ -34,8 +34,9 @@ def test_struct_layouts_match_the_header():
     prog = r'''
 #include <stdio.h>
 #include <stddef.h>
-#include "sesmesh_b200.h"
+#include "sesmesh_b200_surface.h"
 int main(void) {
+  printf("%zu %zu\n", sizeof(smb_surface_stats), offsetof(smb_surface_stats, upload_bytes));
   printf("%zu %zu %zu %zu %zu\n", sizeof(smb_grid_ref), sizeof(smb_arrangement_ref), sizeof(smb_lattice_ref),
          sizeof(smb_batch_times), sizeof(smb_device_info));
   printf("%zu %zu %zu\n", offsetof(smb_arrangement_ref, sphere_grid), offsetof(smb_arrangement_ref, probe),
@@ -49,7 +50,8 @@ int main(void) {
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
         out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
     got = [int(v) for v in out]
-    want = [C.sizeof(native.GridRef), C.sizeof(native.ArrangementRef), C.sizeof(native.LatticeRef),
+    want = [C.sizeof(native.SurfaceStats_), native.SurfaceStats_.upload_bytes.offset,
+            C.sizeof(native.GridRef), C.sizeof(native.ArrangementRef), C.sizeof(native.LatticeRef),
             C.sizeof(native.BatchTimes), C.sizeof(native.DeviceInfo),
             native.ArrangementRef.sphere_grid.offset, native.ArrangementRef.probe.offset,
             native.LatticeRef.band.offset]
