@@ -40,7 +40,8 @@ enum {
     SMB_ERR_RANGE = 5,     /* coordinates beyond the brick key range */
     SMB_ERR_MEMORY = 6,    /* allocation failed or a list exceeds a limit */
     SMB_ERR_STATE = 7,     /* call out of order (e.g. run before classify) */
-    SMB_ERR_TIMEOUT = 8    /* a bounded device wait gave up */
+    SMB_ERR_TIMEOUT = 8,   /* a bounded device wait gave up */
+    SMB_ERR_CANCELLED = 9  /* stopped by its cancel flag (Error::Cancelled, control.rs:114-121) */
 };
 
 typedef struct smb_device smb_device;
@@ -261,11 +262,13 @@ int smb_batch_info_get(const smb_batch* batch, smb_batch_info* out);
 int smb_batch_count_ops(smb_batch* batch, unsigned long long* ops, unsigned long long* samples, char* err,
                         size_t errlen);
 /* Learned warm start of fast mode (no counterpart in the reference; the
- * reference's fast mode starts every edge from the linear guess): an MLP
- * 32 -> 64 -> 64 -> 1 (GELU, sigmoid output t in [0, 1]) with BF16 weights
- * on the tensor cores and FP32 accumulation, proposing each crossing edge's
- * root parameter.  Parameters are SMB_MLP_NPARAM f32 values: W1 [64][32],
- * b1 [64], W2 [64][64], b2 [64], w3 [64], b3 (row-major, out x in). */
+ * reference's fast mode starts every edge from the linear guess,
+ * mesh/extract.rs:425-535 with field/gpu.rs:207-221): an MLP
+ * 32 -> 64 -> 64 -> 1 (GELU, sigmoid output in [0, 1]) with BF16 weights
+ * on the tensor cores and FP32 accumulation, proposing where each crossing
+ * edge's root search starts.  Parameters are SMB_MLP_NPARAM f32 values:
+ * W1 [64][32], b1 [64], W2 [64][64], b2 [64], w3 [64], b3 (row-major,
+ * out x in). */
 #define SMB_MLP_NPARAM 6337
 #define SMB_MLP_FEATURES 32
 typedef struct smb_mlp smb_mlp;
@@ -273,6 +276,13 @@ int smb_mlp_new(smb_device* dev, const float* params, smb_mlp** out, char* err, 
 void smb_mlp_free(smb_mlp* mlp);
 int smb_mlp_set_params(smb_mlp* mlp, const float* params, char* err, size_t errlen);
 int smb_mlp_get_params(const smb_mlp* mlp, float* params);
+/* How smb_refine_warm uses the output: SMB_MLP_GATE (default) starts an edge
+ * at t_c (below) where the output is >= 0.5 and at the linear guess
+ * elsewhere; SMB_MLP_ROOT starts it at the output itself, a root parameter
+ * in [0, 1] (parameters trained on the exact root). */
+#define SMB_MLP_GATE 0
+#define SMB_MLP_ROOT 1
+int smb_mlp_set_use(smb_mlp* mlp, int use);
 /* t[i] = MLP(x[32 i .. 32 i + 31]) for host arrays (tests, diagnostics). */
 int smb_mlp_forward(smb_mlp* mlp, const float* x, size_t n, float* t, char* err, size_t errlen);
 /* Loss (mean squared error of t, *loss) and its gradient over the
@@ -285,31 +295,45 @@ int smb_mlp_gradient(smb_mlp* mlp, const float* x, const float* target, size_t n
  * (ceil(n / batch) values) when non-null. */
 int smb_mlp_train_epoch(smb_mlp* mlp, const float* x, const float* target, size_t n, size_t batch, float lr,
                         float* losses, char* err, size_t errlen);
-/* smb_refine with each edge's starting point chosen by the MLP.  For the
- * sphere candidate whose contact sphere (radius R - probe) best explains the
- * edge's two samples, the kernel runs smb_refine's own iteration on that
- * sphere alone (no field evaluation): where the sphere is the surface's
- * nearest feature along the whole edge, that is where smb_refine would stop.
- * Where the MLP answers >= 0.5 the edge starts there, else at the linear
- * guess fa / (fa - fb) that smb_refine always takes (x:
- * smb_batch_edge_features).  The iteration that follows is smb_refine's,
+/* on = 1: the sampling pass of the batch's later runs also records every
+ * sampled point's nearest feature (the candidate that sets its value, in
+ * the smb_batch_edges feature encoding; the values are unchanged), which
+ * the warm start reads; on = 0 (default) skips it. */
+int smb_batch_record_features(smb_batch* batch, int on);
+/* The last run's nearest-feature words, (b+1)^3 per brick like
+ * smb_batch_values; meaningful at samples a sampled sub-block owns
+ * (SMB_ERR_STATE when the run did not record them). */
+int smb_batch_sample_features(const smb_batch* batch, uint32_t* out);
+/* smb_refine with each edge's starting point chosen by the MLP.  The
+ * sampler's nearest features at the edge's two samples name one candidate
+ * (a sphere, a circle or a SAS vertex); a feature pass runs smb_refine's
+ * own iteration (the same f32 operations) on that candidate alone, without
+ * evaluating the field: where the candidate is the surface's nearest
+ * feature at its iterates, that result t_c is where smb_refine would stop.
+ * The MLP, over each edge's features (smb_batch_edge_features), then gives
+ * the start (smb_mlp_set_use): t_c or the linear guess fa / (fa - fb) that
+ * smb_refine always takes.  The iteration that follows is smb_refine's,
  * with its bracket, tolerance, budgets and outputs: a start the field
  * judges within the tolerance is accepted after one evaluation, any other
- * start falls back to the bracketed refinement.  The MLP runs inside the
- * refinement kernel, 128 edges per tensor-core tile.  A null mlp is
- * smb_refine. */
+ * falls back to the bracketed refinement.  The last smb_run must have
+ * recorded the features (smb_batch_record_features; else SMB_ERR_STATE).
+ * A null mlp is smb_refine. */
 int smb_refine_warm(smb_resident* res, smb_batch* batch, const smb_mlp* mlp, double* ms, char* err, size_t errlen);
 /* The MLP's input for every crossing edge of the last run (32 f32 per edge,
  * marching-cubes edge order; zeros for edges the device does not refine)
- * and covered[k] = 1 where the device refines edge k (its sub-block was
- * sampled).  Features: fa / h, fb / h; finite-difference gradients of the
- * samples at both ends (6); the 4 sphere candidates whose contact spheres
- * best explain the two samples, centre offset from the edge midpoint and
- * contact radius, / 4 A (16); the mismatch of the first two,
- * log10(max(m, 1e-9)) / 9 + 1 (2); (t_c - t_lin) * 8 clamped to [-4, 4],
- * t_c the contact iteration's result and t_lin the linear guess; t_lin; h;
- * probe radius; both gradients along the edge scaled by h / (fb - fa),
- * clamped to [-10, 10].  Discards the last refinement. */
+ * and covered[k] = 1 where the device refines edge k.  With t_lin = fa /
+ * (fa - fb) and t_c as above: fa / h, fb / h; finite-difference gradients
+ * of the samples at both ends (6); t_lin; the candidate's kind, one-hot
+ * (sphere, circle, vertex: 3); both samples name the same feature; they
+ * name two different candidates; t_c's iteration converged; its steps / 8;
+ * (t_c - t_lin) * 8 clamped to [-4, 4]; t_c (t_lin where it did not
+ * converge); log10(max(m, 1e-9)) / 9 + 1 of its last |g| and of the
+ * candidate's mismatch at both samples (3); the candidate's centre (or
+ * position) less the edge midpoint / 4 A (3) and its radius / 4 A; h; the
+ * probe radius; both gradients along the edge times h / (fb - fa), clamped
+ * to [-10, 10] (2); |gradient| - 1 at both ends, clamped to [-4, 4] (2);
+ * the other sample's feature kind / 4.  The last run must have recorded
+ * the features.  Discards the last refinement. */
 int smb_batch_edge_features(smb_resident* res, smb_batch* batch, float* features, uint8_t* covered, char* err,
                             size_t errlen);
 

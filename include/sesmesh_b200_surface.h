@@ -49,7 +49,52 @@ typedef struct {
      * the uploaded arrangement). */
     int arrangement_where, finished_on_host;
     uint64_t upload_bytes;
+    /* The grid spacing meshed (the requested one unless the memory guard
+     * coarsened it) and the guard's estimate of the device bytes there. */
+    double spacing_used;
+    uint64_t device_bytes_estimate;
 } smb_surface_stats;
+
+/* Cooperative cancellation, progress and a device-memory guard for one
+ * computation: Control (crates/sesmesh/src/control.rs:54-131) and
+ * SurfaceParams::with_max_memory / with_auto_coarsen (surface.rs:226-236,
+ * 309-370; the guard, fit_memory, surface.rs:776-890, estimates host peak
+ * bytes; this one estimates the device stage's bytes).
+ *   cancel: when *cancel becomes nonzero the computation returns
+ *     SMB_ERR_CANCELLED promptly: it is polled per sphere while the host
+ *     builds the arrangement, and between device passes and host stages.
+ *   progress: called with (stage, 0, total) when a stage starts and
+ *     (stage, total, total) when it ends (total = surface bricks for
+ *     SMB_STAGE_MESH, 1 otherwise; structures for a batch's mesh stage),
+ *     from the calling thread.
+ *   max_device_bytes: with a nonzero limit, after classification the
+ *     device stage's bytes are estimated from the surface bricks
+ *     (smb_device_bytes_estimate) plus the resident arrangement; above the
+ *     limit the call returns SMB_ERR_MEMORY before any mesh-stage buffer is
+ *     taken, or, with auto_coarsen (smb_compute_surface_with only), meshes
+ *     at the smallest spacing up to 10 A whose estimate fits
+ *     (stats.spacing_used). */
+enum {
+    SMB_STAGE_GEOMETRY = 0,
+    SMB_STAGE_CLASSIFY = 1,
+    SMB_STAGE_MESH = 2,
+    SMB_STAGE_ASSEMBLE = 3,
+    SMB_STAGE_MEASURE = 4
+};
+typedef void (*smb_progress_fn)(void* user, int stage, uint64_t done, uint64_t total);
+typedef struct {
+    const volatile int32_t* cancel;
+    smb_progress_fn progress;
+    void* user;
+    uint64_t max_device_bytes;
+    int auto_coarsen;
+} smb_control;
+/* Device bytes of the mesh stage for this many surface bricks of this edge
+ * at this spacing and probe (values, records, candidate lists,
+ * marching-cubes and refinement outputs, exact-mode vertices and the device
+ * finish; conservative). */
+uint64_t smb_device_bytes_estimate(size_t surface_bricks, uint32_t brick, double spacing, double probe_radius,
+                                   int refine);
 
 typedef struct smb_engine smb_engine;
 typedef struct smb_surface smb_surface;
@@ -57,10 +102,22 @@ typedef struct smb_surface smb_surface;
 /* compute_surface (surface.rs:599): spheres as n rows (x, y, z, r). */
 int smb_compute_surface(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p,
                         smb_surface** out, char* err, size_t errlen);
+/* compute_surface_with (surface.rs:614-631) with a control (may be null). */
+int smb_compute_surface_with(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p,
+                             const smb_control* control, smb_surface** out, char* err, size_t errlen);
 /* SurfaceEngine-style reuse: arrangement and upload once, then meshes. */
 int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out,
                    char* err, size_t errlen);
 void smb_engine_free(smb_engine* e);
+/* smb_engine_new under a control (its cancel flag and progress cover the
+ * arrangement); the engine keeps the control for its later calls. */
+int smb_engine_new_with(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p,
+                        const smb_control* control, smb_engine** out, char* err, size_t errlen);
+/* Replaces the engine's control (null: none). */
+int smb_engine_set_control(smb_engine* e, const smb_control* control);
+/* Device bytes the engine holds now: the resident arrangement, the batch's
+ * buffers and the measure's tables (what the memory guard estimates). */
+uint64_t smb_engine_device_bytes(const smb_engine* e);
 int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size_t errlen);
 size_t smb_engine_bricks(const smb_engine* e);
 int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen);
@@ -167,6 +224,11 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
 int smb_multi_set_device_finish(smb_multi* m, int on);
 smb_surface* smb_multi_surface(smb_multi* m, size_t i);
 int smb_multi_latency(const smb_multi* m, double* ms);
+/* A batch's control: the cancel flag is polled between groups and between
+ * structures' host stages (SMB_ERR_CANCELLED); progress reports the mesh
+ * stage in structures finished.  The memory fields are not used (the batch
+ * sizes its groups to a third of the free device memory). */
+int smb_multi_set_control(smb_multi* m, const smb_control* control);
 
 /* The host arrangement of an engine (views valid while it lives; an
  * arrangement built on the device is copied to the host on first use).
@@ -188,6 +250,10 @@ int smb_engine_arrangement(const smb_engine* e, smb_arrangement_info* out);
 /* Builds only the host arrangement (no device; smb_engine_arrangement). */
 int smb_arrangement_build(const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out, char* err,
                           size_t errlen);
+/* The same under a control (cancel flag polled per sphere, geometry
+ * progress). */
+int smb_arrangement_build_with(const double* xyzr, size_t n, const smb_surface_params* p,
+                               const smb_control* control, smb_engine** out, char* err, size_t errlen);
 
 #ifdef __cplusplus
 }

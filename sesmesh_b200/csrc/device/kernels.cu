@@ -20,6 +20,10 @@
 
 namespace smb {
 
+// Feature words (the reference's DeviceEdges encoding, field/gpu.rs:155-179):
+// kind << 29 | id.
+constexpr uint32_t FEAT_SHIFT_D = 29;
+
 // ---------------------------------------------------------------------------
 // Arithmetic self-test: IEEE f32 and f64 operations whose results the host
 // recomputes; a build with contracted multiply-adds or approximate division
@@ -651,12 +655,17 @@ constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;     // bounded wait
 
 // list (single structure): blocks whose packed block exceeds limit_units
 // append their index to list (list[0] = count) and return; LIST: block b
-// samples the list's b-th entry (none past the count).
-template <bool TMA, bool COUNT, bool MANY, bool LIST = false>
+// samples the list's b-th entry (none past the count).  FEAT: each owned
+// sample's nearest feature also goes to feats (same layout as values), in
+// the refinement's encoding kind << 29 | id (0 solvent, 1 beyond, 2 sphere,
+// 3 circle, 4 SAS vertex; ids of the structure's arrangement): the candidate
+// that set the sample's least distance, the first of equal ones.  Values are
+// the same with and without it.
+template <bool TMA, bool COUNT, bool MANY, bool LIST = false, bool FEAT = false>
 __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work,
                                                 const uint32_t* rec, const uint4* pack, float* values,
                                                 unsigned long long* counters, Scene SC, uint32_t limit_units,
-                                                uint32_t* list) {
+                                                uint32_t* list, const uint32_t* ids, uint32_t* feats) {
     extern __shared__ __align__(16) uint4 sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t sts[8];
@@ -736,13 +745,20 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
             inside |= (dx * dx + dy * dy + dz * dz) < a.w;
         }
         float value = probe;
+        uint32_t fk = 0, fi = 0;  // FEAT: kind and list position of the nearest feature
         if (inside) {
             if (COUNT) ops += 9ull * nv + 2;
             float best2 = cutoff2;
+            fk = 1;
             for (int v = 0; v < nv; v++) {
                 float4 q = V[v];
                 float dx = px - q.x, dy = py - q.y, dz = pz - q.z;
-                best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                if (FEAT) {
+                    if (d2 < best2) best2 = d2, fk = 4, fi = uint32_t(v);
+                } else {
+                    best2 = fminf(best2, d2);
+                }
             }
             for (int si = 0; si < ns; si++) {
                 const float kk = s_key[si];
@@ -767,7 +783,10 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
                         break;
                     }
                 }
-                if (valid) best2 = lb2;
+                if (valid) {
+                    best2 = lb2;
+                    if (FEAT) fk = 2, fi = uint32_t(si);
+                }
             }
             for (int ci = 0; ci < nc; ci++) {
                 const float kk = c_key[ci];
@@ -797,11 +816,24 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
                         break;
                     }
                 }
-                if (valid) best2 = d2;
+                if (valid) {
+                    best2 = d2;
+                    if (FEAT) fk = 3, fi = uint32_t(ci);
+                }
             }
             value = probe - sqrtf(best2);
         }
         out[(z * side + y) * side + x] = value;
+        if (FEAT) {
+            // List position to the arrangement's id: the sub-block's id words
+            // are near, S, S offsets, S blockers, C, C offsets, C blockers, V.
+            const uint32_t* l = ids + R[R_IDS];
+            uint32_t id = 0;
+            if (fk == 2) id = l[nn + fi];
+            else if (fk == 3) id = l[nn + 2 * ns + 1 + nsb + fi];
+            else if (fk == 4) id = l[nn + 2 * ns + 1 + nsb + 2 * nc + 1 + R[R_CBLK] + fi];
+            feats[size_t(brick) * L.spb + (z * side + y) * side + x] = (fk << FEAT_SHIFT_D) | id;
+        }
     }
     if (COUNT) {
         atomicAdd(&counters[CNT_OPS], ops);
@@ -947,128 +979,6 @@ struct RefOut {
     uint32_t* evals;
 };
 
-constexpr uint32_t FEAT_SHIFT_D = 29;
-
-// The refinement iteration of k_refine (Newton with the Illinois bracket,
-// MAX_ITER steps) run on one atom's contact sphere alone, F(x) = |x - c| - r:
-// where that sphere is the surface's nearest feature along the whole edge,
-// this is the iteration k_refine itself would run, so its result is where
-// the reference's fast mode would stop.  No field evaluation.
-__device__ __forceinline__ float contact_iteration(float ax, float ay, float az, int axis, float h, float hd,
-                                                   float4 c, float r, float fa, float fb, const RefineConsts& RC) {
-    float t = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
-    float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
-    int side = 0;
-    for (uint32_t it = 0; it < RC.max_iter; it++) {
-        float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f),
-              z = az + (axis == 2 ? hd * t : 0.0f);
-        float dx = x - c.x, dy = y - c.y, dz = z - c.z;
-        float len = sqrtf(dx * dx + dy * dy + dz * dz);
-        float gv = len - r;
-        if (fabsf(gv) <= RC.tol) break;
-        if ((gv < 0.0f) == (g0 < 0.0f)) {
-            t0 = t, g0 = gv;
-            if (side == -1) g1 *= 0.5f;
-            side = -1;
-        } else {
-            t1 = t, g1 = gv;
-            if (side == 1) g0 *= 0.5f;
-            side = 1;
-        }
-        float slope = len > 1e-12f ? ((axis == 0 ? dx : (axis == 1 ? dy : dz)) / len) * h : 0.0f;
-        float newton = t - gv / slope;
-        if (fabsf(slope) > 1e-3f * hd && newton > t0 && newton < t1) {
-            t = newton;
-        } else {
-            float s = (t0 * g1 - t1 * g0) / (g1 - g0);
-            t = (isfinite(s) && s > t0 && s < t1) ? s : 0.5f * (t0 + t1);
-        }
-    }
-    return t;
-}
-
-// Sphere candidates scanned for the features: the first of the sub-block's
-// S list, which is sorted by the candidate's value at the sub-block centre.
-constexpr int FEATURE_SCAN = 32;
-
-// Features of one crossing edge for the warm-start MLP (32 values):
-//   0-1   fa / h, fb / h (sample values at the ends)
-//   2-7   finite-difference gradients of the sampled field at both ends
-//         (central where both neighbours are in the brick, else one-sided)
-//   8-23  the 4 class-S candidates (of the first FEATURE_SCAN) whose contact
-//         spheres (radius r = R - probe) best explain the two end samples (smallest
-//         mismatch max(| |a - c| - r - fa |, | |b - c| - r - fb |)):
-//         centre minus edge midpoint / 4 A, and r / 4 A (zeros when fewer)
-//   24-25 the mismatch of the first two, log10(max(m, 1e-9)) / 9 + 1
-//   26    (t_c - t_lin) * 8 clamped to [-4, 4]: t_c the contact iteration
-//         on the first candidate's sphere (contact_iteration)
-//   27    t_lin = fa / (fa - fb) (the linear guess)
-//   28-29 spacing h and probe radius (A)
-//   30-31 the gradients' components along the edge times h / (fb - fa),
-//         clamped to [-10, 10]
-// Returns t_c (t_lin without candidates), in f32 at full precision.
-__device__ __forceinline__ float edge_features(const float* val, int b, float h, float hd, float probe, int ex, int ey,
-                                               int ez, float ax, float ay, float az, int axis, float fa, float fb,
-                                               const float4* S, int ns, const RefineConsts& RC, float* f) {
-    const int side = b + 1;
-    auto V = [&](int x, int y, int z) { return val[(z * side + y) * side + x]; };
-    auto grad = [&](int x, int y, int z, float* g) {
-        int c[3] = {x, y, z};
-        for (int d = 0; d < 3; d++) {
-            int lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
-            lo[d]--, hi[d]++;
-            if (lo[d] >= 0 && hi[d] <= b) g[d] = (V(hi[0], hi[1], hi[2]) - V(lo[0], lo[1], lo[2])) / (2.0f * h);
-            else if (hi[d] <= b) g[d] = (V(hi[0], hi[1], hi[2]) - V(x, y, z)) / h;
-            else g[d] = (V(x, y, z) - V(lo[0], lo[1], lo[2])) / h;
-        }
-    };
-    const float t_lin = fa / (fa - fb);
-    f[0] = fa / h, f[1] = fb / h;
-    grad(ex, ey, ez, f + 2);
-    grad(ex + (axis == 0), ey + (axis == 1), ez + (axis == 2), f + 5);
-    const float mx = (float(ex) + (axis == 0 ? 0.5f : 0.0f)) * h, my = (float(ey) + (axis == 1 ? 0.5f : 0.0f)) * h,
-                mz = (float(ez) + (axis == 2 ? 0.5f : 0.0f)) * h;
-    const float bx = ax + (axis == 0 ? hd : 0.0f), by = ay + (axis == 1 ? hd : 0.0f), bz = az + (axis == 2 ? hd : 0.0f);
-    float bd[4] = {3.4e38f, 3.4e38f, 3.4e38f, 3.4e38f};
-    int bi[4] = {-1, -1, -1, -1};
-    for (int i = 0; i < min(ns, FEATURE_SCAN); i++) {
-        float4 c = S[i];
-        const float r = c.w - probe;
-        float dx = ax - c.x, dy = ay - c.y, dz = az - c.z;
-        float ea = fabsf(sqrtf(dx * dx + dy * dy + dz * dz) - r - fa);
-        dx = bx - c.x, dy = by - c.y, dz = bz - c.z;
-        float eb = fabsf(sqrtf(dx * dx + dy * dy + dz * dz) - r - fb);
-        float d = fmaxf(ea, eb);
-        if (d < bd[3]) {
-            int q = 3;
-            while (q > 0 && d < bd[q - 1]) bd[q] = bd[q - 1], bi[q] = bi[q - 1], q--;
-            bd[q] = d, bi[q] = i;
-        }
-    }
-    for (int q = 0; q < 4; q++) {
-        if (bi[q] >= 0) {
-            float4 c = S[bi[q]];
-            f[8 + 4 * q] = (c.x - mx) * 0.25f, f[9 + 4 * q] = (c.y - my) * 0.25f, f[10 + 4 * q] = (c.z - mz) * 0.25f;
-            f[11 + 4 * q] = (c.w - probe) * 0.25f;
-        } else {
-            f[8 + 4 * q] = f[9 + 4 * q] = f[10 + 4 * q] = f[11 + 4 * q] = 0.0f;
-        }
-    }
-    f[24] = bi[0] >= 0 ? log10f(fmaxf(bd[0], 1e-9f)) / 9.0f + 1.0f : 1.0f;
-    f[25] = bi[1] >= 0 ? log10f(fmaxf(bd[1], 1e-9f)) / 9.0f + 1.0f : 1.0f;
-    float t_c = t_lin;
-    if (bi[0] >= 0) {
-        float4 c = S[bi[0]];
-        t_c = contact_iteration(ax, ay, az, axis, h, hd, c, c.w - probe, fa, fb, RC);
-    }
-    f[26] = fminf(fmaxf(t_c - t_lin, -0.5f), 0.5f) * 8.0f;
-    f[27] = t_lin;
-    f[28] = h, f[29] = probe;
-    const float inv = h / (fb - fa);
-    f[30] = fminf(fmaxf(f[2 + axis] * inv, -10.0f), 10.0f);
-    f[31] = fminf(fmaxf(f[5 + axis] * inv, -10.0f), 10.0f);
-    return t_c;
-}
 
 // Sub-block edge lists for refinement: per work item (a sampled sub-block;
 // without flags unless any_flags: the f32 refinement stages the sampler's
@@ -1412,10 +1322,15 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
 // The f32 root search of one crossing edge (extract.rs:425-535 iteration:
 // Newton with the Illinois bracket for MAX_ITER evaluations, then
 // bisection), from t_start; writes edge k's outputs.
+// expect (the warm start's candidate, 0 for none): the first evaluation is
+// at t_start and is accepted only within the tolerance and on that
+// candidate; otherwise the iteration starts over from the linear guess, as
+// from t_start = t_lin with expect = 0 (the reference's fast mode).
 template <int RG>
 __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const RefineConsts& RC, float probe, float band,
                                                 float ax, float ay, float az, uint32_t axis, float fa, float fb,
-                                                float t_start, uint32_t k, const RefOut& out, int gl, uint32_t gm) {
+                                                float t_start, uint32_t expect, uint32_t k, const RefOut& out, int gl,
+                                                uint32_t gm) {
     const float h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
     float t = t_start;
     float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
@@ -1424,7 +1339,16 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
     uint32_t evals = 0;
     Eval last;
     last.feat = 1u << FEAT_SHIFT_D, last.qx = last.qy = last.qz = 0.0f, last.value = 0.0f;
-    for (uint32_t it = 0; it < RC.max_iter; it++) {
+    if (expect) {
+        const float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f),
+                    z = az + (axis == 2 ? hd * t : 0.0f);
+        const Eval e = eval_f32<RG>(st, probe, band, x, y, z, gl, gm);
+        evals++;
+        last = e;
+        if (fabsf(e.value) <= RC.tol && e.feat == expect) converged = true;
+        else t = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
+    }
+    for (uint32_t it = 0; it < RC.max_iter && !converged; it++) {
         float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
         Eval e = eval_f32<RG>(st, probe, band, x, y, z, gl, gm);
         evals++;
@@ -1478,68 +1402,384 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
     out.evals[k] = evals | (converged ? 0x80000000u : 0u);
 }
 
+// ---------------------------------------------------------------------------
+// Learned warm start of the f32 refinement.  Per listed edge (row e of the
+// items' edge lists): the nearest feature the sampler recorded at the edge's
+// two samples (k_sample<.., FEAT>) names one candidate, a sphere, a circle or
+// a SAS vertex of the structure; refine_edge_f32's own iteration (its Newton
+// / Illinois steps, the same f32 operations) run on that candidate alone
+// gives t_c with no field evaluation.  Where the candidate is the surface's
+// nearest feature at the iterates, t_c is where the refinement would stop.
+// The edge's features then go through the MLP (k_mlp_forward), whose output
+// picks each edge's start: t_c or the linear guess (or, with the root head,
+// is the start itself).  The refinement (k_refine<REFINE_WARM>) is the plain
+// one from those starts: a start the field judges within the tolerance is
+// accepted after one evaluation, any other falls back to the bracketed
+// iteration.
+
+// One candidate in the refinement's brick-local f32 form (stage_candidates):
+// S a = (x, y, z, R); C a = (centre, radius), b = (axis, e1.x), c = (e1.y,
+// e1.z, -, -); V a = (x, y, z, -).
+struct WarmCand {
+    float4 a, b, c;
+    uint32_t kind;
+};
+
+__device__ __forceinline__ WarmCand warm_cand(const DArr& A, const DLat& L, const BrickFrame& F, uint32_t word) {
+    WarmCand w;
+    w.kind = word >> FEAT_SHIFT_D;
+    const uint32_t id = word & ((1u << FEAT_SHIFT_D) - 1);
+    w.a = w.b = w.c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    // A word outside the arrangement's tables (none the sampler writes) is
+    // no candidate.
+    if ((w.kind == 2 && id >= A.n) || (w.kind == 3 && id >= A.nc) || (w.kind == 4 && id >= A.nv)) w.kind = 1;
+    float x, y, z;
+    if (w.kind == 2) {
+        const double4 c = A.sph[id];
+        to_local(L, F, c.x, c.y, c.z, x, y, z);
+        w.a = make_float4(x, y, z, float(c.w));
+    } else if (w.kind == 3) {
+        const double* c = A.circ + 12 * size_t(id);
+        to_local(L, F, c[0], c[1], c[2], x, y, z);
+        w.a = make_float4(x, y, z, float(c[9]));
+        w.b = make_float4(float(c[3]), float(c[4]), float(c[5]), float(c[6]));
+        w.c = make_float4(float(c[7]), float(c[8]), 0.0f, 0.0f);
+    } else if (w.kind == 4) {
+        const double4 p = A.vert[id];
+        to_local(L, F, p.x, p.y, p.z, x, y, z);
+        w.a = make_float4(x, y, z, 0.0f);
+    } else {
+        w.kind = 1;
+    }
+    return w;
+}
+
+// The candidate's part of eval_f32 at (x, y, z): probe less its distance
+// when that is below probe + band (found), else -band; q its closest point.
+// The inside test and the blockers are not applied: the field judges the
+// result.
+__device__ __forceinline__ float cand_eval(const WarmCand& w, float probe, float band, float x, float y, float z,
+                                           float& qx, float& qy, float& qz, bool& found) {
+    float best = probe + band;
+    found = false;
+    qx = x, qy = y, qz = z;
+    if (w.kind == 2) {
+        const float dx = x - w.a.x, dy = y - w.a.y, dz = z - w.a.z;
+        const float len = sqrtf(dx * dx + dy * dy + dz * dz);
+        const float lb = fabsf(len - w.a.w);
+        if (!(lb >= best || len < 1e-12f)) {
+            const float sc = w.a.w / len;
+            qx = w.a.x + dx * sc, qy = w.a.y + dy * sc, qz = w.a.z + dz * sc;
+            best = lb, found = true;
+        }
+    } else if (w.kind == 3) {
+        const float4 m = w.a, u = w.b;
+        const float yx = x - m.x, yy = y - m.y, yz = z - m.z;
+        const float along = yx * u.x + yy * u.y + yz * u.z;
+        const float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
+        const float wl = sqrtf(wx * wx + wy * wy + wz * wz);
+        const float tt = wl - m.w;
+        const float dist = sqrtf(along * along + tt * tt);
+        if (!(dist >= best)) {
+            if (wl > 1e-12f) {
+                qx = m.x + (wx / wl) * m.w, qy = m.y + (wy / wl) * m.w, qz = m.z + (wz / wl) * m.w;
+            } else {
+                qx = m.x + u.w * m.w, qy = m.y + w.c.x * m.w, qz = m.z + w.c.y * m.w;
+            }
+            best = dist, found = true;
+        }
+    } else if (w.kind == 4) {
+        const float dx = x - w.a.x, dy = y - w.a.y, dz = z - w.a.z;
+        const float v = sqrtf(dx * dx + dy * dy + dz * dz);
+        if (v < best) qx = w.a.x, qy = w.a.y, qz = w.a.z, best = v, found = true;
+    }
+    return probe - best;
+}
+
+// refine_edge_f32's Newton / Illinois steps on the candidate alone (no
+// bisection): t_c where |g| <= tol within MAX_ITER steps (*conv), the
+// steps taken and the last |g|.
+__device__ __forceinline__ float cand_iteration(const WarmCand& w, const RefineConsts& RC, float probe, float band,
+                                                float ax, float ay, float az, uint32_t axis, float fa, float fb,
+                                                int* iters, float* last_g, bool* conv) {
+    const float h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
+    float t = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
+    float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
+    int side_ = 0, it = 0;
+    *conv = false;
+    float gv = fa;
+    for (; it < int(RC.max_iter); it++) {
+        const float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f),
+                    z = az + (axis == 2 ? hd * t : 0.0f);
+        float qx, qy, qz;
+        bool found;
+        gv = cand_eval(w, probe, band, x, y, z, qx, qy, qz, found);
+        if (fabsf(gv) <= RC.tol) {
+            *conv = true;
+            it++;
+            break;
+        }
+        if ((gv < 0.0f) == (g0 < 0.0f)) {
+            t0 = t, g0 = gv;
+            if (side_ == -1) g1 *= 0.5f;
+            side_ = -1;
+        } else {
+            t1 = t, g1 = gv;
+            if (side_ == 1) g0 *= 0.5f;
+            side_ = 1;
+        }
+        float slope = 0.0f;
+        if (found) {
+            const float wx = qx - x, wy = qy - y, wz = qz - z;
+            const float len = sqrtf(wx * wx + wy * wy + wz * wz);
+            if (len > 1e-12f) slope = ((axis == 0 ? wx : (axis == 1 ? wy : wz)) / len) * h;
+        }
+        const float newton = t - gv / slope;
+        if (fabsf(slope) > 1e-3f * hd && newton > t0 && newton < t1) {
+            t = newton;
+        } else {
+            const float sv = (t0 * g1 - t1 * g0) / (g1 - g0);
+            t = (isfinite(sv) && sv > t0 && sv < t1) ? sv : 0.5f * (t0 + t1);
+        }
+    }
+    *iters = it;
+    *last_g = fabsf(gv);
+    return t;
+}
+
+__device__ __forceinline__ float log_mismatch(float m) { return log10f(fmaxf(m, 1e-9f)) / 9.0f + 1.0f; }
+__device__ __forceinline__ float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+
+// Features of row e (SMB_MLP_FEATURES = 32 f32):
+//   0-1   fa / h, fb / h
+//   2-7   finite-difference gradients of the samples at both ends (central
+//         inside the brick, else one-sided)
+//   8     t_lin = fa / (fa - fb)
+//   9-11  the candidate's kind, one-hot (sphere, circle, SAS vertex; zeros
+//         without one)
+//   12    1 where both samples name the same feature
+//   13    1 where they name two different candidates
+//   14    1 where the candidate's iteration converged
+//   15    its steps / 8
+//   16    (t_c - t_lin) * 8, clamped to [-4, 4]
+//   17    t_c (t_lin without a converged candidate)
+//   18    log10(max(m, 1e-9)) / 9 + 1 of its last |g|
+//   19-20 the same of the candidate's mismatch at the two samples,
+//         |g(end) - f(end)|
+//   21-23 the candidate's centre (sphere, circle) or position (vertex)
+//         less the edge midpoint, / 4 A
+//   24    its size / 4 A: the atom radius R - probe (sphere), the circle's
+//         radius, 0 (vertex)
+//   25-26 spacing h and probe radius (A)
+//   27-28 both gradients along the edge times h / (fb - fa), clamped to
+//         [-10, 10]
+//   29-30 |gradient| - 1 at both ends, clamped to [-4, 4]
+//   31    the other sample's feature kind / 4
+// starts[e] = (t_c, or -1 without a converged candidate; t_lin).
+// Row e's features into f and its starts (t_c or -1, t_lin); *cand gets the
+// candidate's feature word (0 without one).
+template <bool MANY>
+__device__ __forceinline__ float2 warm_row(const DArr& A0, const DLat& L0, const RefineConsts& RC0, const int4* keys,
+                                           const uint32_t* work, uint32_t n_items, const uint32_t* rec,
+                                           const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off,
+                                           const uint32_t* item_edges, const float* values, const uint32_t* feats,
+                                           const Scene& S, uint32_t e, float* f, uint32_t* cand) {
+    uint32_t lo = 0, hi = n_items;  // the item holding row e: item_off[lo] <= e < item_off[lo + 1]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (item_off[mid] <= e) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t brick = work[lo] >> 3;
+    const int4 key = keys[brick];
+    const DArr& A = MANY ? S.arr[key.w] : A0;
+    const DLat& L = MANY ? S.lat[key.w] : L0;
+    const RefineConsts& RC = MANY ? S.rc[key.w] : RC0;
+    const uint32_t k = item_edges[e];
+    const int b = L.b, side = b + 1;
+    const float h = RC.h_hi, hd = RC.h_hi + RC.h_lo, probe = L.probe32, band = L.band32;
+    const uint32_t code = edges[k], cell = code / 3, axis = code % 3;
+    const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
+    const float ax = float(ex) * h + float(ex) * RC.h_lo, ay = float(ey) * h + float(ey) * RC.h_lo,
+                az = float(ez) * h + float(ez) * RC.h_lo;
+    const float2 fv = edge_vals[k];
+    const float fa = fv.x, fb = fv.y;
+    const float t_lin = fminf(fmaxf(fa / (fa - fb), 0.0f), 1.0f);
+    const float* val = values + size_t(brick) * L.spb;
+    uint32_t st[8];
+    for (int q = 0; q < 8; q++) st[q] = rec[(size_t(brick) * 8 + q) * REC_WORDS + R_STATE];
+    // The recorded feature of a sample its sampled, unflagged owner wrote.
+    auto word = [&](int x, int y, int z) -> uint32_t {
+        bool positive;
+        const int o = sample_owner(x, y, z, L.sub, st, &positive);
+        if (o < 0 || rec[(size_t(brick) * 8 + o) * REC_WORDS + R_FLAGS] != 0) return 1u << FEAT_SHIFT_D;
+        return feats[size_t(brick) * L.spb + (z * side + y) * side + x];
+    };
+    const int bx = ex + (axis == 0), by = ey + (axis == 1), bz = ez + (axis == 2);
+    const uint32_t wa = word(ex, ey, ez), wb = word(bx, by, bz);
+    const uint32_t ka = wa >> FEAT_SHIFT_D, kb = wb >> FEAT_SHIFT_D;
+    const uint32_t primary = ka >= 2 ? wa : (kb >= 2 ? wb : (1u << FEAT_SHIFT_D));
+    const BrickFrame F = brick_frame(L, RC, key);
+    const WarmCand w = warm_cand(A, L, F, primary);
+    *cand = w.kind >= 2 ? primary : 0u;
+    auto V = [&](int x, int y, int z) { return val[(z * side + y) * side + x]; };
+    auto grad = [&](int x, int y, int z, float* g) {
+        const int c[3] = {x, y, z};
+        for (int d = 0; d < 3; d++) {
+            int lo3[3] = {c[0], c[1], c[2]}, hi3[3] = {c[0], c[1], c[2]};
+            lo3[d]--, hi3[d]++;
+            if (lo3[d] >= 0 && hi3[d] <= b) g[d] = (V(hi3[0], hi3[1], hi3[2]) - V(lo3[0], lo3[1], lo3[2])) / (2.0f * h);
+            else if (hi3[d] <= b) g[d] = (V(hi3[0], hi3[1], hi3[2]) - V(x, y, z)) / h;
+            else g[d] = (V(x, y, z) - V(lo3[0], lo3[1], lo3[2])) / h;
+        }
+    };
+    f[0] = fa / h, f[1] = fb / h;
+    grad(ex, ey, ez, f + 2);
+    grad(bx, by, bz, f + 5);
+    f[8] = t_lin;
+    f[9] = w.kind == 2, f[10] = w.kind == 3, f[11] = w.kind == 4;
+    f[12] = wa == wb;
+    f[13] = ka >= 2 && kb >= 2 && wa != wb;
+    float t_c = -1.0f;
+    if (w.kind >= 2) {
+        int iters = 0;
+        float last_g = 0.0f;
+        bool conv = false;
+        const float tc = cand_iteration(w, RC, probe, band, ax, ay, az, axis, fa, fb, &iters, &last_g, &conv);
+        if (conv) t_c = tc;
+        f[14] = conv, f[15] = float(iters) * 0.125f;
+        f[16] = clampf(tc - t_lin, -0.5f, 0.5f) * 8.0f;
+        f[17] = conv ? tc : t_lin;
+        f[18] = log_mismatch(last_g);
+        float qx, qy, qz;
+        bool found;
+        const float bxf = ax + (axis == 0 ? hd : 0.0f), byf = ay + (axis == 1 ? hd : 0.0f),
+                    bzf = az + (axis == 2 ? hd : 0.0f);
+        f[19] = log_mismatch(fabsf(cand_eval(w, probe, band, ax, ay, az, qx, qy, qz, found) - fa));
+        f[20] = log_mismatch(fabsf(cand_eval(w, probe, band, bxf, byf, bzf, qx, qy, qz, found) - fb));
+        const float mx = ax + (axis == 0 ? 0.5f * hd : 0.0f), my = ay + (axis == 1 ? 0.5f * hd : 0.0f),
+                    mz = az + (axis == 2 ? 0.5f * hd : 0.0f);
+        f[21] = (w.a.x - mx) * 0.25f, f[22] = (w.a.y - my) * 0.25f, f[23] = (w.a.z - mz) * 0.25f;
+        f[24] = (w.kind == 2 ? w.a.w - probe : (w.kind == 3 ? w.a.w : 0.0f)) * 0.25f;
+    } else {
+        f[14] = 0.0f, f[15] = 0.0f, f[16] = 0.0f, f[17] = t_lin, f[18] = 1.0f, f[19] = 1.0f, f[20] = 1.0f;
+        f[21] = f[22] = f[23] = f[24] = 0.0f;
+    }
+    f[25] = h, f[26] = probe;
+    const float inv = h / (fb - fa);
+    f[27] = clampf(f[2 + axis] * inv, -10.0f, 10.0f);
+    f[28] = clampf(f[5 + axis] * inv, -10.0f, 10.0f);
+    f[29] = clampf(sqrtf(f[2] * f[2] + f[3] * f[3] + f[4] * f[4]) - 1.0f, -4.0f, 4.0f);
+    f[30] = clampf(sqrtf(f[5] * f[5] + f[6] * f[6] + f[7] * f[7]) - 1.0f, -4.0f, 4.0f);
+    f[31] = float(primary == wa ? kb : ka) * 0.25f;
+    return make_float2(t_c, t_lin);
+}
+
+// Features of every row (export for training: smb_batch_edge_features).
+template <bool MANY>
+__global__ void __launch_bounds__(256) k_warm_features(DArr A0, DLat L0, RefineConsts RC0, const int4* keys,
+                                                       const uint32_t* work, uint32_t n_host, const uint32_t* rec,
+                                                       const uint32_t* edges, const float2* edge_vals,
+                                                       const uint32_t* item_off, const uint32_t* item_edges,
+                                                       const float* values, const uint32_t* feats, float* x_out,
+                                                       Scene S) {
+    const uint32_t n_items = MANY ? uint32_t(*S.n_work) : n_host;
+    const uint32_t E = item_off[n_items];
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        float f[MLP_IN];
+        uint32_t cand;
+        warm_row<MANY>(A0, L0, RC0, keys, work, n_items, rec, edges, edge_vals, item_off, item_edges, values, feats, S,
+                       e, f, &cand);
+        float4* xo = reinterpret_cast<float4*>(x_out + size_t(e) * MLP_IN);
+        for (int c = 0; c < MLP_IN / 4; c++) xo[c] = make_float4(f[4 * c], f[4 * c + 1], f[4 * c + 2], f[4 * c + 3]);
+    }
+}
+
+// The warm start's choice per row, features and MLP fused: a persistent CTA
+// of 128 threads per 128-row tile at a time (thread r computes row r's
+// features into the tile, one tensor-core forward pass per tile, weights
+// and TMEM set up once per CTA).  start[e] = (t_c, the candidate's feature
+// word) where the gate answers >= 0.5 and the candidate's iteration
+// converged, else (t_lin, 0) (use 0); or (the output itself, a root
+// parameter in [0, 1], 0) (use 1).  The word travels as float bits.
+template <bool MANY>
+__global__ void __launch_bounds__(128) k_warm_starts(DArr A0, DLat L0, RefineConsts RC0, const int4* keys,
+                                                     const uint32_t* work, uint32_t n_host, const uint32_t* rec,
+                                                     const uint32_t* edges, const float2* edge_vals,
+                                                     const uint32_t* item_off, const uint32_t* item_edges,
+                                                     const float* values, const uint32_t* feats, MlpDev P, int use,
+                                                     float2* start, unsigned long long* counters, Scene S) {
+    const uint32_t n_items = MANY ? uint32_t(*S.n_work) : n_host;
+    const uint32_t E = item_off[n_items];
+    const uint32_t tiles = (E + MLP_ROWS - 1) / MLP_ROWS;
+    if (blockIdx.x >= tiles) return;  // the whole CTA, before any TMEM is taken
+    extern __shared__ __align__(128) unsigned char wsm[];
+    MlpSmem& M = *reinterpret_cast<MlpSmem*>(wsm);
+    mlp_setup(M, P);
+    uint32_t phase = 0;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t e = tile * MLP_ROWS + threadIdx.x;
+        float f[MLP_IN];
+        float2 sc = make_float2(-1.0f, 0.0f);
+        uint32_t cand = 0;
+        if (e < E) {
+            sc = warm_row<MANY>(A0, L0, RC0, keys, work, n_items, rec, edges, edge_vals, item_off, item_edges, values,
+                                feats, S, e, f, &cand);
+        } else {
+            for (int c = 0; c < MLP_IN; c++) f[c] = 0.0f;
+        }
+        mlp_put_row(M, f);
+        float p = 0.0f;
+        const bool ok = mlp_forward(M, phase, &p, nullptr, nullptr, nullptr);
+        if (!ok && threadIdx.x == 0) atomicAdd(&counters[CNT_TIMEOUT], 1ull);
+        if (e < E) {
+            float2 w = make_float2(sc.y, 0.0f);
+            if (ok && use == 1) w.x = p;
+            else if (ok && p >= 0.5f && sc.x >= 0.0f) w = make_float2(sc.x, __uint_as_float(cand));
+            start[e] = w;
+        }
+    }
+    mlp_teardown(M);
+}
+
 // Fast-mode refinement over the work items' edge lists (k_item_edges).
 // Work is claimed from a queue (counters[CNT_QUEUE]) by persistent CTAs:
-//   REFINE_PLAIN:  each warp claims items and refines the item's edges from
-//                  the linear guess (the reference's fast mode), a group
-//                  of RG lanes per edge, candidates staged in the warp's
-//                  shared region;
-//   REFINE_MLP:    each CTA claims REFINE_BATCH quads of REFINE_WARPS items.
-//                  Phase A: the batch's edges, packed densely in 128-row
-//                  tiles (thread r holds row r), get their features and one
-//                  tensor-core MLP pass per tile gives each its start.
-//                  Phase B: the warps refine the batch's items as PLAIN from
-//                  those starts.  Weights and TMEM are set up once per CTA;
-//                  the tiles share bytes with the candidate staging;
-//   EDGE_FEATURES: the features alone, to feat_out (evals[k] = 1 marks the
-//                  edges covered).
-// WIDE: candidates too large for a region per warp; the CTA refines one
-// item at a time with all its threads.
+// each warp claims items and refines the item's edges, a group of RG lanes
+// per edge, candidates staged in the warp's shared region; REFINE_PLAIN
+// starts each edge at the linear guess (the reference's fast mode),
+// REFINE_WARM at start[e] (row e of the edge lists: the warm start's
+// choice).  WIDE: candidates too large for a region per warp; the CTA
+// refines one item at a time with all its threads.
 constexpr int REFINE_WARPS = 4;
 // Warps of a block in the plain pass over the listed sub-blocks (those over
 // a warp's region): the block's warps take one sub-block's edges.
 #ifndef WIDE_LIST_WARPS
 #define WIDE_LIST_WARPS 16
 #endif
-// Most quads a CTA claims at once: phase A for all of them, then phase B
-// with the warps claiming the batch's items one by one (a barrier per batch,
-// not per quad, so warps with quick items do not wait for slow ones).  Small
-// runs claim fewer, so that every CTA gets several claims.
-constexpr uint32_t REFINE_BATCH = 8;
 
 struct RefinePlan {
-    uint32_t batch;       // quads per claim, 1..REFINE_BATCH
     uint32_t cand_bytes;  // one staging region
-    uint32_t stage_off;   // first staging region (after the MLP's weights)
-    uint32_t first_off;   // phase A: first S candidates, REFINE_WARPS x REFINE_BATCH x FEATURE_SCAN float4
 };
 
 template <int MODE, bool WIDE, bool MANY, int RG, int NT = 32 * REFINE_WARPS>
 __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
     DArr A0, DLat L0, RefineConsts RC0, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
     const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
-    uint32_t n_host, RefOut out, const float* values, MlpDev mlp, float* feat_out, RefinePlan P,
-    unsigned long long* counters, Scene S, uint32_t* ovf, const uint32_t* list) {
+    uint32_t n_host, RefOut out, const float2* start, RefinePlan P, unsigned long long* counters, Scene S,
+    uint32_t* ovf, const uint32_t* list) {
     const uint32_t n_items = MANY ? uint32_t(*S.n_work) : n_host;
     extern __shared__ __align__(128) float4 rs[];
-    __shared__ uint32_t sh_q, sh_next, sh_edge, sh_wedge[REFINE_WARPS];
-    __shared__ uint32_t sh_off[REFINE_WARPS * REFINE_BATCH + 1], sh_sbase[REFINE_WARPS * REFINE_BATCH],
-        sh_brick[REFINE_WARPS * REFINE_BATCH];
-    __shared__ int sh_ns[REFINE_WARPS * REFINE_BATCH];
+    __shared__ uint32_t sh_q, sh_edge, sh_wedge[REFINE_WARPS];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* smem = reinterpret_cast<unsigned char*>(rs);
-    MlpSmem* M = reinterpret_cast<MlpSmem*>(smem);
-    float4* first_s = reinterpret_cast<float4*>(smem + P.first_off);  // per batch item, FEATURE_SCAN each
-    unsigned char* mine = smem + P.stage_off + (WIDE ? 0 : size_t(warp) * P.cand_bytes);
+    unsigned char* mine = reinterpret_cast<unsigned char*>(rs) + (WIDE ? 0 : size_t(warp) * P.cand_bytes);
     unsigned int* queue = reinterpret_cast<unsigned int*>(&counters[CNT_QUEUE]);
-    const uint32_t n_quads = (n_items + REFINE_WARPS - 1) / REFINE_WARPS;
-    auto edge_geom = [&](const DLat& L, const RefineConsts& RC, uint32_t k, uint32_t& axis, int& ex, int& ey, int& ez,
-                         float& ax, float& ay, float& az) {
+    auto edge_geom = [&](const DLat& L, const RefineConsts& RC, uint32_t k, uint32_t& axis, float& ax, float& ay,
+                         float& az) {
         const int b = L.b;
         const float h = RC.h_hi;
         const uint32_t code = edges[k], cell = code / 3;
         axis = code % 3;
-        ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
+        const int ex = int(cell % b), ey = int((cell / b) % b), ez = int(cell / (b * b));
         ax = float(ex) * h + float(ex) * RC.h_lo, ay = float(ey) * h + float(ey) * RC.h_lo,
         az = float(ez) * h + float(ez) * RC.h_lo;
     };
@@ -1585,12 +1825,16 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
         auto edge = [&](uint32_t e) {
             const uint32_t k = item_edges[e];
             uint32_t axis;
-            int ex, ey, ez;
             float ax, ay, az;
-            edge_geom(L, RC, k, axis, ex, ey, ez, ax, ay, az);
+            edge_geom(L, RC, k, axis, ax, ay, az);
             const float2 fv = edge_vals[k];
-            const float t0 = MODE == REFINE_MLP ? out.t[k] : fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
-            refine_edge_f32<RG>(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, k, out, int(gl), gm);
+            float t0 = fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
+            uint32_t expect = 0;
+            if (MODE == REFINE_WARM) {
+                const float2 w = start[e];
+                t0 = w.x, expect = __float_as_uint(w.y);
+            }
+            refine_edge_f32<RG>(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, expect, k, out, int(gl), gm);
         };
         if (WIDE || RG < 32) {
             // The block's (warp's) groups claim the edges one at a time
@@ -1608,7 +1852,7 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
             for (uint32_t e = a0 + lane / RG; e < a1; e += step) edge(e);
         }
     };
-    if constexpr (MODE == REFINE_PLAIN && WIDE) {
+    if constexpr (WIDE) {
         if (list) {
             // The sub-blocks the per-warp pass listed, one per block at a time.
             const uint32_t n = *list;
@@ -1622,8 +1866,17 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
             }
             return;
         }
-    }
-    if constexpr (MODE == REFINE_PLAIN && !WIDE) {
+        // Items in queue order, one per block at a time.
+        for (;;) {
+            __syncthreads();
+            if (threadIdx.x == 0) sh_q = atomicAdd(queue, 1u);
+            __syncthreads();
+            const uint32_t q = sh_q;
+            if (q >= n_items) break;
+            refine_item(q);
+        }
+        return;
+    } else {
         for (;;) {
             uint32_t i = 0;
             if (lane == 0) i = atomicAdd(queue, 1u);
@@ -1631,109 +1884,7 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
             if (i >= n_items) break;
             refine_item(i);
         }
-        return;
     }
-    if (MODE == REFINE_MLP) mlp_setup(*M, mlp, 64);
-    uint32_t phase = 0;
-    for (;;) {
-        __syncthreads();  // sh_q, sh_next and the shared regions are free again
-        if (threadIdx.x == 0) sh_q = atomicAdd(queue, P.batch), sh_next = 0;
-        __syncthreads();
-        const uint32_t q0 = sh_q;
-        if (q0 >= n_quads) break;
-        const uint32_t q1 = min(q0 + P.batch, n_quads);
-        // Phase A: the batch's edges, densely packed in 128-row tiles,
-        // through the features and the MLP.  First each item's first S
-        // candidates, frame and offsets into shared memory.
-        const uint32_t i0 = q0 * REFINE_WARPS, i1 = min(q1 * REFINE_WARPS, n_items), ni = i1 - i0;
-        if (MODE != REFINE_PLAIN) {
-            if (threadIdx.x <= ni) sh_off[threadIdx.x] = item_off[i0 + threadIdx.x];
-            if (threadIdx.x < ni) {
-                const uint32_t j = work[i0 + threadIdx.x];
-                const uint32_t* R = rec + size_t(j) * REC_WORDS;
-                sh_ns[threadIdx.x] = min(int(R[R_S]), FEATURE_SCAN);
-                sh_sbase[threadIdx.x] = R[R_IDS] + R[R_NEAR];
-                sh_brick[threadIdx.x] = j >> 3;
-            }
-            __syncthreads();
-            for (uint32_t x = threadIdx.x; x < ni * FEATURE_SCAN; x += blockDim.x) {
-                const uint32_t it = x / FEATURE_SCAN, c = x % FEATURE_SCAN;
-                if (int(c) >= sh_ns[it] || sh_off[it] == sh_off[it + 1]) continue;
-                const int4 key = keys[sh_brick[it]];
-                const DArr& A = MANY ? S.arr[key.w] : A0;
-                const DLat& L = MANY ? S.lat[key.w] : L0;
-                const RefineConsts& RC = MANY ? S.rc[key.w] : RC0;
-                const BrickFrame F = brick_frame(L, RC, key);
-                double4 sp = A.sph[ids[sh_sbase[it] + c]];
-                float lx, ly, lz;
-                to_local(L, F, sp.x, sp.y, sp.z, lx, ly, lz);
-                first_s[x] = make_float4(lx, ly, lz, float(sp.w));
-            }
-            __syncthreads();
-            const uint32_t E0 = sh_off[0], E1 = sh_off[ni];
-            for (uint32_t c0 = E0; c0 < E1; c0 += blockDim.x) {
-                const uint32_t e = c0 + threadIdx.x;
-                const bool have = e < E1;
-                float f[MLP_IN];
-                for (int c = 0; c < MLP_IN; c++) f[c] = 0.0f;
-                float t_c = 0.0f, t_lin = 0.0f;
-                uint32_t k = 0;
-                if (have) {
-                    uint32_t lo = 0, hi = ni;  // the item holding edge e: sh_off[lo] <= e < sh_off[lo + 1]
-                    while (hi - lo > 1) {
-                        const uint32_t mid = (lo + hi) >> 1;
-                        if (sh_off[mid] <= e) lo = mid;
-                        else hi = mid;
-                    }
-                    k = item_edges[e];
-                    const int st = keys[sh_brick[lo]].w;
-                    const DLat& L = MANY ? S.lat[st] : L0;
-                    const RefineConsts& RC = MANY ? S.rc[st] : RC0;
-                    uint32_t axis;
-                    int ex, ey, ez;
-                    float ax, ay, az;
-                    edge_geom(L, RC, k, axis, ex, ey, ez, ax, ay, az);
-                    const float2 fv = edge_vals[k];
-                    t_c = edge_features(values + size_t(sh_brick[lo]) * L.spb, L.b, RC.h_hi, RC.h_hi + RC.h_lo,
-                                        L.probe32, ex, ey, ez, ax, ay, az, int(axis), fv.x, fv.y,
-                                        first_s + lo * FEATURE_SCAN, sh_ns[lo], RC, f);
-                    t_lin = fminf(fmaxf(fv.x / (fv.x - fv.y), 0.0f), 1.0f);
-                }
-                if (MODE == EDGE_FEATURES) {
-                    if (have) {
-                        for (int c = 0; c < MLP_IN; c++) feat_out[size_t(k) * MLP_IN + c] = f[c];
-                        out.evals[k] = 1;
-                    }
-                    continue;
-                }
-                mlp_put_row(*M, f);
-                float tm = 0.0f;
-                const bool ok = mlp_forward(*M, phase, &tm, nullptr, nullptr, nullptr, 0);
-                if (!ok && threadIdx.x == 0) atomicAdd(&counters[CNT_TIMEOUT], 1ull);
-                // The MLP chooses the start: the contact iteration's result
-                // where it answers >= 0.5 (and that is within half an edge
-                // of the linear guess), else the linear guess.
-                if (have) out.t[k] = (ok && tm >= 0.5f && fabsf(f[26]) < 4.0f) ? t_c : t_lin;
-            }
-            __syncthreads();  // the tiles' bytes become staging regions
-        }
-        if (MODE == EDGE_FEATURES) continue;
-        // Phase B: the batch's items, claimed one at a time by the warps
-        // (WIDE: taken in order by the whole block).  The starts written
-        // above are this block's.
-        if (WIDE) {
-            for (uint32_t i = i0; i < i1; i++) refine_item(i);
-        } else {
-            for (;;) {
-                uint32_t i = 0;
-                if (lane == 0) i = i0 + atomicAdd(&sh_next, 1u);
-                i = __shfl_sync(0xffffffffu, i, 0);
-                if (i >= i1) break;
-                refine_item(i);
-            }
-        }
-    }
-    if (MODE == REFINE_MLP) mlp_teardown(*M, 64);
 }
 
 // ---------------------------------------------------------------------------
@@ -1815,10 +1966,15 @@ cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const 
 
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
-                          bool count, cudaStream_t s, const Scene* many, uint32_t* list, size_t small) {
+                          bool count, cudaStream_t s, const Scene* many, uint32_t* list, size_t small,
+                          const uint32_t* ids, uint32_t* feats) {
     if (!n) return cudaSuccess;
     size_t smem = size_t(max_units) * 16;
-    auto kern = many ? k_sample<true, false, true>
+    const bool feat = feats != nullptr && !count;
+    auto kern = feat ? (many ? k_sample<true, false, true, false, true>
+                             : (tma ? k_sample<true, false, false, false, true>
+                                    : k_sample<false, false, false, false, true>))
+                     : many ? k_sample<true, false, true>
                      : (count ? k_sample<true, true, false>
                               : (tma ? k_sample<true, false, false> : k_sample<false, false, false>));
     // Shared memory for the largest block on every CTA can leave an SM a
@@ -1831,13 +1987,13 @@ cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work,
     if (split && (e = cudaMemsetAsync(list, 0, 4, s)) != cudaSuccess) return e;
     COUNT(1);
     kern<<<n, 128, first, s>>>(L, keys, work, n, rec, pack, values, counters, many ? *many : Scene{},
-                               uint32_t(first / 16), split ? list : nullptr);
+                               uint32_t(first / 16), split ? list : nullptr, ids, feats);
     if (!split) return cudaGetLastError();
-    auto rest = k_sample<true, false, false, true>;
+    auto rest = feat ? k_sample<true, false, false, true, true> : k_sample<true, false, false, true>;
     if ((e = cudaFuncSetAttribute(rest, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))) != cudaSuccess)
         return e;
     COUNT(1);
-    rest<<<n, 128, smem, s>>>(L, keys, work, n, rec, pack, values, counters, Scene{}, 0, list);
+    rest<<<n, 128, smem, s>>>(L, keys, work, n, rec, pack, values, counters, Scene{}, 0, list, ids, feats);
     return cudaGetLastError();
 }
 
@@ -1894,88 +2050,108 @@ void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const ui
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
                           const uint32_t* rec, const uint32_t* ids, const uint32_t* edges, const float2* edge_vals,
                           const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
-                          uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float* values,
-                          const MlpDev* mlp, float* feat_out, unsigned long long* counters, int sms,
-                          size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many, uint32_t* ovf,
-                          size_t region, int group) {
+                          uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float2* start,
+                          unsigned long long* counters, int sms, size_t smem_limit, cudaStream_t s, size_t* smem_out,
+                          const Scene* many, uint32_t* ovf, size_t region, int group) {
     auto al = [](size_t v) { return (v + 127) / 128 * 128; };
     RefinePlan P;
     P.cand_bytes = uint32_t(al(cand_bytes));
-    // MLP: weights (kept) then tiles and the first S candidates (per tile),
-    // the latter two in bytes the staging regions reuse.
-    const size_t keep = mode == REFINE_MLP ? al(offsetof(MlpSmem, x)) : 0;
-    const size_t tiles = mode == REFINE_MLP ? al(sizeof(MlpSmem) - offsetof(MlpSmem, x)) : 0;
-    P.stage_off = uint32_t(keep);
-    P.first_off = uint32_t(keep + tiles);
-    const size_t phase_a = mode == REFINE_PLAIN ? 0 : tiles + size_t(REFINE_WARPS) * REFINE_BATCH * FEATURE_SCAN * 16;
-    const size_t narrow = keep + std::max(phase_a, size_t(REFINE_WARPS) * P.cand_bytes);
-    const size_t wide = keep + std::max(phase_a, size_t(P.cand_bytes));
+    const size_t narrow = size_t(REFINE_WARPS) * P.cand_bytes;
+    const size_t wide = P.cand_bytes;
     // One staging region per warp (an item per warp in flight, as many items
     // per SM as regions fit) while four fit in a block, else one per block.
-    // The plain single-structure pass instead keeps per-warp regions of the
-    // size asked for (default: two blocks of four to an SM) and hands the
+    // The single-structure pass instead keeps per-warp regions of the size
+    // asked for (default: two blocks of four to an SM) and hands the
     // sub-blocks that outgrow them to a whole-block pass over a list.
     const bool use_wide = narrow > smem_limit;
     size_t small = region ? region / 128 * 128 : (smem_limit / 2 - 1024) / REFINE_WARPS / 128 * 128;
     small = std::max<size_t>(std::min(small, size_t(P.cand_bytes)), 128);
-    const bool split = mode == REFINE_PLAIN && !many && ovf && (use_wide || small < P.cand_bytes);
+    const bool split = !many && ovf && (use_wide || small < P.cand_bytes);
     const size_t smem = use_wide ? wide : narrow;
     if (smem_out) *smem_out = smem;
     if (!n_items) return cudaSuccess;
-    MlpDev md = mlp ? *mlp : MlpDev{nullptr, nullptr, nullptr};
     // Launches kern with `bytes` of shared memory on as many CTAs as stay
-    // resident (the plain kernel of that width sets the occupancy; the TMEM
-    // columns cap the MLP kernel).
-    auto run = [&](auto kern, auto occ, const RefinePlan& PL, size_t bytes, uint32_t* o, const uint32_t* list,
-                   uint32_t units, int threads = 32 * REFINE_WARPS) -> cudaError_t {
+    // resident.
+    auto run = [&](auto kern, const RefinePlan& PL, size_t bytes, uint32_t* o, const uint32_t* list, uint32_t units,
+                   int threads = 32 * REFINE_WARPS) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(occ, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-        if (e != cudaSuccess) return e;
         int per_sm = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, occ, threads, bytes);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, bytes);
         if (e != cudaSuccess) return e;
-        if (mode == REFINE_MLP) per_sm = std::min(per_sm, 8);  // 64 TMEM columns per CTA of the SM's 512
         const uint32_t grid = std::min<uint32_t>(units, uint32_t(std::max(1, sms * std::max(per_sm, 1))));
-        RefinePlan Q = PL;
-        Q.batch = std::max<uint32_t>(1, std::min<uint32_t>(REFINE_BATCH, units / (4 * grid)));
         cudaMemsetAsync(&counters[CNT_QUEUE], 0, sizeof(unsigned long long), s);
         COUNT(1);
-        kern<<<grid, threads, bytes, s>>>(A, L, RC, keys, work, rec, ids, edges, edge_vals, item_off,
-                                                     item_edges, n_items, RefOut{t, feat, q, evals}, values, md,
-                                                     feat_out, Q, counters, many ? *many : Scene{}, o, list);
+        kern<<<grid, threads, bytes, s>>>(A, L, RC, keys, work, rec, ids, edges, edge_vals, item_off, item_edges,
+                                          n_items, RefOut{t, feat, q, evals}, start, PL, counters,
+                                          many ? *many : Scene{}, o, list);
         return cudaGetLastError();
     };
     const uint32_t quads = (n_items + REFINE_WARPS - 1) / REFINE_WARPS;
-    const bool g32 = group == 32;
+    const bool g32 = group == 32, warm = mode == REFINE_WARM;
     if (split) {
         RefinePlan PS = P;
         PS.cand_bytes = uint32_t(small);
         cudaError_t e = cudaMemsetAsync(ovf, 0, 4, s);
         if (e != cudaSuccess) return e;
-        auto kn = g32 ? k_refine<REFINE_PLAIN, false, false, 32> : k_refine<REFINE_PLAIN, false, false, 8>;
+        auto kn = warm ? (g32 ? k_refine<REFINE_WARM, false, false, 32> : k_refine<REFINE_WARM, false, false, 8>)
+                       : (g32 ? k_refine<REFINE_PLAIN, false, false, 32> : k_refine<REFINE_PLAIN, false, false, 8>);
         // The list pass: WIDE_LIST_WARPS warps share each sub-block's lists.
-        auto kw = g32 ? k_refine<REFINE_PLAIN, true, false, 32, 32 * WIDE_LIST_WARPS>
-                      : k_refine<REFINE_PLAIN, true, false, 8, 32 * WIDE_LIST_WARPS>;
-        e = run(kn, kn, PS, size_t(REFINE_WARPS) * small, ovf, nullptr, quads);
+        auto kw = warm ? (g32 ? k_refine<REFINE_WARM, true, false, 32, 32 * WIDE_LIST_WARPS>
+                              : k_refine<REFINE_WARM, true, false, 8, 32 * WIDE_LIST_WARPS>)
+                       : (g32 ? k_refine<REFINE_PLAIN, true, false, 32, 32 * WIDE_LIST_WARPS>
+                              : k_refine<REFINE_PLAIN, true, false, 8, 32 * WIDE_LIST_WARPS>);
+        e = run(kn, PS, size_t(REFINE_WARPS) * small, ovf, nullptr, quads);
         if (e != cudaSuccess) return e;
-        return run(kw, kw, P, wide, nullptr, ovf, n_items, 32 * WIDE_LIST_WARPS);
+        return run(kw, P, wide, nullptr, ovf, n_items, 32 * WIDE_LIST_WARPS);
     }
     // Groups of lanes per edge: one lane in the many-structure pass (short
     // lists, few evaluations after the warm start), else 8 or 32 as asked.
     auto pick = [&](auto narrow_k, auto wide_k) { return use_wide ? wide_k : narrow_k; };
     auto kern =
-        many ? (mode == REFINE_MLP ? pick(k_refine<REFINE_MLP, false, true, 1>, k_refine<REFINE_MLP, true, true, 1>)
-                                   : pick(k_refine<REFINE_PLAIN, false, true, 1>, k_refine<REFINE_PLAIN, true, true, 1>))
-        : mode == REFINE_MLP
-            ? (g32 ? pick(k_refine<REFINE_MLP, false, false, 32>, k_refine<REFINE_MLP, true, false, 32>)
-                   : pick(k_refine<REFINE_MLP, false, false, 8>, k_refine<REFINE_MLP, true, false, 8>))
-        : mode == EDGE_FEATURES
-            ? pick(k_refine<EDGE_FEATURES, false, false, 8>, k_refine<EDGE_FEATURES, true, false, 8>)
-            : (g32 ? pick(k_refine<REFINE_PLAIN, false, false, 32>, k_refine<REFINE_PLAIN, true, false, 32>)
-                   : pick(k_refine<REFINE_PLAIN, false, false, 8>, k_refine<REFINE_PLAIN, true, false, 8>));
-    auto occ = use_wide ? k_refine<REFINE_PLAIN, true, false, 8> : k_refine<REFINE_PLAIN, false, false, 8>;
-    return run(kern, occ, P, smem, nullptr, nullptr, quads);
+        many ? (warm ? pick(k_refine<REFINE_WARM, false, true, 1>, k_refine<REFINE_WARM, true, true, 1>)
+                     : pick(k_refine<REFINE_PLAIN, false, true, 1>, k_refine<REFINE_PLAIN, true, true, 1>))
+        : warm ? (g32 ? pick(k_refine<REFINE_WARM, false, false, 32>, k_refine<REFINE_WARM, true, false, 32>)
+                      : pick(k_refine<REFINE_WARM, false, false, 8>, k_refine<REFINE_WARM, true, false, 8>))
+               : (g32 ? pick(k_refine<REFINE_PLAIN, false, false, 32>, k_refine<REFINE_PLAIN, true, false, 32>)
+                      : pick(k_refine<REFINE_PLAIN, false, false, 8>, k_refine<REFINE_PLAIN, true, false, 8>));
+    return run(kern, P, smem, nullptr, nullptr, use_wide ? n_items : quads);
+}
+
+void launch_warm_features(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
+                          uint32_t n_items, const uint32_t* rec, const uint32_t* edges, const float2* edge_vals,
+                          const uint32_t* item_off, const uint32_t* item_edges, const float* values,
+                          const uint32_t* feats, float* x_out, size_t max_rows, int sms, cudaStream_t s,
+                          const Scene* many) {
+    if (!many && !n_items) return;
+    const uint32_t grid = uint32_t(std::max<size_t>(1, std::min<size_t>((max_rows + 255) / 256, size_t(sms) * 16)));
+    COUNT(1);
+    if (many)
+        k_warm_features<true><<<grid, 256, 0, s>>>(A, L, RC, keys, work, n_items, rec, edges, edge_vals, item_off,
+                                                   item_edges, values, feats, x_out, *many);
+    else
+        k_warm_features<false><<<grid, 256, 0, s>>>(A, L, RC, keys, work, n_items, rec, edges, edge_vals, item_off,
+                                                    item_edges, values, feats, x_out, Scene{});
+}
+
+cudaError_t launch_warm_starts(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys,
+                               const uint32_t* work, uint32_t n_items, const uint32_t* rec, const uint32_t* edges,
+                               const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
+                               const float* values, const uint32_t* feats, const MlpDev& P, int use, float2* start,
+                               unsigned long long* counters, size_t max_rows, int sms, cudaStream_t s,
+                               const Scene* many) {
+    if ((!many && !n_items) || !max_rows) return cudaSuccess;
+    const size_t smem = sizeof(MlpSmem) + 128;
+    auto kern = many ? k_warm_starts<true> : k_warm_starts<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    if (e != cudaSuccess) return e;
+    // Four CTAs per SM: 128 TMEM columns each of the SM's 512.
+    const size_t tiles = (max_rows + MLP_ROWS - 1) / MLP_ROWS;
+    const uint32_t grid = uint32_t(std::max<size_t>(1, std::min<size_t>(tiles, size_t(sms) * 4)));
+    COUNT(1);
+    kern<<<grid, MLP_ROWS, smem, s>>>(A, L, RC, keys, work, n_items, rec, edges, edge_vals, item_off, item_edges,
+                                      values, feats, P, use, start, counters, many ? *many : Scene{});
+    return cudaGetLastError();
 }
 
 }  // namespace smb

@@ -72,8 +72,7 @@ struct Scene {
 };
 
 size_t refine_smem_bytes(uint32_t nn, uint32_t ns, uint32_t nc, uint32_t nv, uint32_t nsb, uint32_t ncb);
-enum : int { REFINE_PLAIN = 0, REFINE_MLP = 1, EDGE_FEATURES = 2 };
-struct MlpDev;
+enum : int { REFINE_PLAIN = 0, REFINE_WARM = 1 };
 // Per refinable work item, its edge list (counts, exclusive offsets with the
 // total at item_off[n], edge indices); the largest count goes to
 // counters[CNT_MAXITEM].  With a mask, only the edges k with mask[k] != 0.
@@ -86,8 +85,10 @@ void launch_item_edges(const DLat& L, const uint32_t* work, uint32_t n, const ui
                        const uint8_t* mask = nullptr, bool all_items = false);
 void launch_put_total(uint32_t* dst, const unsigned long long* total, cudaStream_t s);
 void launch_copy_count(unsigned long long* dst, const unsigned long long* src, cudaStream_t s);
-// Persistent refinement (or feature pass) over the items' edge lists; grid
-// = SMs x resident CTAs.  *smem_out gets the shared memory it needs (also
+// Persistent refinement over the items' edge lists, each edge started at the
+// linear guess (REFINE_PLAIN) or as start[e], row e of the lists, says
+// (REFINE_WARM: the start and the candidate its first evaluation must name
+// to be accepted, as float bits, 0 for none); grid = SMs x resident CTAs.  *smem_out gets the shared memory it needs (also
 // when it does not launch, for n_items = 0).  With ovf (n_items + 1 words)
 // the plain single-structure pass runs per-warp regions of `region` bytes
 // (0: an eighth of smem_limit, two blocks to an SM) where four regions for the largest sub-block
@@ -97,10 +98,27 @@ void launch_copy_count(unsigned long long* dst, const unsigned long long* src, c
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
                           const uint32_t* rec, const uint32_t* ids, const uint32_t* edges, const float2* edge_vals,
                           const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
-                          uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float* values,
-                          const MlpDev* mlp, float* feat_out, unsigned long long* counters, int sms,
-                          size_t smem_limit, cudaStream_t s, size_t* smem_out, const Scene* many = nullptr,
-                          uint32_t* ovf = nullptr, size_t region = 0, int group = 8);
+                          uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float2* start,
+                          unsigned long long* counters, int sms, size_t smem_limit, cudaStream_t s, size_t* smem_out,
+                          const Scene* many = nullptr, uint32_t* ovf = nullptr, size_t region = 0, int group = 8);
+// The warm start's features of every row of the items' edge lists (32 f32
+// per row into x_out); feats: the sampler's nearest-feature words
+// (launch_sample with feats).  Grid-strided over at most max_rows rows (the
+// many-structure pass reads its item count on the device).
+void launch_warm_features(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
+                          uint32_t n_items, const uint32_t* rec, const uint32_t* edges, const float2* edge_vals,
+                          const uint32_t* item_off, const uint32_t* item_edges, const float* values,
+                          const uint32_t* feats, float* x_out, size_t max_rows, int sms, cudaStream_t s,
+                          const Scene* many = nullptr);
+// The warm start's start per row (features and the MLP in one kernel, the
+// tensor cores for the MLP): start[e] for the REFINE_WARM refinement.
+struct MlpDev;
+cudaError_t launch_warm_starts(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys,
+                               const uint32_t* work, uint32_t n_items, const uint32_t* rec, const uint32_t* edges,
+                               const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
+                               const float* values, const uint32_t* feats, const MlpDev& P, int use, float2* start,
+                               unsigned long long* counters, size_t max_rows, int sms, cudaStream_t s,
+                               const Scene* many = nullptr);
 
 unsigned long long kernel_launches();
 void count_launches(unsigned long long n);
@@ -173,7 +191,7 @@ cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const 
 cudaError_t launch_sample(const DLat& L, const int4* keys, const uint32_t* work, uint32_t n, const uint32_t* rec,
                           const uint4* pack, uint32_t max_units, float* values, unsigned long long* counters, bool tma,
                           bool count, cudaStream_t s, const Scene* many = nullptr, uint32_t* list = nullptr,
-                          size_t small = 0);
+                          size_t small = 0, const uint32_t* ids = nullptr, uint32_t* feats = nullptr);
 cudaError_t launch_mc(const DLat& L, uint32_t n, float* values, const uint32_t* rec, uint32_t* counts, const uint32_t* edge_off,
                       const uint32_t* tri_off, uint32_t* edges, float2* edge_vals, uint32_t* tris, bool fill,
                       cudaStream_t s, const int4* keys = nullptr,

@@ -213,9 +213,14 @@ std::string check_spheres(const double* xyzr, size_t ns, double probe) {
     return "";
 }
 
-std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arrangement& A) {
+const char* const CANCELLED = "cancelled";
+
+std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arrangement& A, const Control* ctl) {
     std::string bad = check_spheres(xyzr, ns, probe);
     if (!bad.empty()) return bad;
+    // The flag is polled per sphere in every pass (control.rs:94-131).
+    auto stop = [&] { return ctl && ctl->cancelled(); };
+    if (stop()) return CANCELLED;
     A = Arrangement();
     A.probe = probe;
     std::vector<uint32_t> active;
@@ -257,6 +262,7 @@ std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arran
     // Containment (arrangement.rs:497-514).
     std::vector<uint8_t> contained(n, 0);
     parallel_for(n, [&](size_t i, int) {
+        if (stop()) return;
         V3 ci = A.c(uint32_t(i));
         bool found = false;
         A.cells.near(ci, R[i] + max_expanded, [&](uint32_t j) {
@@ -267,11 +273,12 @@ std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arran
         contained[i] = found;
     });
     for (uint8_t c : contained) A.n_contained += c;
+    if (stop()) return CANCELLED;
 
     // Neighbour rows, ascending (arrangement.rs:522-545).
     std::vector<std::vector<uint32_t>> rows(n);
     parallel_for(n, [&](size_t i, int) {
-        if (contained[i]) return;
+        if (contained[i] || stop()) return;
         V3 ci = A.c(uint32_t(i));
         auto& r = rows[i];
         A.cells.near(ci, R[i] + max_expanded, [&](uint32_t j) {
@@ -279,6 +286,7 @@ std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arran
         });
         std::sort(r.begin(), r.end());
     });
+    if (stop()) return CANCELLED;
     std::vector<uint32_t> nb_off(n + 1, 0), nb_items;
     for (size_t i = 0; i < n; i++) nb_off[i + 1] = nb_off[i] + uint32_t(rows[i].size());
     nb_items.reserve(nb_off[n]);
@@ -289,7 +297,7 @@ std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arran
     // Circles (i, j > i), blockers, triple points (arrangement.rs:674-752).
     std::vector<SpherePart> parts(n);
     parallel_for(n, [&](size_t iu, int) {
-        if (contained[iu]) return;
+        if (contained[iu] || stop()) return;
         const uint32_t i = uint32_t(iu);
         SpherePart& out = parts[i];
         std::vector<Span> spans;
@@ -360,6 +368,7 @@ std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arran
             out.blk.insert(out.blk.end(), blockers.begin(), blockers.end());
         }
     });
+    if (stop()) return CANCELLED;
     std::vector<uint8_t> exposed(n);
     for (size_t i = 0; i < n; i++) exposed[i] = !contained[i] && nb_off[i + 1] == nb_off[i];
     A.cb_off.assign(1, 0);

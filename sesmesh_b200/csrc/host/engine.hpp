@@ -30,6 +30,9 @@ struct smb_engine {
     smb_batch* batch = nullptr;
     double t_geometry = 0, t_upload = 0;
     int arr_where = 0;          // smb_surface_stats::arrangement_where
+    smbh::Control ctl;          // cancel flag and progress of the engine's calls
+    uint64_t max_device_bytes = 0;  // the memory guard's limit (0: none)
+    uint64_t last_estimate = 0;     // the guard's estimate at the last classification
     uint64_t upload_bytes = 0;  // bytes copied host to device for the arrangement
     // Host copies of the last device run.
     std::vector<int32_t> keys;

@@ -91,8 +91,25 @@ struct Arrangement {
     size_t n_vertices() const { return vertex_atoms.size() / 3; }
 };
 
-// Builds the SES arrangement of n spheres (x, y, z, r rows); error text or "".
-std::string build_arrangement(const double* xyzr, size_t n, double probe, Arrangement& out);
+// Cooperative cancellation and progress (Control, crates/sesmesh/src/
+// control.rs:54-131): a flag polled per sphere and per brick, and a
+// callback told (0, total) and (total, total) of each stage.
+struct Control {
+    const volatile int32_t* cancel = nullptr;
+    void (*progress)(void* user, int stage, uint64_t done, uint64_t total) = nullptr;
+    void* user = nullptr;
+    bool cancelled() const { return cancel && *cancel != 0; }
+    void report(int stage, uint64_t done, uint64_t total) const {
+        if (progress) progress(user, stage, done, total);
+    }
+};
+// The error text of a computation stopped by its control.
+extern const char* const CANCELLED;
+
+// Builds the SES arrangement of n spheres (x, y, z, r rows); error text or
+// "" (CANCELLED when ctl's flag was set before it finished).
+std::string build_arrangement(const double* xyzr, size_t n, double probe, Arrangement& out,
+                              const Control* ctl = nullptr);
 // The input checks of build_arrangement alone; error text or "".
 std::string check_spheres(const double* xyzr, size_t n, double probe);
 

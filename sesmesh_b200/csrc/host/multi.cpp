@@ -122,6 +122,7 @@ struct smb_multi {
     const smb_mlp* warm = nullptr;
     smb_multi_config cfg{};
     bool tuned = false;
+    smbh::Control ctl;  // cancel flag and progress of the runs
     double t_setup = 0, t_tune = 0;
     // Descriptors of the current brick edge.
     int desc_brick = 0;
@@ -135,6 +136,7 @@ struct smb_multi {
     DBuf flags, list, surf, cells, tiles, tot, keys, rec, sampled, work, retry, values, counters, totals, ids, pack;
     DBuf mc_counts, edge_off, tri_off, edges, edge_vals, tris, item_counts, item_off, item_edges;
     DBuf e_t, e_feat, e_q, e_evals;
+    DBuf w_feats, w_start;  // warm start: the sampler's nearest features, each row's start
     size_t edge_cap = 0, tri_cap = 0;
     // Groups of structures, one pass (and one recorded graph) each.
     std::vector<Group> groups;
@@ -157,7 +159,7 @@ struct smb_multi {
     std::vector<DBuf*> bufs() {
         return {&d_arr, &d_lat, &d_rc, &d_box, &d_flag_off, &d_sph_off, &d_err, &d_fail, &flags, &list, &surf,
                 &cells, &tiles, &tot, &keys, &rec, &sampled, &work, &retry, &values, &counters, &totals, &ids, &pack,
-                &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &item_counts, &item_off, &item_edges,
+                &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &item_counts, &item_off, &item_edges, &w_feats, &w_start,
                 &e_t, &e_feat, &e_q, &e_evals};
     }
     size_t n() const { return eng.size(); }
@@ -336,7 +338,9 @@ int reserve_pass(smb_multi* m, size_t max_nb, char* err, size_t errlen) {
         (rc = m->item_off.reserve(nsub * 4 + 4, err, errlen)) ||
         (rc = m->item_edges.reserve(m->edge_cap * 4, err, errlen)) || (rc = m->e_t.reserve(m->edge_cap * 4, err, errlen)) ||
         (rc = m->e_feat.reserve(m->edge_cap * 4, err, errlen)) || (rc = m->e_q.reserve(m->edge_cap * 12, err, errlen)) ||
-        (rc = m->e_evals.reserve(m->edge_cap * 4, err, errlen)))
+        (rc = m->e_evals.reserve(m->edge_cap * 4, err, errlen)) ||
+        (m->warm && ((rc = m->w_feats.reserve(nb * spb * 4, err, errlen)) ||
+                     (rc = m->w_start.reserve(m->edge_cap * 8, err, errlen)))))
         return rc;
     return SMB_OK;
 }
@@ -382,7 +386,8 @@ int enqueue_pass(smb_multi* m, const Group& G, char* err, size_t errlen) {
         if (e != cudaSuccess) return set_err(err, errlen, "gather launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     }
     e = launch_sample(DLat{}, keys, m->work.as<uint32_t>(), nsub, m->rec.as<uint32_t>(), m->pack.as<uint4>(),
-                      m->unit_cap, m->values.as<float>(), cnt, true, false, s, &S);
+                      m->unit_cap, m->values.as<float>(), cnt, true, false, s, &S, nullptr, 0, m->ids.as<uint32_t>(),
+                      m->warm ? m->w_feats.as<uint32_t>() : nullptr);
     if (e != cudaSuccess) return set_err(err, errlen, "sample launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     e = launch_mc(L, nb, m->values.as<float>(), m->rec.as<uint32_t>(), m->mc_counts.as<uint32_t>(), nullptr, nullptr,
                   nullptr, nullptr, nullptr, false, s, keys, ~0ull, ~0ull, &S);
@@ -400,16 +405,22 @@ int enqueue_pass(smb_multi* m, const Group& G, char* err, size_t errlen) {
     launch_item_edges(L, m->work.as<uint32_t>(), nsub, m->rec.as<uint32_t>(), m->edge_off.as<uint32_t>(),
                       m->edges.as<uint32_t>(), m->item_counts.as<uint32_t>(), m->item_off.as<uint32_t>(),
                       m->item_edges.as<uint32_t>(), m->tiles.as<unsigned long long>(), tot + 3, cnt, s, &S, keys);
-    const int mode = m->warm ? REFINE_MLP : REFINE_PLAIN;
-    MlpDev md{nullptr, nullptr, nullptr};
-    if (m->warm) md = mlp_dev(m->warm);
+    const int mode = m->warm ? REFINE_WARM : REFINE_PLAIN;
+    if (m->warm) {
+        e = launch_warm_starts(DArr{}, DLat{}, RefineConsts{}, keys, m->work.as<uint32_t>(), nsub,
+                               m->rec.as<uint32_t>(), m->edges.as<uint32_t>(), m->edge_vals.as<float2>(),
+                               m->item_off.as<uint32_t>(), m->item_edges.as<uint32_t>(), m->values.as<float>(),
+                               m->w_feats.as<uint32_t>(), mlp_dev(m->warm), mlp_use(m->warm), m->w_start.as<float2>(),
+                               cnt, m->edge_cap, d->info.multiprocessors, s, &S);
+        if (e != cudaSuccess) return set_err(err, errlen, "warm start launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    }
     const size_t cand = size_t(m->unit_cap) * 16 + 64;
     e = launch_refine(DArr{}, DLat{}, RefineConsts{}, keys, m->work.as<uint32_t>(), m->rec.as<uint32_t>(),
                       m->ids.as<uint32_t>(), m->edges.as<uint32_t>(), m->edge_vals.as<float2>(),
                       m->item_off.as<uint32_t>(), m->item_edges.as<uint32_t>(), nsub, m->e_t.as<float>(),
                       m->e_feat.as<uint32_t>(), m->e_q.as<float>(), m->e_evals.as<uint32_t>(), cand, mode,
-                      m->values.as<float>(), m->warm ? &md : nullptr, nullptr, cnt, d->info.multiprocessors,
-                      d->smem_optin, s, nullptr, &S);
+                      m->warm ? m->w_start.as<float2>() : nullptr, cnt, d->info.multiprocessors, d->smem_optin, s,
+                      nullptr, &S);
     if (e != cudaSuccess) return set_err(err, errlen, "refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     return SMB_OK;
 }
@@ -607,6 +618,13 @@ void smb_multi_free(smb_multi* m) {
     dev_release(d);
 }
 
+int smb_multi_set_control(smb_multi* m, const smb_control* c) {
+    if (!m) return SMB_ERR_ARG;
+    m->ctl = smbh::Control();
+    if (c) m->ctl.cancel = c->cancel, m->ctl.progress = c->progress, m->ctl.user = c->user;
+    return SMB_OK;
+}
+
 int smb_multi_set_warm_start(smb_multi* m, const smb_mlp* mlp) {
     if (!m) return SMB_ERR_ARG;
     m->warm = mlp;
@@ -797,13 +815,23 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
     std::thread worker;
     auto t_host0 = clk::now();
     double t_host = 0;
+    size_t finished = 0;
+    m->ctl.report(SMB_STAGE_MESH, 0, n);
     for (size_t gi = 0; gi < m->groups.size(); gi++) {
         Group& G = m->groups[gi];
         float dms = 0;
+        // Cancellation between groups (the host stages of the group before
+        // finish first).
+        if (m->ctl.cancelled()) {
+            if (worker.joinable()) worker.join();
+            return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
+        }
         if ((rc = run_group(m, G, &dms, err, errlen))) {
             if (worker.joinable()) worker.join();
             return rc;
         }
+        if (gi) m->ctl.report(SMB_STAGE_MESH, finished, n);
+        finished = G.s1;
         graphs = graphs && (G.graph != nullptr || G.k1 == G.k0);
         t_device += dms;
         auto t1 = clk::now();
@@ -925,6 +953,7 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
     size_t n_redone = 0;
     for (size_t i = 0; i < n; i++) {
         if (!m->redone[i]) continue;
+        if (m->ctl.cancelled()) return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
         n_redone++;
         smb_surface* s = nullptr;
         smb_engine* e = m->eng[i];
@@ -937,6 +966,8 @@ int smb_multi_run(smb_multi* m, smb_multi_times* times, char* err, size_t errlen
         m->latency[i] = ms_since(t_start);
     }
     double t_redo = ms_since(t3b);
+    if (m->ctl.cancelled()) return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
+    m->ctl.report(SMB_STAGE_MESH, n, n);
     if (times) {
         smb_multi_times& T = *times;
         T = smb_multi_times{};

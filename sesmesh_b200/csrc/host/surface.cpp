@@ -3,7 +3,9 @@
 // classification and mesh-stage kernels, host f64 refinement (exact) or
 // placement of the device's f32 roots (fast), assembly, validation,
 // components and OBJ output.
+#include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -111,8 +113,67 @@ extern "C" {
 
 void smb_set_device_arrangement_min(size_t n) { g_device_arrangement_min = n; }
 
+uint64_t smb_device_bytes_estimate(size_t surface_bricks, uint32_t brick, double spacing, double probe,
+                                   int refine) {
+    // Per surface brick: sample values (and the warm start's feature words),
+    // sub-block records and work lists, the candidate lists of its sampled
+    // sub-blocks, and its share of the crossing edges (marching-cubes
+    // outputs, refinement outputs or exact vertices, the finished mesh and
+    // the measure's tables) with two triangles per edge.  The candidate
+    // count of a sub-block's ball is taken at 0.06 spheres per A^3 (above
+    // protein packing) within the largest ball any of its lists uses; 250
+    // bytes per candidate cover its list entries, blockers and packed
+    // coordinates.  The crossing edges of a brick are taken as 1.5 b^2
+    // (a surface crossing it diagonally).
+    const double b = double(brick), sub = 0.5 * b;
+    const double spb = (b + 1) * (b + 1) * (b + 1);
+    const double band = std::sqrt(3.0) * spacing * 1.01, rho = 0.5 * std::sqrt(3.0) * sub * spacing;
+    const double r_ball = 1.8 + probe + probe + band + rho;
+    const double per_ball = 0.06 * 4.18879020478639 * r_ball * r_ball * r_ball * 250.0;
+    const double edges = 1.5 * b * b;
+    const double per_edge = 4 + 8 + 4 + 4 + (refine == SMB_REFINE_FAST ? 28.0 : 37.0) + 2 * 12 + 64;
+    const double per_brick = spb * (refine == SMB_REFINE_FAST ? 8.0 : 4.0) + 8 * (SMB_REC_WORDS * 4 + 16) +
+                             8 * per_ball + edges * per_edge;
+    return uint64_t(double(surface_bricks) * per_brick) + (uint64_t(64) << 20);
+}
+
 int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out,
                    char* err, size_t errlen) {
+    return smb_engine_new_with(dev, xyzr, n, p, nullptr, out, err, errlen);
+}
+
+static void set_control(smb_engine* e, const smb_control* c) {
+    e->ctl = smbh::Control();
+    e->max_device_bytes = 0;
+    if (!c) return;
+    e->ctl.cancel = c->cancel;
+    e->ctl.progress = c->progress;
+    e->ctl.user = c->user;
+    e->max_device_bytes = c->max_device_bytes;
+}
+
+uint64_t smb_engine_device_bytes(const smb_engine* e) {
+    if (!e) return 0;
+    uint64_t n = e->res ? smb_resident_bytes(e->res) : 0;
+    if (e->batch)
+        for (smb::DBuf* b : const_cast<smb_batch*>(e->batch)->bufs()) n += b->cap;
+    smb::MeasureScratch& M = const_cast<smb_engine*>(e)->measure;
+    for (smb::DBuf* b : {&M.pos, &M.nrm, &M.tris, &M.tris_out, &M.keys, &M.cnt, &M.dup, &M.parent, &M.flag, &M.cid,
+                         &M.id, &M.counters, &M.comp_v, &M.comp_t, &M.area, &M.volume, &M.parts, &M.pkey, &M.pidx,
+                         &M.pkey2, &M.pidx2, &M.first, &M.tkey, &M.tidx, &M.tkey2, &M.tidx2, &M.tiles, &M.cub,
+                         &M.packed, &M.err, &M.tri_a, &M.tri_v})
+        n += b->cap;
+    return n;
+}
+
+int smb_engine_set_control(smb_engine* e, const smb_control* control) {
+    if (!e) return SMB_ERR_ARG;
+    set_control(e, control);
+    return SMB_OK;
+}
+
+int smb_engine_new_with(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p,
+                        const smb_control* control, smb_engine** out, char* err, size_t errlen) {
     if (!dev || !p || !out || (n && !xyzr)) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
     *out = nullptr;
     if (p->kind != SMB_SES) return set_err(err, errlen, "only the SES is meshed on the device"), SMB_ERR_ARG;
@@ -126,9 +187,13 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
     auto e = std::make_unique<smb_engine>();
     e->dev = dev;
     e->params = *p;
+    set_control(e.get(), control);
     auto t0 = clk::now();
     std::string m = check_spheres(xyzr, n, p->probe_radius);
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
+    const Control& ctl = e->ctl;
+    if (ctl.cancelled()) return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
+    ctl.report(SMB_STAGE_GEOMETRY, 0, 1);
     // The arrangement: on the device for large inputs (the host builds it
     // when the device declines), else on the host threads.
     bool on_device = false;
@@ -137,9 +202,15 @@ int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surf
         on_device = smb::build_arrangement_device(dev, xyzr, n, p->probe_radius, e->darr, &why) == 0;
     }
     if (!on_device) {
-        m = build_arrangement(xyzr, n, p->probe_radius, e->arr);
+        m = build_arrangement(xyzr, n, p->probe_radius, e->arr, &ctl);
+        if (m == CANCELLED) return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
         if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
     }
+    if (ctl.cancelled()) {
+        if (on_device) e->darr.release();
+        return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
+    }
+    ctl.report(SMB_STAGE_GEOMETRY, 1, 1);
     e->arr_ready = !on_device;
     e->arr_where = on_device ? 1 : (n >= g_device_arrangement_min ? 2 : 0);
     const Arrangement& A = e->arr;
@@ -259,15 +330,34 @@ void smb_engine_free(smb_engine* e) {
 // refinement); results stay on the device.
 int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size_t errlen) {
     if (!e) return SMB_ERR_ARG;
+    const Control& ctl = e->ctl;
+    auto cancelled = [&] { return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED; };
+    if (ctl.cancelled()) return cancelled();
     size_t touched = 0, surface = 0;
+    ctl.report(SMB_STAGE_CLASSIFY, 0, 1);
     auto t0 = clk::now();
     int rc = smb_classify(e->res, &touched, &surface, err, errlen);
     if (rc != SMB_OK) return rc;
     e->t_classify = ms_since(t0);
     e->touched = touched;
+    ctl.report(SMB_STAGE_CLASSIFY, 1, 1);
+    // The memory guard, before any mesh-stage buffer is taken.
+    e->last_estimate = smb_device_bytes_estimate(surface, uint32_t(e->mp.b), e->mp.h, e->params.probe_radius,
+                                                 e->params.refine) +
+                       smb_resident_bytes(e->res);
+    if (e->max_device_bytes && e->last_estimate > e->max_device_bytes)
+        return set_err(err, errlen,
+                       "estimated device memory (%llu bytes for %zu surface bricks at %g A) exceeds the limit of "
+                       "%llu bytes",
+                       (unsigned long long)e->last_estimate, surface, e->mp.h,
+                       (unsigned long long)e->max_device_bytes),
+               SMB_ERR_MEMORY;
+    if (ctl.cancelled()) return cancelled();
+    ctl.report(SMB_STAGE_MESH, 0, surface);
     smb_batch_times t{};
     rc = smb_run(e->res, 0, surface, e->batch, &t, err, errlen);
     if (rc != SMB_OK) return rc;
+    if (ctl.cancelled()) return cancelled();
     e->rows_ready = false;
     if (e->params.refine == SMB_REFINE_FAST) {
         double ms = 0;
@@ -286,6 +376,8 @@ int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size
     }
     e->times = t;
     if (times) *times = t;
+    if (ctl.cancelled()) return cancelled();
+    ctl.report(SMB_STAGE_MESH, surface, surface);
     return SMB_OK;
 }
 
@@ -382,6 +474,8 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
     auto t_all = clk::now();
     int rc = smb_engine_run_device(e, nullptr, err, errlen);
     if (rc != SMB_OK) return rc;
+    const Control& ctl = e->ctl;
+    ctl.report(SMB_STAGE_ASSEMBLE, 0, 1);
     auto fill_times = [&](smb_surface_stats& st, double t_d2h) {
         st.touched_bricks = e->touched;
         st.t_geometry = e->t_geometry;
@@ -397,6 +491,11 @@ int smb_engine_mesh(smb_engine* e, smb_surface** out, char* err, size_t errlen) 
         st.arrangement_where = e->arr_where;
         st.finished_on_host = e->exact_device && !e->note.empty();
         st.upload_bytes = e->upload_bytes;
+        st.spacing_used = e->mp.h;
+        st.device_bytes_estimate = e->last_estimate;
+        ctl.report(SMB_STAGE_ASSEMBLE, 1, 1);
+        ctl.report(SMB_STAGE_MEASURE, 0, 1);
+        ctl.report(SMB_STAGE_MEASURE, 1, 1);
     };
     e->note.clear();
     if (e->exact_device && e->res->n_bricks) {
@@ -477,14 +576,17 @@ int smb_engine_set_exact_device(smb_engine* e, int on) {
 int smb_engine_set_warm_start(smb_engine* e, const smb_mlp* mlp) {
     if (!e) return SMB_ERR_ARG;
     e->warm = mlp;
-    return SMB_OK;
+    // The warm start reads the sampler's nearest features.
+    return smb_batch_record_features(e->batch, mlp != nullptr);
 }
 
 int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, size_t cap, size_t* n, char* err,
                                size_t errlen) {
     if (!e || !n) return SMB_ERR_ARG;
     if (!e->rows_ready) {
+        smb_batch_record_features(e->batch, 1);
         int rc = smb_engine_run_device(e, nullptr, err, errlen);
+        smb_batch_record_features(e->batch, e->warm != nullptr);
         if (rc != SMB_OK) return rc;
         if ((rc = fetch_mc(e, err, errlen)) != SMB_OK) return rc;
         if ((rc = smb_resident_set_refinement(e->res, err, errlen)) != SMB_OK) return rc;
@@ -492,14 +594,22 @@ int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, si
         std::vector<float> x(ne * SMB_MLP_FEATURES);
         std::vector<uint8_t> covered(ne);
         if ((rc = smb_batch_edge_features(e->res, e->batch, x.data(), covered.data(), err, errlen)) != SMB_OK) return rc;
-        MeshOut mo;
-        refine_exact(host_arrangement(e), e->mp, e->keys.data(), e->res->n_bricks, e->edge_off.data(), e->edges.data(),
-                     e->edge_vals.data(), mo);
+        // The labels: exact mode's f64 root parameter (before the edge clamp)
+        // from the device refinement, which equals the host's bit for bit;
+        // edges it leaves to the host (evals = 0) are left out.
+        double ms = 0;
+        if ((rc = smb_refine_exact(e->res, e->batch, &ms, err, errlen)) != SMB_OK) return rc;
+        std::vector<float> pos(3 * ne), nrm(3 * ne), t(ne);
+        std::vector<uint32_t> atoms(ne), evals(ne);
+        std::vector<uint8_t> patches(ne);
+        if (ne && (rc = smb_batch_vertices(e->batch, pos.data(), nrm.data(), atoms.data(), patches.data(), t.data(),
+                                           evals.data())) != SMB_OK)
+            return set_err(err, errlen, "vertex copy"), rc;
         e->row_x.clear(), e->row_t.clear();
         for (size_t k = 0; k < ne; k++) {
-            if (!covered[k]) continue;
+            if (!covered[k] || evals[k] == 0) continue;
             e->row_x.insert(e->row_x.end(), x.begin() + k * SMB_MLP_FEATURES, x.begin() + (k + 1) * SMB_MLP_FEATURES);
-            e->row_t.push_back(mo.t[k]);
+            e->row_t.push_back(t[k]);
         }
         e->rows_ready = true;
     }
@@ -513,14 +623,37 @@ int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, si
 
 int smb_compute_surface(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p, smb_surface** out,
                         char* err, size_t errlen) {
+    return smb_compute_surface_with(dev, xyzr, n, p, nullptr, out, err, errlen);
+}
+
+int smb_compute_surface_with(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p,
+                             const smb_control* control, smb_surface** out, char* err, size_t errlen) {
+    if (!p || !out) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
+    *out = nullptr;
     auto t0 = clk::now();
-    smb_engine* e = nullptr;
-    int rc = smb_engine_new(dev, xyzr, n, p, &e, err, errlen);
-    if (rc != SMB_OK) return rc;
-    rc = smb_engine_mesh(e, out, err, errlen);
-    smb_engine_free(e);
-    if (rc == SMB_OK) (*out)->stats.t_total = ms_since(t0);
-    return rc;
+    smb_surface_params q = *p;
+    const bool coarsen = control && control->auto_coarsen && control->max_device_bytes;
+    // With auto_coarsen, a refused spacing is raised by the square root of
+    // the estimate's excess (surface bricks go as 1 / h^2 at a fixed brick
+    // edge) until it fits, at most 10 A (surface.rs:825-860 does the same
+    // search on its own estimate).
+    for (int attempt = 0;; attempt++) {
+        smb_engine* e = nullptr;
+        int rc = smb_engine_new_with(dev, xyzr, n, &q, control, &e, err, errlen);
+        if (rc != SMB_OK) return rc;
+        rc = smb_engine_mesh(e, out, err, errlen);
+        const uint64_t est = e->last_estimate;
+        smb_engine_free(e);
+        if (rc == SMB_OK) {
+            (*out)->stats.t_total = ms_since(t0);
+            return SMB_OK;
+        }
+        if (rc != SMB_ERR_MEMORY || !coarsen || !est || attempt >= 12 || q.spacing >= 10.0) return rc;
+        const double excess = double(est) / double(control->max_device_bytes);
+        double h = q.spacing * std::sqrt(excess) * 1.05;
+        if (!(h > q.spacing)) h = q.spacing * 1.05;
+        q.spacing = std::min(h, 10.0);
+    }
 }
 
 void smb_surface_free(smb_surface* s) { delete s; }
@@ -610,12 +743,22 @@ int smb_engine_arrangement(const smb_engine* e, smb_arrangement_info* out) {
 // Host-only construction (no device): the arrangement and lattice constants.
 int smb_arrangement_build(const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out, char* err,
                           size_t errlen) {
+    return smb_arrangement_build_with(xyzr, n, p, nullptr, out, err, errlen);
+}
+
+int smb_arrangement_build_with(const double* xyzr, size_t n, const smb_surface_params* p,
+                               const smb_control* control, smb_engine** out, char* err, size_t errlen) {
     if (!p || !out) return SMB_ERR_ARG;
+    *out = nullptr;
     auto e = std::make_unique<smb_engine>();
     e->params = *p;
+    set_control(e.get(), control);
     set_threads(p->threads);
-    std::string m = build_arrangement(xyzr, n, p->probe_radius, e->arr);
+    e->ctl.report(SMB_STAGE_GEOMETRY, 0, 1);
+    std::string m = build_arrangement(xyzr, n, p->probe_radius, e->arr, &e->ctl);
+    if (m == CANCELLED) return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
+    e->ctl.report(SMB_STAGE_GEOMETRY, 1, 1);
     *out = e.release();
     return SMB_OK;
 }

@@ -63,7 +63,6 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* x, uint32_t n,
     mlp_teardown(S);
 }
 
-
 // ---------------------------------------------------------------------------
 // Training step: forward and backward of one 128-row tile per CTA, every
 // matrix product on the tensor cores (tcgen05, bf16 operands, f32 TMEM
@@ -288,12 +287,14 @@ struct smb_mlp {
     smb_device* dev = nullptr;
     DBuf p, w1t, w2t, w2tt, x, y, t, counters, partial, loss, grad, m, v;
     long step = 0;
+    int use = SMB_MLP_GATE;
 };
 
 namespace smb {
 MlpDev mlp_dev(const smb_mlp* m) {
     return MlpDev{m->p.as<float>(), m->w1t.as<__nv_bfloat16>(), m->w2t.as<__nv_bfloat16>()};
 }
+int mlp_use(const smb_mlp* m) { return m->use; }
 size_t mlp_smem_bytes() { return sizeof(MlpSmem) + 128; }
 const smb_device* mlp_device(const smb_mlp* m) { return m->dev; }
 }  // namespace smb
@@ -343,6 +344,12 @@ int smb_mlp_set_params(smb_mlp* m, const float* params, char* err, size_t errlen
     CK(cudaMemsetAsync(m->v.p, 0, MLP_NPARAM * 4, s));
     m->step = 0;
     CK(cudaStreamSynchronize(s));
+    return SMB_OK;
+}
+
+int smb_mlp_set_use(smb_mlp* m, int use) {
+    if (!m || (use != SMB_MLP_GATE && use != SMB_MLP_ROOT)) return SMB_ERR_ARG;
+    m->use = use;
     return SMB_OK;
 }
 

@@ -750,8 +750,10 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
         (rc = b->tiles.reserve(size_t(scan_tiles_needed(uint32_t(nsub))) * 8, err, errlen)) ||
         (rc = b->totals.reserve(64, err, errlen)) || (rc = b->counters.reserve(CNT_N * 8, err, errlen)) ||
         (rc = b->mc_counts.reserve(count * 8, err, errlen)) || (rc = b->edge_off.reserve(count * 4 + 4, err, errlen)) ||
-        (rc = b->tri_off.reserve(count * 4 + 4, err, errlen)) || (rc = b->x_window.reserve(nsub, err, errlen)))
+        (rc = b->tri_off.reserve(count * 4 + 4, err, errlen)) || (rc = b->x_window.reserve(nsub, err, errlen)) ||
+        (b->record_features && (rc = b->w_feats.reserve(count * size_t(L.spb) * 4, err, errlen))))
         return rc;
+    b->have_features = false;
     cudaEventRecord(b->ev[0], s);
     launch_substates(r->A, L, keys, uint32_t(count), b->rec.as<uint32_t>(), b->sampled.as<uint32_t>(), s);
     launch_scan(b->sampled.as<uint32_t>(), uint32_t(nsub), nullptr, b->work.as<uint32_t>(),
@@ -845,8 +847,10 @@ int smb_run(smb_resident* r, size_t first, size_t count, smb_batch* b, smb_batch
     cudaError_t e = launch_sample(L, keys, b->work.as<uint32_t>(), uint32_t(n_work), b->rec.as<uint32_t>(),
                                   b->pack.as<uint4>(), b->max_pack, b->values.as<float>(),
                                   b->counters.as<unsigned long long>(), b->use_tma, false, s, nullptr,
-                                  size_t(b->max_pack) * 16 > small ? b->s_list.as<uint32_t>() : nullptr, small);
+                                  size_t(b->max_pack) * 16 > small ? b->s_list.as<uint32_t>() : nullptr, small,
+                                  b->ids.as<uint32_t>(), b->record_features ? b->w_feats.as<uint32_t>() : nullptr);
     if (e != cudaSuccess) return set_err(err, errlen, "sample launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
+    b->have_features = b->record_features;
     cudaEventRecord(b->ev[3], s);
 
     // (d) marching cubes: counts, offsets, fill.
@@ -918,15 +922,20 @@ static int exact_group(const smb_batch* b) {
 }
 
 // One refinement-kernel pass over the sampled sub-blocks of the last run:
-// plain (linear start), warm (MLP start) or the feature pass (features of
-// each covered edge into e_x, evals = 1 marks it covered).
-static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* mlp, double* ms, char* err,
+// plain (linear start), warm (the MLP's starts: features, MLP, then the
+// refinement from them) or the feature pass alone (FEATURES: the rows'
+// features into e_x, evals = 1 marks the edges covered).
+enum { PASS_PLAIN = 0, PASS_WARM = 1, PASS_FEATURES = 2 };
+static int refine_pass(smb_resident* r, smb_batch* b, int pass, const smb_mlp* mlp, double* ms, char* err,
                        size_t errlen) {
     if (!r || !b || b->res != r) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
     if (!r->refine_ready) return set_err(err, errlen, "smb_resident_set_refinement must run first"), SMB_ERR_STATE;
     smb_device* d = r->dev;
-    if (mode == REFINE_MLP && (!mlp || mlp_device(mlp) != d))
+    if (pass == PASS_WARM && (!mlp || mlp_device(mlp) != d))
         return set_err(err, errlen, "the MLP must live on the resident's device"), SMB_ERR_ARG;
+    if (pass != PASS_PLAIN && !b->have_features)
+        return set_err(err, errlen, "the last run did not record the nearest features (smb_batch_record_features)"),
+               SMB_ERR_STATE;
     CK(cudaSetDevice(d->index));
     cudaStream_t s = d->stream;
     size_t ne = b->n_edges;
@@ -934,22 +943,24 @@ static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* m
     if ((rc = b->e_t.reserve(ne * 4, err, errlen)) || (rc = b->e_feat.reserve(ne * 4, err, errlen)) ||
         (rc = b->e_q.reserve(ne * 12, err, errlen)) || (rc = b->e_evals.reserve(ne * 4, err, errlen)))
         return rc;
-    if (mode == EDGE_FEATURES && (rc = b->e_x.reserve(ne * 4 * 32, err, errlen))) return rc;
+    if ((pass == PASS_FEATURES && (rc = b->e_x.reserve(ne * 4 * 32, err, errlen))) ||
+        (pass == PASS_WARM && (rc = b->w_start.reserve(ne * 8, err, errlen))))
+        return rc;
     b->refined = false;
     b->refined_exact = false;
     if (ms) *ms = 0;
     if (ne == 0 || b->n_work == 0) {
         if (ne) CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
-        if (ne && mode == EDGE_FEATURES) CK(cudaMemsetAsync(b->e_x.p, 0, ne * 4 * 32, s));
         CK(cudaStreamSynchronize(s));
-        b->refined = mode != EDGE_FEATURES;
+        b->refined = pass != PASS_FEATURES;
         return SMB_OK;
     }
     const size_t cand = size_t(b->max_pack) * 16 + 64;
+    const int mode = pass == PASS_WARM ? REFINE_WARM : REFINE_PLAIN;
     size_t smem = 0;
     launch_refine(r->A, r->L, r->rc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
-                  nullptr, nullptr, nullptr, nullptr, cand, mode, nullptr, nullptr, nullptr, nullptr,
-                  d->info.multiprocessors, d->smem_optin, s, &smem);
+                  nullptr, nullptr, nullptr, nullptr, cand, mode, nullptr, nullptr, d->info.multiprocessors,
+                  d->smem_optin, s, &smem);
     if (smem > size_t(d->smem_optin))
         return set_err(err, errlen, "a sub-block's candidates exceed shared memory for refinement"), SMB_ERR_MEMORY;
     const uint32_t nw = b->n_work;
@@ -957,11 +968,10 @@ static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* m
         (rc = b->item_off.reserve(size_t(nw) * 4 + 4, err, errlen)) ||
         (rc = b->item_edges.reserve(ne * 4, err, errlen)) ||
         (rc = b->tiles.reserve(size_t(scan_tiles_needed(nw)) * 8, err, errlen)) ||
-        (mode == REFINE_PLAIN && (rc = b->x_ovf.reserve(size_t(nw) * 4 + 8, err, errlen))))
+        (rc = b->x_ovf.reserve(size_t(nw) * 4 + 8, err, errlen)))
         return rc;
     cudaEventRecord(b->ev[4], s);
     CK(cudaMemsetAsync(b->e_evals.p, 0, ne * 4, s));
-    if (mode == EDGE_FEATURES) CK(cudaMemsetAsync(b->e_x.p, 0, ne * 4 * 32, s));
     unsigned long long* cnt = b->counters.as<unsigned long long>();
     CK(cudaMemsetAsync(cnt + CNT_TIMEOUT, 0, 8, s));
     CK(cudaMemsetAsync(cnt + CNT_MAXITEM, 0, 8, s));
@@ -969,16 +979,28 @@ static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* m
                       b->edges.as<uint32_t>(), b->item_counts.as<uint32_t>(), b->item_off.as<uint32_t>(),
                       b->item_edges.as<uint32_t>(), b->tiles.as<unsigned long long>(),
                       b->totals.as<unsigned long long>() + 3, cnt, s);
-    MlpDev md{nullptr, nullptr, nullptr};
-    if (mlp) md = mlp_dev(mlp);
+    if (pass == PASS_FEATURES) {
+        launch_warm_features(r->A, r->L, r->rc, r->keys + b->first, b->work.as<uint32_t>(), nw, b->rec.as<uint32_t>(),
+                             b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->item_off.as<uint32_t>(),
+                             b->item_edges.as<uint32_t>(), b->values.as<float>(), b->w_feats.as<uint32_t>(),
+                             b->e_x.as<float>(), ne, d->info.multiprocessors, s);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+        return SMB_OK;
+    }
+    if (pass == PASS_WARM)
+        CK(launch_warm_starts(r->A, r->L, r->rc, r->keys + b->first, b->work.as<uint32_t>(), nw, b->rec.as<uint32_t>(),
+                              b->edges.as<uint32_t>(), b->edge_vals.as<float2>(), b->item_off.as<uint32_t>(),
+                              b->item_edges.as<uint32_t>(), b->values.as<float>(), b->w_feats.as<uint32_t>(),
+                              mlp_dev(mlp), mlp_use(mlp), b->w_start.as<float2>(), cnt, ne, d->info.multiprocessors,
+                              s));
     cudaError_t e = launch_refine(r->A, r->L, r->rc, r->keys + b->first, b->work.as<uint32_t>(), b->rec.as<uint32_t>(),
                                   b->ids.as<uint32_t>(), b->edges.as<uint32_t>(), b->edge_vals.as<float2>(),
                                   b->item_off.as<uint32_t>(), b->item_edges.as<uint32_t>(), nw,
                                   b->e_t.as<float>(), b->e_feat.as<uint32_t>(), b->e_q.as<float>(),
-                                  b->e_evals.as<uint32_t>(), cand, mode, b->values.as<float>(),
-                                  mode == REFINE_MLP ? &md : nullptr, b->e_x.as<float>(), cnt,
-                                  d->info.multiprocessors, d->smem_optin, s, nullptr, nullptr,
-                                  mode == REFINE_PLAIN ? b->x_ovf.as<uint32_t>() : nullptr, b->r_region,
+                                  b->e_evals.as<uint32_t>(), cand, mode,
+                                  pass == PASS_WARM ? b->w_start.as<float2>() : nullptr, cnt, d->info.multiprocessors,
+                                  d->smem_optin, s, nullptr, nullptr, b->x_ovf.as<uint32_t>(), b->r_region,
                                   refine_group(b));
     if (e != cudaSuccess) return set_err(err, errlen, "refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     cudaEventRecord(b->ev[5], s);
@@ -989,31 +1011,56 @@ static int refine_pass(smb_resident* r, smb_batch* b, int mode, const smb_mlp* m
     float t = 0;
     cudaEventElapsedTime(&t, b->ev[4], b->ev[5]);
     if (ms) *ms = t;
-    b->refined = mode != EDGE_FEATURES;
+    b->refined = true;
     return SMB_OK;
 }
 
 int smb_refine(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errlen) {
-    return refine_pass(r, b, REFINE_PLAIN, nullptr, ms, err, errlen);
+    return refine_pass(r, b, PASS_PLAIN, nullptr, ms, err, errlen);
 }
 
 int smb_refine_warm(smb_resident* r, smb_batch* b, const smb_mlp* mlp, double* ms, char* err, size_t errlen) {
-    if (!mlp) return refine_pass(r, b, REFINE_PLAIN, nullptr, ms, err, errlen);
-    return refine_pass(r, b, REFINE_MLP, mlp, ms, err, errlen);
+    if (!mlp) return refine_pass(r, b, PASS_PLAIN, nullptr, ms, err, errlen);
+    return refine_pass(r, b, PASS_WARM, mlp, ms, err, errlen);
+}
+
+int smb_batch_record_features(smb_batch* b, int on) {
+    if (!b) return SMB_ERR_ARG;
+    b->record_features = on != 0;
+    return SMB_OK;
+}
+
+int smb_batch_sample_features(const smb_batch* b, uint32_t* out) {
+    if (!b || !out) return SMB_ERR_ARG;
+    if (!b->have_features) return SMB_ERR_STATE;
+    const size_t n = size_t(b->n) * size_t(b->res->L.spb);
+    if (n && cudaMemcpy(out, b->w_feats.p, n * 4, cudaMemcpyDeviceToHost) != cudaSuccess) return SMB_ERR_CUDA;
+    return SMB_OK;
 }
 
 int smb_batch_edge_features(smb_resident* r, smb_batch* b, float* features, uint8_t* covered, char* err,
                             size_t errlen) {
-    int rc = refine_pass(r, b, EDGE_FEATURES, nullptr, nullptr, err, errlen);
+    int rc = refine_pass(r, b, PASS_FEATURES, nullptr, nullptr, err, errlen);
     if (rc != SMB_OK) return rc;
-    size_t ne = b->n_edges;
+    const size_t ne = b->n_edges;
     if (!ne) return SMB_OK;
-    if (features)
-        CK(cudaMemcpy(features, b->e_x.p, ne * 4 * 32, cudaMemcpyDeviceToHost));
-    if (covered) {
-        std::vector<uint32_t> ev(ne);
-        CK(cudaMemcpy(ev.data(), b->e_evals.p, ne * 4, cudaMemcpyDeviceToHost));
-        for (size_t k = 0; k < ne; k++) covered[k] = ev[k] ? 1 : 0;
+    if (features) std::memset(features, 0, ne * 4 * 32);
+    if (covered) std::memset(covered, 0, ne);
+    if (b->n_work == 0) return SMB_OK;
+    // Rows (the items' edge lists) to marching-cubes edge order.
+    unsigned long long n_rows = 0;
+    CK(cudaMemcpy(&n_rows, b->totals.as<unsigned long long>() + 3, 8, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> k_of(n_rows);
+    std::vector<float> x(n_rows * 32);
+    if (n_rows) {
+        CK(cudaMemcpy(k_of.data(), b->item_edges.p, n_rows * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(x.data(), b->e_x.p, n_rows * 4 * 32, cudaMemcpyDeviceToHost));
+    }
+    for (size_t e = 0; e < n_rows; e++) {
+        const size_t k = k_of[e];
+        if (k >= ne) return set_err(err, errlen, "edge list entry out of range"), SMB_ERR_STATE;
+        if (features) std::memcpy(features + k * 32, x.data() + e * 32, 32 * 4);
+        if (covered) covered[k] = 1;
     }
     return SMB_OK;
 }

@@ -51,6 +51,8 @@ struct MlpDev;
 MlpDev mlp_dev(const smb_mlp* m);
 const smb_device* mlp_device(const smb_mlp* m);
 size_t mlp_smem_bytes();
+// How the warm start uses the MLP's output (SMB_MLP_GATE or SMB_MLP_ROOT).
+int mlp_use(const smb_mlp* m);
 
 }  // namespace smb
 
@@ -107,7 +109,11 @@ struct smb_batch {
     smb::DBuf rec, sampled, work, retry_a, retry_b, values, tiles, totals, counters;
     smb::DBuf ids, pack, mc_counts, edge_off, tri_off, edges, edge_vals, tris;
     smb::DBuf e_t, e_feat, e_q, e_evals;  // fast-mode refinement results
-    smb::DBuf e_x;                        // warm-start features (32 f32 per edge)
+    smb::DBuf e_x;                        // warm-start features (32 f32 per row of the items' edge lists)
+    smb::DBuf w_feats;                    // per sample: the sampler's nearest feature (record_features)
+    smb::DBuf w_start;                    // per row: the warm start's chosen start
+    bool record_features = false;         // the sampler records w_feats
+    bool have_features = false;           // the last run recorded them
     smb::DBuf item_counts, item_off, item_edges;  // per sampled sub-block edge lists
     // Vertices refined or placed on the device: position, normal, atom, patch,
     // t, evaluations; overflowed items, summary words, fast-mode exact mask.
@@ -131,7 +137,7 @@ struct smb_batch {
     cudaEvent_t ev[6] = {};
     std::vector<smb::DBuf*> bufs() {
         return {&rec, &sampled, &work, &retry_a, &retry_b, &values, &tiles, &totals, &counters,
-                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &item_counts, &item_off, &item_edges,
+                &ids, &pack, &mc_counts, &edge_off, &tri_off, &edges, &edge_vals, &tris, &e_t, &e_feat, &e_q, &e_evals, &e_x, &w_feats, &w_start, &item_counts, &item_off, &item_edges,
                 &x_pos, &x_nrm, &x_atom, &x_patch, &x_t, &x_evals, &x_ovf, &x_sum, &x_mask, &x_slab, &s_list, &x_window};
     }
 };

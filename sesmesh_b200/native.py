@@ -15,7 +15,7 @@ SYNTH_PATH = os.path.join(_HERE, "libsesmesh_synth.so")
 
 SMB_OK = 0
 ERRORS = {1: "argument", 2: "cuda", 3: "no device", 4: "self-test", 5: "range", 6: "memory", 7: "state",
-          8: "timeout"}
+          8: "timeout", 9: "cancelled"}
 REC_WORDS = 12
 
 
@@ -69,7 +69,16 @@ class SurfaceStats_(C.Structure):
                                                            ("euler", C.c_int64), ("refine_evaluations", C.c_uint64),
                                                            ("refine_cpu_edges", C.c_uint64)]
                 + [(f, C.c_double) for f in TIME_FIELDS] + [("host_threads", C.c_int)]
-                + [("arrangement_where", C.c_int), ("finished_on_host", C.c_int), ("upload_bytes", C.c_uint64)])
+                + [("arrangement_where", C.c_int), ("finished_on_host", C.c_int), ("upload_bytes", C.c_uint64),
+                   ("spacing_used", C.c_double), ("device_bytes_estimate", C.c_uint64)])
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_uint64, C.c_uint64)
+
+
+class Control_(C.Structure):
+    _fields_ = [("cancel", C.POINTER(C.c_int32)), ("progress", PROGRESS_FN), ("user", C.c_void_p),
+                ("max_device_bytes", C.c_uint64), ("auto_coarsen", C.c_int)]
 
 
 class ArrangementInfo(C.Structure):
@@ -133,6 +142,8 @@ SIGNATURES = {
     "smb_batch_edges": (C.c_int, [_vp, _fp, _u32p, _fp, _u32p]),
     "smb_refine_warm": (C.c_int, [_vp, _vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
     "smb_batch_edge_features": (C.c_int, [_vp, _vp, _fp, C.POINTER(C.c_uint8), _cp, _sz]),
+    "smb_batch_record_features": (C.c_int, [_vp, C.c_int]),
+    "smb_batch_sample_features": (C.c_int, [_vp, C.POINTER(C.c_uint32)]),
     "smb_resident_set_exact": (C.c_int, [_vp, _u32p, _u32p, _sz, _u32p, _sz, C.c_double, _cp, _sz]),
     "smb_refine_exact": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
     "smb_batch_vertices": (C.c_int, [_vp, _fp, _fp, _u32p, C.POINTER(C.c_uint8), _fp, _u32p]),
@@ -154,6 +165,17 @@ SIGNATURES = {
     "smb_mlp_free": (None, [_vp]),
     "smb_mlp_set_params": (C.c_int, [_vp, _fp, _cp, _sz]),
     "smb_mlp_get_params": (C.c_int, [_vp, _fp]),
+    "smb_compute_surface_with": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_),
+                                           C.POINTER(Control_), C.POINTER(_vp), _cp, _sz]),
+    "smb_engine_new_with": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_),
+                                      C.POINTER(Control_), C.POINTER(_vp), _cp, _sz]),
+    "smb_engine_set_control": (C.c_int, [_vp, C.POINTER(Control_)]),
+    "smb_multi_set_control": (C.c_int, [_vp, C.POINTER(Control_)]),
+    "smb_arrangement_build_with": (C.c_int, [C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_),
+                                             C.POINTER(Control_), C.POINTER(_vp), _cp, _sz]),
+    "smb_device_bytes_estimate": (C.c_uint64, [_sz, C.c_uint32, C.c_double, C.c_double, C.c_int]),
+    "smb_engine_device_bytes": (C.c_uint64, [_vp]),
+    "smb_mlp_set_use": (C.c_int, [_vp, C.c_int]),
     "smb_mlp_forward": (C.c_int, [_vp, _fp, _sz, _fp, _cp, _sz]),
     "smb_mlp_gradient": (C.c_int, [_vp, _fp, _fp, _sz, _fp, _fp, _cp, _sz]),
     "smb_mlp_train_epoch": (C.c_int, [_vp, _fp, _fp, _sz, _sz, C.c_float, _fp, _cp, _sz]),
@@ -415,11 +437,27 @@ class Batch:
         _check(lib().smb_batch_count_ops(self.h, C.byref(ops), C.byref(n), err, 1024), err)
         return ops.value, n.value
 
+    def record_features(self, on=True):
+        """Later runs' sampling also records each sample's nearest feature
+        (the warm start's input; smb_batch_record_features)."""
+        _check(lib().smb_batch_record_features(self.h, 1 if on else 0), C.create_string_buffer(8))
+
+    def sample_features(self):
+        """The last run's nearest-feature words, (bricks, (b+1)^3) like
+        values(); meaningful at samples a sampled sub-block owns."""
+        v = np.zeros((self.n, (self.res.brick + 1) ** 3), np.uint32)
+        if self.n:
+            rc = lib().smb_batch_sample_features(self.h, _p(v, C.c_uint32))
+            if rc != SMB_OK:
+                raise SmbError(rc, "smb_batch_sample_features")
+        return v
+
     def refine(self, mlp=None, region=None):
         """Fast-mode f32 refinement of the last run's crossing edges on the
-        device (smb_refine; smb_refine_warm with an Mlp); device ms.  region:
-        per-warp bytes when four whole regions do not fit (0: an eighth of
-        the SM's shared memory)."""
+        device (smb_refine; smb_refine_warm with an Mlp, which needs a run
+        that recorded the features); device ms.  region: per-warp bytes when
+        four whole regions do not fit (0: an eighth of the SM's shared
+        memory)."""
         err = C.create_string_buffer(1024)
         lib().smb_resident_set_refinement(self.res.h, err, 1024)
         if region is not None:
@@ -547,6 +585,12 @@ class Mlp:
         out = np.zeros(MLP_NPARAM, np.float32)
         lib().smb_mlp_get_params(self.h, _p(out, C.c_float))
         return out
+
+    def set_use(self, use):
+        """"gate" (start at t_c where the output is >= 0.5, else the linear
+        guess) or "root" (start at the output itself)."""
+        if lib().smb_mlp_set_use(self.h, {"gate": 0, "root": 1}[use]) != SMB_OK:
+            raise ValueError(use)
 
     def forward(self, x):
         x = np.ascontiguousarray(x, np.float32).reshape(-1, MLP_FEATURES)

@@ -149,6 +149,38 @@ class SurfaceOutput:
         self.close()
 
 
+STAGES = ("geometry", "classify", "mesh", "assemble", "measure")
+
+
+class Control:
+    """Control (crates/sesmesh/src/control.rs:54-131) plus the device-memory
+    guard: cancel() makes a computation under it return SMB_ERR_CANCELLED
+    promptly (from any thread); progress(stage, done, total) is called with
+    the stage name when a stage starts and ends; max_device_bytes refuses a
+    computation whose estimated device bytes exceed it (SMB_ERR_MEMORY), or,
+    with auto_coarsen, meshes at the smallest spacing up to 10 A that fits."""
+
+    def __init__(self, progress=None, max_device_bytes=0, auto_coarsen=False):
+        self.flag = C.c_int32(0)
+        self._user = progress
+        self._cb = native.PROGRESS_FN(self._report) if progress else native.PROGRESS_FN()
+        self.c = native.Control_()
+        self.c.cancel = C.pointer(self.flag)
+        self.c.progress = self._cb
+        self.c.user = None
+        self.c.max_device_bytes = int(max_device_bytes)
+        self.c.auto_coarsen = 1 if auto_coarsen else 0
+
+    def _report(self, user, stage, done, total):
+        self._user(STAGES[stage] if 0 <= stage < len(STAGES) else stage, int(done), int(total))
+
+    def cancel(self):
+        self.flag.value = 1
+
+    def is_cancelled(self):
+        return self.flag.value != 0
+
+
 _DEVICES = {}
 
 
@@ -176,19 +208,39 @@ def compute_surface(spheres, params=SurfaceParams()):
     return SurfaceOutput(h)
 
 
+def compute_surface_with(spheres, params, control):
+    """compute_surface_with (surface.rs:614-631): compute_surface under a
+    Control."""
+    s = _spheres(spheres)
+    dev = _device(params.device)
+    err = C.create_string_buffer(1024)
+    h = C.c_void_p()
+    p = params._c()
+    _check(lib().smb_compute_surface_with(dev.h, _p(s, C.c_double), len(s), C.byref(p), C.byref(control.c),
+                                          C.byref(h), err, 1024), err)
+    return SurfaceOutput(h)
+
+
 class SurfaceEngine:
     """SurfaceEngine (surface.rs:633-711): arrangement built and uploaded
     once, then meshed (or its device stage run) any number of times."""
 
-    def __init__(self, spheres, params=SurfaceParams()):
+    def __init__(self, spheres, params=SurfaceParams(), control=None):
         s = _spheres(spheres)
         self.params = params
         self.dev = _device(params.device)
+        self.control = control  # kept alive while the engine uses it
         err = C.create_string_buffer(1024)
         h = C.c_void_p()
         p = params._c()
-        _check(lib().smb_engine_new(self.dev.h, _p(s, C.c_double), len(s), C.byref(p), C.byref(h), err, 1024), err)
+        _check(lib().smb_engine_new_with(self.dev.h, _p(s, C.c_double), len(s), C.byref(p),
+                                         C.byref(control.c) if control is not None else None, C.byref(h), err,
+                                         1024), err)
         self.h = h
+
+    def set_control(self, control):
+        self.control = control
+        lib().smb_engine_set_control(self.h, C.byref(control.c) if control is not None else None)
 
     def run_device(self):
         """Classification, gather, sampling and marching cubes (and fast-mode
@@ -301,13 +353,15 @@ def _arrangement_arrays(h):
     return out
 
 
-def host_arrangement(spheres, params=SurfaceParams()):
+def host_arrangement(spheres, params=SurfaceParams(), control=None):
     """The host-built arrangement (no device), as numpy copies."""
     s = _spheres(spheres)
     err = C.create_string_buffer(1024)
     h = C.c_void_p()
     p = params._c()
-    _check(lib().smb_arrangement_build(_p(s, C.c_double), len(s), C.byref(p), C.byref(h), err, 1024), err)
+    _check(lib().smb_arrangement_build_with(_p(s, C.c_double), len(s), C.byref(p),
+                                            C.byref(control.c) if control is not None else None, C.byref(h), err,
+                                            1024), err)
     try:
         return _arrangement_arrays(h)
     finally:
@@ -353,6 +407,11 @@ class MultiBatch:
     def set_warm_start(self, mlp):
         self.warm = mlp  # kept alive while the batch uses it
         lib().smb_multi_set_warm_start(self.h, mlp.h if mlp is not None else None)
+
+    def set_control(self, control):
+        """Cancel flag and progress (structures finished) of the runs."""
+        self.control = control
+        lib().smb_multi_set_control(self.h, C.byref(control.c) if control is not None else None)
 
     def set_device_finish(self, on=True):
         """Finish each structure on the device (default) or on the host threads."""

@@ -3,29 +3,36 @@ the committed weights.
 
 The MLP (32 -> 64 -> 64 -> 1, GELU, sigmoid; BF16 weights on the tensor
 cores, FP32 accumulation) chooses where each crossing edge's root search
-begins.  For the sphere candidate whose contact sphere best explains the
-edge's two samples, the refinement kernel runs the refinement iteration on
-that sphere alone, without evaluating the field (t_c); where the MLP
-answers >= 0.5 the edge starts at t_c, else at the linear guess
-t_lin = fa / (fa - fb).  The reference's bracketed Newton / Illinois /
-bisection iteration then runs unchanged (smb_refine_warm): a start the
-field judges within the tolerance is accepted after one evaluation, any
-other falls back to the bracketed refinement.  The reference's fast mode
+begins.  The sampler records every sample's nearest feature; at an edge's
+two samples it names one candidate (a sphere, a circle or a SAS vertex),
+and the refinement iteration run on that candidate alone, without
+evaluating the field, gives t_c.  With the gate head (the default, weights
+data/warm_start.f32) the edge starts at t_c where the MLP answers >= 0.5
+and at the linear guess t_lin = fa / (fa - fb) elsewhere; with the root
+head (data/warm_root.f32, smb_mlp_set_use ROOT) it starts at the MLP's
+output itself.  The reference's bracketed Newton / Illinois / bisection
+iteration then runs unchanged (smb_refine_warm): a start the field judges
+within the tolerance is accepted after one evaluation, any other falls back
+to the bracketed refinement.  The reference's fast mode
 (crates/sesmesh/src/field/gpu.rs:207-221 with the iteration of
 crates/sesmesh/src/mesh/extract.rs:425-535) always starts at t_lin.  Where
-the sphere is the surface's nearest feature along the whole edge, t_c is
-where that iteration would stop, so the warm start keeps fast mode's
-vertices (and its area and volume against exact mode) while it saves the
-evaluations.
+the candidate is the surface's nearest feature at the iterates, t_c is
+where that iteration would stop, so the gate keeps fast mode's vertices (and
+its area and volume against exact mode) while it saves evaluations.
 
-Training rows come from seeded synthetic globules (none of them the
-330-atom globule or the ring assemblies the tests and the benchmark use):
-features from the device feature pass (smb_batch_edge_features) and the
-root parameter that exact mode's f64 host refinement finds on the same edge
-(smb_engine_warm_start_rows).  The label is 1 where t_c lies within
-2e-6 A of that root, else 0 (mean squared error on the sigmoid output).
+Training rows come from 200 seeded synthetic globules of 300-30,000 atoms
+(log-uniform; none of them the 330-atom globule, the ring assemblies or the
+shell that the tests and the benchmark use) at 0.1, 0.25, 0.35, 0.5 and
+1 A (0.1 A for globules of at most 8,000 atoms),
+at most ROWS_PER_GLOBULE rows each (about 1e7 in all): features from the
+device feature pass (smb_batch_edge_features) and, as the label source,
+the root parameter that exact mode's f64 refinement finds on the same edge
+(smb_engine_warm_start_rows).  Gate label: 1 where t_c lies within 2e-6 A
+of that root, else 0; root head: the root itself (mean squared error on
+the sigmoid output for both).
 
-    python -m sesmesh_b200.warm_start            # on a B200: rewrites data/warm_start.f32
+    python -m sesmesh_b200.warm_start [--out-dir DIR]   # on a B200: writes
+                                                      # warm_start.f32, warm_root.f32
 """
 import argparse
 import json
@@ -37,15 +44,30 @@ import numpy as np
 from . import native, workloads
 from .surface import SurfaceEngine, SurfaceParams, _device
 
-WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "warm_start.f32")
+DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+WEIGHTS = os.path.join(DATA, "warm_start.f32")
+ROOT_WEIGHTS = os.path.join(DATA, "warm_root.f32")
 
-# (seed, atoms, spacing): globules of 150-1200 atoms, probe 1.4 A, brick 10,
-# at the spacings fast mode is used at.
-TRAIN_SET = [(7000 + k, n, h) for k, (n, h) in enumerate(
-    [(150, 0.5), (300, 0.5), (600, 0.5), (1200, 0.5),
-     (150, 0.35), (300, 0.35), (600, 0.35), (1200, 0.35),
-     (150, 0.25), (300, 0.25), (600, 0.25), (800, 0.25)])]
 PROBE = 1.4
+N_GLOBULES = 200
+ROWS_PER_GLOBULE = 50000
+SPACINGS = (0.1, 0.25, 0.35, 0.5, 1.0)
+FINE_ATOMS = 8000  # above it a 0.1 A turn takes 0.25 A (the edge count grows as 1 / h^2)
+
+
+def train_set(n=N_GLOBULES, seed=7000):
+    """(seed, atoms, spacing) of the training globules: atoms log-uniform in
+    300..30,000, spacing cycling through SPACINGS (the spacings of the
+    benchmark configurations and fast mode's usual ones)."""
+    rng = np.random.default_rng(seed)
+    atoms = np.exp(rng.uniform(np.log(300), np.log(30000), n)).round().astype(int)
+    out = []
+    for k in range(n):
+        h = SPACINGS[k % len(SPACINGS)]
+        if h < 0.25 and atoms[k] > FINE_ATOMS:
+            h = 0.25
+        out.append((seed + k, int(atoms[k]), h))
+    return out
 
 
 def init_params(seed=0):
@@ -62,7 +84,8 @@ def init_params(seed=0):
 
 
 def load(path=WEIGHTS):
-    """The committed warm-start parameters (SMB_MLP_NPARAM f32, little endian)."""
+    """The committed warm-start parameters (SMB_MLP_NPARAM f32, little
+    endian): the gate head by default, ROOT_WEIGHTS for the root head."""
     p = np.fromfile(path, dtype="<f4")
     if p.size != native.MLP_NPARAM:
         raise ValueError("%s holds %d values, not %d" % (path, p.size, native.MLP_NPARAM))
@@ -70,7 +93,7 @@ def load(path=WEIGHTS):
 
 
 def save(params, path=WEIGHTS):
-    os.makedirs(os.path.dirname(path), exist_ok=True)
+    os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
     np.asarray(params, "<f4").tofile(path)
 
 
@@ -84,25 +107,33 @@ def rows(spheres, spacing, probe=PROBE, brick=10):
         eng.close()
 
 
+# Feature columns (smb_batch_edge_features): t_c's iteration converged, t_c
+# (t_lin where it did not), spacing.
+F_CONV, F_TC, F_H = 14, 17, 25
+
+
 def contact_start(x):
-    """t_c as the features give it (-1 where it is half an edge or more from
-    t_lin, which the kernel does not take)."""
-    d = x[:, 26].astype(np.float64) / 8.0
-    return np.where(np.abs(d) < 0.5, x[:, 27].astype(np.float64) + d, -1.0)
+    """t_c as the features give it (-1 where the candidate's iteration did
+    not converge or there is no candidate)."""
+    return np.where(x[:, F_CONV] > 0.5, x[:, F_TC].astype(np.float64), -1.0)
 
 
-def target_of(x, t_exact, spacing=None):
-    """1 where the contact iteration's result lies within 2e-6 A of the
-    exact root, else 0 (spacing per row: feature 28)."""
-    h = x[:, 28].astype(np.float64) if spacing is None else spacing
+def target_of(x, t_exact):
+    """Gate label: 1 where t_c lies within 2e-6 A of the exact root."""
+    h = x[:, F_H].astype(np.float64)
     tc = contact_start(x)
     return ((tc >= 0) & (np.abs(tc - t_exact) * h <= 2e-6)).astype(np.float32)
 
 
-def training_rows(train_set=TRAIN_SET, log=None):
+def training_rows(sets=None, per=ROWS_PER_GLOBULE, log=None):
+    sets = train_set() if sets is None else sets
+    rng = np.random.default_rng(1)
     xs, ts = [], []
-    for seed, n, h in train_set:
+    for seed, n, h in sets:
         x, t = rows(workloads.globule(seed, n), h)
+        if len(x) > per:
+            keep = np.sort(rng.choice(len(x), per, replace=False))
+            x, t = x[keep], t[keep]
         xs.append(x)
         ts.append(t)
         if log:
@@ -129,7 +160,7 @@ def train(x, target, epochs=40, batch=4096, lr=2e-3, seed=0, device=0, log=None)
 
 
 def evaluate(params, x, t_exact, device=0):
-    """How the MLP's choices compare with the labels: the fraction of edges
+    """How the gate's choices compare with the labels: the fraction of edges
     sent to t_c, the fraction whose label is 1, precision and recall."""
     mlp = native.Mlp(_device(device), params)
     y = mlp.forward(x) >= 0.5
@@ -139,25 +170,40 @@ def evaluate(params, x, t_exact, device=0):
                 precision=tp / max(1.0, float(y.sum())), recall=tp / max(1.0, float(lab.sum())))
 
 
+def evaluate_root(params, x, t_exact, device=0):
+    """The root head's error against the exact root, in A (median, 90th
+    percentile)."""
+    mlp = native.Mlp(_device(device), params)
+    d = np.abs(mlp.forward(x).astype(np.float64) - t_exact) * x[:, F_H]
+    return dict(rows=int(len(x)), median_A=float(np.median(d)), p90_A=float(np.percentile(d, 90)))
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--out", default=WEIGHTS)
-    ap.add_argument("--epochs", type=int, default=40)
-    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--out-dir", default=DATA)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--globules", type=int, default=N_GLOBULES)
     a = ap.parse_args(argv)
     log = lambda m: print(m, flush=True)
     t0 = time.time()
-    x, t = training_rows(log=log)
+    x, t = training_rows(train_set(a.globules), log=log)
     log("%d rows in %.1f s" % (len(x), time.time() - t0))
-    params, hist = train(x, target_of(x, t), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, log=log)
-    save(params, a.out)
+    t1 = time.time()
+    gate, hist = train(x, target_of(x, t), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, log=log)
+    save(gate, os.path.join(a.out_dir, "warm_start.f32"))
+    root, hist_r = train(x, t.astype(np.float32), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed + 7, log=log)
+    save(root, os.path.join(a.out_dir, "warm_root.f32"))
+    t_train = time.time() - t1
     held = workloads.globule330()
     xh, th = rows(held["spheres"], held["spacing"], held["probe"], held["brick"])
-    summary = dict(train=evaluate(params, x, t), held_out_globule330=evaluate(params, xh, th),
-                   final_loss=hist[-1], seconds=time.time() - t0, out=a.out)
-    print(json.dumps(summary))
+    summary = dict(rows=int(len(x)), globules=a.globules, train_gate=evaluate(gate, x, t),
+                   held_out_globule330_gate=evaluate(gate, xh, th), held_out_globule330_root=evaluate_root(root, xh, th),
+                   final_loss_gate=hist[-1], final_loss_root=hist_r[-1], seconds_rows=t1 - t0, seconds_train=t_train,
+                   out_dir=a.out_dir)
+    print(json.dumps(summary), flush=True)
 
 
 if __name__ == "__main__":
