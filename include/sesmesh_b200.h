@@ -97,7 +97,14 @@ typedef struct {
     const double* vertex;     /* 3 per SAS vertex */
     smb_grid_ref sphere_grid, circle_grid, vertex_grid;
     double max_expanded, rho_max, probe;
+    /* The surface (SurfaceKind, field/mod.rs:33-41): SMB_KIND_SES, or a
+     * sphere field, SMB_KIND_SAS / SMB_KIND_VDW (min |x - c| - R over the
+     * spheres; expanded = r + probe for the SAS, r for the vdW surface; no
+     * circles or vertices; field/kernel.rs:957-981, point.rs:566-579,
+     * 723-736). */
+    int kind;
 } smb_arrangement_ref;
+enum { SMB_KIND_SES = 0, SMB_KIND_SAS = 1, SMB_KIND_VDW = 2 };
 
 /* The sampling lattice (Lattice, field/lattice.rs:26-45; Engine::new,
  * field/kernel.rs:204-271).  brick must be even, 4..32 (the device path

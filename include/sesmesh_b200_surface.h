@@ -16,12 +16,18 @@
 extern "C" {
 #endif
 
-enum { SMB_SES = 0 };
+/* Surface kinds (SurfaceKind, field/mod.rs:33-41): the SES, the SAS (the
+ * spheres expanded by the probe) and the vdW surface (the spheres; also the
+ * SES with probe 0).  Equal to SMB_KIND_*. */
+enum { SMB_SES = 0, SMB_SAS = 1, SMB_VDW = 2 };
 enum { SMB_REFINE_EXACT = 0, SMB_REFINE_LINEAR = 1, SMB_REFINE_FAST = 2 };
 
 /* SurfaceParams (surface.rs:195-241) restricted to what the device path
- * takes: SES, spacing, brick_size (even, 4..32; reference default 10),
- * refine exact | fast.  threads: host threads (0 = all cores). */
+ * takes: kind (SES, SAS or vdW; the vdW surface ignores the probe radius,
+ * SurfaceParams::effective_probe), spacing, brick_size (even, 4..32;
+ * reference default 10), refine exact | fast (a sphere field refines fast
+ * mode from the linear guess: the learned warm start is the SES's).
+ * threads: host threads (0 = all cores). */
 typedef struct {
     int kind;
     double probe_radius;
@@ -90,11 +96,12 @@ typedef struct {
     int auto_coarsen;
 } smb_control;
 /* Device bytes of the mesh stage for this many surface bricks of this edge
- * at this spacing and probe (values, records, candidate lists,
- * marching-cubes and refinement outputs, exact-mode vertices and the device
- * finish; conservative). */
+ * at this spacing and probe, for an input of `spheres` spheres on a device
+ * of `multiprocessors` SMs (values, records, candidate lists,
+ * marching-cubes and refinement outputs, exact-mode vertices, the exact
+ * refinement's list slabs and the device finish; conservative). */
 uint64_t smb_device_bytes_estimate(size_t surface_bricks, uint32_t brick, double spacing, double probe_radius,
-                                   int refine);
+                                   size_t spheres, int refine, int multiprocessors);
 
 typedef struct smb_engine smb_engine;
 typedef struct smb_surface smb_surface;
@@ -145,14 +152,17 @@ smb_batch* smb_engine_batch(smb_engine* e);
 int smb_engine_set_warm_start(smb_engine* e, const smb_mlp* mlp);
 /* Training rows of the warm start (no counterpart in the reference): runs
  * the device stage, then for every edge the device refines (marching-cubes
- * order) its SMB_MLP_FEATURES features and, as the label, the root
- * parameter that exact mode's f64 host refinement finds on that edge
- * (before the edge clamp).  *n gets the row count; the rows are copied when
- * features and labels are non-null (SMB_ERR_MEMORY if cap < *n).  The rows
- * are kept until the next device run, so a first call with null buffers
- * sizes them and a second one copies them. */
-int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, size_t cap, size_t* n, char* err,
-                               size_t errlen);
+ * order) its SMB_MLP_FEATURES features, as the label the root parameter
+ * that exact mode's f64 refinement finds on that edge (before the edge
+ * clamp), and the root parameter plain f32 refinement (smb_refine) stops
+ * at (NaN where it does not converge).  Edges the device's exact
+ * refinement leaves to the host are left out.  *n gets the row count; the
+ * rows are copied when features, labels and plain are non-null
+ * (SMB_ERR_MEMORY if cap < *n).  The rows are kept until the next device
+ * run, so a first call with null buffers sizes them and a second one
+ * copies them. */
+int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, float* plain, size_t cap, size_t* n,
+                               char* err, size_t errlen);
 
 void smb_surface_free(smb_surface* s);
 int smb_surface_stats_get(const smb_surface* s, smb_surface_stats* out);

@@ -30,11 +30,12 @@ extern "C" {
 void orc_set_threads(int n) { set_threads(n); }
 int orc_threads(void) { return threads(); }
 
-void* orc_engine_new(const double* xyzr, size_t n, double probe, double spacing, size_t brick, char* err,
+// kind: 0 SES, 1 SAS, 2 vdW (field/mod.rs:33-41).
+void* orc_engine_new(const double* xyzr, size_t n, double probe, double spacing, size_t brick, int kind, char* err,
                      size_t errlen) {
     auto s = spheres(xyzr, n);
     SesField f;
-    std::string m = build_field(s.data(), n, probe, f);
+    std::string m = build_field(s.data(), n, probe, f, kind);
     if (!m.empty()) return set_err(err, errlen, m), nullptr;
     auto* h = new Handle();
     m = make_engine(std::move(f), spacing, brick, h->e);
@@ -197,6 +198,19 @@ void orc_engine_field(void* hp, const double* pts, size_t n, double* out) {
     });
 }
 
+// SesField::sample at n points: value and, where it has one, the normal
+// (has[i] = 1), for the accuracy checks of tests/surface.rs:23-43.
+void orc_engine_field_normals(void* hp, const double* pts, size_t n, double* out, double* normals, uint8_t* has) {
+    const Engine& e = static_cast<Handle*>(hp)->e;
+    parallel_for(n, [&](size_t i, int) {
+        V3 nrm;
+        bool h = false;
+        out[i] = e.field.value(V3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]), &nrm, &h);
+        normals[3 * i] = nrm.x, normals[3 * i + 1] = nrm.y, normals[3 * i + 2] = nrm.z;
+        has[i] = h;
+    });
+}
+
 // CPU mesh stage on a sample of bricks (Engine::evaluate + mesh_brick per
 // brick, chunks of bricks over all threads, as fold_brick_chunks_with):
 // wall seconds; *evals gets the refinement evaluations.
@@ -222,11 +236,11 @@ double orc_engine_mesh_sample(void* hp, const int32_t* bricks, size_t n, uint64_
 }
 
 // Whole CPU pipeline; returns a handle or null with err set.
-void* orc_surface_new(const double* xyzr, size_t n, double probe, double spacing, size_t brick, char* err,
+void* orc_surface_new(const double* xyzr, size_t n, double probe, double spacing, size_t brick, int kind, char* err,
                       size_t errlen) {
     auto s = spheres(xyzr, n);
     auto* h = new SurfaceHandle();
-    std::string m = compute_surface(s.data(), n, probe, spacing, brick, h->out);
+    std::string m = compute_surface(s.data(), n, probe, spacing, brick, h->out, kind);
     if (!m.empty()) {
         delete h;
         return set_err(err, errlen, m), nullptr;

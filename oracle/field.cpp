@@ -96,6 +96,17 @@ void SesField::try_vertex(const V3& x, uint32_t vi, PointEval& best) const {
 void SesField::gather_local(const V3& b, double rho, double band, LocalCandidates& out) const {
     const Arrangement& a = arr;
     out.clear();
+    if (kind != KIND_SES) {  // point.rs:566-579
+        double reach = band + rho;
+        a.cells.for_each_near(b, reach + a.max_expanded, [&](uint32_t k) {
+            if (a.status[k] != CONTAINED && b.dist(a.centers[k]) - a.expanded[k] < reach)
+                out.order.push_back({b.dist(a.centers[k]) - a.expanded[k], k});
+        });
+        sort_nearest(out.order);
+        for (auto& o : out.order) out.inside.push_back(o.second);
+        out.order.clear();
+        return;
+    }
     double reach = probe + band + rho;
     a.cells.for_each_near(b, reach + a.max_expanded, [&](uint32_t k) {
         if (a.status[k] == CONTAINED) return;
@@ -144,6 +155,15 @@ void SesField::gather_local(const V3& b, double rho, double band, LocalCandidate
 // point.rs:686-738 (SES branch)
 NearEval SesField::eval_local(const V3& x, double band, const LocalCandidates& l) const {
     const Arrangement& a = arr;
+    if (kind != KIND_SES) {  // point.rs:723-736
+        double best = band;
+        int64_t bi = -1;
+        for (uint32_t k : l.inside) {
+            double v = x.dist(a.centers[k]) - a.expanded[k];
+            if (v < best) best = v, bi = k;
+        }
+        return NearEval{best, bi < 0 ? Feature{F_BEYOND, 0} : Feature{F_SPHERE, uint32_t(bi)}, x};
+    }
     bool inside = false;
     for (uint32_t k : l.inside)
         if (x.dist(a.centers[k]) < a.expanded[k]) {
@@ -173,12 +193,33 @@ std::pair<double, int64_t> SesField::sphere_eval(const V3& x, double cutoff) con
 }
 
 // point.rs:760-765
-double SesField::clamped_value(const V3& x, double band) const { return probe - ses_eval(x, probe + band).distance; }
+double SesField::clamped_value(const V3& x, double band) const {
+    if (kind != KIND_SES) return sphere_eval(x, band).first;
+    return probe - ses_eval(x, probe + band).distance;
+}
 
 // point.rs:304-349 (SES): value with the growing cutoff, and the normal.
 double SesField::value(const V3& x, V3* normal, bool* has_normal) const {
     if (has_normal) *has_normal = false;
-    if (arr.centers.empty()) return probe;
+    if (arr.centers.empty()) return kind == KIND_SES ? probe : INFINITY;
+    if (kind != KIND_SES) {  // point.rs:340-370
+        double cutoff = 4.0;
+        std::pair<double, int64_t> r;
+        for (;;) {
+            r = sphere_eval(x, cutoff);
+            if (r.second >= 0 || cutoff > extent) break;
+            cutoff *= 2.0;
+        }
+        if (r.second >= 0) {
+            V3 dir = x - arr.centers[size_t(r.second)];
+            double len = dir.norm();
+            if (len > 1e-12) {
+                if (normal) *normal = dir / len;
+                if (has_normal) *has_normal = true;
+            }
+        }
+        return r.first;
+    }
     double cutoff = probe + 4.0;
     PointEval e;
     for (;;) {
@@ -271,6 +312,11 @@ int uniform_sign(const SesField& f, const V3& center, double rho) {
             s_vdw = std::fmin(s_vdw, d - a.radii[k]);
         }
     });
+    if (f.kind != KIND_SES) {  // lattice.rs:213-215: the sign of s_sas alone
+        if (s_sas > margin) return 1;
+        if (s_sas < -margin) return 0;
+        return -1;
+    }
     if (s_sas >= margin) return 1;
     if (s_vdw <= -margin) return 0;
     double cutoff = f.probe + margin + CLASSIFY_EPS;
@@ -595,7 +641,18 @@ static float ses_sample(const Gathered& g, float x, float y, float z, float prob
     return probe - std::sqrt(best2);
 }
 
-// kernel.rs:415-446 (SES) with prepare_sub (kernel.rs:553-600)
+// sphere_kernel (kernel.rs:957-981) at one point: the clamped union of
+// spheres, min(band, min_k(|x - c_k| - R_k)) over every gathered sphere.
+static float sphere_sample(const Gathered& g, float x, float y, float z, float band) {
+    float best = band;
+    for (size_t k = 0; k < g.nx.size(); k++) {
+        float dx = x - g.nx[k], dy = y - g.ny[k], dz = z - g.nz[k];
+        best = std::fmin(best, std::sqrt(dx * dx + dy * dy + dz * dz) - g.nr[k]);
+    }
+    return best;
+}
+
+// kernel.rs:415-446 with prepare_sub (kernel.rs:553-600)
 void evaluate(const Engine& e, const int32_t key[3], BrickScratch& s) {
     int state[8];
     sub_states(e, key, state);
@@ -620,6 +677,13 @@ void evaluate(const Engine& e, const int32_t key[3], BrickScratch& s) {
         }
         double rho;
         V3 center = sub_center(e, key, sb, &rho);
+        if (e.field.kind != KIND_SES) {
+            // gather_spheres + sphere_kernel (kernel.rs:651-654, 957-981).
+            gather_near(e, center, rho, e.band + rho, s);
+            for (size_t j = 0; j < grp.size(); j++)
+                s.values[grp[j]] = sphere_sample(s.g, s.xs[j], s.ys[j], s.zs[j], float(e.band));
+            continue;
+        }
         gather_ses(e, center, rho, s);
         for (size_t j = 0; j < grp.size(); j++)
             s.values[grp[j]] = ses_sample(s.g, s.xs[j], s.ys[j], s.zs[j], probe, cutoff2);

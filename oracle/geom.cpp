@@ -244,9 +244,9 @@ static bool exposed_arcs(std::vector<Buried>& iv, std::vector<Merged>& merged) {
     return any;
 }
 
-// arrangement.rs:437-646 (with circles, without arcs, as SesField::new_with
-// builds it for the SES, point.rs:235-237).
-static std::string build_arrangement(const Sphere* sp, size_t ns, double probe, Arrangement& A) {
+// arrangement.rs:437-646 (without arcs; with circles for the SES, without
+// for SAS and vdW, as SesField::new_with builds them, point.rs:229-237).
+static std::string build_arrangement(const Sphere* sp, size_t ns, double probe, Arrangement& A, bool with_circles) {
     if (!(std::isfinite(probe) && probe >= 0.0)) return "probe radius must be finite and >= 0";
     for (size_t i = 0; i < ns; i++) {
         V3 c(sp[i].c[0], sp[i].c[1], sp[i].c[2]);
@@ -332,7 +332,7 @@ static std::string build_arrangement(const Sphere* sp, size_t ns, double probe, 
     std::vector<Part> parts(n);
     const Csr& NB = A.neighbors;
     parallel_for(n, [&](size_t i, int) {
-        if (contained[i]) return;
+        if (contained[i] || !with_circles) return;
         Part& out = parts[i];
         std::vector<Buried> intervals;
         std::vector<Merged> merged;
@@ -399,8 +399,10 @@ static std::string build_arrangement(const Sphere* sp, size_t ns, double probe, 
             out.blockers.push_back(blockers);
         }
     });
+    // arrangement.rs:568-571: without circles every sphere not contained is
+    // exposed.
     std::vector<uint8_t> exposed(n);
-    for (size_t i = 0; i < n; i++) exposed[i] = !contained[i] && NB.row_len(i) == 0;
+    for (size_t i = 0; i < n; i++) exposed[i] = !contained[i] && (!with_circles || NB.row_len(i) == 0);
     A.circle_blockers.off.assign(1, 0);
     for (size_t i = 0; i < n; i++) {
         Part& p = parts[i];
@@ -421,10 +423,11 @@ static std::string build_arrangement(const Sphere* sp, size_t ns, double probe, 
 }
 
 // point.rs:213-285
-std::string build_field(const Sphere* s, size_t n, double probe, SesField& F) {
+std::string build_field(const Sphere* s, size_t n, double probe, SesField& F, int kind) {
     if (!(std::isfinite(probe) && probe >= 0.0)) return "probe radius must be finite and >= 0";
-    if (probe == 0.0) return "probe radius 0 selects the vdW surface, which this oracle does not cover";
-    std::string err = build_arrangement(s, n, probe, F.arr);
+    if (kind == KIND_SES && probe == 0.0) kind = KIND_VDW;  // point.rs:224-228
+    F.kind = kind;
+    std::string err = build_arrangement(s, n, kind == KIND_VDW ? 0.0 : probe, F.arr, kind == KIND_SES);
     if (!err.empty()) return err;
     F.probe = probe;
     Arrangement& A = F.arr;

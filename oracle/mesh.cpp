@@ -35,9 +35,10 @@ double edge_clamp(const Engine& e) {
 }
 
 // extract.rs:539-549
-static bool gradient(const V3& x, const NearEval& e, V3& out) {
+static bool gradient(const SesField& f, const V3& x, const NearEval& e, V3& out) {
     if (e.feature.kind == F_SOLVENT || e.feature.kind == F_BEYOND) return false;
-    V3 w = e.closest - x;
+    if (f.kind != KIND_SES && e.feature.kind != F_SPHERE) return false;
+    V3 w = f.kind == KIND_SES ? e.closest - x : x - f.arr.centers[e.feature.id];
     double len = w.norm();
     if (!(len > 1e-12)) return false;
     out = w / len;
@@ -62,7 +63,11 @@ static void attributes(const Engine& E, const V3& v, const NearEval& e, const V3
         }
         return a.orig[bi];
     };
-    switch (e.feature.kind) {
+    if (E.field.kind != KIND_SES && e.feature.kind == F_SPHERE) {  // extract.rs:583-587
+        normal = unit(v - a.centers[e.feature.id]), patch = 0, atom = a.orig[e.feature.id];
+        return;
+    }
+    switch (E.field.kind != KIND_SES ? uint32_t(F_BEYOND) : e.feature.kind) {
         case F_SPHERE:
             normal = unit(e.closest - v), patch = 0, atom = a.orig[e.feature.id];
             return;
@@ -113,7 +118,7 @@ static void vertex(const Engine& E, const V3& pa, const V3& pb, double fa, doubl
             side = 1;
         }
         V3 n;
-        double slope = gradient(pa + d * t, e, n) ? n.dot(d) : 0.0;
+        double slope = gradient(field, pa + d * t, e, n) ? n.dot(d) : 0.0;
         double newton = t - g / slope;
         if (std::fabs(slope) > 1e-3 * d.norm() && newton > t0 && newton < t1) {
             t = newton;
@@ -490,12 +495,13 @@ std::string obj_bytes(const Mesh& m, int precision, bool normals) {
 
 // surface.rs:1001-1300 with the default parameters and the CPU back end
 // (mesh stage in chunks of par::chunk_len bricks, par.rs:66).
-std::string compute_surface(const Sphere* s, size_t n, double probe, double spacing, size_t brick, SurfaceOut& out) {
+std::string compute_surface(const Sphere* s, size_t n, double probe, double spacing, size_t brick, SurfaceOut& out,
+                            int kind) {
     using clk = std::chrono::steady_clock;
     auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
     auto t0 = clk::now();
     SesField field;
-    std::string err = build_field(s, n, probe, field);
+    std::string err = build_field(s, n, probe, field, kind);
     if (!err.empty()) return err;
     Engine E;
     err = make_engine(std::move(field), spacing, brick, E);

@@ -149,8 +149,12 @@ struct LocalCandidates {
     void clear();
 };
 
+// field/mod.rs:33-41: the surface a field describes.
+enum Kind : int { KIND_SES = 0, KIND_SAS = 1, KIND_VDW = 2 };
+
 struct SesField {
     Arrangement arr;
+    int kind = KIND_SES;
     double probe = 0;
     CellGrid circle_cells, vertex_cells;
     double rho_max = 0, extent = 0;
@@ -170,7 +174,7 @@ struct SesField {
 };
 
 // Returns an error message (empty on success).
-std::string build_field(const Sphere* s, size_t n, double probe, SesField& out);
+std::string build_field(const Sphere* s, size_t n, double probe, SesField& out, int kind = KIND_SES);
 
 // ---- field/lattice.rs ---------------------------------------------------------
 constexpr int64_t KEY_BIAS = int64_t(1) << 20;
@@ -280,7 +284,7 @@ struct SurfaceOut {
     SurfaceStats stats;
 };
 std::string compute_surface(const Sphere* s, size_t n, double probe, double spacing, size_t brick,
-                            SurfaceOut& out);
+                            SurfaceOut& out, int kind = KIND_SES);
 
 // Threads used by the parallel loops (0 = hardware concurrency).
 void set_threads(int n);

@@ -29,7 +29,7 @@ def lib():
         vp, sz, dp, fp = C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_float)
         u32p, i32p = C.POINTER(C.c_uint32), C.POINTER(C.c_int32)
         L.orc_engine_new.restype = vp
-        L.orc_engine_new.argtypes = [dp, sz, C.c_double, C.c_double, sz, C.c_char_p, sz]
+        L.orc_engine_new.argtypes = [dp, sz, C.c_double, C.c_double, sz, C.c_int, C.c_char_p, sz]
         L.orc_engine_free.argtypes = [vp]
         L.orc_engine_info.argtypes = [vp, dp]
         L.orc_engine_arrangement.argtypes = [vp, dp, C.POINTER(C.c_uint8), u32p, dp, dp]
@@ -44,10 +44,12 @@ def lib():
         L.orc_engine_gather.argtypes = [vp, i32p, C.c_int, u32p, sz]
         L.orc_mc_brick.argtypes = [C.c_int, fp, u32p, u32p, C.POINTER(sz)]
         L.orc_engine_field.argtypes = [vp, dp, sz, dp]
+        L.orc_engine_field_normals.restype = None
+        L.orc_engine_field_normals.argtypes = [vp, dp, sz, dp, dp, C.POINTER(C.c_uint8)]
         L.orc_engine_mesh_sample.restype = C.c_double
         L.orc_engine_mesh_sample.argtypes = [vp, i32p, sz, C.POINTER(C.c_uint64)]
         L.orc_surface_new.restype = vp
-        L.orc_surface_new.argtypes = [dp, sz, C.c_double, C.c_double, sz, C.c_char_p, sz]
+        L.orc_surface_new.argtypes = [dp, sz, C.c_double, C.c_double, sz, C.c_int, C.c_char_p, sz]
         L.orc_surface_free.argtypes = [vp]
         L.orc_surface_stats.argtypes = [vp, dp]
         L.orc_surface_mesh.argtypes = [vp, fp, fp, u32p, u32p, C.POINTER(C.c_uint8)]
@@ -84,6 +86,7 @@ INFO_KEYS = ("frame_x", "frame_y", "frame_z", "band", "coord_max", "f32_ok", "n_
              "n_circles", "n_vertices", "max_expanded", "rho_max", "nb_items", "cb_items", "sub", "nsub",
              "edge_clamp")
 
+KINDS = {"ses": 0, "sas": 1, "vdw": 2}
 STAT_KEYS = ("touched", "surface_bricks", "vertices", "triangles", "components", "area", "volume", "euler",
              "refine_evaluations", "t_geometry", "t_classify", "t_mesh", "t_assemble", "t_measure")
 
@@ -91,11 +94,11 @@ STAT_KEYS = ("touched", "surface_bricks", "vertices", "triangles", "components",
 class Engine:
     """SesField + Engine of the oracle for one sphere set."""
 
-    def __init__(self, spheres, probe, spacing, brick=10):
+    def __init__(self, spheres, probe, spacing, brick=10, kind="ses"):
         s = _xyzr(spheres)
         self._keep = s
         err = C.create_string_buffer(512)
-        self.h = lib().orc_engine_new(_p(s, C.c_double), len(s), probe, spacing, brick, err, 512)
+        self.h = lib().orc_engine_new(_p(s, C.c_double), len(s), probe, spacing, brick, KINDS[kind], err, 512)
         if not self.h:
             raise ValueError(err.value.decode())
         self.brick = brick
@@ -192,6 +195,16 @@ class Engine:
         lib().orc_engine_field(self.h, _p(p, C.c_double), len(p), _p(out, C.c_double))
         return out
 
+    def field_normals(self, pts):
+        """(values, normals (n, 3), has-normal mask) of SesField::sample."""
+        p = np.ascontiguousarray(pts, np.float64).reshape(-1, 3)
+        out = np.zeros(len(p))
+        nrm = np.zeros((len(p), 3))
+        has = np.zeros(len(p), np.uint8)
+        lib().orc_engine_field_normals(self.h, _p(p, C.c_double), len(p), _p(out, C.c_double),
+                                       _p(nrm, C.c_double), _p(has, C.c_uint8))
+        return out, nrm, has.astype(bool)
+
 
 def mc_brick(b, values):
     v = np.ascontiguousarray(values, np.float32)
@@ -206,10 +219,10 @@ def mc_brick(b, values):
 class Surface:
     """The oracle's whole CPU pipeline (compute_surface, CPU back end)."""
 
-    def __init__(self, spheres, probe, spacing, brick=10):
+    def __init__(self, spheres, probe, spacing, brick=10, kind="ses"):
         s = _xyzr(spheres)
         err = C.create_string_buffer(512)
-        self.h = lib().orc_surface_new(_p(s, C.c_double), len(s), probe, spacing, brick, err, 512)
+        self.h = lib().orc_surface_new(_p(s, C.c_double), len(s), probe, spacing, brick, KINDS[kind], err, 512)
         if not self.h:
             raise ValueError(err.value.decode())
         out = np.zeros(len(STAT_KEYS))

@@ -39,10 +39,13 @@ struct DGrid {
 
 // DArr::pad flags.
 constexpr uint32_t DARR_ROWS_SORTED = 1;  // every neighbour row and circle-blocker list ascends
+// A sphere field (SAS or vdW, field/mod.rs:33-41): min(|x - c| - R) over the
+// spheres, no circles or vertices, every sphere not contained exposed.
+constexpr uint32_t DARR_SPHERES = 2;
 
 // The resident arrangement, internal (Morton) sphere order.
 struct DArr {
-    uint32_t n, nc, nv, pad;
+    uint32_t n, nc, nv, flags;  // DARR_* bits
     const double4* sph;      // centre x, y, z, expanded radius R
     const double* rvdw;      // vdW radius r
     const uint32_t* status;  // STATUS_*
@@ -65,7 +68,7 @@ struct DLat {
     double rho_sub;          // 0.5 sqrt(3) sub h
     double rho_brick;        // 0.5 sqrt(3) b h
     float h32, band32, probe32, cutoff2;
-    int b, sub, spb, pad;    // brick edge, sub-block edge, samples per brick
+    int b, sub, spb, kind;   // brick edge, sub-block edge, samples per brick; 1: a sphere field
 };
 
 // geom/cells.rs:91-104 on one axis.
@@ -246,6 +249,7 @@ __device__ inline int uniform_sign_warp(const DArr& A, double x, double y, doubl
     });
     s_sas = warp_min(s_sas);
     s_vdw = warp_min(s_vdw);
+    if (A.flags & DARR_SPHERES) return s_sas > margin ? 1 : (s_sas < -margin ? 0 : -1);  // lattice.rs:213-215
     if (s_sas >= margin) return 1;
     if (s_vdw <= -margin) return 0;
     double cutoff = A.probe + margin + CLASSIFY_EPS;

@@ -238,7 +238,7 @@ constexpr int X_HINT_SLACK = 4;
 template <bool WIDE>
 __device__ bool x_blockers(const DArr& A, unsigned char* base, size_t cap, size_t tail, uint32_t tid, uint32_t T,
                            XView& v) {
-    const bool sorted = A.pad & DARR_ROWS_SORTED;
+    const bool sorted = A.flags & DARR_ROWS_SORTED;
     x_blocker_counts(v, v.s_id, v.ns, A.nb_off, A.nb_items, v.s_off, sorted, tid, T);
     x_blocker_counts(v, v.c_id, v.nc, A.cb_off, A.cb_items, v.c_off, sorted, tid, T);
     x_sync<WIDE>();
@@ -320,6 +320,52 @@ __device__ bool x_ball_from_ids(const DArr& A, double cx, double cy, double cz, 
     return x_blockers<WIDE>(A, base, cap, tail, tid, T, v);
 }
 
+// gather_local of a sphere field (point.rs:566-579): the spheres not
+// contained with |b - c| - R < band + rho, by (that value, index), into
+// in_c (centre, R), s_id and s_key; ni = ns = their count.
+template <bool WIDE>
+__device__ bool x_ball_spheres(const DArr& A, const DLat& L, double cx, double cy, double cz, double rho,
+                               unsigned char* base, size_t cap, uint32_t* cnt, uint32_t tid, uint32_t T, XView& v) {
+    const double reach = L.band + rho;
+    x_sync<WIDE>();
+    if (tid < 8) cnt[tid] = 0;
+    x_sync<WIDE>();
+    x_for_near(A.gs, cx, cy, cz, reach + A.max_expanded, tid, T, [&](uint32_t k) {
+        if (A.status[k] == STATUS_CONTAINED) return;
+        const double4 c = A.sph[k];
+        if (dist3(cx, cy, cz, c.x, c.y, c.z) - c.w < reach) atomicAdd(&cnt[0], 1u);
+    });
+    x_sync<WIDE>();
+    const uint32_t n = cnt[0];
+    size_t tail = 0;
+    const size_t need = x_layout(XCounts{0, n, n, 0, 0}, base, v, &tail);
+    x_sync<WIDE>();
+    if (need > cap) return false;
+    if (tid < 8) cnt[tid] = 0;
+    x_sync<WIDE>();
+    x_for_near(A.gs, cx, cy, cz, reach + A.max_expanded, tid, T, [&](uint32_t k) {
+        if (A.status[k] == STATUS_CONTAINED) return;
+        const double4 c = A.sph[k];
+        const double key = dist3(cx, cy, cz, c.x, c.y, c.z) - c.w;
+        if (key < reach) {
+            const uint32_t p = atomicAdd(&cnt[0], 1u);
+            if (p < n) v.t_key[p] = key, v.t_id[p] = k;
+        }
+    });
+    x_sync<WIDE>();
+    for (uint32_t i = tid; i < n; i += T) {
+        const double key = v.t_key[i];
+        const uint32_t id = v.t_id[i];
+        uint32_t r = 0;
+        for (uint32_t q = 0; q < n; q++) r += (v.t_key[q] < key || (v.t_key[q] == key && v.t_id[q] < id)) ? 1u : 0u;
+        v.in_c[r] = A.sph[id];
+        v.s_id[r] = id;
+        v.s_key[r] = key;
+    }
+    x_sync<WIDE>();
+    return true;
+}
+
 template <bool WIDE>
 __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsigned char* base, size_t cap,
                        uint32_t* cnt, uint32_t tid, uint32_t T, XView& v, const uint32_t* hint = nullptr,
@@ -335,6 +381,7 @@ __device__ bool x_ball(const DArr& A, const DLat& L, int4 key, uint32_t j, unsig
     const double rho = 0.5 * sqrt(3.0) * subd * h * (1.0 + 1e-9) + 1e-9;
     const double reach = A.probe + L.band + rho;
     v.cx = cx, v.cy = cy, v.cz = cz, v.rho = rho;
+    if (A.flags & DARR_SPHERES) return x_ball_spheres<WIDE>(A, L, cx, cy, cz, rho, base, cap, cnt, tid, T, v);
     bool hinted = hint && hint[R_FLAGS] == 0;
     if (hinted && ids && window && window[j] == 0 && slack > 0)
         return x_ball_from_ids<WIDE>(A, cx, cy, cz, rho, base, cap, tid, T, v, hint, ids + hint[R_IDS]);
@@ -748,6 +795,53 @@ __device__ __forceinline__ XEval x_eval_group(const XView& v, const double* circ
     return e;
 }
 
+// eval_local of a sphere field (point.rs:723-736): the least |x - c| - R
+// over the ball's spheres, band when none is below it; the closest point
+// carries the minimising sphere's centre (the gradient's x - c).  COUNT: 9
+// per sphere.
+template <bool COUNT = false>
+__device__ __forceinline__ XEval x_eval_spheres(const XView& v, double band, double x, double y, double z,
+                                                unsigned long long* ops = nullptr) {
+    XEval e;
+    e.qx = x, e.qy = y, e.qz = z, e.kind = XF_BEYOND, e.id = 0;
+    double best = band;
+    for (uint32_t i = 0; i < v.ni; i++) {
+        const double4 c = v.in_c[i];
+        const double val = dist3(x, y, z, c.x, c.y, c.z) - c.w;
+        if (val < best) best = val, e.kind = XF_SPHERE, e.id = v.s_id[i], e.qx = c.x, e.qy = c.y, e.qz = c.z;
+    }
+    if (COUNT) *ops += 9ull * v.ni;
+    e.value = best;
+    return e;
+}
+
+// The same by a group of RG lanes (x_eval_group's rules: the least value,
+// the earliest sphere on ties, so the result is the one-lane walk's).
+template <int RG>
+__device__ __forceinline__ XEval x_eval_spheres_group(const XView& v, double band, double x, double y, double z,
+                                                      int gl, uint32_t gm) {
+    const double inf = __longlong_as_double(0x7ff0000000000000LL);
+    XEval e;
+    e.qx = x, e.qy = y, e.qz = z, e.kind = XF_BEYOND, e.id = 0;
+    double best = band;
+    for (uint32_t i0 = 0; i0 < v.ni; i0 += RG) {
+        const uint32_t i = i0 + gl;
+        double val = inf;
+        if (i < v.ni) {
+            const double4 c = v.in_c[i];
+            val = dist3(x, y, z, c.x, c.y, c.z) - c.w;
+        }
+        int w = int(i);
+        x_argmin<RG>(gm, val, w);
+        if (val < best) {
+            const double4 c = v.in_c[w];
+            best = val, e.kind = XF_SPHERE, e.id = v.s_id[w], e.qx = c.x, e.qy = c.y, e.qz = c.z;
+        }
+    }
+    e.value = best;
+    return e;
+}
+
 __device__ __forceinline__ double x_clamp(double v, double lo, double hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 // The atom nearest to p among ids (extract.rs:566-576): its input index.
@@ -793,7 +887,16 @@ __device__ void x_attributes(const DArr& A, const DLat& L, const ExactAttr& X, u
     if (!(fa < 0.0)) ox = dx * -1.0, oy = dy * -1.0, oz = dz * -1.0;
     const double on = sqrt(ox * ox + oy * oy + oz * oz);
     ox = ox / on, oy = oy / on, oz = oz / on;
-    if (kind == XF_SPHERE || kind == XF_CIRCLE || kind == XF_VERTEX) {
+    if ((A.flags & DARR_SPHERES) && kind == XF_SPHERE) {  // extract.rs:583-587: unit(v - c)
+        const double4 c = A.sph[id];
+        nx = px - c.x, ny = py - c.y, nz = pz - c.z;
+        const double nl = sqrt(nx * nx + ny * ny + nz * nz);
+        if (nl > 1e-9) nx = nx / nl, ny = ny / nl, nz = nz / nl;
+        else nx = ox, ny = oy, nz = oz;
+        atom = X.orig[id], patch = 0;
+        return;
+    }
+    if ((A.flags & DARR_SPHERES) == 0 && (kind == XF_SPHERE || kind == XF_CIRCLE || kind == XF_VERTEX)) {
         nx = qx - px, ny = qy - py, nz = qz - pz;
         const double nl = sqrt(nx * nx + ny * ny + nz * nz);
         if (nl > 1e-9) nx = nx / nl, ny = ny / nl, nz = nz / nl;
@@ -834,10 +937,16 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
     int side = 0;
     bool converged = false;
     uint32_t evals = 0;
+    const bool spheres = A.flags & DARR_SPHERES;
+    auto eval = [&](double x, double y, double z) {
+        if (spheres)
+            return RG == 1 ? x_eval_spheres<COUNT>(v, band, x, y, z, ops) : x_eval_spheres_group<RG>(v, band, x, y, z, gl, gm);
+        return RG == 1 ? x_eval<COUNT>(v, A.circ, probe, band, x, y, z, ops)
+                       : x_eval_group<RG>(v, A.circ, probe, band, x, y, z, gl, gm);
+    };
     for (int it = 0; it < X_MAX_ITER; it++) {
         const double x = pax + dx * t, y = pay + dy * t, z = paz + dz * t;
-        const XEval e = RG == 1 ? x_eval<COUNT>(v, A.circ, probe, band, x, y, z, ops)
-                                : x_eval_group<RG>(v, A.circ, probe, band, x, y, z, gl, gm);
+        const XEval e = eval(x, y, z);
         evals++;
         last = e;
         const double g = e.value;
@@ -856,7 +965,10 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
         }
         double slope = 0.0;
         if (e.kind != XF_SOLVENT && e.kind != XF_BEYOND) {
-            const double wx = e.qx - x, wy = e.qy - y, wz = e.qz - z;
+            // gradient (extract.rs:539-549): towards the closest point (SES)
+            // or away from the sphere's centre (a sphere field).
+            const double wx = spheres ? x - e.qx : e.qx - x, wy = spheres ? y - e.qy : e.qy - y,
+                         wz = spheres ? z - e.qz : e.qz - z;
             const double len = sqrt(wx * wx + wy * wy + wz * wz);
             if (len > 1e-12) slope = (wx / len) * dx + (wy / len) * dy + (wz / len) * dz;
         }
@@ -874,8 +986,7 @@ __device__ __forceinline__ void x_edge(const XView& v, const DArr& A, const DLat
         for (int it = 0; it < X_MAX_BISECT; it++) {
             t = 0.5 * (t0 + t1);
             const double x = pax + dx * t, y = pay + dy * t, z = paz + dz * t;
-            const XEval e = RG == 1 ? x_eval<COUNT>(v, A.circ, probe, band, x, y, z, ops)
-                                    : x_eval_group<RG>(v, A.circ, probe, band, x, y, z, gl, gm);
+            const XEval e = eval(x, y, z);
             evals++;
             last = e;
             if (fabs(e.value) <= X_TOL || (t1 - t0) * len <= 2.0 * X_TOL) break;

@@ -337,7 +337,11 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
     const double bx = px + (double(sb & 1) * sub + half) * h, by = py + (double((sb >> 1) & 1) * sub + half) * h,
                  bz = pz + (double((sb >> 2) & 1) * sub + half) * h;
     const double rho = L.rho_sub;
-    const double reach = A.probe + L.band + rho;
+    // A sphere field gathers the near spheres alone, within band + rho
+    // (gather_spheres, field/kernel.rs:651-654).
+    const bool spheres = A.flags & DARR_SPHERES;
+    const double reach_probe = spheres ? 0.0 : A.probe;
+    const double reach = reach_probe + L.band + rho;
     // The exact refinement's ball (exact.cu x_ball: rho with a relative and
     // an absolute 1e-9 margin).  With O.window the scans cover its larger
     // boxes (the extra cells hold nothing this ball keeps, so the lists and
@@ -345,7 +349,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
     // it; a disagreement marks the sub-block.
     const bool win = O.window != nullptr;
     const double rho_x = 0.5 * sqrt(3.0) * sub * h * (1.0 + 1e-9) + 1e-9;
-    const double reach_x = A.probe + L.band + rho_x;
+    const double reach_x = reach_probe + L.band + rho_x;
     const double r_sph = win ? reach_x + A.max_expanded : reach + A.max_expanded;
     const double r_circ = win ? reach_x + A.rho_max : reach + A.rho_max, r_vert = win ? reach_x : reach;
     bool differ = false;
@@ -374,7 +378,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
                 const bool near = !(d >= c.w + reach);
                 keep = near && (contains == (pass == 0));
                 if (win && pass == 0) {
-                    const bool exposed = A.status[k] == STATUS_EXPOSED;
+                    const bool exposed = !spheres && A.status[k] == STATUS_EXPOSED;
                     const double lb = fabs(d - c.w);
                     differ |= (d < c.w + reach_x) != near || (d < c.w + rho_x) != contains ||
                               (exposed && lb <= reach_x) != (exposed && near && lb <= reach);
@@ -405,7 +409,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         bool p = false;
         double lb = 0;
         uint32_t k = 0;
-        if (i < nn) {
+        if (i < nn && !spheres) {
             k = near_ids[i];
             if (A.status[k] == STATUS_EXPOSED) {
                 double4 c = A.sph[k];
@@ -544,7 +548,8 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         float r32 = float(c.w);
         float rt = fmaxf(r32 - INSIDE_TOL, 0.0f);
         p_nearA[i] = make_float4(x, y, z, r32 * r32);
-        p_nearT[i] = make_float4(x, y, z, rt * rt);
+        // A sphere field has no blockers: its samples take R itself.
+        p_nearT[i] = make_float4(x, y, z, spheres ? r32 : rt * rt);
     }
     for (int r = lane; r <= ns; r += 32) w_soff[r] = s_off[r], p_soff[r] = s_off[r];
     // Pruning keys: every sample the sub-block evaluates lies within rho of
@@ -731,6 +736,40 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
     // COUNT: arithmetic operations as executed (the algorithmic count of the
     // roofline; compares and selects are not counted).
     unsigned long long ops = 0, owned = 0;
+    if (L.kind) {
+        // A sphere field (sphere_kernel, field/kernel.rs:957-981): the least
+        // |x - c| - R over every near sphere, clamped at band; nearT holds
+        // (x, y, z, R).  COUNT: 9 per sphere.
+        const float band = L.band32;
+        for (int t = threadIdx.x; t < sp * sp * sp; t += blockDim.x) {
+            int x = ox + t % sp, y = oy + (t / sp) % sp, z = oz + t / (sp * sp);
+            bool positive;
+            if (sample_owner(x, y, z, sub, st, &positive) != int(sb)) continue;
+            const float px = float(gx + x) * L.h32, py = float(gy + y) * L.h32, pz = float(gz + z) * L.h32;
+            if (COUNT) owned++, ops += 9ull * nn;
+            float best = band;
+            uint32_t fi = 0xFFFFFFFFu;
+            for (int k = 0; k < nn; k++) {
+                const float4 a = nearT[k];
+                const float dx = px - a.x, dy = py - a.y, dz = pz - a.z;
+                const float v = sqrtf(dx * dx + dy * dy + dz * dz) - a.w;
+                if (FEAT) {
+                    if (v < best) best = v, fi = uint32_t(k);
+                } else {
+                    best = fminf(best, v);
+                }
+            }
+            out[(z * side + y) * side + x] = best;
+            if (FEAT)
+                feats[size_t(brick) * L.spb + (z * side + y) * side + x] =
+                    fi == 0xFFFFFFFFu ? (1u << FEAT_SHIFT_D) : ((2u << FEAT_SHIFT_D) | ids[R[R_IDS] + fi]);
+        }
+        if (COUNT) {
+            atomicAdd(&counters[CNT_OPS], ops);
+            atomicAdd(&counters[CNT_OWNED], owned);
+        }
+        return;
+    }
     for (int t = threadIdx.x; t < sp * sp * sp; t += blockDim.x) {
         int x = ox + t % sp, y = oy + (t / sp) % sp, z = oz + t / (sp * sp);
         bool positive;
@@ -1076,6 +1115,11 @@ struct RefStage {
     // region has no room for the S keys (then neither list is pruned).
     const float* s_key;
     float cx, cy, cz, rho;
+    // A sphere field: every near sphere is a candidate (eval_point's
+    // non-SES branch, sesmesh.cuh:486-503); near_id their ids.
+    int nn;
+    const uint32_t* near_id;
+    bool spheres;
 };
 
 // One warp (BLOCK = false) or the whole block: stages work item j's
@@ -1164,7 +1208,7 @@ __device__ RefStage stage_candidates(const DArr& A, const DLat& L, const BrickFr
     if (BLOCK) __syncthreads();
     else __syncwarp();
     return RefStage{nearA, nearT, S,  C,  V,  s_id, s_off, s_blk, c_off, c_blk, n_in, ns, nc, nv,
-                    keyed ? s_key : nullptr, cx, cy, cz, rho};
+                    keyed ? s_key : nullptr, cx, cy, cz, rho, nn, l_near, (A.flags & DARR_SPHERES) != 0};
 }
 
 struct Eval {
@@ -1197,6 +1241,29 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
     static_assert(RG == 1 || RG == 8 || RG == 32, "groups of 1, 8 or 32 lanes");
     Eval e;
     e.qx = x, e.qy = y, e.qz = z;
+    if (st.spheres) {
+        // min(band, min |x - c| - R) over the near spheres; q carries the
+        // minimising sphere's centre for the slope (the refinement writes x).
+        float best = band;
+        e.feat = 1u << FEAT_SHIFT_D;
+        for (int k0 = 0; k0 < st.nn; k0 += RG) {
+            const int k = k0 + gl;
+            float v = INFINITY;
+            if (k < st.nn) {
+                const float4 a = st.nearA[k];
+                const float dx = x - a.x, dy = y - a.y, dz = z - a.z;
+                v = sqrtf(dx * dx + dy * dy + dz * dz) - a.w;
+            }
+            int w = k;
+            group_argmin<RG>(gm, v, w);
+            if (v < best) {
+                const float4 a = st.nearA[w];
+                best = v, e.feat = (2u << FEAT_SHIFT_D) | st.near_id[w], e.qx = a.x, e.qy = a.y, e.qz = a.z;
+            }
+        }
+        e.value = best;
+        return e;
+    }
     bool inside = false;
     for (int k0 = 0; k0 < st.n_in; k0 += RG) {
         const int k = k0 + gl;
@@ -1370,7 +1437,10 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
         float slope = 0.0f;
         uint32_t kind = e.feat >> FEAT_SHIFT_D;
         if (kind != 0 && kind != 1) {
+            // slope_of (sesmesh.cuh:599-618): towards the closest point (SES),
+            // away from the sphere's centre (a sphere field).
             float wx = e.qx - x, wy = e.qy - y, wz = e.qz - z;
+            if (st.spheres) wx = -wx, wy = -wy, wz = -wz;
             float len = sqrtf(wx * wx + wy * wy + wz * wz);
             if (len > 1e-12f) slope = ((axis == 0 ? wx : (axis == 1 ? wy : wz)) / len) * h;
         }
@@ -1396,6 +1466,10 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
         }
     }
     if (gl) return;
+    if (st.spheres) {  // a sphere field's closest point is the evaluated point (sesmesh.cuh:499-501)
+        last.qx = ax + (axis == 0 ? hd * t : 0.0f), last.qy = ay + (axis == 1 ? hd * t : 0.0f),
+        last.qz = az + (axis == 2 ? hd * t : 0.0f);
+    }
     out.t[k] = t;
     out.feat[k] = last.feat;
     out.q[3 * size_t(k)] = last.qx, out.q[3 * size_t(k) + 1] = last.qy, out.q[3 * size_t(k) + 2] = last.qz;

@@ -746,7 +746,7 @@ int build_arrangement_device(smb_device* d, const double* xyzr, size_t ns, doubl
     count_launches(7);
     A.nb_off = nb_off, A.nb_items = nb_items;
     A.nc = uint32_t(nc), A.nv = uint32_t(nv);
-    A.pad = DARR_ROWS_SORTED;  // rows sorted in k_rows, blockers listed in row order
+    A.flags = DARR_ROWS_SORTED;  // rows sorted in k_rows, blockers listed in row order
     A.circ = circ, A.cb_off = cb_off, A.cb_items = cb_items, A.vert = vert;
     out.circle_ij = ij, out.vertex_atoms = vatoms;
     out.n_circles = nc, out.n_vertices = nv, out.nb_items = size_t(h_nb), out.cb_items = ncb;

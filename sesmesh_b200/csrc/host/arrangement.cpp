@@ -202,8 +202,9 @@ struct SpherePart {
 
 }  // namespace
 
-std::string check_spheres(const double* xyzr, size_t ns, double probe) {
-    if (!(std::isfinite(probe) && probe > 0.0)) return "probe radius must be finite and > 0 for the SES";
+std::string check_spheres(const double* xyzr, size_t ns, double probe, int kind) {
+    if (kind == 0 && !(std::isfinite(probe) && probe > 0.0)) return "probe radius must be finite and > 0 for the SES";
+    if (!(std::isfinite(probe) && probe >= 0.0)) return "probe radius must be finite and >= 0";
     for (size_t i = 0; i < ns; i++) {
         const double* s = xyzr + 4 * i;
         if (!(std::isfinite(s[0]) && std::isfinite(s[1]) && std::isfinite(s[2])))
@@ -215,13 +216,18 @@ std::string check_spheres(const double* xyzr, size_t ns, double probe) {
 
 const char* const CANCELLED = "cancelled";
 
-std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arrangement& A, const Control* ctl) {
-    std::string bad = check_spheres(xyzr, ns, probe);
+// kind != 0: a sphere field (SAS, or vdW with probe 0): containment alone,
+// every sphere not contained exposed, no circles or vertices
+// (arrangement.rs:437-646 with with_circles false, point.rs:229-237).
+std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arrangement& A, const Control* ctl,
+                              int kind) {
+    std::string bad = check_spheres(xyzr, ns, probe, kind);
     if (!bad.empty()) return bad;
     // The flag is polled per sphere in every pass (control.rs:94-131).
     auto stop = [&] { return ctl && ctl->cancelled(); };
     if (stop()) return CANCELLED;
     A = Arrangement();
+    A.kind = kind;
     A.probe = probe;
     std::vector<uint32_t> active;
     for (size_t i = 0; i < ns; i++)
@@ -274,6 +280,20 @@ std::string build_arrangement(const double* xyzr, size_t ns, double probe, Arran
     });
     for (uint8_t c : contained) A.n_contained += c;
     if (stop()) return CANCELLED;
+    if (kind != 0) {
+        A.status.resize(n);
+        for (size_t i = 0; i < n; i++) A.status[i] = contained[i] ? CONTAINED : EXPOSED;
+        A.nb_off.assign(n + 1, 0);
+        A.cb_off.assign(1, 0);
+        A.circle_cells.build(A.circle.data(), 0, 10, cell);
+        A.vertex_cells.build(A.vertex.data(), 0, 3, cell);
+        if (n) {
+            V3 lo = A.c(0), hi = lo;
+            for (size_t i = 0; i < n; i++) lo = lo.lo(A.c(uint32_t(i))), hi = hi.hi(A.c(uint32_t(i)));
+            A.extent = (hi - lo).norm() + 4.0 * max_expanded + 4.0 * probe + 1.0;
+        }
+        return "";
+    }
 
     // Neighbour rows, ascending (arrangement.rs:522-545).
     std::vector<std::vector<uint32_t>> rows(n);

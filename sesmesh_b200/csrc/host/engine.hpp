@@ -50,7 +50,7 @@ struct smb_engine {
     smb::MeasureScratch measure;    // device buffers of the validation and measure
     // Warm-start training rows of the last device run.
     bool rows_ready = false;
-    std::vector<float> row_x, row_t;
+    std::vector<float> row_x, row_t, row_p;
 };
 
 // The engine's host arrangement (copied from the device on first use when

@@ -73,7 +73,8 @@ enum : uint32_t { EXPOSED = 0, BURIED = 1, CONTAINED = 2 };
 // The SAS arrangement for one probe radius (geom/arrangement.rs:205-228),
 // internal Morton order, flat arrays in the upload layout.
 struct Arrangement {
-    double probe = 0;
+    int kind = 0;     // SMB_KIND_SES, SMB_KIND_SAS or SMB_KIND_VDW (a sphere field: no circles or vertices)
+    double probe = 0;  // the probe the spheres were expanded by (0 for the vdW surface)
     size_t n = 0, n_contained = 0;
     std::vector<double> center, expanded, radius;  // center: 3 per sphere
     std::vector<uint32_t> orig, status;
@@ -109,9 +110,9 @@ extern const char* const CANCELLED;
 // Builds the SES arrangement of n spheres (x, y, z, r rows); error text or
 // "" (CANCELLED when ctl's flag was set before it finished).
 std::string build_arrangement(const double* xyzr, size_t n, double probe, Arrangement& out,
-                              const Control* ctl = nullptr);
+                              const Control* ctl = nullptr, int kind = 0);
 // The input checks of build_arrangement alone; error text or "".
-std::string check_spheres(const double* xyzr, size_t n, double probe);
+std::string check_spheres(const double* xyzr, size_t n, double probe, int kind = 0);
 
 void set_threads(int n);
 int threads();

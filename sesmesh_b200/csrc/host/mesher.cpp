@@ -88,7 +88,12 @@ void attributes(const Arrangement& A, const MeshParams& P, const V3& v, const Ne
         }
         return A.orig[bi];
     };
-    switch (e.feature.kind) {
+    if (A.kind != 0 && e.feature.kind == F_SPHERE) {  // extract.rs:583-587
+        normal = unit(v - A.c(e.feature.id)), patch = 0, atom = A.orig[e.feature.id];
+        return;
+    }
+    const uint32_t kind = A.kind != 0 ? uint32_t(F_BEYOND) : uint32_t(e.feature.kind);
+    switch (kind) {
         case F_SPHERE:
             normal = unit(e.closest - v), patch = 0, atom = A.orig[e.feature.id];
             return;
@@ -143,7 +148,7 @@ Vertex refine_edge(const Arrangement& A, const MeshParams& P, const V3& pa, cons
         }
         double slope = 0.0;  // gradient (extract.rs:539-549) along the edge
         if (e.feature.kind != F_SOLVENT && e.feature.kind != F_BEYOND) {
-            V3 w = e.closest - x;
+            V3 w = A.kind != 0 ? x - A.c(e.feature.id) : e.closest - x;
             double len = w.norm();
             if (len > 1e-12) slope = (w / len).dot(d);
         }
@@ -243,6 +248,17 @@ void gather_local(const Arrangement& A, const V3& b, double rho, double band, Lo
     out.c_blk.clear(), out.vertices.clear(), out.order.clear();
     out.s_key.clear(), out.c_key.clear(), out.v_key.clear();
     out.s_off.assign(1, 0), out.c_off.assign(1, 0);
+    if (A.kind != 0) {  // point.rs:566-579: sphere fields, by (centre value, index)
+        const double reach = band + rho;
+        A.cells.near(b, reach + A.max_expanded, [&](uint32_t k) {
+            if (A.status[k] != CONTAINED && b.dist(A.c(k)) - A.expanded[k] < reach)
+                out.order.push_back({b.dist(A.c(k)) - A.expanded[k], k});
+        });
+        nearest_first(out.order);
+        for (auto& o : out.order) out.inside.push_back(o.second);
+        out.order.clear();
+        return;
+    }
     const double reach = A.probe + band + rho;
     A.cells.near(b, reach + A.max_expanded, [&](uint32_t k) {
         if (A.status[k] == CONTAINED) return;
@@ -291,6 +307,20 @@ void gather_local(const Arrangement& A, const V3& b, double rho, double band, Lo
 
 // point.rs:686-738 (SES)
 NearEval eval_local(const Arrangement& A, const V3& x, double band, const Local& l) {
+    if (A.kind != 0) {  // point.rs:723-736
+        double best = band;
+        int64_t bi = -1;
+        for (uint32_t k : l.inside) {
+            double v = x.dist(A.c(k)) - A.expanded[k];
+            if (v < best) best = v, bi = k;
+        }
+        NearEval r;
+        r.value = best;
+        r.feature.kind = bi < 0 ? F_BEYOND : F_SPHERE;
+        r.feature.id = bi < 0 ? 0u : uint32_t(bi);
+        r.closest = x;
+        return r;
+    }
     bool inside = false;
     for (uint32_t k : l.inside)
         if (x.dist(A.c(k)) < A.expanded[k]) {

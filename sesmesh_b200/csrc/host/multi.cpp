@@ -573,9 +573,12 @@ int smb_multi_new(smb_device* dev, size_t n, const double* const* xyzr, const si
     if (c.caps_level > 1) return set_err(err, errlen, "caps level must be 0 or 1"), SMB_ERR_ARG;
     if (c.gather_warps && c.gather_warps != 1 && c.gather_warps != 2 && c.gather_warps != 4 && c.gather_warps != 8)
         return set_err(err, errlen, "gather warps must be 0 (tuned), 1, 2, 4 or 8"), SMB_ERR_ARG;
-    for (size_t i = 0; i < n; i++)
+    for (size_t i = 0; i < n; i++) {
         if (params[i].refine != SMB_REFINE_FAST)
             return set_err(err, errlen, "structure %zu: the batch meshes in fast mode", i), SMB_ERR_ARG;
+        if (params[i].kind != SMB_SES || !(params[i].probe_radius > 0.0))
+            return set_err(err, errlen, "structure %zu: the batch meshes the SES (probe > 0)", i), SMB_ERR_ARG;
+    }
     auto t0 = clk::now();
     auto m = std::make_unique<smb_multi>();
     m->dev = dev;

@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 
 #include "../../../include/sesmesh_b200.h"
@@ -114,27 +115,30 @@ extern "C" {
 void smb_set_device_arrangement_min(size_t n) { g_device_arrangement_min = n; }
 
 uint64_t smb_device_bytes_estimate(size_t surface_bricks, uint32_t brick, double spacing, double probe,
-                                   int refine) {
-    // Per surface brick: sample values (and the warm start's feature words),
-    // sub-block records and work lists, the candidate lists of its sampled
-    // sub-blocks, and its share of the crossing edges (marching-cubes
-    // outputs, refinement outputs or exact vertices, the finished mesh and
-    // the measure's tables) with two triangles per edge.  The candidate
-    // count of a sub-block's ball is taken at 0.06 spheres per A^3 (above
-    // protein packing) within the largest ball any of its lists uses; 250
-    // bytes per candidate cover its list entries, blockers and packed
-    // coordinates.  The crossing edges of a brick are taken as 1.5 b^2
-    // (a surface crossing it diagonally).
+                                   size_t spheres, int refine, int multiprocessors) {
+    // Measured on B200 (globules of 330 and 2,800 spheres at 0.1 to 1 A,
+    // exact and fast mode) and rounded up:
+    // * fixed: the exact refinement's global list slabs (256 KiB for each of
+    //   4 warps of 4 CTAs per SM) and about 200 MB of classification,
+    //   queue, scan and measure tables;
+    // * per sampled sub-block (at most 6 per surface brick counted): its
+    //   candidate lists, at least the 12 KiB the gather's pools start from,
+    //   else 250 bytes for each sphere of its largest ball at 0.05 spheres
+    //   per A^3 (at most every sphere), with the pools' 25 % growth margins;
+    // * per surface brick: its sample values (and the warm start's feature
+    //   words), records and work lists;
+    // * per crossing edge (2 b^2 per brick counted): the marching-cubes,
+    //   refinement, vertex, triangle and measure arrays.
     const double b = double(brick), sub = 0.5 * b;
     const double spb = (b + 1) * (b + 1) * (b + 1);
     const double band = std::sqrt(3.0) * spacing * 1.01, rho = 0.5 * std::sqrt(3.0) * sub * spacing;
     const double r_ball = 1.8 + probe + probe + band + rho;
-    const double per_ball = 0.06 * 4.18879020478639 * r_ball * r_ball * r_ball * 250.0;
-    const double edges = 1.5 * b * b;
-    const double per_edge = 4 + 8 + 4 + 4 + (refine == SMB_REFINE_FAST ? 28.0 : 37.0) + 2 * 12 + 64;
-    const double per_brick = spb * (refine == SMB_REFINE_FAST ? 8.0 : 4.0) + 8 * (SMB_REC_WORDS * 4 + 16) +
-                             8 * per_ball + edges * per_edge;
-    return uint64_t(double(surface_bricks) * per_brick) + (uint64_t(64) << 20);
+    const double in_ball = std::min(double(spheres), 0.05 * 4.18879020478639 * r_ball * r_ball * r_ball);
+    const double per_sub = std::max(12288.0, 250.0 * in_ball) * 1.5625;
+    const double per_brick = 6.0 * per_sub + spb * (refine == SMB_REFINE_FAST ? 8.0 : 4.0) * 1.25 +
+                             8.0 * (SMB_REC_WORDS * 4 + 16) * 1.25 + 2.0 * b * b * 320.0;
+    const uint64_t slabs = uint64_t(std::max(multiprocessors, 1)) * 4 * 4 * (uint64_t(256) << 10);
+    return uint64_t(double(surface_bricks) * per_brick) + slabs + (uint64_t(224) << 20);
 }
 
 int smb_engine_new(smb_device* dev, const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out,
@@ -176,7 +180,8 @@ int smb_engine_new_with(smb_device* dev, const double* xyzr, size_t n, const smb
                         const smb_control* control, smb_engine** out, char* err, size_t errlen) {
     if (!dev || !p || !out || (n && !xyzr)) return set_err(err, errlen, "null argument"), SMB_ERR_ARG;
     *out = nullptr;
-    if (p->kind != SMB_SES) return set_err(err, errlen, "only the SES is meshed on the device"), SMB_ERR_ARG;
+    if (p->kind != SMB_SES && p->kind != SMB_SAS && p->kind != SMB_VDW)
+        return set_err(err, errlen, "unknown surface kind %d", p->kind), SMB_ERR_ARG;
     if (p->refine != SMB_REFINE_EXACT && p->refine != SMB_REFINE_FAST)
         return set_err(err, errlen, "refine mode must be exact or fast on the device"), SMB_ERR_ARG;
     if (!(p->spacing >= 0.01) || !std::isfinite(p->spacing))
@@ -187,9 +192,15 @@ int smb_engine_new_with(smb_device* dev, const double* xyzr, size_t n, const smb
     auto e = std::make_unique<smb_engine>();
     e->dev = dev;
     e->params = *p;
+    // SurfaceParams::effective_probe (surface.rs:411-417) and SesField::new's
+    // SES with probe 0, the vdW surface (point.rs:224-228).
+    if (e->params.kind == SMB_SES && p->probe_radius == 0.0) e->params.kind = SMB_VDW;
+    if (e->params.kind == SMB_VDW) e->params.probe_radius = 0.0;
+    const int kind = e->params.kind;
+    const double probe = e->params.probe_radius;
     set_control(e.get(), control);
     auto t0 = clk::now();
-    std::string m = check_spheres(xyzr, n, p->probe_radius);
+    std::string m = check_spheres(xyzr, n, probe, kind);
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
     const Control& ctl = e->ctl;
     if (ctl.cancelled()) return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
@@ -197,12 +208,12 @@ int smb_engine_new_with(smb_device* dev, const double* xyzr, size_t n, const smb
     // The arrangement: on the device for large inputs (the host builds it
     // when the device declines), else on the host threads.
     bool on_device = false;
-    if (n >= g_device_arrangement_min) {
+    if (n >= g_device_arrangement_min && kind == SMB_SES) {
         std::string why;
-        on_device = smb::build_arrangement_device(dev, xyzr, n, p->probe_radius, e->darr, &why) == 0;
+        on_device = smb::build_arrangement_device(dev, xyzr, n, probe, e->darr, &why) == 0;
     }
     if (!on_device) {
-        m = build_arrangement(xyzr, n, p->probe_radius, e->arr, &ctl);
+        m = build_arrangement(xyzr, n, probe, e->arr, &ctl, kind);
         if (m == CANCELLED) return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
         if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
     }
@@ -238,14 +249,14 @@ int smb_engine_new_with(smb_device* dev, const double* xyzr, size_t n, const smb
     P.frame[0] = to_i64(std::round(center.x / P.h));
     P.frame[1] = to_i64(std::round(center.y / P.h));
     P.frame[2] = to_i64(std::round(center.z / P.h));
-    double reach = half + 2.0 * max_expanded + 2.0 * p->probe_radius + 4.0 * double(P.b) * P.h;
+    double reach = half + 2.0 * max_expanded + 2.0 * probe + 4.0 * double(P.b) * P.h;
     P.f32_ok = reach < 2000.0 && reach / P.h < double(1u << 23);
     if (!P.f32_ok)
         return set_err(err, errlen, "extent beyond the f32 frame (%g A): the device path does not take it", reach),
                SMB_ERR_RANGE;
     P.band = std::sqrt(3.0) * P.h * 1.01;
     P.coord_max = std::fmax(std::fmax(std::fabs(center.x), std::fabs(center.y)), std::fabs(center.z)) + half +
-                  max_expanded + p->probe_radius + 2.0 * P.band;
+                  max_expanded + probe + 2.0 * P.band;
     {  // edge_clamp (extract.rs:47-51)
         double cm = P.coord_max < 1.0 ? 1.0 : (P.coord_max > double(3.4028234663852886e38f) / 4.0 ? double(3.4028234663852886e38f) / 4.0 : P.coord_max);
         float mf = float(cm), nx;
@@ -304,6 +315,7 @@ int smb_engine_new_with(smb_device* dev, const double* xyzr, size_t n, const smb
     r.max_expanded = A.max_expanded;
     r.rho_max = A.rho_max;
     r.probe = A.probe;
+    r.kind = kind;
     rc = smb_resident_new(dev, &r, &lat, &e->res, err, errlen);
     if (rc != SMB_OK) return rc;
     rc = smb_batch_new(e->res, &e->batch, err, errlen);
@@ -343,7 +355,7 @@ int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size
     ctl.report(SMB_STAGE_CLASSIFY, 1, 1);
     // The memory guard, before any mesh-stage buffer is taken.
     e->last_estimate = smb_device_bytes_estimate(surface, uint32_t(e->mp.b), e->mp.h, e->params.probe_radius,
-                                                 e->params.refine) +
+                                                 e->n_spheres, e->params.refine, e->dev->info.multiprocessors) +
                        smb_resident_bytes(e->res);
     if (e->max_device_bytes && e->last_estimate > e->max_device_bytes)
         return set_err(err, errlen,
@@ -361,8 +373,10 @@ int smb_engine_run_device(smb_engine* e, smb_batch_times* times, char* err, size
     e->rows_ready = false;
     if (e->params.refine == SMB_REFINE_FAST) {
         double ms = 0;
-        rc = e->warm ? smb_refine_warm(e->res, e->batch, e->warm, &ms, err, errlen)
-                     : smb_refine(e->res, e->batch, &ms, err, errlen);
+        // The warm start's candidates are the SES's features; a sphere
+        // field refines from the linear guess.
+        rc = e->warm && e->params.kind == SMB_SES ? smb_refine_warm(e->res, e->batch, e->warm, &ms, err, errlen)
+                                                  : smb_refine(e->res, e->batch, &ms, err, errlen);
         if (rc != SMB_OK) return rc;
         t.total += ms;
         if (e->exact_device) {
@@ -580,8 +594,8 @@ int smb_engine_set_warm_start(smb_engine* e, const smb_mlp* mlp) {
     return smb_batch_record_features(e->batch, mlp != nullptr);
 }
 
-int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, size_t cap, size_t* n, char* err,
-                               size_t errlen) {
+int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, float* plain, size_t cap, size_t* n,
+                               char* err, size_t errlen) {
     if (!e || !n) return SMB_ERR_ARG;
     if (!e->rows_ready) {
         smb_batch_record_features(e->batch, 1);
@@ -594,10 +608,17 @@ int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, si
         std::vector<float> x(ne * SMB_MLP_FEATURES);
         std::vector<uint8_t> covered(ne);
         if ((rc = smb_batch_edge_features(e->res, e->batch, x.data(), covered.data(), err, errlen)) != SMB_OK) return rc;
+        // Where plain f32 refinement stops (the reference's fast mode).
+        double ms = 0;
+        std::vector<float> tp(ne);
+        std::vector<uint32_t> fp(ne), ep(ne);
+        std::vector<float> qp(3 * ne);
+        if ((rc = smb_refine(e->res, e->batch, &ms, err, errlen)) != SMB_OK) return rc;
+        if (ne && (rc = smb_batch_edges(e->batch, tp.data(), fp.data(), qp.data(), ep.data())) != SMB_OK)
+            return set_err(err, errlen, "edge results copy"), rc;
         // The labels: exact mode's f64 root parameter (before the edge clamp)
         // from the device refinement, which equals the host's bit for bit;
         // edges it leaves to the host (evals = 0) are left out.
-        double ms = 0;
         if ((rc = smb_refine_exact(e->res, e->batch, &ms, err, errlen)) != SMB_OK) return rc;
         std::vector<float> pos(3 * ne), nrm(3 * ne), t(ne);
         std::vector<uint32_t> atoms(ne), evals(ne);
@@ -605,19 +626,21 @@ int smb_engine_warm_start_rows(smb_engine* e, float* features, float* labels, si
         if (ne && (rc = smb_batch_vertices(e->batch, pos.data(), nrm.data(), atoms.data(), patches.data(), t.data(),
                                            evals.data())) != SMB_OK)
             return set_err(err, errlen, "vertex copy"), rc;
-        e->row_x.clear(), e->row_t.clear();
+        e->row_x.clear(), e->row_t.clear(), e->row_p.clear();
         for (size_t k = 0; k < ne; k++) {
             if (!covered[k] || evals[k] == 0) continue;
             e->row_x.insert(e->row_x.end(), x.begin() + k * SMB_MLP_FEATURES, x.begin() + (k + 1) * SMB_MLP_FEATURES);
             e->row_t.push_back(t[k]);
+            e->row_p.push_back((ep[k] & 0x80000000u) ? tp[k] : std::numeric_limits<float>::quiet_NaN());
         }
         e->rows_ready = true;
     }
     *n = e->row_t.size();
-    if (!features || !labels) return SMB_OK;
+    if (!features || !labels || !plain) return SMB_OK;
     if (cap < *n) return set_err(err, errlen, "%zu rows do not fit in %zu", *n, cap), SMB_ERR_MEMORY;
     std::copy(e->row_x.begin(), e->row_x.end(), features);
     std::copy(e->row_t.begin(), e->row_t.end(), labels);
+    std::copy(e->row_p.begin(), e->row_p.end(), plain);
     return SMB_OK;
 }
 
@@ -755,7 +778,12 @@ int smb_arrangement_build_with(const double* xyzr, size_t n, const smb_surface_p
     set_control(e.get(), control);
     set_threads(p->threads);
     e->ctl.report(SMB_STAGE_GEOMETRY, 0, 1);
-    std::string m = build_arrangement(xyzr, n, p->probe_radius, e->arr, &e->ctl);
+    int kind = p->kind;
+    double probe = p->probe_radius;
+    if (kind == SMB_SES && probe == 0.0) kind = SMB_VDW;
+    if (kind == SMB_VDW) probe = 0.0;
+    e->params.kind = kind, e->params.probe_radius = probe;
+    std::string m = build_arrangement(xyzr, n, probe, e->arr, &e->ctl, kind);
     if (m == CANCELLED) return set_err(err, errlen, "cancelled"), SMB_ERR_CANCELLED;
     if (!m.empty()) return set_err(err, errlen, "%s", m.c_str()), SMB_ERR_ARG;
     e->ctl.report(SMB_STAGE_GEOMETRY, 1, 1);

@@ -430,7 +430,8 @@ static bool csr_ok(const uint32_t* off, size_t rows, size_t items) {
 }
 
 // Lattice constants, computed here in the CPU's f64 operation order.
-static void set_lattice(DLat& L, const smb_lattice_ref* lat, double probe) {
+static void set_lattice(DLat& L, const smb_lattice_ref* lat, double probe, int kind) {
+    L.kind = kind != SMB_KIND_SES ? 1 : 0;
     L.h = lat->spacing;
     L.b = int(lat->brick);
     L.sub = L.b / 2;
@@ -456,6 +457,10 @@ int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_latt
     if (!(lat->spacing >= 0.01) || !std::isfinite(lat->spacing))
         return set_err(err, errlen, "grid spacing must be at least 0.01"), SMB_ERR_ARG;
     size_t n = a->n_spheres, nc = a->n_circles, nv = a->n_vertices;
+    if (a->kind != SMB_KIND_SES && a->kind != SMB_KIND_SAS && a->kind != SMB_KIND_VDW)
+        return set_err(err, errlen, "unknown surface kind %d", a->kind), SMB_ERR_ARG;
+    if (a->kind != SMB_KIND_SES && (nc || nv))
+        return set_err(err, errlen, "a sphere field has no circles or vertices"), SMB_ERR_ARG;
     if (n >= (size_t(1) << 32) || nc >= (size_t(1) << 32) || nv >= (size_t(1) << 32))
         return set_err(err, errlen, "too many spheres, circles or vertices"), SMB_ERR_ARG;
     // Shapes, as batch::validate (batch.rs:323-338).
@@ -528,7 +533,7 @@ int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_latt
         for (size_t c = 0; c < nc && sorted; c++)
             for (uint32_t p = a->cb_off[c] + 1; p < a->cb_off[c + 1] && sorted; p++)
                 sorted = a->cb_items[p - 1] < a->cb_items[p];
-        A.pad = sorted ? DARR_ROWS_SORTED : 0u;
+        A.flags = (sorted ? DARR_ROWS_SORTED : 0u) | (a->kind != SMB_KIND_SES ? DARR_SPHERES : 0u);
     }
     void* p;
     if ((rc = up(&p, sph.data(), sph.size() * 8)) != SMB_OK) return fail(rc);
@@ -563,7 +568,7 @@ int smb_resident_new(smb_device* d, const smb_arrangement_ref* a, const smb_latt
         D.items = static_cast<const uint32_t*>(p);
     }
     A.max_expanded = a->max_expanded, A.rho_max = a->rho_max, A.probe = a->probe;
-    set_lattice(r->L, lat, a->probe);
+    set_lattice(r->L, lat, a->probe, a->kind);
     cudaError_t e = cudaStreamSynchronize(d->stream);
     if (e != cudaSuccess) {
         set_err(err, errlen, "upload failed: %s", cudaGetErrorString(e));
@@ -1085,7 +1090,7 @@ int resident_from_device(smb_device* d, DevArrangement& D, const smb_lattice_ref
     r->bytes = D.bytes;
     D.bytes = 0;
     for (int k = 0; k < 3; k++) r->lo[k] = D.lo[k], r->hi[k] = D.hi[k];
-    set_lattice(r->L, lat, D.A.probe);
+    set_lattice(r->L, lat, D.A.probe, SMB_KIND_SES);
     r->xa = ExactAttr{D.orig, D.circle_ij, D.vertex_atoms, 0.0};
     *out = r;
     return SMB_OK;

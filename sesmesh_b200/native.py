@@ -37,7 +37,7 @@ class ArrangementRef(C.Structure):
                 ("n_circles", C.c_size_t), ("circle", C.POINTER(C.c_double)), ("cb_off", C.POINTER(C.c_uint32)),
                 ("cb_items", C.POINTER(C.c_uint32)), ("n_vertices", C.c_size_t), ("vertex", C.POINTER(C.c_double)),
                 ("sphere_grid", GridRef), ("circle_grid", GridRef), ("vertex_grid", GridRef),
-                ("max_expanded", C.c_double), ("rho_max", C.c_double), ("probe", C.c_double)]
+                ("max_expanded", C.c_double), ("rho_max", C.c_double), ("probe", C.c_double), ("kind", C.c_int)]
 
 
 class LatticeRef(C.Structure):
@@ -173,7 +173,7 @@ SIGNATURES = {
     "smb_multi_set_control": (C.c_int, [_vp, C.POINTER(Control_)]),
     "smb_arrangement_build_with": (C.c_int, [C.POINTER(C.c_double), _sz, C.POINTER(SurfaceParams_),
                                              C.POINTER(Control_), C.POINTER(_vp), _cp, _sz]),
-    "smb_device_bytes_estimate": (C.c_uint64, [_sz, C.c_uint32, C.c_double, C.c_double, C.c_int]),
+    "smb_device_bytes_estimate": (C.c_uint64, [_sz, C.c_uint32, C.c_double, C.c_double, _sz, C.c_int, C.c_int]),
     "smb_engine_device_bytes": (C.c_uint64, [_vp]),
     "smb_mlp_set_use": (C.c_int, [_vp, C.c_int]),
     "smb_mlp_forward": (C.c_int, [_vp, _fp, _sz, _fp, _cp, _sz]),
@@ -194,7 +194,7 @@ SIGNATURES = {
     "smb_engine_set_exact_device": (C.c_int, [_vp, C.c_int]),
     "smb_engine_note": (C.c_char_p, [_vp]),
     "smb_engine_field": (C.c_int, [_vp, C.POINTER(C.c_double), _sz, C.POINTER(C.c_double)]),
-    "smb_engine_warm_start_rows": (C.c_int, [_vp, _fp, _fp, _sz, C.POINTER(_sz), _cp, _sz]),
+    "smb_engine_warm_start_rows": (C.c_int, [_vp, _fp, _fp, _fp, _sz, C.POINTER(_sz), _cp, _sz]),
     "smb_surface_free": (None, [_vp]),
     "smb_surface_arrays": (C.c_int, [_vp] + [C.POINTER(_vp)] * 6),
     "smb_surface_stats_get": (C.c_int, [_vp, C.POINTER(SurfaceStats_)]),
@@ -334,6 +334,7 @@ class Resident:
         ref.max_expanded = float(arr["max_expanded"])
         ref.rho_max = float(arr["rho_max"])
         ref.probe = float(arr["probe"])
+        ref.kind = {"ses": 0, "sas": 1, "vdw": 2}[arr.get("kind", "ses")]
         L = LatticeRef()
         L.spacing = float(lat["spacing"])
         L.brick = int(lat["brick"])

@@ -15,14 +15,15 @@ from . import native
 from .native import SmbError, _check, _p, lib
 
 REFINE = {"exact": 0, "linear": 1, "fast": 2}
+KINDS = {"ses": 0, "sas": 1, "vdw": 2}
 QUALITY = {"draft": 1.0, "medium": 0.5, "high": 0.25, "ultra": 0.125}
 
 
 @dataclass(frozen=True)
 class SurfaceParams:
-    """SurfaceParams (surface.rs:195-241): SES with probe radius, grid spacing
-    (default Quality::Medium, 0.5 A), refine mode, brick edge (default 10),
-    CUDA device, host threads (0 = all)."""
+    """SurfaceParams (surface.rs:195-241): surface kind (ses, sas or vdw)
+    with probe radius, grid spacing (default Quality::Medium, 0.5 A), refine
+    mode, brick edge (default 10), CUDA device, host threads (0 = all)."""
     probe_radius: float = 1.4
     spacing: float = 0.5
     refine: str = "exact"
@@ -34,6 +35,16 @@ class SurfaceParams:
     @staticmethod
     def ses(probe_radius):
         return SurfaceParams(probe_radius=float(probe_radius))
+
+    @staticmethod
+    def sas(probe_radius):
+        """SurfaceParams::sas (surface.rs:272-277): the spheres expanded by the probe."""
+        return SurfaceParams(probe_radius=float(probe_radius), kind="sas")
+
+    @staticmethod
+    def vdw():
+        """SurfaceParams::vdw (surface.rs:280-285): the spheres themselves."""
+        return SurfaceParams(probe_radius=0.0, kind="vdw")
 
     def with_spacing(self, h):
         return replace(self, spacing=float(h))
@@ -50,10 +61,10 @@ class SurfaceParams:
         return replace(self, brick_size=int(b))
 
     def _c(self):
-        if self.kind != "ses":
-            raise SmbError(1, "only the SES is meshed on the device")
+        if self.kind not in KINDS:
+            raise SmbError(1, "surface kind must be ses, sas or vdw")
         p = native.SurfaceParams_()
-        p.kind = 0
+        p.kind = KINDS[self.kind]
         p.probe_radius = float(self.probe_radius)
         p.spacing = float(self.spacing)
         p.brick_size = int(self.brick_size)
@@ -308,16 +319,18 @@ class SurfaceEngine:
         lib().smb_engine_set_warm_start(self.h, mlp.h if mlp is not None else None)
 
     def warm_start_rows(self):
-        """(features (n, 32), exact root parameters (n,)) for every edge the
-        device refines, from a fresh device run."""
+        """(features (n, 32), exact root parameters (n,), plain f32 root
+        parameters (n,), NaN where plain refinement did not converge) for
+        every edge the device refines, from a fresh device run."""
         err = C.create_string_buffer(1024)
         n = C.c_size_t(0)
-        _check(lib().smb_engine_warm_start_rows(self.h, None, None, 0, C.byref(n), err, 1024), err)
+        _check(lib().smb_engine_warm_start_rows(self.h, None, None, None, 0, C.byref(n), err, 1024), err)
         x = np.zeros((max(n.value, 1), native.MLP_FEATURES), np.float32)
         t = np.zeros(max(n.value, 1), np.float32)
-        _check(lib().smb_engine_warm_start_rows(self.h, _p(x, C.c_float), _p(t, C.c_float), len(t), C.byref(n), err,
-                                                1024), err)
-        return x[:n.value], t[:n.value]
+        tp = np.zeros(max(n.value, 1), np.float32)
+        _check(lib().smb_engine_warm_start_rows(self.h, _p(x, C.c_float), _p(t, C.c_float), _p(tp, C.c_float), len(t),
+                                                C.byref(n), err, 1024), err)
+        return x[:n.value], t[:n.value], tp[:n.value]
 
     def close(self):
         self.warm = None

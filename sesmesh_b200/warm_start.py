@@ -27,9 +27,11 @@ shell that the tests and the benchmark use) at 0.1, 0.25, 0.35, 0.5 and
 at most ROWS_PER_GLOBULE rows each (about 1e7 in all): features from the
 device feature pass (smb_batch_edge_features) and, as the label source,
 the root parameter that exact mode's f64 refinement finds on the same edge
-(smb_engine_warm_start_rows).  Gate label: 1 where t_c lies within 2e-6 A
-of that root, else 0; root head: the root itself (mean squared error on
-the sigmoid output for both).
+(smb_engine_warm_start_rows), with the root plain f32 refinement stops at.
+Gate label: 1 where t_c is that plain f32 root (the candidate's iteration
+followed the field's own) and lies within 2e-6 A of the exact root, else 0;
+root head: the exact root itself (mean squared error on the sigmoid output
+for both).
 
     python -m sesmesh_b200.warm_start [--out-dir DIR]   # on a B200: writes
                                                       # warm_start.f32, warm_root.f32
@@ -98,7 +100,8 @@ def save(params, path=WEIGHTS):
 
 
 def rows(spheres, spacing, probe=PROBE, brick=10):
-    """(features, exact t) of every edge the device refines for one input."""
+    """(features, exact t, plain f32 t) of every edge the device refines for
+    one input."""
     params = SurfaceParams.ses(probe).with_spacing(spacing).with_brick_size(brick)
     eng = SurfaceEngine(spheres, params)
     try:
@@ -118,27 +121,32 @@ def contact_start(x):
     return np.where(x[:, F_CONV] > 0.5, x[:, F_TC].astype(np.float64), -1.0)
 
 
-def target_of(x, t_exact):
-    """Gate label: 1 where t_c lies within 2e-6 A of the exact root."""
+def target_of(x, t_exact, t_plain):
+    """Gate label: 1 where t_c is where plain f32 refinement stops (the same
+    f32 value: the candidate's iteration followed the field's own) and lies
+    within 2e-6 A of the exact root.  Accepting t_c there keeps plain fast
+    mode's vertex, so area and volume keep their distance to exact mode's."""
     h = x[:, F_H].astype(np.float64)
     tc = contact_start(x)
-    return ((tc >= 0) & (np.abs(tc - t_exact) * h <= 2e-6)).astype(np.float32)
+    same = np.asarray(x[:, F_TC], np.float32) == np.asarray(t_plain, np.float32)
+    return ((tc >= 0) & same & (np.abs(tc - t_exact) * h <= 2e-6)).astype(np.float32)
 
 
 def training_rows(sets=None, per=ROWS_PER_GLOBULE, log=None):
     sets = train_set() if sets is None else sets
     rng = np.random.default_rng(1)
-    xs, ts = [], []
+    xs, ts, ps = [], [], []
     for seed, n, h in sets:
-        x, t = rows(workloads.globule(seed, n), h)
+        x, t, tp = rows(workloads.globule(seed, n), h)
         if len(x) > per:
             keep = np.sort(rng.choice(len(x), per, replace=False))
-            x, t = x[keep], t[keep]
+            x, t, tp = x[keep], t[keep], tp[keep]
         xs.append(x)
         ts.append(t)
+        ps.append(tp)
         if log:
             log("seed %d: %d atoms at %.2f A -> %d rows" % (seed, n, h, len(x)))
-    return np.concatenate(xs), np.concatenate(ts)
+    return np.concatenate(xs), np.concatenate(ts), np.concatenate(ps)
 
 
 def train(x, target, epochs=40, batch=4096, lr=2e-3, seed=0, device=0, log=None):
@@ -159,12 +167,12 @@ def train(x, target, epochs=40, batch=4096, lr=2e-3, seed=0, device=0, log=None)
     return mlp.params(), hist
 
 
-def evaluate(params, x, t_exact, device=0):
+def evaluate(params, x, t_exact, t_plain, device=0):
     """How the gate's choices compare with the labels: the fraction of edges
     sent to t_c, the fraction whose label is 1, precision and recall."""
     mlp = native.Mlp(_device(device), params)
     y = mlp.forward(x) >= 0.5
-    lab = target_of(x, t_exact) > 0.5
+    lab = target_of(x, t_exact, t_plain) > 0.5
     tp = float(np.sum(y & lab))
     return dict(rows=int(len(x)), sent_to_contact=float(y.mean()), label_rate=float(lab.mean()),
                 precision=tp / max(1.0, float(y.sum())), recall=tp / max(1.0, float(lab.sum())))
@@ -189,18 +197,19 @@ def main(argv=None):
     a = ap.parse_args(argv)
     log = lambda m: print(m, flush=True)
     t0 = time.time()
-    x, t = training_rows(train_set(a.globules), log=log)
+    x, t, tp = training_rows(train_set(a.globules), log=log)
     log("%d rows in %.1f s" % (len(x), time.time() - t0))
     t1 = time.time()
-    gate, hist = train(x, target_of(x, t), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, log=log)
+    gate, hist = train(x, target_of(x, t, tp), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, log=log)
     save(gate, os.path.join(a.out_dir, "warm_start.f32"))
     root, hist_r = train(x, t.astype(np.float32), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed + 7, log=log)
     save(root, os.path.join(a.out_dir, "warm_root.f32"))
     t_train = time.time() - t1
     held = workloads.globule330()
-    xh, th = rows(held["spheres"], held["spacing"], held["probe"], held["brick"])
-    summary = dict(rows=int(len(x)), globules=a.globules, train_gate=evaluate(gate, x, t),
-                   held_out_globule330_gate=evaluate(gate, xh, th), held_out_globule330_root=evaluate_root(root, xh, th),
+    xh, th, tph = rows(held["spheres"], held["spacing"], held["probe"], held["brick"])
+    summary = dict(rows=int(len(x)), globules=a.globules, train_gate=evaluate(gate, x, t, tp),
+                   held_out_globule330_gate=evaluate(gate, xh, th, tph),
+                   held_out_globule330_root=evaluate_root(root, xh, th),
                    final_loss_gate=hist[-1], final_loss_root=hist_r[-1], seconds_rows=t1 - t0, seconds_train=t_train,
                    out_dir=a.out_dir)
     print(json.dumps(summary), flush=True)

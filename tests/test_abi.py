@@ -39,8 +39,8 @@ int main(void) {
   printf("%zu %zu\n", sizeof(smb_surface_stats), offsetof(smb_surface_stats, upload_bytes));
   printf("%zu %zu %zu %zu %zu\n", sizeof(smb_grid_ref), sizeof(smb_arrangement_ref), sizeof(smb_lattice_ref),
          sizeof(smb_batch_times), sizeof(smb_device_info));
-  printf("%zu %zu %zu\n", offsetof(smb_arrangement_ref, sphere_grid), offsetof(smb_arrangement_ref, probe),
-         offsetof(smb_lattice_ref, band));
+  printf("%zu %zu %zu %zu\n", offsetof(smb_arrangement_ref, sphere_grid), offsetof(smb_arrangement_ref, probe),
+         offsetof(smb_arrangement_ref, kind), offsetof(smb_lattice_ref, band));
   return 0;
 }
 '''
@@ -54,7 +54,7 @@ int main(void) {
             C.sizeof(native.GridRef), C.sizeof(native.ArrangementRef), C.sizeof(native.LatticeRef),
             C.sizeof(native.BatchTimes), C.sizeof(native.DeviceInfo),
             native.ArrangementRef.sphere_grid.offset, native.ArrangementRef.probe.offset,
-            native.LatticeRef.band.offset]
+            native.ArrangementRef.kind.offset, native.LatticeRef.band.offset]
     assert got == want
 
 

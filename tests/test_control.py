@@ -68,11 +68,13 @@ def test_host_build_reports_geometry_progress():
 def test_device_bytes_estimate_scales():
     from sesmesh_b200.native import lib
     est = lib().smb_device_bytes_estimate
-    a = est(1000, 10, 0.25, 1.4, 0)
-    assert est(2000, 10, 0.25, 1.4, 0) > a > 0
-    assert est(1000, 10, 0.5, 1.4, 0) > a  # larger sub-blocks gather more candidates
-    assert est(1000, 16, 0.25, 1.4, 0) > a
-    assert est(0, 10, 0.25, 1.4, 0) == 64 << 20
+    a = est(1000, 10, 0.25, 1.4, 100000, 0, 148)
+    fixed = est(0, 10, 0.25, 1.4, 100000, 0, 148)
+    assert fixed == 148 * 4 * 4 * (256 << 10) + (224 << 20)
+    assert est(2000, 10, 0.25, 1.4, 100000, 0, 148) - fixed == 2 * (a - fixed)
+    assert est(1000, 10, 1.0, 1.4, 100000, 0, 148) > a  # larger sub-blocks gather more candidates
+    assert est(1000, 10, 1.0, 1.4, 50, 0, 148) < est(1000, 10, 1.0, 1.4, 100000, 0, 148)  # at most every sphere
+    assert est(1000, 16, 0.25, 1.4, 100000, 0, 148) > a
 
 
 def _rank(rank, world, port, q):
@@ -154,17 +156,20 @@ def test_cancel_at_mesh_stage_then_run_again():
 @pytest.mark.gpu
 def test_memory_guard_refuses_and_coarsens():
     from sesmesh_b200 import native, surface as S, workloads
+    from sesmesh_b200.native import lib
     g = workloads.globule330()
-    p = S.SurfaceParams.ses(1.4).with_spacing(0.25)
+    p = S.SurfaceParams.ses(1.4).with_spacing(0.1)
     ref = S.compute_surface(g["spheres"], p)
     est = ref.stats["device_bytes_estimate"]
-    assert est > 0
+    fixed = lib().smb_device_bytes_estimate(0, 10, 0.1, 1.4, 330, 0, S._device(0).multiprocessors)
+    assert est > fixed
+    limit = (est + fixed) // 2
     with pytest.raises(native.SmbError) as e:
-        S.compute_surface_with(g["spheres"], p, S.Control(max_device_bytes=est // 4))
-    assert e.value.code == 6 and b"exceeds the limit" in str(e.value).encode()
-    out = S.compute_surface_with(g["spheres"], p, S.Control(max_device_bytes=est // 4, auto_coarsen=True))
-    assert out.stats["spacing_used"] > 0.25
-    assert out.stats["device_bytes_estimate"] <= est // 4
+        S.compute_surface_with(g["spheres"], p, S.Control(max_device_bytes=limit))
+    assert e.value.code == 6 and "exceeds the limit" in str(e.value)
+    out = S.compute_surface_with(g["spheres"], p, S.Control(max_device_bytes=limit, auto_coarsen=True))
+    assert out.stats["spacing_used"] > 0.1
+    assert out.stats["device_bytes_estimate"] <= limit
     want = S.compute_surface(g["spheres"], p.with_spacing(out.stats["spacing_used"]))
     assert out.obj() == want.obj()
 

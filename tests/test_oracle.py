@@ -117,3 +117,27 @@ def test_mc_table_meshes_random_grids_closed_and_oriented():
         p0, p1, p2 = pos[tris[:, 0]], pos[tris[:, 1]], pos[tris[:, 2]]
         vol = np.einsum("ij,ij->i", p0, np.cross(p1, p2)).sum() / 6.0
         assert vol > 0
+
+
+def test_single_sphere_all_kinds():
+    """tests/surface.rs:55-82 (single_sphere_all_kinds): one sphere of radius
+    1.8 meshed as SES (probe 1.4), SAS (probe 1.4: radius 3.2) and vdW at
+    0.25 A gives one component with Euler characteristic 2, area within
+    5e-3 and volume within 1.2e-2 relative of the sphere's, every vertex
+    within 1e-4 h + 2e-6 of the surface and normals within 0.01 degrees."""
+    s = np.array([[0.3, -0.2, 0.1, 1.8]])
+    h = 0.25
+    for kind, probe, r in (("ses", 1.4, 1.8), ("sas", 1.4, 3.2), ("vdw", 0.0, 1.8)):
+        out = O.Surface(s, probe, h, kind=kind)
+        st = out.stats
+        assert st["components"] == 1 and st["euler"] == 2, kind
+        area, vol = 4 * np.pi * r * r, 4.0 / 3.0 * np.pi * r ** 3
+        assert abs(st["area"] - area) / area < 5e-3, kind
+        assert abs(st["volume"] - vol) / vol < 1.2e-2, kind
+        m = out.mesh()
+        f, nrm, has = O.Engine(s, probe, h, kind=kind).field_normals(m["positions"].astype(np.float64))
+        assert np.abs(f).max() < 1e-4 * h + 2e-6, kind
+        b = m["normals"].astype(np.float64)[has]
+        a = nrm[has]
+        ang = np.degrees(np.arctan2(np.linalg.norm(np.cross(a, b), axis=1), (a * b).sum(1)))
+        assert has.sum() > 0.9 * len(has) and ang.max() < 0.01, (kind, ang.max())

@@ -39,12 +39,13 @@ def test_committed_weights_load():
 
 def test_target_marks_contact_starts_at_the_root():
     from sesmesh_b200 import warm_start
-    x = np.zeros((4, 32), np.float32)
-    x[:, warm_start.F_CONV] = [1, 1, 0, 1]
-    x[:, warm_start.F_TC] = [0.25, 0.4, 0.5, 0.9]
+    x = np.zeros((5, 32), np.float32)
+    x[:, warm_start.F_CONV] = [1, 1, 0, 1, 1]
+    x[:, warm_start.F_TC] = [0.25, 0.4, 0.5, 0.9, 0.3]
     x[:, warm_start.F_H] = 0.25
-    t = np.array([0.25 + 4e-6, 0.5, 0.5, 0.1])
-    assert np.array_equal(warm_start.target_of(x, t), [1.0, 0.0, 0.0, 0.0])
+    t = np.array([0.25 + 4e-6, 0.5, 0.5, 0.1, 0.3])
+    tp = np.array([0.25, 0.4, 0.5, 0.9, 0.3 + 1e-7], np.float32)  # the last: plain stops elsewhere
+    assert np.array_equal(warm_start.target_of(x, t, tp), [1.0, 0.0, 0.0, 0.0, 0.0])
 
 
 def test_training_set_spans_the_stated_sizes():
@@ -370,7 +371,7 @@ def test_training_rows_are_exact_roots(device):
     s, probe = random_chain(11, 60)
     h = 0.3
     eng = S.SurfaceEngine(s, S.SurfaceParams.ses(probe).with_spacing(h))
-    x, t = eng.warm_start_rows()
+    x, t, tp = eng.warm_start_rows()
     eng.close()
     assert len(x) > 100 and np.all((t >= 0) & (t <= 1))
     _, _, res, b = _batch(device, s, probe, h)
@@ -381,6 +382,9 @@ def test_training_rows_are_exact_roots(device):
     conv = (ev[cov] >> 31) == 1
     if len(x) == cov.sum():
         assert np.array_equal(xf[cov], x)
+        # The plain roots are this batch's own converged f32 roots.
+        assert np.array_equal(tp[conv].view(np.uint32), td[cov][conv].view(np.uint32))
+        assert np.all(np.isnan(tp[~conv]))
         dt = np.abs(td[cov] - t)[conv] * h
         assert np.percentile(dt, 99) <= 1e-4, np.percentile(dt, 99)
 
