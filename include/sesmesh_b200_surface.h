@@ -257,6 +257,28 @@ typedef struct {
  * 16384; 0 = always, SIZE_MAX = never. */
 void smb_set_device_arrangement_min(size_t n);
 int smb_engine_arrangement(const smb_engine* e, smb_arrangement_info* out);
+/* Structure input (io::read_bytes + Structure::select + radii::assign,
+ * crates/sesmesh/src/io/mod.rs:188-260, structure/select.rs:140-360,
+ * radii/mod.rs:166-250): the atoms of PDB (ATOM / HETATM records, MODEL /
+ * ENDMDL) or mmCIF (the _atom_site loop) bytes as (x, y, z, r) rows in file
+ * order, under a selection: `model` 0 the first model, else the model with
+ * that number; alternate locations resolved per residue by the highest
+ * total occupancy (first on ties); hydrogens (H, D, T), waters (HOH, WAT,
+ * TIP3, ...) and hetero atoms kept or dropped (default: drop, drop, keep).
+ * Radii: the element's Bondi radius (Bondi 1964 completed with Mantina
+ * 2009 and Alvarez 2013), 1.80 A for elements without one; the element comes
+ * from the element column or type_symbol, else from the atom name.  *n gets
+ * the atom count; xyzr (4 doubles per atom) is filled when non-null
+ * (SMB_ERR_MEMORY when cap < *n).  format: SMB_FORMAT_AUTO (mmCIF when the
+ * bytes open a data_ block), _PDB or _MMCIF.  No device is used. */
+enum { SMB_FORMAT_AUTO = 0, SMB_FORMAT_PDB = 1, SMB_FORMAT_MMCIF = 2 };
+typedef struct {
+    int model;
+    int hydrogens, waters, hetero;
+} smb_selection;
+int smb_read_structure(const char* data, size_t len, int format, const smb_selection* selection, double* xyzr,
+                       size_t cap, size_t* n, char* err, size_t errlen);
+
 /* Builds only the host arrangement (no device; smb_engine_arrangement). */
 int smb_arrangement_build(const double* xyzr, size_t n, const smb_surface_params* p, smb_engine** out, char* err,
                           size_t errlen);

@@ -73,6 +73,10 @@ class SurfaceStats_(C.Structure):
                    ("spacing_used", C.c_double), ("device_bytes_estimate", C.c_uint64)])
 
 
+class Selection_(C.Structure):
+    _fields_ = [("model", C.c_int), ("hydrogens", C.c_int), ("waters", C.c_int), ("hetero", C.c_int)]
+
+
 PROGRESS_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int, C.c_uint64, C.c_uint64)
 
 
@@ -175,6 +179,8 @@ SIGNATURES = {
                                              C.POINTER(Control_), C.POINTER(_vp), _cp, _sz]),
     "smb_device_bytes_estimate": (C.c_uint64, [_sz, C.c_uint32, C.c_double, C.c_double, _sz, C.c_int, C.c_int]),
     "smb_engine_device_bytes": (C.c_uint64, [_vp]),
+    "smb_read_structure": (C.c_int, [C.c_char_p, _sz, C.c_int, C.POINTER(Selection_), C.POINTER(C.c_double), _sz,
+                                     C.POINTER(_sz), _cp, _sz]),
     "smb_mlp_set_use": (C.c_int, [_vp, C.c_int]),
     "smb_mlp_forward": (C.c_int, [_vp, _fp, _sz, _fp, _cp, _sz]),
     "smb_mlp_gradient": (C.c_int, [_vp, _fp, _fp, _sz, _fp, _fp, _cp, _sz]),
