@@ -368,6 +368,8 @@ def run_ours(a):
         O.set_threads(cores)
         line["cpu_baseline_one_core"] = {"value": len(one) * spb_ / t1 / 1e6, "unit": "Mgridpts/s", "cores": 1,
                                          "kind": "port", "sample": "%d surface bricks (%.1f s)" % (len(one), t1)}
+        if O.ref_gpu_available():
+            line["ref_kernels"] = ref_kernels_leg(ceng, w, stage, line.get("fast_mode"))
     if rank == 0:
         print(json.dumps(line), flush=True)
     del out
@@ -440,6 +442,34 @@ def fast_leg(w, params, exact_stats, grid_points, reps=2):
     # Amdahl: the warm start only changes the device refinement, so even a
     # free refinement bounds the end-to-end gain.
     out["e2e_ceiling_if_refine_free"] = p["e2e_ms_per_mesh"] / max(p["e2e_ms_per_mesh"] - p["device_refine_ms"], 1e-9)
+    return out
+
+
+def ref_kernels_leg(ceng, w, stage, fast, reps=5):
+    """The reference's own CUDA kernels (sesmesh.cuh, built from their
+    source into oracle/_ref) on every surface brick of the workload, pass by
+    pass as cuda::Resident::run and ::refine issue them (64 threads per
+    sub-block; the list-size and edge-count scans on the host), best of
+    `reps` after a warm-up, beside this library's passes on the same bricks:
+    list build (count + scan + fill against sub-block states + gather),
+    sampling, crossing-edge enumeration (edge_count + scan against marching
+    cubes with edge compaction) and the plain f32 refinement (fast mode)."""
+    import oracle as O
+    bricks, _ = ceng.classify()
+    _, t, fr = O.ref_gpu_run(ceng, bricks, w["spacing"], w["brick"], w["probe"], reps=reps, fast=True)
+    ref = {"count": t["count_ms"], "scan_host": t["scan_ms"], "fill": t["fill_ms"], "sample": t["sample_ms"],
+           "edge_count": t["edge_count_ms"], "edge_scan_host": t["edge_scan_ms"], "refine": t["refine_ms"]}
+    ours = {"lists": stage["substates"] + stage["gather"], "sample": stage["sample"], "edges": stage["mc"]}
+    if fast:
+        ours["refine_f32"] = fast["plain"]["device_refine_ms"]
+    out = {"bricks": int(len(bricks)), "edges_refined": int(len(fr["t"])),
+           "evaluations": int((fr["evals"] & 0x7FFFFFFF).astype(np.int64).sum()),
+           "reference_ms": ref, "ours_ms": ours,
+           "speedup": {"lists": (ref["count"] + ref["scan_host"] + ref["fill"]) / max(ours["lists"], 1e-9),
+                       "sample": ref["sample"] / max(ours["sample"], 1e-9),
+                       "edges": (ref["edge_count"] + ref["edge_scan_host"]) / max(ours["edges"], 1e-9)}}
+    if fast:
+        out["speedup"]["refine_f32"] = ref["refine"] / max(ours["refine_f32"], 1e-9)
     return out
 
 

@@ -284,8 +284,9 @@ void smb_mlp_free(smb_mlp* mlp);
 int smb_mlp_set_params(smb_mlp* mlp, const float* params, char* err, size_t errlen);
 int smb_mlp_get_params(const smb_mlp* mlp, float* params);
 /* How smb_refine_warm uses the output: SMB_MLP_GATE (default) starts an edge
- * at t_c (below) where the output is >= 0.5 and at the linear guess
- * elsewhere; SMB_MLP_ROOT starts it at the output itself, a root parameter
+ * at t_c (below) where the output is >= 0.5 and both samples name t_c's
+ * candidate, and at the linear guess elsewhere; SMB_MLP_ROOT starts it at
+ * the output itself, a root parameter
  * in [0, 1] (parameters trained on the exact root). */
 #define SMB_MLP_GATE 0
 #define SMB_MLP_ROOT 1

@@ -292,6 +292,23 @@ class _RefTimes(C.Structure):
                 ("sample_ms", C.c_double), ("total_ms", C.c_double), ("ids", C.c_ulonglong)]
 
 
+class _RefFast(C.Structure):
+    _fields_ = [("sphere_lo", C.c_void_p), ("circle_lo", C.c_void_p), ("vertex_lo", C.c_void_p),
+                ("h_hi", C.c_float), ("h_lo", C.c_float), ("tol", C.c_float), ("max_iter", C.c_uint),
+                ("max_bisect", C.c_uint), ("edge_off", C.c_void_p), ("t", C.c_void_p), ("feat", C.c_void_p),
+                ("q", C.c_void_p), ("evals", C.c_void_p), ("cap", C.c_ulonglong), ("n_edges", C.c_ulonglong),
+                ("edge_count_ms", C.c_double), ("scan_ms", C.c_double), ("refine_ms", C.c_double)]
+
+
+def _residuals(points, fo):
+    """(x - f64(f32(x))) as f32 of the frame-local points, x, y, z rows
+    (Residuals::new, crates/sesmesh/src/field/gpu.rs:184-204)."""
+    if len(points) == 0:
+        return np.zeros((3, 1), np.float32)
+    d = np.asarray(points, np.float64)[:, :3] - fo
+    return np.ascontiguousarray((d - d.astype(np.float32).astype(np.float64)).T.astype(np.float32))
+
+
 def ref_gpu_path():
     return os.path.join(_HERE, "_ref", "libsesmesh_refgpu.so")
 
@@ -300,16 +317,26 @@ def ref_gpu_available():
     return os.path.exists(ref_gpu_path())
 
 
-def ref_gpu_run(eng, bricks, spacing, brick, probe, reps=3):
+def ref_gpu_run(eng, bricks, spacing, brick, probe, reps=3, fast=False, cap=None):
     """Sample values of the given surface bricks from the reference's own
     CUDA kernels (count, host scan, fill, sample, as cuda::Resident::run)
     with the inputs gpu.rs builds for them, and the best time of each pass
-    over `reps` runs (the first a warm-up): ((n, (b+1)^3) f32, times)."""
+    over `reps` runs (the first a warm-up): ((n, (b+1)^3) f32, times).
+
+    With fast, then cuda::Resident::refine's passes (edge count, host scan,
+    refine; resident.rs:632-687) on those values with the refinement
+    constants of Residuals::as_ref (gpu.rs:206-222), and a third result:
+    dict(edge_off (8n + 1, per sub-block), t, feat, q (n_edges, 3), evals)
+    in the kernels' order (sub-blocks in turn, each in crossing_edge's
+    z, y, x, axis order)."""
     global _REFGPU
     if _REFGPU is None:
         L = C.CDLL(ref_gpu_path())
         L.refgpu_run.restype = C.c_int
         L.refgpu_run.argtypes = [C.POINTER(_RefInput), C.c_int, C.POINTER(C.c_float), C.POINTER(_RefTimes)]
+        L.refgpu_run_fast.restype = C.c_int
+        L.refgpu_run_fast.argtypes = [C.POINTER(_RefInput), C.c_int, C.POINTER(C.c_float), C.POINTER(_RefTimes),
+                                      C.POINTER(_RefFast)]
         _REFGPU = L
     i = eng.info
     h, b = float(spacing), int(brick)
@@ -371,7 +398,31 @@ def ref_gpu_run(eng, bricks, spacing, brick, probe, reps=3):
     ri.b, ri.sub, ri.bricks, ri.n_bricks = b, sub, bk.ctypes.data, len(bk)
     out = np.zeros((len(bk), (b + 1) ** 3), np.float32)
     t = _RefTimes()
-    rc = _REFGPU.refgpu_run(C.byref(ri), int(reps), _p(out, C.c_float), C.byref(t))
+    if not fast:
+        rc = _REFGPU.refgpu_run(C.byref(ri), int(reps), _p(out, C.c_float), C.byref(t))
+        if rc:
+            raise RuntimeError("reference kernels failed (%d)" % rc)
+        return out, {name: getattr(t, name) for name, _ in t._fields_}
+    if cap is None:
+        cap = 3 * b * b * b * len(bk)
+    cap = max(int(cap), 1)
+    lo = [_residuals(sph, fo), _residuals(circ[:, 2:5] if nc else circ, fo),
+          _residuals(vert[:, :3] if nv else vert, fo)]
+    fr = dict(edge_off=np.zeros(8 * len(bk) + 1, np.uint32), t=np.zeros(cap, np.float32),
+              feat=np.zeros(cap, np.uint32), q=np.zeros((cap, 3), np.float32), evals=np.zeros(cap, np.uint32))
+    f = _RefFast()
+    f.sphere_lo, f.circle_lo, f.vertex_lo = (x.ctypes.data for x in lo)
+    f.h_hi = float(np.float32(h))
+    f.h_lo = float(np.float32(h - float(np.float32(h))))
+    f.tol, f.max_iter, f.max_bisect = float(np.float32(1e-5)), 8, 64
+    f.edge_off, f.t, f.feat = fr["edge_off"].ctypes.data, fr["t"].ctypes.data, fr["feat"].ctypes.data
+    f.q, f.evals, f.cap = fr["q"].ctypes.data, fr["evals"].ctypes.data, cap
+    rc = _REFGPU.refgpu_run_fast(C.byref(ri), int(reps), _p(out, C.c_float), C.byref(t), C.byref(f))
     if rc:
         raise RuntimeError("reference kernels failed (%d)" % rc)
-    return out, {name: getattr(t, name) for name, _ in t._fields_}
+    ne = int(f.n_edges)
+    for k in ("t", "feat", "q", "evals"):
+        fr[k] = fr[k][:ne]
+    times = {name: getattr(t, name) for name, _ in t._fields_}
+    times.update(edge_count_ms=f.edge_count_ms, edge_scan_ms=f.scan_ms, refine_ms=f.refine_ms)
+    return out, times, fr

@@ -1773,9 +1773,12 @@ __global__ void __launch_bounds__(256) k_warm_features(DArr A0, DLat L0, RefineC
 // of 128 threads per 128-row tile at a time (thread r computes row r's
 // features into the tile, one tensor-core forward pass per tile, weights
 // and TMEM set up once per CTA).  start[e] = (t_c, the candidate's feature
-// word) where the gate answers >= 0.5 and the candidate's iteration
-// converged, else (t_lin, 0) (use 0); or (the output itself, a root
-// parameter in [0, 1], 0) (use 1).  The word travels as float bits.
+// word) where the gate answers >= 0.5, the candidate's iteration converged
+// and both samples name that candidate (feature 12: where they name two,
+// the edge can hold a root of each, and t_c may be the one the iteration
+// from t_lin does not reach), else (t_lin, 0) (use 0); or (the output
+// itself, a root parameter in [0, 1], 0) (use 1).  The word travels as
+// float bits.
 template <bool MANY>
 __global__ void __launch_bounds__(128) k_warm_starts(DArr A0, DLat L0, RefineConsts RC0, const int4* keys,
                                                      const uint32_t* work, uint32_t n_host, const uint32_t* rec,
@@ -1809,7 +1812,7 @@ __global__ void __launch_bounds__(128) k_warm_starts(DArr A0, DLat L0, RefineCon
         if (e < E) {
             float2 w = make_float2(sc.y, 0.0f);
             if (ok && use == 1) w.x = p;
-            else if (ok && p >= 0.5f && sc.x >= 0.0f) w = make_float2(sc.x, __uint_as_float(cand));
+            else if (ok && p >= 0.5f && sc.x >= 0.0f && f[12] > 0.5f) w = make_float2(sc.x, __uint_as_float(cand));
             start[e] = w;
         }
     }

@@ -594,8 +594,9 @@ class Mlp:
         return out
 
     def set_use(self, use):
-        """"gate" (start at t_c where the output is >= 0.5, else the linear
-        guess) or "root" (start at the output itself)."""
+        """"gate" (start at t_c where the output is >= 0.5 and both samples
+        name t_c's candidate, else the linear guess) or "root" (start at the
+        output itself)."""
         if lib().smb_mlp_set_use(self.h, {"gate": 0, "root": 1}[use]) != SMB_OK:
             raise ValueError(use)
 

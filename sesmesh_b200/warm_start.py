@@ -7,8 +7,9 @@ begins.  The sampler records every sample's nearest feature; at an edge's
 two samples it names one candidate (a sphere, a circle or a SAS vertex),
 and the refinement iteration run on that candidate alone, without
 evaluating the field, gives t_c.  With the gate head (the default, weights
-data/warm_start.f32) the edge starts at t_c where the MLP answers >= 0.5
-and at the linear guess t_lin = fa / (fa - fb) elsewhere; with the root
+data/warm_start.f32) the edge starts at t_c where both samples name the
+candidate and the MLP answers >= 0.5, and at the linear guess
+t_lin = fa / (fa - fb) elsewhere; with the root
 head (data/warm_root.f32, smb_mlp_set_use ROOT) it starts at the MLP's
 output itself.  The reference's bracketed Newton / Illinois / bisection
 iteration then runs unchanged (smb_refine_warm): a start the field judges
@@ -28,10 +29,12 @@ at most ROWS_PER_GLOBULE rows each (about 1e7 in all): features from the
 device feature pass (smb_batch_edge_features) and, as the label source,
 the root parameter that exact mode's f64 refinement finds on the same edge
 (smb_engine_warm_start_rows), with the root plain f32 refinement stops at.
-Gate label: 1 where t_c is that plain f32 root (the candidate's iteration
-followed the field's own) and lies within 2e-6 A of the exact root, else 0;
-root head: the exact root itself (mean squared error on the sigmoid output
-for both).
+Gate label: 1 where both samples name the candidate, t_c is that plain f32
+root (the candidate's iteration followed the field's own) and lies within
+2e-6 A of the exact root, else 0; the gate trains on the rows where both
+samples name the candidate (the only rows it decides), those labelled 0
+repeated NEG_REPEAT times.  Root head: the exact root itself, every row
+(mean squared error on the sigmoid output for both).
 
     python -m sesmesh_b200.warm_start [--out-dir DIR]   # on a B200: writes
                                                       # warm_start.f32, warm_root.f32
@@ -54,6 +57,7 @@ PROBE = 1.4
 N_GLOBULES = 200
 ROWS_PER_GLOBULE = 50000
 SPACINGS = (0.1, 0.25, 0.35, 0.5, 1.0)
+NEG_REPEAT = 10
 FINE_ATOMS = 8000  # above it a 0.1 A turn takes 0.25 A (the edge count grows as 1 / h^2)
 
 
@@ -110,9 +114,9 @@ def rows(spheres, spacing, probe=PROBE, brick=10):
         eng.close()
 
 
-# Feature columns (smb_batch_edge_features): t_c's iteration converged, t_c
-# (t_lin where it did not), spacing.
-F_CONV, F_TC, F_H = 14, 17, 25
+# Feature columns (smb_batch_edge_features): both samples name the same
+# feature, t_c's iteration converged, t_c (t_lin where it did not), spacing.
+F_AGREE, F_CONV, F_TC, F_H = 12, 14, 17, 25
 
 
 def contact_start(x):
@@ -121,15 +125,23 @@ def contact_start(x):
     return np.where(x[:, F_CONV] > 0.5, x[:, F_TC].astype(np.float64), -1.0)
 
 
+def eligible(x):
+    """Rows on which the gate decides: the candidate's iteration converged
+    and both samples name the candidate (k_warm_starts sends every other row
+    to t_lin whatever the gate answers)."""
+    return (contact_start(x) >= 0) & (x[:, F_AGREE] > 0.5)
+
+
 def target_of(x, t_exact, t_plain):
-    """Gate label: 1 where t_c is where plain f32 refinement stops (the same
-    f32 value: the candidate's iteration followed the field's own) and lies
-    within 2e-6 A of the exact root.  Accepting t_c there keeps plain fast
-    mode's vertex, so area and volume keep their distance to exact mode's."""
+    """Gate label: 1 on an eligible row where t_c is where plain f32
+    refinement stops (the same f32 value: the candidate's iteration followed
+    the field's own) and lies within 2e-6 A of the exact root.  Accepting t_c
+    there keeps plain fast mode's vertex, so area and volume keep their
+    distance to exact mode's."""
     h = x[:, F_H].astype(np.float64)
     tc = contact_start(x)
     same = np.asarray(x[:, F_TC], np.float32) == np.asarray(t_plain, np.float32)
-    return ((tc >= 0) & same & (np.abs(tc - t_exact) * h <= 2e-6)).astype(np.float32)
+    return (eligible(x) & same & (np.abs(tc - t_exact) * h <= 2e-6)).astype(np.float32)
 
 
 def training_rows(sets=None, per=ROWS_PER_GLOBULE, log=None):
@@ -147,6 +159,22 @@ def training_rows(sets=None, per=ROWS_PER_GLOBULE, log=None):
         if log:
             log("seed %d: %d atoms at %.2f A -> %d rows" % (seed, n, h, len(x)))
     return np.concatenate(xs), np.concatenate(ts), np.concatenate(ps)
+
+
+def gate_rows(x, t_exact, t_plain, neg_repeat=None):
+    """The gate's training rows: the eligible rows alone (the gate decides
+    no other), those labelled 0 repeated neg_repeat times.  Sending a row to
+    t_c that the label rejects can move a vertex to another root on its edge,
+    while the reverse costs only evaluations, so the repetition weights the
+    first error above the second."""
+    neg_repeat = NEG_REPEAT if neg_repeat is None else neg_repeat
+    keep = eligible(x)
+    xg, yg = x[keep], target_of(x, t_exact, t_plain)[keep]
+    neg = np.nonzero(yg < 0.5)[0]
+    if neg_repeat > 1 and len(neg):
+        extra = np.tile(neg, neg_repeat - 1)
+        xg, yg = np.concatenate([xg, xg[extra]]), np.concatenate([yg, yg[extra]])
+    return xg, yg
 
 
 def train(x, target, epochs=40, batch=4096, lr=2e-3, seed=0, device=0, log=None):
@@ -171,7 +199,7 @@ def evaluate(params, x, t_exact, t_plain, device=0):
     """How the gate's choices compare with the labels: the fraction of edges
     sent to t_c, the fraction whose label is 1, precision and recall."""
     mlp = native.Mlp(_device(device), params)
-    y = mlp.forward(x) >= 0.5
+    y = (mlp.forward(x) >= 0.5) & eligible(x)
     lab = target_of(x, t_exact, t_plain) > 0.5
     tp = float(np.sum(y & lab))
     return dict(rows=int(len(x)), sent_to_contact=float(y.mean()), label_rate=float(lab.mean()),
@@ -194,13 +222,17 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--globules", type=int, default=N_GLOBULES)
+    ap.add_argument("--neg-repeat", type=int, default=NEG_REPEAT)
     a = ap.parse_args(argv)
     log = lambda m: print(m, flush=True)
     t0 = time.time()
     x, t, tp = training_rows(train_set(a.globules), log=log)
     log("%d rows in %.1f s" % (len(x), time.time() - t0))
     t1 = time.time()
-    gate, hist = train(x, target_of(x, t, tp), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, log=log)
+    xg, yg = gate_rows(x, t, tp, a.neg_repeat)
+    log("gate: %d eligible rows, %d labelled 0 (each repeated %d times)" % (len(xg), int((yg < 0.5).sum()) //
+                                                                         max(1, a.neg_repeat), a.neg_repeat))
+    gate, hist = train(xg, yg, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed, log=log)
     save(gate, os.path.join(a.out_dir, "warm_start.f32"))
     root, hist_r = train(x, t.astype(np.float32), epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed + 7, log=log)
     save(root, os.path.join(a.out_dir, "warm_root.f32"))

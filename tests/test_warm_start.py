@@ -39,13 +39,20 @@ def test_committed_weights_load():
 
 def test_target_marks_contact_starts_at_the_root():
     from sesmesh_b200 import warm_start
-    x = np.zeros((5, 32), np.float32)
-    x[:, warm_start.F_CONV] = [1, 1, 0, 1, 1]
-    x[:, warm_start.F_TC] = [0.25, 0.4, 0.5, 0.9, 0.3]
+    x = np.zeros((6, 32), np.float32)
+    x[:, warm_start.F_CONV] = [1, 1, 0, 1, 1, 1]
+    x[:, warm_start.F_AGREE] = [1, 1, 1, 1, 1, 0]
+    x[:, warm_start.F_TC] = [0.25, 0.4, 0.5, 0.9, 0.3, 0.25]
     x[:, warm_start.F_H] = 0.25
-    t = np.array([0.25 + 4e-6, 0.5, 0.5, 0.1, 0.3])
-    tp = np.array([0.25, 0.4, 0.5, 0.9, 0.3 + 1e-7], np.float32)  # the last: plain stops elsewhere
-    assert np.array_equal(warm_start.target_of(x, t, tp), [1.0, 0.0, 0.0, 0.0, 0.0])
+    t = np.array([0.25 + 4e-6, 0.5, 0.5, 0.1, 0.3, 0.25])
+    # The fifth: plain stops elsewhere; the sixth: the samples name two features.
+    tp = np.array([0.25, 0.4, 0.5, 0.9, 0.3 + 1e-7, 0.25], np.float32)
+    assert np.array_equal(warm_start.target_of(x, t, tp), [1.0, 0.0, 0.0, 0.0, 0.0, 0.0])
+    assert np.array_equal(warm_start.eligible(x), [True, True, False, True, True, False])
+    xg, yg = warm_start.gate_rows(x, t, tp, neg_repeat=3)
+    # Eligible rows 0, 1, 3, 4; the three labelled 0 twice more each.
+    assert len(xg) == 4 + 2 * 3 and yg.sum() == 1.0
+    assert np.array_equal(xg[:4], x[[0, 1, 3, 4]])
 
 
 def test_training_set_spans_the_stated_sizes():
