@@ -102,6 +102,30 @@ __device__ __forceinline__ double dist3(double ax, double ay, double az, double 
     return sqrt(dx * dx + dy * dy + dz * dz);
 }
 
+// Comparisons of a correctly rounded square root with a threshold T >= 0,
+// decided from the square when it is clear of T^2: t2 = fl(T T) is within
+// 2^-53 of T^2, so d2 >= fl(t2 (1 + 2^-49)) gives sqrt(d2) >= T (1 + 6 2^-53)
+// and fl(sqrt(d2)) > T; d2 <= fl(t2 (1 - 2^-49)) with t2 > 0 gives
+// fl(sqrt(d2)) < T.  Only in between is the square root taken.  The results
+// are those of fl(sqrt(d2)) >= T and fl(sqrt(d2)) < T exactly (NaN: false
+// for both).
+__device__ __forceinline__ bool sqrt_ge(double d2, double T) {
+    const double t2 = T * T;
+    if (d2 >= t2 * (1.0 + 0x1p-49)) return true;
+    if (d2 <= t2 * (1.0 - 0x1p-49)) return false;
+    return sqrt(d2) >= T;
+}
+__device__ __forceinline__ bool sqrt_lt(double d2, double T) {
+    const double t2 = T * T;
+    if (d2 <= t2 * (1.0 - 0x1p-49) && t2 > 0.0) return true;
+    if (d2 >= t2 * (1.0 + 0x1p-49)) return false;
+    return sqrt(d2) < T;
+}
+__device__ __forceinline__ double sq3(double ax, double ay, double az, double bx, double by, double bz) {
+    const double dx = ax - bx, dy = ay - by, dz = az - bz;
+    return dx * dx + dy * dy + dz * dz;
+}
+
 __device__ __forceinline__ double warp_min(double v) {
     for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
@@ -158,6 +182,9 @@ __device__ __forceinline__ void warp_for_near(const DGrid& g, double x, double y
 
 // SesField::try_sphere_with (field/point.rs:422-444): the candidate's
 // distance if its radial projection is unblocked and below best, else best.
+// Threshold tests on distances go through sqrt_ge / sqrt_lt (the root only
+// where the square leaves them open), with the results of the plain
+// comparisons.
 __device__ __forceinline__ double try_sphere(const DArr& A, double x, double y, double z, uint32_t i, double best) {
     double4 c = A.sph[i];
     double vx = x - c.x, vy = y - c.y, vz = z - c.z;
@@ -168,7 +195,7 @@ __device__ __forceinline__ double try_sphere(const DArr& A, double x, double y, 
     double qx = c.x + vx * s, qy = c.y + vy * s, qz = c.z + vz * s;
     for (uint32_t p = A.nb_off[i], e = A.nb_off[i + 1]; p < e; p++) {
         double4 k = A.sph[A.nb_items[p]];
-        if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - GEOM_EPS)) return best;
+        if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - GEOM_EPS)) return best;
     }
     return lb;
 }
@@ -178,11 +205,13 @@ __device__ __forceinline__ double try_circle(const DArr& A, double x, double y, 
     const double* c = A.circ + 12 * size_t(ci);
     double yx = x - c[0], yy = y - c[1], yz = z - c[2];
     double along = yx * c[3] + yy * c[4] + yz * c[5];
+    const double a2 = along * along;
     double wx = yx - c[3] * along, wy = yy - c[4] * along, wz = yz - c[5] * along;
     double wl = sqrt(wx * wx + wy * wy + wz * wz);
     double t = wl - c[9];
-    double dist = sqrt(along * along + t * t);
-    if (dist >= best) return best;
+    const double dist2 = a2 + t * t;
+    if (sqrt_ge(dist2, best)) return best;
+    double dist = sqrt(dist2);
     double dx, dy, dz;
     if (wl > 1e-12) {
         dx = wx / wl, dy = wy / wl, dz = wz / wl;
@@ -192,7 +221,7 @@ __device__ __forceinline__ double try_circle(const DArr& A, double x, double y, 
     double qx = c[0] + dx * c[9], qy = c[1] + dy * c[9], qz = c[2] + dz * c[9];
     for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++) {
         double4 k = A.sph[A.cb_items[p]];
-        if (!(dist3(qx, qy, qz, k.x, k.y, k.z) >= k.w - GEOM_EPS)) return best;
+        if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - GEOM_EPS)) return best;
     }
     return dist;
 }
@@ -216,7 +245,7 @@ __device__ inline double ses_eval_warp(const DArr& A, double x, double y, double
     warp_for_near(A.gs, x, y, z, A.max_expanded, lane, [&](uint32_t k) {
         if (!inside && A.status[k] != STATUS_CONTAINED) {
             double4 c = A.sph[k];
-            if (dist3(x, y, z, c.x, c.y, c.z) < c.w) inside = true;
+            if (sqrt_lt(sq3(x, y, z, c.x, c.y, c.z), c.w)) inside = true;
         }
     });
     if (!__any_sync(0xffffffffu, inside)) return 0.0;
@@ -228,21 +257,29 @@ __device__ inline double ses_eval_warp(const DArr& A, double x, double y, double
     warp_for_near(A.gc, x, y, z, cutoff + A.rho_max, lane, [&](uint32_t ci) { best = try_circle(A, x, y, z, ci, best); });
     warp_for_near(A.gv, x, y, z, cutoff, lane, [&](uint32_t vi) {
         double4 p = A.vert[vi];
-        double d = dist3(x, y, z, p.x, p.y, p.z);
-        if (d < best) best = d;
+        const double d2 = sq3(x, y, z, p.x, p.y, p.z);
+        if (sqrt_lt(d2, best)) best = sqrt(d2);
     });
     return warp_min(best);
 }
 
 // lattice::uniform_sign (field/lattice.rs:190-227), one warp: 1 uniformly
 // outside, 0 uniformly inside, -1 the surface may pass.
+// A sphere with fl(|x - c|) - R clear of margin by a factor 2^-40 (decided
+// from the square, as sqrt_ge does) enters neither minimum's tests: its
+// terms are above +margin (R >= r), so s_sas >= margin, s_vdw <= -margin and
+// the sphere field's s_sas > margin and s_sas < -margin come out as with it;
+// the square root is taken for the others alone.
 __device__ inline int uniform_sign_warp(const DArr& A, double x, double y, double z, double rho, int lane) {
     double margin = rho + CLASSIFY_EPS;
     double s_sas = __longlong_as_double(0x7ff0000000000000LL), s_vdw = s_sas;
     warp_for_near(A.gs, x, y, z, margin + A.max_expanded, lane, [&](uint32_t k) {
         if (A.status[k] != STATUS_CONTAINED) {
             double4 c = A.sph[k];
-            double d = dist3(x, y, z, c.x, c.y, c.z);
+            const double d2 = sq3(x, y, z, c.x, c.y, c.z);
+            const double T = c.w + margin;
+            if (d2 >= T * T * (1.0 + 0x1p-38)) return;
+            double d = sqrt(d2);
             s_sas = fmin(s_sas, d - c.w);
             s_vdw = fmin(s_vdw, d - A.rvdw[k]);
         }

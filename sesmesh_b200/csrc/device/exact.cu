@@ -539,29 +539,6 @@ struct XEval {
     uint32_t kind, id;
 };
 
-// Comparisons of a correctly rounded square root with a positive threshold
-// T, decided from the square when it is clear of T^2: t2 = fl(T T) is within
-// 2^-53 of T^2, so d2 >= fl(t2 (1 + 2^-49)) gives sqrt(d2) >= T (1 + 6 2^-53)
-// and fl(sqrt(d2)) > T; d2 <= fl(t2 (1 - 2^-49)) gives fl(sqrt(d2)) < T.
-// Only in between is the square root taken.  The results are those of
-// fl(sqrt(d2)) >= T and fl(sqrt(d2)) < T exactly (NaN: false for both).
-__device__ __forceinline__ bool sqrt_ge(double d2, double T) {
-    const double t2 = T * T;
-    if (d2 >= t2 * (1.0 + 0x1p-49)) return true;
-    if (d2 <= t2 * (1.0 - 0x1p-49)) return false;
-    return sqrt(d2) >= T;
-}
-__device__ __forceinline__ bool sqrt_lt(double d2, double T) {
-    const double t2 = T * T;
-    if (d2 <= t2 * (1.0 - 0x1p-49)) return true;
-    if (d2 >= t2 * (1.0 + 0x1p-49)) return false;
-    return sqrt(d2) < T;
-}
-__device__ __forceinline__ double sq3(double ax, double ay, double az, double bx, double by, double bz) {
-    const double dx = ax - bx, dy = ay - by, dz = az - bz;
-    return dx * dx + dy * dy + dz * dz;
-}
-
 // eval_local (point.rs:686-738) against the ball's lists: value, feature and
 // closest point.  COUNT: adds the f64 arithmetic operations executed to ops
 // (sqrt and division one each; compares, selects, fabs not counted): 9 per
