@@ -459,15 +459,26 @@ def ref_kernels_leg(ceng, w, stage, fast, reps=5):
     _, t, fr = O.ref_gpu_run(ceng, bricks, w["spacing"], w["brick"], w["probe"], reps=reps, fast=True)
     ref = {"count": t["count_ms"], "scan_host": t["scan_ms"], "fill": t["fill_ms"], "sample": t["sample_ms"],
            "edge_count": t["edge_count_ms"], "edge_scan_host": t["edge_scan_ms"], "refine": t["refine_ms"]}
-    ours = {"lists": stage["substates"] + stage["gather"], "sample": stage["sample"], "edges": stage["mc"]}
+    ours = {"substates": stage["substates"], "gather": stage["gather"], "sample": stage["sample"],
+            "mc": stage["mc"]}
     if fast:
         ours["refine_f32"] = fast["plain"]["device_refine_ms"]
+    # The passes do not split the work alike (this library's gather also
+    # computes the keys, blockers and packed f32 blocks the reference's
+    # sample pass derives per sample; its marching cubes also writes the
+    # triangles, which the reference builds on the host), so the like-for-
+    # like comparisons are the sampled values (lists + sampling) and the
+    # refinement.
+    ref_values = ref["count"] + ref["scan_host"] + ref["fill"] + ref["sample"]
+    our_values = ours["substates"] + ours["gather"] + ours["sample"]
     out = {"bricks": int(len(bricks)), "edges_refined": int(len(fr["t"])),
            "evaluations": int((fr["evals"] & 0x7FFFFFFF).astype(np.int64).sum()),
            "reference_ms": ref, "ours_ms": ours,
-           "speedup": {"lists": (ref["count"] + ref["scan_host"] + ref["fill"]) / max(ours["lists"], 1e-9),
+           "speedup": {"values": ref_values / max(our_values, 1e-9),
+                       "lists": (ref["count"] + ref["scan_host"] + ref["fill"]) /
+                                max(ours["substates"] + ours["gather"], 1e-9),
                        "sample": ref["sample"] / max(ours["sample"], 1e-9),
-                       "edges": (ref["edge_count"] + ref["edge_scan_host"]) / max(ours["edges"], 1e-9)}}
+                       "edges_vs_mc": (ref["edge_count"] + ref["edge_scan_host"]) / max(ours["mc"], 1e-9)}}
     if fast:
         out["speedup"]["refine_f32"] = ref["refine"] / max(ours["refine_f32"], 1e-9)
     return out
@@ -644,6 +655,12 @@ def run_batch(a):
         dist.destroy_process_group()
 
 
+# DRAM bytes (read + write) per step of the dominant kernel, from one ncu
+# capture of the same workload (profiles/mc_item_edges_refine_exact_traffic_
+# rings58800_h025.md: both passes of k_refine_exact).
+TRAFFIC = {("rings58800", 0.25, "k_refine_exact"): 418628608 + 259481344 + 92997632 + 80039168}
+
+
 def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops=0):
     """Roofline of the dominant kernel: its counted operations (or bytes) per
     launch over the launch's device time, against the matching peak."""
@@ -653,7 +670,8 @@ def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops=0
     if dominant == "refine" and xops:
         achieved = xops / (ms / 1e3) / 1e12
         return {"kernel": "k_refine_exact", "bound": "fp64", "achieved": achieved, "peak": FP64_NOFMA_TOPS,
-                "unit": "Tops/s", "frac": achieved / FP64_NOFMA_TOPS, "traffic": None,
+                "unit": "Tops/s", "frac": achieved / FP64_NOFMA_TOPS,
+                "traffic": TRAFFIC.get((w["name"], w["spacing"], "k_refine_exact")),
                 "peak_source": "nominal: 148 SMs x 64 FP64 lanes x 1965 MHz, one op per lane-cycle "
                                "(no FMA contraction, bit-exact f64; sqrt and division counted as one op)",
                 "algorithmic_ops": xops, "ms": ms,

@@ -319,11 +319,13 @@ int smb_batch_sample_features(const smb_batch* batch, uint32_t* out);
  * evaluating the field: where the candidate is the surface's nearest
  * feature at its iterates, that result t_c is where smb_refine would stop.
  * The MLP, over each edge's features (smb_batch_edge_features), then gives
- * the start (smb_mlp_set_use): t_c or the linear guess fa / (fa - fb) that
- * smb_refine always takes.  The iteration that follows is smb_refine's,
- * with its bracket, tolerance, budgets and outputs: a start the field
- * judges within the tolerance is accepted after one evaluation, any other
- * falls back to the bracketed refinement.  The last smb_run must have
+ * the start (smb_mlp_set_use): t_c where both samples name the candidate,
+ * its iteration converged and the gate answers >= 0.5, else the linear
+ * guess fa / (fa - fb) that smb_refine always takes.  The iteration that
+ * follows is smb_refine's, with its bracket, tolerance, budgets and
+ * outputs: a start at which the field is within the tolerance and names
+ * the candidate is accepted after one evaluation, any other falls back to
+ * the bracketed refinement from the linear guess.  The last smb_run must have
  * recorded the features (smb_batch_record_features; else SMB_ERR_STATE).
  * A null mlp is smb_refine. */
 int smb_refine_warm(smb_resident* res, smb_batch* batch, const smb_mlp* mlp, double* ms, char* err, size_t errlen);

@@ -237,6 +237,23 @@ __device__ __forceinline__ double circle_reach_dist(const DArr& A, double x, dou
     return sqrt(along * along + (wl - c[9]) * (wl - c[9]));
 }
 
+// circle_reach_dist, or +infinity where the distance to the circle's plane
+// alone puts it above T: the distance squared fl(a2 + t t) is at least a2,
+// and a2 >= fl(T T (1 + 2^-49)) gives fl(sqrt(a2)) > T (sqrt_ge's margin),
+// so the distance exceeds T too and every test against a threshold up to
+// T comes out as with it.
+__device__ __forceinline__ double circle_reach_dist_above(const DArr& A, double x, double y, double z, uint32_t ci,
+                                                          double T) {
+    const double* c = A.circ + 12 * size_t(ci);
+    double yx = x - c[0], yy = y - c[1], yz = z - c[2];
+    double along = yx * c[3] + yy * c[4] + yz * c[5];
+    const double a2 = along * along;
+    if (a2 >= T * T * (1.0 + 0x1p-49)) return __longlong_as_double(0x7ff0000000000000LL);
+    double wx = yx - c[3] * along, wy = yy - c[4] * along, wz = yz - c[5] * along;
+    double wl = sqrt(wx * wx + wy * wy + wz * wz);
+    return sqrt(a2 + (wl - c[9]) * (wl - c[9]));
+}
+
 // SesField::ses_eval distance (field/point.rs:385-411), one warp.  The result
 // is min(cutoff, min over unblocked candidates), which does not depend on the
 // visiting order, so lanes keep partial minima that are merged at the end.

@@ -366,31 +366,58 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         }
     };
 
-    // Near spheres, two passes (gather_near).
-    int nn = 0, n_in = 0;
-    for (int pass = 0; pass < 2; pass++) {
-        warp_scan_box(A.gs, bx, by, bz, r_sph, lane, [&](bool valid, uint32_t k) {
-            bool keep = false;
-            if (valid && A.status[k] != STATUS_CONTAINED) {
-                double4 c = A.sph[k];
-                double d = dist3(bx, by, bz, c.x, c.y, c.z);
-                bool contains = d < c.w + rho;
+    // Near spheres (gather_near: those that can contain a sample first, each
+    // class in scan order), in one scan: the kept ids, bit 31 marking the
+    // first class, go in scan order to the near table's space, and a stable
+    // partition puts them in place.  A sphere whose squared distance is
+    // clear of (R + the largest reach)^2 by 2^-38 is beyond every threshold
+    // below (its rounded distance exceeds each of them), so it is neither
+    // kept nor a disagreement, and its square root is not taken.
+    uint32_t* scan_buf = reinterpret_cast<uint32_t*>(near_tab);
+    int nn = 0;
+    warp_scan_box(A.gs, bx, by, bz, r_sph, lane, [&](bool valid, uint32_t k) {
+        bool keep = false, contains = false;
+        if (valid && A.status[k] != STATUS_CONTAINED) {
+            double4 c = A.sph[k];
+            const double d2 = sq3(bx, by, bz, c.x, c.y, c.z);
+            const double T = c.w + (win ? reach_x : reach);
+            if (d2 < T * T * (1.0 + 0x1p-38)) {
+                const double d = sqrt(d2);
+                contains = d < c.w + rho;
                 const bool near = !(d >= c.w + reach);
-                keep = near && (contains == (pass == 0));
-                if (win && pass == 0) {
+                keep = near;
+                if (win) {
                     const bool exposed = !spheres && A.status[k] == STATUS_EXPOSED;
                     const double lb = fabs(d - c.w);
                     differ |= (d < c.w + reach_x) != near || (d < c.w + rho_x) != contains ||
                               (exposed && lb <= reach_x) != (exposed && near && lb <= reach);
                 }
             }
-            int pos = warp_append(keep, nn);
-            if (pos >= 0 && pos < caps.near) near_ids[pos] = k;
-        });
-        if (pass == 0) n_in = nn;
-    }
+        }
+        int pos = warp_append(keep, nn);
+        if (pos >= 0 && pos < caps.near) scan_buf[pos] = k | (contains ? 0x80000000u : 0u);
+    });
     if (lane == 0) atomicMax(&O.counters[CNT_MAXNN], (unsigned long long)nn);
     if (nn > caps.near) return overflow(REC_OVERFLOW);
+    __syncwarp();
+    int n_in = 0;
+    for (int b0 = 0; b0 < nn; b0 += 32) {
+        const int i = b0 + lane;
+        n_in += __popc(__ballot_sync(0xffffffffu, i < nn && (scan_buf[i] >> 31)));
+    }
+    {
+        const uint32_t below = (1u << lane) - 1u;
+        int at_in = 0, at_out = n_in;
+        for (int b0 = 0; b0 < nn; b0 += 32) {
+            const int i = b0 + lane;
+            const uint32_t w = i < nn ? scan_buf[i] : 0u;
+            const bool f = i < nn && (w >> 31), g = i < nn && !(w >> 31);
+            const uint32_t mf = __ballot_sync(0xffffffffu, f), mg = __ballot_sync(0xffffffffu, g);
+            if (f) near_ids[at_in + __popc(mf & below)] = w & 0x7FFFFFFFu;
+            if (g) near_ids[at_out + __popc(mg & below)] = w;
+            at_in += __popc(mf), at_out += __popc(mg);
+        }
+    }
     __syncwarp();
     // The near table for blocker lookups (positions in the near list).
     for (uint32_t i = lane; i < (1u << tab_bits); i += 32) near_tab[i] = 0xFFFFu;
@@ -423,7 +450,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
     // Class C candidates.
     int nc = 0;
     warp_scan_box(A.gc, bx, by, bz, r_circ, lane, [&](bool valid, uint32_t ci) {
-        double d = valid ? circle_reach_dist(A, bx, by, bz, ci) : 0.0;
+        double d = valid ? circle_reach_dist_above(A, bx, by, bz, ci, win ? reach_x : reach) : 0.0;
         bool p = valid && d <= reach;
         if (win && valid) differ |= (d <= reach_x) != p;
         int pos = warp_append(p, nc);
@@ -656,6 +683,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 constexpr uint32_t BULK_CHUNK = 32768;            // bytes per bulk copy
+constexpr int SAMPLE_CHUNK = 512;                 // samples per ownership compaction
 constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;     // bounded wait
 
 // list (single structure): blocks whose packed block exceeds limit_units
@@ -674,6 +702,8 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
     extern __shared__ __align__(16) uint4 sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t sts[8];
+    __shared__ uint32_t own_mask[SAMPLE_CHUNK / 32];
+    __shared__ uint16_t own_list[SAMPLE_CHUNK];
     if (MANY && blockIdx.x >= uint32_t(*SC.n_work)) return;
     if (LIST && blockIdx.x >= list[0]) return;
     const uint32_t slot = LIST ? list[1 + blockIdx.x] : blockIdx.x;
@@ -728,6 +758,44 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
 
     const int sub = L.sub, side = L.b + 1, sp = sub + 1;
     const int ox = int(sb & 1) * sub, oy = int((sb >> 1) & 1) * sub, oz = int((sb >> 2) & 1) * sub;
+    // The sub-block's owned samples (sample_owner), compacted in sample
+    // order a chunk of SAMPLE_CHUNK at a time, so that the threads take
+    // owned samples only: the samples of a face that a neighbouring
+    // sub-block owns cost no masked-off lanes.  f(x, y, z) per owned sample.
+    const int n_samples = sp * sp * sp;
+    auto for_owned = [&](auto&& f) {
+        const int lane = int(threadIdx.x & 31), warp = int(threadIdx.x >> 5), nw = int(blockDim.x >> 5);
+        for (int c0 = 0; c0 < n_samples; c0 += SAMPLE_CHUNK) {
+            for (int q = warp; q < SAMPLE_CHUNK / 32; q += nw) {
+                const int t = c0 + q * 32 + lane;
+                bool own = false;
+                if (t < n_samples) {
+                    const int x = ox + t % sp, y = oy + (t / sp) % sp, z = oz + t / (sp * sp);
+                    bool positive;
+                    own = sample_owner(x, y, z, sub, st, &positive) == int(sb);
+                }
+                const uint32_t m = __ballot_sync(0xffffffffu, own);
+                if (lane == 0) own_mask[q] = m;
+            }
+            __syncthreads();
+            int total = 0;
+            for (int q = 0; q < SAMPLE_CHUNK / 32; q++) total += __popc(own_mask[q]);
+            for (int q = warp; q < SAMPLE_CHUNK / 32; q += nw) {
+                const uint32_t m = own_mask[q];
+                if ((m >> lane) & 1u) {
+                    int before = 0;
+                    for (int p = 0; p < q; p++) before += __popc(own_mask[p]);
+                    own_list[before + __popc(m & ((1u << lane) - 1u))] = uint16_t(q * 32 + lane);
+                }
+            }
+            __syncthreads();
+            for (int i = int(threadIdx.x); i < total; i += int(blockDim.x)) {
+                const int t = c0 + int(own_list[i]);
+                f(ox + t % sp, oy + (t / sp) % sp, oz + t / (sp * sp));
+            }
+            __syncthreads();
+        }
+    };
     const int4 key = keys[brick];
     const long long gx = (long long)key.x * L.b - L.frame[0], gy = (long long)key.y * L.b - L.frame[1],
                     gz = (long long)key.z * L.b - L.frame[2];
@@ -741,10 +809,7 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
         // |x - c| - R over every near sphere, clamped at band; nearT holds
         // (x, y, z, R).  COUNT: 9 per sphere.
         const float band = L.band32;
-        for (int t = threadIdx.x; t < sp * sp * sp; t += blockDim.x) {
-            int x = ox + t % sp, y = oy + (t / sp) % sp, z = oz + t / (sp * sp);
-            bool positive;
-            if (sample_owner(x, y, z, sub, st, &positive) != int(sb)) continue;
+        for_owned([&](int x, int y, int z) {
             const float px = float(gx + x) * L.h32, py = float(gy + y) * L.h32, pz = float(gz + z) * L.h32;
             if (COUNT) owned++, ops += 9ull * nn;
             float best = band;
@@ -763,17 +828,14 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
             if (FEAT)
                 feats[size_t(brick) * L.spb + (z * side + y) * side + x] =
                     fi == 0xFFFFFFFFu ? (1u << FEAT_SHIFT_D) : ((2u << FEAT_SHIFT_D) | ids[R[R_IDS] + fi]);
-        }
+        });
         if (COUNT) {
             atomicAdd(&counters[CNT_OPS], ops);
             atomicAdd(&counters[CNT_OWNED], owned);
         }
         return;
     }
-    for (int t = threadIdx.x; t < sp * sp * sp; t += blockDim.x) {
-        int x = ox + t % sp, y = oy + (t / sp) % sp, z = oz + t / (sp * sp);
-        bool positive;
-        if (sample_owner(x, y, z, sub, st, &positive) != int(sb)) continue;
+    for_owned([&](int x, int y, int z) {
         // Lattice::local (field/lattice.rs:69): from integers only.
         const float px = float(gx + x) * L.h32, py = float(gy + y) * L.h32, pz = float(gz + z) * L.h32;
         if (COUNT) owned++, ops += 8ull * n_in;
@@ -830,14 +892,19 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
             for (int ci = 0; ci < nc; ci++) {
                 const float kk = c_key[ci];
                 if (kk > 0.0f && kk * kk >= best2) break;
-                if (COUNT) ops += 26;
+                if (COUNT) ops += 9;
                 float4 m = C[3 * ci], u = C[3 * ci + 1], e2 = C[3 * ci + 2];
                 float yx = px - m.x, yy = py - m.y, yz = pz - m.z;
                 float along = yx * u.x + yy * u.y + yz * u.z;
+                // d2 = fl(a2 + tt tt) >= a2 (rounding is monotone): where the
+                // plane distance alone fails the test, d2 fails it too.
+                const float a2 = along * along;
+                if (!(a2 < best2)) continue;
+                if (COUNT) ops += 17;
                 float wx = yx - u.x * along, wy = yy - u.y * along, wz = yz - u.z * along;
                 float wl = sqrtf(wx * wx + wy * wy + wz * wz);
                 float tt = wl - m.w;
-                float d2 = along * along + tt * tt;
+                float d2 = a2 + tt * tt;
                 if (!(d2 < best2)) continue;
                 if (COUNT) ops += 7;
                 bool degenerate = wl < 1e-6f;
@@ -873,7 +940,7 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
             else if (fk == 4) id = l[nn + 2 * ns + 1 + nsb + 2 * nc + 1 + R[R_CBLK] + fi];
             feats[size_t(brick) * L.spb + (z * side + y) * side + x] = (fk << FEAT_SHIFT_D) | id;
         }
-    }
+    });
     if (COUNT) {
         atomicAdd(&counters[CNT_OPS], ops);
         atomicAdd(&counters[CNT_OWNED], owned);
