@@ -259,8 +259,13 @@ __device__ bool x_blockers(const DArr& A, unsigned char* base, size_t cap, size_
 // sub-block's CSR words, hint its record), for a sub-block whose gather
 // found no candidate on which the two balls disagree: the sets are then
 // equal, S and C come in the same (key, index) order, the near list's
-// first R_INSIDE entries are the inside spheres; near is re-sorted by index
-// and V by (distance, index).  False when they do not fit in cap.
+// first R_INSIDE entries are the inside spheres, and the gather's blocker
+// lists (the rows kept to near spheres, in row order) are this ball's.
+// The near list keeps the gather's order, so the blocker positions carry
+// over as they are: near order reaches the results only through the
+// blocker tests, whose outcome (any blocker contains the point) and count
+// do not depend on it.  V is re-sorted by (distance, index).  False when
+// the lists do not fit in cap.
 template <bool WIDE>
 __device__ bool x_ball_from_ids(const DArr& A, double cx, double cy, double cz, double rho, unsigned char* base,
                                 size_t cap, uint32_t tid, uint32_t T, XView& v, const uint32_t* hint,
@@ -269,13 +274,23 @@ __device__ bool x_ball_from_ids(const DArr& A, double cx, double cy, double cz, 
     size_t tail = 0;
     const size_t need = x_layout(c, base, v, &tail);
     x_sync<WIDE>();
-    if (need > cap) return false;
+    const size_t nsb = hint[R_SBLK], ncb = hint[R_CBLK];
+    if (need > cap || xal(tail + nsb * 4) + ncb * 4 > cap) return false;
     const uint32_t* l_near = ids;
     const uint32_t* l_s = l_near + c.nn;
-    const uint32_t* l_c = l_s + c.ns + (c.ns + 1) + hint[R_SBLK];
-    const uint32_t* l_v = l_c + c.nc + (c.nc + 1) + hint[R_CBLK];
-    for (uint32_t i = tid; i < c.nn; i += T) v.t_id[i] = l_near[i];
-    for (uint32_t i = tid; i < c.ni; i += T) v.in_c[i] = A.sph[l_near[i]];
+    const uint32_t* l_soff = l_s + c.ns;
+    const uint32_t* l_sblk = l_soff + c.ns + 1;
+    const uint32_t* l_c = l_sblk + nsb;
+    const uint32_t* l_coff = l_c + c.nc;
+    const uint32_t* l_cblk = l_coff + c.nc + 1;
+    const uint32_t* l_v = l_cblk + ncb;
+    for (uint32_t i = tid; i < c.nn; i += T) {
+        const uint32_t k = l_near[i];
+        const double4 sp = A.sph[k];
+        v.near_id[i] = k;
+        v.near_c[i] = sp;
+        if (i < c.ni) v.in_c[i] = sp;
+    }
     for (uint32_t i = tid; i < c.ns; i += T) {
         const uint32_t k = l_s[i];
         const double4 s = A.sph[k];
@@ -291,16 +306,9 @@ __device__ bool x_ball_from_ids(const DArr& A, double cx, double cy, double cz, 
         v.c_m[i] = make_double4(C[0], C[1], C[2], C[9]);
         v.c_u[i] = make_double4(C[3], C[4], C[5], C[6]);
     }
-    x_sync<WIDE>();
-    for (uint32_t i = tid; i < c.nn; i += T) {
-        const uint32_t id = v.t_id[i];
-        uint32_t r = 0;
-        for (uint32_t q = 0; q < c.nn; q++) r += v.t_id[q] < id ? 1u : 0u;
-        v.near_id[r] = id;
-        v.near_c[r] = A.sph[id];
-    }
-    x_sync<WIDE>();
-    // V: (distance, index) pairs in the scratch (the near ids are placed).
+    for (uint32_t i = tid; i <= c.ns; i += T) v.s_off[i] = l_soff[i];
+    for (uint32_t i = tid; i <= c.nc; i += T) v.c_off[i] = l_coff[i];
+    // V: (distance, index) pairs in the scratch.
     for (uint32_t i = tid; i < c.nv; i += T) {
         const uint32_t vi = l_v[i];
         const double4 p = A.vert[vi];
@@ -317,7 +325,13 @@ __device__ bool x_ball_from_ids(const DArr& A, double cx, double cy, double cz, 
         v.v_p[r] = A.vert[vi];
     }
     x_sync<WIDE>();
-    return x_blockers<WIDE>(A, base, cap, tail, tid, T, v);
+    // The blocker lists take the scratch's place.
+    v.s_blk = reinterpret_cast<uint32_t*>(base + tail);
+    v.c_blk = reinterpret_cast<uint32_t*>(base + xal(tail + nsb * 4));
+    for (uint32_t p = tid; p < nsb; p += T) v.s_blk[p] = l_sblk[p];
+    for (uint32_t p = tid; p < ncb; p += T) v.c_blk[p] = l_cblk[p];
+    x_sync<WIDE>();
+    return true;
 }
 
 // gather_local of a sphere field (point.rs:566-579): the spheres not
