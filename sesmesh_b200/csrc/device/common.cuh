@@ -257,14 +257,18 @@ __device__ __forceinline__ double circle_reach_dist_above(const DArr& A, double 
 // SesField::ses_eval distance (field/point.rs:385-411), one warp.  The result
 // is min(cutoff, min over unblocked candidates), which does not depend on the
 // visiting order, so lanes keep partial minima that are merged at the end.
-__device__ inline double ses_eval_warp(const DArr& A, double x, double y, double z, double cutoff, int lane) {
-    bool inside = false;
-    warp_for_near(A.gs, x, y, z, A.max_expanded, lane, [&](uint32_t k) {
-        if (!inside && A.status[k] != STATUS_CONTAINED) {
-            double4 c = A.sph[k];
-            if (sqrt_lt(sq3(x, y, z, c.x, c.y, c.z), c.w)) inside = true;
-        }
-    });
+// inside_known: 1 or 0 when the caller's scan already settled whether some
+// sphere contains the point (it covered every sphere that can), -1 to scan.
+__device__ inline double ses_eval_warp(const DArr& A, double x, double y, double z, double cutoff, int lane,
+                                       int inside_known = -1) {
+    bool inside = inside_known > 0;
+    if (inside_known < 0)
+        warp_for_near(A.gs, x, y, z, A.max_expanded, lane, [&](uint32_t k) {
+            if (!inside && A.status[k] != STATUS_CONTAINED) {
+                double4 c = A.sph[k];
+                if (sqrt_lt(sq3(x, y, z, c.x, c.y, c.z), c.w)) inside = true;
+            }
+        });
     if (!__any_sync(0xffffffffu, inside)) return 0.0;
     double best = cutoff;
     warp_for_near(A.gs, x, y, z, cutoff + A.max_expanded, lane, [&](uint32_t i) {
@@ -290,6 +294,9 @@ __device__ inline double ses_eval_warp(const DArr& A, double x, double y, double
 __device__ inline int uniform_sign_warp(const DArr& A, double x, double y, double z, double rho, int lane) {
     double margin = rho + CLASSIFY_EPS;
     double s_sas = __longlong_as_double(0x7ff0000000000000LL), s_vdw = s_sas;
+    // The same scan answers ses_eval's inside test (some sphere with
+    // |x - c| < R: every such sphere lies in this box and is not skipped).
+    bool inside = false;
     warp_for_near(A.gs, x, y, z, margin + A.max_expanded, lane, [&](uint32_t k) {
         if (A.status[k] != STATUS_CONTAINED) {
             double4 c = A.sph[k];
@@ -297,6 +304,7 @@ __device__ inline int uniform_sign_warp(const DArr& A, double x, double y, doubl
             const double T = c.w + margin;
             if (d2 >= T * T * (1.0 + 0x1p-38)) return;
             double d = sqrt(d2);
+            inside = inside || d < c.w;
             s_sas = fmin(s_sas, d - c.w);
             s_vdw = fmin(s_vdw, d - A.rvdw[k]);
         }
@@ -307,7 +315,7 @@ __device__ inline int uniform_sign_warp(const DArr& A, double x, double y, doubl
     if (s_sas >= margin) return 1;
     if (s_vdw <= -margin) return 0;
     double cutoff = A.probe + margin + CLASSIFY_EPS;
-    double v = A.probe - ses_eval_warp(A, x, y, z, cutoff, lane);
+    double v = A.probe - ses_eval_warp(A, x, y, z, cutoff, lane, __any_sync(0xffffffffu, inside) ? 1 : 0);
     if (v > margin) return 1;
     if (v < -margin) return 0;
     return -1;
