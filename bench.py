@@ -488,8 +488,7 @@ def fallbacks(st):
     """Work the device path handed to the host: the arrangement (1 built on
     the device, 0 on the host below the device threshold, 2 the device
     declined), meshes finished on the host, edges refined on the host."""
-    return {"arrangement_where": int(st["arrangement_where"]), "finished_on_host": int(st["finished_on_host"]),
-            "refine_cpu_edges": int(st["refine_cpu_edges"])}
+    return {k: int(st.get(k, 0)) for k in ("arrangement_where", "finished_on_host", "refine_cpu_edges")}
 
 
 def shell_leg(dev, reps=2):
