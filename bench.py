@@ -3,19 +3,27 @@
 
 Workload (N=1): rings58800 -- 58,800 spheres (21 copies of a seeded
 2,800-sphere globule on three stacked 7-fold rings), probe 1.4 A, spacing
-0.25 A, brick 10, exact mode: sesmesh's 1AON-at-0.25-A analogue.
+0.25 A, brick 10: sesmesh's 1AON-at-0.25-A analogue, in fast mode with the
+learned warm start (the configuration the metric compares with plain f32
+refinement); --refine exact|fast|warm picks the main leg's mode.
 
 * value -- device mesh-stage throughput in Mgridpts/s (grid points =
   surface bricks x (b+1)^3, as sesmesh counts samples) with the arrangement
   resident in HBM: brick classification, sub-block states, candidate gather,
-  field sampling, marching-cubes compaction and the vertex refinement (f64
-  in exact mode), timed with CUDA events on the library's stream; L2
-  flushed (256 MiB write) before every step.
-* e2e -- the same metric through the public API (compute_surface from host
-  sphere arrays): the arrangement (on the device for 16,384 spheres or
-  more), the device stage, the mesh's assembly, validation, components,
-  area and volume on the device, and the finished mesh copied back to
-  page-locked host memory; wall clock.
+  field sampling, marching-cubes compaction and the vertex refinement (the
+  warm starts, f32 refinement and placement in fast mode; f64 in exact
+  mode), timed with CUDA events on the library's stream; L2 flushed
+  (256 MiB write) before every step.
+* e2e -- the same metric through the public API from host sphere arrays
+  (compute_surface; with the warm start, an engine with the model set):
+  the arrangement (on the device for 16,384 spheres or more), the device
+  stage, the mesh's assembly, validation, components, area and volume on
+  the device, and the finished mesh copied back to page-locked host memory;
+  wall clock.
+* exact_mode -- the same assembly in exact mode (meshes byte-identical to
+  the CPU back end), with its own value, e2e and roofline; fast_mode --
+  plain f32 refinement against the warm start (end to end, device
+  refinement, evaluations, area and volume against exact mode, vertex |F|).
 * roofline -- the dominant kernel against its bound: counted operations of
   its evaluations per launch over the launch's CUDA-event time.
 * cpu_baseline -- the CPU oracle (C++ restatement of sesmesh's CPU back end)
@@ -54,13 +62,15 @@ def args_():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="rings58800",
                    choices=["rings58800", "globule330", "globule2800", "shell2400k", "batch512"])
-    p.add_argument("--refine", default=None, choices=[None, "exact", "fast"])
+    p.add_argument("--refine", default=None, choices=[None, "exact", "fast", "warm"],
+                   help="mode of the main leg (default: warm for rings58800, the workload's own otherwise)")
     p.add_argument("--spacing", type=float, default=None, help="override the workload's grid spacing")
     p.add_argument("--spheres", type=int, default=None,
                    help="keep the workload's first N spheres (smaller cases of the same kind, for ncu captures)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--no-fast", action="store_true", help="skip the fast-mode (plain vs warm start) leg")
+    p.add_argument("--no-exact", action="store_true", help="skip the exact-mode block of a fast-mode line")
     p.add_argument("--no-configs", action="store_true",
                    help="skip the shell2400k and batch512 blocks of the default line")
     return p.parse_args()
@@ -198,7 +208,9 @@ def run_reference(a):
         return
     if a.workload == "batch512":
         return run_reference_batch(a)
-    w = workload(a.workload, a.refine, a.spacing, a.spheres)
+    w = workload(a.workload, None, a.spacing, a.spheres)
+    mode = a.refine or ("warm" if a.workload == "rings58800" else w["refine"])
+    w["refine"] = "exact" if mode == "exact" else "fast"
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     eng, sample, spb, k, nb = cpu_leg(w, budget_s=6.0)
@@ -212,16 +224,156 @@ def run_reference(a):
     value = len(sample) * spb / (np.mean(times)) / 1e6
     cores = O.threads()
     line = {
-        "impl": "reference", "metric": "Mgridpts/s (SES mesh stage)", "value": value, "unit": "Mgridpts/s",
+        "impl": "reference", "metric": "Mgridpts/s (SES mesh stage, %s)" % MODE_NAMES[mode], "value": value,
+        "unit": "Mgridpts/s",
         "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
-        "config": {"workload": describe(w), "surface_bricks": nb, "sample": "every %d-th surface brick (%d bricks)" % (k, len(sample)),
-                   "stage": "Engine::evaluate + mesh_brick (exact f64 refinement) per brick"},
+        "config": {"workload": describe(w) + ("" if mode != "warm" else " + learned warm start"),
+                   "surface_bricks": nb, "sample": "every %d-th surface brick (%d bricks)" % (k, len(sample)),
+                   "stage": "Engine::evaluate + mesh_brick per brick (exact f64 refinement: the reference's CPU "
+                            "back end has no fast mode, its fast mode is the GPU's)"},
         "cpu_baseline": {"value": value, "unit": "Mgridpts/s", "cores": cores, "kind": "port",
                          "sample": "%d of %d surface bricks of %s" % (len(sample), nb, w["name"])},
         "e2e": {"value": value, "unit": "Mgridpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+MODE_NAMES = {"exact": "exact f64 refinement", "fast": "fast mode, plain f32 refinement",
+              "warm": "fast mode, f32 refinement from the learned warm start"}
+
+
+def mode_params(w, mode, local):
+    """SurfaceParams of a mode: exact, fast (plain f32) or warm (fast with
+    the learned warm start)."""
+    from sesmesh_b200 import surface as S
+    p = S.SurfaceParams.ses(w["probe"]).with_spacing(w["spacing"]).with_brick_size(w["brick"]).with_refine(
+        "exact" if mode == "exact" else "fast")
+    return S.SurfaceParams(**{**p.__dict__, "device": local})
+
+
+def new_engine(w, params, mlp):
+    from sesmesh_b200 import surface as S
+    eng = S.SurfaceEngine(w["spheres"], params)
+    if mlp is not None:
+        eng.set_warm_start(mlp)
+    return eng
+
+
+def mode_leg(a, w, mode, local, dev, barrier, max_over_ranks, world, flush, counted=True):
+    """One mode of the workload: the device stage with the arrangement
+    resident (CUDA events, L2 flushed before every step, max over ranks),
+    then end to end through the public API, then the roofline of the
+    dominant kernel."""
+    from sesmesh_b200 import native, warm_start
+    from sesmesh_b200 import surface as S
+    import torch
+    params = mode_params(w, mode, local)
+    mlp = native.Mlp(S._device(local), warm_start.load()) if mode == "warm" else None
+    eng = new_engine(w, params, mlp)
+    for _ in range(max(3, a.warmup)):
+        eng.run_device()
+    n_bricks = eng.bricks
+    spb = (w["brick"] + 1) ** 3
+    grid_points = n_bricks * spb
+    launches0 = native.lib().smb_kernel_launches()
+    clocks = Clocks(local)
+    barrier()
+    step_ms, parts = [], []
+    for _ in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t = eng.run_device()
+        cls = eng.batch_info()["classify_ms"]
+        step_ms.append(cls + t["total"])
+        parts.append(dict(t, classify=cls))
+    barrier()
+    clk = clocks.stop()
+    launches = native.lib().smb_kernel_launches() - launches0
+    mean_ms = max_over_ranks(float(np.mean(step_ms)))
+    value = world * grid_points / (mean_ms / 1e3) / 1e6
+    stage = {k: float(np.mean([p[k] for p in parts])) for k in ("classify", "substates", "gather", "sample", "mc")}
+    # Vertex refinement on the device: f64 in exact mode; in fast mode the
+    # warm starts, the f32 refinement and the placement.
+    stage["refine"] = float(np.mean([p["total"] - p["substates"] - p["gather"] - p["sample"] - p["mc"]
+                                     for p in parts]))
+    dominant = max(stage, key=stage.get)
+
+    # End to end through the public API, host arrays in, mesh out: exact and
+    # plain fast mode through compute_surface, the warm start through an
+    # engine with the model set (arrangement, upload, device stage, finish,
+    # copies back).  Two warm-up calls, so that the timed calls find the
+    # memory caches in their steady state.
+    def mesh_once():
+        if mlp is None:
+            return S.compute_surface(w["spheres"], params), None
+        e = new_engine(w, params, mlp)
+        return e.mesh(), e
+
+    e2e_ms, st, out = [], None, None
+    for _ in range(2 if a.e2e_steps else 0):
+        out, e = mesh_once()
+        if e is not None:
+            out.close(), e.close()
+    for _ in range(a.e2e_steps):
+        if out is not None:
+            out.close()
+        barrier()
+        t0 = time.perf_counter()
+        out, e = mesh_once()
+        torch.cuda.synchronize(dev)
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+        if e is not None:
+            st = dict(out.stats)
+            out.close(), e.close()
+            out = None
+    if out is not None:
+        st = dict(out.stats)
+        out.close()
+    e2e_mean = max_over_ranks(float(np.mean(e2e_ms)) if e2e_ms else float("nan"))
+    info = eng.batch_info()
+    st = st or {}
+    # Host to device: the sphere rows when the device builds the arrangement,
+    # else the uploaded arrangement (what the engine copied, counted by it).
+    h2d = int(st.get("upload_bytes", 0))
+    nv, nt = int(st.get("vertices", 0)), int(st.get("triangles", 0))
+    if mode == "exact":
+        # Finished on the device: the mesh alone (position, normal, atom,
+        # component, patch per vertex; triangles) and 16 B of totals.
+        d2h = nv * 33 + nt * 12 + 16
+    else:
+        d2h = n_bricks * 16 + (n_bricks + 1) * 8 + nv * 12 + nt * 12 + nv * 24
+    pk, pk_kind = peaks()
+    ops, owned = eng.count_ops() if counted else (0, 0)
+    if counted and mode == "exact":
+        rops = eng.count_exact_ops()
+    elif counted:
+        rops = eng.count_refine_ops(mlp)
+    else:
+        rops = 0
+    roof = roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, rops, mode)
+    evals = int(st.get("refine_evaluations", 0))
+    if roof.get("kernel", "").startswith("k_refine"):
+        roof["evaluations"] = evals
+    eng.close()
+    leg = {
+        "mode": mode, "value": value, "ms_per_step": mean_ms, "grid_points": int(grid_points),
+        "surface_bricks": int(n_bricks), "stage_ms": stage,
+        "lists": {"sampled_subblocks": int(info["sampled_subblocks"]), "ids_words": int(info["ids_words"]),
+                  "pack_bytes_mean": float(info["pack_units"]) * 16 / max(1, info["sampled_subblocks"]),
+                  "pack_bytes_max": int(info["max_pack_units"]) * 16, "edges": int(info["edges"]),
+                  "triangles": int(info["triangles"])},
+        "e2e": {"value": world * grid_points / (e2e_mean / 1e3) / 1e6, "unit": "Mgridpts/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h), "ms_per_mesh": e2e_mean,
+                "host_threads": st.get("host_threads"),
+                "stages_ms": {k: st.get(k) for k in ("t_geometry", "t_upload", "t_device", "t_d2h", "t_host_refine",
+                                                     "t_assemble", "t_measure", "t_total")},
+                "mesh": {"vertices": nv, "triangles": nt, "area": st.get("area"), "volume": st.get("volume"),
+                         "refine_evaluations": evals, "refine_cpu_edges": st.get("refine_cpu_edges")},
+                "fallbacks": fallbacks(st)},
+        "roofline": roof, "gpu_launches": int(launches), "clocks": clk,
+    }
+    return leg, st
 
 
 def run_ours(a):
@@ -250,105 +402,33 @@ def run_ours(a):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    from sesmesh_b200 import native
-    from sesmesh_b200 import surface as S
-    w = workload(a.workload, a.refine, a.spacing, a.spheres)
-    params = S.SurfaceParams.ses(w["probe"]).with_spacing(w["spacing"]).with_brick_size(w["brick"]).with_refine(
-        w["refine"])
-    params = S.SurfaceParams(**{**params.__dict__, "device": local})
-    eng = S.SurfaceEngine(w["spheres"], params)
+    w = workload(a.workload, None, a.spacing, a.spheres)
+    mode = a.refine or ("warm" if a.workload == "rings58800" else w["refine"])
+    w["refine"] = "exact" if mode == "exact" else "fast"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    for _ in range(max(3, a.warmup)):
-        eng.run_device()
-    n_bricks = eng.bricks
-    spb = (w["brick"] + 1) ** 3
-    grid_points = n_bricks * spb
-    launches0 = native.lib().smb_kernel_launches()
-    clocks = Clocks(local)
-    barrier()
-    step_ms, parts = [], []
-    for _ in range(a.steps):
-        flush.zero_()
-        torch.cuda.synchronize(dev)
-        t = eng.run_device()
-        cls = eng.batch_info()["classify_ms"]
-        step_ms.append(cls + t["total"])
-        parts.append(dict(t, classify=cls))
-    barrier()
-    clk = clocks.stop()
-    launches = native.lib().smb_kernel_launches() - launches0
-    mean_ms = max_over_ranks(float(np.mean(step_ms)))
-    value = world * grid_points / (mean_ms / 1e3) / 1e6
-    stage = {k: float(np.mean([p[k] for p in parts])) for k in ("classify", "substates", "gather", "sample", "mc")}
-    # Vertex refinement on the device: f32 in fast mode, f64 in exact mode.
-    stage["refine"] = float(np.mean([p["total"] - p["substates"] - p["gather"] - p["sample"] - p["mc"]
-                                     for p in parts]))
-    dominant = max(stage, key=stage.get)
-
-    # End to end through the public API, host arrays in, mesh out.
-    e2e_ms, st = [], None
-    # Warm-up: two calls, so that the timed calls find the memory a previous
-    # result still holds and the one the call before released in the caches
-    # (the steady state of a caller that keeps its last result).
-    out = None
-    for _ in range(2 if a.e2e_steps else 0):
-        out = S.compute_surface(w["spheres"], params)
-    for _ in range(a.e2e_steps):
-        barrier()
-        t0 = time.perf_counter()
-        out = S.compute_surface(w["spheres"], params)
-        torch.cuda.synchronize(dev)
-        e2e_ms.append(1e3 * (time.perf_counter() - t0))
-    st = out.stats if out is not None else {k: 0 for k in ("vertices", "triangles", "host_threads", "area", "volume",
-                                                          "refine_evaluations", "refine_cpu_edges", "t_geometry",
-                                                          "t_upload", "t_device", "t_d2h", "t_host_refine",
-                                                          "t_assemble", "t_measure", "t_total")}
-    e2e_mean = max_over_ranks(float(np.mean(e2e_ms)) if e2e_ms else float("nan"))
-    info = eng.batch_info()
-    # Host to device: the sphere rows when the device builds the arrangement,
-    # else the uploaded arrangement (what the engine copied, counted by it).
-    h2d = int(st["upload_bytes"]) if out is not None else 0
-    d2h = int(n_bricks * 16 + (n_bricks + 1) * 8 + st["vertices"] * 12 + st["triangles"] * 12)
-    if w["refine"] == "fast":
-        d2h += int(st["vertices"] * 24)  # per edge: t, feature, closest point, evaluations
-    else:
-        # Exact mode finished on the device: the finished mesh alone (position,
-        # normal, atom, component, patch per vertex; triangles) and 16 B of totals.
-        d2h = int(st["vertices"] * 33 + st["triangles"] * 12 + 16)
-
-    pk, pk_kind = peaks()
-    ops, owned = eng.count_ops()
-    xops = eng.count_exact_ops() if w["refine"] == "exact" else 0
-    roof = roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops)
-    if roof.get("kernel") == "k_refine_exact":
-        roof["evaluations"] = int(st["refine_evaluations"])
+    leg, st = mode_leg(a, w, mode, local, dev, barrier, max_over_ranks, world, flush)
     line = {
-        "metric": "Mgridpts/s (SES mesh stage)", "value": value, "unit": "Mgridpts/s", "n_gpus": world,
-        "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": mean_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
-        "config": {"workload": describe(w), "spheres": int(len(w["spheres"])), "surface_bricks": int(n_bricks),
-                   "grid_points": int(grid_points), "refine": w["refine"], "parallelism": "replicas x%d" % world,
+        "metric": "Mgridpts/s (SES mesh stage, %s)" % MODE_NAMES[mode], "value": leg["value"], "unit": "Mgridpts/s",
+        "n_gpus": world, "steps": a.steps, "warmup": max(3, a.warmup), "ms_per_step": leg["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if mode == "exact" else "f32 (bf16 MLP)" if mode == "warm" else "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": describe(w) + ("" if mode != "warm" else " + learned warm start"),
+                   "spheres": int(len(w["spheres"])), "surface_bricks": leg["surface_bricks"],
+                   "grid_points": leg["grid_points"], "refine": mode, "parallelism": "replicas x%d" % world,
                    "l2": "flushed before every step (256 MiB write)"},
-        "stage_ms": stage,
-        "lists": {"sampled_subblocks": int(info["sampled_subblocks"]), "ids_words": int(info["ids_words"]),
-                  "pack_bytes_mean": float(info["pack_units"]) * 16 / max(1, info["sampled_subblocks"]),
-                  "pack_bytes_max": int(info["max_pack_units"]) * 16, "edges": int(info["edges"]),
-                  "triangles": int(info["triangles"])},
-        "e2e": {"value": world * grid_points / (e2e_mean / 1e3) / 1e6, "unit": "Mgridpts/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_mesh": e2e_mean,
-                "host_threads": st["host_threads"],
-                "stages_ms": {k: st[k] for k in ("t_geometry", "t_upload", "t_device", "t_d2h", "t_host_refine",
-                                                 "t_assemble", "t_measure", "t_total")},
-                "mesh": {"vertices": st["vertices"], "triangles": st["triangles"], "area": st["area"],
-                         "volume": st["volume"], "refine_evaluations": st["refine_evaluations"],
-                         "refine_cpu_edges": st["refine_cpu_edges"]},
-                "fallbacks": fallbacks(st)},
-        "roofline": roof,
-        "gpu_launches": int(launches),
-        "clocks": clk,
+        "stage_ms": leg["stage_ms"], "lists": leg["lists"], "e2e": leg["e2e"], "roofline": leg["roofline"],
+        "gpu_launches": leg["gpu_launches"], "clocks": leg["clocks"],
     }
-    if rank == 0 and world == 1 and not a.no_fast and w["refine"] == "exact":
-        line["fast_mode"] = fast_leg(w, params, st, grid_points)
+    exact_stats = st if mode == "exact" else None
+    if rank == 0 and world == 1 and mode != "exact" and not a.no_exact:
+        # Config 1: the same assembly in exact mode (byte-identical meshes).
+        xleg, exact_stats = mode_leg(a, dict(w, refine="exact"), "exact", local, dev, barrier, max_over_ranks, 1,
+                                     flush)
+        line["exact_mode"] = {k: xleg[k] for k in ("value", "ms_per_step", "stage_ms", "e2e", "roofline",
+                                                   "gpu_launches", "clocks")}
+    if rank == 0 and world == 1 and not a.no_fast and exact_stats:
+        line["fast_mode"] = fast_leg(w, mode_params(w, "fast", local), exact_stats, leg["grid_points"])
     if rank == 0 and world == 1 and not a.no_configs and a.workload == "rings58800" and not a.spheres:
         line["shell2400k"] = shell_leg(dev)
         line["batch512"] = batch_leg(dev)
@@ -359,7 +439,8 @@ def run_ours(a):
         line["cpu_baseline"] = {"value": len(sample) * spb_ / t / 1e6, "unit": "Mgridpts/s", "cores": O.threads(),
                                 "kind": "port",
                                 "sample": "every %d-th of %d surface bricks (%d bricks, %.1f s): CPU oracle evaluate + "
-                                          "mesh_brick (exact f64 refinement)" % (k, nb, len(sample), t)}
+                                          "mesh_brick (exact f64 refinement; the reference's CPU back end has no "
+                                          "fast mode)" % (k, nb, len(sample), t)}
         # The same restatement on one core, on a smaller sample.
         cores = O.threads()
         O.set_threads(1)
@@ -369,11 +450,10 @@ def run_ours(a):
         line["cpu_baseline_one_core"] = {"value": len(one) * spb_ / t1 / 1e6, "unit": "Mgridpts/s", "cores": 1,
                                          "kind": "port", "sample": "%d surface bricks (%.1f s)" % (len(one), t1)}
         if O.ref_gpu_available():
-            line["ref_kernels"] = ref_kernels_leg(ceng, w, stage, line.get("fast_mode"))
+            stage_x = line.get("exact_mode", {}).get("stage_ms", line["stage_ms"])
+            line["ref_kernels"] = ref_kernels_leg(ceng, w, stage_x, line.get("fast_mode"))
     if rank == 0:
         print(json.dumps(line), flush=True)
-    del out
-    eng.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -657,15 +737,27 @@ def run_batch(a):
 # DRAM bytes (read + write) per step of the dominant kernel, from one ncu
 # capture of the same workload (profiles/mc_item_edges_refine_exact_traffic_
 # rings58800_h025.md: both passes of k_refine_exact).
-TRAFFIC = {("rings58800", 0.25, "k_refine_exact"): 418628608 + 259481344 + 92997632 + 80039168}
+TRAFFIC = {("rings58800", 0.25, "k_refine_exact"): 1152510464 + 277156352 + 216691712 + 104072448}
 
 
-def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops=0):
+def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops=0, mode="exact"):
     """Roofline of the dominant kernel: its counted operations (or bytes) per
     launch over the launch's device time, against the matching peak."""
     ms = stage[dominant]
     hbm = pk.get("hbm_gbs", PEAKS_FALLBACK["hbm_gbs"])
     spb = (w["brick"] + 1) ** 3
+    if dominant == "refine" and xops and mode != "exact":
+        achieved = xops / (ms / 1e3) / 1e12
+        return {"kernel": "k_refine", "bound": "fp32", "achieved": achieved, "peak": FP32_NOFMA_TOPS,
+                "unit": "Tops/s", "frac": achieved / FP32_NOFMA_TOPS,
+                "traffic": TRAFFIC.get((w["name"], w["spacing"], "k_refine_" + mode)),
+                "peak_source": "nominal: 148 SMs x 128 FP32 lanes x 1965 MHz, one op per lane-cycle "
+                               "(no FMA contraction, bit-exact f32; sqrt and division counted as one op)",
+                "algorithmic_ops": xops,
+                "ms": ms, "ms_note": "the refinement stage: edge lists, warm starts (warm mode), the f32 "
+                                     "refinement and the vertex placement; the operations are those of the "
+                                     "refinement's field evaluations",
+                "sampler": roofline("sample", stage, info, ops, owned, w, pk, pk_kind, n_bricks)}
     if dominant == "refine" and xops:
         achieved = xops / (ms / 1e3) / 1e12
         return {"kernel": "k_refine_exact", "bound": "fp64", "achieved": achieved, "peak": FP64_NOFMA_TOPS,

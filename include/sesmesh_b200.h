@@ -329,6 +329,14 @@ int smb_batch_sample_features(const smb_batch* batch, uint32_t* out);
  * recorded the features (smb_batch_record_features; else SMB_ERR_STATE).
  * A null mlp is smb_refine. */
 int smb_refine_warm(smb_resident* res, smb_batch* batch, const smb_mlp* mlp, double* ms, char* err, size_t errlen);
+/* Re-runs the last run's f32 refinement (smb_refine, or smb_refine_warm
+ * with mlp) counting the f32 arithmetic operations of its field
+ * evaluations into *ops (the algorithmic count of its roofline: sqrt and
+ * division one each, compares and selects not counted; groups of 8 lanes;
+ * the edge results are written again, identically).  Discards the last
+ * placement (smb_place_fast). */
+int smb_batch_count_refine_ops(smb_batch* batch, const smb_mlp* mlp, unsigned long long* ops, char* err,
+                               size_t errlen);
 /* The MLP's input for every crossing edge of the last run (32 f32 per edge,
  * marching-cubes edge order; zeros for edges the device does not refine)
  * and covered[k] = 1 where the device refines edge k.  With t_lin = fa /

@@ -1302,9 +1302,9 @@ __device__ __forceinline__ void group_argmin(uint32_t gm, float& v, int& i) {
     }
 }
 
-template <int RG>
+template <int RG, bool COUNT = false>
 __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float band, float x, float y, float z,
-                                         int gl, uint32_t gm) {
+                                         int gl, uint32_t gm, unsigned long long* ops = nullptr) {
     static_assert(RG == 1 || RG == 8 || RG == 32, "groups of 1, 8 or 32 lanes");
     Eval e;
     e.qx = x, e.qy = y, e.qz = z;
@@ -1320,6 +1320,7 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
                 const float4 a = st.nearA[k];
                 const float dx = x - a.x, dy = y - a.y, dz = z - a.z;
                 v = sqrtf(dx * dx + dy * dy + dz * dz) - a.w;
+                if (COUNT) *ops += 9;
             }
             int w = k;
             group_argmin<RG>(gm, v, w);
@@ -1339,6 +1340,7 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
             float4 a = st.nearA[k];
             float dx = x - a.x, dy = y - a.y, dz = z - a.z;
             in = sqrtf(dx * dx + dy * dy + dz * dz) < a.w;
+            if (COUNT) *ops += 9;
         }
         if (__any_sync(gm, in)) {
             inside = true;
@@ -1363,6 +1365,7 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
     if (pruned) {
         const float qx = x - st.cx, qy = y - st.cy, qz = z - st.cz;
         slack = fmaxf(st.rho - sqrtf(qx * qx + qy * qy + qz * qz) - 1e-5f, 0.0f);
+        if (COUNT && gl == 0) *ops += 11;
     }
     const int g0 = int(threadIdx.x & 31) & ~(RG - 1);  // the group's first lane
     for (int i0 = 0; i0 < st.ns; i0 += RG) {
@@ -1375,11 +1378,14 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
             float dx = x - cx, dy = y - cy, dz = z - cz;
             float len = sqrtf(dx * dx + dy * dy + dz * dz);
             float lb = fabsf(len - rr);
+            if (COUNT) *ops += 10;
             if (!(lb >= best || len < 1e-12f)) {
                 float sc = rr / len;
                 qx = cx + dx * sc, qy = cy + dy * sc, qz = cz + dz * sc;
+                if (COUNT) *ops += 7;
                 bool free = true;
                 for (uint32_t p = st.s_off[i], e2 = st.s_off[i + 1]; p < e2 && free; p++) {
+                    if (COUNT) *ops += 8;
                     float4 t = st.nearT[st.s_blk[p]];
                     float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
                     free = ex * ex + ey * ey + ez * ez >= t.w;
@@ -1409,7 +1415,9 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
                 float wl = sqrtf(wx * wx + wy * wy + wz * wz);
                 float tt = wl - m.w;
                 float dist = sqrtf(along * along + tt * tt);
+                if (COUNT) *ops += 26;
                 if (!(dist >= best)) {
+                    if (COUNT) *ops += 9;
                     if (wl > 1e-12f) {
                         qx = m.x + (wx / wl) * m.w, qy = m.y + (wy / wl) * m.w, qz = m.z + (wz / wl) * m.w;
                     } else {
@@ -1417,6 +1425,7 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
                     }
                     bool free = true;
                     for (uint32_t p = st.c_off[i], e2 = st.c_off[i + 1]; p < e2 && free; p++) {
+                        if (COUNT) *ops += 8;
                         float4 t = st.nearT[st.c_blk[p]];
                         float ex = qx - t.x, ey = qy - t.y, ez = qz - t.z;
                         free = ex * ex + ey * ey + ez * ez >= t.w;
@@ -1441,6 +1450,7 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
             float4 p = st.V[i];
             float dx = x - p.x, dy = y - p.y, dz = z - p.z;
             v = sqrtf(dx * dx + dy * dy + dz * dz);
+            if (COUNT) *ops += 9;
         }
         int w = i;
         group_argmin<RG>(gm, v, w);
@@ -1449,6 +1459,7 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
             best = v, e.feat = (4u << FEAT_SHIFT_D) | uint32_t(__float_as_int(p.w)), e.qx = p.x, e.qy = p.y, e.qz = p.z;
         }
     }
+    if (COUNT && gl == 0) *ops += 1;
     e.value = probe - best;
     return e;
 }
@@ -1460,11 +1471,11 @@ __device__ __forceinline__ Eval eval_f32(const RefStage& st, float probe, float 
 // at t_start and is accepted only within the tolerance and on that
 // candidate; otherwise the iteration starts over from the linear guess, as
 // from t_start = t_lin with expect = 0 (the reference's fast mode).
-template <int RG>
+template <int RG, bool COUNT = false>
 __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const RefineConsts& RC, float probe, float band,
                                                 float ax, float ay, float az, uint32_t axis, float fa, float fb,
                                                 float t_start, uint32_t expect, uint32_t k, const RefOut& out, int gl,
-                                                uint32_t gm) {
+                                                uint32_t gm, unsigned long long* ops = nullptr) {
     const float h = RC.h_hi, hd = RC.h_hi + RC.h_lo;
     float t = t_start;
     float t0 = 0.0f, g0 = fa, t1 = 1.0f, g1 = fb;
@@ -1476,7 +1487,7 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
     if (expect) {
         const float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f),
                     z = az + (axis == 2 ? hd * t : 0.0f);
-        const Eval e = eval_f32<RG>(st, probe, band, x, y, z, gl, gm);
+        const Eval e = eval_f32<RG, COUNT>(st, probe, band, x, y, z, gl, gm, ops);
         evals++;
         last = e;
         if (fabsf(e.value) <= RC.tol && e.feat == expect) converged = true;
@@ -1484,7 +1495,7 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
     }
     for (uint32_t it = 0; it < RC.max_iter && !converged; it++) {
         float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
-        Eval e = eval_f32<RG>(st, probe, band, x, y, z, gl, gm);
+        Eval e = eval_f32<RG, COUNT>(st, probe, band, x, y, z, gl, gm, ops);
         evals++;
         last = e;
         float gv = e.value;
@@ -1524,7 +1535,7 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
         for (uint32_t it = 0; it < RC.max_bisect; it++) {
             t = 0.5f * (t0 + t1);
             float x = ax + (axis == 0 ? hd * t : 0.0f), y = ay + (axis == 1 ? hd * t : 0.0f), z = az + (axis == 2 ? hd * t : 0.0f);
-            Eval e = eval_f32<RG>(st, probe, band, x, y, z, gl, gm);
+            Eval e = eval_f32<RG, COUNT>(st, probe, band, x, y, z, gl, gm, ops);
             evals++;
             last = e;
             if (fabsf(e.value) <= RC.tol || (t1 - t0) * hd <= 2.0f * RC.tol) break;
@@ -1905,7 +1916,7 @@ struct RefinePlan {
     uint32_t cand_bytes;  // one staging region
 };
 
-template <int MODE, bool WIDE, bool MANY, int RG, int NT = 32 * REFINE_WARPS>
+template <int MODE, bool WIDE, bool MANY, int RG, int NT = 32 * REFINE_WARPS, bool COUNT = false>
 __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
     DArr A0, DLat L0, RefineConsts RC0, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
     const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
@@ -1978,7 +1989,13 @@ __global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
                 const float2 w = start[e];
                 t0 = w.x, expect = __float_as_uint(w.y);
             }
-            refine_edge_f32<RG>(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, expect, k, out, int(gl), gm);
+            unsigned long long ops = 0;
+            refine_edge_f32<RG, COUNT>(st, RC, probe, band, ax, ay, az, axis, fv.x, fv.y, t0, expect, k, out, int(gl),
+                                       gm, COUNT ? &ops : nullptr);
+            if (COUNT) {
+                for (int o = RG / 2; o; o >>= 1) ops += __shfl_xor_sync(gm, ops, o);
+                if (gl == 0 && ops) atomicAdd(&counters[CNT_OPS], ops);
+            }
         };
         if (WIDE || RG < 32) {
             // The block's (warp's) groups claim the edges one at a time
@@ -2196,7 +2213,7 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
                           const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
                           uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float2* start,
                           unsigned long long* counters, int sms, size_t smem_limit, cudaStream_t s, size_t* smem_out,
-                          const Scene* many, uint32_t* ovf, size_t region, int group) {
+                          const Scene* many, uint32_t* ovf, size_t region, int group, bool count) {
     auto al = [](size_t v) { return (v + 127) / 128 * 128; };
     RefinePlan P;
     P.cand_bytes = uint32_t(al(cand_bytes));
@@ -2233,6 +2250,16 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
     };
     const uint32_t quads = (n_items + REFINE_WARPS - 1) / REFINE_WARPS;
     const bool g32 = group == 32, warm = mode == REFINE_WARM;
+    auto pick = [&](auto narrow_k, auto wide_k) { return use_wide ? wide_k : narrow_k; };
+    if (count && !many) {
+        // The counting pass: groups of 8, every sub-block in one pass.
+        constexpr int NW = 32 * REFINE_WARPS;
+        auto kern = warm ? pick(k_refine<REFINE_WARM, false, false, 8, NW, true>,
+                                k_refine<REFINE_WARM, true, false, 8, NW, true>)
+                         : pick(k_refine<REFINE_PLAIN, false, false, 8, NW, true>,
+                                k_refine<REFINE_PLAIN, true, false, 8, NW, true>);
+        return run(kern, P, smem, nullptr, nullptr, use_wide ? n_items : quads);
+    }
     if (split) {
         RefinePlan PS = P;
         PS.cand_bytes = uint32_t(small);
@@ -2251,7 +2278,6 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
     }
     // Groups of lanes per edge: one lane in the many-structure pass (short
     // lists, few evaluations after the warm start), else 8 or 32 as asked.
-    auto pick = [&](auto narrow_k, auto wide_k) { return use_wide ? wide_k : narrow_k; };
     auto kern =
         many ? (warm ? pick(k_refine<REFINE_WARM, false, true, 1>, k_refine<REFINE_WARM, true, true, 1>)
                      : pick(k_refine<REFINE_PLAIN, false, true, 1>, k_refine<REFINE_PLAIN, true, true, 1>))

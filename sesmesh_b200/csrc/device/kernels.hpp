@@ -94,13 +94,16 @@ void launch_copy_count(unsigned long long* dst, const unsigned long long* src, c
 // (0: an eighth of smem_limit, two blocks to an SM) where four regions for the largest sub-block
 // would not fit or `region` is smaller, then a whole-block pass over the
 // sub-blocks that outgrow them.  group: lanes per edge in the single-
-// structure passes, 8 or 32 (32 pays for long candidate lists).
+// structure passes, 8 or 32 (32 pays for long candidate lists).  count
+// (single structure): the f32 operations of the field evaluations are added
+// to counters[CNT_OPS] (groups of 8, every sub-block in one pass).
 cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, const int4* keys, const uint32_t* work,
                           const uint32_t* rec, const uint32_t* ids, const uint32_t* edges, const float2* edge_vals,
                           const uint32_t* item_off, const uint32_t* item_edges, uint32_t n_items, float* t,
                           uint32_t* feat, float* q, uint32_t* evals, size_t cand_bytes, int mode, const float2* start,
                           unsigned long long* counters, int sms, size_t smem_limit, cudaStream_t s, size_t* smem_out,
-                          const Scene* many = nullptr, uint32_t* ovf = nullptr, size_t region = 0, int group = 8);
+                          const Scene* many = nullptr, uint32_t* ovf = nullptr, size_t region = 0, int group = 8,
+                          bool count = false);
 // The warm start's features of every row of the items' edge lists (32 f32
 // per row into x_out); feats: the sampler's nearest-feature words
 // (launch_sample with feats).  Grid-strided over at most max_rows rows (the

@@ -932,7 +932,7 @@ static int exact_group(const smb_batch* b) {
 // features into e_x, evals = 1 marks the edges covered).
 enum { PASS_PLAIN = 0, PASS_WARM = 1, PASS_FEATURES = 2 };
 static int refine_pass(smb_resident* r, smb_batch* b, int pass, const smb_mlp* mlp, double* ms, char* err,
-                       size_t errlen) {
+                       size_t errlen, bool count = false) {
     if (!r || !b || b->res != r) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
     if (!r->refine_ready) return set_err(err, errlen, "smb_resident_set_refinement must run first"), SMB_ERR_STATE;
     smb_device* d = r->dev;
@@ -980,6 +980,7 @@ static int refine_pass(smb_resident* r, smb_batch* b, int pass, const smb_mlp* m
     unsigned long long* cnt = b->counters.as<unsigned long long>();
     CK(cudaMemsetAsync(cnt + CNT_TIMEOUT, 0, 8, s));
     CK(cudaMemsetAsync(cnt + CNT_MAXITEM, 0, 8, s));
+    if (count) CK(cudaMemsetAsync(cnt + CNT_OPS, 0, 8, s));
     launch_item_edges(r->L, b->work.as<uint32_t>(), nw, b->rec.as<uint32_t>(), b->edge_off.as<uint32_t>(),
                       b->edges.as<uint32_t>(), b->item_counts.as<uint32_t>(), b->item_off.as<uint32_t>(),
                       b->item_edges.as<uint32_t>(), b->tiles.as<unsigned long long>(),
@@ -1006,7 +1007,7 @@ static int refine_pass(smb_resident* r, smb_batch* b, int pass, const smb_mlp* m
                                   b->e_evals.as<uint32_t>(), cand, mode,
                                   pass == PASS_WARM ? b->w_start.as<float2>() : nullptr, cnt, d->info.multiprocessors,
                                   d->smem_optin, s, nullptr, nullptr, b->x_ovf.as<uint32_t>(), b->r_region,
-                                  refine_group(b));
+                                  refine_group(b), count);
     if (e != cudaSuccess) return set_err(err, errlen, "refine launch: %s", cudaGetErrorString(e)), SMB_ERR_CUDA;
     cudaEventRecord(b->ev[5], s);
     CK(cudaStreamSynchronize(s));
@@ -1022,6 +1023,15 @@ static int refine_pass(smb_resident* r, smb_batch* b, int pass, const smb_mlp* m
 
 int smb_refine(smb_resident* r, smb_batch* b, double* ms, char* err, size_t errlen) {
     return refine_pass(r, b, PASS_PLAIN, nullptr, ms, err, errlen);
+}
+
+int smb_batch_count_refine_ops(smb_batch* b, const smb_mlp* mlp, unsigned long long* ops, char* err,
+                               size_t errlen) {
+    if (!b || !ops) return set_err(err, errlen, "bad arguments"), SMB_ERR_ARG;
+    int rc = refine_pass(b->res, b, mlp ? PASS_WARM : PASS_PLAIN, mlp, nullptr, err, errlen, true);
+    if (rc) return rc;
+    CK(cudaMemcpy(ops, b->counters.as<unsigned long long>() + CNT_OPS, 8, cudaMemcpyDeviceToHost));
+    return SMB_OK;
 }
 
 int smb_refine_warm(smb_resident* r, smb_batch* b, const smb_mlp* mlp, double* ms, char* err, size_t errlen) {

@@ -161,6 +161,7 @@ SIGNATURES = {
                                           C.POINTER(C.c_ulonglong)]),
     "smb_place_fast": (C.c_int, [_vp, _vp, C.POINTER(C.c_double), _cp, _sz]),
     "smb_batch_count_exact_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), _cp, _sz]),
+    "smb_batch_count_refine_ops": (C.c_int, [_vp, _vp, C.POINTER(C.c_ulonglong), _cp, _sz]),
     "smb_kernel_launches": (C.c_ulonglong, []),
     "smb_batch_info_get": (C.c_int, [_vp, C.POINTER(BatchInfo)]),
     "smb_batch_count_ops": (C.c_int, [_vp, C.POINTER(C.c_ulonglong), C.POINTER(C.c_ulonglong), _cp, _sz]),

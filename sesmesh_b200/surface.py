@@ -281,6 +281,17 @@ class SurfaceEngine:
         _check(lib().smb_batch_count_exact_ops(b, C.byref(ops), err, 1024), err)
         return ops.value
 
+    def count_refine_ops(self, mlp=None):
+        """f32 operations of the field evaluations of the last run's fast-mode
+        refinement (plain, or from the warm start with mlp), counted by
+        re-running it."""
+        b = lib().smb_engine_batch(self.h)
+        err = C.create_string_buffer(1024)
+        ops = C.c_ulonglong(0)
+        _check(lib().smb_batch_count_refine_ops(b, mlp.h if mlp is not None else None, C.byref(ops), err, 1024),
+               err)
+        return ops.value
+
     def count_ops(self):
         """f32 operations and evaluated samples of the last run's sampling pass."""
         b = lib().smb_engine_batch(self.h)
