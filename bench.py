@@ -736,8 +736,10 @@ def run_batch(a):
 
 # DRAM bytes (read + write) per step of the dominant kernel, from one ncu
 # capture of the same workload (profiles/mc_item_edges_refine_exact_traffic_
-# rings58800_h025.md: both passes of k_refine_exact).
-TRAFFIC = {("rings58800", 0.25, "k_refine_exact"): 1152510464 + 277156352 + 216691712 + 104072448}
+# rings58800_h025.md: both passes of k_refine_exact; profiles/
+# refine_f32_warm_rings58800_h025.md: k_refine from the warm starts).
+TRAFFIC = {("rings58800", 0.25, "k_refine_exact"): 1152510464 + 277156352 + 216691712 + 104072448,
+           ("rings58800", 0.25, "k_refine_warm"): 1361073920 + 193664000}
 
 
 def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops=0, mode="exact"):
