@@ -567,8 +567,15 @@ def ref_kernels_leg(ceng, w, stage, fast, reps=5):
 def fallbacks(st):
     """Work the device path handed to the host: the arrangement (1 built on
     the device, 0 on the host below the device threshold, 2 the device
-    declined), meshes finished on the host, edges refined on the host."""
-    return {k: int(st.get(k, 0)) for k in ("arrangement_where", "finished_on_host", "refine_cpu_edges")}
+    declined), meshes finished on the host and their host-refined edges.
+    In fast mode the edges whose f32 search ends without converging go to
+    the f64 refinement, as the reference sends them to its CPU refiner
+    (refine_cpu_edges); on the device path that f64 pass runs on the
+    device (f64_pass_edges)."""
+    host = int(st.get("finished_on_host", 0))
+    cpu = int(st.get("refine_cpu_edges", 0))
+    return {"arrangement_where": int(st.get("arrangement_where", 0)), "finished_on_host": host,
+            "host_refined_edges": cpu if host else 0, "f64_pass_edges": 0 if host else cpu}
 
 
 def shell_leg(dev, reps=2):

@@ -358,29 +358,60 @@ __device__ int any_exposed(Spans& S, const Circle& C, const double4* sph) {
     return 0;
 }
 
+// The row entries (i, j) with j > i, whose circles k_circles builds: rows
+// ascend, so they are each row's tail; per row their count, then (at the
+// scanned offsets) each one's entry index and row.
+__global__ void k_upper_count(const uint32_t* nb_off, const uint32_t* nb_items, size_t n, uint32_t* cnt) {
+    const size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    uint32_t lo = nb_off[i], hi = nb_off[i + 1];
+    const uint32_t end = hi;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (nb_items[mid] <= uint32_t(i)) lo = mid + 1;
+        else hi = mid;
+    }
+    cnt[i] = end - lo;
+}
+
+__global__ void k_upper_fill(const uint32_t* nb_off, const uint32_t* cnt, const uint32_t* uoff, size_t n,
+                             uint32_t* uent, uint32_t* urow) {
+    const size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t c = cnt[i], end = nb_off[i + 1], o = uoff[i];
+    for (uint32_t t = 0; t < c; t++) uent[o + t] = end - c + t, urow[o + t] = uint32_t(i);
+}
+
+// The upper entries whose circle is exposed, at their circle's index.
+__global__ void k_exposed_list(const uint32_t* uent, size_t n_upper, const uint32_t* c_ex, const uint32_t* o_circ,
+                               uint32_t* xlist) {
+    const size_t u = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (u >= n_upper) return;
+    const uint32_t e = uent[u];
+    if (c_ex[e]) xlist[o_circ[e]] = uint32_t(u);
+}
+
 // Circles, blockers and triple points of each row entry (i, j > i)
-// (arrangement.rs:674-752).  Count pass: per entry the circle's exposure
-// (0/1), blocker and vertex counts, exposed[] of both spheres; fill pass:
-// the records at the scanned offsets.
+// (arrangement.rs:674-752), a thread per upper entry (uent, urow).  Count
+// pass: per entry the circle's exposure (0/1), blocker and vertex counts
+// (zero beforehand for every entry), exposed[] of both spheres; fill pass,
+// a thread per exposed circle (xlist): the records at the scanned offsets.
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_circles(const double4* sph, size_t n, const uint32_t* nb_off,
-                                                 const uint32_t* nb_items, size_t n_entries, uint32_t* c_ex,
+                                                 const uint32_t* nb_items, size_t n_threads, const uint32_t* uent,
+                                                 const uint32_t* urow, const uint32_t* xlist, uint32_t* c_ex,
                                                  uint32_t* c_blk, uint32_t* c_vtx, uint32_t* exposed,
                                                  const uint32_t* o_circ, const uint32_t* o_blk, const uint32_t* o_vtx,
                                                  double* circ, uint32_t* ij, uint32_t* cb_off, uint32_t* cb_items,
                                                  double4* vert, uint32_t* vatoms, uint32_t* decline) {
-    const size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
-    if (e >= n_entries) return;
+    const size_t id = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (id >= n_threads) return;
+    const uint32_t u = FILL ? xlist[id] : uint32_t(id);
+    const size_t e = uent[u];
     auto zero = [&] {
         if (!FILL) c_ex[e] = 0, c_blk[e] = 0, c_vtx[e] = 0;
     };
-    size_t lo = 0, hi = n;  // the row holding entry e: nb_off[lo] <= e < nb_off[lo + 1]
-    while (hi - lo > 1) {
-        const size_t mid = (lo + hi) >> 1;
-        if (nb_off[mid] <= e) lo = mid;
-        else hi = mid;
-    }
-    const uint32_t i = uint32_t(lo), j = nb_items[e];
+    const uint32_t i = urow[u], j = nb_items[e];
     if (j <= i) return zero();
     if (FILL && !c_ex[e]) return;
     const double4 si = sph[i], sj = sph[j];
@@ -687,12 +718,37 @@ int build_arrangement_device(smb_device* d, const double* xyzr, size_t ns, doubl
     unsigned long long* tiles_e =
         static_cast<unsigned long long*>(X.alloc(size_t(scan_tiles_needed(uint32_t(n_entries))) * 8 + 64, false));
     if (!X.ok) return fail("device memory");
+    uint32_t* ucnt = static_cast<uint32_t*>(X.alloc(n * 4 + 4, false));
+    uint32_t* uoff = static_cast<uint32_t*>(X.alloc(n * 4 + 4, false));
+    if (!X.ok) return fail("device memory");
     cudaMemsetAsync(exposed, 0, n * 4 + 4, s);
     cudaMemsetAsync(decline, 0, 16, s);
+    // The upper entries (j > i) as a list, so that every thread of the
+    // circle passes has a pair to build.
+    size_t n_upper = 0;
+    uint32_t *uent = nullptr, *urow = nullptr;
     if (n_entries) {
-        k_circles<false><<<blocks_for(n_entries, 128), 128, 0, s>>>(
-            sph, n, roff, items, n_entries, c_ex, c_blk, c_vtx, exposed, nullptr, nullptr, nullptr, nullptr, nullptr,
-            nullptr, nullptr, nullptr, nullptr, decline);
+        k_upper_count<<<blocks_for(n), 256, 0, s>>>(roff, items, n, ucnt);
+        launch_scan(ucnt, uint32_t(n), uoff, nullptr, tiles, total, s);
+        unsigned long long h_up = 0;
+        if (cudaMemcpyAsync(&h_up, total, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return fail("upper entries");
+        n_upper = size_t(h_up);
+        uent = static_cast<uint32_t*>(X.alloc(n_upper * 4 + 4, false));
+        urow = static_cast<uint32_t*>(X.alloc(n_upper * 4 + 4, false));
+        if (!X.ok) return fail("device memory");
+        k_upper_fill<<<blocks_for(n), 256, 0, s>>>(roff, ucnt, uoff, n, uent, urow);
+        count_launches(3);
+    }
+    if (n_entries) {
+        cudaMemsetAsync(c_ex, 0, n_entries * 4, s);
+        cudaMemsetAsync(c_blk, 0, n_entries * 4, s);
+        cudaMemsetAsync(c_vtx, 0, n_entries * 4, s);
+        if (n_upper)
+            k_circles<false><<<blocks_for(n_upper, 128), 128, 0, s>>>(
+                sph, n, roff, items, n_upper, uent, urow, nullptr, c_ex, c_blk, c_vtx, exposed, nullptr, nullptr,
+                nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, decline);
         launch_scan(c_ex, uint32_t(n_entries), o_circ, nullptr, tiles_e, total, s);
         launch_scan(c_blk, uint32_t(n_entries), o_blk, nullptr, tiles_e, total + 1, s);
         launch_scan(c_vtx, uint32_t(n_entries), o_vtx, nullptr, tiles_e, total + 2, s);
@@ -723,10 +779,15 @@ int build_arrangement_device(smb_device* d, const double* xyzr, size_t ns, doubl
     uint32_t* keep_len = static_cast<uint32_t*>(X.alloc(n * 4, false));
     uint32_t* nb_off = static_cast<uint32_t*>(X.alloc((n + 1) * 4, true));
     if (!X.ok) return fail("device memory");
-    if (n_entries)
-        k_circles<true><<<blocks_for(n_entries, 128), 128, 0, s>>>(sph, n, roff, items, n_entries, c_ex, c_blk, c_vtx,
-                                                                 exposed, o_circ, o_blk, o_vtx, circ, ij, cb_off,
-                                                                 cb_items, vert, vatoms, decline);
+    if (nc) {
+        uint32_t* xlist = static_cast<uint32_t*>(X.alloc(nc * 4, false));
+        if (!X.ok) return fail("device memory");
+        k_exposed_list<<<blocks_for(n_upper), 256, 0, s>>>(uent, n_upper, c_ex, o_circ, xlist);
+        k_circles<true><<<blocks_for(nc, 128), 128, 0, s>>>(sph, n, roff, items, nc, uent, urow, xlist, c_ex, c_blk,
+                                                          c_vtx, exposed, o_circ, o_blk, o_vtx, circ, ij, cb_off,
+                                                          cb_items, vert, vatoms, decline);
+        count_launches(1);
+    }
     k_put<<<1, 32, 0, s>>>(cb_off + nc, uint32_t(ncb));
     // Statuses and the rows of exposed spheres.
     if (n) {
