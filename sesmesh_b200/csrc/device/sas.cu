@@ -234,7 +234,8 @@ __global__ void k_rows(const double4* sph, const uint32_t* contained, size_t n, 
     grid_near(g, ci, si.w + max_expanded, [&](uint32_t j) {
         if (j == i || contained[j]) return;
         const double4 sj = sph[j];
-        if (distp(ci, xyz(sj)) < si.w + sj.w - S_EPS) {
+        const D3 dc = ci - xyz(sj);
+        if (sqrt_lt(dotp(dc, dc), si.w + sj.w - S_EPS)) {  // |ci - cj| < Ri + Rj - eps
             if (FILL) row[c] = j;
             c++;
         }
@@ -474,8 +475,11 @@ __global__ void __launch_bounds__(128) k_circles(const double4* sph, size_t n, c
             for (uint32_t pl = ri0; pl < ri1 && free; pl++) {
                 const uint32_t l = nb_items[pl];
                 if (l != j && l != k) {
+                    // |p - c| >= R - eps, decided from the square where it
+                    // is clear (sqrt_ge: the same result as the rounded root).
                     const double4 sl = sph[l];
-                    free = distp(p, xyz(sl)) >= sl.w - S_EPS;
+                    const D3 dp = p - xyz(sl);
+                    free = sqrt_ge(dotp(dp, dp), sl.w - S_EPS);
                 }
             }
             if (free) {
