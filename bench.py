@@ -432,6 +432,7 @@ def run_ours(a):
     if rank == 0 and world == 1 and not a.no_configs and a.workload == "rings58800" and not a.spheres:
         line["shell2400k"] = shell_leg(dev)
         line["batch512"] = batch_leg(dev)
+        line["1AON"] = aon_leg(dev)
     if rank == 0 and world == 1 and not a.no_cpu:
         ceng, sample, spb_, k, nb = cpu_leg(w)
         t, _ = ceng.mesh_sample(sample)
@@ -576,6 +577,63 @@ def fallbacks(st):
     cpu = int(st.get("refine_cpu_edges", 0))
     return {"arrangement_where": int(st.get("arrangement_where", 0)), "finished_on_host": host,
             "host_refined_edges": cpu if host else 0, "f64_pass_edges": 0 if host else cpu}
+
+
+# The reference's published wall times for 1AON at 0.25 A (CLI, best of 5,
+# OBJ written to /dev/null, device open excluded; mesh stage in brackets):
+# docs/05-gpu-hip.md:613 and docs/06-gpu-cuda.md:177.
+AON_PUBLISHED_MS = {
+    "cpu_16_zen5": {"total": 3403, "mesh_stage": 2504},
+    "radeon_8060s_exact": {"total": 2366, "mesh_stage": 1463}, "radeon_8060s_fast": {"total": 1411, "mesh_stage": 534},
+    "rtx2070_exact": {"total": 6984, "mesh_stage": 4497}, "rtx2070_fast": {"total": 4192, "mesh_stage": 1357},
+}
+
+
+def aon_leg(dev, reps=3):
+    """1AON (GroEL-GroES, the reference's own data/1aon.pdb, 58,870 atoms
+    after the default selection) at 0.25 A, timed as the reference's CLI
+    numbers are: parse the PDB text, mesh, write the OBJ to /dev/null; exact
+    mode, plain fast mode and fast mode with the learned warm start; best of
+    `reps` after a warm-up.  Gzip decompression of the committed fixture is
+    outside the timing (the reference reads the plain file)."""
+    import gzip
+    from sesmesh_b200 import native, structure, warm_start
+    from sesmesh_b200 import surface as S
+    with gzip.open(os.path.join(ROOT, "tests", "golden", "1AON.pdb.gz"), "rb") as f:
+        text = f.read()
+    out = {"workload": "1AON (58,870 atoms), probe 1.4 A, spacing 0.25 A, brick 10",
+           "published_ms": AON_PUBLISHED_MS}
+    mlp = None
+    for mode in ("exact", "fast", "fast+warm"):
+        p = S.SurfaceParams.ses(1.4).with_spacing(0.25).with_refine("exact" if mode == "exact" else "fast")
+        best, st = None, None
+        for r in range(reps + 1):
+            t0 = time.perf_counter()
+            spheres = structure.read_bytes(text, "pdb")
+            t1 = time.perf_counter()
+            if mode == "fast+warm":
+                eng = S.SurfaceEngine(spheres, p)
+                if mlp is None:
+                    mlp = native.Mlp(eng.dev, warm_start.load())
+                eng.set_warm_start(mlp)
+                mesh = eng.mesh()
+            else:
+                eng = None
+                mesh = S.compute_surface(spheres, p)
+            t2 = time.perf_counter()
+            mesh.write_obj(os.devnull)
+            t3 = time.perf_counter()
+            times = {"parse": 1e3 * (t1 - t0), "mesh": 1e3 * (t2 - t1), "obj": 1e3 * (t3 - t2),
+                     "total": 1e3 * (t3 - t0)}
+            if r and (best is None or times["total"] < best["total"]):
+                best = times
+            st = mesh.stats
+            mesh.close()
+            if eng is not None:
+                eng.close()
+        out[mode] = {"ms": best, "vertices": int(st["vertices"]), "triangles": int(st["triangles"]),
+                     "area": st["area"], "volume": st["volume"], "refine_evaluations": int(st["refine_evaluations"])}
+    return out
 
 
 def shell_leg(dev, reps=2):
