@@ -61,7 +61,7 @@ struct smb_surface {
     Mesh mesh;
     std::vector<Component> comps;
     smb_surface_stats stats{};
-    std::string obj;
+    smbh::ObjText obj;
     // A mesh finished on the device stays in the page-locked block its
     // results came back in (view points into it); else view is of mesh.
     void* block = nullptr;

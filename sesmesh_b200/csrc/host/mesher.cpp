@@ -699,6 +699,22 @@ void components_and_group(Mesh& m, std::vector<Component>& comps, const EdgeUses
     m.triangles.swap(out);
 }
 
+// Decimal digits of v (what "%llu" prints) at the end of d[20]; their count.
+static inline int u64_digits(uint64_t v, char d[20]) {
+    int n = 0;
+    do {
+        d[19 - n++] = char('0' + v % 10);
+        v /= 10;
+    } while (v);
+    return n;
+}
+
+static inline void push_u64(std::string& buf, uint64_t v) {
+    char d[20];
+    const int n = u64_digits(v, d);
+    buf.append(d + 20 - n, size_t(n));
+}
+
 // export/fmt.rs:30-53: exact for f32 because x * 10^prec is exact in f64.
 void push_fixed(std::string& buf, float x, int prec) {
     static const uint64_t P10[10] = {1, 10, 100, 1000, 10000, 100000, 1000000, 10000000, 100000000, 1000000000};
@@ -715,9 +731,7 @@ void push_fixed(std::string& buf, float x, int prec) {
     }
     if (std::signbit(x)) buf.push_back('-');
     uint64_t mnt = uint64_t(std::fabs(scaled));
-    char digits[24];
-    int nd = std::snprintf(digits, sizeof digits, "%llu", (unsigned long long)(mnt / P10[prec]));
-    buf.append(digits, size_t(nd));
+    push_u64(buf, mnt / P10[prec]);
     if (prec > 0) {
         buf.push_back('.');
         uint64_t f = mnt % P10[prec];
@@ -727,53 +741,163 @@ void push_fixed(std::string& buf, float x, int prec) {
     }
 }
 
+// push_fixed into a raw buffer (room for 64 bytes at p); the end.  The
+// common case (finite, |x 10^prec| < 1e18) is written directly, the rest
+// through push_fixed.  P is the precision when it is known at compile time
+// (the default 4), else 0 and prec is used.
+template <int P>
+static inline char* put_fixed(char* p, float x, int prec) {
+    static const uint64_t P10[10] = {1, 10, 100, 1000, 10000, 100000, 1000000, 10000000, 100000000, 1000000000};
+    const int pr = P ? P : prec;
+    const double scaled = std::nearbyint(double(x) * double(P ? P10[P] : P10[pr]));
+    if (!std::isfinite(scaled) || std::fabs(scaled) >= 1e18) {
+        std::string tmp;
+        push_fixed(tmp, x, pr);
+        std::memcpy(p, tmp.data(), tmp.size());
+        return p + tmp.size();
+    }
+    if (std::signbit(x)) *p++ = '-';
+    const uint64_t mnt = uint64_t(std::fabs(scaled));
+    const uint64_t ip = P ? mnt / P10[P] : mnt / P10[pr];
+    uint64_t f = mnt - ip * (P ? P10[P] : P10[pr]);
+    char d[20];
+    const int n = u64_digits(ip, d);
+    std::memcpy(p, d + 20 - n, size_t(n));
+    p += n;
+    if (pr > 0) {
+        *p++ = '.';
+        for (int k = pr - 1; k >= 0; k--) p[k] = char('0' + f % 10), f /= 10;
+        p += pr;
+    }
+    return p;
+}
+
+// Bytes put_fixed writes for x.
+template <int P>
+static inline size_t fixed_len(float x, int prec) {
+    static const uint64_t P10[10] = {1, 10, 100, 1000, 10000, 100000, 1000000, 10000000, 100000000, 1000000000};
+    const int pr = P ? P : prec;
+    const double scaled = std::nearbyint(double(x) * double(P ? P10[P] : P10[pr]));
+    if (!std::isfinite(scaled) || std::fabs(scaled) >= 1e18) {
+        std::string tmp;
+        push_fixed(tmp, x, pr);
+        return tmp.size();
+    }
+    const uint64_t ip = uint64_t(std::fabs(scaled)) / (P ? P10[P] : P10[pr]);
+    size_t n = 1;
+    for (uint64_t v = ip; v >= 10; v /= 10) n++;
+    return (std::signbit(x) ? 1 : 0) + n + (pr > 0 ? 1 + size_t(pr) : 0);
+}
+
+static inline size_t u64_len(uint64_t v) {
+    size_t n = 1;
+    for (; v >= 10; v /= 10) n++;
+    return n;
+}
+
 // export/obj.rs:144-236, default options: header, object "ses", v, vn, f a//a.
-std::string obj_text(const MeshRef& m, int precision, bool normals) {
-    normals = normals && m.nrm;
+// Two passes over chunks of lines on the host threads: the exact byte count
+// of each chunk, then each chunk formatted straight into its place, so the
+// text is written once into one buffer (no intermediate copies).
+static const char OBJ_HEAD[] = "# sesmesh 1.3.2\no ses\n";
+constexpr size_t OBJ_CH = 1 << 15;
+
+struct ObjPlan {
+    std::vector<size_t> at;  // chunk start offsets: v chunks, vn chunks, f chunks, then the end
+    size_t nvc = 0, nfc = 0;
+    bool normals = false;
+};
+
+static ObjPlan obj_plan(const MeshRef& m, int precision, bool normals) {
+    ObjPlan P;
+    P.normals = normals && m.nrm;
     const size_t nv = m.nv, nt = m.nt;
-    const size_t CH = 1 << 15;
-    auto vec_lines = [&](const float* data, const char* tag, std::vector<std::string>& out) {
-        out.assign((nv + CH - 1) / CH, std::string());
-        parallel_for(out.size(), [&](size_t c, int) {
-            std::string& s = out[c];
-            s.reserve(CH * 32);
-            for (size_t i = c * CH; i < std::min(nv, (c + 1) * CH); i++) {
-                s += tag;
+    P.nvc = (nv + OBJ_CH - 1) / OBJ_CH, P.nfc = (nt + OBJ_CH - 1) / OBJ_CH;
+    const size_t nvec = P.normals ? 2 : 1, nch = nvec * P.nvc + P.nfc;
+    std::vector<size_t> len(nch, 0);
+    parallel_for(nch, [&](size_t c, int) {
+        size_t n = 0;
+        if (c < nvec * P.nvc) {
+            const bool nrm = c >= P.nvc;
+            const float* data = nrm ? m.nrm : m.pos;
+            const size_t ch = nrm ? c - P.nvc : c;
+            for (size_t i = ch * OBJ_CH, e = std::min(nv, (ch + 1) * OBJ_CH); i < e; i++) {
+                n += (nrm ? 3 : 2) + 2 + 1;  // tag, two spaces, newline
+                for (int k = 0; k < 3; k++)
+                    n += precision == 4 ? fixed_len<4>(data[3 * i + k], 4) : fixed_len<0>(data[3 * i + k], precision);
+            }
+        } else {
+            const size_t ch = c - nvec * P.nvc;
+            for (size_t t = ch * OBJ_CH, e = std::min(nt, (ch + 1) * OBJ_CH); t < e; t++) {
+                n += 2;  // 'f', newline
                 for (int k = 0; k < 3; k++) {
-                    if (k) s.push_back(' ');
-                    push_fixed(s, data[3 * i + k], precision);
+                    const size_t d = u64_len(uint64_t(m.tris[3 * t + k]) + 1);
+                    n += 1 + (P.normals ? 2 * d + 2 : d);
                 }
-                s.push_back('\n');
             }
-        });
-    };
-    std::vector<std::string> v, vn, f;
-    vec_lines(m.pos, "v ", v);
-    if (normals) vec_lines(m.nrm, "vn ", vn);
-    f.assign((nt + CH - 1) / CH, std::string());
-    parallel_for(f.size(), [&](size_t c, int) {
-        std::string& s = f[c];
-        s.reserve(CH * 40);
-        char num[24];
-        for (size_t t = c * CH; t < std::min(nt, (c + 1) * CH); t++) {
-            s.push_back('f');
-            for (int k = 0; k < 3; k++) {
-                int len = std::snprintf(num, sizeof num, "%llu", (unsigned long long)(uint64_t(m.tris[3 * t + k]) + 1));
-                s.push_back(' ');
-                s.append(num, size_t(len));
-                if (normals) s += "//", s.append(num, size_t(len));
+        }
+        len[c] = n;
+    });
+    P.at.assign(nch + 1, sizeof OBJ_HEAD - 1);
+    for (size_t c = 0; c < nch; c++) P.at[c + 1] = P.at[c] + len[c];
+    return P;
+}
+
+static void obj_fill(const MeshRef& m, int precision, const ObjPlan& P, char* out) {
+    std::memcpy(out, OBJ_HEAD, sizeof OBJ_HEAD - 1);
+    const size_t nv = m.nv, nt = m.nt;
+    const size_t nvec = P.normals ? 2 : 1, nch = nvec * P.nvc + P.nfc;
+    parallel_for(nch, [&](size_t c, int) {
+        char* p = out + P.at[c];
+        if (c < nvec * P.nvc) {
+            const bool nrm = c >= P.nvc;
+            const float* data = nrm ? m.nrm : m.pos;
+            const size_t ch = nrm ? c - P.nvc : c;
+            for (size_t i = ch * OBJ_CH, e = std::min(nv, (ch + 1) * OBJ_CH); i < e; i++) {
+                *p++ = 'v';
+                if (nrm) *p++ = 'n';
+                *p++ = ' ';
+                for (int k = 0; k < 3; k++) {
+                    if (k) *p++ = ' ';
+                    p = precision == 4 ? put_fixed<4>(p, data[3 * i + k], 4) : put_fixed<0>(p, data[3 * i + k], precision);
+                }
+                *p++ = '\n';
             }
-            s.push_back('\n');
+        } else {
+            const size_t ch = c - nvec * P.nvc;
+            for (size_t t = ch * OBJ_CH, e = std::min(nt, (ch + 1) * OBJ_CH); t < e; t++) {
+                *p++ = 'f';
+                for (int k = 0; k < 3; k++) {
+                    char d[20];
+                    const int n = u64_digits(uint64_t(m.tris[3 * t + k]) + 1, d);
+                    *p++ = ' ';
+                    std::memcpy(p, d + 20 - n, size_t(n));
+                    p += n;
+                    if (P.normals) {
+                        *p++ = '/', *p++ = '/';
+                        std::memcpy(p, d + 20 - n, size_t(n));
+                        p += n;
+                    }
+                }
+                *p++ = '\n';
+            }
         }
     });
-    size_t total = 32;
-    for (auto* part : {&v, &vn, &f})
-        for (auto& s : *part) total += s.size();
-    std::string out;
-    out.reserve(total);
-    out += "# sesmesh 1.3.2\no ses\n";
-    for (auto* part : {&v, &vn, &f})
-        for (auto& s : *part) out += s;
+}
+
+ObjText obj_text_buffer(const MeshRef& m, int precision, bool normals) {
+    const ObjPlan P = obj_plan(m, precision, normals);
+    ObjText t;
+    t.size = P.at.back();
+    t.data.reset(new char[t.size]);
+    obj_fill(m, precision, P, t.data.get());
+    return t;
+}
+
+std::string obj_text(const MeshRef& m, int precision, bool normals) {
+    const ObjPlan P = obj_plan(m, precision, normals);
+    std::string out(P.at.back(), '\0');
+    obj_fill(m, precision, P, &out[0]);
     return out;
 }
 

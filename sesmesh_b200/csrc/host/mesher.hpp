@@ -5,6 +5,7 @@
 #include <array>
 #include <cstdint>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include "geom.hpp"
@@ -139,6 +140,13 @@ struct MeshRef {
 };
 
 std::string obj_text(const MeshRef& m, int precision = 4, bool normals = true);
+// The same text in a buffer that is written once (not zero-filled first).
+struct ObjText {
+    std::unique_ptr<char[]> data;
+    size_t size = 0;
+    bool empty() const { return !data; }
+};
+ObjText obj_text_buffer(const MeshRef& m, int precision = 4, bool normals = true);
 inline std::string obj_text(const Mesh& m, int precision = 4, bool normals = true) {
     return obj_text(MeshRef::of(m), precision, normals);
 }

@@ -718,19 +718,19 @@ int smb_surface_arrays(const smb_surface* s, const float** pos, const float** nr
 
 size_t smb_surface_obj(smb_surface* s, char* out, size_t cap) {
     if (!s) return 0;
-    if (s->obj.empty()) s->obj = obj_text(s->ref());
-    if (out) std::memcpy(out, s->obj.data(), s->obj.size() < cap ? s->obj.size() : cap);
-    return s->obj.size();
+    if (s->obj.empty()) s->obj = obj_text_buffer(s->ref());
+    if (out) std::memcpy(out, s->obj.data.get(), s->obj.size < cap ? s->obj.size : cap);
+    return s->obj.size;
 }
 
 int smb_surface_write_obj(smb_surface* s, const char* path, char* err, size_t errlen) {
     if (!s || !path) return SMB_ERR_ARG;
-    if (s->obj.empty()) s->obj = obj_text(s->ref());
+    if (s->obj.empty()) s->obj = obj_text_buffer(s->ref());
     FILE* f = std::fopen(path, "wb");
     if (!f) return set_err(err, errlen, "cannot open %s", path), SMB_ERR_ARG;
-    size_t w = std::fwrite(s->obj.data(), 1, s->obj.size(), f);
+    size_t w = std::fwrite(s->obj.data.get(), 1, s->obj.size, f);
     std::fclose(f);
-    if (w != s->obj.size()) return set_err(err, errlen, "short write to %s", path), SMB_ERR_ARG;
+    if (w != s->obj.size) return set_err(err, errlen, "short write to %s", path), SMB_ERR_ARG;
     return SMB_OK;
 }
 
