@@ -123,6 +123,35 @@ std::string trim(const char* s, size_t n) {
 
 bool parse_double(const std::string& t, double& v) {
     if (t.empty()) return false;
+    // [+-]digits[.digits] with at most 15 digits (the fixed-point columns of
+    // PDB and mmCIF coordinates): mantissa / 10^k, both exact in f64, so the
+    // one division rounds the decimal value correctly, as strtod does.
+    {
+        size_t i = 0, nd = 0, frac = 0;
+        bool neg = false, dot = false, ok = true;
+        uint64_t mant = 0;
+        if (t[0] == '+' || t[0] == '-') neg = t[0] == '-', i = 1;
+        for (; i < t.size(); i++) {
+            const char c = t[i];
+            if (c >= '0' && c <= '9') {
+                mant = mant * 10 + uint64_t(c - '0');
+                nd++;
+                if (dot) frac++;
+            } else if (c == '.' && !dot) {
+                dot = true;
+            } else {
+                ok = false;
+                break;
+            }
+        }
+        if (ok && nd > 0 && nd <= 15) {
+            static const double P10[16] = {1e0, 1e1, 1e2, 1e3, 1e4, 1e5, 1e6, 1e7,
+                                           1e8, 1e9, 1e10, 1e11, 1e12, 1e13, 1e14, 1e15};
+            const double a = double(mant) / P10[frac];
+            v = neg ? -a : a;
+            return true;
+        }
+    }
     char* end = nullptr;
     v = std::strtod(t.c_str(), &end);
     return end == t.c_str() + t.size() && std::isfinite(v);

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libsesmesh_b200.so")
 SYNTH_PATH = os.path.join(_HERE, "libsesmesh_synth.so")
 
 SMB_OK = 0
+SMB_ERR_MEMORY = 6
 ERRORS = {1: "argument", 2: "cuda", 3: "no device", 4: "self-test", 5: "range", 6: "memory", 7: "state",
           8: "timeout", 9: "cancelled"}
 REC_WORDS = 12

@@ -24,12 +24,17 @@ def read_bytes(data, fmt="auto", model=None, hydrogens=False, waters=False, hete
     sel = native.Selection_(int(model or 0), int(bool(hydrogens)), int(bool(waters)), int(bool(hetero)))
     err = C.create_string_buffer(1024)
     n = C.c_size_t(0)
-    _check(lib().smb_read_structure(data, len(data), FORMATS[fmt], C.byref(sel), None, 0, C.byref(n), err, 1024),
-           err)
-    out = np.zeros((n.value, 4))
-    _check(lib().smb_read_structure(data, len(data), FORMATS[fmt], C.byref(sel), _p(out, C.c_double), n.value,
-                                    C.byref(n), err, 1024), err)
-    return out
+    # One pass for the usual case: an atom record takes more than 32 bytes of
+    # text, so this capacity holds every atom; a second pass only if not.
+    out = np.zeros((len(data) // 32 + 16, 4))
+    rc = lib().smb_read_structure(data, len(data), FORMATS[fmt], C.byref(sel), _p(out, C.c_double), len(out),
+                                  C.byref(n), err, 1024)
+    if rc == native.SMB_ERR_MEMORY:
+        out = np.zeros((n.value, 4))
+        rc = lib().smb_read_structure(data, len(data), FORMATS[fmt], C.byref(sel), _p(out, C.c_double), len(out),
+                                      C.byref(n), err, 1024)
+    _check(rc, err)
+    return out[:n.value].copy()
 
 
 def read_path(path, model=None, hydrogens=False, waters=False, hetero=True):
