@@ -243,6 +243,21 @@ MODE_NAMES = {"exact": "exact f64 refinement", "fast": "fast mode, plain f32 ref
               "warm": "fast mode, f32 refinement from the learned warm start"}
 
 
+def rank_max(x, dist, device):
+    """x's maximum over the ranks of the process group (x itself alone)."""
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(grid_points, world, step_ms):
+    """Whole-job throughput of N replicas (each rank meshes its own copy of
+    the workload): all ranks' grid points over the slowest rank's step."""
+    return world * grid_points / (step_ms / 1e3) / 1e6
+
+
 def mode_params(w, mode, local):
     """SurfaceParams of a mode: exact, fast (plain f32) or warm (fast with
     the learned warm start)."""
@@ -291,7 +306,7 @@ def mode_leg(a, w, mode, local, dev, barrier, max_over_ranks, world, flush, coun
     clk = clocks.stop()
     launches = native.lib().smb_kernel_launches() - launches0
     mean_ms = max_over_ranks(float(np.mean(step_ms)))
-    value = world * grid_points / (mean_ms / 1e3) / 1e6
+    value = replica_value(grid_points, world, mean_ms)
     stage = {k: float(np.mean([p[k] for p in parts])) for k in ("classify", "substates", "gather", "sample", "mc")}
     # Vertex refinement on the device: f64 in exact mode; in fast mode the
     # warm starts, the f32 refinement and the placement.
@@ -363,7 +378,7 @@ def mode_leg(a, w, mode, local, dev, barrier, max_over_ranks, world, flush, coun
                   "pack_bytes_mean": float(info["pack_units"]) * 16 / max(1, info["sampled_subblocks"]),
                   "pack_bytes_max": int(info["max_pack_units"]) * 16, "edges": int(info["edges"]),
                   "triangles": int(info["triangles"])},
-        "e2e": {"value": world * grid_points / (e2e_mean / 1e3) / 1e6, "unit": "Mgridpts/s",
+        "e2e": {"value": replica_value(grid_points, world, e2e_mean), "unit": "Mgridpts/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(d2h), "ms_per_mesh": e2e_mean,
                 "host_threads": st.get("host_threads"),
                 "stages_ms": {k: st.get(k) for k in ("t_geometry", "t_upload", "t_device", "t_d2h", "t_host_refine",
@@ -397,10 +412,7 @@ def run_ours(a):
         torch.cuda.synchronize(dev)
 
     def max_over_ranks(x):
-        t = torch.tensor([float(x)], device=dev, dtype=torch.float64)
-        if dist is not None:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, dist, dev)
 
     w = workload(a.workload, None, a.spacing, a.spheres)
     mode = a.refine or ("warm" if a.workload == "rings58800" else w["refine"])
