@@ -235,7 +235,7 @@ __device__ __forceinline__ int sample_owner(int x, int y, int z, int sub, const 
 // independent of the brick's other sub-blocks (the +-band values of samples
 // no sampled sub-block owns are written by the marching-cubes count pass).
 template <bool MANY>
-__global__ void __launch_bounds__(256) k_substates(DArr A0, DLat L0, const int4* keys, uint32_t n_bricks, uint32_t* rec,
+__global__ void __launch_bounds__(256, 5) k_substates(DArr A0, DLat L0, const int4* keys, uint32_t n_bricks, uint32_t* rec,
                                                    uint32_t* sampled, Scene S) {
     const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
@@ -638,7 +638,7 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
 // Warp per work item, the grid striding over the items (many structures:
 // the item count is read on the device).
 template <bool MANY>
-__global__ void __launch_bounds__(256, MANY ? 2 : 3) k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
+__global__ void __launch_bounds__(256, MANY ? 2 : 4) k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
                          GatherCaps caps, Scene S) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t n = MANY ? uint32_t(*S.n_work) : n_work;
