@@ -1565,7 +1565,7 @@ __device__ __forceinline__ void refine_edge_f32(const RefStage& st, const Refine
 // The edge's features then go through the MLP (k_mlp_forward), whose output
 // picks each edge's start: t_c or the linear guess (or, with the root head,
 // is the start itself).  The refinement (k_refine<REFINE_WARM>) is the plain
-// one from those starts: a start the field judges within the tolerance is
+// one from those starts: a start at which the field is within the tolerance is
 // accepted after one evaluation, any other falls back to the bracketed
 // iteration.
 
@@ -1608,7 +1608,7 @@ __device__ __forceinline__ WarmCand warm_cand(const DArr& A, const DLat& L, cons
 
 // The candidate's part of eval_f32 at (x, y, z): probe less its distance
 // when that is below probe + band (found), else -band; q its closest point.
-// The inside test and the blockers are not applied: the field judges the
+// The inside test and the blockers are not applied: the field decides the
 // result.
 __device__ __forceinline__ float cand_eval(const WarmCand& w, float probe, float band, float x, float y, float z,
                                            float& qx, float& qy, float& qz, bool& found) {

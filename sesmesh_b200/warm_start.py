@@ -12,7 +12,7 @@ candidate and the MLP answers >= 0.5, and at the linear guess
 t_lin = fa / (fa - fb) elsewhere; with the root
 head (data/warm_root.f32, smb_mlp_set_use ROOT) it starts at the MLP's
 output itself.  The reference's bracketed Newton / Illinois / bisection
-iteration then runs unchanged (smb_refine_warm): a start the field judges
+iteration then runs unchanged (smb_refine_warm): a start at which the field is
 within the tolerance is accepted after one evaluation, any other falls back
 to the bracketed refinement.  The reference's fast mode
 (crates/sesmesh/src/field/gpu.rs:207-221 with the iteration of
