@@ -7,6 +7,7 @@
 // and f32 sample values follow the CPU back end of sesmesh 1.3.2
 // operation by operation, so every output is bit-identical to it.
 #include <atomic>
+#include <type_traits>
 #include <cstdio>
 
 #include "common.cuh"
@@ -15,7 +16,9 @@
 #include "kernels.hpp"
 #include "mlp.cuh"
 #include "scan.cuh"
-#define SMB_MC_QUAL __constant__
+// Global memory (read through the L1), not __constant__: threads of a warp
+// read different entries.
+#define SMB_MC_QUAL __device__
 #include "../mc_table.inc"
 
 namespace smb {
@@ -228,6 +231,30 @@ __device__ __forceinline__ int sample_owner(int x, int y, int z, int sub, const 
                 pos = st[sb] == ST_OUT;
             }
     *positive = pos;
+    return -1;
+}
+
+// The sub-blocks whose closed box holds lattice coordinate v on one axis, as
+// a two-bit mask (bit 0 the lower half, bit 1 the upper): the index ranges
+// sample_owner scans.
+__device__ __forceinline__ uint32_t axis_halves(int v, int sub) {
+    const int hi = min(v / sub, 1);
+    const int lo = (v > 0 && v % sub == 0) ? min(v / sub - 1, 1) : hi;
+    return (2u << hi) - (1u << lo);
+}
+
+// sample_owner on state masks (bit q of sampled / out: sub-block q is
+// ST_SAMPLE / ST_OUT): the containing sub-blocks in sample_owner's scan order
+// are the set bits of `held` in ascending order (sb = sx + 2 sy + 4 sz), so
+// the owner is the lowest held sampled sub-block, and without one the sign
+// is the state of the highest held sub-block, the last one the scan visits.
+__device__ __forceinline__ int owner_of_masks(uint32_t xm, uint32_t ym, uint32_t zm, uint32_t sampled, uint32_t out,
+                                              bool* positive) {
+    const uint32_t row = ((ym & 1u) ? xm : 0u) | ((ym & 2u) ? xm << 2 : 0u);
+    const uint32_t held = ((zm & 1u) ? row : 0u) | ((zm & 2u) ? row << 4 : 0u);
+    const uint32_t m = held & sampled;
+    if (m) return __ffs(int(m)) - 1;
+    *positive = (out >> (31 - __clz(int(held)))) & 1u;
     return -1;
 }
 
@@ -953,18 +980,24 @@ __global__ void __launch_bounds__(128) k_sample(DLat L0, const int4* keys, const
 // and triangle references (code << 28 | local edge id) in cell order, both
 // compacted with a block scan over contiguous cell ranges per thread.
 constexpr int MC_THREADS = 256;
-__constant__ uint8_t c_edge_lower[12] = {0, 2, 4, 6, 0, 1, 4, 5, 0, 1, 2, 3};
 
-template <bool FILL, bool MANY>
+// Lower corner of cube edge e (edges 0-3 along x, 4-7 along y, 8-11 along
+// z), corner bits x | y << 1 | z << 2, one nibble per edge:
+// {0, 2, 4, 6, 0, 1, 4, 5, 0, 1, 2, 3}.
+constexpr unsigned long long MC_EDGE_LOWER = 0x321054106420ull;
+
+// BC: the brick edge when it is known at compile time (constant divisors),
+// 0 to read it from the lattice; the outputs do not depend on it.
+template <bool FILL, bool MANY, int BC>
 __global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L0, uint32_t n_bricks, float* values, const uint32_t* rec, uint32_t* counts,
                                                    const uint32_t* edge_off, const uint32_t* tri_off, uint32_t* edges,
                                                    float2* edge_vals, uint32_t* tris, const int4* keys,
                                                    unsigned long long edge_cap, unsigned long long tri_cap, Scene S) {
     extern __shared__ float v[];
     __shared__ uint16_t t_off[257];
-    __shared__ uint8_t t_edges[SMB_MC_TRIANGLES * 3];
+    __shared__ uint8_t t_edges[FILL ? SMB_MC_TRIANGLES * 3 : 1];
     __shared__ unsigned long long sh[MC_THREADS / 32];
-    __shared__ uint32_t sts[8];
+    __shared__ uint32_t masks[2];
     const uint32_t brick = blockIdx.x;
     if (brick >= n_bricks) return;
     const DLat& L = MANY ? S.lat[keys[brick].w] : L0;
@@ -972,21 +1005,28 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L0, uint32_t n_bricks, f
         if (MANY && threadIdx.x == 0) S.fail[keys[brick].w] = 1;
         return;
     }
-    const int b = L.b, s = b + 1;
-    float* src = values + size_t(brick) * L.spb;
+    const int b = BC ? BC : L.b, s = b + 1, spb = s * s * s;
+    float* src = values + size_t(brick) * spb;
     if (!FILL) {
         // Samples that no sampled sub-block owns get +-band here (Engine::
         // assign, field/kernel.rs:489-546): the sign of the last containing
         // uniform sub-block.
-        if (threadIdx.x < 8) sts[threadIdx.x] = rec[(size_t(brick) * 8 + threadIdx.x) * REC_WORDS + R_STATE];
+        const int sub = BC ? BC / 2 : L.sub;
+        if (threadIdx.x < 32) {
+            const uint32_t q = threadIdx.x & 7;
+            const uint32_t st = rec[(size_t(brick) * 8 + q) * REC_WORDS + R_STATE];
+            const uint32_t ms = __ballot_sync(0xffffffffu, threadIdx.x < 8 && st == ST_SAMPLE);
+            const uint32_t mo = __ballot_sync(0xffffffffu, threadIdx.x < 8 && st == ST_OUT);
+            if (threadIdx.x == 0) masks[0] = ms, masks[1] = mo;
+        }
         __syncthreads();
-        uint32_t st[8];
-        for (int q = 0; q < 8; q++) st[q] = sts[q];
-        for (int i = threadIdx.x; i < L.spb; i += blockDim.x) {
-            int x = i % s, y = (i / s) % s, z = i / (s * s);
+        const uint32_t ms = masks[0], mo = masks[1];
+        const float band = L.band32;
+        for (int i = threadIdx.x; i < spb; i += blockDim.x) {
+            const int x = i % s, y = (i / s) % s, z = i / (s * s);
             bool positive;
-            if (sample_owner(x, y, z, L.sub, st, &positive) < 0) {
-                float bv = positive ? L.band32 : -L.band32;
+            if (owner_of_masks(axis_halves(x, sub), axis_halves(y, sub), axis_halves(z, sub), ms, mo, &positive) < 0) {
+                const float bv = positive ? band : -band;
                 src[i] = bv;
                 v[i] = bv;
             } else {
@@ -994,24 +1034,31 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L0, uint32_t n_bricks, f
             }
         }
     } else {
-        for (int i = threadIdx.x; i < L.spb; i += blockDim.x) v[i] = src[i];
+        for (int i = threadIdx.x; i < spb; i += blockDim.x) v[i] = src[i];
+        const uint8_t* te = &SMB_TRI_EDGES[0][0];
+        for (int i = threadIdx.x; i < SMB_MC_TRIANGLES * 3; i += blockDim.x) t_edges[i] = te[i];
     }
     for (int i = threadIdx.x; i < 257; i += blockDim.x) t_off[i] = SMB_TRI_OFFSET[i];
-    for (int i = threadIdx.x; i < SMB_MC_TRIANGLES * 3; i += blockDim.x) t_edges[i] = SMB_TRI_EDGES[i / 3][i % 3];
     __syncthreads();
     const int cells = b * b * b;
     const int per = (cells + MC_THREADS - 1) / MC_THREADS;
     const int c0 = min(int(threadIdx.x) * per, cells), c1 = min(c0 + per, cells);
-    const int st[3] = {1, s, s * s};
-    const int corner[8] = {0, 1, s, s + 1, s * s, s * s + 1, s * s + s, s * s + s + 1};
+    const int ss = s * s;
     unsigned ne = 0, nt = 0;
     for (int c = c0; c < c1; c++) {
-        int x = c % b, y = (c / b) % b, z = c / (b * b);
-        int i = (z * s + y) * s + x;
-        bool a = v[i] < 0.0f;
-        for (int ax = 0; ax < 3; ax++) ne += (a != (v[i + st[ax]] < 0.0f));
+        const int x = c % b, y = (c / b) % b, z = c / (b * b);
+        const int i = (z * s + y) * s + x;
+        const bool a = v[i] < 0.0f;
+        ne += (a != (v[i + 1] < 0.0f)) + (a != (v[i + s] < 0.0f)) + (a != (v[i + ss] < 0.0f));
         int cs = 0;
-        for (int q = 0; q < 8; q++) cs |= (v[i + corner[q]] < 0.0f) << q;
+        cs |= int(a);
+        cs |= int(v[i + 1] < 0.0f) << 1;
+        cs |= int(v[i + s] < 0.0f) << 2;
+        cs |= int(v[i + s + 1] < 0.0f) << 3;
+        cs |= int(v[i + ss] < 0.0f) << 4;
+        cs |= int(v[i + ss + 1] < 0.0f) << 5;
+        cs |= int(v[i + ss + s] < 0.0f) << 6;
+        cs |= int(v[i + ss + s + 1] < 0.0f) << 7;
         nt += t_off[cs + 1] - t_off[cs];
     }
     unsigned long long te, tt;
@@ -1023,31 +1070,36 @@ __global__ void __launch_bounds__(MC_THREADS) k_mc(DLat L0, uint32_t n_bricks, f
     }
     uint32_t eo = edge_off[brick] + uint32_t(pe), to = tri_off[brick] + uint32_t(pt);
     for (int c = c0; c < c1; c++) {
-        int x = c % b, y = (c / b) % b, z = c / (b * b);
-        int i = (z * s + y) * s + x;
-        float va = v[i];
+        const int x = c % b, y = (c / b) % b, z = c / (b * b);
+        const int i = (z * s + y) * s + x;
+        const float va = v[i];
+        const float vn[3] = {v[i + 1], v[i + s], v[i + ss]};
         for (int ax = 0; ax < 3; ax++) {
-            float vb = v[i + st[ax]];
-            if ((va < 0.0f) != (vb < 0.0f)) {
+            if ((va < 0.0f) != (vn[ax] < 0.0f)) {
                 edges[eo] = uint32_t(c * 3 + ax);
-                edge_vals[eo] = make_float2(va, vb);
+                edge_vals[eo] = make_float2(va, vn[ax]);
                 eo++;
             }
         }
         int cs = 0;
-        for (int q = 0; q < 8; q++) cs |= (v[i + corner[q]] < 0.0f) << q;
+        cs |= int(va < 0.0f);
+        cs |= int(vn[0] < 0.0f) << 1;
+        cs |= int(vn[1] < 0.0f) << 2;
+        cs |= int(v[i + s + 1] < 0.0f) << 3;
+        cs |= int(vn[2] < 0.0f) << 4;
+        cs |= int(v[i + ss + 1] < 0.0f) << 5;
+        cs |= int(v[i + ss + s] < 0.0f) << 6;
+        cs |= int(v[i + ss + s + 1] < 0.0f) << 7;
         for (int t = t_off[cs]; t < t_off[cs + 1]; t++) {
             for (int k = 0; k < 3; k++) {
-                int e = t_edges[3 * t + k];
-                int axis = e >> 2, lo = c_edge_lower[e];
-                int l[3] = {x + (lo & 1), y + ((lo >> 1) & 1), z + ((lo >> 2) & 1)};
-                uint32_t code = 0;
-                int lc[3] = {0, 0, 0};
-                for (int a2 = 0; a2 < 3; a2++) {
-                    if (l[a2] == b) code |= 1u << a2;
-                    else lc[a2] = l[a2];
-                }
-                tris[3 * size_t(to) + k] = (code << 28) | uint32_t(((lc[2] * b + lc[1]) * b + lc[0]) * 3 + axis);
+                const int e = t_edges[3 * t + k];
+                const int axis = e >> 2, lo = int((MC_EDGE_LOWER >> (4 * e)) & 0xFu);
+                const int lx = x + (lo & 1), ly = y + ((lo >> 1) & 1), lz = z + (lo >> 2);
+                // A vertex on the brick's upper face belongs to the next
+                // brick: its code bit is set and its coordinate is 0 there.
+                const uint32_t code = uint32_t(lx == b) | uint32_t(ly == b) << 1 | uint32_t(lz == b) << 2;
+                const int cx = lx == b ? 0 : lx, cy = ly == b ? 0 : ly, cz = lz == b ? 0 : lz;
+                tris[3 * size_t(to) + k] = (code << 28) | uint32_t(((cz * b + cy) * b + cx) * 3 + axis);
             }
             to++;
         }
@@ -2164,7 +2216,17 @@ cudaError_t launch_mc(const DLat& L, uint32_t n, float* values, const uint32_t* 
                       const Scene* many) {
     if (!n) return cudaSuccess;
     size_t smem = size_t(L.spb) * 4;
-    auto kern = many ? (fill ? k_mc<true, true> : k_mc<false, true>) : (fill ? k_mc<true, false> : k_mc<false, false>);
+    // Brick edges 10 (the default) and 8 and 16 (those the many-structure
+    // tuning tries) with constant divisors.
+    auto pick = [&](auto bc) {
+        constexpr int BC = decltype(bc)::value;
+        return many ? (fill ? k_mc<true, true, BC> : k_mc<false, true, BC>)
+                    : (fill ? k_mc<true, false, BC> : k_mc<false, false, BC>);
+    };
+    auto kern = L.b == 10  ? pick(std::integral_constant<int, 10>{})
+                : L.b == 8  ? pick(std::integral_constant<int, 8>{})
+                : L.b == 16 ? pick(std::integral_constant<int, 16>{})
+                            : pick(std::integral_constant<int, 0>{});
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     COUNT(1);
