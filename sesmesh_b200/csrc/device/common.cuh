@@ -180,6 +180,25 @@ __device__ __forceinline__ void warp_for_near(const DGrid& g, double x, double y
     });
 }
 
+// No sphere of items[p .. e) blocks q (each centre at least R - GEOM_EPS
+// from q), in list order, stopping at the first that does; two spheres'
+// loads in flight at a time (the tests have no side effects, so reading one
+// past the first blocker changes nothing).
+__device__ __forceinline__ bool unblocked(const DArr& A, const uint32_t* items, uint32_t p, uint32_t e, double qx,
+                                          double qy, double qz) {
+    for (; p + 2 <= e; p += 2) {
+        const uint32_t i0 = items[p], i1 = items[p + 1];
+        const double4 k0 = A.sph[i0], k1 = A.sph[i1];
+        if (!sqrt_ge(sq3(qx, qy, qz, k0.x, k0.y, k0.z), k0.w - GEOM_EPS)) return false;
+        if (!sqrt_ge(sq3(qx, qy, qz, k1.x, k1.y, k1.z), k1.w - GEOM_EPS)) return false;
+    }
+    if (p < e) {
+        const double4 k = A.sph[items[p]];
+        if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - GEOM_EPS)) return false;
+    }
+    return true;
+}
+
 // SesField::try_sphere_with (field/point.rs:422-444): the candidate's
 // distance if its radial projection is unblocked and below best, else best.
 // Threshold tests on distances go through sqrt_ge / sqrt_lt (the root only
@@ -193,11 +212,7 @@ __device__ __forceinline__ double try_sphere(const DArr& A, double x, double y, 
     if (lb >= best || len < 1e-12) return best;
     double s = c.w / len;
     double qx = c.x + vx * s, qy = c.y + vy * s, qz = c.z + vz * s;
-    for (uint32_t p = A.nb_off[i], e = A.nb_off[i + 1]; p < e; p++) {
-        double4 k = A.sph[A.nb_items[p]];
-        if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - GEOM_EPS)) return best;
-    }
-    return lb;
+    return unblocked(A, A.nb_items, A.nb_off[i], A.nb_off[i + 1], qx, qy, qz) ? lb : best;
 }
 
 // SesField::try_circle_with (field/point.rs:452-476).
@@ -219,11 +234,7 @@ __device__ __forceinline__ double try_circle(const DArr& A, double x, double y, 
         dx = c[6], dy = c[7], dz = c[8];
     }
     double qx = c[0] + dx * c[9], qy = c[1] + dy * c[9], qz = c[2] + dz * c[9];
-    for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++) {
-        double4 k = A.sph[A.cb_items[p]];
-        if (!sqrt_ge(sq3(qx, qy, qz, k.x, k.y, k.z), k.w - GEOM_EPS)) return best;
-    }
-    return dist;
+    return unblocked(A, A.cb_items, A.cb_off[ci], A.cb_off[ci + 1], qx, qy, qz) ? dist : best;
 }
 
 // Distance from (x, y, z) to the circle ci as gather_ses / gather_local
