@@ -318,6 +318,57 @@ __device__ __forceinline__ int lookup_near(const uint16_t* tab, uint32_t bits, c
     }
 }
 
+// One candidate's blocker row: the near-list members among items[p .. e)
+// (lookup_near on each), counted, and with w their near-list positions
+// written in order to w[0 ..] and pk[0 ..].  Four ids at a time: their
+// loads and first probes are issued together, so a lane has four lookups in
+// flight instead of one dependent chain per id; a probe that meets another
+// sphere goes on probing.  Not inlined: the four rows of a sub-block (S and
+// C, counted and written) share one copy, which keeps the gather within the
+// instruction cache.
+__device__ __noinline__ uint32_t near_members(const uint16_t* tab, uint32_t bits, const uint32_t* near_ids,
+                                              const uint32_t* items, uint32_t p, uint32_t e, uint32_t* w,
+                                              uint32_t* pk) {
+    const uint32_t mask = (1u << bits) - 1;
+    uint32_t n = 0;
+    auto take = [&](uint32_t l) {
+        if (w) w[n] = l, pk[n] = l;
+        n++;
+    };
+    constexpr int W = 4;
+    for (; p + W <= e; p += W) {
+        uint32_t id[W], h[W], slot[W], at[W];
+#pragma unroll
+        for (int u = 0; u < W; u++) id[u] = items[p + u];
+#pragma unroll
+        for (int u = 0; u < W; u++) h[u] = near_hash(id[u], bits), slot[u] = tab[h[u]];
+        // An empty slot reads near_ids[0] (in the scratch, unused).
+#pragma unroll
+        for (int u = 0; u < W; u++) at[u] = near_ids[slot[u] == 0xFFFFu ? 0u : slot[u]];
+#pragma unroll
+        for (int u = 0; u < W; u++) {
+            if (slot[u] == 0xFFFFu) continue;
+            if (at[u] == id[u]) {
+                take(slot[u]);
+                continue;
+            }
+            for (uint32_t q = (h[u] + 1) & mask;; q = (q + 1) & mask) {
+                const uint32_t l = tab[q];
+                if (l == 0xFFFFu) break;
+                if (near_ids[l] == id[u]) {
+                    take(l);
+                    break;
+                }
+            }
+        }
+    }
+    for (; p < e; p++) {
+        const int l = lookup_near(tab, bits, near_ids, items[p]);
+        if (l >= 0) take(uint32_t(l));
+    }
+    return n;
+}
+
 __device__ __forceinline__ unsigned warp_inclusive_scan(unsigned v) {
     int lane = threadIdx.x & 31;
     for (int o = 1; o < 32; o <<= 1) {
@@ -329,7 +380,11 @@ __device__ __forceinline__ unsigned warp_inclusive_scan(unsigned v) {
 
 
 // One warp: the lists of work item `item` (a sampled sub-block).
-template <bool MANY>
+// WIDE: blocker rows through near_members (four lookups in flight), which
+// pays where a sub-block's lists fill several rounds of the warp's lanes
+// (rings58800, 30 near spheres: 12.1 -> 13.2 ms; shell2400k at 1 A, 141:
+// 291 -> 256 ms); otherwise a lane walks its row one lookup at a time.
+template <bool MANY, bool WIDE>
 __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const DLat& L0, const int4* keys,
                                             const uint32_t* work, const GatherOut& O, const GatherCaps& caps,
                                             const Scene& S, unsigned char* smem_raw) {
@@ -527,8 +582,12 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         unsigned cnt = 0;
         if (r < ns) {
             uint32_t k = s_id[s_perm[r]];
-            for (uint32_t p = A.nb_off[k], e = A.nb_off[k + 1]; p < e; p++)
-                cnt += lookup_near(near_tab, tab_bits, near_ids, A.nb_items[p]) >= 0;
+            if constexpr (WIDE)
+                cnt = near_members(near_tab, tab_bits, near_ids, A.nb_items, A.nb_off[k], A.nb_off[k + 1], nullptr,
+                                   nullptr);
+            else
+                for (uint32_t p = A.nb_off[k], e = A.nb_off[k + 1]; p < e; p++)
+                    cnt += lookup_near(near_tab, tab_bits, near_ids, A.nb_items[p]) >= 0;
         }
         unsigned inc = warp_inclusive_scan(cnt);
         if (r < ns) s_off[r + 1] = run + inc;
@@ -542,8 +601,12 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         unsigned cnt = 0;
         if (r < nc) {
             uint32_t ci = c_id[c_perm[r]];
-            for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++)
-                cnt += lookup_near(near_tab, tab_bits, near_ids, A.cb_items[p]) >= 0;
+            if constexpr (WIDE)
+                cnt = near_members(near_tab, tab_bits, near_ids, A.cb_items, A.cb_off[ci], A.cb_off[ci + 1], nullptr,
+                                   nullptr);
+            else
+                for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++)
+                    cnt += lookup_near(near_tab, tab_bits, near_ids, A.cb_items[p]) >= 0;
         }
         unsigned inc = warp_inclusive_scan(cnt);
         if (r < nc) c_off[r + 1] = run + inc;
@@ -621,9 +684,14 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         double4 c = A.sph[k];
         p_s[r] = make_float4(float(c.x - L.fx), float(c.y - L.fy), float(c.z - L.fz), float(c.w));
         uint32_t o = s_off[r];
-        for (uint32_t p = A.nb_off[k], e = A.nb_off[k + 1]; p < e; p++) {
-            int l = lookup_near(near_tab, tab_bits, near_ids, A.nb_items[p]);
-            if (l >= 0) w_sblk[o] = uint32_t(l), p_sblk[o] = uint32_t(l), o++;
+        if constexpr (WIDE) {
+            near_members(near_tab, tab_bits, near_ids, A.nb_items, A.nb_off[k], A.nb_off[k + 1], w_sblk + o,
+                         p_sblk + o);
+        } else {
+            for (uint32_t p = A.nb_off[k], e = A.nb_off[k + 1]; p < e; p++) {
+                int l = lookup_near(near_tab, tab_bits, near_ids, A.nb_items[p]);
+                if (l >= 0) w_sblk[o] = uint32_t(l), p_sblk[o] = uint32_t(l), o++;
+            }
         }
     }
     for (int r = lane; r <= nc; r += 32) w_coff[r] = c_off[r], p_coff[r] = c_off[r];
@@ -635,9 +703,14 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
         p_c[3 * r + 1] = make_float4(float(c[3]), float(c[4]), float(c[5]), float(c[6]));
         p_c[3 * r + 2] = make_float4(float(c[7]), float(c[8]), 0.0f, 0.0f);
         uint32_t o = c_off[r];
-        for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++) {
-            int l = lookup_near(near_tab, tab_bits, near_ids, A.cb_items[p]);
-            if (l >= 0) w_cblk[o] = uint32_t(l), p_cblk[o] = uint32_t(l), o++;
+        if constexpr (WIDE) {
+            near_members(near_tab, tab_bits, near_ids, A.cb_items, A.cb_off[ci], A.cb_off[ci + 1], w_cblk + o,
+                         p_cblk + o);
+        } else {
+            for (uint32_t p = A.cb_off[ci], e = A.cb_off[ci + 1]; p < e; p++) {
+                int l = lookup_near(near_tab, tab_bits, near_ids, A.cb_items[p]);
+                if (l >= 0) w_cblk[o] = uint32_t(l), p_cblk[o] = uint32_t(l), o++;
+            }
         }
     }
     for (int i = lane; i < nv; i += 32) {
@@ -664,14 +737,14 @@ __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const
 
 // Warp per work item, the grid striding over the items (many structures:
 // the item count is read on the device).
-template <bool MANY>
+template <bool MANY, bool WIDE>
 __global__ void __launch_bounds__(256, MANY ? 2 : 4) k_gather(DArr A0, DLat L0, const int4* keys, const uint32_t* work, uint32_t n_work, GatherOut O,
                          GatherCaps caps, Scene S) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t n = MANY ? uint32_t(*S.n_work) : n_work;
     const uint32_t wpb = blockDim.x >> 5;
     for (uint32_t item = blockIdx.x * wpb + (threadIdx.x >> 5); item < n; item += gridDim.x * wpb)
-        gather_item<MANY>(item, A0, L0, keys, work, O, caps, S, smem_raw);
+        gather_item<MANY, WIDE>(item, A0, L0, keys, work, O, caps, S, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -2165,7 +2238,9 @@ cudaError_t launch_gather(const DArr& A, const DLat& L, const int4* keys, const 
                           const GatherOut& O, const GatherCaps& caps, int warps, cudaStream_t s, const Scene* many) {
     if (!n) return cudaSuccess;
     size_t smem = gather_smem_bytes(caps) * size_t(warps);
-    auto kern = many ? k_gather<true> : k_gather<false>;
+    // Lists of several warp rounds (the caps come from the largest lists
+    // seen): blocker rows with four lookups in flight.
+    auto kern = many ? k_gather<true, false> : caps.near >= 128 ? k_gather<false, true> : k_gather<false, false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     if (e != cudaSuccess) return e;
     COUNT(1);
