@@ -816,7 +816,7 @@ def run_batch(a):
 # rings58800_h025.md: both passes of k_refine_exact; profiles/
 # refine_f32_warm_rings58800_h025.md: k_refine from the warm starts).
 TRAFFIC = {("rings58800", 0.25, "k_refine_exact"): 1152510464 + 277156352 + 216691712 + 104072448,
-           ("rings58800", 0.25, "k_refine_warm"): 1361073920 + 193664000}
+           ("rings58800", 0.25, "k_refine_warm"): 1360927744 + 193899264}
 
 
 def roofline(dominant, stage, info, ops, owned, w, pk, pk_kind, n_bricks, xops=0, mode="exact"):

@@ -2037,12 +2037,16 @@ constexpr int REFINE_WARPS = 4;
 #define WIDE_LIST_WARPS 16
 #endif
 
+// Largest staging region for the two-warp blocks of the single-structure
+// refinement (ten or more blocks to an SM).
+constexpr size_t PAIR_REGION_MAX = 20480;
+
 struct RefinePlan {
     uint32_t cand_bytes;  // one staging region
 };
 
 template <int MODE, bool WIDE, bool MANY, int RG, int NT = 32 * REFINE_WARPS, bool COUNT = false>
-__global__ void __launch_bounds__(NT, NT > 32 * REFINE_WARPS ? 2 : 1) k_refine(
+__global__ void __launch_bounds__(NT, NT == 64 ? 8 : (NT > 32 * REFINE_WARPS ? 2 : 1)) k_refine(
     DArr A0, DLat L0, RefineConsts RC0, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
     const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
     uint32_t n_host, RefOut out, const float2* start, RefinePlan P, unsigned long long* counters, Scene S,
@@ -2396,6 +2400,17 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
                          : pick(k_refine<REFINE_PLAIN, false, false, 8, NW, true>,
                                 k_refine<REFINE_PLAIN, true, false, 8, NW, true>);
         return run(kern, P, smem, nullptr, nullptr, use_wide ? n_items : quads);
+    }
+    // Lists of up to PAIR_REGION_MAX bytes (single structure, groups of 8,
+    // no region asked for): blocks of two warps that share one staging
+    // region per sub-block.  A region then costs a warp half of what a region
+    // of its own does, so the registers, not the shared memory, set the warps
+    // per SM (22 instead of 12 on rings58800's 16 KiB lists) and more warps
+    // hide the evaluations' dependent latency; the edges and their outputs
+    // are the same.
+    if (!many && !g32 && region == 0 && P.cand_bytes <= PAIR_REGION_MAX) {
+        auto kp = warm ? k_refine<REFINE_WARM, true, false, 8, 64> : k_refine<REFINE_PLAIN, true, false, 8, 64>;
+        return run(kp, P, wide, nullptr, nullptr, n_items, 64);
     }
     if (split) {
         RefinePlan PS = P;
