@@ -2038,7 +2038,8 @@ constexpr int REFINE_WARPS = 4;
 #endif
 
 // Largest staging region for the two-warp blocks of the single-structure
-// refinement (ten or more blocks to an SM).
+// refinement (ten or more blocks to an SM; at most 80 registers, so twelve
+// blocks where the regions allow).
 constexpr size_t PAIR_REGION_MAX = 20480;
 
 struct RefinePlan {
@@ -2046,7 +2047,7 @@ struct RefinePlan {
 };
 
 template <int MODE, bool WIDE, bool MANY, int RG, int NT = 32 * REFINE_WARPS, bool COUNT = false>
-__global__ void __launch_bounds__(NT, NT == 64 ? 8 : (NT > 32 * REFINE_WARPS ? 2 : 1)) k_refine(
+__global__ void __launch_bounds__(NT, NT == 64 ? 12 : (NT > 32 * REFINE_WARPS ? 2 : 1)) k_refine(
     DArr A0, DLat L0, RefineConsts RC0, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
     const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
     uint32_t n_host, RefOut out, const float2* start, RefinePlan P, unsigned long long* counters, Scene S,
