@@ -1860,12 +1860,19 @@ __device__ __forceinline__ float2 warm_row(const DArr& A0, const DLat& L0, const
                                            const uint32_t* work, uint32_t n_items, const uint32_t* rec,
                                            const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off,
                                            const uint32_t* item_edges, const float* values, const uint32_t* feats,
-                                           const Scene& S, uint32_t e, float* f, uint32_t* cand) {
-    uint32_t lo = 0, hi = n_items;  // the item holding row e: item_off[lo] <= e < item_off[lo + 1]
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (item_off[mid] <= e) lo = mid;
-        else hi = mid;
+                                           const Scene& S, uint32_t e, float* f, uint32_t* cand,
+                                           uint32_t item = 0xFFFFFFFFu) {
+    // The item holding row e: the last lo with item_off[lo] <= e (items
+    // without rows repeat an offset); `item` when the caller found it.
+    uint32_t lo = item;
+    if (lo == 0xFFFFFFFFu) {
+        lo = 0;
+        uint32_t hi = n_items;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (item_off[mid] <= e) lo = mid;
+            else hi = mid;
+        }
     }
     const uint32_t brick = work[lo] >> 3;
     const int4 key = keys[brick];
@@ -1952,6 +1959,32 @@ __device__ __forceinline__ float2 warm_row(const DArr& A0, const DLat& L0, const
     return make_float2(t_c, t_lin);
 }
 
+// The item holding row e (the last lo with item_off[lo] <= e), found by a
+// warp for its 32 consecutive rows e0 .. e0 + 31 (e0 < E = item_off[n]):
+// each step probes 32 points that split (lo, hi) 33 ways, keeping
+// item_off[lo] <= e0 < item_off[hi], so a few steps replace the 19 of a
+// lane's own binary search over 384 K items; each lane then walks from the
+// warp's item to its own row's.  All 32 lanes take part.
+__device__ __forceinline__ uint32_t warp_item_of(const uint32_t* item_off, uint32_t n_items, uint32_t e0, uint32_t e,
+                                                 uint32_t E) {
+    const int lane = int(threadIdx.x & 31);
+    uint32_t lo = 0, hi = n_items;
+    while (hi - lo > 1) {
+        const uint32_t span = hi - lo;
+        const uint32_t p = span <= 32 ? lo + 1 + uint32_t(lane)
+                                      : lo + uint32_t((unsigned long long)span * uint32_t(lane + 1) / 33ull);
+        const bool valid = p > lo && p < hi;
+        const bool le = valid && item_off[p] <= e0;
+        const uint32_t m_le = __ballot_sync(0xffffffffu, le), m_gt = __ballot_sync(0xffffffffu, valid && !le);
+        const uint32_t nlo = m_le ? __shfl_sync(0xffffffffu, p, 31 - __clz(int(m_le))) : lo;
+        const uint32_t nhi = m_gt ? __shfl_sync(0xffffffffu, p, __ffs(int(m_gt)) - 1) : hi;
+        lo = nlo, hi = nhi;
+    }
+    if (e < E)
+        while (item_off[lo + 1] <= e) lo++;
+    return lo;
+}
+
 // Features of every row (export for training: smb_batch_edge_features).
 template <bool MANY>
 __global__ void __launch_bounds__(256) k_warm_features(DArr A0, DLat L0, RefineConsts RC0, const int4* keys,
@@ -1999,12 +2032,14 @@ __global__ void __launch_bounds__(128) k_warm_starts(DArr A0, DLat L0, RefineCon
     uint32_t phase = 0;
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint32_t e = tile * MLP_ROWS + threadIdx.x;
+        const uint32_t e0 = e & ~31u;  // the warp's first row (warp-uniform)
+        const uint32_t item = e0 < E ? warp_item_of(item_off, n_items, e0, e, E) : 0u;
         float f[MLP_IN];
         float2 sc = make_float2(-1.0f, 0.0f);
         uint32_t cand = 0;
         if (e < E) {
             sc = warm_row<MANY>(A0, L0, RC0, keys, work, n_items, rec, edges, edge_vals, item_off, item_edges, values,
-                                feats, S, e, f, &cand);
+                                feats, S, e, f, &cand, item);
         } else {
             for (int c = 0; c < MLP_IN; c++) f[c] = 0.0f;
         }
