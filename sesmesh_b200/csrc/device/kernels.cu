@@ -2115,13 +2115,14 @@ __global__ void __launch_bounds__(NT, NT == 64 ? 12 : (NT > 32 * REFINE_WARPS ? 
         const float probe = L.probe32, band = L.band32;
         const BrickFrame F = brick_frame(L, RC, key);
         const uint32_t* R = rec + size_t(j) * REC_WORDS;
-        if (!WIDE && ovf) {
-            // A sub-block whose candidates outgrow this warp's region goes
-            // to the list the whole-block pass takes after this one.
+        if (ovf) {
+            // A sub-block whose candidates outgrow this warp's (block's)
+            // region goes to the list the whole-block pass takes after this
+            // one.
             const size_t nn = R[R_NEAR], ns = R[R_S], nc = R[R_C], nv = R[R_V];
             const size_t need = (2 * nn + ns + 3 * nc + nv) * 16 + (2 * ns + 1 + R[R_SBLK] + nc + 1 + R[R_CBLK]) * 4;
             if (need > P.cand_bytes) {
-                if (lane == 0) ovf[1 + atomicAdd(ovf, 1u)] = i;
+                if (WIDE ? threadIdx.x == 0 : lane == 0) ovf[1 + atomicAdd(ovf, 1u)] = i;
                 return;
             }
         }
@@ -2398,9 +2399,11 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
     const size_t wide = P.cand_bytes;
     // One staging region per warp (an item per warp in flight, as many items
     // per SM as regions fit) while four fit in a block, else one per block.
-    // The single-structure pass instead keeps per-warp regions of the size
-    // asked for (default: two blocks of four to an SM) and hands the
-    // sub-blocks that outgrow them to a whole-block pass over a list.
+    // The single-structure pass instead gives blocks of two warps one region
+    // each: of the largest sub-block's size where that is at most
+    // PAIR_REGION_MAX, else of the size asked for (default: an eighth of the
+    // SM's shared memory), handing the sub-blocks that outgrow it to a
+    // whole-block pass over a list.
     const bool use_wide = narrow > smem_limit;
     size_t small = region ? region / 128 * 128 : (smem_limit / 2 - 1024) / REFINE_WARPS / 128 * 128;
     small = std::max<size_t>(std::min(small, size_t(P.cand_bytes)), 128);
@@ -2453,14 +2456,16 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
         PS.cand_bytes = uint32_t(small);
         cudaError_t e = cudaMemsetAsync(ovf, 0, 4, s);
         if (e != cudaSuccess) return e;
-        auto kn = warm ? (g32 ? k_refine<REFINE_WARM, false, false, 32> : k_refine<REFINE_WARM, false, false, 8>)
-                       : (g32 ? k_refine<REFINE_PLAIN, false, false, 32> : k_refine<REFINE_PLAIN, false, false, 8>);
         // The list pass: WIDE_LIST_WARPS warps share each sub-block's lists.
         auto kw = warm ? (g32 ? k_refine<REFINE_WARM, true, false, 32, 32 * WIDE_LIST_WARPS>
                               : k_refine<REFINE_WARM, true, false, 8, 32 * WIDE_LIST_WARPS>)
                        : (g32 ? k_refine<REFINE_PLAIN, true, false, 32, 32 * WIDE_LIST_WARPS>
                               : k_refine<REFINE_PLAIN, true, false, 8, 32 * WIDE_LIST_WARPS>);
-        e = run(kn, PS, size_t(REFINE_WARPS) * small, ovf, nullptr, quads);
+        // Two-warp blocks sharing a region of the same size over the
+        // sub-blocks that fit it (twice the warps per SM of per-warp regions).
+        auto kp = warm ? (g32 ? k_refine<REFINE_WARM, true, false, 32, 64> : k_refine<REFINE_WARM, true, false, 8, 64>)
+                       : (g32 ? k_refine<REFINE_PLAIN, true, false, 32, 64> : k_refine<REFINE_PLAIN, true, false, 8, 64>);
+        e = run(kp, PS, small, ovf, nullptr, n_items, 64);
         if (e != cudaSuccess) return e;
         return run(kw, P, wide, nullptr, ovf, n_items, 32 * WIDE_LIST_WARPS);
     }
