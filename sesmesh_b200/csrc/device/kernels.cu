@@ -2081,7 +2081,9 @@ struct RefinePlan {
     uint32_t cand_bytes;  // one staging region
 };
 
-template <int MODE, bool WIDE, bool MANY, int RG, int NT = 32 * REFINE_WARPS, bool COUNT = false>
+// OVF: a block-wide pass (WIDE) that lists the sub-blocks over its region
+// (the split pass); per-warp passes always can.
+template <int MODE, bool WIDE, bool MANY, int RG, int NT = 32 * REFINE_WARPS, bool COUNT = false, bool OVF = false>
 __global__ void __launch_bounds__(NT, NT == 64 ? 12 : (NT > 32 * REFINE_WARPS ? 2 : 1)) k_refine(
     DArr A0, DLat L0, RefineConsts RC0, const int4* keys, const uint32_t* work, const uint32_t* rec, const uint32_t* ids,
     const uint32_t* edges, const float2* edge_vals, const uint32_t* item_off, const uint32_t* item_edges,
@@ -2115,7 +2117,7 @@ __global__ void __launch_bounds__(NT, NT == 64 ? 12 : (NT > 32 * REFINE_WARPS ? 
         const float probe = L.probe32, band = L.band32;
         const BrickFrame F = brick_frame(L, RC, key);
         const uint32_t* R = rec + size_t(j) * REC_WORDS;
-        if (ovf) {
+        if ((!WIDE || OVF) && ovf) {
             // A sub-block whose candidates outgrow this warp's (block's)
             // region goes to the list the whole-block pass takes after this
             // one.
@@ -2463,8 +2465,10 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
                               : k_refine<REFINE_PLAIN, true, false, 8, 32 * WIDE_LIST_WARPS>);
         // Two-warp blocks sharing a region of the same size over the
         // sub-blocks that fit it (twice the warps per SM of per-warp regions).
-        auto kp = warm ? (g32 ? k_refine<REFINE_WARM, true, false, 32, 64> : k_refine<REFINE_WARM, true, false, 8, 64>)
-                       : (g32 ? k_refine<REFINE_PLAIN, true, false, 32, 64> : k_refine<REFINE_PLAIN, true, false, 8, 64>);
+        auto kp = warm ? (g32 ? k_refine<REFINE_WARM, true, false, 32, 64, false, true>
+                              : k_refine<REFINE_WARM, true, false, 8, 64, false, true>)
+                       : (g32 ? k_refine<REFINE_PLAIN, true, false, 32, 64, false, true>
+                              : k_refine<REFINE_PLAIN, true, false, 8, 64, false, true>);
         e = run(kp, PS, small, ovf, nullptr, n_items, 64);
         if (e != cudaSuccess) return e;
         return run(kw, P, wide, nullptr, ovf, n_items, 32 * WIDE_LIST_WARPS);
