@@ -382,8 +382,9 @@ __device__ __forceinline__ unsigned warp_inclusive_scan(unsigned v) {
 // One warp: the lists of work item `item` (a sampled sub-block).
 // WIDE: blocker rows through near_members (four lookups in flight), which
 // pays where a sub-block's lists fill several rounds of the warp's lanes
-// (rings58800, 30 near spheres: 12.1 -> 13.2 ms; shell2400k at 1 A, 141:
-// 291 -> 256 ms); otherwise a lane walks its row one lookup at a time.
+// (a 2.4 M-sphere shell at 1 A, 141 near spheres per sub-block: 291 -> 256
+// ms; a 58,800-sphere assembly at 0.25 A, 30: 12.1 -> 13.2 ms); otherwise a
+// lane walks its row one lookup at a time.
 template <bool MANY, bool WIDE>
 __device__ __forceinline__ void gather_item(uint32_t item, const DArr& A0, const DLat& L0, const int4* keys,
                                             const uint32_t* work, const GatherOut& O, const GatherCaps& caps,
@@ -2446,7 +2447,7 @@ cudaError_t launch_refine(const DArr& A, const DLat& L, const RefineConsts& RC, 
     // no region asked for): blocks of two warps that share one staging
     // region per sub-block.  A region then costs a warp half of what a region
     // of its own does, so the registers, not the shared memory, set the warps
-    // per SM (22 instead of 12 on rings58800's 16 KiB lists) and more warps
+    // per SM (24 instead of 12 with 16 KiB lists) and more warps
     // hide the evaluations' dependent latency; the edges and their outputs
     // are the same.
     if (!many && !g32 && region == 0 && P.cand_bytes <= PAIR_REGION_MAX) {
