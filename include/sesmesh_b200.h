@@ -228,13 +228,12 @@ int smb_batch_count_exact_ops(smb_batch* batch, unsigned long long* ops, char* e
 /* Shared memory per warp for one sub-block's f64 lists in smb_refine_exact
  * (1 KiB..48 KiB; default 13 KiB); larger sub-blocks go to warps with global list slabs. */
 int smb_batch_set_exact_region(smb_batch* batch, size_t bytes);
-/* Shared memory per warp for one sub-block's f32 lists in smb_refine
- * (1 KiB..56 KiB; 0, the default: the largest sub-block's lists, or an
- * eighth of the SM's shared memory when four of those do not fit in one);
- * larger sub-blocks go to a second pass that gives each a whole block.
- * With the default, groups of 8 and lists of at most 20 KiB, blocks of two
- * warps share one region per sub-block instead.  The roots do not depend
- * on it. */
+/* Shared memory for one sub-block's f32 lists in smb_refine, staged once
+ * for a block of two warps (1 KiB..56 KiB; 0, the default: the largest
+ * sub-block's lists when they fit 20 KiB and the groups are of 8 lanes,
+ * else an eighth of the SM's shared memory); larger sub-blocks go to a
+ * second pass that gives each a whole block.  The roots do not depend on
+ * it. */
 int smb_batch_set_refine_region(smb_batch* batch, size_t bytes);
 /* Lanes that evaluate one edge's points together in smb_refine and
  * smb_refine_warm: 8 or 32 (0, the default: 32 when the sub-blocks' lists
